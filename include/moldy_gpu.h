@@ -1,0 +1,188 @@
+/*
+ * moldy_gpu.h -- C ABI of the B200 (sm_100a) MOLDY EAM hot-path library.
+ *
+ * libmoldy_gpu.so replaces the bodies of the reference's hot-path Fortran
+ * subroutines (gjackland/moldy).  The reference has no argument-passing API:
+ * its routines act on module globals.  Each entry point below names the
+ * routine it replaces; a Fortran ISO_C_BINDING shim keeps the original
+ * names and copies the module globals in and out of these calls.
+ *
+ * Conventions (identical to the reference):
+ *  - FP64 everywhere at the boundary; int32 integers;
+ *  - positions x0,y0,z0 are fractional, x1 = B0^-1 v dt, x2 = B0^-1 a dt^2/2;
+ *  - 3x3 matrices are column-major, exactly Fortran's B0(3,3);
+ *  - atom and link-cell indices exported to the caller are 1-based;
+ *  - nlist is Fortran NLIST(nnbrs, nm): column i holds atom i's neighbours.
+ * Every call returns an int status (MOLDY_OK = 0); the message of the last
+ * failure on the calling thread is returned by moldy_gpu_last_error().
+ * A handle is not re-entrant: call it from one host thread at a time.
+ */
+#ifndef MOLDY_GPU_H
+#define MOLDY_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes ----------------------------------------------------------*/
+#define MOLDY_OK 0
+#define MOLDY_ERR_INVALID 1            /* bad argument */
+#define MOLDY_ERR_NEIGHBOUR_OVERFLOW 2 /* numn(i) > nnbrs: src/neighbourlist_m.F90:222-229 "stop" */
+#define MOLDY_ERR_SINGULAR_BOX 3       /* det(tg) == 0: src/matrix_m.F90:110-113 "stop" */
+#define MOLDY_ERR_CUDA 4               /* CUDA runtime failure (message has the CUDA error) */
+#define MOLDY_ERR_ORDER 5              /* call order, e.g. force before the potential is set
+                                          (src/fetransmetal.F90:110-113 exits here) */
+#define MOLDY_ERR_CAPACITY 6           /* an internal capacity was exceeded (message says which) */
+#define MOLDY_ERR_UNSUPPORTED 7        /* option not provided by this build */
+#define MOLDY_ERR_NO_DEVICE 8          /* no CUDA device, or the kernels were not built for it */
+
+/* precision of the pair arithmetic */
+#define MOLDY_PREC_FP64 0   /* all arithmetic in FP64 */
+#define MOLDY_PREC_MIXED 1  /* FP32 geometry/tables/pair forces, FP64 accumulation and state */
+
+/* Run parameters: the subset of simparameters (src/params_m.F90:44-162) the
+ * hot path reads, already in model units (src/params_m.F90:207-208,412,454). */
+typedef struct moldy_params {
+    double rnear;     /* neighbour radius rcut + rpad (src/moldin.F90:248) */
+    double deltat;    /* time step, model units */
+    double press;     /* external pressure, model units */
+    double bdel2;     /* deltat^2 / (2 * bmass * nm) (src/params_m.F90:207-208) */
+    int32_t nm;       /* number of atoms */
+    int32_t nnbrs;    /* neighbour-list capacity per atom (default 150) */
+    int32_t ivol;     /* 0 NPT, 1 NVE, 2 free z, 3 cluster, 4 z-only box, 5 pillar */
+    int32_t ntcm;     /* neighbour-list rebuild interval ("nbrupdate") */
+    int32_t ntc;      /* steps since the last rebuild (normally 0 at start) */
+    int32_t nlcx, nlcy, nlcz; /* link cells; 0 = derive as moldin does (src/moldin.F90:252-257) */
+    int32_t atomstress;       /* accumulate per-atom stress (src/dynamics_m.F90:279-283) */
+    int32_t precision;        /* MOLDY_PREC_FP64 or MOLDY_PREC_MIXED */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t reserved;
+} moldy_params;
+
+/* Results of one force evaluation: the module globals force() sets. */
+typedef struct moldy_force_out {
+    double pe;        /* potential energy (eV) */
+    double vol;       /* box volume (A^3) */
+    double tp[9];     /* configurational virial (src/dynamics_m.F90:288-296) */
+    double tk[9];     /* kinetic stress (src/thermostat_m.F90:127-164) */
+    double tc[9];     /* cofactors of B0 (src/dynamics_m.F90:365-373) */
+    double tg[9];     /* B0^T B0 */
+    double tgdot[9];  /* B0^T B1 + B1^T B0 */
+    double tgid[9];   /* tg^-1 tgdot used by the integrator */
+    double fb[9];     /* box force tk + tp - P tc (src/dynamics_m.F90:390-394) */
+    int32_t ntc;      /* rebuild counter after the call */
+    int32_t rebuilt;  /* 1 when this call rebuilt the neighbour list */
+} moldy_force_out;
+
+/* One mdloop iteration's thermodynamics (src/moldin.F90:760-791). */
+typedef struct moldy_thermo {
+    double ke, pe, te, h, th, vol;  /* eV, eV, eV, eV, eV, A^3 */
+    double s1, s2, s3;              /* update_therm_avs sums (src/dynamics_m.F90:649-734) */
+    double temp, boxke;             /* K, eV */
+    int32_t ntc, rebuilt;
+} moldy_thermo;
+
+typedef struct moldy_gpu moldy_gpu;
+
+/* lifecycle ---------------------------------------------------------------*/
+/* Allocates the device state for p->nm atoms (init_particles_m,
+ * init_neighbourlist_m, init_linkcell_m, init_dynamics_m). */
+int moldy_gpu_create(const moldy_params *p, moldy_gpu **out);
+int moldy_gpu_destroy(moldy_gpu *h);
+/* Message for the last failing call on this thread ("" if none). */
+const char *moldy_gpu_last_error(void);
+/* Library version string. */
+const char *moldy_gpu_version(void);
+
+/* potential ---------------------------------------------------------------*/
+/* FETRANSMETAL Fe-Fe from the pot_026_026.in coefficients: runs set_up_m
+ * (src/fetransmetal.F90:768-926) and, for uselookup != 0, builds the lookup_m
+ * tables with nlookup intervals (src/potential_m.F90:181-228,
+ * src/lookup_m.F90:161-251); uselookup == 0 evaluates the *_src functions
+ * exactly (src/potential_m.F90:272-280). */
+int moldy_gpu_set_fetm_fe(moldy_gpu *h, int32_t nv, const double *av, const double *rv,
+                          int32_t np, const double *ap, const double *rp,
+                          int32_t uselookup, int32_t nlookup);
+/* Caller-built lookup tables for one species pair (potential_set_lookup
+ * output): vee, dvee, phi, dphi on r in [rmin, rmax], emb, demb on rho in
+ * [rhomin, rhomax], each with nlookup+1 entries (0:nlookup). */
+int moldy_gpu_set_tables(moldy_gpu *h, int32_t nlookup, double rmin, double rmax,
+                         double rhomin, double rhomax, const double *vee,
+                         const double *dvee, const double *phi, const double *dphi,
+                         const double *emb, const double *demb);
+/* Copies the six tables back (any pointer may be NULL). */
+int moldy_gpu_get_tables(moldy_gpu *h, double *vee, double *dvee, double *phi,
+                         double *dphi, double *emb, double *demb);
+
+/* state (particles_m / parrinellorahman_m globals) ------------------------*/
+/* Any pointer may be NULL to leave that array unchanged. */
+int moldy_gpu_set_state(moldy_gpu *h, const double *x0, const double *y0, const double *z0,
+                        const double *x1, const double *y1, const double *z1,
+                        const double *x2, const double *y2, const double *z2,
+                        const double *b0, const double *b1, const double *b2,
+                        const int32_t *atomic_number, const double *atomic_mass,
+                        const double *del2, const double *tgid);
+int moldy_gpu_get_state(moldy_gpu *h, double *x0, double *y0, double *z0,
+                        double *x1, double *y1, double *z1,
+                        double *x2, double *y2, double *z2,
+                        double *b0, double *b1, double *b2, double *tgid);
+/* fx, fy, fz of dynamics_m (fractional forces; real force is B0 f) */
+int moldy_gpu_get_forces(moldy_gpu *h, double *fx, double *fy, double *fz);
+/* rho, afrho = F(rho), dafrho = F'(rho) of particles_m */
+int moldy_gpu_get_density(moldy_gpu *h, double *rho, double *afrho, double *dafrho);
+/* stressx/y/z of particles_m (only accumulated when atomstress != 0) */
+int moldy_gpu_get_atomstress(moldy_gpu *h, double *sx, double *sy, double *sz);
+int moldy_gpu_set_ntc(moldy_gpu *h, int32_t ntc);
+
+/* link cells and neighbour list ---------------------------------------------*/
+int moldy_gpu_linkup(moldy_gpu *h);   /* src/linkcell_m.F90:122-198 */
+int moldy_gpu_relink(moldy_gpu *h);   /* src/linkcell_m.F90:215-274 */
+/* l0(ncell), link(nm), ic(nm) exactly as linkcell_m holds them (1-based). */
+int moldy_gpu_get_linkcells(moldy_gpu *h, int32_t *l0, int32_t *link, int32_t *ic);
+/* src/neighbourlist_m.F90:103-276 */
+int moldy_gpu_update_neighbourlist(moldy_gpu *h);
+/* NLIST(nnbrs, nm) and NUMN(nm), entries 1-based, same order as the reference. */
+int moldy_gpu_get_neighbourlist(moldy_gpu *h, int32_t *nlist, int32_t *numn);
+
+/* the hot path --------------------------------------------------------------*/
+/* dynamics_m::force (src/dynamics_m.F90:135-401): rebuild schedule (ntc),
+ * rhoset, embed, pair and embedding forces, virial, tc, kinten, fb.
+ * out may be NULL; forces stay on the device (moldy_gpu_get_forces). */
+int moldy_gpu_force(moldy_gpu *h, moldy_force_out *out);
+/* quench_m::velocityverlet (src/quench_m.F90:562-624), one step. */
+int moldy_gpu_velocityverlet(moldy_gpu *h, moldy_force_out *out);
+/* dynamics_m::update_therm_avs (src/dynamics_m.F90:649-734): s123 = s1, s2, s3 */
+int moldy_gpu_update_therm_avs(moldy_gpu *h, double *s123);
+/* moldin strain-loop preparation (src/moldin.F90:445-477): force, then
+ * tgid = tg^-1 tgdot, x2 = del2 f - tgid x1 / 2, b2 = bdel2 fb. */
+int moldy_gpu_md_init(moldy_gpu *h, moldy_force_out *out);
+/* nsteps mdloop iterations (src/moldin.F90:752-791): velocityverlet,
+ * update_therm_avs, thermodynamics, relink when ntc wraps.  thermo (may be
+ * NULL) receives nsteps records. */
+int moldy_gpu_md_steps(moldy_gpu *h, int32_t nsteps, moldy_thermo *thermo);
+/* dynamics_m::energy_calc (src/dynamics_m.F90:412-483): per-atom energy with
+ * the exact pair function. */
+int moldy_gpu_energy_calc(moldy_gpu *h, double *en_atom);
+/* Waits for all work queued on the handle's stream. */
+int moldy_gpu_synchronize(moldy_gpu *h);
+
+/* instrumentation (no counterpart in the reference) --------------------------*/
+/* The cudaStream_t all of the handle's work is queued on. */
+int moldy_gpu_get_stream(moldy_gpu *h, void **stream);
+/* Per-kernel-family timing with CUDA events on that stream (off by default);
+ * launch counts are always kept. */
+int moldy_gpu_set_profiling(moldy_gpu *h, int32_t enable);
+int moldy_gpu_reset_kernel_stats(moldy_gpu *h);
+/* Accumulated device time (ms, when profiling) and kernel launches of one
+ * family since the last reset; kernel ids are 0 .. MOLDY_KERNEL_FAMILIES-1. */
+int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64_t *launches);
+const char *moldy_gpu_kernel_name(int32_t kernel);
+#define MOLDY_KERNEL_FAMILIES 13
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOLDY_GPU_H */

@@ -1,0 +1,901 @@
+// api.cu -- the Engine (host orchestration of one system on one GPU) and the
+// extern "C" entry points declared in include/moldy_gpu.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace moldy {
+
+int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv, int np,
+                      const double *ap, const double *rp, int uselookup, int nlookup);
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(MOLDY_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+int dev_alloc(T **p, size_t n, const char *what) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(MOLDY_ERR_CUDA, std::string("cudaMalloc ") + what + " (" +
+                                        std::to_string(n * sizeof(T)) + " bytes): " +
+                                        cudaGetErrorString(e));
+    }
+    return MOLDY_OK;
+}
+
+#define CHECK(call)                                                       \
+    do {                                                                  \
+        int rc_ = (call);                                                 \
+        if (rc_ != MOLDY_OK) return rc_;                                  \
+    } while (0)
+
+#define CUDA_CHECK(call, what)                                            \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what);                \
+    } while (0)
+
+__global__ void k_pack_pos(int nm, const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, int mask, double4 *__restrict__ pos) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    double4 p = pos[a];
+    if (mask & 1) p.x = x[a];
+    if (mask & 2) p.y = y[a];
+    if (mask & 4) p.z = z[a];
+    pos[a] = p;
+}
+
+__global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__restrict__ xyz) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    double4 p = pos[a];
+    xyz[a] = p.x;
+    xyz[nm + a] = p.y;
+    xyz[2 * nm + a] = p.z;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- Profiler --
+const char *const kKernelNames[K_COUNT] = {
+    "drift", "linkup", "relink", "build_nlist", "density", "embed_kinten", "pair_forces",
+    "finalize_force", "vv_second_half", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
+
+cudaEvent_t Profiler::get() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void Profiler::begin(int id, cudaStream_t s) {
+    if (!on) return;
+    open_id = id;
+    open_ev = get();
+    cudaEventRecord(open_ev, s);
+}
+
+void Profiler::end(int id, cudaStream_t s) {
+    if (!on || open_id != id || !open_ev) return;
+    cudaEvent_t b = get();
+    cudaEventRecord(b, s);
+    pending.push_back({id, open_ev, b});
+    open_id = -1;
+    open_ev = nullptr;
+}
+
+void Profiler::harvest() {
+    for (auto &p : pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) total_ms[p.id] += ms;
+        pool.push_back(p.a);
+        pool.push_back(p.b);
+    }
+    pending.clear();
+    cudaGetLastError();
+}
+
+void Profiler::reset() {
+    harvest();
+    for (int k = 0; k < K_COUNT; ++k) { launches[k] = 0; total_ms[k] = 0.0; }
+}
+
+Profiler::~Profiler() {
+    for (auto &p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+}
+
+// one launcher call = nk kernels of family id
+#define LAUNCH(E, id, nk, s, call)          \
+    do {                                    \
+        (E).prof.begin((id), (s));          \
+        call;                               \
+        (E).prof.end((id), (s));            \
+        (E).prof.launches[(id)] += (nk);    \
+    } while (0)
+
+// ------------------------------------------------------------------ Engine --
+Engine::Engine(const moldy_params &p) {
+    prm.rnear = p.rnear;
+    prm.deltat = p.deltat;
+    prm.press = p.press;
+    prm.bdel2 = p.bdel2;
+    prm.nm = p.nm;
+    prm.nnbrs = p.nnbrs;
+    prm.ivol = p.ivol;
+    prm.atomstress = p.atomstress;
+    prm.nlcx = p.nlcx;
+    prm.nlcy = p.nlcy;
+    prm.nlcz = p.nlcz;
+    prm.ncell = 0;
+    ntcm_ = p.ntcm;
+    ntc_ = p.ntc;
+    precision_ = p.precision;
+    device_ = p.device;
+    std::memset(&tab, 0, sizeof(tab));
+}
+
+Engine::~Engine() {
+    if (device_ >= 0) cudaSetDevice(device_);
+    void *bufs[] = {d.pos, d.x1, d.x2, d.f, d.rho, d.afrho, d.dafrho, d.stress, d.mass, d.del2,
+                    d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
+                    d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
+                    d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.tab_r4, d.tab_e2,
+                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (host_box_) cudaFreeHost(host_box_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+static int alloc_cells(Engine &E) {
+    Params &p = E.prm;
+    DeviceState &d = E.d;
+    p.ncell = p.nlcx * p.nlcy * p.nlcz;
+    int nc = p.ncell;
+    CHECK(dev_alloc(&d.cell_start, nc + 1, "cell_start"));
+    CHECK(dev_alloc(&d.cell_count, nc, "cell_count"));
+    CHECK(dev_alloc(&d.arr_count, nc, "arr_count"));
+    CHECK(dev_alloc(&d.arr_start, nc + 1, "arr_start"));
+    CHECK(dev_alloc(&d.new_count, nc, "new_count"));
+    CHECK(dev_alloc(&d.new_start, nc + 1, "new_start"));
+    return MOLDY_OK;
+}
+
+static int init_engine(Engine &E, int device) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MOLDY_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= ndev) return fail(MOLDY_ERR_INVALID, "device ordinal out of range");
+    CUDA_CHECK(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop;
+    CUDA_CHECK(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10) return fail(MOLDY_ERR_NO_DEVICE, "kernels are built for sm_100a only; device is sm_" +
+                                                              std::to_string(prop.major * 10 + prop.minor));
+    const Params &p = E.prm;
+    DeviceState &d = E.d;
+    size_t nm = (size_t)p.nm;
+    CHECK(dev_alloc(&d.pos, nm, "pos"));
+    CHECK(dev_alloc(&d.x1, 3 * nm, "x1"));
+    CHECK(dev_alloc(&d.x2, 3 * nm, "x2"));
+    CHECK(dev_alloc(&d.f, 3 * nm, "f"));
+    CHECK(dev_alloc(&d.rho, nm, "rho"));
+    CHECK(dev_alloc(&d.afrho, nm, "afrho"));
+    CHECK(dev_alloc(&d.dafrho, nm, "dafrho"));
+    CHECK(dev_alloc(&d.stress, 3 * nm, "stress"));
+    CHECK(dev_alloc(&d.mass, nm, "mass"));
+    CHECK(dev_alloc(&d.del2, nm, "del2"));
+    CHECK(dev_alloc(&d.znum, nm, "atomic_number"));
+    CHECK(dev_alloc(&d.en_atom, 3 * nm, "en_atom/staging"));
+    CHECK(dev_alloc(&d.ic, nm, "ic"));
+    CHECK(dev_alloc(&d.cell_atoms, nm, "cell_atoms"));
+    CHECK(dev_alloc(&d.cell_pos, nm, "cell_pos"));
+    CHECK(dev_alloc(&d.ic_new, nm, "ic_new"));
+    CHECK(dev_alloc(&d.arr_list, nm, "arr_list"));
+    CHECK(dev_alloc(&d.work, 2 * nm, "relink work"));
+    CHECK(dev_alloc(&d.cell_atoms2, nm, "cell_atoms2"));
+    CHECK(dev_alloc(&d.nlist, nm * (size_t)p.nnbrs, "nlist"));
+    CHECK(dev_alloc(&d.numn, nm, "numn"));
+    CHECK(dev_alloc(&d.partials, 2 * (size_t)kMaxBlocks * kPartials, "partials"));
+    CHECK(dev_alloc(&d.flags, 8, "flags"));
+    CHECK(dev_alloc(&d.box, 1, "box"));
+    CUDA_CHECK(cudaMemset(d.pos, 0, nm * sizeof(double4)), "memset pos");
+    CUDA_CHECK(cudaMemset(d.x1, 0, 3 * nm * sizeof(double)), "memset x1");
+    CUDA_CHECK(cudaMemset(d.x2, 0, 3 * nm * sizeof(double)), "memset x2");
+    CUDA_CHECK(cudaMemset(d.f, 0, 3 * nm * sizeof(double)), "memset f");
+    CUDA_CHECK(cudaMemset(d.rho, 0, nm * sizeof(double)), "memset rho");
+    CUDA_CHECK(cudaMemset(d.afrho, 0, nm * sizeof(double)), "memset afrho");
+    CUDA_CHECK(cudaMemset(d.dafrho, 0, nm * sizeof(double)), "memset dafrho");
+    CUDA_CHECK(cudaMemset(d.stress, 0, 3 * nm * sizeof(double)), "memset stress");
+    CUDA_CHECK(cudaMemset(d.numn, 0, nm * sizeof(int32_t)), "memset numn");
+    CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
+    CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
+    if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
+    return MOLDY_OK;
+}
+
+int Engine::check_ready() {
+    if (!potential_set_) return fail(MOLDY_ERR_ORDER, "the potential must be set (set_up) before force evaluation");
+    if (!state_set_) return fail(MOLDY_ERR_ORDER, "moldy_gpu_set_state must be called first");
+    if (prm.ncell == 0) return fail(MOLDY_ERR_ORDER, "link cells undefined: give nlcx/nlcy/nlcz or B0");
+    return MOLDY_OK;
+}
+
+int Engine::upload_tables() {
+    HostTables &h = ht;
+    int n = h.nlookup;
+    // first node from which all four r tables are zero to the end
+    int cut = n + 1;
+    for (int i = n; i >= 0; --i) {
+        if (h.vee[i] != 0.0 || h.dvee[i] != 0.0 || h.phi[i] != 0.0 || h.dphi[i] != 0.0) break;
+        cut = i;
+    }
+    int nr = (cut <= n - 1) ? cut + 2 : n + 1;
+    std::vector<double4> r4(nr);
+    std::vector<float4> r4f(nr);
+    for (int i = 0; i < nr; ++i) {
+        r4[i] = make_double4(h.vee[i], h.dvee[i], h.phi[i], h.dphi[i]);
+        r4f[i] = make_float4((float)h.vee[i], (float)h.dvee[i], (float)h.phi[i], (float)h.dphi[i]);
+    }
+    std::vector<double2> e2(n + 1);
+    std::vector<float2> e2f(n + 1);
+    for (int i = 0; i <= n; ++i) {
+        e2[i] = make_double2(h.emb[i], h.demb[i]);
+        e2f[i] = make_float2((float)h.emb[i], (float)h.demb[i]);
+    }
+    void *old[] = {d.tab_r4, d.tab_e2, d.tab_r4f, d.tab_e2f};
+    for (void *b : old)
+        if (b) cudaFree(b);
+    CHECK(dev_alloc(&d.tab_r4, nr, "tables"));
+    CHECK(dev_alloc(&d.tab_r4f, nr, "tables"));
+    CHECK(dev_alloc(&d.tab_e2, n + 1, "tables"));
+    CHECK(dev_alloc(&d.tab_e2f, n + 1, "tables"));
+    CUDA_CHECK(cudaMemcpy(d.tab_r4, r4.data(), nr * sizeof(double4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(d.tab_r4f, r4f.data(), nr * sizeof(float4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(d.tab_e2, e2.data(), (n + 1) * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(d.tab_e2f, e2f.data(), (n + 1) * sizeof(float2), cudaMemcpyHostToDevice), "tables");
+
+    Tables &t = tab;
+    t.r4 = d.tab_r4; t.e2 = d.tab_e2; t.r4f = d.tab_r4f; t.e2f = d.tab_e2f;
+    t.nlookup = n;
+    t.nr = nr;
+    t.idx_cut = cut;
+    t.exact = h.exact ? 1 : 0;
+    t.vp_rmin = h.rmin; t.vp_rmax = h.rmax;
+    t.vp_range = h.rmax - h.rmin;
+    t.vp_reciprange = 1.0 / t.vp_range;
+    t.vp_recipnlkp = 1.0 / (double)n;
+    t.vp_recipstep = (double)n / t.vp_range;
+    t.e_rmin = h.rhomin; t.e_rmax = h.rhomax;
+    t.e_range = h.rhomax - h.rhomin;
+    t.e_reciprange = 1.0 / t.e_range;
+    t.e_recipnlkp = 1.0 / (double)n;
+    t.e_recipstep = (double)n / t.e_range;
+    double rcull;
+    if (h.exact) {
+        rcull = 0.0;
+        for (int i = 0; i < h.nv; ++i) rcull = std::max(rcull, h.rv[i]);
+        for (int i = 0; i < h.np; ++i) rcull = std::max(rcull, h.rp[i]);
+    } else if (cut <= n - 1) {
+        rcull = h.rmin + (double)cut * t.vp_range * t.vp_recipnlkp;
+    } else {
+        rcull = 1.0e300;
+    }
+    double rc = rcull < 1e150 ? rcull * (1.0 + 1.0e-12) : 1.0e150;
+    t.rcull2 = rc * rc;
+    t.rcull2f = (float)(rc * rc * (1.0 + 1.0e-6));
+    t.nv = h.nv; t.np = h.np;
+    for (int i = 0; i < 8; ++i) { t.av[i] = h.av[i]; t.rv[i] = h.rv[i]; t.ap[i] = h.ap[i]; t.rp[i] = h.rp[i]; }
+    t.bier_cut1 = h.bier_cut1; t.bier_cut2 = h.bier_cut2;
+    for (int k = 0; k < 4; ++k) t.sc[k] = h.sc[k];
+    t.phi_cut1 = h.phi_cut1; t.phi_cut2 = h.phi_cut2;
+    t.bier_a = h.bier_a; t.bier_zed = h.bier_zed;
+    potential_set_ = true;
+    return MOLDY_OK;
+}
+
+int Engine::set_fetm(int nv, const double *av, const double *rv, int np, const double *ap,
+                     const double *rp, int uselookup, int nlookup) {
+    if (!av || !rv || !ap || !rp) return fail(MOLDY_ERR_INVALID, "null coefficient pointer");
+    int rc = build_fetm_tables(ht, nv, av, rv, np, ap, rp, uselookup, nlookup);
+    if (rc != MOLDY_OK) return fail(rc, "FETRANSMETAL set-up failed (coefficient counts 1..8, phi must have a maximum in [0,3])");
+    return upload_tables();
+}
+
+int Engine::set_tables(int nlookup, double rmin, double rmax, double rhomin, double rhomax,
+                       const double *vee, const double *dvee, const double *phi, const double *dphi,
+                       const double *emb, const double *demb) {
+    if (nlookup < 2) return fail(MOLDY_ERR_INVALID, "nlookup must be >= 2");
+    if (!vee || !dvee || !phi || !dphi || !emb || !demb) return fail(MOLDY_ERR_INVALID, "null table pointer");
+    if (!(rmax > rmin) || !(rhomax > rhomin)) return fail(MOLDY_ERR_INVALID, "empty table range");
+    size_t n = (size_t)nlookup + 1;
+    ht = HostTables();
+    ht.nlookup = nlookup;
+    ht.rmin = rmin; ht.rmax = rmax; ht.rhomin = rhomin; ht.rhomax = rhomax;
+    ht.vee.assign(vee, vee + n); ht.dvee.assign(dvee, dvee + n);
+    ht.phi.assign(phi, phi + n); ht.dphi.assign(dphi, dphi + n);
+    ht.emb.assign(emb, emb + n); ht.demb.assign(demb, demb + n);
+    ht.set = true;
+    return upload_tables();
+}
+
+int Engine::get_tables(double *vee, double *dvee, double *phi, double *dphi, double *emb, double *demb) {
+    if (!ht.set) return fail(MOLDY_ERR_ORDER, "no tables");
+    size_t n = (size_t)ht.nlookup + 1;
+    const std::vector<double> *src[] = {&ht.vee, &ht.dvee, &ht.phi, &ht.dphi, &ht.emb, &ht.demb};
+    double *dst[] = {vee, dvee, phi, dphi, emb, demb};
+    for (int k = 0; k < 6; ++k)
+        if (dst[k]) std::memcpy(dst[k], src[k]->data(), n * sizeof(double));
+    return MOLDY_OK;
+}
+
+int Engine::set_state(const double *x0, const double *y0, const double *z0, const double *x1,
+                      const double *y1, const double *z1, const double *x2, const double *y2,
+                      const double *z2, const double *b0, const double *b1, const double *b2,
+                      const int32_t *zn, const double *mass, const double *del2, const double *tgid) {
+    size_t nm = (size_t)prm.nm, nb = nm * sizeof(double);
+    cudaStream_t s = stream_;
+    if (x0 || y0 || z0) {
+        double *tmp = d.en_atom;   // 3*nm staging
+        if (x0) CUDA_CHECK(cudaMemcpyAsync(tmp, x0, nb, cudaMemcpyHostToDevice, s), "set x0");
+        if (y0) CUDA_CHECK(cudaMemcpyAsync(tmp + nm, y0, nb, cudaMemcpyHostToDevice, s), "set y0");
+        if (z0) CUDA_CHECK(cudaMemcpyAsync(tmp + 2 * nm, z0, nb, cudaMemcpyHostToDevice, s), "set z0");
+        int mask = (x0 ? 1 : 0) | (y0 ? 2 : 0) | (z0 ? 4 : 0);
+        k_pack_pos<<<(prm.nm + 255) / 256, 256, 0, s>>>(prm.nm, tmp, tmp + nm, tmp + 2 * nm, mask, d.pos);
+    }
+    const double *v1[3] = {x1, y1, z1}, *v2[3] = {x2, y2, z2};
+    for (int k = 0; k < 3; ++k) {
+        if (v1[k]) CUDA_CHECK(cudaMemcpyAsync(d.x1 + k * nm, v1[k], nb, cudaMemcpyHostToDevice, s), "set x1");
+        if (v2[k]) CUDA_CHECK(cudaMemcpyAsync(d.x2 + k * nm, v2[k], nb, cudaMemcpyHostToDevice, s), "set x2");
+    }
+    if (b0) CUDA_CHECK(cudaMemcpyAsync(d.box->b0, b0, 9 * sizeof(double), cudaMemcpyHostToDevice, s), "set b0");
+    if (b1) CUDA_CHECK(cudaMemcpyAsync(d.box->b1, b1, 9 * sizeof(double), cudaMemcpyHostToDevice, s), "set b1");
+    if (b2) CUDA_CHECK(cudaMemcpyAsync(d.box->b2, b2, 9 * sizeof(double), cudaMemcpyHostToDevice, s), "set b2");
+    if (tgid) CUDA_CHECK(cudaMemcpyAsync(d.box->tgid, tgid, 9 * sizeof(double), cudaMemcpyHostToDevice, s), "set tgid");
+    if (zn) CUDA_CHECK(cudaMemcpyAsync(d.znum, zn, nm * sizeof(int32_t), cudaMemcpyHostToDevice, s), "set atomic_number");
+    if (mass) CUDA_CHECK(cudaMemcpyAsync(d.mass, mass, nb, cudaMemcpyHostToDevice, s), "set atomic_mass");
+    if (del2) CUDA_CHECK(cudaMemcpyAsync(d.del2, del2, nb, cudaMemcpyHostToDevice, s), "set del2");
+    if (b0 && prm.ncell == 0) {
+        // src/moldin.F90:252-257: diagonal elements only, at least 3 cells
+        int n3[3];
+        for (int k = 0; k < 3; ++k) {
+            int v = (int)(b0[4 * k] / prm.rnear);
+            n3[k] = v < 3 ? 3 : v;
+        }
+        prm.nlcx = n3[0]; prm.nlcy = n3[1]; prm.nlcz = n3[2];
+        CHECK(alloc_cells(*this));
+    }
+    if (x0 && zn && mass && del2 && b0) state_set_ = true;
+    CUDA_CHECK(cudaStreamSynchronize(s), "set_state");
+    return MOLDY_OK;
+}
+
+int Engine::get_state(double *x0, double *y0, double *z0, double *x1, double *y1, double *z1,
+                      double *x2, double *y2, double *z2, double *b0, double *b1, double *b2,
+                      double *tgid) {
+    size_t nm = (size_t)prm.nm, nb = nm * sizeof(double);
+    cudaStream_t s = stream_;
+    if (x0 || y0 || z0) {
+        double *tmp = d.en_atom;
+        k_unpack_pos<<<(prm.nm + 255) / 256, 256, 0, s>>>(prm.nm, d.pos, tmp);
+        if (x0) CUDA_CHECK(cudaMemcpyAsync(x0, tmp, nb, cudaMemcpyDeviceToHost, s), "get x0");
+        if (y0) CUDA_CHECK(cudaMemcpyAsync(y0, tmp + nm, nb, cudaMemcpyDeviceToHost, s), "get y0");
+        if (z0) CUDA_CHECK(cudaMemcpyAsync(z0, tmp + 2 * nm, nb, cudaMemcpyDeviceToHost, s), "get z0");
+    }
+    double *v1[3] = {x1, y1, z1}, *v2[3] = {x2, y2, z2};
+    for (int k = 0; k < 3; ++k) {
+        if (v1[k]) CUDA_CHECK(cudaMemcpyAsync(v1[k], d.x1 + k * nm, nb, cudaMemcpyDeviceToHost, s), "get x1");
+        if (v2[k]) CUDA_CHECK(cudaMemcpyAsync(v2[k], d.x2 + k * nm, nb, cudaMemcpyDeviceToHost, s), "get x2");
+    }
+    if (b0) CUDA_CHECK(cudaMemcpyAsync(b0, d.box->b0, 9 * sizeof(double), cudaMemcpyDeviceToHost, s), "get b0");
+    if (b1) CUDA_CHECK(cudaMemcpyAsync(b1, d.box->b1, 9 * sizeof(double), cudaMemcpyDeviceToHost, s), "get b1");
+    if (b2) CUDA_CHECK(cudaMemcpyAsync(b2, d.box->b2, 9 * sizeof(double), cudaMemcpyDeviceToHost, s), "get b2");
+    if (tgid) CUDA_CHECK(cudaMemcpyAsync(tgid, d.box->tgid, 9 * sizeof(double), cudaMemcpyDeviceToHost, s), "get tgid");
+    CUDA_CHECK(cudaStreamSynchronize(s), "get_state");
+    return MOLDY_OK;
+}
+
+int Engine::get_array3(const double *dev, double *a, double *b, double *c) {
+    size_t nm = (size_t)prm.nm, nb = nm * sizeof(double);
+    double *o[3] = {a, b, c};
+    for (int k = 0; k < 3; ++k)
+        if (o[k]) CUDA_CHECK(cudaMemcpyAsync(o[k], dev + k * nm, nb, cudaMemcpyDeviceToHost, stream_), "get array");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "get array");
+    return MOLDY_OK;
+}
+
+int Engine::get_density(double *rho, double *afrho, double *dafrho) {
+    size_t nb = (size_t)prm.nm * sizeof(double);
+    if (rho) CUDA_CHECK(cudaMemcpyAsync(rho, d.rho, nb, cudaMemcpyDeviceToHost, stream_), "get rho");
+    if (afrho) CUDA_CHECK(cudaMemcpyAsync(afrho, d.afrho, nb, cudaMemcpyDeviceToHost, stream_), "get afrho");
+    if (dafrho) CUDA_CHECK(cudaMemcpyAsync(dafrho, d.dafrho, nb, cudaMemcpyDeviceToHost, stream_), "get dafrho");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "get density");
+    return MOLDY_OK;
+}
+
+int Engine::linkup() {
+    if (!state_set_) return fail(MOLDY_ERR_ORDER, "linkup before set_state");
+    if (prm.ncell == 0) return fail(MOLDY_ERR_ORDER, "link cells undefined");
+    LAUNCH(*this, K_LINKUP, 4, stream_, launch_linkup(d, prm, stream_));
+    cells_ready_ = true;
+    CUDA_CHECK(cudaGetLastError(), "linkup");
+    return MOLDY_OK;
+}
+
+int Engine::relink() {
+    if (!cells_ready_) return linkup();
+    LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
+    CUDA_CHECK(cudaGetLastError(), "relink");
+    return MOLDY_OK;
+}
+
+int Engine::get_linkcells(int32_t *l0, int32_t *link, int32_t *ic) {
+    if (!cells_ready_) return fail(MOLDY_ERR_ORDER, "link cells not built");
+    int32_t *dl0 = nullptr, *dlink = nullptr;
+    CHECK(dev_alloc(&dl0, prm.ncell, "export"));
+    int rc = dev_alloc(&dlink, prm.nm, "export");
+    if (rc != MOLDY_OK) { cudaFree(dl0); return rc; }
+    launch_export_linkcells(d, prm, dl0, dlink, stream_);
+    std::vector<int32_t> icv(prm.nm);
+    cudaMemcpyAsync(icv.data(), d.ic, prm.nm * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+    if (l0) cudaMemcpyAsync(l0, dl0, prm.ncell * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+    if (link) cudaMemcpyAsync(link, dlink, prm.nm * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+    cudaError_t e = cudaStreamSynchronize(stream_);
+    cudaFree(dl0);
+    cudaFree(dlink);
+    if (e != cudaSuccess) return cuda_fail(e, "get_linkcells");
+    if (ic)
+        for (int a = 0; a < prm.nm; ++a) ic[a] = icv[a] + 1;
+    return MOLDY_OK;
+}
+
+int Engine::check_flags() {
+    int32_t f[8];
+    CUDA_CHECK(cudaMemcpyAsync(f, d.flags, sizeof(f), cudaMemcpyDeviceToHost, stream_), "flags");
+    int32_t st = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&st, &d.box->status, sizeof(st), cudaMemcpyDeviceToHost, stream_), "flags");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "synchronize");
+    prof.harvest();
+    if (f[0]) {
+        cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
+        char msg[200];
+        std::snprintf(msg, sizeof msg,
+                      "attempt to list more than %d neighbours of atom %d: increase nnbrs "
+                      "(src/neighbourlist_m.F90:222-229)", prm.nnbrs, f[2]);
+        return fail(MOLDY_ERR_NEIGHBOUR_OVERFLOW, msg);
+    }
+    if (st) {
+        cudaMemsetAsync(&d.box->status, 0, sizeof(int32_t), stream_);
+        return fail(MOLDY_ERR_SINGULAR_BOX, "matrix_invert: determinant is zero (src/matrix_m.F90:110-113)");
+    }
+    return MOLDY_OK;
+}
+
+int Engine::update_neighbourlist() {
+    CHECK(check_ready());
+    if (!cells_ready_) CHECK(linkup());
+    LAUNCH(*this, K_NLIST, 1, stream_, launch_build_nlist(d, prm, stream_));
+    list_ready_ = true;
+    CUDA_CHECK(cudaGetLastError(), "update_neighbourlist");
+    return check_flags();
+}
+
+int Engine::get_neighbourlist(int32_t *nlist, int32_t *numn) {
+    if (!list_ready_) return fail(MOLDY_ERR_ORDER, "neighbour list not built");
+    size_t ne = (size_t)prm.nm * prm.nnbrs;
+    if (nlist) {
+        int32_t *tmp = nullptr;
+        CHECK(dev_alloc(&tmp, ne, "nlist export"));
+        launch_export_nlist(d, prm, tmp, stream_);
+        cudaError_t e = cudaMemcpyAsync(nlist, tmp, ne * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return cuda_fail(e, "get_neighbourlist");
+    }
+    if (numn) {
+        CUDA_CHECK(cudaMemcpyAsync(numn, d.numn, prm.nm * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "numn");
+        CUDA_CHECK(cudaStreamSynchronize(stream_), "numn");
+    }
+    return MOLDY_OK;
+}
+
+// Queues dynamics_m::force; mode 0 force, 1 velocity Verlet, 2 md_init.
+static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_ready, bool &list_ready,
+                       bool *rebuilt, cudaStream_t s) {
+    DeviceState &d = E.d;
+    const Params &p = E.prm;
+    ntc = ntc + 1;
+    bool rb = false;
+    if (ntc == 1 || !list_ready) {
+        if (!cells_ready) { LAUNCH(E, K_LINKUP, 4, s, launch_linkup(d, p, s)); cells_ready = true; }
+        LAUNCH(E, K_NLIST, 1, s, launch_build_nlist(d, p, s));
+        list_ready = true;
+        rb = true;
+    }
+    if (ntc == ntcm) ntc = 0;
+    size_t nm = (size_t)p.nm;
+    cudaMemsetAsync(d.rho, 0, nm * sizeof(double), s);
+    cudaMemsetAsync(d.f, 0, 3 * nm * sizeof(double), s);
+    if (p.atomstress) cudaMemsetAsync(d.stress, 0, 3 * nm * sizeof(double), s);
+    double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
+    LAUNCH(E, K_DENSITY, 1, s, launch_density(d, p, E.tab, s));
+    LAUNCH(E, K_EMBED, 1, s, launch_embed_kinten(d, p, E.tab, pe, s));
+    LAUNCH(E, K_PAIR, 1, s, launch_pair_forces(d, p, E.tab, pf, s));
+    LAUNCH(E, K_FINALIZE, 1, s,
+           launch_finalize_force(d, p, pe, grid_blocks(p.nm, kAtomThreads), pf,
+                                 grid_blocks((long long)p.nm * kPairTPA, 256), mode, s));
+    if (rebuilt) *rebuilt = rb;
+    return MOLDY_OK;
+}
+
+int Engine::force_device(bool *rebuilt) {
+    return queue_force(*this, 0, ntc_, ntcm_, cells_ready_, list_ready_, rebuilt, stream_);
+}
+
+int Engine::fetch_force_out(moldy_force_out *out) {
+    if (!host_box_) {
+        CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * 4), "pinned staging");
+        host_box_cap_ = 4;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(host_box_, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, stream_), "box");
+    CHECK(check_flags());
+    CUDA_CHECK(cudaGetLastError(), "force");
+    if (out) {
+        const BoxState &B = host_box_[0];
+        out->pe = B.pe;
+        out->vol = B.vol;
+        std::memcpy(out->tp, B.tp, sizeof(out->tp));
+        std::memcpy(out->tk, B.tk, sizeof(out->tk));
+        std::memcpy(out->tc, B.tc, sizeof(out->tc));
+        std::memcpy(out->tg, B.tg, sizeof(out->tg));
+        std::memcpy(out->tgdot, B.tgdot, sizeof(out->tgdot));
+        std::memcpy(out->tgid, B.tgid, sizeof(out->tgid));
+        std::memcpy(out->fb, B.fb, sizeof(out->fb));
+        out->ntc = ntc_;
+    }
+    return MOLDY_OK;
+}
+
+int Engine::force(moldy_force_out *out) {
+    CHECK(check_ready());
+    bool rb = false;
+    CHECK(force_device(&rb));
+    CHECK(fetch_force_out(out));
+    if (out) out->rebuilt = rb ? 1 : 0;
+    return MOLDY_OK;
+}
+
+int Engine::velocityverlet(moldy_force_out *out) {
+    CHECK(check_ready());
+    bool rb = false;
+    LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
+    CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
+    LAUNCH(*this, K_VV2, 1, stream_, launch_vv_second_half(d, prm, stream_));
+    CHECK(fetch_force_out(out));
+    if (out) out->rebuilt = rb ? 1 : 0;
+    return MOLDY_OK;
+}
+
+int Engine::update_therm_avs(double *s123) {
+    CHECK(check_ready());
+    int nb = 0;
+    LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));
+    LAUNCH(*this, K_THERM_FIN, 1, stream_, launch_finalize_therm(d, prm, nb, stream_));
+    if (!host_box_) {
+        CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * 4), "pinned staging");
+        host_box_cap_ = 4;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(host_box_, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, stream_), "box");
+    CHECK(check_flags());
+    if (s123) { s123[0] = host_box_[0].s1; s123[1] = host_box_[0].s2; s123[2] = host_box_[0].s3; }
+    return MOLDY_OK;
+}
+
+int Engine::md_init(moldy_force_out *out) {
+    CHECK(check_ready());
+    bool rb = false;
+    CHECK(queue_force(*this, 2, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
+    LAUNCH(*this, K_MDINIT, 1, stream_, launch_md_init_x2(d, prm, stream_));
+    CHECK(fetch_force_out(out));
+    if (out) out->rebuilt = rb ? 1 : 0;
+    return MOLDY_OK;
+}
+
+int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
+    CHECK(check_ready());
+    if (nsteps < 0) return fail(MOLDY_ERR_INVALID, "nsteps < 0");
+    if (thermo && host_box_cap_ < nsteps) {
+        if (host_box_) cudaFreeHost(host_box_);
+        host_box_ = nullptr;
+        CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * nsteps), "pinned staging");
+        host_box_cap_ = nsteps;
+    }
+    std::vector<int> ntcs(nsteps), rbs(nsteps);
+    for (int k = 0; k < nsteps; ++k) {
+        bool rb = false;
+        LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
+        CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
+        LAUNCH(*this, K_VV2, 1, stream_, launch_vv_second_half(d, prm, stream_));
+        int nb = 0;
+        LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));
+        LAUNCH(*this, K_THERM_FIN, 1, stream_, launch_finalize_therm(d, prm, nb, stream_));
+        if (thermo)
+            CUDA_CHECK(cudaMemcpyAsync(host_box_ + k, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost,
+                                       stream_), "thermo");
+        ntcs[k] = ntc_;
+        rbs[k] = rb ? 1 : 0;
+        if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
+    }
+    CUDA_CHECK(cudaGetLastError(), "md_steps launch");
+    CHECK(check_flags());
+    if (thermo) {
+        for (int k = 0; k < nsteps; ++k) {
+            const BoxState &B = host_box_[k];
+            moldy_thermo &t = thermo[k];
+            t.ke = B.ke; t.pe = B.pe; t.te = B.te; t.h = B.h; t.th = B.th; t.vol = B.vol;
+            t.s1 = B.s1; t.s2 = B.s2; t.s3 = B.s3; t.temp = B.temp; t.boxke = B.boxke;
+            t.ntc = ntcs[k]; t.rebuilt = rbs[k];
+        }
+    }
+    return MOLDY_OK;
+}
+
+int Engine::energy_calc(double *en_atom) {
+    CHECK(check_ready());
+    if (!ht.fetm) return fail(MOLDY_ERR_UNSUPPORTED, "energy_calc needs the analytic pair function (FETRANSMETAL set-up)");
+    if (!list_ready_) return fail(MOLDY_ERR_ORDER, "energy_calc before any force evaluation");
+    LAUNCH(*this, K_ENERGY, 1, stream_, launch_energy_calc(d, prm, tab, stream_));
+    if (en_atom) CUDA_CHECK(cudaMemcpyAsync(en_atom, d.en_atom, prm.nm * sizeof(double), cudaMemcpyDeviceToHost, stream_), "en_atom");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "energy_calc");
+    CUDA_CHECK(cudaGetLastError(), "energy_calc");
+    return MOLDY_OK;
+}
+
+int Engine::synchronize() {
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "synchronize");
+    prof.harvest();
+    return MOLDY_OK;
+}
+
+}  // namespace moldy
+
+// ================================================================ C ABI ====
+using moldy::Engine;
+using moldy::fail;
+
+struct moldy_gpu {
+    Engine *e;
+};
+
+#define GUARD(h)                                                                   \
+    do {                                                                           \
+        if (!(h) || !(h)->e) return fail(MOLDY_ERR_INVALID, "null handle");        \
+        cudaSetDevice((h)->e->device());                                          \
+    } while (0)
+
+#define TRY(expr)                                                                  \
+    try {                                                                          \
+        return (expr);                                                             \
+    } catch (const std::bad_alloc &) {                                             \
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");                 \
+    } catch (...) {                                                                \
+        return fail(MOLDY_ERR_INVALID, "unexpected exception");                    \
+    }
+
+namespace moldy {
+int engine_create(const moldy_params *p, Engine **out);
+}
+
+extern "C" {
+
+const char *moldy_gpu_last_error(void) { return moldy::g_last_error.c_str(); }
+
+const char *moldy_gpu_version(void) { return "moldy_b200 0.1 (sm_100a)"; }
+
+int moldy_gpu_create(const moldy_params *p, moldy_gpu **out) {
+    if (!p || !out) return fail(MOLDY_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (p->nm < 1) return fail(MOLDY_ERR_INVALID, "nm must be >= 1");
+    if (p->nnbrs < 1) return fail(MOLDY_ERR_INVALID, "nnbrs must be >= 1");
+    if (p->ivol < 0 || p->ivol > 5) return fail(MOLDY_ERR_INVALID, "ivol must be 0..5");
+    if (p->ntcm < 1) return fail(MOLDY_ERR_INVALID, "ntcm (nbrupdate) must be >= 1");
+    if (!(p->rnear > 0.0)) return fail(MOLDY_ERR_INVALID, "rnear must be > 0");
+    if (!(p->deltat > 0.0)) return fail(MOLDY_ERR_INVALID, "deltat must be > 0");
+    if ((p->nlcx || p->nlcy || p->nlcz) && (p->nlcx < 3 || p->nlcy < 3 || p->nlcz < 3))
+        return fail(MOLDY_ERR_INVALID, "link cells must be >= 3 per direction (src/moldin.F90:255-257)");
+    if (p->precision != MOLDY_PREC_FP64 && p->precision != MOLDY_PREC_MIXED)
+        return fail(MOLDY_ERR_INVALID, "precision must be MOLDY_PREC_FP64 or MOLDY_PREC_MIXED");
+    if ((long long)p->nm * (long long)p->nnbrs > (1LL << 40)) return fail(MOLDY_ERR_INVALID, "nm*nnbrs too large");
+    Engine *e = nullptr;
+    int rc;
+    try {
+        rc = moldy::engine_create(p, &e);
+    } catch (const std::bad_alloc &) {
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
+    if (rc != MOLDY_OK) return rc;
+    moldy_gpu *h = new (std::nothrow) moldy_gpu;
+    if (!h) { delete e; return fail(MOLDY_ERR_CAPACITY, "host allocation failed"); }
+    h->e = e;
+    *out = h;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_destroy(moldy_gpu *h) {
+    if (!h) return MOLDY_OK;
+    delete h->e;
+    delete h;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_set_fetm_fe(moldy_gpu *h, int32_t nv, const double *av, const double *rv, int32_t np,
+                          const double *ap, const double *rp, int32_t uselookup, int32_t nlookup) {
+    GUARD(h);
+    TRY(h->e->set_fetm(nv, av, rv, np, ap, rp, uselookup, nlookup));
+}
+
+int moldy_gpu_set_tables(moldy_gpu *h, int32_t nlookup, double rmin, double rmax, double rhomin,
+                         double rhomax, const double *vee, const double *dvee, const double *phi,
+                         const double *dphi, const double *emb, const double *demb) {
+    GUARD(h);
+    TRY(h->e->set_tables(nlookup, rmin, rmax, rhomin, rhomax, vee, dvee, phi, dphi, emb, demb));
+}
+
+int moldy_gpu_get_tables(moldy_gpu *h, double *vee, double *dvee, double *phi, double *dphi,
+                         double *emb, double *demb) {
+    GUARD(h);
+    TRY(h->e->get_tables(vee, dvee, phi, dphi, emb, demb));
+}
+
+int moldy_gpu_set_state(moldy_gpu *h, const double *x0, const double *y0, const double *z0,
+                        const double *x1, const double *y1, const double *z1, const double *x2,
+                        const double *y2, const double *z2, const double *b0, const double *b1,
+                        const double *b2, const int32_t *atomic_number, const double *atomic_mass,
+                        const double *del2, const double *tgid) {
+    GUARD(h);
+    TRY(h->e->set_state(x0, y0, z0, x1, y1, z1, x2, y2, z2, b0, b1, b2, atomic_number, atomic_mass,
+                        del2, tgid));
+}
+
+int moldy_gpu_get_state(moldy_gpu *h, double *x0, double *y0, double *z0, double *x1, double *y1,
+                        double *z1, double *x2, double *y2, double *z2, double *b0, double *b1,
+                        double *b2, double *tgid) {
+    GUARD(h);
+    TRY(h->e->get_state(x0, y0, z0, x1, y1, z1, x2, y2, z2, b0, b1, b2, tgid));
+}
+
+int moldy_gpu_get_forces(moldy_gpu *h, double *fx, double *fy, double *fz) {
+    GUARD(h);
+    TRY(h->e->get_array3(h->e->d.f, fx, fy, fz));
+}
+
+int moldy_gpu_get_density(moldy_gpu *h, double *rho, double *afrho, double *dafrho) {
+    GUARD(h);
+    TRY(h->e->get_density(rho, afrho, dafrho));
+}
+
+int moldy_gpu_get_atomstress(moldy_gpu *h, double *sx, double *sy, double *sz) {
+    GUARD(h);
+    TRY(h->e->get_array3(h->e->d.stress, sx, sy, sz));
+}
+
+int moldy_gpu_set_ntc(moldy_gpu *h, int32_t ntc) {
+    GUARD(h);
+    if (ntc < 0) return fail(MOLDY_ERR_INVALID, "ntc < 0");
+    h->e->set_ntc(ntc);
+    return MOLDY_OK;
+}
+
+int moldy_gpu_linkup(moldy_gpu *h) { GUARD(h); TRY(h->e->linkup()); }
+int moldy_gpu_relink(moldy_gpu *h) { GUARD(h); TRY(h->e->relink()); }
+
+int moldy_gpu_get_linkcells(moldy_gpu *h, int32_t *l0, int32_t *link, int32_t *ic) {
+    GUARD(h);
+    TRY(h->e->get_linkcells(l0, link, ic));
+}
+
+int moldy_gpu_update_neighbourlist(moldy_gpu *h) { GUARD(h); TRY(h->e->update_neighbourlist()); }
+
+int moldy_gpu_get_neighbourlist(moldy_gpu *h, int32_t *nlist, int32_t *numn) {
+    GUARD(h);
+    TRY(h->e->get_neighbourlist(nlist, numn));
+}
+
+int moldy_gpu_force(moldy_gpu *h, moldy_force_out *out) { GUARD(h); TRY(h->e->force(out)); }
+
+int moldy_gpu_velocityverlet(moldy_gpu *h, moldy_force_out *out) { GUARD(h); TRY(h->e->velocityverlet(out)); }
+
+int moldy_gpu_update_therm_avs(moldy_gpu *h, double *s123) { GUARD(h); TRY(h->e->update_therm_avs(s123)); }
+
+int moldy_gpu_md_init(moldy_gpu *h, moldy_force_out *out) { GUARD(h); TRY(h->e->md_init(out)); }
+
+int moldy_gpu_md_steps(moldy_gpu *h, int32_t nsteps, moldy_thermo *thermo) {
+    GUARD(h);
+    TRY(h->e->md_steps(nsteps, thermo));
+}
+
+int moldy_gpu_energy_calc(moldy_gpu *h, double *en_atom) { GUARD(h); TRY(h->e->energy_calc(en_atom)); }
+
+int moldy_gpu_synchronize(moldy_gpu *h) { GUARD(h); TRY(h->e->synchronize()); }
+
+int moldy_gpu_get_stream(moldy_gpu *h, void **stream) {
+    GUARD(h);
+    if (!stream) return fail(MOLDY_ERR_INVALID, "null argument");
+    *stream = (void *)h->e->stream_ref();
+    return MOLDY_OK;
+}
+
+int moldy_gpu_set_profiling(moldy_gpu *h, int32_t enable) {
+    GUARD(h);
+    h->e->prof.harvest();
+    h->e->prof.on = enable != 0;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_reset_kernel_stats(moldy_gpu *h) {
+    GUARD(h);
+    cudaStreamSynchronize(h->e->stream_ref());
+    h->e->prof.reset();
+    return MOLDY_OK;
+}
+
+int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64_t *launches) {
+    GUARD(h);
+    if (kernel < 0 || kernel >= moldy::K_COUNT) return fail(MOLDY_ERR_INVALID, "kernel id out of range");
+    cudaStreamSynchronize(h->e->stream_ref());
+    h->e->prof.harvest();
+    if (total_ms) *total_ms = h->e->prof.total_ms[kernel];
+    if (launches) *launches = h->e->prof.launches[kernel];
+    return MOLDY_OK;
+}
+
+const char *moldy_gpu_kernel_name(int32_t kernel) {
+    if (kernel < 0 || kernel >= moldy::K_COUNT) return "";
+    return moldy::kKernelNames[kernel];
+}
+
+}  // extern "C"
+
+namespace moldy {
+int engine_create(const moldy_params *p, Engine **out) {
+    Engine *e = new Engine(*p);
+    int rc = init_engine(*e, p->device);
+    if (rc == MOLDY_OK) {
+        cudaError_t ce = cudaStreamCreateWithFlags(&e->stream_ref(), cudaStreamNonBlocking);
+        if (ce != cudaSuccess) rc = cuda_fail(ce, "cudaStreamCreate");
+    }
+    if (rc != MOLDY_OK) {
+        delete e;
+        return rc;
+    }
+    *out = e;
+    return MOLDY_OK;
+}
+}  // namespace moldy

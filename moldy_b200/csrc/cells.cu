@@ -1,0 +1,250 @@
+// cells.cu -- link cells (linkcell_m) on the GPU.
+//
+// The reference keeps each link cell as a circular singly-linked chain
+// (l0 = chain start, link = successor, src/linkcell_m.F90:61-64).  Here a cell
+// is a CSR segment listing its atoms in chain traversal order starting at l0.
+// linkup (src/linkcell_m.F90:122-198) inserts atoms in index order, so every
+// segment is ascending.  relink (src/linkcell_m.F90:215-274) is a sequential
+// loop over atoms; its effect on one cell depends only on the removals from
+// and insertions into that cell, taken in atom-index order, so each cell is
+// replayed independently by one thread:
+//   remove x: the chain start moves to x's successor;
+//   insert i: i goes right after the current start and becomes the start.
+#include "engine.h"
+
+namespace moldy {
+
+__global__ void k_assign_cells(const double4 *__restrict__ pos, int nm, int nlcx, int nlcy,
+                               int nlcz, int32_t *__restrict__ ic_out,
+                               int32_t *__restrict__ count) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    double4 p = pos[a];
+    int ix = cell_coord(p.x, nlcx), iy = cell_coord(p.y, nlcy), iz = cell_coord(p.z, nlcz);
+    int c = ix + nlcx * iy + nlcx * nlcy * iz;
+    ic_out[a] = c;
+    if (count) atomicAdd(&count[c], 1);
+}
+
+__global__ void k_fill_cells(const int32_t *__restrict__ ic, int nm,
+                             const int32_t *__restrict__ start, int32_t *__restrict__ cursor,
+                             int32_t *__restrict__ atoms) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    int c = ic[a];
+    int k = atomicAdd(&cursor[c], 1);
+    atoms[start[c] + k] = a;
+}
+
+// ascending order inside each cell = linkup's chain order
+__global__ void k_sort_cells(int ncell, const int32_t *__restrict__ start,
+                             const int32_t *__restrict__ count, int32_t *__restrict__ atoms,
+                             int32_t *__restrict__ cell_pos) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int32_t *seg = atoms + start[c];
+    int n = count[c];
+    for (int i = 1; i < n; ++i) {
+        int v = seg[i], k = i - 1;
+        while (k >= 0 && seg[k] > v) { seg[k + 1] = seg[k]; --k; }
+        seg[k + 1] = v;
+    }
+    for (int i = 0; i < n; ++i) cell_pos[seg[i]] = i;
+}
+
+// single-block exclusive scan: out[0..n-1] exclusive sums, out[n] total
+__global__ void k_exclusive_scan(const int32_t *__restrict__ in, int32_t *__restrict__ out, int n) {
+    __shared__ int32_t wsum[32];
+    __shared__ int32_t carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < n ? in[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < nw) wsum[lane] = w;
+        }
+        __syncthreads();
+        int excl = carry + (warp > 0 ? wsum[warp - 1] : 0) + x - v;
+        if (i < n) out[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s) {
+    k_exclusive_scan<<<1, 1024, 0, s>>>(in, out, n);
+}
+
+void launch_linkup(DeviceState &d, const Params &p, cudaStream_t s) {
+    int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
+    int nbc = (p.ncell + kAtomThreads - 1) / kAtomThreads;
+    cudaMemsetAsync(d.cell_count, 0, sizeof(int32_t) * p.ncell, s);
+    k_assign_cells<<<nb, kAtomThreads, 0, s>>>(d.pos, p.nm, p.nlcx, p.nlcy, p.nlcz, d.ic, d.cell_count);
+    launch_exclusive_scan(d.cell_count, d.cell_start, p.ncell, s);
+    cudaMemsetAsync(d.new_count, 0, sizeof(int32_t) * p.ncell, s);
+    k_fill_cells<<<nb, kAtomThreads, 0, s>>>(d.ic, p.nm, d.cell_start, d.new_count, d.cell_atoms);
+    k_sort_cells<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms,
+                                              d.cell_pos);
+}
+
+// ------------------------------------------------------------------ relink --
+__global__ void k_relink_assign(const double4 *__restrict__ pos, int nm, int nlcx, int nlcy,
+                                int nlcz, const int32_t *__restrict__ ic,
+                                int32_t *__restrict__ ic_new, int32_t *__restrict__ arr_count) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    double4 p = pos[a];
+    int ix = cell_coord(p.x, nlcx), iy = cell_coord(p.y, nlcy), iz = cell_coord(p.z, nlcz);
+    int c = ix + nlcx * iy + nlcx * nlcy * iz;
+    ic_new[a] = c;
+    if (c != ic[a]) atomicAdd(&arr_count[c], 1);
+}
+
+__global__ void k_relink_arrivals(int nm, const int32_t *__restrict__ ic,
+                                  const int32_t *__restrict__ ic_new,
+                                  const int32_t *__restrict__ arr_start,
+                                  int32_t *__restrict__ cursor, int32_t *__restrict__ arr_list) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nm) return;
+    int c = ic_new[a];
+    if (c == ic[a]) return;
+    int k = atomicAdd(&cursor[c], 1);
+    arr_list[arr_start[c] + k] = a;
+}
+
+// Replays relink's chain surgery for one cell.  The working sequence W holds
+// the circular chain order; st is the position of the chain start.  W has
+// room for the old atoms plus all arrivals.
+__global__ void k_relink_cells(int ncell, const int32_t *__restrict__ cell_start,
+                               const int32_t *__restrict__ cell_count,
+                               const int32_t *__restrict__ cell_atoms,
+                               const int32_t *__restrict__ ic, const int32_t *__restrict__ ic_new,
+                               const int32_t *__restrict__ arr_start,
+                               int32_t *__restrict__ arr_count_rot, int32_t *__restrict__ arr_list,
+                               int32_t *__restrict__ work, int32_t *__restrict__ new_count) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int L = cell_count[c];
+    const int32_t *old = cell_atoms + cell_start[c];
+    int32_t *W = work + cell_start[c] + arr_start[c];
+    for (int k = 0; k < L; ++k) W[k] = old[k];
+    int na = arr_count_rot[c];
+    int32_t *A = arr_list + arr_start[c];
+    for (int i = 1; i < na; ++i) {   // arrivals in atom-index order
+        int v = A[i], k = i - 1;
+        while (k >= 0 && A[k] > v) { A[k + 1] = A[k]; --k; }
+        A[k + 1] = v;
+    }
+    int st = 0, ia = 0, last = -1;
+    const int kInf = 0x7fffffff;
+    for (;;) {
+        int lmin = kInf, lpos = -1;
+        for (int k = 0; k < L; ++k) {
+            int x = W[k];
+            if (x > last && x < lmin && ic[x] == c && ic_new[x] != c) { lmin = x; lpos = k; }
+        }
+        int nxt = ia < na ? A[ia] : kInf;
+        if (lmin == kInf && nxt == kInf) break;
+        if (lmin < nxt) {            // remove lmin; start moves to its successor
+            for (int k = lpos; k < L - 1; ++k) W[k] = W[k + 1];
+            --L;
+            st = (L == 0) ? 0 : (lpos < L ? lpos : 0);
+            last = lmin;
+        } else {                     // insert after the start; it becomes the start
+            if (L == 0) {
+                W[0] = nxt; L = 1; st = 0;
+            } else {
+                for (int k = L; k > st + 1; --k) W[k] = W[k - 1];
+                W[st + 1] = nxt;
+                ++L;
+                st = st + 1;
+            }
+            ++ia;
+        }
+    }
+    new_count[c] = L;
+    arr_count_rot[c] = st;
+}
+
+__global__ void k_relink_write(int ncell, const int32_t *__restrict__ cell_start,
+                               const int32_t *__restrict__ arr_start,
+                               const int32_t *__restrict__ rot, const int32_t *__restrict__ work,
+                               const int32_t *__restrict__ new_count,
+                               const int32_t *__restrict__ new_start, int32_t *__restrict__ atoms2,
+                               int32_t *__restrict__ cell_pos) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int L = new_count[c], st = rot[c];
+    const int32_t *W = work + cell_start[c] + arr_start[c];
+    int32_t *out = atoms2 + new_start[c];
+    for (int k = 0; k < L; ++k) {
+        int x = W[(st + k) % L];
+        out[k] = x;
+        cell_pos[x] = k;
+    }
+}
+
+void launch_relink(DeviceState &d, const Params &p, cudaStream_t s) {
+    int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
+    int nbc = (p.ncell + kAtomThreads - 1) / kAtomThreads;
+    cudaMemsetAsync(d.arr_count, 0, sizeof(int32_t) * p.ncell, s);
+    k_relink_assign<<<nb, kAtomThreads, 0, s>>>(d.pos, p.nm, p.nlcx, p.nlcy, p.nlcz, d.ic, d.ic_new,
+                                                d.arr_count);
+    launch_exclusive_scan(d.arr_count, d.arr_start, p.ncell, s);
+    cudaMemsetAsync(d.new_count, 0, sizeof(int32_t) * p.ncell, s);
+    k_relink_arrivals<<<nb, kAtomThreads, 0, s>>>(p.nm, d.ic, d.ic_new, d.arr_start, d.new_count,
+                                                  d.arr_list);
+    k_relink_cells<<<nbc, 128, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms, d.ic,
+                                       d.ic_new, d.arr_start, d.arr_count, d.arr_list, d.work,
+                                       d.new_count);
+    launch_exclusive_scan(d.new_count, d.new_start, p.ncell, s);
+    k_relink_write<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.arr_start, d.arr_count,
+                                                d.work, d.new_count, d.new_start, d.cell_atoms2,
+                                                d.cell_pos);
+    // commit (copies keep buffer addresses fixed for graph capture)
+    cudaMemcpyAsync(d.cell_atoms, d.cell_atoms2, sizeof(int32_t) * p.nm, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.cell_start, d.new_start, sizeof(int32_t) * (p.ncell + 1),
+                    cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.cell_count, d.new_count, sizeof(int32_t) * p.ncell, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.ic, d.ic_new, sizeof(int32_t) * p.nm, cudaMemcpyDeviceToDevice, s);
+}
+
+// -------------------------------------------------------------- export -----
+__global__ void k_export_cells(int ncell, const int32_t *__restrict__ start,
+                               const int32_t *__restrict__ count,
+                               const int32_t *__restrict__ atoms, int32_t *__restrict__ l0,
+                               int32_t *__restrict__ link) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int n = count[c];
+    const int32_t *seg = atoms + start[c];
+    l0[c] = n > 0 ? seg[0] + 1 : 0;
+    for (int k = 0; k < n; ++k) link[seg[k]] = seg[(k + 1) % n] + 1;
+}
+
+void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0, int32_t *link,
+                             cudaStream_t s) {
+    int nbc = (p.ncell + kAtomThreads - 1) / kAtomThreads;
+    k_export_cells<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms,
+                                                l0, link);
+}
+
+}  // namespace moldy

@@ -1,0 +1,313 @@
+// common.cuh -- device-side types and helpers shared by the MOLDY kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace moldy {
+
+// column-major 3x3 access with Fortran (1-based) indices, as B0(i,j)
+#define MAT(a, i, j) ((a)[((i) - 1) + 3 * ((j) - 1)])
+
+constexpr int kPartials = 32;   // doubles of per-block partial sums
+
+// Box tensors and scalar results held on the device so that a step needs no
+// host round trip (parrinellorahman_m module data, src/parrinellorahman_m.F90:102-115).
+struct BoxState {
+    double b0[9], b1[9], b2[9];
+    double tgid[9];                // tg^-1 tgdot from the last update_therm_avs
+    double tg[9], tgdot[9], tginv[9];
+    double tk[9], tp[9], tc[9], fb[9];
+    double vol, pe, pe_emb, pe_pair;
+    double s1, s2, s3, ke, te, h, th, boxke, temp;
+    double maxdisp;
+    int32_t status;                // nonzero: singular box in a device-side inversion
+    int32_t pad;
+};
+
+// Per-launch constant parameters.
+struct Params {
+    double rnear;
+    double deltat, press, bdel2;
+    int nm, nnbrs, ivol, atomstress;
+    int nlcx, nlcy, nlcz, ncell;
+};
+
+// Lookup-table description (lookup_m module data, src/lookup_m.F90:64-78).
+struct Tables {
+    const double4 *r4;      // per node (vee, dvee, phi, dphi), nodes 0..nr-1
+    const double2 *e2;      // per node (emb, demb), nodes 0..nlookup
+    const float4 *r4f;      // FP32 copy of r4 for the mixed path
+    const float2 *e2f;
+    int nlookup;            // intervals
+    int nr;                 // stored r nodes (culled tail removed)
+    int idx_cut;            // first node from which all r tables are zero
+    int exact;              // 1: evaluate *_src analytically, not from tables
+    double vp_rmin, vp_rmax, vp_range, vp_reciprange, vp_recipnlkp, vp_recipstep;
+    double e_rmin, e_rmax, e_range, e_reciprange, e_recipnlkp, e_recipstep;
+    double rcull2;          // pairs with r^2 above this contribute exactly zero
+    float rcull2f;
+    // FETRANSMETAL Fe-Fe analytic data for exact mode / energy_calc
+    int nv, np;
+    double av[8], rv[8], ap[8], rp[8];
+    double bier_cut1, bier_cut2, sc[4], phi_cut1, phi_cut2, bier_a, bier_zed;
+};
+
+#ifdef __CUDACC__
+// ------------------------------------------------------------- geometry --
+// Minimum image exactly as pr_get_realsep_from_dx (src/parrinellorahman_m.F90:149-173):
+// NINT rounds half away from zero, which is CUDA's round().
+__device__ __forceinline__ void min_image(int ivol, double &dx, double &dy, double &dz) {
+    if (ivol == 0 || ivol == 1 || ivol == 4) {
+        dx = __dsub_rn(dx, round(dx));
+        dy = __dsub_rn(dy, round(dy));
+        dz = __dsub_rn(dz, round(dz));
+    } else if (ivol == 2) {
+        dx = __dsub_rn(dx, round(dx));
+        dy = __dsub_rn(dy, round(dy));
+    } else if (ivol == 5) {
+        dz = __dsub_rn(dz, round(dz));
+    }
+}
+
+// Real separation with every product and sum rounded separately (no fused
+// multiply-add), so that the comparison r < rnear is bit-identical to the
+// reference's evaluation order.
+__device__ __forceinline__ double realsep_exact(const double *b, double dx, double dy, double dz) {
+    double rx = __dadd_rn(__dadd_rn(__dmul_rn(b[0], dx), __dmul_rn(b[3], dy)), __dmul_rn(b[6], dz));
+    double ry = __dadd_rn(__dadd_rn(__dmul_rn(b[1], dx), __dmul_rn(b[4], dy)), __dmul_rn(b[7], dz));
+    double rz = __dadd_rn(__dadd_rn(__dmul_rn(b[2], dx), __dmul_rn(b[5], dy)), __dmul_rn(b[8], dz));
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)));
+}
+
+// link-cell coordinate of a fractional position (src/linkcell_m.F90:150-152)
+__device__ __forceinline__ int cell_coord(double x, int nlc) {
+    const double hmeps = 0.4999999999;
+    return (int)__dmul_rn(__dadd_rn(__dsub_rn(x, round(x)), hmeps), (double)nlc);
+}
+
+// read-only (non-coherent) 32-byte load as two 16-byte halves
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 lo = __ldg(q), hi = __ldg(q + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+// ---------------------------------------------------------- table lookup --
+// get_value_from_lookup_veephi (src/lookup_m.F90:307-346) for the four r tables
+// at once; returns (vee, dvee, phi, dphi).
+__device__ __forceinline__ double4 lookup_r4(const Tables &t, double r) {
+    if (r >= t.vp_rmax) {
+        int n = t.nlookup < t.nr ? t.nlookup : t.nr - 1;
+        return ldg4(&t.r4[n]);
+    }
+    int idx = (int)(((double)t.nlookup * (r - t.vp_rmin)) * t.vp_reciprange);
+    if (idx >= t.nr - 1) return make_double4(0.0, 0.0, 0.0, 0.0);
+    idx = idx < 0 ? 0 : idx;   // r below rmin (the reference reads out of bounds)
+    double rlow = t.vp_rmin + (t.vp_range * (double)idx) * t.vp_recipnlkp;
+    double dr = (r - rlow) * t.vp_recipstep;
+    double4 a = ldg4(&t.r4[idx]);
+    double4 b = ldg4(&t.r4[idx + 1]);
+    double w = 1.0 - dr;
+    return make_double4(a.x * w + b.x * dr, a.y * w + b.y * dr, a.z * w + b.z * dr, a.w * w + b.w * dr);
+}
+
+__device__ __forceinline__ double lookup_phi(const Tables &t, double r) {
+    if (r >= t.vp_rmax) {
+        int n = t.nlookup < t.nr ? t.nlookup : t.nr - 1;
+        return __ldg(&t.r4[n].z);
+    }
+    int idx = (int)(((double)t.nlookup * (r - t.vp_rmin)) * t.vp_reciprange);
+    if (idx >= t.nr - 1) return 0.0;
+    idx = idx < 0 ? 0 : idx;
+    double rlow = t.vp_rmin + (t.vp_range * (double)idx) * t.vp_recipnlkp;
+    double dr = (r - rlow) * t.vp_recipstep;
+    return __ldg(&t.r4[idx].z) * (1.0 - dr) + __ldg(&t.r4[idx + 1].z) * dr;
+}
+
+// get_value_from_lookup_emb (src/lookup_m.F90:356-394) for (emb, demb)
+__device__ __forceinline__ double2 lookup_e2(const Tables &t, double rho) {
+    if (rho >= t.e_rmax) return __ldg(&t.e2[t.nlookup]);
+    int idx = (int)(((double)t.nlookup * (rho - t.e_rmin)) * t.e_reciprange);
+    idx = idx < 0 ? 0 : (idx > t.nlookup - 1 ? t.nlookup - 1 : idx);
+    double rlow = t.e_rmin + (t.e_range * (double)idx) * t.e_recipnlkp;
+    double dr = (rho - rlow) * t.e_recipstep;
+    double2 a = __ldg(&t.e2[idx]);
+    double2 b = __ldg(&t.e2[idx + 1]);
+    double w = 1.0 - dr;
+    return make_double2(a.x * w + b.x * dr, a.y * w + b.y * dr);
+}
+
+// FP32 variants for the mixed path (index arithmetic in FP32 as well)
+__device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
+    int idx = (int)(((float)t.nlookup * r) * (float)t.vp_reciprange);
+    if (idx >= t.nr - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
+    idx = idx < 0 ? 0 : idx;
+    float dr = r * (float)t.vp_recipstep - (float)idx;
+    float4 a = __ldg(&t.r4f[idx]);
+    float4 b = __ldg(&t.r4f[idx + 1]);
+    return make_float4(fmaf(b.x - a.x, dr, a.x), fmaf(b.y - a.y, dr, a.y),
+                       fmaf(b.z - a.z, dr, a.z), fmaf(b.w - a.w, dr, a.w));
+}
+
+__device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
+    int idx = (int)(((float)t.nlookup * r) * (float)t.vp_reciprange);
+    if (idx >= t.nr - 1) return 0.f;
+    idx = idx < 0 ? 0 : idx;
+    float dr = r * (float)t.vp_recipstep - (float)idx;
+    float a = __ldg(&t.r4f[idx].z);
+    float b = __ldg(&t.r4f[idx + 1].z);
+    return fmaf(b - a, dr, a);
+}
+
+// ------------------------------------------------ exact FETRANSMETAL Fe-Fe --
+// src/fetransmetal.F90:100-159 (vee_src) and 167-219 (dvee_src), Fe-Fe branch;
+// the Biersack screening length and prefactor come precomputed from the host.
+__device__ __forceinline__ double fetm_biersack(const Tables &t, double r) {
+    double x = r / t.bier_a;
+    double p = (double)0.1818f * exp(-((double)3.2f * x));
+    p = p + (double)0.5099f * exp(-((double)0.9423f * x));
+    p = p + (double)0.2802f * exp(-((double)0.4029f * x));
+    p = p + (double)0.02817f * exp(-((double)0.2016f * x));
+    return t.bier_zed * p / r;
+}
+
+__device__ __forceinline__ double fetm_dbiersack(const Tables &t, double r) {
+    double a = t.bier_a, x = r / a;
+    double s = (1.0 / r + 3.2 / a) * 0.1818 * exp(-(3.2 * x));
+    s = s + (1.0 / r + 0.9423 / a) * 0.5099 * exp(-(0.9423 * x));
+    s = s + (1.0 / r + 0.4029 / a) * 0.2802 * exp(-(0.4029 * x));
+    s = s + (1.0 / r + 0.2016 / a) * 0.02817 * exp(-(0.2016 * x));
+    return -((t.bier_zed / r) * s);
+}
+
+__device__ __forceinline__ void hermite_log_join(const Tables &t, double r, double &sp, double &ds) {
+    double a1 = t.bier_cut1, a2 = t.bier_cut2;
+    double vv1 = t.sc[1] / t.sc[0], xx1 = log(t.sc[0]);
+    double vv2 = t.sc[3] / t.sc[2], xx2 = log(t.sc[2]);
+    double h = a2 - a1;
+    double u = (r - a1) / h;
+    double h00 = ((2.0 * u) * u) * u - (3.0 * u) * u + 1.0;
+    double h10 = (u * u) * u - (2.0 * u) * u + u;
+    double h01 = -(((2.0 * u) * u) * u) + (3.0 * u) * u;
+    double h11 = (u * u) * u - u * u;
+    sp = h00 * xx1 + h10 * vv1 * h + h01 * xx2 + h11 * vv2 * h;
+    double d00 = (6.0 * u) * u - 6.0 * u;
+    double d10 = (3.0 * u) * u - 4.0 * u + 1.0;
+    double d01 = -((6.0 * u) * u) + 6.0 * u;
+    double d11 = (3.0 * u) * u - 2.0 * u;
+    ds = (d00 * xx1 + d10 * vv1 * h + d01 * xx2 + d11 * vv2 * h) / h;
+}
+
+__device__ __forceinline__ double fetm_vee(const Tables &t, double r) {
+    if (r > t.bier_cut2) {
+        double s = 0.0;
+        for (int i = 0; i < t.nv; ++i) {
+            double d = t.rv[i] - r;
+            if (d >= 0.0) s += t.av[i] * ((d * d) * d);
+        }
+        return s;
+    } else if (r > t.bier_cut1) {
+        double sp, ds;
+        hermite_log_join(t, r, sp, ds);
+        return exp(sp);
+    } else if (r < t.bier_cut1) {
+        return fetm_biersack(t, r);
+    }
+    return 0.0;
+}
+
+__device__ __forceinline__ double fetm_dvee(const Tables &t, double r) {
+    if (r > t.bier_cut2) {
+        double s = 0.0;
+        for (int i = 0; i < t.nv; ++i) {
+            double d = t.rv[i] - r;
+            if (d >= 0.0) s -= 3.0 * t.av[i] * (d * d);
+        }
+        return s;
+    } else if (r > t.bier_cut1) {
+        double sp, ds;
+        hermite_log_join(t, r, sp, ds);
+        return ds * exp(sp);
+    } else if (r < t.bier_cut1) {
+        return fetm_dbiersack(t, r);
+    }
+    return 0.0;
+}
+
+// src/fetransmetal.F90:227-366: phi flat below its maximum
+__device__ __forceinline__ double fetm_phi(const Tables &t, double r) {
+    if (r < t.phi_cut1) return t.phi_cut2;
+    double s = 0.0;
+    for (int i = 0; i < t.np; ++i) {
+        double d = t.rp[i] - r;
+        if (d >= 0.0) s += t.ap[i] * ((d * d) * d);
+    }
+    return s;
+}
+
+__device__ __forceinline__ double fetm_dphi(const Tables &t, double r) {
+    if (r < t.phi_cut1) return 0.0;
+    double s = 0.0;
+    for (int i = 0; i < t.np; ++i) {
+        double d = t.rp[i] - r;
+        if (d >= 0.0) s -= 3.0 * t.ap[i] * (d * d);
+    }
+    return s;
+}
+
+// (vee, dvee, phi, dphi) at r through the table or the exact functions
+__device__ __forceinline__ double4 pair_funcs(const Tables &t, double r) {
+    if (t.exact) return make_double4(fetm_vee(t, r), fetm_dvee(t, r), fetm_phi(t, r), fetm_dphi(t, r));
+    return lookup_r4(t, r);
+}
+
+__device__ __forceinline__ double density_func(const Tables &t, double r) {
+    if (t.exact) return fetm_phi(t, r);
+    return lookup_phi(t, r);
+}
+
+// (F(rho), F'(rho)): src/fetransmetal.F90:375-404 or the emb tables
+__device__ __forceinline__ double2 embed_funcs(const Tables &t, double rho) {
+    if (t.exact) {
+        double f = -(1.0 * sqrt(rho > 0.0 ? rho : 0.0));
+        double d = rho > 0.0 ? -(0.5 / sqrt(rho)) : 0.0;
+        return make_double2(f, d);
+    }
+    return lookup_e2(t, rho);
+}
+
+// ------------------------------------------------------------ reductions --
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV values per thread into partials[blockIdx.x*kPartials + off + k].
+// Deterministic: fixed shuffle tree, then warps in order.
+template <int NV>
+__device__ __forceinline__ void block_partials(double (&v)[NV], double *partials, int off) {
+    __shared__ double sm[32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double s = warp_sum(v[k]);
+        if (lane == 0) sm[warp][k] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double s = lane < nw ? sm[lane][k] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) partials[(size_t)blockIdx.x * kPartials + off + k] = s;
+        }
+    }
+    __syncthreads();
+}
+
+#endif  // __CUDACC__
+
+}  // namespace moldy

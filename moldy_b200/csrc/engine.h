@@ -1,0 +1,184 @@
+// engine.h -- host-side state of one MOLDY system on one GPU.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/moldy_gpu.h"
+#include "common.cuh"
+
+namespace moldy {
+
+// Device buffers of one system.  Atom arrays are in the reference's atom
+// order; the link-cell structure is a CSR over cells whose segments list each
+// cell's atoms in the reference's chain (traversal) order.
+struct DeviceState {
+    // particles_m
+    double4 *pos = nullptr;       // (x0, y0, z0, -)
+    double *x1 = nullptr;         // 3*nm, SoA x|y|z
+    double *x2 = nullptr;         // 3*nm
+    double *f = nullptr;          // 3*nm fx|fy|fz
+    double *rho = nullptr, *afrho = nullptr, *dafrho = nullptr;
+    double *stress = nullptr;     // 3*nm
+    double *mass = nullptr, *del2 = nullptr;
+    int32_t *znum = nullptr;
+    double *en_atom = nullptr;
+    // link cells (linkcell_m)
+    int32_t *ic = nullptr;        // cell of each atom, 0-based
+    int32_t *cell_start = nullptr, *cell_atoms = nullptr, *cell_pos = nullptr;
+    int32_t *cell_count = nullptr;
+    // relink scratch
+    int32_t *ic_new = nullptr, *arr_count = nullptr, *arr_start = nullptr, *arr_list = nullptr;
+    int32_t *work = nullptr, *new_count = nullptr, *new_start = nullptr, *cell_atoms2 = nullptr;
+    // neighbour list (neighbourlist_m): nlist[i*nnbrs + k], 0-based atom ids
+    int32_t *nlist = nullptr, *numn = nullptr;
+    // mixed-precision mirror of positions
+    float4 *posf = nullptr;
+    // tables
+    double4 *tab_r4 = nullptr;
+    double2 *tab_e2 = nullptr;
+    float4 *tab_r4f = nullptr;
+    float2 *tab_e2f = nullptr;
+    // reductions, flags and box state
+    double *partials = nullptr;
+    int32_t *flags = nullptr;     // [0] neighbour overflow, [1] cell capacity, [2] overflow atom
+    BoxState *box = nullptr;
+    int32_t *scan_tmp = nullptr;
+};
+
+// Host-side table data (potential_m / lookup_m).
+struct HostTables {
+    bool set = false;
+    int nlookup = 0;
+    std::vector<double> vee, dvee, phi, dphi, emb, demb;
+    double rmin = 0, rmax = 6, rhomin = 0, rhomax = 10000;
+    bool fetm = false;      // FETRANSMETAL analytic data available
+    bool exact = false;     // evaluate analytically
+    int nv = 0, np = 0;
+    double av[8] = {0}, rv[8] = {0}, ap[8] = {0}, rp[8] = {0};
+    double bier_cut1 = 0, bier_cut2 = 0, sc[4] = {0, 0, 0, 0};
+    double phi_cut1 = 0, phi_cut2 = 0, bier_a = 0, bier_zed = 0;
+};
+
+// Kernel families timed by the optional per-kernel CUDA-event profiler.
+enum KernelId {
+    K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_EMBED, K_PAIR, K_FINALIZE,
+    K_VV2, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_COUNT
+};
+extern const char *const kKernelNames[K_COUNT];
+
+// Counts launches per kernel family; when enabled, brackets each launch with
+// CUDA events on the engine's stream and accumulates the elapsed times.
+struct Profiler {
+    bool on = false;
+    long long launches[K_COUNT] = {0};
+    double total_ms[K_COUNT] = {0};
+    std::vector<cudaEvent_t> pool;
+    struct Pending { int id; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    int open_id = -1;
+    cudaEvent_t open_ev = nullptr;
+    cudaEvent_t get();
+    void begin(int id, cudaStream_t s);
+    void end(int id, cudaStream_t s);
+    void harvest();          // after a stream synchronisation
+    void reset();
+    ~Profiler();
+};
+
+class Engine {
+  public:
+    explicit Engine(const moldy_params &p);
+    ~Engine();
+
+    int set_fetm(int nv, const double *av, const double *rv, int np, const double *ap,
+                 const double *rp, int uselookup, int nlookup);
+    int set_tables(int nlookup, double rmin, double rmax, double rhomin, double rhomax,
+                   const double *vee, const double *dvee, const double *phi, const double *dphi,
+                   const double *emb, const double *demb);
+    int get_tables(double *vee, double *dvee, double *phi, double *dphi, double *emb, double *demb);
+    int set_state(const double *x0, const double *y0, const double *z0, const double *x1,
+                  const double *y1, const double *z1, const double *x2, const double *y2,
+                  const double *z2, const double *b0, const double *b1, const double *b2,
+                  const int32_t *zn, const double *mass, const double *del2, const double *tgid);
+    int get_state(double *x0, double *y0, double *z0, double *x1, double *y1, double *z1,
+                  double *x2, double *y2, double *z2, double *b0, double *b1, double *b2,
+                  double *tgid);
+    int get_array3(const double *dev, double *a, double *b, double *c);
+    int get_density(double *rho, double *afrho, double *dafrho);
+    int linkup();
+    int relink();
+    int get_linkcells(int32_t *l0, int32_t *link, int32_t *ic);
+    int update_neighbourlist();
+    int get_neighbourlist(int32_t *nlist, int32_t *numn);
+    int force(moldy_force_out *out);
+    int velocityverlet(moldy_force_out *out);
+    int update_therm_avs(double *s123);
+    int md_init(moldy_force_out *out);
+    int md_steps(int nsteps, moldy_thermo *thermo);
+    int energy_calc(double *en_atom);
+    int synchronize();
+    void set_ntc(int ntc) { ntc_ = ntc; }
+    cudaStream_t &stream_ref() { return stream_; }
+    Profiler prof;
+    int device() const { return device_; }
+
+    DeviceState d;
+    Params prm;
+    HostTables ht;
+    Tables tab;
+
+  private:
+    int check_ready();
+    int upload_tables();
+    int force_device(bool *rebuilt);     // queue force on the stream
+    int fetch_force_out(moldy_force_out *out);
+    int check_flags();
+
+    cudaStream_t stream_ = nullptr;
+    int device_ = 0;
+    int ntcm_ = 1, ntc_ = 0;
+    int precision_ = MOLDY_PREC_FP64;
+    bool state_set_ = false, cells_ready_ = false, list_ready_ = false;
+    bool potential_set_ = false;
+    double *part_embed_ = nullptr, *part_force_ = nullptr;   // slices of d.partials
+    BoxState *host_box_ = nullptr;                            // pinned staging
+    int host_box_cap_ = 0;
+};
+
+constexpr int kAtomThreads = 256;
+constexpr int kPairTPA = 8;            // threads per atom in the pair passes
+constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
+
+inline int grid_blocks(long long work, int threads) {
+    long long nb = (work + threads - 1) / threads;
+    if (nb < 1) nb = 1;
+    return (int)(nb < kMaxBlocks ? nb : kMaxBlocks);
+}
+
+// kernel launchers (defined in the .cu files)
+void launch_linkup(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_relink(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s);
+void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0, int32_t *link,
+                             cudaStream_t s);
+void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
+void launch_density(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
+void launch_embed_kinten(DeviceState &d, const Params &p, const Tables &t, double *partials,
+                         cudaStream_t s);
+void launch_pair_forces(DeviceState &d, const Params &p, const Tables &t, double *partials,
+                        cudaStream_t s);
+void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
+                           const double *part_force, int nblk_force, int mode, cudaStream_t s);
+void launch_drift(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_vv_second_half(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
+int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);
+void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
+
+}  // namespace moldy

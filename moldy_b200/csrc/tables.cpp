@@ -1,0 +1,188 @@
+// tables.cpp -- FETRANSMETAL Fe-Fe set-up and the lookup_m tables, built once
+// on the host and uploaded (the reference also builds them on the host,
+// src/potential_m.F90:181-228).
+//
+// The Fe-Fe functions (src/fetransmetal.F90):
+//   V(r)   = sum_k a_k (r_k - r)^3 H(r_k - r)                 r > bier_cut2
+//          = exp(cubic Hermite in log V) joining Biersack to V  bier_cut1 < r < bier_cut2
+//          = Biersack-Ziegler screened Coulomb                  r < bier_cut1
+//   phi(r) = sum_k A_k (R_k - r)^3 H(R_k - r), held flat below its maximum
+//   F(rho) = -sqrt(rho)
+// The reference writes several constants as default-REAL (single precision)
+// literals inside double expressions; those promotions are kept because they
+// change table bits (bier_cut1 = 0.9 is 0.89999997615814209 in double).
+// Host code is compiled without floating-point contraction.
+#include <cmath>
+
+#include "engine.h"
+
+namespace moldy {
+namespace {
+
+struct FeFe {
+    int nv, np;
+    const double *av, *rv, *ap, *rp;
+    double cut1, cut2, join[4], phi_top_r, phi_top_v;
+    double a_screen, zed;
+
+    static double step(double x) { return x < 0.0 ? 0.0 : 1.0; }
+
+    // Biersack-Ziegler (src/fetransmetal.F90:414-454) for Z1 = Z2 = 26
+    void screening() {
+        const double electron = 1.602176487e-19, angstrom = 1.0e-10;
+        zed = (double)(26 * 26) * 8.98755178e9 * electron / angstrom;
+        float p = powf(26.0f, 0.666666667f);
+        float a = (0.8854f * 0.529f) / powf(p + p, 0.5f);
+        a_screen = (double)a;
+    }
+    double biersack(double r) const {
+        double x = r / a_screen;
+        double s = (double)0.1818f * std::exp(-((double)3.2f * x));
+        s = s + (double)0.5099f * std::exp(-((double)0.9423f * x));
+        s = s + (double)0.2802f * std::exp(-((double)0.4029f * x));
+        s = s + (double)0.02817f * std::exp(-((double)0.2016f * x));
+        return zed * s / r;
+    }
+    double dbiersack(double r) const {
+        double a = a_screen, x = r / a;
+        double s = (1.0 / r + 3.2 / a) * 0.1818 * std::exp(-(3.2 * x));
+        s = s + (1.0 / r + 0.9423 / a) * 0.5099 * std::exp(-(0.9423 * x));
+        s = s + (1.0 / r + 0.4029 / a) * 0.2802 * std::exp(-(0.4029 * x));
+        s = s + (1.0 / r + 0.2016 / a) * 0.02817 * std::exp(-(0.2016 * x));
+        return -((zed / r) * s);
+    }
+    // log-space cubic Hermite join, value (src/fetransmetal.F90:511-528) and
+    // derivative (530-551); t is the reduced coordinate on [cut1, cut2]
+    void join_eval(double r, double *v, double *dv) const {
+        double a1 = cut1, a2 = cut2, h = a2 - a1;
+        double s1 = join[1] / join[0], l1 = std::log(join[0]);
+        double s2 = join[3] / join[2], l2 = std::log(join[2]);
+        double t = (r - a1) / h;
+        double e = (((2.0 * t) * t) * t - (3.0 * t) * t + 1.0) * l1 +
+                   ((t * t) * t - (2.0 * t) * t + t) * s1 * h;
+        e = e + (-(((2.0 * t) * t) * t) + (3.0 * t) * t) * l2;
+        e = e + ((t * t) * t - t * t) * s2 * h;
+        if (v) *v = std::exp(e);
+        if (dv) {
+            double d = ((6.0 * t) * t - 6.0 * t) * l1 + ((3.0 * t) * t - 4.0 * t + 1.0) * s1 * h;
+            d = d + (-((6.0 * t) * t) + 6.0 * t) * l2;
+            d = d + ((3.0 * t) * t - 2.0 * t) * s2 * h;
+            d = d / h;
+            *dv = d * std::exp(e);
+        }
+    }
+    double pair_poly(double r) const {
+        double s = 0.0;
+        for (int i = 0; i < nv; ++i) {
+            double d = rv[i] - r;
+            s = s + av[i] * ((d * d) * d) * step(d);
+        }
+        return s;
+    }
+    double dpair_poly(double r) const {
+        double s = 0.0;
+        for (int i = 0; i < nv; ++i) {
+            double d = rv[i] - r;
+            s = s - 1.0 * 3.0 * av[i] * (d * d) * step(d);
+        }
+        return s;
+    }
+    double dens_poly(double r) const {
+        double s = 0.0;
+        for (int i = 0; i < np; ++i) {
+            double d = rp[i] - r;
+            s = s + ap[i] * ((d * d) * d) * step(d);
+        }
+        return s;
+    }
+    double ddens_poly(double r) const {
+        double s = 0.0;
+        for (int i = 0; i < np; ++i) {
+            double d = rp[i] - r;
+            s = s - 3.0 * 1.0 * ap[i] * (d * d) * step(d);
+        }
+        return s;
+    }
+    double vee(double r) const {
+        if (r > cut2) return pair_poly(r);
+        if (r > cut1) { double v; join_eval(r, &v, nullptr); return v; }
+        if (r < cut1) return biersack(r);
+        return 0.0;
+    }
+    double dvee(double r) const {
+        if (r > cut2) return dpair_poly(r);
+        if (r > cut1) { double d; join_eval(r, nullptr, &d); return d; }
+        if (r < cut1) return dbiersack(r);
+        return 0.0;
+    }
+    double phi(double r) const { return r < phi_top_r ? phi_top_v : dens_poly(r); }
+    double dphi(double r) const { return r < phi_top_r ? 0.0 : ddens_poly(r); }
+
+    // set_up_m (src/fetransmetal.F90:768-926) for the Fe-Fe pair
+    bool set_up() {
+        cut1 = (double)0.9f;
+        cut2 = (double)1.9f;
+        screening();
+        const double eps = (double)0.000000000001f;
+        join[0] = biersack(cut1 - eps);
+        join[1] = dbiersack(cut1 - eps);
+        join[2] = pair_poly(cut2 + eps);
+        join[3] = dpair_poly(cut2 + eps);
+        // maximum of phi by 500 bisection steps on its slope over [0, 3]
+        double lo = 0.0, hi = 3.0;
+        if (ddens_poly(lo) < 0.0 || ddens_poly(hi) >= 0.0) return false;
+        for (int i = 0; i < 500; ++i) {
+            double mid = (hi + lo) / 2.0;
+            if (ddens_poly(mid) > 0.0) lo = mid; else hi = mid;
+        }
+        phi_top_r = (hi + lo) / 2.0;
+        phi_top_v = dens_poly(phi_top_r);
+        return true;
+    }
+};
+
+}  // namespace
+
+// Builds ht from the Fe-Fe knots; returns MOLDY_OK or an error code.
+int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv, int np,
+                      const double *ap, const double *rp, int uselookup, int nlookup) {
+    if (nv < 1 || nv > 8 || np < 1 || np > 8) return MOLDY_ERR_INVALID;
+    FeFe f{nv, np, av, rv, ap, rp};
+    if (!f.set_up()) return MOLDY_ERR_INVALID;
+    ht.fetm = true;
+    ht.exact = (uselookup == 0);
+    ht.nv = nv; ht.np = np;
+    for (int i = 0; i < nv; ++i) { ht.av[i] = av[i]; ht.rv[i] = rv[i]; }
+    for (int i = 0; i < np; ++i) { ht.ap[i] = ap[i]; ht.rp[i] = rp[i]; }
+    ht.bier_cut1 = f.cut1; ht.bier_cut2 = f.cut2;
+    for (int k = 0; k < 4; ++k) ht.sc[k] = f.join[k];
+    ht.phi_cut1 = f.phi_top_r; ht.phi_cut2 = f.phi_top_v;
+    ht.bier_a = f.a_screen; ht.bier_zed = f.zed;
+    // tables are built in both modes (exact mode uses them for nothing but
+    // moldy_gpu_get_tables)
+    if (nlookup < 2) nlookup = 5000;
+    ht.nlookup = nlookup;
+    ht.rmin = 0.0; ht.rmax = 6.0; ht.rhomin = 0.0; ht.rhomax = 10000.0;
+    size_t n = (size_t)nlookup + 1;
+    ht.vee.assign(n, 0.0); ht.dvee.assign(n, 0.0); ht.phi.assign(n, 0.0); ht.dphi.assign(n, 0.0);
+    ht.emb.assign(n, 0.0); ht.demb.assign(n, 0.0);
+    // calculate_lookup_table_veephi / _emb (src/lookup_m.F90:161-251)
+    double range = ht.rmax - ht.rmin, recipn = 1.0 / (double)nlookup;
+    for (int i = 0; i <= nlookup; ++i) {
+        double r = ht.rmin + (double)i * range * recipn;
+        ht.vee[i] = f.vee(r);
+        ht.dvee[i] = f.dvee(r);
+        ht.phi[i] = f.phi(r);
+        ht.dphi[i] = f.dphi(r);
+    }
+    double erange = ht.rhomax - ht.rhomin;
+    for (int i = 0; i <= nlookup; ++i) {
+        double rho = ht.rhomin + (double)i * erange * recipn;
+        ht.emb[i] = -(1.0 * std::sqrt(rho > 0.0 ? rho : 0.0));
+        ht.demb[i] = rho > 0.0 ? -(0.5 / std::sqrt(rho)) : 0.0;
+    }
+    ht.set = true;
+    return MOLDY_OK;
+}
+
+}  // namespace moldy

@@ -1,0 +1,150 @@
+"""Seeded synthetic inputs for the MOLDY Fe EAM hot path.
+
+All inputs are generated here (no dataset is involved).  The lattice follows
+the reference's ``read_system`` conventions (``src/io_m.F90:73-256``):
+
+* the box matrix B0 has the box vectors as columns, replicated n times;
+* atoms are numbered with x replicas outermost, then y, then z, then the two
+  bcc basis atoms (0,0,0) and (1/2,1/2,1/2);
+* positions are fractional, never wrapped.
+
+Displacements are Gaussian in Cartesian coordinates and converted with
+B0^-1.  Velocities are Maxwell-Boltzmann (the reference's ``setvel`` draws
+uniform components, ``src/thermostat_m.F90:201-249``), with the centre-of-mass
+motion removed and the kinetic energy scaled to 1.5 (N-1) k T as ``setvel``
+does with ``rqke`` (``src/thermostat_m.F90:94-99``).  They are stored as
+x1 = B0^-1 v dt.  Box velocities start at zero.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import units
+from .potentials import FE_FE, FeFeCoefficients
+
+A0_FE = 2.8665          # bcc Fe lattice parameter (A)
+RCUT_FETM = 6.0         # "range" returned by the FETRANSMETAL module (src/fetransmetal.F90:589-593)
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    nm: int
+    x0: np.ndarray            # (nm, 3) fractional positions
+    x1: np.ndarray            # (nm, 3) fractional velocity * dt
+    x2: np.ndarray            # (nm, 3) fractional acceleration * dt^2 / 2
+    b0: np.ndarray            # (3, 3) box, columns are box vectors (A)
+    b1: np.ndarray
+    b2: np.ndarray
+    atomic_number: np.ndarray
+    atomic_mass: np.ndarray
+    del2: np.ndarray
+    tgid: np.ndarray
+    ivol: int
+    ntcm: int
+    ntc: int
+    nnbrs: int
+    atomstress: int
+    rnear: float
+    deltat: float             # model time units
+    press: float              # model pressure units
+    bdel2: float
+    nlc: tuple
+    coeffs: FeFeCoefficients
+    meta: dict
+
+    def copy(self) -> "Workload":
+        w = dataclasses.replace(self)
+        for f in ("x0", "x1", "x2", "b0", "b1", "b2", "atomic_number", "atomic_mass",
+                  "del2", "tgid"):
+            setattr(w, f, np.array(getattr(self, f), copy=True))
+        w.meta = dict(self.meta)
+        return w
+
+
+def bcc_fractional(n: int) -> np.ndarray:
+    """Fractional bcc positions of an n x n x n supercell in read_system order."""
+    idx = np.arange(n, dtype=np.float64)
+    i, j, k = np.meshgrid(idx, idx, idx, indexing="ij")
+    cells = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)       # x outer, z inner
+    basis = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.5]])
+    pos = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3)
+    return pos / float(n)
+
+
+def link_cell_counts(b0: np.ndarray, rnear: float) -> tuple:
+    """nlc = max(3, int(B0(d,d) / rnear)) from the diagonal only (src/moldin.F90:252-257)."""
+    return tuple(max(3, int(b0[d, d] / rnear)) for d in range(3))
+
+
+def make_workload(n: int, *, a0: float = A0_FE, sigma: float = 0.05,
+                  temperature: float = 300.0, ivol: int = 1, press_gpa: float = 0.0,
+                  boxmass: float = 50.0, dt_fs: float = 1.0, rpad: float = 0.3,
+                  nbrupdate: int = 100, nnbrs: int = 150, seed: int = 1234,
+                  strain: np.ndarray | None = None, atomstress: int = 0,
+                  coeffs: FeFeCoefficients = FE_FE, name: str | None = None) -> Workload:
+    rng = np.random.default_rng(seed)
+    nm = 2 * n ** 3
+    b0 = np.eye(3) * (a0 * n)
+    if strain is not None:
+        b0 = (np.eye(3) + np.asarray(strain, dtype=np.float64)) @ b0
+    binv = np.linalg.inv(b0)
+    x0 = bcc_fractional(n)
+    if sigma > 0.0:
+        disp = rng.normal(0.0, sigma, size=(nm, 3))
+        x0 = x0 + disp @ binv.T
+    mass = np.full(nm, units.FE_MASS)
+    deltat = dt_fs * units.FS_TO_TIME
+    x1 = np.zeros((nm, 3))
+    if temperature > 0.0:
+        v = rng.normal(0.0, 1.0, size=(nm, 3)) * np.sqrt(units.BK * temperature / mass)[:, None]
+        v -= (mass[:, None] * v).sum(axis=0) / mass.sum()
+        ke = 0.5 * float((mass[:, None] * v * v).sum())
+        rqke = 1.5 * units.BK * temperature * (nm - 1)
+        v *= math.sqrt(rqke / ke)
+        x1 = (v * deltat) @ binv.T
+    del2 = np.where(mass > 0.01, deltat * deltat / (2.0 * mass), 0.0)
+    bmass = nm * boxmass
+    bdel2 = deltat * deltat / (2.0 * bmass)
+    rnear = RCUT_FETM + rpad
+    return Workload(
+        name=name or f"bcc_fe_{n}^3",
+        nm=nm, x0=x0, x1=x1, x2=np.zeros((nm, 3)),
+        b0=b0, b1=np.zeros((3, 3)), b2=np.zeros((3, 3)),
+        atomic_number=np.full(nm, 26, dtype=np.int32), atomic_mass=mass, del2=del2,
+        tgid=np.zeros((3, 3)), ivol=ivol, ntcm=nbrupdate, ntc=0, nnbrs=nnbrs,
+        atomstress=atomstress, rnear=rnear, deltat=deltat,
+        press=press_gpa * units.GPA_TO_PRESS, bdel2=bdel2,
+        nlc=link_cell_counts(b0, rnear), coeffs=coeffs,
+        meta=dict(n=n, a0=a0, sigma=sigma, temperature=temperature, seed=seed,
+                  dt_fs=dt_fs, boxmass=boxmass, press_gpa=press_gpa, rpad=rpad),
+    )
+
+
+def config_small_nve(seed: int = 1) -> Workload:
+    """2000-atom bcc Fe, sigma 0.05 A, 300 K, NVE (ivol=1), dt 1 fs, nbrupdate 100."""
+    return make_workload(10, sigma=0.05, temperature=300.0, ivol=1, nbrupdate=100, seed=seed,
+                         name="bcc_fe_2000_nve_300K")
+
+
+def config_large_npt(n: int = 100, seed: int = 2) -> Workload:
+    """2,000,000-atom bcc Fe (n=100), sigma 0.05 A, 1200 K, Parrinello-Rahman NPT
+    at 0 GPa (ivol=0), box mass 50 amu/atom, dt 1 fs, nbrupdate 100."""
+    return make_workload(n, sigma=0.05, temperature=1200.0, ivol=0, press_gpa=0.0,
+                         boxmass=50.0, nbrupdate=100, seed=seed,
+                         name=f"bcc_fe_{2 * n ** 3}_npt_1200K")
+
+
+def config_liquid(n: int = 80, seed: int = 5, temperature: float = 300.0) -> Workload:
+    """1,024,000-atom bcc Fe (n=80) for the heating/melting run, NPT, nbrupdate 20."""
+    return make_workload(n, sigma=0.05, temperature=temperature, ivol=0, press_gpa=0.0,
+                         boxmass=50.0, nbrupdate=20, seed=seed,
+                         name=f"bcc_fe_{2 * n ** 3}_liquid")
+
+
+def random_symmetric_strain(rng: np.random.Generator, amplitude: float) -> np.ndarray:
+    e = rng.uniform(-amplitude, amplitude, size=6)
+    return np.array([[e[0], e[3], e[4]], [e[3], e[1], e[5]], [e[4], e[5], e[2]]])

@@ -1,0 +1,207 @@
+"""GPU parity tests: libmoldy_gpu.so (through its C ABI) against the CPU oracle
+on the same seeded inputs.
+
+Tolerances:
+* link cells, neighbour lists: bit-exact (same l0/link/ic, same NLIST/NUMN);
+* lookup tables: bit-exact (same host build, same arithmetic order);
+* forces, density, energy, virial of one FP64 force call: norm-wise relative
+  error <= 1e-10 (the sums run in another order, with FP64 atomics);
+* trajectories: differences grow from the last bit, so 100 steps are checked
+  against the oracle with a looser, stated bound.
+"""
+import numpy as np
+import pytest
+
+from moldy_b200 import workloads as wl
+from tests.helpers import real_forces, rel_norm_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def _pair(oracle_mod, gpu_lib, w, *, uselookup=True, precision="fp64"):
+    from moldy_b200 import MoldySystem
+    o = oracle_mod.from_workload(w, uselookup=uselookup, threads=1)
+    g = MoldySystem.from_workload(w, uselookup=uselookup, precision=precision)
+    return o, g
+
+
+def test_tables_bit_exact(oracle_mod, gpu_lib):
+    w = wl.make_workload(3, sigma=0.0, temperature=0.0)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    to, tg = o.tables(), g.tables()
+    for k in to:
+        assert np.array_equal(to[k], tg[k], equal_nan=True), k
+
+
+@pytest.mark.parametrize("n,sigma,seed", [(10, 0.05, 1), (4, 0.1, 2), (7, 0.2, 3)])
+def test_linkup_and_neighbour_list_exact(oracle_mod, gpu_lib, n, sigma, seed):
+    w = wl.make_workload(n, sigma=sigma, temperature=0.0, seed=seed)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    g.linkup()
+    lo = o.linkcells()
+    lg = g.linkcells(o.ncell)
+    for a, b in zip(lo, lg):
+        assert np.array_equal(a, b)
+    assert o.update_neighbourlist() == 0
+    g.update_neighbourlist()
+    nlo, nno = o.nlist()
+    nlg, nng = g.neighbour_list()
+    assert np.array_equal(nno, nng)
+    for i in range(w.nm):
+        assert np.array_equal(nlo[i, :nno[i]], nlg[i, :nng[i]]), i
+
+
+def test_strained_box_neighbour_list_exact(oracle_mod, gpu_lib):
+    rng = np.random.default_rng(4)
+    w = wl.make_workload(9, sigma=0.1, temperature=0.0, seed=4,
+                         strain=wl.random_symmetric_strain(rng, 0.02))
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    g.linkup()
+    assert o.update_neighbourlist() == 0
+    g.update_neighbourlist()
+    nlo, nno = o.nlist()
+    nlg, nng = g.neighbour_list()
+    assert np.array_equal(nno, nng)
+    mask = np.arange(w.nnbrs)[None, :] < nno[:, None]
+    assert np.array_equal(nlo[mask], nlg[mask])
+
+
+def test_relink_chain_order_exact(oracle_mod, gpu_lib):
+    """relink replays the reference's chain surgery: same l0/link after moves,
+    and the following neighbour list is identical entry by entry."""
+    w = wl.make_workload(8, sigma=0.05, temperature=0.0, seed=6)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    g.linkup()
+    rng = np.random.default_rng(12)
+    x = w.x0.copy()
+    for _ in range(3):
+        x = x + rng.normal(0.0, 0.02, size=x.shape)
+        o.set_state(x, w.x1, w.x2, w.b0, w.b1, w.b2, w.atomic_number, w.atomic_mass, w.del2)
+        g.set_state(x0=x)
+        o.relink()
+        g.relink()
+        lo = o.linkcells()
+        lg = g.linkcells(o.ncell)
+        for a, b in zip(lo, lg):
+            assert np.array_equal(a, b)
+    assert o.update_neighbourlist() == 0
+    g.update_neighbourlist()
+    nlo, nno = o.nlist()
+    nlg, nng = g.neighbour_list()
+    assert np.array_equal(nno, nng)
+    mask = np.arange(w.nnbrs)[None, :] < nno[:, None]
+    assert np.array_equal(nlo[mask], nlg[mask])
+
+
+@pytest.mark.parametrize("uselookup", [True, False])
+@pytest.mark.parametrize("ivol", [1, 0])
+def test_force_fp64(oracle_mod, gpu_lib, uselookup, ivol):
+    w = wl.make_workload(10, sigma=0.05, temperature=300.0, ivol=ivol, seed=1)
+    o, g = _pair(oracle_mod, gpu_lib, w, uselookup=uselookup)
+    o.force()
+    fg = g.force()
+    fo = o.force_out()
+    assert rel_norm_err(g.forces(), o.forces()) < FP64_TOL
+    do, dg = o.density(), g.density()
+    for k in ("rho", "afrho", "dafrho"):
+        assert rel_norm_err(dg[k], do[k]) < FP64_TOL, k
+    assert abs(fg["pe"] - fo["pe"]) < FP64_TOL * abs(fo["pe"])
+    for k in ("tp", "tk", "tc", "tg", "tgdot", "fb"):
+        assert rel_norm_err(fg[k], fo[k]) < FP64_TOL, k
+    assert abs(fg["vol"] - fo["vol"]) < 1e-12 * fo["vol"]
+    assert fg["ntc"] == o.ntc and fg["rebuilt"]
+
+
+def test_force_perfect_lattice_zero(oracle_mod, gpu_lib):
+    import json, os
+    case = json.load(open(os.path.join(os.path.dirname(__file__), "golden",
+                                       "perfect_lattice.json")))["cases"][0]
+    w = wl.make_workload(6, a0=case["a0"], sigma=0.0, temperature=0.0)
+    _, g = _pair(oracle_mod, gpu_lib, w, uselookup=False)
+    fg = g.force()
+    assert abs(fg["pe"] / w.nm - case["e_per_atom"]) < 1e-12
+    assert np.max(np.abs(real_forces(g.forces(), w.b0))) < 1e-11
+
+
+def test_atomstress_and_energy_calc(oracle_mod, gpu_lib):
+    w = wl.make_workload(6, sigma=0.08, temperature=0.0, seed=8, atomstress=1)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    o.force()
+    g.force()
+    assert rel_norm_err(g.atomstress(), o.atomstress()) < FP64_TOL
+    assert rel_norm_err(g.energy_calc(), o.energy_calc()) < FP64_TOL
+
+
+def test_set_tables_drop_in(oracle_mod, gpu_lib):
+    """Tables handed over by the caller (potential_set_lookup output) give the
+    same forces as the built-in FETRANSMETAL set-up."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(6, sigma=0.08, temperature=0.0, seed=9)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=1)
+    o.force()
+    g = MoldySystem(w.nm, rnear=w.rnear, deltat=w.deltat, ivol=w.ivol, ntcm=w.ntcm, nlc=w.nlc)
+    g.set_tables(o.tables())
+    g.set_state(w.x0, w.x1, w.x2, w.b0, w.b1, w.b2, w.atomic_number, w.atomic_mass, w.del2)
+    g.force()
+    assert rel_norm_err(g.forces(), o.forces()) < FP64_TOL
+
+
+def test_md_trajectory_nve_100_steps(oracle_mod, gpu_lib):
+    """2000-atom bcc Fe, 300 K, NVE, dt 1 fs, 100 steps (lookup tables)."""
+    w = wl.config_small_nve()
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    o.md_init()
+    g.md_init()
+    th_o = [o.md_step() for _ in range(100)]
+    th_g = g.md_steps(100)
+    for k in ("pe", "ke", "te"):
+        a = np.array([t[k] for t in th_o])
+        b = np.array([t[k] for t in th_g])
+        assert np.max(np.abs(a - b)) < 1e-7 * w.nm, k
+    so, sg = o.get_state(), g.get_state()
+    dx = (sg["x0"] - so["x0"]) @ w.b0.T
+    assert np.max(np.abs(dx)) < 1e-8          # Angstrom after 100 fs
+    assert [t["ntc"] for t in th_g] == [int(t["ntc"]) for t in th_o]
+
+
+def test_md_trajectory_npt_box(oracle_mod, gpu_lib):
+    """Parrinello-Rahman NPT (ivol=0) at 1200 K: box matrices follow the oracle."""
+    w = wl.make_workload(6, sigma=0.05, temperature=1200.0, ivol=0, seed=21, nbrupdate=7)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    o.md_init()
+    g.md_init()
+    th_o = [o.md_step() for _ in range(30)]
+    th_g = g.md_steps(30)
+    so, sg = o.get_state(), g.get_state()
+    assert rel_norm_err(sg["b0"], so["b0"]) < 1e-11
+    assert rel_norm_err(sg["b1"], so["b1"]) < 1e-6
+    assert abs(th_g[-1]["vol"] - th_o[-1]["vol"]) < 1e-9 * th_o[-1]["vol"]
+    assert abs(th_g[-1]["th"] - th_o[-1]["th"]) < 1e-8 * abs(th_o[-1]["th"])
+
+
+def test_velocityverlet_single_step_matches(oracle_mod, gpu_lib):
+    w = wl.make_workload(6, sigma=0.05, temperature=600.0, ivol=0, seed=31, nbrupdate=3)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    o.md_init()
+    g.md_init()
+    for _ in range(4):
+        o.velocityverlet()
+        g.velocityverlet()
+        so, sg = o.get_state(), g.get_state()
+        for k in ("x0", "x1", "x2"):
+            assert rel_norm_err(sg[k], so[k]) < 1e-9, k
+        s_o = o.update_therm_avs()
+        s_g = g.update_therm_avs()
+        assert np.allclose(s_g, s_o, rtol=1e-9, atol=0)
+
+
+def test_neighbour_overflow_error(oracle_mod, gpu_lib):
+    from moldy_b200 import MoldyError
+    w = wl.make_workload(4, sigma=0.0, temperature=0.0)
+    w.nnbrs = 12
+    _, g = _pair(oracle_mod, gpu_lib, w)
+    with pytest.raises(MoldyError) as ei:
+        g.force()
+    assert ei.value.code == 2
