@@ -491,6 +491,10 @@ int Engine::check_flags() {
                       "(src/neighbourlist_m.F90:222-229)", prm.nnbrs, f[2]);
         return fail(MOLDY_ERR_NEIGHBOUR_OVERFLOW, msg);
     }
+    if (f[1]) {
+        cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
+        return fail(MOLDY_ERR_CAPACITY, "link-cell relink produced inconsistent cell counts");
+    }
     if (st) {
         cudaMemsetAsync(&d.box->status, 0, sizeof(int32_t), stream_);
         return fail(MOLDY_ERR_SINGULAR_BOX, "matrix_invert: determinant is zero (src/matrix_m.F90:110-113)");

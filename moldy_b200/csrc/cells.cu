@@ -184,19 +184,25 @@ __global__ void k_relink_cells(int ncell, const int32_t *__restrict__ cell_start
     arr_count_rot[c] = st;
 }
 
-__global__ void k_relink_write(int ncell, const int32_t *__restrict__ cell_start,
+__global__ void k_relink_write(int ncell, int nm, const int32_t *__restrict__ cell_start,
                                const int32_t *__restrict__ arr_start,
                                const int32_t *__restrict__ rot, const int32_t *__restrict__ work,
                                const int32_t *__restrict__ new_count,
                                const int32_t *__restrict__ new_start, int32_t *__restrict__ atoms2,
-                               int32_t *__restrict__ cell_pos) {
+                               int32_t *__restrict__ cell_pos, int32_t *__restrict__ flags) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     int L = new_count[c], st = rot[c];
+    int base = new_start[c];
+    if (L < 0 || base < 0 || base + L > nm) {       // inconsistent counts: record, skip
+        atomicExch(&flags[1], 1);
+        return;
+    }
     const int32_t *W = work + cell_start[c] + arr_start[c];
-    int32_t *out = atoms2 + new_start[c];
+    int32_t *out = atoms2 + base;
     for (int k = 0; k < L; ++k) {
         int x = W[(st + k) % L];
+        if (x < 0 || x >= nm) { atomicExch(&flags[1], 1); continue; }
         out[k] = x;
         cell_pos[x] = k;
     }
@@ -212,13 +218,13 @@ void launch_relink(DeviceState &d, const Params &p, cudaStream_t s) {
     cudaMemsetAsync(d.new_count, 0, sizeof(int32_t) * p.ncell, s);
     k_relink_arrivals<<<nb, kAtomThreads, 0, s>>>(p.nm, d.ic, d.ic_new, d.arr_start, d.new_count,
                                                   d.arr_list);
-    k_relink_cells<<<nbc, 128, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms, d.ic,
+    k_relink_cells<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms, d.ic,
                                        d.ic_new, d.arr_start, d.arr_count, d.arr_list, d.work,
                                        d.new_count);
     launch_exclusive_scan(d.new_count, d.new_start, p.ncell, s);
-    k_relink_write<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.arr_start, d.arr_count,
-                                                d.work, d.new_count, d.new_start, d.cell_atoms2,
-                                                d.cell_pos);
+    k_relink_write<<<nbc, kAtomThreads, 0, s>>>(p.ncell, p.nm, d.cell_start, d.arr_start,
+                                                d.arr_count, d.work, d.new_count, d.new_start,
+                                                d.cell_atoms2, d.cell_pos, d.flags);
     // commit (copies keep buffer addresses fixed for graph capture)
     cudaMemcpyAsync(d.cell_atoms, d.cell_atoms2, sizeof(int32_t) * p.nm, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(d.cell_start, d.new_start, sizeof(int32_t) * (p.ncell + 1),

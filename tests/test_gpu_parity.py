@@ -68,10 +68,12 @@ def test_strained_box_neighbour_list_exact(oracle_mod, gpu_lib):
     assert np.array_equal(nlo[mask], nlg[mask])
 
 
-def test_relink_chain_order_exact(oracle_mod, gpu_lib):
+@pytest.mark.parametrize("n", [8, 30])
+def test_relink_chain_order_exact(oracle_mod, gpu_lib, n):
     """relink replays the reference's chain surgery: same l0/link after moves,
-    and the following neighbour list is identical entry by entry."""
-    w = wl.make_workload(8, sigma=0.05, temperature=0.0, seed=6)
+    and the following neighbour list is identical entry by entry (n=30 has
+    13^3 = 2197 link cells, more than one thread block of cells)."""
+    w = wl.make_workload(n, sigma=0.05, temperature=0.0, seed=6)
     o, g = _pair(oracle_mod, gpu_lib, w)
     g.linkup()
     rng = np.random.default_rng(12)
@@ -205,3 +207,23 @@ def test_neighbour_overflow_error(oracle_mod, gpu_lib):
     with pytest.raises(MoldyError) as ei:
         g.force()
     assert ei.value.code == 2
+
+
+def test_md_many_rebuilds_large_box(oracle_mod, gpu_lib):
+    """54,000 atoms (13^3 link cells), NPT 1200 K, rebuild every 3 steps: after
+    12 steps (4 relinks, 5 list builds) thermo, link cells and the neighbour
+    list still follow the oracle."""
+    w = wl.make_workload(30, sigma=0.05, temperature=1200.0, ivol=0, seed=41, nbrupdate=3)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    o.md_init()
+    g.md_init()
+    th_o = [o.md_step() for _ in range(12)]
+    th_g = g.md_steps(12)
+    for k in ("pe", "ke", "th"):
+        a = np.array([t[k] for t in th_o])
+        b = np.array([t[k] for t in th_g])
+        assert np.max(np.abs(a - b)) < 1e-9 * np.max(np.abs(a)), k
+    lo = o.linkcells()
+    lg = g.linkcells(o.ncell)
+    for a, b in zip(lo, lg):
+        assert np.array_equal(a, b)
