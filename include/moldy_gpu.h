@@ -182,6 +182,34 @@ int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64
 const char *moldy_gpu_kernel_name(int32_t kernel);
 #define MOLDY_KERNEL_FAMILIES 13
 
+/* force evaluation without device allocation -----------------------------*/
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (device memory owned by another allocator, or code that must not allocate
+ * while it runs): one EAM force evaluation (rhoset, embed and the pair loop
+ * of src/dynamics_m.F90:135-401) on buffers the caller owns, with its
+ * intermediates in a fixed __device__ array inside this library, so the call
+ * allocates nothing.  Limit: nm <= MOLDY_NOALLOC_MAX_ATOMS, else
+ * MOLDY_ERR_CAPACITY.  Device pointers: x0,y0,z0 (fractional), mass (may be
+ * NULL: every pair enters the virial), nlist/numn (NLIST(nnbrs,nm) with
+ * 1-based entries, NUMN(nm)), the six tables (nlookup+1 entries each),
+ * fx,fy,fz (fractional forces, overwritten) and energy_virial (10 doubles:
+ * pe, then tp column-major).  b0 is a host array (column-major 3x3).  Work
+ * is queued on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * the call returns after it finishes.  The first call on each device looks
+ * up the array's device address; make that first call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU race
+ * and give wrong results. */
+#define MOLDY_NOALLOC_MAX_ATOMS 262144
+int moldy_gpu_force_noalloc(int32_t nm, int32_t nnbrs, int32_t ivol,
+                            const double *x0, const double *y0, const double *z0,
+                            const double *mass, const double *b0,
+                            const int32_t *nlist, const int32_t *numn, int32_t nlookup,
+                            double rmin, double rmax, double rhomin, double rhomax,
+                            const double *vee, const double *dvee, const double *phi,
+                            const double *dphi, const double *emb, const double *demb,
+                            double *fx, double *fy, double *fz, double *energy_virial,
+                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,7 +97,13 @@ SIGNATURES = {
     "moldy_gpu_reset_kernel_stats": [H],
     "moldy_gpu_kernel_stats": [H, ctypes.c_int32, D, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_kernel_name": [ctypes.c_int32],
+    "moldy_gpu_force_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, D, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 11,
 }
+NOALLOC_MAX_ATOMS = 262144
 KERNEL_FAMILIES = 13
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}

@@ -715,6 +715,12 @@ struct moldy_gpu {
 
 namespace moldy {
 int engine_create(const moldy_params *p, Engine **out);
+int force_noalloc(int nm, int nnbrs, int ivol, const double *x0, const double *y0, const double *z0,
+                  const double *mass, const double *b0, const int32_t *nlist, const int32_t *numn,
+                  int nlookup, double rmin, double rmax, double rhomin, double rhomax,
+                  const double *vee, const double *dvee, const double *phi, const double *dphi,
+                  const double *emb, const double *demb, double *fx, double *fy, double *fz,
+                  double *energy_virial, cudaStream_t s, std::string &err);
 }
 
 extern "C" {
@@ -877,6 +883,21 @@ int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64
     h->e->prof.harvest();
     if (total_ms) *total_ms = h->e->prof.total_ms[kernel];
     if (launches) *launches = h->e->prof.launches[kernel];
+    return MOLDY_OK;
+}
+
+int moldy_gpu_force_noalloc(int32_t nm, int32_t nnbrs, int32_t ivol, const double *x0,
+                            const double *y0, const double *z0, const double *mass, const double *b0,
+                            const int32_t *nlist, const int32_t *numn, int32_t nlookup, double rmin,
+                            double rmax, double rhomin, double rhomax, const double *vee,
+                            const double *dvee, const double *phi, const double *dphi,
+                            const double *emb, const double *demb, double *fx, double *fy,
+                            double *fz, double *energy_virial, void *stream) {
+    std::string err;
+    int rc = moldy::force_noalloc(nm, nnbrs, ivol, x0, y0, z0, mass, b0, nlist, numn, nlookup, rmin,
+                                  rmax, rhomin, rhomax, vee, dvee, phi, dphi, emb, demb, fx, fy, fz,
+                                  energy_virial, (cudaStream_t)stream, err);
+    if (rc != MOLDY_OK) return fail(rc, err);
     return MOLDY_OK;
 }
 
