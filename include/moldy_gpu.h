@@ -182,6 +182,21 @@ int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64
 const char *moldy_gpu_kernel_name(int32_t kernel);
 #define MOLDY_KERNEL_FAMILIES 13
 
+/* kernel variants (no counterpart in the reference) -------------------------*/
+/* The screening, density and force passes are compiled in MOLDY_TUNE_VARIANTS
+ * variants each (how many list entries a thread gathers before using them).
+ * moldy_gpu_autotune times every variant on the current configuration with
+ * nreps force evaluations (positions, velocities, the rebuild counter and the
+ * neighbour list are left unchanged) and keeps the fastest of each pass.
+ * times_ms (3*MOLDY_TUNE_VARIANTS, may be NULL) receives the mean time per
+ * launch; chosen (3, may be NULL) the selected variants. */
+#define MOLDY_TUNE_VARIANTS 3
+int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
+int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
+/* Directed interacting pairs (inside the table range) of the last force
+ * evaluation, i.e. twice the number of contributing half-list pairs. */
+int moldy_gpu_get_pair_count(moldy_gpu *h, double *npairs);
+
 /* force evaluation without device allocation -----------------------------*/
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (device memory owned by another allocator, or code that must not allocate

@@ -97,6 +97,9 @@ SIGNATURES = {
     "moldy_gpu_reset_kernel_stats": [H],
     "moldy_gpu_kernel_stats": [H, ctypes.c_int32, D, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_kernel_name": [ctypes.c_int32],
+    "moldy_gpu_autotune": [H, ctypes.c_int32, D, I],
+    "moldy_gpu_set_variants": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
+    "moldy_gpu_get_pair_count": [H, D],
     "moldy_gpu_force_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, D, ctypes.c_void_p, ctypes.c_void_p,
@@ -105,6 +108,7 @@ SIGNATURES = {
 }
 NOALLOC_MAX_ATOMS = 262144
 KERNEL_FAMILIES = 13
+TUNE_VARIANTS = 3
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}
 

@@ -55,7 +55,8 @@ int dev_alloc(T **p, size_t n, const char *what) {
     } while (0)
 
 __global__ void k_pack_pos(int nm, const double *__restrict__ x, const double *__restrict__ y,
-                           const double *__restrict__ z, int mask, double4 *__restrict__ pos) {
+                           const double *__restrict__ z, int mask, double4 *__restrict__ pos,
+                           float4 *__restrict__ posf) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nm) return;
     double4 p = pos[a];
@@ -63,6 +64,7 @@ __global__ void k_pack_pos(int nm, const double *__restrict__ x, const double *_
     if (mask & 2) p.y = y[a];
     if (mask & 4) p.z = z[a];
     pos[a] = p;
+    posf[a] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
 
 __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__restrict__ xyz) {
@@ -78,8 +80,8 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
-    "drift", "linkup", "relink", "build_nlist", "density", "embed_kinten", "pair_forces",
-    "finalize_force", "vv_second_half", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
+    "drift", "linkup", "relink", "build_nlist", "density", "screen", "forces",
+    "finalize_force", "unused", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {
@@ -164,7 +166,8 @@ Engine::~Engine() {
     void *bufs[] = {d.pos, d.x1, d.x2, d.f, d.rho, d.afrho, d.dafrho, d.stress, d.mass, d.del2,
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
-                    d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.tab_r4, d.tab_e2,
+                    d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
+                    d.own_cnt, d.rev_cnt, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -223,6 +226,11 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.cell_atoms2, nm, "cell_atoms2"));
     CHECK(dev_alloc(&d.nlist, nm * (size_t)p.nnbrs, "nlist"));
     CHECK(dev_alloc(&d.numn, nm, "numn"));
+    CHECK(dev_alloc(&d.posf, nm, "posf"));
+    CHECK(dev_alloc(&d.pos2, nm, "pos2"));
+    CHECK(dev_alloc(&d.alist, nm * (size_t)(kOwnCap + kRevCap), "active list"));
+    CHECK(dev_alloc(&d.own_cnt, nm, "own_cnt"));
+    CHECK(dev_alloc(&d.rev_cnt, nm, "rev_cnt"));
     CHECK(dev_alloc(&d.partials, 2 * (size_t)kMaxBlocks * kPartials, "partials"));
     CHECK(dev_alloc(&d.flags, 8, "flags"));
     CHECK(dev_alloc(&d.box, 1, "box"));
@@ -235,6 +243,10 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.dafrho, 0, nm * sizeof(double)), "memset dafrho");
     CUDA_CHECK(cudaMemset(d.stress, 0, 3 * nm * sizeof(double)), "memset stress");
     CUDA_CHECK(cudaMemset(d.numn, 0, nm * sizeof(int32_t)), "memset numn");
+    CUDA_CHECK(cudaMemset(d.posf, 0, nm * sizeof(float4)), "memset posf");
+    CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
+    CUDA_CHECK(cudaMemset(d.own_cnt, 0, nm * sizeof(int32_t)), "memset own_cnt");
+    CUDA_CHECK(cudaMemset(d.rev_cnt, 0, nm * sizeof(int32_t)), "memset rev_cnt");
     CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
@@ -368,7 +380,8 @@ int Engine::set_state(const double *x0, const double *y0, const double *z0, cons
         if (y0) CUDA_CHECK(cudaMemcpyAsync(tmp + nm, y0, nb, cudaMemcpyHostToDevice, s), "set y0");
         if (z0) CUDA_CHECK(cudaMemcpyAsync(tmp + 2 * nm, z0, nb, cudaMemcpyHostToDevice, s), "set z0");
         int mask = (x0 ? 1 : 0) | (y0 ? 2 : 0) | (z0 ? 4 : 0);
-        k_pack_pos<<<(prm.nm + 255) / 256, 256, 0, s>>>(prm.nm, tmp, tmp + nm, tmp + 2 * nm, mask, d.pos);
+        k_pack_pos<<<(prm.nm + 255) / 256, 256, 0, s>>>(prm.nm, tmp, tmp + nm, tmp + 2 * nm, mask, d.pos,
+                                                         d.posf);
     }
     const double *v1[3] = {x1, y1, z1}, *v2[3] = {x2, y2, z2};
     for (int k = 0; k < 3; ++k) {
@@ -495,6 +508,12 @@ int Engine::check_flags() {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
         return fail(MOLDY_ERR_CAPACITY, "link-cell relink produced inconsistent cell counts");
     }
+    if (f[3]) {
+        cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
+        return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[4]) +
+                                            " interacting neighbours on one side, more than the compact list holds (" +
+                                            std::to_string(kOwnCap) + " own / " + std::to_string(kRevCap) + " reverse)");
+    }
     if (st) {
         cudaMemsetAsync(&d.box->status, 0, sizeof(int32_t), stream_);
         return fail(MOLDY_ERR_SINGULAR_BOX, "matrix_invert: determinant is zero (src/matrix_m.F90:110-113)");
@@ -544,17 +563,15 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
         rb = true;
     }
     if (ntc == ntcm) ntc = 0;
-    size_t nm = (size_t)p.nm;
-    cudaMemsetAsync(d.rho, 0, nm * sizeof(double), s);
-    cudaMemsetAsync(d.f, 0, 3 * nm * sizeof(double), s);
-    if (p.atomstress) cudaMemsetAsync(d.stress, 0, 3 * nm * sizeof(double), s);
+    const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
-    LAUNCH(E, K_DENSITY, 1, s, launch_density(d, p, E.tab, s));
-    LAUNCH(E, K_EMBED, 1, s, launch_embed_kinten(d, p, E.tab, pe, s));
-    LAUNCH(E, K_PAIR, 1, s, launch_pair_forces(d, p, E.tab, pf, s));
-    LAUNCH(E, K_FINALIZE, 1, s,
-           launch_finalize_force(d, p, pe, grid_blocks(p.nm, kAtomThreads), pf,
-                                 grid_blocks((long long)p.nm * kPairTPA, 256), mode, s));
+    int nbe = 0, nbf = 0;
+    LAUNCH(E, K_SCREEN, 1, s, launch_screen(d, p, E.tab, mixed, E.variant[K_SCREEN], s));
+    LAUNCH(E, K_DENSITY, 1, s,
+           nbe = launch_density_full(d, p, E.tab, mixed, E.variant[K_DENSITY], pe, s));
+    LAUNCH(E, K_PAIR, 1, s,
+           nbf = launch_forces(d, p, E.tab, mixed, mode == 1 ? 1 : 0, E.variant[K_PAIR], pf, s));
+    LAUNCH(E, K_FINALIZE, 1, s, launch_finalize_force(d, p, pe, nbe, pf, nbf, mode, s));
     if (rebuilt) *rebuilt = rb;
     return MOLDY_OK;
 }
@@ -601,7 +618,6 @@ int Engine::velocityverlet(moldy_force_out *out) {
     bool rb = false;
     LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
     CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
-    LAUNCH(*this, K_VV2, 1, stream_, launch_vv_second_half(d, prm, stream_));
     CHECK(fetch_force_out(out));
     if (out) out->rebuilt = rb ? 1 : 0;
     return MOLDY_OK;
@@ -646,7 +662,6 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         bool rb = false;
         LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
-        LAUNCH(*this, K_VV2, 1, stream_, launch_vv_second_half(d, prm, stream_));
         int nb = 0;
         LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));
         LAUNCH(*this, K_THERM_FIN, 1, stream_, launch_finalize_therm(d, prm, nb, stream_));
@@ -680,6 +695,56 @@ int Engine::energy_calc(double *en_atom) {
     CUDA_CHECK(cudaStreamSynchronize(stream_), "energy_calc");
     CUDA_CHECK(cudaGetLastError(), "energy_calc");
     return MOLDY_OK;
+}
+
+// Times every compiled variant of the screening, density and force passes on
+// the current configuration (force passes only: positions, velocities, the
+// rebuild counter and the neighbour list are left as they are) and keeps the
+// fastest variant of each.  times_ms[3*kVariants] receives the mean time per
+// launch of (family, variant).
+int Engine::autotune(int nreps, double *times_ms) {
+    CHECK(check_ready());
+    if (nreps < 1) nreps = 1;
+    if (!list_ready_) {
+        if (!cells_ready_) CHECK(linkup());
+        LAUNCH(*this, K_NLIST, 1, stream_, launch_build_nlist(d, prm, stream_));
+        list_ready_ = true;
+    }
+    const bool mixed = precision_ == MOLDY_PREC_MIXED;
+    const int fams[3] = {K_SCREEN, K_DENSITY, K_PAIR};
+    double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
+    auto passes = [&]() {
+        LAUNCH(*this, K_SCREEN, 1, stream_, launch_screen(d, prm, tab, mixed, variant[K_SCREEN], stream_));
+        LAUNCH(*this, K_DENSITY, 1, stream_,
+               launch_density_full(d, prm, tab, mixed, variant[K_DENSITY], pe, stream_));
+        LAUNCH(*this, K_PAIR, 1, stream_,
+               launch_forces(d, prm, tab, mixed, 0, variant[K_PAIR], pf, stream_));
+    };
+    bool was_on = prof.on;
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "autotune");
+    prof.harvest();
+    prof.on = true;
+    for (int fi = 0; fi < 3; ++fi) {
+        int fam = fams[fi], best = variant[fam];
+        double best_ms = 1e300;
+        for (int v = 0; v < kVariants; ++v) {
+            variant[fam] = v;
+            passes();                                  // warm-up with this variant
+            CUDA_CHECK(cudaStreamSynchronize(stream_), "autotune");
+            prof.harvest();
+            double t0 = prof.total_ms[fam];
+            for (int r = 0; r < nreps; ++r) passes();
+            CUDA_CHECK(cudaStreamSynchronize(stream_), "autotune");
+            prof.harvest();
+            double ms = (prof.total_ms[fam] - t0) / nreps;
+            if (times_ms) times_ms[fi * kVariants + v] = ms;
+            if (ms < best_ms) { best_ms = ms; best = v; }
+        }
+        variant[fam] = best;
+    }
+    prof.on = was_on;
+    CUDA_CHECK(cudaGetLastError(), "autotune");
+    return check_flags();
 }
 
 int Engine::synchronize() {
@@ -898,6 +963,43 @@ int moldy_gpu_force_noalloc(int32_t nm, int32_t nnbrs, int32_t ivol, const doubl
                                   rmax, rhomin, rhomax, vee, dvee, phi, dphi, emb, demb, fx, fy, fz,
                                   energy_virial, (cudaStream_t)stream, err);
     if (rc != MOLDY_OK) return fail(rc, err);
+    return MOLDY_OK;
+}
+
+int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen) {
+    GUARD(h);
+    int rc;
+    try {
+        rc = h->e->autotune(nreps, times_ms);
+    } catch (const std::bad_alloc &) {
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
+    if (rc == MOLDY_OK && chosen) {
+        chosen[0] = h->e->variant[moldy::K_SCREEN];
+        chosen[1] = h->e->variant[moldy::K_DENSITY];
+        chosen[2] = h->e->variant[moldy::K_PAIR];
+    }
+    return rc;
+}
+
+int moldy_gpu_get_pair_count(moldy_gpu *h, double *npairs) {
+    GUARD(h);
+    if (!npairs) return fail(MOLDY_ERR_INVALID, "null argument");
+    cudaError_t e = cudaMemcpyAsync(npairs, &h->e->d.box->npairs, sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->e->stream_ref());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->e->stream_ref());
+    if (e != cudaSuccess) return moldy::cuda_fail(e, "get_pair_count");
+    return MOLDY_OK;
+}
+
+int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces) {
+    GUARD(h);
+    int v[3] = {screen, density, forces};
+    for (int k = 0; k < 3; ++k)
+        if (v[k] < 0 || v[k] >= moldy::kVariants) return fail(MOLDY_ERR_INVALID, "variant out of range");
+    h->e->variant[moldy::K_SCREEN] = screen;
+    h->e->variant[moldy::K_DENSITY] = density;
+    h->e->variant[moldy::K_PAIR] = forces;
     return MOLDY_OK;
 }
 

@@ -21,6 +21,7 @@ struct BoxState {
     double vol, pe, pe_emb, pe_pair;
     double s1, s2, s3, ke, te, h, th, boxke, temp;
     double maxdisp;
+    double npairs;                 // directed interacting pairs in the last density pass
     int32_t status;                // nonzero: singular box in a device-side inversion
     int32_t pad;
 };

@@ -1,206 +1,9 @@
-// eam.cu -- the two-pass Finnis-Sinclair/EAM evaluation, the virial and the
-// velocity-Verlet / Parrinello-Rahman update (dynamics_m, potential_m,
-// thermostat_m::kinten, quench_m::velocityverlet).
-//
-// The pair passes walk the reference's half list: TPA lanes share one owner
-// atom i, each lane takes every TPA-th neighbour j.  Pairs beyond the last
-// nonzero table node are skipped (their table values are exactly zero).  The
-// j side is scattered with FP64 atomics (the reference uses per-link-cell
-// OpenMP locks), the i side is reduced over the lane group and added once.
+// eam.cu -- box algebra, the velocity-Verlet / Parrinello-Rahman update, the
+// thermodynamic sums and energy_calc (dynamics_m, thermostat_m::kinten,
+// quench_m::velocityverlet).  The pair passes are in pairs.cu.
 #include "engine.h"
 
 namespace moldy {
-
-// --------------------------------------------------------- pass 1: density --
-// rhoset (src/dynamics_m.F90:497-579): rho_j += phi(r), rho_i += phi(r)
-template <int TPA>
-__global__ void __launch_bounds__(256)
-k_density(Params p, Tables t, const double4 *__restrict__ pos, const BoxState *__restrict__ box,
-          const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
-          double *__restrict__ rho) {
-    __shared__ double sb[9];
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    __syncthreads();
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = sb[k];
-    constexpr int GPW = 32 / TPA;                      // groups per warp
-    const int l = threadIdx.x % TPA;
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int base = warp * GPW; base < p.nm; base += nwarps * GPW) {
-        const int g = base + lane / TPA;
-        const bool active = g < p.nm;
-        double rho_i = 0.0;
-        if (active) {
-            const double4 pa = pos[g];
-            const int n = numn[g];
-            const int32_t *row = nlist + (size_t)g * p.nnbrs;
-            for (int k = l; k < n; k += TPA) {
-                int j = row[k];
-                double4 pj = pos[j];
-                double dx = pa.x - pj.x, dy = pa.y - pj.y, dz = pa.z - pj.z;
-                min_image(p.ivol, dx, dy, dz);
-                double rx = b[0] * dx + b[3] * dy + b[6] * dz;
-                double ry = b[1] * dx + b[4] * dy + b[7] * dz;
-                double rz = b[2] * dx + b[5] * dy + b[8] * dz;
-                double r2 = rx * rx + ry * ry + rz * rz;
-                if (r2 > t.rcull2) continue;
-                double phi = density_func(t, sqrt(r2));
-                atomicAdd(&rho[j], phi);
-                rho_i += phi;
-            }
-        }
-#pragma unroll
-        for (int o = TPA / 2; o > 0; o >>= 1) rho_i += __shfl_xor_sync(0xffffffffu, rho_i, o);
-        if (active && l == 0) atomicAdd(&rho[g], rho_i);
-    }
-}
-
-void launch_density(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s) {
-    int nb = grid_blocks((long long)p.nm * kPairTPA, 256);
-    k_density<kPairTPA><<<nb, 256, 0, s>>>(p, t, d.pos, d.box, d.nlist, d.numn, d.rho);
-}
-
-// --------------------------------------------------- embed + kinetic stress --
-// embed (src/potential_m.F90:148-169): rho <= 1e-40 keeps the old F, F'.
-// kinten (src/thermostat_m.F90:127-164): tk(a,b) += x1_b * m (B0 x1)_a.
-// F' is also stored in pos.w for the force pass.
-__global__ void __launch_bounds__(256)
-k_embed_kinten(Params p, Tables t, double4 *__restrict__ pos, const BoxState *__restrict__ box,
-               const double *__restrict__ rho, double *__restrict__ afrho,
-               double *__restrict__ dafrho, const double *__restrict__ x1,
-               const double *__restrict__ mass, const int32_t *__restrict__ znum,
-               double *__restrict__ partials) {
-    __shared__ double sb[9];
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    __syncthreads();
-    double v[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) v[k] = 0.0;
-    const int nm = p.nm;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        double r = rho[a];
-        double fd = dafrho[a];
-        if (r > 1e-40) {
-            double2 e = embed_funcs(t, r);
-            afrho[a] = e.x;
-            dafrho[a] = e.y;
-            fd = e.y;
-            v[0] += e.x;
-        }
-        pos[a].w = fd;
-        if (znum[a] != 0) {
-            double m = mass[a];
-            double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
-            double mvx = (sb[0] * ux + sb[3] * uy + sb[6] * uz) * m;
-            double mvy = (sb[1] * ux + sb[4] * uy + sb[7] * uz) * m;
-            double mvz = (sb[2] * ux + sb[5] * uy + sb[8] * uz) * m;
-            v[1] += ux * mvx; v[2] += ux * mvy; v[3] += ux * mvz;   // tk(:,1)
-            v[4] += uy * mvx; v[5] += uy * mvy; v[6] += uy * mvz;   // tk(:,2)
-            v[7] += uz * mvx; v[8] += uz * mvy; v[9] += uz * mvz;   // tk(:,3)
-        }
-    }
-    block_partials<10>(v, partials, 0);
-}
-
-void launch_embed_kinten(DeviceState &d, const Params &p, const Tables &t, double *partials,
-                         cudaStream_t s) {
-    int nblocks = grid_blocks(p.nm, kAtomThreads);
-    k_embed_kinten<<<nblocks, kAtomThreads, 0, s>>>(p, t, d.pos, d.box, d.rho, d.afrho, d.dafrho,
-                                                    d.x1, d.mass, d.znum, partials);
-}
-
-// ------------------------------------------------------ pass 2: pair forces --
-// force loop (src/dynamics_m.F90:235-346):
-//   fp = -dvee/r - (dphi_ij F'_i + dphi_ji F'_j)/r,  f_j += -dx fp,  f_i -= sum(-dx fp)
-//   tp(a,b) += dx_b (B0 dx)_a fp  when m_i + m_j > 0.1,  pe += vee.
-template <int TPA>
-__global__ void __launch_bounds__(256)
-k_pair_forces(Params p, Tables t, const double4 *__restrict__ pos, const BoxState *__restrict__ box,
-              const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
-              const double *__restrict__ mass, double *__restrict__ f,
-              double *__restrict__ stress, double *__restrict__ partials) {
-    __shared__ double sb[9];
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    __syncthreads();
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = sb[k];
-    double v[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) v[k] = 0.0;
-    constexpr int GPW = 32 / TPA;
-    const int l = threadIdx.x % TPA;
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int nm = p.nm;
-    for (int base = warp * GPW; base < nm; base += nwarps * GPW) {
-        const int g = base + lane / TPA;
-        const bool active = g < nm;
-        double fxi = 0.0, fyi = 0.0, fzi = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-        if (active) {
-            const double4 pa = pos[g];
-            const double ma = mass[g];
-            const int n = numn[g];
-            const int32_t *row = nlist + (size_t)g * p.nnbrs;
-            for (int k = l; k < n; k += TPA) {
-                int j = row[k];
-                double4 pj = pos[j];
-                double dx = pa.x - pj.x, dy = pa.y - pj.y, dz = pa.z - pj.z;
-                min_image(p.ivol, dx, dy, dz);
-                double rx = b[0] * dx + b[3] * dy + b[6] * dz;
-                double ry = b[1] * dx + b[4] * dy + b[7] * dz;
-                double rz = b[2] * dx + b[5] * dy + b[8] * dz;
-                double r2 = rx * rx + ry * ry + rz * rz;
-                if (r2 > t.rcull2) continue;
-                double r = sqrt(r2);
-                double rr = 1.0 / r;
-                double4 tv = pair_funcs(t, r);            // vee, dvee, phi, dphi
-                double fpp = -tv.y * rr;
-                double fcp = -(tv.w * pa.w + tv.w * pj.w) * rr;
-                double fp = fpp + fcp;
-                v[0] += tv.x;
-                if (p.atomstress) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
-                if (ma > 0.1 || ma + mass[j] > 0.1) {
-                    v[1] += dx * rx * fp; v[2] += dx * ry * fp; v[3] += dx * rz * fp;
-                    v[4] += dy * rx * fp; v[5] += dy * ry * fp; v[6] += dy * rz * fp;
-                    v[7] += dz * rx * fp; v[8] += dz * ry * fp; v[9] += dz * rz * fp;
-                }
-                double ddx = -(dx * fp), ddy = -(dy * fp), ddz = -(dz * fp);
-                atomicAdd(&f[j], ddx);
-                atomicAdd(&f[nm + j], ddy);
-                atomicAdd(&f[2 * nm + j], ddz);
-                fxi += ddx; fyi += ddy; fzi += ddz;
-            }
-        }
-#pragma unroll
-        for (int o = TPA / 2; o > 0; o >>= 1) {
-            fxi += __shfl_xor_sync(0xffffffffu, fxi, o);
-            fyi += __shfl_xor_sync(0xffffffffu, fyi, o);
-            fzi += __shfl_xor_sync(0xffffffffu, fzi, o);
-            sx += __shfl_xor_sync(0xffffffffu, sx, o);
-            sy += __shfl_xor_sync(0xffffffffu, sy, o);
-            sz += __shfl_xor_sync(0xffffffffu, sz, o);
-        }
-        if (active && l == 0) {
-            atomicAdd(&f[g], -fxi);
-            atomicAdd(&f[nm + g], -fyi);
-            atomicAdd(&f[2 * nm + g], -fzi);
-            if (p.atomstress) { stress[g] = sx; stress[nm + g] = sy; stress[2 * nm + g] = sz; }
-        }
-    }
-    block_partials<10>(v, partials, 0);
-}
-
-void launch_pair_forces(DeviceState &d, const Params &p, const Tables &t, double *partials,
-                        cudaStream_t s) {
-    int nb = grid_blocks((long long)p.nm * kPairTPA, 256);
-    k_pair_forces<kPairTPA><<<nb, 256, 0, s>>>(p, t, d.pos, d.box, d.nlist, d.numn, d.mass, d.f,
-                                               d.stress, partials);
-}
 
 // ----------------------------------------------------------- box algebra --
 __device__ void mat_cofactor(const double *b, double *tc) {
@@ -280,17 +83,23 @@ __device__ void reduce_partials(const double *__restrict__ part, int nblk, doubl
 __global__ void __launch_bounds__(256)
 k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
                  int nblk_embed, const double *__restrict__ part_force, int nblk_force, int mode) {
-    __shared__ double se[10], sf[10];
-    reduce_partials<10>(part_embed, nblk_embed, se);
-    reduce_partials<10>(part_force, nblk_force, sf);
+    __shared__ double se[8], sf[7];
+    reduce_partials<8>(part_embed, nblk_embed, se);
+    reduce_partials<7>(part_force, nblk_force, sf);
     if (threadIdx.x != 0) return;
     BoxState &B = *box;
     B.pe_emb = se[0];
     B.pe_pair = sf[0];
     B.pe = se[0] + sf[0];
-    for (int k = 0; k < 9; ++k) B.tp[k] = sf[1 + k];
+    B.npairs = se[7];
+    // symmetric moments (xx, yy, zz, xy, xz, yz) -> full 3x3
+    double M[9], D[9];
+    M[0] = se[1]; M[4] = se[2]; M[8] = se[3]; M[3] = M[1] = se[4]; M[6] = M[2] = se[5]; M[7] = M[5] = se[6];
+    D[0] = sf[1]; D[4] = sf[2]; D[8] = sf[3]; D[3] = D[1] = sf[4]; D[6] = D[2] = sf[5]; D[7] = D[5] = sf[6];
     double dt2 = p.deltat * p.deltat;
-    for (int k = 0; k < 9; ++k) B.tk[k] = se[1 + k] / dt2;
+    mat_mul(B.b0, D, B.tp);                       // tp(a,b) = sum r_a d_b fp, r = B0 d
+    mat_mul(B.b0, M, B.tk);                       // tk(a,b) = sum m (B0 x1)_a x1_b
+    for (int k = 0; k < 9; ++k) B.tk[k] = B.tk[k] / dt2;
     mat_cofactor(B.b0, B.tc);
     for (int k = 0; k < 9; ++k) { B.tgdot[k] = 0.0; B.tg[k] = 0.0; }
     for (int i = 1; i <= 3; ++i)
@@ -327,8 +136,8 @@ void launch_finalize_force(DeviceState &d, const Params &p, const double *part_e
 // velocityverlet first half (src/quench_m.F90:574-589):
 //   x1_dt2 = x1 + x2; x0 += x1_dt2; box b1 += b2; b0 += b1 (ivol < 1) or zz only (ivol 4)
 __global__ void __launch_bounds__(256)
-k_drift(Params p, double4 *__restrict__ pos, const double *__restrict__ x1,
-        const double *__restrict__ x2, BoxState *__restrict__ box) {
+k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
+        const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a == 0) {
         BoxState &B = *box;
@@ -348,48 +157,12 @@ k_drift(Params p, double4 *__restrict__ pos, const double *__restrict__ x1,
     q.y = q.y + (x1[nm + a] + x2[nm + a]);
     q.z = q.z + (x1[2 * nm + a] + x2[2 * nm + a]);
     pos[a] = q;
+    posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
 }
 
 void launch_drift(DeviceState &d, const Params &p, cudaStream_t s) {
     int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
-    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.x1, d.x2, d.box);
-}
-
-// velocityverlet second half (src/quench_m.F90:606-622) with the tgid of the
-// previous update_therm_avs:  x2 = del2 f - tgid x1 / 2;  x1 = x1_dt2 + x2.
-__global__ void __launch_bounds__(256)
-k_vv_second_half(Params p, const BoxState *__restrict__ box, const double *__restrict__ f,
-                 double *__restrict__ x1, double *__restrict__ x2, const double *__restrict__ del2,
-                 const double *__restrict__ mass, const int32_t *__restrict__ znum) {
-    __shared__ double tg[9];
-    if (threadIdx.x < 9) tg[threadIdx.x] = box->tgid[threadIdx.x];
-    __syncthreads();
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= p.nm) return;
-    const int nm = p.nm;
-    double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
-    double wx = x2[a], wy = x2[nm + a], wz = x2[2 * nm + a];
-    double hx = ux + wx, hy = uy + wy, hz = uz + wz;       // x1_dt2
-    if (!(znum[a] == 0 || mass[a] < 0.1)) {
-        double sxi = 0.0, syi = 0.0, szi = 0.0;
-        if (p.ivol == 0) {
-            sxi = tg[0] * ux + tg[3] * uy + tg[6] * uz;
-            syi = tg[1] * ux + tg[4] * uy + tg[7] * uz;
-            szi = tg[2] * ux + tg[5] * uy + tg[8] * uz;
-        }
-        if (p.ivol == 4) szi = tg[8] * uz;
-        double d2 = del2[a];
-        wx = d2 * f[a] - 0.5 * sxi;
-        wy = d2 * f[nm + a] - 0.5 * syi;
-        wz = d2 * f[2 * nm + a] - 0.5 * szi;
-        x2[a] = wx; x2[nm + a] = wy; x2[2 * nm + a] = wz;
-    }
-    x1[a] = hx + wx; x1[nm + a] = hy + wy; x1[2 * nm + a] = hz + wz;
-}
-
-void launch_vv_second_half(DeviceState &d, const Params &p, cudaStream_t s) {
-    int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
-    k_vv_second_half<<<nb, kAtomThreads, 0, s>>>(p, d.box, d.f, d.x1, d.x2, d.del2, d.mass, d.znum);
+    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box);
 }
 
 // moldin strain-loop preparation (src/moldin.F90:458-471): every atom with a
@@ -530,10 +303,9 @@ k_energy_pairs(Params p, Tables t, const double4 *__restrict__ pos, const BoxSta
     if (a >= p.nm) return;
     const double4 pa = pos[a];
     const int n = numn[a];
-    const int32_t *row = nlist + (size_t)a * p.nnbrs;
     double own = 0.0;
     for (int k = 0; k < n; ++k) {
-        int j = row[k];
+        int j = nlist[(size_t)k * p.nm + a];
         double4 pj = pos[j];
         double dx = pa.x - pj.x, dy = pa.y - pj.y, dz = pa.z - pj.z;
         min_image(p.ivol, dx, dy, dz);

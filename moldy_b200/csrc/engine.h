@@ -33,10 +33,16 @@ struct DeviceState {
     // relink scratch
     int32_t *ic_new = nullptr, *arr_count = nullptr, *arr_start = nullptr, *arr_list = nullptr;
     int32_t *work = nullptr, *new_count = nullptr, *new_start = nullptr, *cell_atoms2 = nullptr;
-    // neighbour list (neighbourlist_m): nlist[i*nnbrs + k], 0-based atom ids
+    // neighbour list (neighbourlist_m), entry-major: entry k of atom i at
+    // nlist[k*nm + i], 0-based atom ids
     int32_t *nlist = nullptr, *numn = nullptr;
-    // mixed-precision mirror of positions
+    // FP32 mirror of the positions (written by drift) for the screening pass
     float4 *posf = nullptr;
+    // positions with F'(rho) in w, written by the density pass for the force pass
+    double4 *pos2 = nullptr;
+    // compact full list of interacting pairs, entry-major: own entries
+    // (e * nm + i, e < kOwnCap), then reverse entries ((kOwnCap + e) * nm + i)
+    int32_t *alist = nullptr, *own_cnt = nullptr, *rev_cnt = nullptr;
     // tables
     double4 *tab_r4 = nullptr;
     double2 *tab_e2 = nullptr;
@@ -44,7 +50,8 @@ struct DeviceState {
     float2 *tab_e2f = nullptr;
     // reductions, flags and box state
     double *partials = nullptr;
-    int32_t *flags = nullptr;     // [0] neighbour overflow, [1] cell capacity, [2] overflow atom
+    int32_t *flags = nullptr;     // [0] neighbour overflow, [1] relink inconsistency,
+                                  // [2] overflow atom, [3] active-list overflow, [4] its count
     BoxState *box = nullptr;
     int32_t *scan_tmp = nullptr;
 };
@@ -65,7 +72,7 @@ struct HostTables {
 
 // Kernel families timed by the optional per-kernel CUDA-event profiler.
 enum KernelId {
-    K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_EMBED, K_PAIR, K_FINALIZE,
+    K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_SCREEN, K_PAIR, K_FINALIZE,
     K_VV2, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_COUNT
 };
 extern const char *const kKernelNames[K_COUNT];
@@ -125,6 +132,10 @@ class Engine {
     cudaStream_t &stream_ref() { return stream_; }
     Profiler prof;
     int device() const { return device_; }
+    int precision() const { return precision_; }
+    // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
+    int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    int autotune(int nsteps, double *times_ms);
 
     DeviceState d;
     Params prm;
@@ -152,6 +163,10 @@ class Engine {
 constexpr int kAtomThreads = 256;
 constexpr int kPairTPA = 8;            // threads per atom in the pair passes
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
+constexpr int kOwnCap = 24;            // own interacting pairs per atom in the compact list
+constexpr int kRevCap = 24;            // reverse interacting pairs per atom
+constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
+constexpr int kFullTPA = 8;            // lanes per atom in the density and force passes
 
 inline int grid_blocks(long long work, int threads) {
     long long nb = (work + threads - 1) / threads;
@@ -167,15 +182,16 @@ void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
-void launch_density(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
-void launch_embed_kinten(DeviceState &d, const Params &p, const Tables &t, double *partials,
-                         cudaStream_t s);
-void launch_pair_forces(DeviceState &d, const Params &p, const Tables &t, double *partials,
-                        cudaStream_t s);
+constexpr int kVariants = 3;           // compiled variants per tunable pass
+void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
+                   cudaStream_t s);
+int launch_density_full(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
+                        double *partials, cudaStream_t s);
+int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
+                  int variant, double *partials, cudaStream_t s);
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
                            const double *part_force, int nblk_force, int mode, cudaStream_t s);
 void launch_drift(DeviceState &d, const Params &p, cudaStream_t s);
-void launch_vv_second_half(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);

@@ -6,7 +6,10 @@
 // dz=0,dy=0 dx in {0,+1}; otherwise dx,dy in {-1,0,+1}), and inside each cell
 // the atoms in chain order; in i's own cell only the atoms after i.  Lanes
 // test 32 candidates at a time and a ballot appends the accepted ones in
-// order, so NLIST(:, i) matches the reference entry for entry.  The distance
+// order, so NLIST(:, i) matches the reference entry for entry.  The list is
+// stored entry-major (entry k of atom i at k*nm + i) so that the per-step
+// passes, one thread per atom, read it in contiguous 128-byte rows; the export
+// transposes it to the reference's NLIST(nnbrs, nm).  The distance
 // test uses separately rounded products and sums (no FMA), as the Fortran
 // evaluates pr_get_realsep_from_dx, so r < rnear gives the same pair set.
 #include "engine.h"
@@ -43,7 +46,6 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const BoxState *__restr
     const int cx = c % p.nlcx, cy = (c / p.nlcx) % p.nlcy, cz = c / (p.nlcx * p.nlcy);
     const double4 pa = pos[a];
     int count = 0;
-    int32_t *row = nlist + (size_t)a * p.nnbrs;
     const unsigned lt = (1u << lane) - 1u;
     for (int s = 0; s < 14; ++s) {
         int jx = wrap(cx + c_stencil[s][0], p.nlcx);
@@ -68,7 +70,7 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const BoxState *__restr
             unsigned bal = __ballot_sync(0xffffffffu, take);
             if (take) {
                 int slot = count + __popc(bal & lt);
-                if (slot < p.nnbrs) row[slot] = j;
+                if (slot < p.nnbrs) nlist[(size_t)slot * p.nm + a] = j;
             }
             count += __popc(bal);
         }
@@ -95,7 +97,7 @@ __global__ void k_export_nlist(int nm, int nnbrs, const int32_t *__restrict__ nl
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)nm * nnbrs) return;
     int a = (int)(e / nnbrs), k = (int)(e % nnbrs);
-    out[e] = k < numn[a] ? nlist[e] + 1 : 0;
+    out[e] = k < numn[a] ? nlist[(size_t)k * nm + a] + 1 : 0;
 }
 
 void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s) {

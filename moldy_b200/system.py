@@ -271,6 +271,27 @@ class MoldySystem:
     def reset_kernel_stats(self):
         check(self._L.moldy_gpu_reset_kernel_stats(self._h))
 
+    def autotune(self, nreps: int = 5) -> dict:
+        """Times each compiled variant of the screening, density and force
+        passes on the current configuration and keeps the fastest."""
+        import numpy as _np
+        t = _np.zeros(3 * _lib.TUNE_VARIANTS)
+        ch = _np.zeros(3, dtype=_np.int32)
+        check(self._L.moldy_gpu_autotune(self._h, int(nreps), _dp(t), _ip(ch)))
+        names = ("screen", "density", "forces")
+        return {"chosen": dict(zip(names, ch.tolist())),
+                "ms": {n: t[k * _lib.TUNE_VARIANTS:(k + 1) * _lib.TUNE_VARIANTS].tolist()
+                       for k, n in enumerate(names)}}
+
+    def pair_count(self) -> float:
+        """Directed interacting pairs of the last force evaluation."""
+        v = np.zeros(1)
+        check(self._L.moldy_gpu_get_pair_count(self._h, _dp(v)))
+        return float(v[0])
+
+    def set_variants(self, screen: int, density: int, forces: int):
+        check(self._L.moldy_gpu_set_variants(self._h, int(screen), int(density), int(forces)))
+
     def kernel_stats(self) -> dict:
         """{family: (total_ms, launches)} since the last reset."""
         out = {}
