@@ -193,9 +193,11 @@ const char *moldy_gpu_kernel_name(int32_t kernel);
 #define MOLDY_TUNE_VARIANTS 3
 int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
 int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
-/* Directed interacting pairs (inside the table range) of the last force
- * evaluation, i.e. twice the number of contributing half-list pairs. */
-int moldy_gpu_get_pair_count(moldy_gpu *h, double *npairs);
+/* out2[0]: directed interacting pairs (inside the table range) of the last
+ * force evaluation, twice the contributing half-list pairs; out2[1]: how many
+ * times the intermediate list (half-list pairs within the table cut + 0.9 A)
+ * has been built. */
+int moldy_gpu_get_list_stats(moldy_gpu *h, double *out2);
 
 /* force evaluation without device allocation -----------------------------*/
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -99,7 +99,7 @@ SIGNATURES = {
     "moldy_gpu_kernel_name": [ctypes.c_int32],
     "moldy_gpu_autotune": [H, ctypes.c_int32, D, I],
     "moldy_gpu_set_variants": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
-    "moldy_gpu_get_pair_count": [H, D],
+    "moldy_gpu_get_list_stats": [H, D],
     "moldy_gpu_force_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, D, ctypes.c_void_p, ctypes.c_void_p,

@@ -81,7 +81,7 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
     "drift", "linkup", "relink", "build_nlist", "density", "screen", "forces",
-    "finalize_force", "unused", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
+    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {
@@ -167,7 +167,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
-                    d.own_cnt, d.rev_cnt, d.tab_r4, d.tab_e2,
+                    d.own_cnt, d.rev_cnt, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -230,6 +230,9 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.pos2, nm, "pos2"));
     CHECK(dev_alloc(&d.alist, nm * (size_t)(kOwnCap + kRevCap), "active list"));
     CHECK(dev_alloc(&d.own_cnt, nm, "own_cnt"));
+    CHECK(dev_alloc(&d.mlist, nm * (size_t)kMidCap, "intermediate list"));
+    CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
+    CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
     CHECK(dev_alloc(&d.rev_cnt, nm, "rev_cnt"));
     CHECK(dev_alloc(&d.partials, 2 * (size_t)kMaxBlocks * kPartials, "partials"));
     CHECK(dev_alloc(&d.flags, 8, "flags"));
@@ -246,6 +249,8 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.posf, 0, nm * sizeof(float4)), "memset posf");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
     CUDA_CHECK(cudaMemset(d.own_cnt, 0, nm * sizeof(int32_t)), "memset own_cnt");
+    CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
+    CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(double4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.rev_cnt, 0, nm * sizeof(int32_t)), "memset rev_cnt");
     CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
@@ -323,6 +328,8 @@ int Engine::upload_tables() {
     double rc = rcull < 1e150 ? rcull * (1.0 + 1.0e-12) : 1.0e150;
     t.rcull2 = rc * rc;
     t.rcull2f = (float)(rc * rc * (1.0 + 1.0e-6));
+    rcut = rc < 1e150 ? rc : prm.rnear;
+    rmid = std::min(prm.rnear, rcut + kMidSkin);
     t.nv = h.nv; t.np = h.np;
     for (int i = 0; i < 8; ++i) { t.av[i] = h.av[i]; t.rv[i] = h.rv[i]; t.ap[i] = h.ap[i]; t.rp[i] = h.rp[i]; }
     t.bier_cut1 = h.bier_cut1; t.bier_cut2 = h.bier_cut2;
@@ -555,14 +562,18 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     DeviceState &d = E.d;
     const Params &p = E.prm;
     ntc = ntc + 1;
-    bool rb = false;
-    if (ntc == 1 || !list_ready) {
+    const bool rb = (ntc == 1 || !list_ready);
+    // mode 1 (velocity Verlet) advances the box here, after the drift kernel;
+    // force calls outside velocity Verlet always rebuild the intermediate list
+    LAUNCH(E, K_MID, 1, s,
+           launch_mid_decide(d, p, E.rmid, E.rcut, (mode == 1 && !rb) ? 0 : 1, mode == 1 ? 1 : 0, s));
+    if (rb) {
         if (!cells_ready) { LAUNCH(E, K_LINKUP, 4, s, launch_linkup(d, p, s)); cells_ready = true; }
         LAUNCH(E, K_NLIST, 1, s, launch_build_nlist(d, p, s));
         list_ready = true;
-        rb = true;
     }
     if (ntc == ntcm) ntc = 0;
+    LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, s));
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     int nbe = 0, nbf = 0;
@@ -712,6 +723,8 @@ int Engine::autotune(int nreps, double *times_ms) {
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[3] = {K_SCREEN, K_DENSITY, K_PAIR};
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, 1, 0, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
         LAUNCH(*this, K_SCREEN, 1, stream_, launch_screen(d, prm, tab, mixed, variant[K_SCREEN], stream_));
@@ -982,13 +995,19 @@ int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *c
     return rc;
 }
 
-int moldy_gpu_get_pair_count(moldy_gpu *h, double *npairs) {
+int moldy_gpu_get_list_stats(moldy_gpu *h, double *out2) {
     GUARD(h);
-    if (!npairs) return fail(MOLDY_ERR_INVALID, "null argument");
-    cudaError_t e = cudaMemcpyAsync(npairs, &h->e->d.box->npairs, sizeof(double),
-                                    cudaMemcpyDeviceToHost, h->e->stream_ref());
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->e->stream_ref());
-    if (e != cudaSuccess) return moldy::cuda_fail(e, "get_pair_count");
+    if (!out2) return fail(MOLDY_ERR_INVALID, "null argument");
+    double np = 0.0;
+    int32_t nb = 0;
+    cudaStream_t st = h->e->stream_ref();
+    cudaError_t e = cudaMemcpyAsync(&np, &h->e->d.box->npairs, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&nb, &h->e->d.box->mid_builds, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return moldy::cuda_fail(e, "get_list_stats");
+    out2[0] = np;
+    out2[1] = (double)nb;
     return MOLDY_OK;
 }
 

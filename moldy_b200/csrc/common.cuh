@@ -22,6 +22,10 @@ struct BoxState {
     double s1, s2, s3, ke, te, h, th, boxke, temp;
     double maxdisp;
     double npairs;                 // directed interacting pairs in the last density pass
+    double bbuild[9];              // B0 when the intermediate list was built
+    unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
+    int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
+    int32_t mid_builds;            // number of intermediate-list builds so far
     int32_t status;                // nonzero: singular box in a device-side inversion
     int32_t pad;
 };
@@ -276,6 +280,55 @@ __device__ __forceinline__ double2 embed_funcs(const Tables &t, double rho) {
         return make_double2(f, d);
     }
     return lookup_e2(t, rho);
+}
+
+// ----------------------------------------------------------- box algebra --
+__device__ __forceinline__ void mat_cofactor(const double *b, double *tc) {
+    // tc as in src/dynamics_m.F90:365-373
+    MAT(tc, 1, 1) = MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2);
+    MAT(tc, 2, 1) = MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3);
+    MAT(tc, 3, 1) = MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3);
+    MAT(tc, 1, 2) = MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1);
+    MAT(tc, 2, 2) = MAT(b, 3, 3) * MAT(b, 1, 1) - MAT(b, 1, 3) * MAT(b, 3, 1);
+    MAT(tc, 3, 2) = MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3);
+    MAT(tc, 1, 3) = MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2);
+    MAT(tc, 2, 3) = MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2);
+    MAT(tc, 3, 3) = MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 2, 1) * MAT(b, 1, 2);
+}
+
+__device__ __forceinline__ double mat_volume(const double *b) {
+    // pr_get_metric_tensor (src/parrinellorahman_m.F90:223-227)
+    return MAT(b, 1, 1) * (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) +
+           MAT(b, 2, 1) * (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) +
+           MAT(b, 3, 1) * (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3));
+}
+
+// matrix_invert (src/matrix_m.F90:89-119); returns false for det == 0
+__device__ __forceinline__ bool mat_invert(const double *a, double *bo) {
+    double deta = MAT(a, 1, 1) * (MAT(a, 2, 2) * MAT(a, 3, 3) - MAT(a, 2, 3) * MAT(a, 3, 2));
+    deta = deta + MAT(a, 2, 1) * (MAT(a, 3, 2) * MAT(a, 1, 3) - MAT(a, 1, 2) * MAT(a, 3, 3));
+    deta = deta + MAT(a, 3, 1) * (MAT(a, 1, 2) * MAT(a, 2, 3) - MAT(a, 1, 3) * MAT(a, 2, 2));
+    MAT(bo, 1, 1) = MAT(a, 2, 2) * MAT(a, 3, 3) - MAT(a, 2, 3) * MAT(a, 3, 2);
+    MAT(bo, 1, 2) = MAT(a, 3, 1) * MAT(a, 2, 3) - MAT(a, 2, 1) * MAT(a, 3, 3);
+    MAT(bo, 1, 3) = MAT(a, 2, 1) * MAT(a, 3, 2) - MAT(a, 3, 1) * MAT(a, 2, 2);
+    MAT(bo, 2, 1) = MAT(a, 3, 2) * MAT(a, 1, 3) - MAT(a, 1, 2) * MAT(a, 3, 3);
+    MAT(bo, 2, 2) = MAT(a, 1, 1) * MAT(a, 3, 3) - MAT(a, 1, 3) * MAT(a, 3, 1);
+    MAT(bo, 2, 3) = MAT(a, 3, 1) * MAT(a, 1, 2) - MAT(a, 1, 1) * MAT(a, 3, 2);
+    MAT(bo, 3, 1) = MAT(a, 1, 2) * MAT(a, 2, 3) - MAT(a, 1, 3) * MAT(a, 2, 2);
+    MAT(bo, 3, 2) = MAT(a, 2, 1) * MAT(a, 1, 3) - MAT(a, 2, 3) * MAT(a, 1, 1);
+    MAT(bo, 3, 3) = MAT(a, 1, 1) * MAT(a, 2, 2) - MAT(a, 1, 2) * MAT(a, 2, 1);
+    if (fabs(deta) == 0.0) return false;
+    for (int k = 0; k < 9; ++k) bo[k] = bo[k] / deta;
+    return true;
+}
+
+// matrix_multiply (src/matrix_m.F90:60-79)
+__device__ __forceinline__ void mat_mul(const double *a, const double *b, double *c) {
+    for (int i = 1; i <= 3; ++i) {
+        for (int j = 1; j <= 3; ++j) MAT(c, i, j) = 0.0;
+        for (int k = 1; k <= 3; ++k)
+            for (int j = 1; j <= 3; ++j) MAT(c, i, j) = MAT(c, i, j) + MAT(a, i, k) * MAT(b, k, j);
+    }
 }
 
 // ------------------------------------------------------------ reductions --

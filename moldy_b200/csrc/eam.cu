@@ -5,55 +5,6 @@
 
 namespace moldy {
 
-// ----------------------------------------------------------- box algebra --
-__device__ void mat_cofactor(const double *b, double *tc) {
-    // tc as in src/dynamics_m.F90:365-373
-    MAT(tc, 1, 1) = MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2);
-    MAT(tc, 2, 1) = MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3);
-    MAT(tc, 3, 1) = MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3);
-    MAT(tc, 1, 2) = MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1);
-    MAT(tc, 2, 2) = MAT(b, 3, 3) * MAT(b, 1, 1) - MAT(b, 1, 3) * MAT(b, 3, 1);
-    MAT(tc, 3, 2) = MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3);
-    MAT(tc, 1, 3) = MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2);
-    MAT(tc, 2, 3) = MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2);
-    MAT(tc, 3, 3) = MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 2, 1) * MAT(b, 1, 2);
-}
-
-__device__ double mat_volume(const double *b) {
-    // pr_get_metric_tensor (src/parrinellorahman_m.F90:223-227)
-    return MAT(b, 1, 1) * (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) +
-           MAT(b, 2, 1) * (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) +
-           MAT(b, 3, 1) * (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3));
-}
-
-// matrix_invert (src/matrix_m.F90:89-119); returns false for det == 0
-__device__ bool mat_invert(const double *a, double *bo) {
-    double deta = MAT(a, 1, 1) * (MAT(a, 2, 2) * MAT(a, 3, 3) - MAT(a, 2, 3) * MAT(a, 3, 2));
-    deta = deta + MAT(a, 2, 1) * (MAT(a, 3, 2) * MAT(a, 1, 3) - MAT(a, 1, 2) * MAT(a, 3, 3));
-    deta = deta + MAT(a, 3, 1) * (MAT(a, 1, 2) * MAT(a, 2, 3) - MAT(a, 1, 3) * MAT(a, 2, 2));
-    MAT(bo, 1, 1) = MAT(a, 2, 2) * MAT(a, 3, 3) - MAT(a, 2, 3) * MAT(a, 3, 2);
-    MAT(bo, 1, 2) = MAT(a, 3, 1) * MAT(a, 2, 3) - MAT(a, 2, 1) * MAT(a, 3, 3);
-    MAT(bo, 1, 3) = MAT(a, 2, 1) * MAT(a, 3, 2) - MAT(a, 3, 1) * MAT(a, 2, 2);
-    MAT(bo, 2, 1) = MAT(a, 3, 2) * MAT(a, 1, 3) - MAT(a, 1, 2) * MAT(a, 3, 3);
-    MAT(bo, 2, 2) = MAT(a, 1, 1) * MAT(a, 3, 3) - MAT(a, 1, 3) * MAT(a, 3, 1);
-    MAT(bo, 2, 3) = MAT(a, 3, 1) * MAT(a, 1, 2) - MAT(a, 1, 1) * MAT(a, 3, 2);
-    MAT(bo, 3, 1) = MAT(a, 1, 2) * MAT(a, 2, 3) - MAT(a, 1, 3) * MAT(a, 2, 2);
-    MAT(bo, 3, 2) = MAT(a, 2, 1) * MAT(a, 1, 3) - MAT(a, 2, 3) * MAT(a, 1, 1);
-    MAT(bo, 3, 3) = MAT(a, 1, 1) * MAT(a, 2, 2) - MAT(a, 1, 2) * MAT(a, 2, 1);
-    if (fabs(deta) == 0.0) return false;
-    for (int k = 0; k < 9; ++k) bo[k] = bo[k] / deta;
-    return true;
-}
-
-// matrix_multiply (src/matrix_m.F90:60-79)
-__device__ void mat_mul(const double *a, const double *b, double *c) {
-    for (int i = 1; i <= 3; ++i) {
-        for (int j = 1; j <= 3; ++j) MAT(c, i, j) = 0.0;
-        for (int k = 1; k <= 3; ++k)
-            for (int j = 1; j <= 3; ++j) MAT(c, i, j) = MAT(c, i, j) + MAT(a, i, k) * MAT(b, k, j);
-    }
-}
-
 // Sums NV partial columns over nblk blocks in a fixed order into out[NV].
 template <int NV>
 __device__ void reduce_partials(const double *__restrict__ part, int nblk, double *out) {
@@ -133,36 +84,65 @@ void launch_finalize_force(DeviceState &d, const Params &p, const double *part_e
 }
 
 // ------------------------------------------------------------- integrator --
-// velocityverlet first half (src/quench_m.F90:574-589):
-//   x1_dt2 = x1 + x2; x0 += x1_dt2; box b1 += b2; b0 += b1 (ivol < 1) or zz only (ivol 4)
+// velocityverlet first half (src/quench_m.F90:574-589): x1_dt2 = x1 + x2;
+// x0 += x1_dt2.  The box half (b1 += b2; b0 += b1 for ivol < 1, zz only for
+// ivol 4) is applied by k_mid_decide, which runs next.
 __global__ void __launch_bounds__(256)
 k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
-        const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a == 0) {
-        BoxState &B = *box;
+        const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
+        const double4 *__restrict__ xbuild) {
+    // every thread forms the post-drift box exactly as thread 0 stores it
+    __shared__ double nb[9];
+    if (threadIdx.x == 0) {
+        const BoxState &B = *box;
+        double b1[9], b0[9];
+        for (int k = 0; k < 9; ++k) { b1[k] = B.b1[k]; b0[k] = B.b0[k]; }
         if (p.ivol == 4) {
-            MAT(B.b1, 3, 3) = MAT(B.b1, 3, 3) + MAT(B.b2, 3, 3);
-            MAT(B.b0, 3, 3) = MAT(B.b0, 3, 3) + MAT(B.b1, 3, 3);
+            MAT(b1, 3, 3) = MAT(b1, 3, 3) + MAT(B.b2, 3, 3);
+            MAT(b0, 3, 3) = MAT(b0, 3, 3) + MAT(b1, 3, 3);
         }
         if (p.ivol < 1) {
-            for (int k = 0; k < 9; ++k) B.b1[k] = B.b1[k] + B.b2[k];
-            for (int k = 0; k < 9; ++k) B.b0[k] = B.b0[k] + B.b1[k];
+            for (int k = 0; k < 9; ++k) b1[k] = b1[k] + B.b2[k];
+            for (int k = 0; k < 9; ++k) b0[k] = b0[k] + b1[k];
         }
+        for (int k = 0; k < 9; ++k) nb[k] = b0[k];
     }
-    if (a >= p.nm) return;
-    const int nm = p.nm;
-    double4 q = pos[a];
-    q.x = q.x + (x1[a] + x2[a]);
-    q.y = q.y + (x1[nm + a] + x2[nm + a]);
-    q.z = q.z + (x1[2 * nm + a] + x2[2 * nm + a]);
-    pos[a] = q;
-    posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+    __syncthreads();
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double d2 = 0.0;
+    if (a < p.nm) {
+        const int nm = p.nm;
+        double4 q = pos[a];
+        q.x = q.x + (x1[a] + x2[a]);
+        q.y = q.y + (x1[nm + a] + x2[nm + a]);
+        q.z = q.z + (x1[2 * nm + a] + x2[2 * nm + a]);
+        pos[a] = q;
+        posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+        double4 xb = xbuild[a];
+        double ux = q.x - xb.x, uy = q.y - xb.y, uz = q.z - xb.z;
+        double rx = nb[0] * ux + nb[3] * uy + nb[6] * uz;
+        double ry = nb[1] * ux + nb[4] * uy + nb[7] * uz;
+        double rz = nb[2] * ux + nb[5] * uy + nb[8] * uz;
+        d2 = rx * rx + ry * ry + rz * rz;
+    }
+    // block maximum, then one atomic per block (non-negative doubles order as their bits)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    __shared__ double wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+        atomicMax(&box->maxdisp2, (unsigned long long)__double_as_longlong(m));
+    }
+    // the box itself is advanced afterwards by k_mid_decide, so that no block
+    // here can read a box another block has already moved
 }
 
 void launch_drift(DeviceState &d, const Params &p, cudaStream_t s) {
     int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
-    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box);
+    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild);
 }
 
 // moldin strain-loop preparation (src/moldin.F90:458-471): every atom with a

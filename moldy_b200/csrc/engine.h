@@ -43,6 +43,11 @@ struct DeviceState {
     // compact full list of interacting pairs, entry-major: own entries
     // (e * nm + i, e < kOwnCap), then reverse entries ((kOwnCap + e) * nm + i)
     int32_t *alist = nullptr, *own_cnt = nullptr, *rev_cnt = nullptr;
+    // intermediate half list (pairs within r_mid when built), entry-major like
+    // nlist; mid_cnt < 0 marks an atom whose row overflowed (screen then reads
+    // its full half-list row); xbuild holds the positions at build time
+    int32_t *mlist = nullptr, *mid_cnt = nullptr;
+    double4 *xbuild = nullptr;
     // tables
     double4 *tab_r4 = nullptr;
     double2 *tab_e2 = nullptr;
@@ -73,7 +78,7 @@ struct HostTables {
 // Kernel families timed by the optional per-kernel CUDA-event profiler.
 enum KernelId {
     K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_SCREEN, K_PAIR, K_FINALIZE,
-    K_VV2, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_COUNT
+    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_COUNT
 };
 extern const char *const kKernelNames[K_COUNT];
 
@@ -136,6 +141,7 @@ class Engine {
     // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
     int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
     int autotune(int nsteps, double *times_ms);
+    double rmid = 0.0, rcut = 0.0;   // intermediate-list radius and table cut (A)
 
     DeviceState d;
     Params prm;
@@ -165,6 +171,8 @@ constexpr int kPairTPA = 8;            // threads per atom in the pair passes
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
 constexpr int kOwnCap = 24;            // own interacting pairs per atom in the compact list
 constexpr int kRevCap = 24;            // reverse interacting pairs per atom
+constexpr int kMidCap = 40;            // half-list pairs per atom in the intermediate list
+constexpr double kMidSkin = 0.9;       // r_mid = table cut + kMidSkin (A), at most rnear
 constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
 constexpr int kFullTPA = 8;            // lanes per atom in the density and force passes
 
@@ -192,6 +200,9 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
                            const double *part_force, int nblk_force, int mode, cudaStream_t s);
 void launch_drift(DeviceState &d, const Params &p, cudaStream_t s);
+void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
+                       int apply_box, cudaStream_t s);
+void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);

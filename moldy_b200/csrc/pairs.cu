@@ -78,7 +78,8 @@ template <bool MIXED, int B>
 __global__ void __launch_bounds__(256)
 k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
          const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
-         const int32_t *__restrict__ numn, int32_t *__restrict__ alist,
+         const int32_t *__restrict__ numn, const int32_t *__restrict__ mlist,
+         const int32_t *__restrict__ mid_cnt, int32_t *__restrict__ alist,
          int32_t *__restrict__ own_cnt, int32_t *__restrict__ rev_cnt) {
     __shared__ double sb[9];
     __shared__ float srs2, srin2;
@@ -101,8 +102,11 @@ k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__re
     const int nm = p.nm;
     const size_t stride = (size_t)nm;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const int n = numn[a];
-        const int32_t *col = nlist + a;
+        // the intermediate row (pairs within r_mid at its build), or the full
+        // half-list row when that row overflowed
+        const int mc = mid_cnt[a];
+        const int n = mc >= 0 ? mc : numn[a];
+        const int32_t *col = (mc >= 0 ? mlist : nlist) + a;
         const float4 pf = posf[a];
         int cnt = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
@@ -345,6 +349,108 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
     block_partials<7>(v, partials, 0);
 }
 
+// ------------------------------------------------------ intermediate list --
+// The screen walks, per atom, the half-list pairs that were within
+// r_mid = r_cut + skin when the intermediate list was last built.  A pair
+// left out was farther than r_mid - eps then (eps bounds the FP32 distance
+// error); since then its distance can have shrunk by at most
+// 2 max_i |B0 (x_i - x_i,build)| + |B0 - B0_build|_F dmax, with dmax = rnear
+// |B0_build^-1|_F bounding the fractional separation of any listed pair.  The
+// list is rebuilt before that bound reaches the screening radius, and after
+// every half-list rebuild and every force call outside velocity Verlet, so
+// the screen keeps exactly the pairs a walk over the whole half list keeps.
+__device__ double frob(const double *m) {
+    double s = 0.0;
+    for (int k = 0; k < 9; ++k) s += m[k] * m[k];
+    return sqrt(s);
+}
+
+__global__ void k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut,
+                             int force, int apply_box) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    BoxState &B = *box;
+    if (apply_box) {   // velocityverlet box half (src/quench_m.F90:582-589)
+        if (p.ivol == 4) {
+            MAT(B.b1, 3, 3) = MAT(B.b1, 3, 3) + MAT(B.b2, 3, 3);
+            MAT(B.b0, 3, 3) = MAT(B.b0, 3, 3) + MAT(B.b1, 3, 3);
+        }
+        if (p.ivol < 1) {
+            for (int k = 0; k < 9; ++k) B.b1[k] = B.b1[k] + B.b2[k];
+            for (int k = 0; k < 9; ++k) B.b0[k] = B.b0[k] + B.b1[k];
+        }
+    }
+    double md = sqrt(__longlong_as_double((long long)B.maxdisp2));
+    B.maxdisp2 = 0ull;
+    double eps = 2.0e-6 * frob(B.b0) + 1.0e-4;
+    double db[9], inv[9];
+    for (int k = 0; k < 9; ++k) db[k] = B.b0[k] - B.bbuild[k];
+    bool ok = mat_invert(B.bbuild, inv);
+    double dmax = ok ? p.rnear * frob(inv) : 1e300;
+    double shrink = 2.0 * md + frob(db) * dmax;
+    int need = force || !ok || !(shrink < rmid - eps - (rcut + eps));
+    B.mid_rebuild = need;
+    if (need) {
+        for (int k = 0; k < 9; ++k) B.bbuild[k] = B.b0[k];
+        B.mid_builds += 1;
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
+            const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
+            const int32_t *__restrict__ numn, int32_t *__restrict__ mlist,
+            int32_t *__restrict__ mid_cnt, double4 *__restrict__ xbuild) {
+    __shared__ double sb[9];
+    __shared__ float skeep2;
+    __shared__ int sneed;
+    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
+    if (threadIdx.x == 0) sneed = box->mid_rebuild;
+    __syncthreads();
+    if (!sneed) return;
+    if (threadIdx.x == 0) {
+        float keep = (float)(rmid + 2.0 * (2.0e-6 * frob(sb) + 1.0e-4));
+        // when a box is too small for the FP32 screen, keep every listed pair
+        skeep2 = screen_radius2(sb, rmid * rmid) > 1e37f ? 3.0e38f : keep * keep;
+    }
+    __syncthreads();
+    float bf[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) bf[k] = (float)sb[k];
+    const float keep2 = skeep2;
+    const int nm = p.nm;
+    const size_t stride = (size_t)nm;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        const int n = numn[a];
+        const int32_t *col = nlist + a;
+        const float4 pf = posf[a];
+        int cnt = 0;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+            const int j = __ldg(&col[(size_t)k * stride]);
+            const float4 q = __ldg(&posf[j]);
+            float rx, ry, rz, r2, dx, dy, dz;
+            fsep<true>(bf, p.ivol, pf.x - q.x, pf.y - q.y, pf.z - q.z, rx, ry, rz, r2, dx, dy, dz);
+            if (r2 <= keep2) {
+                if (cnt < kMidCap) mlist[(size_t)cnt * stride + a] = j;
+                ++cnt;
+            }
+        }
+        mid_cnt[a] = cnt <= kMidCap ? cnt : -1;
+        xbuild[a] = pos[a];
+    }
+}
+
+void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
+                       int apply_box, cudaStream_t s) {
+    k_mid_decide<<<1, 32, 0, s>>>(p, d.box, rmid, rcut, force, apply_box);
+}
+
+void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
+    int nb = grid_blocks(p.nm, 256);
+    k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist,
+                                   d.mid_cnt, d.xbuild);
+}
+
 // ------------------------------------------------------------ launchers --
 // Variant v selects the batch of list entries whose gathers are issued before
 // any of them is used: screen {4, 8, 16}, density {2, 4, 8}, forces {2, 4, 8}.
@@ -353,7 +459,8 @@ void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed,
                    cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
     cudaMemsetAsync(d.rev_cnt, 0, sizeof(int32_t) * p.nm, s);
-#define SCREEN_ARGS p, t, d.pos, d.posf, d.box, d.nlist, d.numn, d.alist, d.own_cnt, d.rev_cnt
+#define SCREEN_ARGS p, t, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist, d.mid_cnt, d.alist, \
+                    d.own_cnt, d.rev_cnt
 #define SCREEN(M, B) k_screen<M, B><<<nb, 256, 0, s>>>(SCREEN_ARGS)
     switch (variant) {
     case 0: if (mixed) SCREEN(true, 4); else SCREEN(false, 4); break;

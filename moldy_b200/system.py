@@ -283,11 +283,15 @@ class MoldySystem:
                 "ms": {n: t[k * _lib.TUNE_VARIANTS:(k + 1) * _lib.TUNE_VARIANTS].tolist()
                        for k, n in enumerate(names)}}
 
+    def list_stats(self) -> dict:
+        """Directed interacting pairs of the last force evaluation and the
+        number of intermediate-list builds so far."""
+        v = np.zeros(2)
+        check(self._L.moldy_gpu_get_list_stats(self._h, _dp(v)))
+        return {"pairs": float(v[0]), "mid_builds": int(v[1])}
+
     def pair_count(self) -> float:
-        """Directed interacting pairs of the last force evaluation."""
-        v = np.zeros(1)
-        check(self._L.moldy_gpu_get_pair_count(self._h, _dp(v)))
-        return float(v[0])
+        return self.list_stats()["pairs"]
 
     def set_variants(self, screen: int, density: int, forces: int):
         check(self._L.moldy_gpu_set_variants(self._h, int(screen), int(density), int(forces)))

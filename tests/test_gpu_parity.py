@@ -270,3 +270,23 @@ def test_mixed_precision_accuracy(oracle_mod, gpu_lib):
     vol = o64["vol"]
     sig = lambda o: -(w.b0 @ (o["tp"]).T).T / vol * units.PRESS_TO_GPA
     assert np.max(np.abs(sig(omx) - sig(o64))) < 1e-4           # GPa
+
+
+def test_md_hot_intermediate_list_rebuilds(oracle_mod, gpu_lib):
+    """3000 K, 80 steps, no half-list rebuild: atoms move far enough that the
+    intermediate list must be rebuilt from the displacement bound, and the
+    trajectory still follows the oracle, which walks the whole half list."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(8, sigma=0.1, temperature=3000.0, ivol=1, seed=13, nbrupdate=200)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=1)
+    g = MoldySystem.from_workload(w)
+    o.md_init()
+    g.md_init()
+    th_o = [o.md_step() for _ in range(80)]
+    th_g = g.md_steps(80)
+    assert g.list_stats()["mid_builds"] >= 3
+    a = np.array([t["pe"] for t in th_o])
+    b = np.array([t["pe"] for t in th_g])
+    assert np.max(np.abs(a - b)) < 1e-8 * np.max(np.abs(a))
+    so, sg = o.get_state(), g.get_state()
+    assert np.max(np.abs((sg["x0"] - so["x0"]) @ w.b0.T)) < 1e-7
