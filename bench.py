@@ -369,6 +369,7 @@ def run_ours(args):
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
         "clocks": clk.summary(), "gpu_launches": launches,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in stats.items() if v[1]},
+        "autotune_ms_per_launch": tune["ms"],
     }
     print(json.dumps(line), flush=True)
     return 0

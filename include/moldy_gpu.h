@@ -184,13 +184,14 @@ const char *moldy_gpu_kernel_name(int32_t kernel);
 
 /* kernel variants (no counterpart in the reference) -------------------------*/
 /* The screening, density and force passes are compiled in MOLDY_TUNE_VARIANTS
- * variants each (how many list entries a thread gathers before using them).
+ * variants each (how many list entries a thread gathers before using them,
+ * with or without L2 prefetches of the next atom's data).
  * moldy_gpu_autotune times every variant on the current configuration with
  * nreps force evaluations (positions, velocities, the rebuild counter and the
  * neighbour list are left unchanged) and keeps the fastest of each pass.
  * times_ms (3*MOLDY_TUNE_VARIANTS, may be NULL) receives the mean time per
  * launch; chosen (3, may be NULL) the selected variants. */
-#define MOLDY_TUNE_VARIANTS 3
+#define MOLDY_TUNE_VARIANTS 4
 int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
 int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
 /* out2[0]: directed interacting pairs (inside the table range) of the last

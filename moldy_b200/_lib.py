@@ -108,7 +108,7 @@ SIGNATURES = {
 }
 NOALLOC_MAX_ATOMS = 262144
 KERNEL_FAMILIES = 13
-TUNE_VARIANTS = 3
+TUNE_VARIANTS = 4
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}
 

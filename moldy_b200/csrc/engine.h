@@ -190,7 +190,7 @@ void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
-constexpr int kVariants = 3;           // compiled variants per tunable pass
+constexpr int kVariants = 4;           // compiled variants per tunable pass
 void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
                    cudaStream_t s);
 int launch_density_full(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,

@@ -29,6 +29,12 @@
 namespace moldy {
 
 
+// L2 prefetch of one address (no register result; the address is always
+// inside an allocated buffer)
+__device__ __forceinline__ void prefetch_l2(const void *ptr) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 template <bool MIXED>
 __device__ __forceinline__ void fsep(const float *bf, int ivol, float dx, float dy, float dz,
                                      float &rx, float &ry, float &rz, float &r2,
@@ -74,7 +80,7 @@ __device__ float screen_radius2(const double *b, double rcull2) {
 // Keeps pair (a, j) iff its distance is inside the table range.  In FP64 mode
 // the FP32 distance decides outright when it is farther than the error bound
 // from the cut (rin2 .. rscreen2 is the only band that needs the FP64 test).
-template <bool MIXED, int B>
+template <bool MIXED, int B, bool PF>
 __global__ void __launch_bounds__(256)
 k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
          const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
@@ -101,7 +107,15 @@ k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__re
     for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bf[k] = (float)sb[k]; }
     const int nm = p.nm;
     const size_t stride = (size_t)nm;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+    const int astride = gridDim.x * blockDim.x;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += astride) {
+        if (PF && a + astride < nm) {   // next atom of this thread: its rows into L2
+            const int an = a + astride;
+#pragma unroll
+            for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
+            prefetch_l2(&mid_cnt[an]);
+            prefetch_l2(&posf[an]);
+        }
         // the intermediate row (pairs within r_mid at its build), or the full
         // half-list row when that row overflowed
         const int mc = mid_cnt[a];
@@ -164,7 +178,7 @@ __device__ __forceinline__ size_t alist_index(int e, int no, int a, int nm) {
 
 // -------------------------------------------------------------- density --
 // rho_i = sum phi over the compact row; embed; M = sum m x1 x1^T for kinten
-template <bool MIXED, bool EXACT, int B>
+template <bool MIXED, bool EXACT, int B, bool PF>
 __global__ void __launch_bounds__(256)
 k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__restrict__ pos2,
                const BoxState *__restrict__ box, const int32_t *__restrict__ alist,
@@ -184,7 +198,19 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = 0.0;
     const int nm = p.nm;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+    const int astride = gridDim.x * blockDim.x;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += astride) {
+        if (PF && a + astride < nm) {
+            const int an = a + astride;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                prefetch_l2(&alist[(size_t)u * nm + an]);
+                prefetch_l2(&alist[(size_t)(kOwnCap + u) * nm + an]);
+            }
+            prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos[an]);
+            prefetch_l2(&dafrho[an]); prefetch_l2(&mass[an]); prefetch_l2(&znum[an]);
+            prefetch_l2(&x1[an]); prefetch_l2(&x1[nm + an]); prefetch_l2(&x1[2 * nm + an]);
+        }
         int no, nr;
         bool over;
         alist_counts(own_cnt, rev_cnt, a, no, nr, over);
@@ -246,7 +272,7 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
 // --------------------------------------------------------------- forces --
 // f_i = sum dx fp over the compact row; pe and the virial moment
 // D = sum d d^T fp / 2 (tp = B0 D); mode 1 adds the velocity-Verlet second half
-template <bool MIXED, bool EXACT, int B>
+template <bool MIXED, bool EXACT, int B, bool PF>
 __global__ void __launch_bounds__(256)
 k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *__restrict__ box,
          const int32_t *__restrict__ alist, const int32_t *__restrict__ own_cnt,
@@ -268,7 +294,23 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
 #pragma unroll
     for (int k = 0; k < 7; ++k) v[k] = 0.0;
     const int nm = p.nm;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+    const int astride = gridDim.x * blockDim.x;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += astride) {
+        if (PF && a + astride < nm) {
+            const int an = a + astride;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                prefetch_l2(&alist[(size_t)u * nm + an]);
+                prefetch_l2(&alist[(size_t)(kOwnCap + u) * nm + an]);
+            }
+            prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos2[an]);
+            prefetch_l2(&mass[an]);
+            if (mode == 1) {
+                prefetch_l2(&x1[an]); prefetch_l2(&x1[nm + an]); prefetch_l2(&x1[2 * nm + an]);
+                prefetch_l2(&x2[an]); prefetch_l2(&x2[nm + an]); prefetch_l2(&x2[2 * nm + an]);
+                prefetch_l2(&del2[an]); prefetch_l2(&znum[an]);
+            }
+        }
         int no, nr;
         bool over;
         alist_counts(own_cnt, rev_cnt, a, no, nr, over);
@@ -452,20 +494,25 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t
 }
 
 // ------------------------------------------------------------ launchers --
-// Variant v selects the batch of list entries whose gathers are issued before
-// any of them is used: screen {4, 8, 16}, density {2, 4, 8}, forces {2, 4, 8}.
-
+// Variant v: bit 0 selects the batch of list entries whose gathers are issued
+// before any is used (screen {4, 8}, density and forces {2, 4}); bit 1 adds
+// L2 prefetches of the next atom's rows and per-atom data.
 void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
                    cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
     cudaMemsetAsync(d.rev_cnt, 0, sizeof(int32_t) * p.nm, s);
 #define SCREEN_ARGS p, t, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist, d.mid_cnt, d.alist, \
                     d.own_cnt, d.rev_cnt
-#define SCREEN(M, B) k_screen<M, B><<<nb, 256, 0, s>>>(SCREEN_ARGS)
+#define SCREEN(B, PF)                                                                  \
+    do {                                                                               \
+        if (mixed) k_screen<true, B, PF><<<nb, 256, 0, s>>>(SCREEN_ARGS);              \
+        else k_screen<false, B, PF><<<nb, 256, 0, s>>>(SCREEN_ARGS);                   \
+    } while (0)
     switch (variant) {
-    case 0: if (mixed) SCREEN(true, 4); else SCREEN(false, 4); break;
-    case 2: if (mixed) SCREEN(true, 16); else SCREEN(false, 16); break;
-    default: if (mixed) SCREEN(true, 8); else SCREEN(false, 8); break;
+    case 0: SCREEN(4, false); break;
+    case 1: SCREEN(8, false); break;
+    case 2: SCREEN(4, true); break;
+    default: SCREEN(8, true); break;
     }
 #undef SCREEN
 #undef SCREEN_ARGS
@@ -476,16 +523,17 @@ int launch_density_full(DeviceState &d, const Params &p, const Tables &t, bool m
     int nb = grid_blocks(p.nm, 256);
 #define DENSITY_ARGS p, t, d.pos, d.pos2, d.box, d.alist, d.own_cnt, d.rev_cnt, d.rho, d.afrho, \
                      d.dafrho, d.x1, d.mass, d.znum, partials, d.flags
-#define DENSITY(B)                                                                          \
-    do {                                                                                    \
-        if (t.exact) k_density_full<false, true, B><<<nb, 256, 0, s>>>(DENSITY_ARGS);       \
-        else if (mixed) k_density_full<true, false, B><<<nb, 256, 0, s>>>(DENSITY_ARGS);    \
-        else k_density_full<false, false, B><<<nb, 256, 0, s>>>(DENSITY_ARGS);              \
+#define DENSITY(B, PF)                                                                          \
+    do {                                                                                        \
+        if (t.exact) k_density_full<false, true, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);       \
+        else if (mixed) k_density_full<true, false, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);    \
+        else k_density_full<false, false, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);              \
     } while (0)
     switch (variant) {
-    case 0: DENSITY(2); break;
-    case 2: DENSITY(8); break;
-    default: DENSITY(4); break;
+    case 0: DENSITY(2, false); break;
+    case 1: DENSITY(4, false); break;
+    case 2: DENSITY(2, true); break;
+    default: DENSITY(4, true); break;
     }
 #undef DENSITY
 #undef DENSITY_ARGS
@@ -497,16 +545,17 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
     int nb = grid_blocks(p.nm, 256);
 #define FORCE_ARGS p, t, d.pos2, d.box, d.alist, d.own_cnt, d.rev_cnt, d.mass, d.znum, d.del2, d.f, \
                    d.x1, d.x2, d.stress, partials, mode
-#define FORCES(B)                                                                        \
-    do {                                                                                 \
-        if (t.exact) k_forces<false, true, B><<<nb, 256, 0, s>>>(FORCE_ARGS);            \
-        else if (mixed) k_forces<true, false, B><<<nb, 256, 0, s>>>(FORCE_ARGS);         \
-        else k_forces<false, false, B><<<nb, 256, 0, s>>>(FORCE_ARGS);                   \
+#define FORCES(B, PF)                                                                        \
+    do {                                                                                     \
+        if (t.exact) k_forces<false, true, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);            \
+        else if (mixed) k_forces<true, false, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);         \
+        else k_forces<false, false, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);                   \
     } while (0)
     switch (variant) {
-    case 0: FORCES(2); break;
-    case 2: FORCES(8); break;
-    default: FORCES(4); break;
+    case 0: FORCES(2, false); break;
+    case 1: FORCES(4, false); break;
+    case 2: FORCES(2, true); break;
+    default: FORCES(4, true); break;
     }
 #undef FORCES
 #undef FORCE_ARGS

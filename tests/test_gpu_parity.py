@@ -237,14 +237,14 @@ def test_kernel_variants_agree_and_autotune(oracle_mod, gpu_lib):
     g = MoldySystem.from_workload(w)
     g.force()
     f0 = g.forces()
-    for v in range(3):
+    for v in range(4):
         g.set_variants(v, v, v)
         g.force()
         assert rel_norm_err(g.forces(), f0) < 1e-13
     s0 = g.get_state()
     tune = g.autotune(nreps=2)
     assert set(tune["chosen"]) == {"screen", "density", "forces"}
-    assert all(0 <= v < 3 for v in tune["chosen"].values())
+    assert all(0 <= v < 4 for v in tune["chosen"].values())
     s1 = g.get_state()
     for k in ("x0", "x1", "x2", "b0", "b1"):
         assert np.array_equal(s0[k], s1[k]), k
