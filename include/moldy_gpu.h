@@ -180,7 +180,7 @@ int moldy_gpu_reset_kernel_stats(moldy_gpu *h);
  * family since the last reset; kernel ids are 0 .. MOLDY_KERNEL_FAMILIES-1. */
 int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64_t *launches);
 const char *moldy_gpu_kernel_name(int32_t kernel);
-#define MOLDY_KERNEL_FAMILIES 13
+#define MOLDY_KERNEL_FAMILIES 14
 
 /* kernel variants (no counterpart in the reference) -------------------------*/
 /* The screening, density and force passes are compiled in MOLDY_TUNE_VARIANTS
@@ -199,6 +199,44 @@ int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_
  * times the intermediate list (half-list pairs within the table cut + 0.9 A)
  * has been built. */
 int moldy_gpu_get_list_stats(moldy_gpu *h, double *out2);
+
+/* adjoint (no counterpart in the reference) ---------------------------------*/
+/* Gradients of a scalar loss L(E, F, sigma) with respect to the potential, for
+ * force-matching fits.  E is pe, F the real forces B0 f (what
+ * write_energy_forces_stress prints, src/dynamics_m.F90:588-619) and
+ * sigma(i,j) = -sum_k b0(j,k) tp(i,k) / vol, all as the last moldy_gpu_force
+ * (or velocityverlet / md_init / md_steps) computed them at the current state
+ * and tables; otherwise MOLDY_ERR_ORDER.  Inputs: g_energy = dL/dE, g_force =
+ * dL/dF (3*nm host doubles, x|y|z; NULL = 0), g_stress = dL/dsigma (9 host
+ * doubles, column-major; NULL = 0).  Lookup mode only (else
+ * MOLDY_ERR_UNSUPPORTED); the gradient is exact for the linearly interpolated
+ * tables and computed in FP64 whatever the handle's precision, with rho
+ * recomputed on the device.
+ * moldy_gpu_table_gradients: dL/d(table node), nlookup+1 doubles per table
+ * (any pointer may be NULL).
+ * moldy_gpu_knot_gradients: dL/d(knot parameters) of the FETRANSMETAL Fe-Fe
+ * functions set by moldy_gpu_set_fetm_fe (src/fetransmetal.F90:74-77): nv
+ * values each for av and rv, np each for ap and rp (F = -sqrt(rho) has none). */
+int moldy_gpu_table_gradients(moldy_gpu *h, double g_energy, const double *g_force,
+                              const double *g_stress, double *g_vee, double *g_dvee,
+                              double *g_phi, double *g_dphi, double *g_emb, double *g_demb);
+int moldy_gpu_knot_gradients(moldy_gpu *h, double g_energy, const double *g_force,
+                             const double *g_stress, double *g_av, double *g_rv,
+                             double *g_ap, double *g_rp);
+/* Host-only helpers (no device needed).  moldy_fetm_build_tables builds the six
+ * lookup tables (nlookup+1 each) of the Fe-Fe knots as potential_set_lookup
+ * does (src/potential_m.F90:181-228).  moldy_fetm_knot_vjp contracts table
+ * gradients g_vee..g_demb (nlookup+1 each, any may be NULL) with the
+ * derivative of those tables in the knots, as moldy_gpu_knot_gradients does. */
+int moldy_fetm_build_tables(int32_t nv, const double *av, const double *rv, int32_t np,
+                            const double *ap, const double *rp, int32_t nlookup,
+                            double *vee, double *dvee, double *phi, double *dphi,
+                            double *emb, double *demb);
+int moldy_fetm_knot_vjp(int32_t nv, const double *av, const double *rv, int32_t np,
+                        const double *ap, const double *rp, int32_t nlookup,
+                        const double *g_vee, const double *g_dvee, const double *g_phi,
+                        const double *g_dphi, const double *g_emb, const double *g_demb,
+                        double *g_av, double *g_rv, double *g_ap, double *g_rp);
 
 /* force evaluation without device allocation -----------------------------*/
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -100,6 +100,12 @@ SIGNATURES = {
     "moldy_gpu_autotune": [H, ctypes.c_int32, D, I],
     "moldy_gpu_set_variants": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "moldy_gpu_get_list_stats": [H, D],
+    "moldy_gpu_table_gradients": [H, ctypes.c_double, D, D, D, D, D, D, D, D],
+    "moldy_gpu_knot_gradients": [H, ctypes.c_double, D, D, D, D, D, D],
+    "moldy_fetm_build_tables": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,
+                                D, D, D, D, D, D],
+    "moldy_fetm_knot_vjp": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,
+                            D, D, D, D, D, D, D, D, D, D],
     "moldy_gpu_force_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, D, ctypes.c_void_p, ctypes.c_void_p,
@@ -107,7 +113,7 @@ SIGNATURES = {
                                 ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 11,
 }
 NOALLOC_MAX_ATOMS = 262144
-KERNEL_FAMILIES = 13
+KERNEL_FAMILIES = 14
 TUNE_VARIANTS = 4
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}

@@ -81,7 +81,7 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
     "drift", "linkup", "relink", "build_nlist", "density", "screen", "forces",
-    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2"};
+    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint"};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {
@@ -154,6 +154,8 @@ Engine::Engine(const moldy_params &p) {
     prm.nlcy = p.nlcy;
     prm.nlcz = p.nlcz;
     prm.ncell = 0;
+    prm.own_cap = kOwnCap;
+    prm.rev_cap = kRevCap;
     ntcm_ = p.ntcm;
     ntc_ = p.ntc;
     precision_ = p.precision;
@@ -168,7 +170,7 @@ Engine::~Engine() {
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
                     d.own_cnt, d.rev_cnt, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
-                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp};
+                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_box_) cudaFreeHost(host_box_);
@@ -228,7 +230,7 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.numn, nm, "numn"));
     CHECK(dev_alloc(&d.posf, nm, "posf"));
     CHECK(dev_alloc(&d.pos2, nm, "pos2"));
-    CHECK(dev_alloc(&d.alist, nm * (size_t)(kOwnCap + kRevCap), "active list"));
+    CHECK(dev_alloc(&d.alist, nm * (size_t)(p.own_cap + p.rev_cap), "active list"));
     CHECK(dev_alloc(&d.own_cnt, nm, "own_cnt"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)kMidCap, "intermediate list"));
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
@@ -337,6 +339,7 @@ int Engine::upload_tables() {
     t.phi_cut1 = h.phi_cut1; t.phi_cut2 = h.phi_cut2;
     t.bier_a = h.bier_a; t.bier_zed = h.bier_zed;
     potential_set_ = true;
+    forces_current_ = false;
     return MOLDY_OK;
 }
 
@@ -412,7 +415,10 @@ int Engine::set_state(const double *x0, const double *y0, const double *z0, cons
         prm.nlcx = n3[0]; prm.nlcy = n3[1]; prm.nlcz = n3[2];
         CHECK(alloc_cells(*this));
     }
+    if (b0) host_vol_ = std::fabs(b0[0] * (b0[4] * b0[8] - b0[7] * b0[5]) + b0[1] * (b0[5] * b0[6] - b0[3] * b0[8]) +
+                                  b0[2] * (b0[3] * b0[7] - b0[4] * b0[6]));
     if (x0 && zn && mass && del2 && b0) state_set_ = true;
+    if (x0 || y0 || z0 || b0 || mass) forces_current_ = false;
     CUDA_CHECK(cudaStreamSynchronize(s), "set_state");
     return MOLDY_OK;
 }
@@ -517,9 +523,11 @@ int Engine::check_flags() {
     }
     if (f[3]) {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
+        active_overflow_ = f[4];
         return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[4]) +
                                             " interacting neighbours on one side, more than the compact list holds (" +
-                                            std::to_string(kOwnCap) + " own / " + std::to_string(kRevCap) + " reverse)");
+                                            std::to_string(prm.own_cap) + " own / " + std::to_string(prm.rev_cap) +
+                                            " reverse)");
     }
     if (st) {
         cudaMemsetAsync(&d.box->status, 0, sizeof(int32_t), stream_);
@@ -560,6 +568,7 @@ int Engine::get_neighbourlist(int32_t *nlist, int32_t *numn) {
 static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_ready, bool &list_ready,
                        bool *rebuilt, cudaStream_t s) {
     DeviceState &d = E.d;
+    CHECK(E.ensure_active_capacity(0));
     const Params &p = E.prm;
     ntc = ntc + 1;
     const bool rb = (ntc == 1 || !list_ready);
@@ -601,6 +610,7 @@ int Engine::fetch_force_out(moldy_force_out *out) {
     CUDA_CHECK(cudaGetLastError(), "force");
     if (out) {
         const BoxState &B = host_box_[0];
+        host_vol_ = B.vol;
         out->pe = B.pe;
         out->vol = B.vol;
         std::memcpy(out->tp, B.tp, sizeof(out->tp));
@@ -617,10 +627,42 @@ int Engine::fetch_force_out(moldy_force_out *out) {
 
 int Engine::force(moldy_force_out *out) {
     CHECK(check_ready());
-    bool rb = false;
-    CHECK(force_device(&rb));
-    CHECK(fetch_force_out(out));
-    if (out) out->rebuilt = rb ? 1 : 0;
+    const int ntc0 = ntc_;
+    for (int attempt = 0;; ++attempt) {
+        bool rb = false;
+        active_overflow_ = 0;
+        CHECK(force_device(&rb));
+        int rc = fetch_force_out(out);
+        if (rc == MOLDY_ERR_CAPACITY && active_overflow_ > 0 && attempt < 2) {
+            // a force evaluation changes nothing but the rebuild counter and
+            // the lists: grow the compact list and evaluate again
+            CHECK(ensure_active_capacity(active_overflow_ + 8));
+            ntc_ = ntc0;
+            continue;
+        }
+        CHECK(rc);
+        if (out) out->rebuilt = rb ? 1 : 0;
+        forces_current_ = true;
+        return MOLDY_OK;
+    }
+}
+
+int Engine::ensure_active_capacity(int min_cap) {
+    int need = std::max(kOwnCap, min_cap);
+    if (host_vol_ > 0.0 && rcut > 0.0 && rcut < prm.rnear * 2.0) {
+        // pairs inside the cut, (4 pi / 3) rc^3 n/V, with margin: how they split
+        // between an atom's own row and its reverse entries depends on its
+        // place in the cell traversal, so either side may take nearly all
+        double full = (4.0 * M_PI / 3.0) * rcut * rcut * rcut * (double)prm.nm / host_vol_;
+        need = std::max(need, (int)std::ceil(1.25 * full + 8.0));
+    }
+    need = std::min(need, std::max(2 * prm.nnbrs, kOwnCap));
+    if (need <= prm.own_cap && need <= prm.rev_cap) return MOLDY_OK;
+    if (d.alist) cudaFree(d.alist);
+    d.alist = nullptr;
+    CHECK(dev_alloc(&d.alist, (size_t)prm.nm * 2 * (size_t)need, "active list"));
+    prm.own_cap = need;
+    prm.rev_cap = need;
     return MOLDY_OK;
 }
 
@@ -631,6 +673,7 @@ int Engine::velocityverlet(moldy_force_out *out) {
     CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
     CHECK(fetch_force_out(out));
     if (out) out->rebuilt = rb ? 1 : 0;
+    forces_current_ = true;
     return MOLDY_OK;
 }
 
@@ -656,6 +699,7 @@ int Engine::md_init(moldy_force_out *out) {
     LAUNCH(*this, K_MDINIT, 1, stream_, launch_md_init_x2(d, prm, stream_));
     CHECK(fetch_force_out(out));
     if (out) out->rebuilt = rb ? 1 : 0;
+    forces_current_ = true;
     return MOLDY_OK;
 }
 
@@ -694,6 +738,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
             t.ntc = ntcs[k]; t.rebuilt = rbs[k];
         }
     }
+    forces_current_ = true;
     return MOLDY_OK;
 }
 
@@ -758,6 +803,69 @@ int Engine::autotune(int nreps, double *times_ms) {
     prof.on = was_on;
     CUDA_CHECK(cudaGetLastError(), "autotune");
     return check_flags();
+}
+
+// dL/d(table) for L with dL/dE = gE, dL/dF = gF (real forces, 3*nm host,
+// x|y|z) and dL/dsigma = gS (column-major 3x3 host, may be NULL), at the
+// state and neighbour list of the last force evaluation.
+int Engine::table_gradients(double gE, const double *gF, const double *gS, double *const g[6]) {
+    CHECK(check_ready());
+    if (!forces_current_ || !list_ready_)
+        return fail(MOLDY_ERR_ORDER, "table gradients need a force evaluation at the current state and tables");
+    if (ht.exact) return fail(MOLDY_ERR_UNSUPPORTED, "table gradients need lookup mode (uselookup = 1)");
+    const int n = ht.nlookup, nb = n + 1;
+    const size_t smem = adjoint_smem_bytes(n);
+    if (smem > 200 * 1024) return fail(MOLDY_ERR_CAPACITY, "nlookup above 12799 does not fit the shared-memory histograms");
+    const size_t nm = (size_t)prm.nm, need = 12 * (size_t)nb + 7 * nm;
+    if (d.adj_cap < need) {
+        if (d.adj) cudaFree(d.adj);
+        d.adj = nullptr;
+        d.adj_cap = 0;
+        CHECK(dev_alloc(&d.adj, need, "adjoint scratch"));
+        d.adj_cap = need;
+    }
+    double *tabs = d.adj, *grads = tabs + 6 * (size_t)nb, *scr = grads + 6 * (size_t)nb, *dgF = scr + 4 * nm;
+    const std::vector<double> *src[6] = {&ht.vee, &ht.dvee, &ht.phi, &ht.dphi, &ht.emb, &ht.demb};
+    for (int k = 0; k < 6; ++k)
+        CUDA_CHECK(cudaMemcpyAsync(tabs + k * nb, src[k]->data(), nb * sizeof(double), cudaMemcpyHostToDevice,
+                                   stream_), "adjoint tables");
+    if (gF) CUDA_CHECK(cudaMemcpyAsync(dgF, gF, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, stream_), "dL/dF");
+    else CUDA_CHECK(cudaMemsetAsync(dgF, 0, 3 * nm * sizeof(double), stream_), "dL/dF");
+    AdjointArgs a;
+    a.nm = prm.nm; a.ivol = prm.ivol; a.n = n;
+    a.vee = tabs; a.dvee = tabs + nb; a.phi = tabs + 2 * nb; a.dphi = tabs + 3 * nb;
+    a.emb = tabs + 4 * nb; a.demb = tabs + 5 * nb;
+    a.rmin = tab.vp_rmin; a.rmax = tab.vp_rmax;
+    a.r_reciprange = tab.vp_reciprange; a.r_recipstep = tab.vp_recipstep;
+    a.emin = tab.e_rmin; a.emax = tab.e_rmax;
+    a.e_reciprange = tab.e_reciprange; a.e_recipstep = tab.e_recipstep;
+    a.recipn = tab.vp_recipnlkp;
+    for (int k = 0; k < 9; ++k) a.gs[k] = gS ? gS[k] : 0.0;
+    a.gE = gE;
+    LAUNCH(*this, K_ADJOINT, 5, stream_, launch_table_adjoint(d, a, grads, scr, dgF, stream_));
+    for (int k = 0; k < 6; ++k)
+        if (g[k]) CUDA_CHECK(cudaMemcpyAsync(g[k], grads + k * nb, nb * sizeof(double), cudaMemcpyDeviceToHost,
+                                             stream_), "table gradients");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "table gradients");
+    CUDA_CHECK(cudaGetLastError(), "table gradients");
+    prof.harvest();
+    return MOLDY_OK;
+}
+
+// dL/d(knots) of the FETRANSMETAL Fe-Fe functions: the table gradients
+// contracted with the derivative of the tables in the knot parameters.
+int Engine::knot_gradients(double gE, const double *gF, const double *gS, double *g_av, double *g_rv,
+                           double *g_ap, double *g_rp) {
+    if (!ht.fetm) return fail(MOLDY_ERR_UNSUPPORTED, "knot gradients need the FETRANSMETAL set-up");
+    const size_t nb = (size_t)ht.nlookup + 1;
+    std::vector<double> buf(6 * nb);
+    double *g[6];
+    for (int k = 0; k < 6; ++k) g[k] = buf.data() + k * nb;
+    CHECK(table_gradients(gE, gF, gS, g));
+    const double *cg[6] = {g[0], g[1], g[2], g[3], g[4], g[5]};
+    int rc = fetm_knot_vjp(ht, cg, g_av, g_rv, g_ap, g_rp);
+    if (rc != MOLDY_OK) return fail(rc, "knot gradient contraction failed");
+    return MOLDY_OK;
 }
 
 int Engine::synchronize() {
@@ -1020,6 +1128,56 @@ int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_
     h->e->variant[moldy::K_DENSITY] = density;
     h->e->variant[moldy::K_PAIR] = forces;
     return MOLDY_OK;
+}
+
+int moldy_gpu_table_gradients(moldy_gpu *h, double g_energy, const double *g_force, const double *g_stress,
+                              double *g_vee, double *g_dvee, double *g_phi, double *g_dphi, double *g_emb,
+                              double *g_demb) {
+    GUARD(h);
+    double *const g[6] = {g_vee, g_dvee, g_phi, g_dphi, g_emb, g_demb};
+    TRY(h->e->table_gradients(g_energy, g_force, g_stress, g));
+}
+
+int moldy_gpu_knot_gradients(moldy_gpu *h, double g_energy, const double *g_force, const double *g_stress,
+                             double *g_av, double *g_rv, double *g_ap, double *g_rp) {
+    GUARD(h);
+    TRY(h->e->knot_gradients(g_energy, g_force, g_stress, g_av, g_rv, g_ap, g_rp));
+}
+
+int moldy_fetm_build_tables(int32_t nv, const double *av, const double *rv, int32_t np, const double *ap,
+                            const double *rp, int32_t nlookup, double *vee, double *dvee, double *phi,
+                            double *dphi, double *emb, double *demb) {
+    try {
+        if (!av || !rv || !ap || !rp || nlookup < 2) return fail(MOLDY_ERR_INVALID, "null knots or nlookup < 2");
+        moldy::HostTables ht;
+        int rc = moldy::build_fetm_tables(ht, nv, av, rv, np, ap, rp, 1, nlookup);
+        if (rc != MOLDY_OK) return fail(rc, "FETRANSMETAL set-up failed");
+        double *out[6] = {vee, dvee, phi, dphi, emb, demb};
+        const std::vector<double> *src[6] = {&ht.vee, &ht.dvee, &ht.phi, &ht.dphi, &ht.emb, &ht.demb};
+        for (int k = 0; k < 6; ++k)
+            if (out[k]) std::memcpy(out[k], src[k]->data(), src[k]->size() * sizeof(double));
+        return MOLDY_OK;
+    } catch (...) {
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
+}
+
+int moldy_fetm_knot_vjp(int32_t nv, const double *av, const double *rv, int32_t np, const double *ap,
+                        const double *rp, int32_t nlookup, const double *g_vee, const double *g_dvee,
+                        const double *g_phi, const double *g_dphi, const double *g_emb, const double *g_demb,
+                        double *g_av, double *g_rv, double *g_ap, double *g_rp) {
+    try {
+        if (!av || !rv || !ap || !rp || nlookup < 2) return fail(MOLDY_ERR_INVALID, "null knots or nlookup < 2");
+        moldy::HostTables ht;
+        int rc = moldy::build_fetm_tables(ht, nv, av, rv, np, ap, rp, 1, nlookup);
+        if (rc != MOLDY_OK) return fail(rc, "FETRANSMETAL set-up failed");
+        const double *g[6] = {g_vee, g_dvee, g_phi, g_dphi, g_emb, g_demb};
+        rc = moldy::fetm_knot_vjp(ht, g, g_av, g_rv, g_ap, g_rp);
+        if (rc != MOLDY_OK) return fail(rc, "knot gradient contraction failed");
+        return MOLDY_OK;
+    } catch (...) {
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
 }
 
 const char *moldy_gpu_kernel_name(int32_t kernel) {

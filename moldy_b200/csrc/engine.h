@@ -41,7 +41,7 @@ struct DeviceState {
     // positions with F'(rho) in w, written by the density pass for the force pass
     double4 *pos2 = nullptr;
     // compact full list of interacting pairs, entry-major: own entries
-    // (e * nm + i, e < kOwnCap), then reverse entries ((kOwnCap + e) * nm + i)
+    // (e * nm + i, e < own_cap), then reverse entries ((own_cap + e) * nm + i)
     int32_t *alist = nullptr, *own_cnt = nullptr, *rev_cnt = nullptr;
     // intermediate half list (pairs within r_mid when built), entry-major like
     // nlist; mid_cnt < 0 marks an atom whose row overflowed (screen then reads
@@ -59,6 +59,20 @@ struct DeviceState {
                                   // [2] overflow atom, [3] active-list overflow, [4] its count
     BoxState *box = nullptr;
     int32_t *scan_tmp = nullptr;
+    // adjoint (allocated on first use): full tables and their gradients
+    // (6 * (nlookup+1) each), then rho, F', mu, nu and dL/dF (7 * nm)
+    double *adj = nullptr;
+    size_t adj_cap = 0;
+};
+
+// Arguments of the table adjoint: the full tables (device) and dL/dE, dL/dsigma.
+struct AdjointArgs {
+    int nm, ivol, n;
+    const double *vee, *dvee, *phi, *dphi, *emb, *demb;
+    double rmin, rmax, r_reciprange, r_recipstep;
+    double emin, emax, e_reciprange, e_recipstep;
+    double recipn;
+    double gs[9], gE;
 };
 
 // Host-side table data (potential_m / lookup_m).
@@ -78,7 +92,7 @@ struct HostTables {
 // Kernel families timed by the optional per-kernel CUDA-event profiler.
 enum KernelId {
     K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_SCREEN, K_PAIR, K_FINALIZE,
-    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_COUNT
+    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_ADJOINT, K_COUNT
 };
 extern const char *const kKernelNames[K_COUNT];
 
@@ -133,14 +147,20 @@ class Engine {
     int md_steps(int nsteps, moldy_thermo *thermo);
     int energy_calc(double *en_atom);
     int synchronize();
+    int table_gradients(double gE, const double *gF, const double *gS, double *const g[6]);
+    int knot_gradients(double gE, const double *gF, const double *gS, double *g_av, double *g_rv,
+                       double *g_ap, double *g_rp);
     void set_ntc(int ntc) { ntc_ = ntc; }
     cudaStream_t &stream_ref() { return stream_; }
     Profiler prof;
     int device() const { return device_; }
     int precision() const { return precision_; }
     // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
-    int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
     int autotune(int nsteps, double *times_ms);
+    // grows the compact list so that it holds the pairs a table cut of rcut
+    // gives at the current atom density (and at least min_cap per side)
+    int ensure_active_capacity(int min_cap);
     double rmid = 0.0, rcut = 0.0;   // intermediate-list radius and table cut (A)
 
     DeviceState d;
@@ -161,6 +181,9 @@ class Engine {
     int precision_ = MOLDY_PREC_FP64;
     bool state_set_ = false, cells_ready_ = false, list_ready_ = false;
     bool potential_set_ = false;
+    bool forces_current_ = false;   // force outputs match the state and tables
+    double host_vol_ = 0.0;         // last box volume seen on the host
+    int active_overflow_ = 0;       // largest compact-list row of an overflowing evaluation
     double *part_embed_ = nullptr, *part_force_ = nullptr;   // slices of d.partials
     BoxState *host_box_ = nullptr;                            // pinned staging
     int host_box_cap_ = 0;
@@ -169,8 +192,8 @@ class Engine {
 constexpr int kAtomThreads = 256;
 constexpr int kPairTPA = 8;            // threads per atom in the pair passes
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
-constexpr int kOwnCap = 24;            // own interacting pairs per atom in the compact list
-constexpr int kRevCap = 24;            // reverse interacting pairs per atom
+constexpr int kOwnCap = 24;            // least own interacting pairs per atom in the compact list
+constexpr int kRevCap = 24;            // least reverse interacting pairs per atom
 constexpr int kMidCap = 40;            // half-list pairs per atom in the intermediate list
 constexpr double kMidSkin = 0.9;       // r_mid = table cut + kMidSkin (A), at most rnear
 constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
@@ -207,5 +230,10 @@ void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
+size_t adjoint_smem_bytes(int nlookup);
+void launch_table_adjoint(const DeviceState &d, const AdjointArgs &a, double *grads, double *scr,
+                          const double *gF, cudaStream_t s);
+int fetm_knot_vjp(const HostTables &ht, const double *const g[6], double *g_av, double *g_rv,
+                  double *g_ap, double *g_rp);
 
 }  // namespace moldy

@@ -150,10 +150,10 @@ k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__re
                     keep = (sx * sx + sy * sy + sz * sz) <= t.rcull2;
                 }
                 if (keep) {
-                    if (cnt < kOwnCap) alist[(size_t)cnt * stride + a] = j;
+                    if (cnt < p.own_cap) alist[(size_t)cnt * stride + a] = j;
                     ++cnt;
                     int rs = atomicAdd(&rev_cnt[j], 1);
-                    if (rs < kRevCap) alist[((size_t)kOwnCap + rs) * stride + j] = a;
+                    if (rs < p.rev_cap) alist[((size_t)p.own_cap + rs) * stride + j] = a;
                 }
             }
         }
@@ -162,18 +162,18 @@ k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__re
 }
 
 // the compact list of atom a: own entries 0..no-1 then reverse entries
-// 0..nr-1, stored entry-major at (e * nm + a) and ((kOwnCap + e) * nm + a)
-__device__ __forceinline__ void alist_counts(const int32_t *own_cnt, const int32_t *rev_cnt, int a,
-                                             int &no, int &nr, bool &over) {
+// 0..nr-1, stored entry-major at (e * nm + a) and ((own_cap + e) * nm + a)
+__device__ __forceinline__ void alist_counts(const Params &p, const int32_t *own_cnt, const int32_t *rev_cnt,
+                                             int a, int &no, int &nr, bool &over) {
     no = own_cnt[a];
     nr = rev_cnt[a];
-    over = no > kOwnCap || nr > kRevCap;
-    no = no < kOwnCap ? no : kOwnCap;
-    nr = nr < kRevCap ? nr : kRevCap;
+    over = no > p.own_cap || nr > p.rev_cap;
+    no = no < p.own_cap ? no : p.own_cap;
+    nr = nr < p.rev_cap ? nr : p.rev_cap;
 }
 
-__device__ __forceinline__ size_t alist_index(int e, int no, int a, int nm) {
-    return (size_t)(e < no ? e : kOwnCap + (e - no)) * (size_t)nm + a;
+__device__ __forceinline__ size_t alist_index(const Params &p, int e, int no, int a, int nm) {
+    return (size_t)(e < no ? e : p.own_cap + (e - no)) * (size_t)nm + a;
 }
 
 // -------------------------------------------------------------- density --
@@ -205,7 +205,7 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 prefetch_l2(&alist[(size_t)u * nm + an]);
-                prefetch_l2(&alist[(size_t)(kOwnCap + u) * nm + an]);
+                prefetch_l2(&alist[(size_t)(p.own_cap + u) * nm + an]);
             }
             prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos[an]);
             prefetch_l2(&dafrho[an]); prefetch_l2(&mass[an]); prefetch_l2(&znum[an]);
@@ -213,7 +213,7 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
         }
         int no, nr;
         bool over;
-        alist_counts(own_cnt, rev_cnt, a, no, nr, over);
+        alist_counts(p, own_cnt, rev_cnt, a, no, nr, over);
         v[7] += (double)(no + nr);
         if (over) {
             atomicExch(&flags[3], 1);
@@ -225,7 +225,7 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
         for (int e0 = 0; e0 < ne; e0 += B) {
             int jj[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(e0 + u, no, a, nm)] : -1;
+            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(p, e0 + u, no, a, nm)] : -1;
             double4 qq[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) qq[u] = pos[jj[u] >= 0 ? jj[u] : a];
@@ -301,7 +301,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 prefetch_l2(&alist[(size_t)u * nm + an]);
-                prefetch_l2(&alist[(size_t)(kOwnCap + u) * nm + an]);
+                prefetch_l2(&alist[(size_t)(p.own_cap + u) * nm + an]);
             }
             prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos2[an]);
             prefetch_l2(&mass[an]);
@@ -313,7 +313,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
         }
         int no, nr;
         bool over;
-        alist_counts(own_cnt, rev_cnt, a, no, nr, over);
+        alist_counts(p, own_cnt, rev_cnt, a, no, nr, over);
         const double4 pa = pos2[a];
         const double ma = mass[a];
         double fxa = 0.0, fya = 0.0, fza = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
@@ -321,7 +321,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
         for (int e0 = 0; e0 < ne; e0 += B) {
             int jj[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(e0 + u, no, a, nm)] : -1;
+            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(p, e0 + u, no, a, nm)] : -1;
             double4 qq[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) qq[u] = pos2[jj[u] >= 0 ? jj[u] : a];

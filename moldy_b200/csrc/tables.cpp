@@ -185,4 +185,90 @@ int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv
     return MOLDY_OK;
 }
 
+// Contracts table gradients g[6] (vee, dvee, phi, dphi, emb, demb; nlookup+1
+// each) with d(table)/d(knot) of the functions above: dL/da_k, dL/dr_k of the
+// pair sum, dL/dA_k, dL/dR_k of the density sum.  Below bier_cut1 the pair
+// function is Biersack alone and has no knot dependence; between the cuts it
+// depends on the knots through the join's end values V(c), V'(c) at
+// c = bier_cut2 + 1e-12; phi below its maximum r_top is the value at r_top,
+// whose knot derivative is the partial one (phi' vanishes at r_top).  The emb
+// tables of F = -sqrt(rho) carry no knot parameters.
+int fetm_knot_vjp(const HostTables &ht, const double *const g[6], double *g_av, double *g_rv,
+                  double *g_ap, double *g_rp) {
+    if (!ht.fetm || ht.nlookup < 2) return MOLDY_ERR_UNSUPPORTED;
+    const int nv = ht.nv, np = ht.np, n = ht.nlookup;
+    const double *av = ht.av, *rv = ht.rv, *ap = ht.ap, *rp = ht.rp;
+    double gav[8] = {0}, grv[8] = {0}, gap[8] = {0}, grp[8] = {0};
+    const double cut1 = ht.bier_cut1, cut2 = ht.bier_cut2, top = ht.phi_cut1;
+    const double c = cut2 + (double)0.000000000001f;
+    const double j0 = ht.sc[0], j1 = ht.sc[1], j2 = ht.sc[2], j3 = ht.sc[3];
+    const double h = cut2 - cut1, l1 = std::log(j0), s1 = j1 / j0, l2 = std::log(j2), s2 = j3 / j2;
+    double gj2 = 0.0, gj3 = 0.0;   // dL/dV(c), dL/dV'(c)
+    // phi below r_top: partial derivatives at r_top
+    double dtop_a[8], dtop_r[8];
+    for (int k = 0; k < np; ++k) {
+        double d = rp[k] - top, H = d < 0.0 ? 0.0 : 1.0;
+        dtop_a[k] = d * d * d * H;
+        dtop_r[k] = 3.0 * ap[k] * d * d * H;
+    }
+    const double range = ht.rmax - ht.rmin, recipn = 1.0 / (double)n;
+    for (int i = 0; i <= n; ++i) {
+        const double r = ht.rmin + (double)i * range * recipn;
+        const double gv = g[0] ? g[0][i] : 0.0, gd = g[1] ? g[1][i] : 0.0;
+        const double gp = g[2] ? g[2][i] : 0.0, gdp = g[3] ? g[3][i] : 0.0;
+        if (gv != 0.0 || gd != 0.0) {
+            if (r > cut2) {
+                for (int k = 0; k < nv; ++k) {
+                    double d = rv[k] - r;
+                    if (d < 0.0) continue;
+                    gav[k] += gv * d * d * d - gd * 3.0 * d * d;
+                    grv[k] += gv * 3.0 * av[k] * d * d - gd * 6.0 * av[k] * d;
+                }
+            } else if (r > cut1) {
+                double t = (r - cut1) / h;
+                double h00 = 2 * t * t * t - 3 * t * t + 1, h10 = t * t * t - 2 * t * t + t;
+                double h01 = -2 * t * t * t + 3 * t * t, h11 = t * t * t - t * t;
+                double d00 = 6 * t * t - 6 * t, d10 = 3 * t * t - 4 * t + 1;
+                double d01 = -6 * t * t + 6 * t, d11 = 3 * t * t - 2 * t;
+                double e = h00 * l1 + h10 * s1 * h + h01 * l2 + h11 * s2 * h;
+                double dl = (d00 * l1 + d10 * s1 * h + d01 * l2 + d11 * s2 * h) / h;
+                double V = std::exp(e);
+                double de2 = h01 / j2 - h11 * h * j3 / (j2 * j2), de3 = h11 * h / j2;
+                double dd2 = (d01 / j2 - d11 * h * j3 / (j2 * j2)) / h, dd3 = d11 / j2;
+                // V = exp(e), D = dl V
+                gj2 += gv * V * de2 + gd * (dd2 * V + dl * V * de2);
+                gj3 += gv * V * de3 + gd * (dd3 * V + dl * V * de3);
+            }
+        }
+        if (gp != 0.0 || gdp != 0.0) {
+            if (r < top) {
+                for (int k = 0; k < np; ++k) { gap[k] += gp * dtop_a[k]; grp[k] += gp * dtop_r[k]; }
+            } else {
+                for (int k = 0; k < np; ++k) {
+                    double d = rp[k] - r;
+                    if (d < 0.0) continue;
+                    gap[k] += gp * d * d * d - gdp * 3.0 * d * d;
+                    grp[k] += gp * 3.0 * ap[k] * d * d - gdp * 6.0 * ap[k] * d;
+                }
+            }
+        }
+    }
+    // V(c) = sum a_k (r_k - c)^3, V'(c) = -3 sum a_k (r_k - c)^2 (terms with r_k >= c)
+    for (int k = 0; k < nv; ++k) {
+        double d = rv[k] - c;
+        if (d < 0.0) continue;
+        gav[k] += gj2 * d * d * d - gj3 * 3.0 * d * d;
+        grv[k] += gj2 * 3.0 * av[k] * d * d - gj3 * 6.0 * av[k] * d;
+    }
+    for (int k = 0; k < nv; ++k) {
+        if (g_av) g_av[k] = gav[k];
+        if (g_rv) g_rv[k] = grv[k];
+    }
+    for (int k = 0; k < np; ++k) {
+        if (g_ap) g_ap[k] = gap[k];
+        if (g_rp) g_rp[k] = grp[k];
+    }
+    return MOLDY_OK;
+}
+
 }  // namespace moldy

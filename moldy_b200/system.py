@@ -108,6 +108,7 @@ class MoldySystem:
         check(self._L.moldy_gpu_set_fetm_fe(self._h, len(av), _dp(av), _dp(rv), len(ap), _dp(ap),
                                             _dp(rp), int(bool(uselookup)), int(nlookup)))
         self.nlookup = int(nlookup)
+        self.n_knots = (len(av), len(ap))
 
     def set_tables(self, tables: dict, *, rmin=0.0, rmax=6.0, rhomin=0.0, rhomax=10000.0):
         t = {k: _f64(tables[k]) for k in ("vee", "dvee", "phi", "dphi", "emb", "demb")}
@@ -224,6 +225,43 @@ class MoldySystem:
         o = _lib.ForceOut()
         check(self._L.moldy_gpu_force(self._h, ctypes.byref(o)))
         return self._force_dict(o)
+
+    def energy_forces_stress(self, out: dict | None = None):
+        """(pe, real forces [nm,3], sigma [3,3]) as write_energy_forces_stress
+        prints them (src/dynamics_m.F90:588-619) after a force evaluation:
+        F = B0 f and sigma(i,j) = -sum_k b0(j,k) tp(i,k) / vol."""
+        if out is None:
+            out = self.force()
+        b0 = self.get_state()["b0"]
+        f = self.forces() @ b0.T
+        sigma = -(out["tp"] @ b0.T) / out["vol"]
+        return out["pe"], f, sigma
+
+    # --------------------------------------------------------------- adjoint
+    @staticmethod
+    def _grad_inputs(nm, g_force, g_stress):
+        gf = None if g_force is None else _f64(np.asarray(g_force, dtype=np.float64).reshape(nm, 3).T)
+        gs = _mat_f(g_stress)
+        return gf, gs
+
+    def table_gradients(self, g_energy=0.0, g_force=None, g_stress=None) -> dict:
+        """dL/d(table node) for dL/dE = g_energy, dL/dF = g_force [nm,3] (real
+        forces) and dL/dsigma = g_stress [3,3], at the last force evaluation."""
+        gf, gs = self._grad_inputs(self.nm, g_force, g_stress)
+        n = self.nlookup + 1
+        t = [np.zeros(n) for _ in range(6)]
+        check(self._L.moldy_gpu_table_gradients(self._h, float(g_energy), _dp(gf), _dp(gs),
+                                                *[_dp(a) for a in t]))
+        return dict(zip(["vee", "dvee", "phi", "dphi", "emb", "demb"], t))
+
+    def knot_gradients(self, g_energy=0.0, g_force=None, g_stress=None) -> dict:
+        """dL/d(av, rv, ap, rp) of the Fe-Fe knots set by set_up_fetm."""
+        gf, gs = self._grad_inputs(self.nm, g_force, g_stress)
+        nv, npk = self.n_knots
+        out = [np.zeros(nv), np.zeros(nv), np.zeros(npk), np.zeros(npk)]
+        check(self._L.moldy_gpu_knot_gradients(self._h, float(g_energy), _dp(gf), _dp(gs),
+                                               *[_dp(a) for a in out]))
+        return dict(zip(["av", "rv", "ap", "rp"], out))
 
     def velocityverlet(self) -> dict:
         o = _lib.ForceOut()

@@ -148,3 +148,26 @@ def config_liquid(n: int = 80, seed: int = 5, temperature: float = 300.0) -> Wor
 def random_symmetric_strain(rng: np.random.Generator, amplitude: float) -> np.ndarray:
     e = rng.uniform(-amplitude, amplitude, size=6)
     return np.array([[e[0], e[3], e[4]], [e[3], e[1], e[5]], [e[4], e[5], e[2]]])
+
+
+K_EFF_FE = 5.0          # effective spring constant for thermal displacements (eV/A^2)
+
+
+def config_adjoint(nconf: int = 256, n: int = 8, seed: int = 4,
+                   t_range: tuple = (300.0, 1800.0), strain_amplitude: float = 0.03) -> list:
+    """Force-matching set: nconf seeded bcc Fe configurations of 2 n^3 atoms
+    (default 256 x 1024).  Each has a temperature uniform in t_range, Gaussian
+    displacements with sigma = sqrt(k T / k_eff), k_eff = 5 eV/A^2, and a
+    symmetric strain with components uniform in +/- strain_amplitude."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(nconf):
+        t = float(rng.uniform(*t_range))
+        sigma = math.sqrt(units.BK * t / K_EFF_FE)
+        strain = random_symmetric_strain(rng, strain_amplitude)
+        w = make_workload(n, sigma=sigma, temperature=0.0, ivol=1, nbrupdate=100,
+                          seed=int(rng.integers(1 << 30)), strain=strain,
+                          name=f"bcc_fe_{2 * n ** 3}_fm{c:03d}")
+        w.meta.update(config_temperature=t, strain=strain)
+        out.append(w)
+    return out
