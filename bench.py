@@ -155,12 +155,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def kernel_bytes_per_atom(name, n_half, n_full):
-    """Algorithmic DRAM bytes per atom of one launch (DESIGN.md, section 5).
-    n_half: mean half-list length; n_full: mean interacting (directed) pairs."""
+def kernel_bytes_per_atom(name, n_half, n_full, n_screen):
+    """Algorithmic DRAM bytes per atom of one launch.
+    n_half: mean half-list length; n_full: mean interacting (directed) pairs;
+    n_screen: mean list entries the screening pass reads (intermediate rows)."""
     table = {
-        # half-list row + count + own FP32 position + compact-list entries and counts
-        "screen": 4.0 * n_half + 4 + 16 + 4.0 * n_full + 8,
+        # screened row + count + own FP32 position + compact-list entries and counts
+        "screen": 4.0 * n_screen + 4 + 16 + 4.0 * n_full + 8,
         # compact row + counts + own position, writes of (x,F') rho F F', old F', x1, mass, Z
         "density": 4.0 * n_full + 8 + 32 + 32 + 24 + 8 + 24 + 8 + 4,
         # compact row + counts + own (x,F') + mass, forces, x1 and x2 read+write, del2, Z
@@ -303,21 +304,22 @@ def run_ours(args):
     _, numn = sysm.neighbour_list() if w.nm <= 4_000_000 else (None, None)
     n_half = float(np.mean(numn)) if numn is not None else 44.0
 
-    n_full = sysm.pair_count() / w.nm
+    lst = sysm.list_stats()
+    n_full = lst["pairs"] / w.nm
+    n_screen = lst["screened"] / w.nm
     # dominant kernel and its roofline
     dom = max(stats.items(), key=lambda kv: kv[1][0])
     dname, (dms, dlaunch) = dom
     peak, peak_kind = load_peaks()
-    bpa = kernel_bytes_per_atom(dname, n_half, n_full)
+    bpa = kernel_bytes_per_atom(dname, n_half, n_full, n_screen)
     roofline = None
     if bpa is not None and dlaunch > 0:
         per_launch_s = dms / 1000.0 / dlaunch
         achieved = bpa * w.nm / per_launch_s / 1e9
         traffic = None
-        tr = load_traffic()
-        if tr and dname in tr.get("kernels", {}):
-            k = tr["kernels"][dname]
-            traffic = float(k["dram_bytes_per_atom"]) * w.nm
+        tr = (load_traffic() or {}).get(args.precision, {})
+        if dname in tr.get("kernels", {}):
+            traffic = float(tr["kernels"][dname]["dram_bytes_per_atom"]) * w.nm
         roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "algorithmic_bytes_per_launch": bpa * w.nm,
@@ -364,6 +366,7 @@ def run_ours(args):
         "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded bcc Fe lattice, Gaussian displacements, Maxwell-Boltzmann velocities)",
         "config": config_dict(w, args.precision, {"neighbours_half_mean": n_half,
+                                                  "screened_entries_per_atom": n_screen,
                                                   "interacting_pairs_per_atom": n_full,
                                                   "autotuned_variants": tune["chosen"]}),
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,

@@ -194,11 +194,12 @@ const char *moldy_gpu_kernel_name(int32_t kernel);
 #define MOLDY_TUNE_VARIANTS 4
 int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
 int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
-/* out2[0]: directed interacting pairs (inside the table range) of the last
- * force evaluation, twice the contributing half-list pairs; out2[1]: how many
+/* out3[0]: directed interacting pairs (inside the table range) of the last
+ * force evaluation, twice the contributing half-list pairs; out3[1]: how many
  * times the intermediate list (half-list pairs within the table cut + 0.9 A)
- * has been built. */
-int moldy_gpu_get_list_stats(moldy_gpu *h, double *out2);
+ * has been built; out3[2]: list entries the screening pass reads per step
+ * (the intermediate rows, or the half-list row where one overflowed). */
+int moldy_gpu_get_list_stats(moldy_gpu *h, double *out3);
 
 /* adjoint (no counterpart in the reference) ---------------------------------*/
 /* Gradients of a scalar loss L(E, F, sigma) with respect to the potential, for

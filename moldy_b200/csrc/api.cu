@@ -1103,19 +1103,29 @@ int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *c
     return rc;
 }
 
-int moldy_gpu_get_list_stats(moldy_gpu *h, double *out2) {
+int moldy_gpu_get_list_stats(moldy_gpu *h, double *out3) {
     GUARD(h);
-    if (!out2) return fail(MOLDY_ERR_INVALID, "null argument");
+    if (!out3) return fail(MOLDY_ERR_INVALID, "null argument");
+    moldy::Engine &E = *h->e;
     double np = 0.0;
     int32_t nb = 0;
-    cudaStream_t st = h->e->stream_ref();
-    cudaError_t e = cudaMemcpyAsync(&np, &h->e->d.box->npairs, sizeof(double), cudaMemcpyDeviceToHost, st);
+    unsigned long long ns = 0;
+    cudaStream_t st = E.stream_ref();
+    // the reduction scratch is idle between calls
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(E.d.partials);
+    cudaError_t e = cudaMemcpyAsync(&np, &E.d.box->npairs, sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&nb, &h->e->d.box->mid_builds, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(&nb, &E.d.box->mid_builds, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && nb > 0) {
+        moldy::launch_count_screened(E.d, E.prm, cnt, st);
+        e = cudaMemcpyAsync(&ns, cnt, sizeof(ns), cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return moldy::cuda_fail(e, "get_list_stats");
-    out2[0] = np;
-    out2[1] = (double)nb;
+    out3[0] = np;
+    out3[1] = (double)nb;
+    out3[2] = (double)ns;
     return MOLDY_OK;
 }
 

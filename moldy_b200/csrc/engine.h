@@ -230,6 +230,7 @@ void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
+void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s);
 size_t adjoint_smem_bytes(int nlookup);
 void launch_table_adjoint(const DeviceState &d, const AdjointArgs &a, double *grads, double *scr,
                           const double *gF, cudaStream_t s);

@@ -562,4 +562,22 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
     return nb;
 }
 
+// list entries the screening pass reads per step: the intermediate row, or
+// the half-list row of an atom whose intermediate row overflowed
+__global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_cnt, const int32_t *__restrict__ numn,
+                                 unsigned long long *__restrict__ out) {
+    unsigned long long s = 0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        int mc = mid_cnt[a];
+        s += (unsigned long long)(mc >= 0 ? mc : numn[a]);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+    k_count_screened<<<grid_blocks(p.nm, kAtomThreads), kAtomThreads, 0, s>>>(p.nm, d.mid_cnt, d.numn, out);
+}
+
 }  // namespace moldy

@@ -322,11 +322,12 @@ class MoldySystem:
                        for k, n in enumerate(names)}}
 
     def list_stats(self) -> dict:
-        """Directed interacting pairs of the last force evaluation and the
-        number of intermediate-list builds so far."""
-        v = np.zeros(2)
+        """Directed interacting pairs of the last force evaluation, the number
+        of intermediate-list builds so far and the list entries the screening
+        pass reads per step."""
+        v = np.zeros(3)
         check(self._L.moldy_gpu_get_list_stats(self._h, _dp(v)))
-        return {"pairs": float(v[0]), "mid_builds": int(v[1])}
+        return {"pairs": float(v[0]), "mid_builds": int(v[1]), "screened": float(v[2])}
 
     def pair_count(self) -> float:
         return self.list_stats()["pairs"]
