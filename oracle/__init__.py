@@ -83,6 +83,7 @@ def _load():
         "orc_energy_calc": (None, [vp, _D]),
         "orc_md_init": (ctypes.c_int, [vp]),
         "orc_md_step": (ctypes.c_int, [vp, _D]),
+        "orc_quench": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -287,6 +288,23 @@ class Oracle:
             raise RuntimeError(f"oracle md_step status {st}")
         keys = ["ke", "pe", "te", "h", "th", "vol", "s1", "s2", "s3", "temp", "boxke", "ntc"]
         return dict(zip(keys, o.tolist()))
+
+    def quench(self, maxfn=1000, criterion=0, fmax=1e-4):
+        """quench_m::quench (VA14CD + derivs).  criterion 0: the reference's
+        gsumsq <= 5e-7 nm; 1: max real force <= fmax (eV/A)."""
+        o = np.zeros(8)
+        st = self._lib.orc_quench(self._h, int(maxfn), int(criterion), float(fmax), _dp(o))
+        if st:
+            raise RuntimeError(f"oracle quench status {st}")
+        return _quench_dict(o)
+
+
+def _quench_dict(o8):
+    keys = ["f", "pe", "gsumsq", "fmax", "nfev", "iterations", "iflag", "status"]
+    d = dict(zip(keys, o8.tolist()))
+    for k in ("nfev", "iterations", "iflag", "status"):
+        d[k] = int(d[k])
+    return d
 
 
 def from_workload(w, *, uselookup=True, nlookup=5000, threads=None) -> Oracle:

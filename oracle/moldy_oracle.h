@@ -83,6 +83,11 @@ void orc_update_therm_avs(orc_sys *s, double *s123);  /* dynamics_m::update_ther
 void orc_energy_calc(orc_sys *s, double *en_atom);    /* dynamics_m::energy_calc */
 /* moldin strain-loop preparation: force, tgid, initial x2 and b2 */
 int orc_md_init(orc_sys *s);
+/* quench_m::quench with VA14CD and derivs (src/quench_m.F90:100-551); maxfn is
+ * NSTEPS; criterion 0: gsumsq <= 5e-7 nm, 1: max real force <= fmax.
+ * out8: f, pe, gsumsq, max |B0 f|, evaluations, iterations, iflag, status
+ * (pe and max |B0 f| are those of the last evaluation). */
+int orc_quench(orc_sys *s, int maxfn, int criterion, double fmax, double *out8);
 /* one mdloop iteration: velocityverlet, update_therm_avs, thermo, relink.
  * out12 = ke, pe, te, h, th, vol, s1, s2, s3, temperature, boxke, ntc */
 int orc_md_step(orc_sys *s, double *out12);

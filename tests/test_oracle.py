@@ -200,3 +200,28 @@ def test_nve_energy_conservation_exact(oracle_mod):
     o.md_init()
     te = [o.md_step()["te"] for _ in range(60)]
     assert np.ptp(te) / w.nm < 2e-5
+
+
+@pytest.mark.parametrize("case", json.load(open(os.path.join(GOLDEN, "perfect_lattice.json")))["cases"])
+def test_quench_reaches_perfect_lattice_energy(oracle_mod, case):
+    """VA14CD + derivs (exact mode) from a displaced lattice at a fixed box
+    ends at the 30-digit perfect-lattice energy."""
+    w = wl.make_workload(4, a0=case["a0"], sigma=0.1, temperature=0.0, ivol=1, seed=7)
+    o = oracle_mod.from_workload(w, uselookup=False, threads=2)
+    q = o.quench(maxfn=5000, criterion=1, fmax=1e-7)
+    assert q["iflag"] == 0 and q["fmax"] <= 1e-7
+    assert abs(q["f"] / w.nm - case["e_per_atom"]) < 1e-12
+
+
+def test_quench_reference_criterion(oracle_mod):
+    """The reference's acceptance test: sum of squared gradient <= 5e-7 nm."""
+    rng = np.random.default_rng(3)
+    w = wl.make_workload(5, sigma=0.1, temperature=0.0, ivol=1, seed=3,
+                         strain=wl.random_symmetric_strain(rng, 0.02))
+    o = oracle_mod.from_workload(w, uselookup=True, threads=2)
+    o.force()
+    e0 = float(o.energy_calc().sum())
+    q = o.quench(maxfn=5000, criterion=0)
+    assert q["iflag"] == 0
+    assert q["gsumsq"] <= 5e-7 * w.nm
+    assert q["f"] < e0
