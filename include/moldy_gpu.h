@@ -239,6 +239,58 @@ int moldy_fetm_knot_vjp(int32_t nv, const double *av, const double *rv, int32_t 
                         const double *g_dphi, const double *g_emb, const double *g_demb,
                         double *g_av, double *g_rv, double *g_ap, double *g_rp);
 
+/* batched supercells (no counterpart in the reference's API) ----------------*/
+/* Many independent systems of uneven size (strained or perturbed replicas)
+ * evaluated together: each launch covers every system.  Atoms of all systems
+ * are concatenated, each system's in the reference's order.  Per system the
+ * results are those of force() + energy_calc() (src/dynamics_m.F90:135-483)
+ * in lookup mode, and the quench is quench_m::quench with VA14CD and derivs
+ * (src/quench_m.F90:100-551) at a fixed box (ivol = 1).  Pairs are found by
+ * neighbour-cell tiles at every evaluation (all pairs inside the table cut),
+ * not by the Verlet list; beyond the cut every pair contributes zero, so the
+ * sums are those of a complete list.  Each box must be wider than twice the
+ * interaction range in every direction (MOLDY_ERR_INVALID otherwise). */
+typedef struct moldy_batch moldy_batch;
+int moldy_gpu_batch_create(int32_t nsys, const int32_t *natoms, double press, int32_t device,
+                           moldy_batch **out);
+int moldy_gpu_batch_destroy(moldy_batch *h);
+/* FETRANSMETAL Fe-Fe knots, lookup tables of nlookup intervals (as
+ * moldy_gpu_set_fetm_fe with uselookup = 1); energy_calc uses the exact pair function. */
+int moldy_gpu_batch_set_fetm_fe(moldy_batch *h, int32_t nv, const double *av, const double *rv,
+                                int32_t np, const double *ap, const double *rp, int32_t nlookup);
+/* x0, y0, z0: concatenated fractional positions; b0: 9 doubles per system
+ * (column-major); mass: per atom, NULL keeps the current (55.845 by default).
+ * Any pointer may be NULL to keep that part; b0 fixes the cell grids. */
+int moldy_gpu_batch_set_state(moldy_batch *h, const double *x0, const double *y0,
+                              const double *z0, const double *b0, const double *mass);
+int moldy_gpu_batch_get_state(moldy_batch *h, double *x0, double *y0, double *z0);
+/* One evaluation of every system.  out13 (13 doubles per system, may be NULL):
+ * pe of energy_calc (F + exact pair function), pe of force (F + tabulated pair
+ * function), largest real force |B0 f| (eV/A), vol, tp (column-major, the
+ * virial of force(), pairs with m_i + m_j > 0.1). */
+int moldy_gpu_batch_force(moldy_batch *h, double *out13);
+/* fractional forces, per-atom energies (energy_calc; force routine), rho/F/F' */
+int moldy_gpu_batch_get_forces(moldy_batch *h, double *fx, double *fy, double *fz);
+int moldy_gpu_batch_get_energies(moldy_batch *h, double *en_calc, double *en_force);
+int moldy_gpu_batch_get_density(moldy_batch *h, double *rho, double *afrho, double *dafrho);
+/* Conjugate-gradient quench of every system with at most maxfn function values
+ * each (VA14CD's MAXFN = NSTEPS).  criterion 0: the reference's acceptance,
+ * sum of squared gradient <= 5e-7 nm; 1: largest real force <= fmax (eV/A).
+ * out8 (8 doubles per system, may be NULL): f = pe + press vol at the returned
+ * point, pe and largest real force of the last evaluation, sum of squared
+ * gradient, function values, iterations, iflag (0 converged, 1 maxfn reached,
+ * 2 VA14CD's conjugate-gradient error return), 0.  The positions are left at
+ * the returned points (moldy_gpu_batch_get_state). */
+int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, double fmax,
+                           double *out8);
+/* Tile shape: lanes per home atom (4, 8, 16 or 32; default 8) and how many
+ * candidates a warp stages in shared memory (0..256, default 256; the rest are
+ * read from global memory). */
+int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
+/* Kernel launches queued so far by this handle; its cudaStream_t. */
+int moldy_gpu_batch_launches(moldy_batch *h, int64_t *launches);
+int moldy_gpu_batch_get_stream(moldy_batch *h, void **stream);
+
 /* force evaluation without device allocation -----------------------------*/
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (device memory owned by another allocator, or code that must not allocate

@@ -10,5 +10,6 @@ routine names on top of it.
 from ._lib import MoldyError, load  # noqa: F401
 from .potentials import FE_FE, FeFeCoefficients, read_pot_file  # noqa: F401
 from .system import MoldySystem  # noqa: F401
+from .batch import MoldyBatch  # noqa: F401
 
-__all__ = ["MoldySystem", "MoldyError", "FE_FE", "FeFeCoefficients", "read_pot_file", "load"]
+__all__ = ["MoldySystem", "MoldyBatch", "MoldyError", "FE_FE", "FeFeCoefficients", "read_pot_file", "load"]

@@ -102,6 +102,19 @@ SIGNATURES = {
     "moldy_gpu_get_list_stats": [H, D],
     "moldy_gpu_table_gradients": [H, ctypes.c_double, D, D, D, D, D, D, D, D],
     "moldy_gpu_knot_gradients": [H, ctypes.c_double, D, D, D, D, D, D],
+    "moldy_gpu_batch_create": [ctypes.c_int32, I, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(H)],
+    "moldy_gpu_batch_destroy": [H],
+    "moldy_gpu_batch_set_fetm_fe": [H, ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32],
+    "moldy_gpu_batch_set_state": [H, D, D, D, D, D],
+    "moldy_gpu_batch_get_state": [H, D, D, D],
+    "moldy_gpu_batch_force": [H, D],
+    "moldy_gpu_batch_get_forces": [H, D, D, D],
+    "moldy_gpu_batch_get_energies": [H, D, D],
+    "moldy_gpu_batch_get_density": [H, D, D, D],
+    "moldy_gpu_batch_quench": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, D],
+    "moldy_gpu_batch_set_tiles": [H, ctypes.c_int32, ctypes.c_int32],
+    "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],
+    "moldy_gpu_batch_get_stream": [H, ctypes.POINTER(ctypes.c_void_p)],
     "moldy_fetm_build_tables": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,
                                 D, D, D, D, D, D],
     "moldy_fetm_knot_vjp": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,

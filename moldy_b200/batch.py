@@ -1,0 +1,131 @@
+"""Many independent supercells on one GPU (the ``moldy_gpu_batch_*`` C ABI).
+
+Each system's energy, forces and virial are those of force() + energy_calc()
+(src/dynamics_m.F90:135-483) in lookup mode, and :meth:`MoldyBatch.quench` is
+quench_m::quench with VA14CD and derivs (src/quench_m.F90:100-551) at a fixed
+box, run for every system at once on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+from .system import _dp, _f64, _mat_f, _mat_from_f
+
+
+class MoldyBatch:
+    """nsys systems of natoms[s] atoms each, concatenated in system order."""
+
+    def __init__(self, natoms, *, press=0.0, device=0):
+        self._L = _lib.load()
+        na = np.ascontiguousarray(natoms, dtype=np.int32)
+        h = _lib.H()
+        check(self._L.moldy_gpu_batch_create(len(na), na.ctypes.data_as(_lib.I), float(press), int(device),
+                                             ctypes.byref(h)))
+        self._h = h
+        self.natoms = na.astype(np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.natoms)])
+        self.nsys = len(na)
+        self.ntot = int(self.offsets[-1])
+
+    @classmethod
+    def from_workloads(cls, ws, *, nlookup=5000, device=0):
+        b = cls([w.nm for w in ws], press=ws[0].press, device=device)
+        b.set_up_fetm(ws[0].coeffs, nlookup=nlookup)
+        b.set_state(np.concatenate([w.x0 for w in ws]), [w.b0 for w in ws],
+                    np.concatenate([w.atomic_mass for w in ws]))
+        return b
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.moldy_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_up_fetm(self, coeffs, *, nlookup=5000):
+        av, rv, ap, rp = (_f64(v) for v in (coeffs.av, coeffs.rv, coeffs.ap, coeffs.rp))
+        check(self._L.moldy_gpu_batch_set_fetm_fe(self._h, len(av), _dp(av), _dp(rv), len(ap), _dp(ap), _dp(rp),
+                                                  int(nlookup)))
+
+    def set_state(self, x0=None, b0=None, mass=None):
+        """x0: (ntot, 3) fractional positions; b0: nsys 3x3 boxes (columns are
+        box vectors); mass: (ntot,)."""
+        cols = [None, None, None]
+        if x0 is not None:
+            a = np.asarray(x0, dtype=np.float64).reshape(self.ntot, 3)
+            cols = [_f64(a[:, k]) for k in range(3)]
+        bb = None
+        if b0 is not None:
+            bb = _f64(np.concatenate([_mat_f(m) for m in b0]))
+        m = None if mass is None else _f64(mass)
+        check(self._L.moldy_gpu_batch_set_state(self._h, *[_dp(c) for c in cols], _dp(bb), _dp(m)))
+
+    def get_state(self) -> np.ndarray:
+        c = [np.zeros(self.ntot) for _ in range(3)]
+        check(self._L.moldy_gpu_batch_get_state(self._h, *[_dp(a) for a in c]))
+        return np.stack(c, axis=1)
+
+    def force(self) -> dict:
+        """One evaluation of every system: per-system arrays pe_calc
+        (energy_calc), pe (force routine), fmax (largest |B0 f|), vol, tp."""
+        o = np.zeros(13 * self.nsys)
+        check(self._L.moldy_gpu_batch_force(self._h, _dp(o)))
+        o = o.reshape(self.nsys, 13)
+        return {"pe_calc": o[:, 0].copy(), "pe": o[:, 1].copy(), "fmax": o[:, 2].copy(), "vol": o[:, 3].copy(),
+                "tp": np.stack([_mat_from_f(o[s, 4:13]) for s in range(self.nsys)])}
+
+    def forces(self) -> np.ndarray:
+        c = [np.zeros(self.ntot) for _ in range(3)]
+        check(self._L.moldy_gpu_batch_get_forces(self._h, *[_dp(a) for a in c]))
+        return np.stack(c, axis=1)
+
+    def energies(self):
+        a, b = np.zeros(self.ntot), np.zeros(self.ntot)
+        check(self._L.moldy_gpu_batch_get_energies(self._h, _dp(a), _dp(b)))
+        return a, b
+
+    def density(self) -> dict:
+        d = [np.zeros(self.ntot) for _ in range(3)]
+        check(self._L.moldy_gpu_batch_get_density(self._h, *[_dp(a) for a in d]))
+        return dict(rho=d[0], afrho=d[1], dafrho=d[2])
+
+    def quench(self, maxfn=1000, criterion=0, fmax=1e-4) -> dict:
+        """VA14CD quench of every system; criterion 0 is the reference's
+        (sum of squared gradient <= 5e-7 nm), 1 is max |B0 f| <= fmax."""
+        o = np.zeros(8 * self.nsys)
+        check(self._L.moldy_gpu_batch_quench(self._h, int(maxfn), int(criterion), float(fmax), _dp(o)))
+        o = o.reshape(self.nsys, 8)
+        return {"f": o[:, 0].copy(), "pe": o[:, 1].copy(), "gsumsq": o[:, 2].copy(), "fmax": o[:, 3].copy(),
+                "nfev": o[:, 4].astype(np.int64), "iterations": o[:, 5].astype(np.int64),
+                "iflag": o[:, 6].astype(np.int64)}
+
+    def set_tiles(self, lanes=8, staged=256):
+        check(self._L.moldy_gpu_batch_set_tiles(self._h, int(lanes), int(staged)))
+
+    def launches(self) -> int:
+        v = ctypes.c_int64(0)
+        check(self._L.moldy_gpu_batch_launches(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def stream_handle(self) -> int:
+        p = ctypes.c_void_p()
+        check(self._L.moldy_gpu_batch_get_stream(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def split(self, arr):
+        """Per-system views of a concatenated per-atom array."""
+        return [arr[self.offsets[s]:self.offsets[s + 1]] for s in range(self.nsys)]

@@ -267,10 +267,14 @@ int Engine::check_ready() {
     return MOLDY_OK;
 }
 
-int Engine::upload_tables() {
-    HostTables &h = ht;
+// Device copies of the host tables (lookup_m layout): double4 r nodes up to
+// the first node from which vee, dvee, phi and dphi are all zero, double2 rho
+// nodes, FP32 copies of both, and the Tables descriptor.  rcull is the radius
+// at and beyond which every pair contributes exactly zero (exact mode: the
+// largest knot), times 1 + 1e-12; 1e150 when the tables never reach zero.
+int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, double2 **e2d, float2 **e2fd,
+                         Tables &t, double *rcull_out) {
     int n = h.nlookup;
-    // first node from which all four r tables are zero to the end
     int cut = n + 1;
     for (int i = n; i >= 0; --i) {
         if (h.vee[i] != 0.0 || h.dvee[i] != 0.0 || h.phi[i] != 0.0 || h.dphi[i] != 0.0) break;
@@ -289,20 +293,20 @@ int Engine::upload_tables() {
         e2[i] = make_double2(h.emb[i], h.demb[i]);
         e2f[i] = make_float2((float)h.emb[i], (float)h.demb[i]);
     }
-    void *old[] = {d.tab_r4, d.tab_e2, d.tab_r4f, d.tab_e2f};
+    void *old[] = {*r4d, *e2d, *r4fd, *e2fd};
     for (void *b : old)
         if (b) cudaFree(b);
-    CHECK(dev_alloc(&d.tab_r4, nr, "tables"));
-    CHECK(dev_alloc(&d.tab_r4f, nr, "tables"));
-    CHECK(dev_alloc(&d.tab_e2, n + 1, "tables"));
-    CHECK(dev_alloc(&d.tab_e2f, n + 1, "tables"));
-    CUDA_CHECK(cudaMemcpy(d.tab_r4, r4.data(), nr * sizeof(double4), cudaMemcpyHostToDevice), "tables");
-    CUDA_CHECK(cudaMemcpy(d.tab_r4f, r4f.data(), nr * sizeof(float4), cudaMemcpyHostToDevice), "tables");
-    CUDA_CHECK(cudaMemcpy(d.tab_e2, e2.data(), (n + 1) * sizeof(double2), cudaMemcpyHostToDevice), "tables");
-    CUDA_CHECK(cudaMemcpy(d.tab_e2f, e2f.data(), (n + 1) * sizeof(float2), cudaMemcpyHostToDevice), "tables");
+    *r4d = nullptr; *e2d = nullptr; *r4fd = nullptr; *e2fd = nullptr;
+    CHECK(dev_alloc(r4d, nr, "tables"));
+    CHECK(dev_alloc(r4fd, nr, "tables"));
+    CHECK(dev_alloc(e2d, n + 1, "tables"));
+    CHECK(dev_alloc(e2fd, n + 1, "tables"));
+    CUDA_CHECK(cudaMemcpy(*r4d, r4.data(), nr * sizeof(double4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(*r4fd, r4f.data(), nr * sizeof(float4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(*e2d, e2.data(), (n + 1) * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(*e2fd, e2f.data(), (n + 1) * sizeof(float2), cudaMemcpyHostToDevice), "tables");
 
-    Tables &t = tab;
-    t.r4 = d.tab_r4; t.e2 = d.tab_e2; t.r4f = d.tab_r4f; t.e2f = d.tab_e2f;
+    t.r4 = *r4d; t.e2 = *e2d; t.r4f = *r4fd; t.e2f = *e2fd;
     t.nlookup = n;
     t.nr = nr;
     t.idx_cut = cut;
@@ -330,14 +334,23 @@ int Engine::upload_tables() {
     double rc = rcull < 1e150 ? rcull * (1.0 + 1.0e-12) : 1.0e150;
     t.rcull2 = rc * rc;
     t.rcull2f = (float)(rc * rc * (1.0 + 1.0e-6));
-    rcut = rc < 1e150 ? rc : prm.rnear;
-    rmid = std::min(prm.rnear, rcut + kMidSkin);
     t.nv = h.nv; t.np = h.np;
     for (int i = 0; i < 8; ++i) { t.av[i] = h.av[i]; t.rv[i] = h.rv[i]; t.ap[i] = h.ap[i]; t.rp[i] = h.rp[i]; }
     t.bier_cut1 = h.bier_cut1; t.bier_cut2 = h.bier_cut2;
     for (int k = 0; k < 4; ++k) t.sc[k] = h.sc[k];
     t.phi_cut1 = h.phi_cut1; t.phi_cut2 = h.phi_cut2;
     t.bier_a = h.bier_a; t.bier_zed = h.bier_zed;
+    *rcull_out = rc;
+    return MOLDY_OK;
+}
+
+int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
+int Engine::upload_tables() {
+    double rc = 0.0;
+    CHECK(upload_device_tables(ht, &d.tab_r4, &d.tab_r4f, &d.tab_e2, &d.tab_e2f, tab, &rc));
+    rcut = rc < 1e150 ? rc : prm.rnear;
+    rmid = std::min(prm.rnear, rcut + kMidSkin);
     potential_set_ = true;
     forces_current_ = false;
     return MOLDY_OK;

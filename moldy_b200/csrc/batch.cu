@@ -1,0 +1,1128 @@
+// batch.cu -- many independent supercells of uneven size in one set of
+// launches: energy, forces and virial by neighbour-cell tiles, and the device
+// conjugate-gradient quench.  No counterpart in the reference's API; each
+// system's results are those of force() + energy_calc()
+// (src/dynamics_m.F90:135-483) and its quench is quench()/VA14CD/derivs
+// (src/quench_m.F90:100-551) at a fixed box.
+//
+// Layout.  Atoms of all systems are concatenated, each system's in the
+// reference's order.  Every evaluation bins the atoms of the systems that
+// need one into a per-system grid of cells at least the interaction range
+// wide (in each direction, perpendicular to the cell faces), sorts each cell
+// by atom index, and copies positions into cell order.  One warp owns one
+// cell: it stages the atoms of the 27 (fewer for grids under 3 cells)
+// surrounding cells in shared memory and evaluates every pair of a home atom
+// with its lanes, reducing with shuffles.  Each pair is evaluated from both
+// ends, so there are no atomics and every sum has a fixed order.
+//
+// Pairs.  The reference sums over its Verlet list (pairs within rnear at the
+// last rebuild); every pair beyond the table cut contributes exactly zero, so
+// a complete set of the pairs inside the cut gives the same sums.  The tiles
+// find every pair within the cut at every evaluation.
+//
+// The quench keeps VA14CD's state per system in device memory.  One block per
+// system runs the state machine between function evaluations; a round is the
+// binning, the two tile passes and one control launch, captured once in a
+// CUDA graph and replayed until every system has finished.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace moldy {
+namespace {
+
+constexpr int kTileWarps = 4;     // cells (warps) per block
+constexpr int kTileCap = 256;     // staged candidates per warp
+constexpr int kCgThreads = 256;   // control block
+
+struct BSys {
+    int atom0, nm, cell0, ncell;
+    int nc[3], nst[3];            // cells per dimension; stencil offsets per dimension (1, 2 or 3)
+    int active;                   // evaluated in the next round
+    int pad;
+    double b0[9], tg[9], vol;
+};
+
+// VA14CD state of one system (src/quench_m.F90:323-551)
+struct CgState {
+    double f, xnew, dgstep, fmin, dginit, xmin, finit, gsinit, gmin, gm, xbound, clt, gnew;
+    double ggstar, beta, gamden, gsumsq, pe, last_fmax;
+    int itcrs, maxfnk, noerr, iflag, iretry, iterc, maxfnc, label, done, pad;
+};
+
+struct TileArgs {
+    const BSys *sys;
+    const int32_t *cell_sys, *cell_start, *sorted;
+    const double4 *spos;          // cell order: x, y, z, mass
+    const double *sfp;            // cell order: F'(rho)
+    int ncell;
+    int cap;                      // staged candidates per warp (<= kTileCap)
+    double rc2;                   // pairs at or beyond sqrt(rc2) contribute zero
+};
+
+__device__ __forceinline__ int stencil_off(int k, int nst) { return nst == 3 ? k - 1 : k; }
+
+__device__ __forceinline__ int wrapc(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+
+// Stages the candidates of cell c (the union of its stencil cells, in stencil
+// order) into the warp's tile; returns the count.  pre[0..ns] holds the prefix
+// of the stencil-cell sizes, cs[0..ns) their first sorted slot.
+template <bool FP>
+__device__ int stage_tile(const TileArgs &a, const BSys &S, int c, double4 *tp, double *tf, int *ti, int *pre,
+                          int *cs) {
+    const int lane = threadIdx.x & 31;
+    const int local = c - S.cell0;
+    const int cx = local % S.nc[0], cy = (local / S.nc[0]) % S.nc[1], cz = local / (S.nc[0] * S.nc[1]);
+    const int ns = S.nst[0] * S.nst[1] * S.nst[2];
+    int cnt = 0, start = 0;
+    if (lane < ns) {
+        int kx = lane % S.nst[0], ky = (lane / S.nst[0]) % S.nst[1], kz = lane / (S.nst[0] * S.nst[1]);
+        int ix = wrapc(cx + stencil_off(kx, S.nst[0]), S.nc[0]);
+        int iy = wrapc(cy + stencil_off(ky, S.nst[1]), S.nc[1]);
+        int iz = wrapc(cz + stencil_off(kz, S.nst[2]), S.nc[2]);
+        int cc = S.cell0 + ix + S.nc[0] * (iy + S.nc[1] * iz);
+        start = a.cell_start[cc];
+        cnt = a.cell_start[cc + 1] - start;
+    }
+    // inclusive scan of the counts over the lanes
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < ns) { pre[lane + 1] = inc; cs[lane] = start; }
+    if (lane == 0) pre[0] = 0;
+    const int total = __shfl_sync(0xffffffffu, inc, 31);
+    __syncwarp();
+    const int nstage = total < a.cap ? total : a.cap;
+    for (int k = lane; k < nstage; k += 32) {
+        int q = 0;
+        while (pre[q + 1] <= k) ++q;
+        int slot = cs[q] + (k - pre[q]);
+        tp[k] = a.spos[slot];
+        if (FP) tf[k] = a.sfp[slot];
+        ti[k] = slot;
+    }
+    __syncwarp();
+    return total;
+}
+
+// candidate k of the staged tile, or from global memory past the tile's capacity
+template <bool FP>
+__device__ __forceinline__ void candidate(const TileArgs &a, int k, const double4 *tp, const double *tf,
+                                          const int *ti, const int *pre, const int *cs, double4 &p, double &fp,
+                                          int &slot) {
+    if (k < a.cap) {
+        p = tp[k];
+        fp = FP ? tf[k] : 0.0;
+        slot = ti[k];
+    } else {
+        int q = 0;
+        while (pre[q + 1] <= k) ++q;
+        slot = cs[q] + (k - pre[q]);
+        p = a.spos[slot];
+        fp = FP ? a.sfp[slot] : 0.0;
+    }
+}
+
+__device__ __forceinline__ void pair_u(const double *b, double dx, double dy, double dz, double &ux, double &uy,
+                                       double &uz) {
+    ux = b[0] * dx + b[3] * dy + b[6] * dz;
+    uy = b[1] * dx + b[4] * dy + b[7] * dz;
+    uz = b[2] * dx + b[5] * dy + b[8] * dz;
+}
+
+template <int LPH>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = LPH / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ---------------------------------------------------------------- binning --
+__global__ void k_bin(int ntot, const double *__restrict__ X, const int32_t *__restrict__ atom_sys,
+                      const BSys *__restrict__ sys, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= ntot) return;
+    const BSys &S = sys[atom_sys[a]];
+    if (!S.active) { cell_of[a] = -1; return; }
+    int ic[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double x = X[3 * (size_t)a + d];
+        double u = x - floor(x);
+        int c = (int)(u * (double)S.nc[d]);
+        ic[d] = c < 0 ? 0 : (c >= S.nc[d] ? S.nc[d] - 1 : c);
+    }
+    int c = S.cell0 + ic[0] + S.nc[0] * (ic[1] + S.nc[1] * ic[2]);
+    cell_of[a] = c;
+    atomicAdd(&cell_count[c], 1);
+}
+
+__global__ void k_bin_fill(int ntot, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ cell_start,
+                           int32_t *__restrict__ cursor, int32_t *__restrict__ sorted) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= ntot) return;
+    int c = cell_of[a];
+    if (c < 0) return;
+    int k = atomicAdd(&cursor[c], 1);
+    sorted[cell_start[c] + k] = a;
+}
+
+// ascending atom order inside each cell, then positions and masses in cell order
+__global__ void k_bin_sort(int ncell, const int32_t *__restrict__ cell_start, int32_t *__restrict__ sorted,
+                           const double *__restrict__ X, const double *__restrict__ mass,
+                           double4 *__restrict__ spos) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int s0 = cell_start[c], s1 = cell_start[c + 1];
+    for (int i = s0 + 1; i < s1; ++i) {
+        int v = sorted[i], j = i - 1;
+        while (j >= s0 && sorted[j] > v) { sorted[j + 1] = sorted[j]; --j; }
+        sorted[j + 1] = v;
+    }
+    for (int i = s0; i < s1; ++i) {
+        int a = sorted[i];
+        spos[i] = make_double4(X[3 * (size_t)a], X[3 * (size_t)a + 1], X[3 * (size_t)a + 2], mass[a]);
+    }
+}
+
+// ------------------------------------------------------------ tile passes --
+// rho_i (rhoset), then F and F' (embed, src/potential_m.F90:148-169)
+template <int LPH>
+__global__ void __launch_bounds__(32 * kTileWarps)
+k_tile_density(TileArgs a, Tables t, double *__restrict__ sfp, double *__restrict__ rho_out,
+               double *__restrict__ afrho_out, double *__restrict__ fp_out) {
+    __shared__ double4 tpos[kTileWarps][kTileCap];
+    __shared__ int tidx[kTileWarps][kTileCap];
+    __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kTileWarps + w;
+    if (c >= a.ncell) return;
+    const BSys &S = a.sys[a.cell_sys[c]];
+    if (!S.active) return;
+    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
+    if (h1 == h0) return;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
+    const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
+    const int g = lane / LPH, gl = lane % LPH;
+    for (int hb = h0; hb < h1; hb += 32 / LPH) {
+        const int hs = hb + g;
+        double rho = 0.0;
+        if (hs < h1) {
+            const double4 ph = a.spos[hs];
+            for (int k = gl; k < total; k += LPH) {
+                double4 p; double fpk; int slot;
+                candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
+                if (slot == hs) continue;
+                double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                double ux, uy, uz;
+                pair_u(b, dx, dy, dz, ux, uy, uz);
+                double r2 = ux * ux + uy * uy + uz * uz;
+                if (r2 >= a.rc2) continue;
+                rho += density_func(t, sqrt(r2));
+            }
+        }
+        rho = group_sum<LPH>(rho);
+        if (hs < h1 && gl == 0) {
+            double f = 0.0, fd = 0.0;
+            if (rho > 1e-40) {
+                double2 e = embed_funcs(t, rho);
+                f = e.x; fd = e.y;
+            }
+            sfp[hs] = fd;
+            const int at = a.sorted[hs];
+            rho_out[at] = rho;
+            afrho_out[at] = f;
+            fp_out[at] = fd;
+        }
+    }
+}
+
+// Forces on each home atom (the pair loop of force(), src/dynamics_m.F90:232-318),
+// its energy_calc energy F + sum V_src/2 (src/dynamics_m.F90:412-483), the
+// force-routine energy F + sum V/2, and with VIR the per-atom virial
+// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1.
+template <int LPH, bool VIR>
+__global__ void __launch_bounds__(32 * kTileWarps)
+k_tile_forces(TileArgs a, Tables t, const double *__restrict__ afrho, double *__restrict__ fout,
+              double *__restrict__ en_calc, double *__restrict__ en_force, double *__restrict__ vir) {
+    __shared__ double4 tpos[kTileWarps][kTileCap];
+    __shared__ double tfp[kTileWarps][kTileCap];
+    __shared__ int tidx[kTileWarps][kTileCap];
+    __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kTileWarps + w;
+    if (c >= a.ncell) return;
+    const BSys &S = a.sys[a.cell_sys[c]];
+    if (!S.active) return;
+    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
+    if (h1 == h0) return;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
+    const int total = stage_tile<true>(a, S, c, tpos[w], tfp[w], tidx[w], tpre[w], tcs[w]);
+    const int g = lane / LPH, gl = lane % LPH;
+    for (int hb = h0; hb < h1; hb += 32 / LPH) {
+        const int hs = hb + g;
+        double fx = 0.0, fy = 0.0, fz = 0.0, ec = 0.0, ef = 0.0;
+        double v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = 0.0;
+        if (hs < h1) {
+            const double4 ph = a.spos[hs];
+            const double fph = a.sfp[hs];
+            for (int k = gl; k < total; k += LPH) {
+                double4 p; double fpk; int slot;
+                candidate<true>(a, k, tpos[w], tfp[w], tidx[w], tpre[w], tcs[w], p, fpk, slot);
+                if (slot == hs) continue;
+                double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                double ux, uy, uz;
+                pair_u(b, dx, dy, dz, ux, uy, uz);
+                double r2 = ux * ux + uy * uy + uz * uz;
+                if (r2 >= a.rc2) continue;
+                double r = sqrt(r2);
+                double4 q = pair_funcs(t, r);     // V, V', phi, phi'
+                double rr = 1.0 / r;
+                double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
+                fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+                ef += 0.5 * q.x;
+                ec += 0.5 * fetm_vee(t, r);
+                if (VIR && (ph.w + p.w) > 0.1) {
+                    double hf = 0.5 * fpair;
+                    v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
+                    v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
+                    v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
+                }
+            }
+        }
+        fx = group_sum<LPH>(fx); fy = group_sum<LPH>(fy); fz = group_sum<LPH>(fz);
+        ec = group_sum<LPH>(ec); ef = group_sum<LPH>(ef);
+        if (VIR) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) v[k] = group_sum<LPH>(v[k]);
+        }
+        if (hs < h1 && gl == 0) {
+            const int at = a.sorted[hs];
+            fout[3 * (size_t)at] = fx;
+            fout[3 * (size_t)at + 1] = fy;
+            fout[3 * (size_t)at + 2] = fz;
+            en_calc[at] = afrho[at] + ec;
+            en_force[at] = afrho[at] + ef;
+            if (VIR) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------ block reductions --
+// fixed-order sum over the block, returned to every thread
+__device__ double block_sum(double v, double *sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double x = lane < nw ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[32] = x;
+    }
+    __syncthreads();
+    return sh[32];
+}
+
+__device__ double block_max(double v, double *sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double x = lane < nw ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) sh[32] = x;
+    }
+    __syncthreads();
+    return sh[32];
+}
+
+// per-system sums of one evaluation: pe (energy_calc), pe (force), virial,
+// largest real force
+__global__ void __launch_bounds__(kCgThreads)
+k_sys_reduce(const BSys *__restrict__ sys, const double *__restrict__ en_calc, const double *__restrict__ en_force,
+             const double *__restrict__ vir, const double *__restrict__ f, int with_vir, double *__restrict__ out) {
+    __shared__ double sh[33];
+    const BSys &S = sys[blockIdx.x];
+    double ec = 0.0, ef = 0.0, fm = 0.0, v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < S.nm; i += blockDim.x) {
+        const int at = S.atom0 + i;
+        ec += en_calc[at];
+        ef += en_force[at];
+        if (with_vir)
+            for (int k = 0; k < 9; ++k) v[k] += vir[9 * (size_t)at + k];
+        double gx = f[3 * (size_t)at], gy = f[3 * (size_t)at + 1], gz = f[3 * (size_t)at + 2];
+        double rx, ry, rz;
+        pair_u(S.b0, gx, gy, gz, rx, ry, rz);
+        fm = fmax(fm, sqrt(rx * rx + ry * ry + rz * rz));
+    }
+    double o[13];
+    o[0] = block_sum(ec, sh);
+    o[1] = block_sum(ef, sh);
+    o[2] = block_max(fm, sh);
+    o[3] = S.vol;
+    for (int k = 0; k < 9; ++k) o[4 + k] = with_vir ? block_sum(v[k], sh) : 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 13; ++k) out[13 * (size_t)blockIdx.x + k] = o[k];
+}
+
+// --------------------------------------------------------- CG control --
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+struct CgVecs {
+    double *X, *G, *D, *GS, *XX, *GG, *DR, *DGR;
+};
+
+// One block per system.  On entry after an evaluation it finishes derivs
+// (pe = sum of energy_calc energies, g = -tg f, f = pe + press vol) and runs
+// VA14CD until it needs the next function value (it then leaves x set and
+// marks the system active) or returns (the system is done).  Scalars are
+// computed identically by every thread; vector sums use fixed-order block
+// reductions.  The statement labels follow src/quench_m.F90:323-551.
+__global__ void __launch_bounds__(kCgThreads)
+k_cg(BSys *__restrict__ sys, CgState *__restrict__ cg, CgVecs v, const double *__restrict__ fvec,
+     const double *__restrict__ en_calc, double press, int maxfn, int criterion, double fmax_tol,
+     int *__restrict__ n_active) {
+    __shared__ double sh[33];
+    BSys &S = sys[blockIdx.x];
+    CgState st = cg[blockIdx.x];
+    if (st.done) return;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = 3 * S.nm;            // atom variables; the nine box variables stay 0 in g and d
+    const int nref = n + 9;            // N of VA14CD
+    const size_t base = 3 * (size_t)S.atom0;
+    double *X = v.X + base, *G = v.G + base, *D = v.D + base, *GS = v.GS + base;
+    double *XX = v.XX + base, *GG = v.GG + base, *DR = v.DR + base, *DGR = v.DGR + base;
+    const double dfn = 0.1, acc = 5.0e-7 * (double)S.nm;
+    double c = 0.0, dtest, gamma, toplin, xold;
+    int guard = 0;
+
+    if (st.label == 0) {
+        st.xnew = 0.0; st.dgstep = 0.0; st.itcrs = 0; st.maxfnk = 0; st.fmin = 0.0; st.dginit = 0.0;
+        st.xmin = 0.0; st.finit = 0.0; st.gsinit = 0.0; st.gmin = 0.0; st.gm = 0.0; st.xbound = 0.0;
+        st.clt = 0.0; st.gnew = 0.0; st.ggstar = 0.0; st.beta = 0.0; st.noerr = 0; st.gamden = 0.0;
+        st.iflag = 0; st.iretry = -2; st.iterc = 0; st.maxfnc = 1; st.gsumsq = 0.0;
+        goto CALLF;
+    }
+    {
+        // derivs (src/quench_m.F90:215-313) for the evaluation just made
+        double pe = 0.0, fm = 0.0;
+        const double *tg = S.tg;
+        for (int i = tid; i < S.nm; i += nt) {
+            const size_t at = (size_t)S.atom0 + i;
+            pe += en_calc[at];
+            double fx = fvec[3 * at], fy = fvec[3 * at + 1], fz = fvec[3 * at + 2];
+            G[3 * i] = (-tg[0] * fx - tg[3] * fy - tg[6] * fz);
+            G[3 * i + 1] = (-tg[1] * fx - tg[4] * fy - tg[7] * fz);
+            G[3 * i + 2] = (-tg[2] * fx - tg[5] * fy - tg[8] * fz);
+            double rx, ry, rz;
+            pair_u(S.b0, fx, fy, fz, rx, ry, rz);
+            fm = fmax(fm, sqrt(rx * rx + ry * ry + rz * rz));
+        }
+        st.pe = block_sum(pe, sh);
+        st.last_fmax = block_max(fm, sh);
+        st.f = st.pe + press * S.vol;
+    }
+    goto L190_AFTER;
+
+L10:
+    st.xnew = fabs(dfn + dfn) / st.gsumsq;
+    st.dgstep = -st.gsumsq;
+L20:
+    st.itcrs = nref + 1;
+L30:
+    if (++guard > 100000) { st.iflag = 4; goto DONE; }
+    if (st.maxfnk >= st.maxfnc) goto L50;
+    st.f = st.fmin;
+    for (int i = tid; i < n; i += nt) { X[i] = XX[i]; G[i] = GG[i]; }
+    __syncthreads();
+L50:
+    if (st.iflag > 0) goto DONE;
+    if (st.itcrs <= nref) goto L70;
+    for (int i = tid; i < n; i += nt) D[i] = -G[i];
+    __syncthreads();
+L70:
+    st.iterc = st.iterc + 1;
+    {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) { GS[i] = G[i]; s += D[i] * G[i]; }
+        st.dginit = block_sum(s, sh);
+    }
+    if (st.dginit >= 0.0) goto L320;
+    st.xmin = 0.0;
+    st.fmin = st.f;
+    st.finit = st.f;
+    st.gsinit = st.gsumsq;
+    st.gmin = st.dginit;
+    st.gm = st.dginit;
+    st.xbound = -1.0;
+    st.xnew = st.xnew * dmin(1.0, st.dgstep / st.dginit);
+    st.dgstep = st.dginit;
+L170:
+    if (++guard > 100000) { st.iflag = 4; goto DONE; }
+    c = st.xnew - st.xmin;
+    {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) {
+            X[i] = XX[i] + c * D[i];
+            s += fabs(X[i] - XX[i]);
+        }
+        dtest = block_sum(s, sh);
+    }
+    if (dtest <= 0.0) st.clt = 0.7;
+    if (dtest <= 0.0) goto L300;
+    if (dmax(st.xbound, st.xmin - c) < 0.0) st.clt = 0.1;
+    st.maxfnc = st.maxfnc + 1;
+    goto CALLF;
+
+L190_AFTER:
+    if (st.maxfnc <= 1) goto L210;
+    {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) s += D[i] * G[i];
+        st.gnew = block_sum(s, sh);
+    }
+    if (st.f < st.fmin) goto L210;
+    if (st.f > st.fmin) goto L250;
+    if (fabs(st.gnew) > fabs(st.gmin)) goto L250;
+L210:
+    st.maxfnk = st.maxfnc;
+    {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) s += G[i] * G[i];
+        st.gsumsq = block_sum(s, sh);
+    }
+    if (criterion == 1 ? !(st.last_fmax <= fmax_tol) : (st.gsumsq > acc)) goto L250;
+    goto DONE;
+L250:
+    if (st.maxfnc != maxfn) goto L270;
+    st.iflag = 1;
+    goto L30;
+L270:
+    if (st.maxfnk < st.maxfnc) goto L300;
+    for (int i = tid; i < n; i += nt) { XX[i] = X[i]; GG[i] = G[i]; }
+    __syncthreads();
+    if (st.maxfnc <= 1) goto L10;
+    st.gm = st.gnew;
+    if (st.gm <= st.dginit) goto L310;
+    {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) s += GS[i] * G[i];
+        st.ggstar = block_sum(s, sh);
+    }
+    st.beta = (st.gsumsq - st.ggstar) / (st.gm - st.dginit);
+L300:
+    if (fabs(st.gm) > st.clt * fabs(st.dginit)) goto L310;
+    if (fabs(st.gm * st.beta) <= st.clt * st.gsumsq) goto L380;
+L310:
+    st.clt = st.clt + 0.3;
+    if (st.clt <= 0.8) goto L340;
+L320:
+    st.iretry = -st.iretry;
+    if (min(st.iretry, st.maxfnk) >= 2) goto L20;
+    st.noerr = st.noerr + 1;
+    if (st.noerr < 5) goto L20;
+    st.iflag = 2;
+    goto L30;
+L340:
+    xold = st.xnew;
+    st.xnew = 0.5 * (st.xmin + xold);
+    if (st.maxfnk < st.maxfnc) goto L350;
+    if (st.gmin * st.gnew <= 0.0) goto L350;
+    st.xnew = 10.0 * xold;
+    if (st.xbound >= 0.0) st.xnew = 0.5 * (xold + st.xbound);
+L350:
+    toplin = (3.0 * st.gnew + st.gmin - 4.0 * (st.f - st.fmin) / (xold - st.xmin));
+    c = st.gnew - toplin * (xold - st.xnew) / (xold - st.xmin);
+    if (st.maxfnk < st.maxfnc) goto L360;
+    if (st.gmin * st.gnew <= 0.0) st.xbound = st.xmin;
+    st.xmin = xold;
+    st.fmin = st.f;
+    st.gmin = st.gnew;
+    goto L370;
+L360:
+    st.xbound = xold;
+L370:
+    if (c * st.gmin >= 0.0) goto L170;
+    st.xnew = (st.xmin * c - st.xnew * st.gmin) / (c - st.gmin);
+    goto L170;
+L380:
+    if (dmin(st.f, st.fmin) < st.finit) goto L390;
+    if (st.gsumsq >= st.gsinit) goto L320;
+L390:
+    if (st.itcrs >= nref) goto L420;
+    if (fabs(st.ggstar) >= 0.2 * st.gsumsq) goto L420;
+    {
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = tid; i < n; i += nt) { s1 += GG[i] * DGR[i]; s2 += GG[i] * DR[i]; }
+        gamma = block_sum(s1, sh);
+        c = block_sum(s2, sh);
+    }
+    gamma = gamma / st.gamden;
+    if (fabs(st.beta * st.gm + gamma * c) >= 0.2 * st.gsumsq) goto L420;
+    for (int i = tid; i < n; i += nt) D[i] = -GG[i] + st.beta * D[i] + gamma * DR[i];
+    __syncthreads();
+    st.itcrs = st.itcrs + 1;
+    goto L30;
+L420:
+    st.itcrs = 2;
+    st.gamden = st.gm - st.dginit;
+    for (int i = tid; i < n; i += nt) {
+        DR[i] = D[i];
+        DGR[i] = GG[i] - GS[i];
+        D[i] = -GG[i] + st.beta * D[i];
+    }
+    __syncthreads();
+    goto L30;
+
+CALLF:
+    __syncthreads();
+    if (tid == 0) {
+        st.label = 1;
+        cg[blockIdx.x] = st;
+        S.active = 1;
+        atomicAdd(n_active, 1);
+    }
+    return;
+DONE:
+    __syncthreads();
+    if (tid == 0) {
+        st.done = 1;
+        cg[blockIdx.x] = st;
+        S.active = 0;
+    }
+}
+
+// deinterleaved copy of the variables x(3i-2..3i) <-> x0, y0, z0
+__global__ void k_pack(int ntot, const double *__restrict__ x, const double *__restrict__ y,
+                       const double *__restrict__ z, double *__restrict__ X) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= ntot) return;
+    X[3 * (size_t)a] = x[a]; X[3 * (size_t)a + 1] = y[a]; X[3 * (size_t)a + 2] = z[a];
+}
+
+__global__ void k_unpack(int ntot, const double *__restrict__ X, double *__restrict__ x, double *__restrict__ y,
+                         double *__restrict__ z) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= ntot) return;
+    x[a] = X[3 * (size_t)a]; y[a] = X[3 * (size_t)a + 1]; z[a] = X[3 * (size_t)a + 2];
+}
+
+__global__ void k_set_active(int nsys, BSys *sys, int v) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsys) sys[s].active = v;
+}
+
+}  // namespace
+
+constexpr int kTileCapMax = kTileCap;
+
+// =============================================================== engine ====
+class BatchEngine {
+  public:
+    int nsys = 0, ntot = 0, ncell = 0, device = 0;
+    double press = 0.0;
+    int lph = 8;                        // lanes per home atom in the tile passes
+    int cap = kTileCap;                 // staged candidates per warp
+    std::vector<int> natoms, atom0;
+    std::vector<BSys> hsys;
+    HostTables ht;
+    Tables tab;
+    double rcut = 0.0;
+    bool potential_set = false, state_set = false;
+    cudaStream_t stream = nullptr;
+    // device buffers
+    BSys *sys = nullptr;
+    int32_t *atom_sys = nullptr, *cell_sys = nullptr, *cell_of = nullptr, *cell_count = nullptr;
+    int32_t *cell_start = nullptr, *cursor = nullptr, *sorted = nullptr, *n_active = nullptr;
+    double *X = nullptr, *mass = nullptr, *f = nullptr, *rho = nullptr, *afrho = nullptr, *fp = nullptr;
+    double *en_calc = nullptr, *en_force = nullptr, *vir = nullptr, *sfp = nullptr, *sysout = nullptr;
+    double *cgv = nullptr;              // G, D, GS, XX, GG, DR, DGR (3*ntot each)
+    double4 *spos = nullptr;
+    CgState *cg = nullptr;
+    double4 *tab_r4 = nullptr;
+    double2 *tab_e2 = nullptr;
+    float4 *tab_r4f = nullptr;
+    float2 *tab_e2f = nullptr;
+    double *stage = nullptr;            // host-to-device staging (3*ntot)
+    int *host_active = nullptr;         // pinned
+    cudaGraphExec_t graph = nullptr;
+    int graph_lph = -1, graph_cap = -1, graph_maxfn = -1, graph_criterion = -1;
+    double graph_fmax = -1.0;
+    long long launches = 0;
+
+    ~BatchEngine();
+    int init(int n, const int32_t *na, double p, int dev);
+    int set_fetm(int nv, const double *av, const double *rv, int np, const double *ap, const double *rp,
+                 int nlookup);
+    int set_state(const double *x0, const double *y0, const double *z0, const double *b0, const double *m);
+    int get_state(double *x0, double *y0, double *z0);
+    int force(double *out13);
+    int quench(int maxfn, int criterion, double fmax, double *out8);
+    int get_array(const double *dev, int stride, double *a, double *b, double *c);
+    void queue_evaluation(bool with_vir);
+    int ready();
+};
+
+#define BCHECK(call)                                                      \
+    do {                                                                  \
+        int rc_ = (call);                                                 \
+        if (rc_ != MOLDY_OK) return rc_;                                  \
+    } while (0)
+#define BCUDA(call, what)                                                 \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) {                                          \
+            cudaGetLastError();                                           \
+            return set_last_error(MOLDY_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+        }                                                                 \
+    } while (0)
+
+template <typename T>
+static int balloc(T **p, size_t n, const char *what) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return set_last_error(MOLDY_ERR_CUDA, std::string("cudaMalloc ") + what + ": " + cudaGetErrorString(e));
+    }
+    return MOLDY_OK;
+}
+
+BatchEngine::~BatchEngine() {
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, mass,
+                    f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
+                    tab_r4f, tab_e2f, stage};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (host_active) cudaFreeHost(host_active);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_last_error(MOLDY_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (dev < 0 || dev >= ndev) return set_last_error(MOLDY_ERR_INVALID, "device ordinal out of range");
+    BCUDA(cudaSetDevice(dev), "cudaSetDevice");
+    cudaDeviceProp prop;
+    BCUDA(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+    if (prop.major != 10) return set_last_error(MOLDY_ERR_NO_DEVICE, "kernels are built for sm_100a only");
+    device = dev;
+    nsys = n;
+    press = p;
+    natoms.assign(na, na + n);
+    atom0.resize(n);
+    long long tot = 0;
+    for (int s = 0; s < n; ++s) {
+        if (na[s] < 2) return set_last_error(MOLDY_ERR_INVALID, "every system needs at least 2 atoms");
+        atom0[s] = (int)tot;
+        tot += na[s];
+    }
+    if (tot > (1LL << 28)) return set_last_error(MOLDY_ERR_CAPACITY, "more than 2^28 atoms in one batch");
+    ntot = (int)tot;
+    BCUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+    size_t nt = (size_t)ntot;
+    BCHECK(balloc(&sys, n, "systems"));
+    BCHECK(balloc(&atom_sys, nt, "atom_sys"));
+    BCHECK(balloc(&cell_of, nt, "cell_of"));
+    BCHECK(balloc(&sorted, nt, "sorted"));
+    BCHECK(balloc(&n_active, 1, "n_active"));
+    BCHECK(balloc(&X, 3 * nt, "X"));
+    BCHECK(balloc(&mass, nt, "mass"));
+    BCHECK(balloc(&f, 3 * nt, "f"));
+    BCHECK(balloc(&rho, nt, "rho"));
+    BCHECK(balloc(&afrho, nt, "afrho"));
+    BCHECK(balloc(&fp, nt, "fp"));
+    BCHECK(balloc(&en_calc, nt, "en_calc"));
+    BCHECK(balloc(&en_force, nt, "en_force"));
+    BCHECK(balloc(&vir, 9 * nt, "virial"));
+    BCHECK(balloc(&sfp, nt, "sfp"));
+    BCHECK(balloc(&spos, nt, "spos"));
+    BCHECK(balloc(&sysout, 13 * (size_t)n, "system results"));
+    BCHECK(balloc(&cgv, 7 * 3 * nt, "CG vectors"));
+    BCHECK(balloc(&cg, n, "CG state"));
+    BCHECK(balloc(&stage, 3 * nt, "staging"));
+    BCUDA(cudaMallocHost((void **)&host_active, sizeof(int)), "pinned");
+    std::vector<int32_t> as(nt);
+    for (int s = 0; s < n; ++s)
+        for (int i = 0; i < na[s]; ++i) as[atom0[s] + i] = s;
+    BCUDA(cudaMemcpy(atom_sys, as.data(), nt * sizeof(int32_t), cudaMemcpyHostToDevice), "atom_sys");
+    std::vector<double> m(nt, 55.845);
+    BCUDA(cudaMemcpy(mass, m.data(), nt * sizeof(double), cudaMemcpyHostToDevice), "mass");
+    hsys.assign(n, BSys());
+    return MOLDY_OK;
+}
+
+int BatchEngine::set_fetm(int nv, const double *av, const double *rv, int np, const double *ap, const double *rp,
+                          int nlookup) {
+    if (!av || !rv || !ap || !rp) return set_last_error(MOLDY_ERR_INVALID, "null coefficient pointer");
+    int rc = build_fetm_tables(ht, nv, av, rv, np, ap, rp, 1, nlookup);
+    if (rc != MOLDY_OK) return set_last_error(rc, "FETRANSMETAL set-up failed");
+    double rcull = 0.0;
+    BCHECK(upload_device_tables(ht, &tab_r4, &tab_r4f, &tab_e2, &tab_e2f, tab, &rcull));
+    // every pair beyond the table cut and the pair function's knots contributes zero
+    double r = rcull < 1e150 ? rcull : 0.0;
+    for (int i = 0; i < nv; ++i) r = std::max(r, rv[i] * (1.0 + 1e-12));
+    if (!(r > 0.0) || r > 1e100) return set_last_error(MOLDY_ERR_UNSUPPORTED, "tables without a finite cut");
+    rcut = r;
+    potential_set = true;
+    return MOLDY_OK;
+}
+
+int BatchEngine::set_state(const double *x0, const double *y0, const double *z0, const double *b0,
+                           const double *m) {
+    if (!potential_set) return set_last_error(MOLDY_ERR_ORDER, "set the potential before the state");
+    size_t nt = (size_t)ntot;
+    if (x0 && y0 && z0) {
+        BCUDA(cudaMemcpyAsync(stage, x0, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "x0");
+        BCUDA(cudaMemcpyAsync(stage + nt, y0, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "y0");
+        BCUDA(cudaMemcpyAsync(stage + 2 * nt, z0, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "z0");
+        k_pack<<<(ntot + 255) / 256, 256, 0, stream>>>(ntot, stage, stage + nt, stage + 2 * nt, X);
+    }
+    if (m) BCUDA(cudaMemcpyAsync(mass, m, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "mass");
+    if (b0) {
+        // per-system cell grids: at least rcut wide perpendicular to each face
+        int cell = 0;
+        std::vector<int32_t> csys;
+        for (int s = 0; s < nsys; ++s) {
+            BSys &S = hsys[s];
+            const double *b = b0 + 9 * (size_t)s;
+            for (int k = 0; k < 9; ++k) S.b0[k] = b[k];
+            double vol = b[0] * (b[4] * b[8] - b[7] * b[5]) + b[1] * (b[5] * b[6] - b[3] * b[8]) +
+                         b[2] * (b[3] * b[7] - b[4] * b[6]);
+            if (!(std::fabs(vol) > 0.0)) return set_last_error(MOLDY_ERR_SINGULAR_BOX, "singular box");
+            S.vol = vol;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double t = 0.0;
+                    for (int k = 0; k < 3; ++k) t += b[k + 3 * i] * b[k + 3 * j];
+                    S.tg[i + 3 * j] = t;
+                }
+            for (int d = 0; d < 3; ++d) {
+                const double *p = b + 3 * ((d + 1) % 3), *q = b + 3 * ((d + 2) % 3);
+                double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
+                double w = std::fabs(vol) / std::sqrt(cx * cx + cy * cy + cz * cz);
+                if (!(w > 2.0 * rcut))
+                    return set_last_error(MOLDY_ERR_INVALID, "system " + std::to_string(s) +
+                                                                 ": box narrower than twice the interaction range");
+                int nc = (int)std::floor(w / rcut);
+                nc = std::max(1, std::min(nc, 1024));
+                S.nc[d] = nc;
+                S.nst[d] = nc >= 3 ? 3 : nc;
+            }
+            S.atom0 = atom0[s];
+            S.nm = natoms[s];
+            S.cell0 = cell;
+            S.ncell = S.nc[0] * S.nc[1] * S.nc[2];
+            S.active = 1;
+            cell += S.ncell;
+            csys.insert(csys.end(), S.ncell, s);
+        }
+        if (cell != ncell) {
+            void *bufs[] = {cell_sys, cell_count, cell_start, cursor};
+            for (void *bp : bufs)
+                if (bp) cudaFree(bp);
+            cell_sys = cell_count = cell_start = cursor = nullptr;
+            ncell = cell;
+            BCHECK(balloc(&cell_sys, ncell, "cell_sys"));
+            BCHECK(balloc(&cell_count, ncell, "cell_count"));
+            BCHECK(balloc(&cell_start, ncell + 1, "cell_start"));
+            BCHECK(balloc(&cursor, ncell, "cursor"));
+            if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        }
+        BCUDA(cudaMemcpyAsync(cell_sys, csys.data(), csys.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream),
+              "cell_sys");
+        BCUDA(cudaMemcpyAsync(sys, hsys.data(), nsys * sizeof(BSys), cudaMemcpyHostToDevice, stream), "systems");
+        BCUDA(cudaStreamSynchronize(stream), "set_state");
+    }
+    if (x0 && y0 && z0 && b0) state_set = true;
+    BCUDA(cudaStreamSynchronize(stream), "set_state");
+    BCUDA(cudaGetLastError(), "set_state");
+    return MOLDY_OK;
+}
+
+int BatchEngine::ready() {
+    if (!potential_set) return set_last_error(MOLDY_ERR_ORDER, "the potential is not set");
+    if (!state_set) return set_last_error(MOLDY_ERR_ORDER, "positions and boxes are not set");
+    return MOLDY_OK;
+}
+
+template <int LPH>
+static void launch_tiles(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
+    const int nb = (E.ncell + kTileWarps - 1) / kTileWarps;
+    k_tile_density<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.sfp, E.rho, E.afrho, E.fp);
+    if (with_vir)
+        k_tile_forces<LPH, true><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.afrho, E.f, E.en_calc, E.en_force, E.vir);
+    else
+        k_tile_forces<LPH, false><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.afrho, E.f, E.en_calc, E.en_force,
+                                                                  E.vir);
+}
+
+// binning and the two tile passes for the systems marked active
+void BatchEngine::queue_evaluation(bool with_vir) {
+    cudaStream_t s = stream;
+    const int nb = (ntot + 255) / 256, nbc = (ncell + 255) / 256;
+    cudaMemsetAsync(cell_count, 0, sizeof(int32_t) * ncell, s);
+    k_bin<<<nb, 256, 0, s>>>(ntot, X, atom_sys, sys, cell_of, cell_count);
+    launch_exclusive_scan(cell_count, cell_start, ncell, s);
+    cudaMemsetAsync(cursor, 0, sizeof(int32_t) * ncell, s);
+    k_bin_fill<<<nb, 256, 0, s>>>(ntot, cell_of, cell_start, cursor, sorted);
+    k_bin_sort<<<nbc, 256, 0, s>>>(ncell, cell_start, sorted, X, mass, spos);
+    TileArgs a;
+    a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
+    a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
+    switch (lph) {
+        case 4: launch_tiles<4>(*this, a, with_vir, s); break;
+        case 16: launch_tiles<16>(*this, a, with_vir, s); break;
+        case 32: launch_tiles<32>(*this, a, with_vir, s); break;
+        default: launch_tiles<8>(*this, a, with_vir, s); break;
+    }
+    launches += 6;
+}
+
+int BatchEngine::force(double *out13) {
+    BCHECK(ready());
+    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1);
+    queue_evaluation(true);
+    k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+    launches += 2;
+    if (out13)
+        BCUDA(cudaMemcpyAsync(out13, sysout, 13 * (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost, stream),
+              "results");
+    BCUDA(cudaStreamSynchronize(stream), "batch force");
+    BCUDA(cudaGetLastError(), "batch force");
+    return MOLDY_OK;
+}
+
+int BatchEngine::get_array(const double *dev, int stride, double *a, double *b, double *c) {
+    size_t nt = (size_t)ntot;
+    if (stride == 3) {
+        k_unpack<<<(ntot + 255) / 256, 256, 0, stream>>>(ntot, dev, stage, stage + nt, stage + 2 * nt);
+        double *outs[3] = {a, b, c};
+        for (int k = 0; k < 3; ++k)
+            if (outs[k])
+                BCUDA(cudaMemcpyAsync(outs[k], stage + k * nt, nt * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                      "copy back");
+    } else if (a) {
+        BCUDA(cudaMemcpyAsync(a, dev, nt * sizeof(double), cudaMemcpyDeviceToHost, stream), "copy back");
+    }
+    BCUDA(cudaStreamSynchronize(stream), "copy back");
+    return MOLDY_OK;
+}
+
+int BatchEngine::get_state(double *x0, double *y0, double *z0) { return get_array(X, 3, x0, y0, z0); }
+
+int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
+    BCHECK(ready());
+    if (maxfn < 1) return set_last_error(MOLDY_ERR_INVALID, "maxfn < 1");
+    cudaStream_t s = stream;
+    size_t nt3 = 3 * (size_t)ntot;
+    CgVecs v;
+    v.X = X; v.G = cgv; v.D = cgv + nt3; v.GS = cgv + 2 * nt3; v.XX = cgv + 3 * nt3; v.GG = cgv + 4 * nt3;
+    v.DR = cgv + 5 * nt3; v.DGR = cgv + 6 * nt3;
+    BCUDA(cudaMemsetAsync(cgv, 0, 7 * nt3 * sizeof(double), s), "CG vectors");
+    BCUDA(cudaMemsetAsync(cg, 0, nsys * sizeof(CgState), s), "CG state");
+    BCUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s), "counter");
+    // first pass: every system asks for its first function value
+    k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active);
+    launches += 1;
+    BCUDA(cudaGetLastError(), "quench start");
+    // one round: evaluate the active systems, then advance every state machine
+    if (!graph || graph_lph != lph || graph_cap != cap || graph_maxfn != maxfn || graph_criterion != criterion || graph_fmax != fmax) {
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        cudaGraph_t g = nullptr;
+        BCUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+        queue_evaluation(false);
+        cudaMemsetAsync(n_active, 0, sizeof(int), s);
+        k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active);
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (g) cudaGraphDestroy(g);
+            return set_last_error(MOLDY_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        }
+        e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            graph = nullptr;
+            return set_last_error(MOLDY_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+        }
+        graph_lph = lph; graph_cap = cap; graph_maxfn = maxfn; graph_criterion = criterion; graph_fmax = fmax;
+        launches -= 6;   // captured, not run; counted per replay below
+    }
+    // VA14CD evaluates at most maxfn times; a few rounds more let every
+    // system reach its return
+    const int rounds = maxfn + 8;
+    for (int r = 0; r < rounds; ++r) {
+        BCUDA(cudaGraphLaunch(graph, s), "graph launch");
+        launches += 7;
+        if ((r & 7) == 7 || r == rounds - 1) {
+            BCUDA(cudaMemcpyAsync(host_active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s), "counter");
+            BCUDA(cudaStreamSynchronize(s), "quench");
+            if (*host_active == 0) break;
+        }
+    }
+    BCUDA(cudaStreamSynchronize(s), "quench");
+    BCUDA(cudaGetLastError(), "quench");
+    std::vector<CgState> hs(nsys);
+    BCUDA(cudaMemcpy(hs.data(), cg, nsys * sizeof(CgState), cudaMemcpyDeviceToHost), "CG state");
+    int unfinished = 0;
+    for (int k = 0; k < nsys; ++k) {
+        const CgState &c = hs[k];
+        if (!c.done) ++unfinished;
+        if (out8) {
+            double *o = out8 + 8 * (size_t)k;
+            o[0] = c.f; o[1] = c.pe; o[2] = c.gsumsq; o[3] = c.last_fmax;
+            o[4] = c.maxfnc; o[5] = c.iterc; o[6] = c.done ? c.iflag : 5; o[7] = 0.0;
+        }
+    }
+    // leave every system active for later force calls
+    k_set_active<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, sys, 1);
+    BCUDA(cudaStreamSynchronize(s), "quench");
+    if (unfinished) return set_last_error(MOLDY_ERR_CAPACITY, std::to_string(unfinished) + " systems did not finish");
+    return MOLDY_OK;
+}
+
+}  // namespace moldy
+
+// ================================================================ C ABI ====
+struct moldy_batch {
+    moldy::BatchEngine *e;
+};
+
+#define BGUARD(h)                                                                      \
+    do {                                                                               \
+        if (!(h) || !(h)->e) return moldy::set_last_error(MOLDY_ERR_INVALID, "null handle"); \
+        cudaSetDevice((h)->e->device);                                                \
+    } while (0)
+#define BTRY(expr)                                                                     \
+    try {                                                                              \
+        return (expr);                                                                 \
+    } catch (...) {                                                                    \
+        return moldy::set_last_error(MOLDY_ERR_CAPACITY, "host allocation failed");    \
+    }
+
+extern "C" {
+
+int moldy_gpu_batch_create(int32_t nsys, const int32_t *natoms, double press, int32_t device, moldy_batch **out) {
+    if (!out || !natoms || nsys < 1) return moldy::set_last_error(MOLDY_ERR_INVALID, "invalid arguments");
+    *out = nullptr;
+    try {
+        moldy::BatchEngine *e = new moldy::BatchEngine();
+        int rc = e->init(nsys, natoms, press, device);
+        if (rc != MOLDY_OK) { delete e; return rc; }
+        *out = new moldy_batch{e};
+        return MOLDY_OK;
+    } catch (...) {
+        return moldy::set_last_error(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
+}
+
+int moldy_gpu_batch_destroy(moldy_batch *h) {
+    if (!h) return MOLDY_OK;
+    delete h->e;
+    delete h;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_fetm_fe(moldy_batch *h, int32_t nv, const double *av, const double *rv, int32_t np,
+                                const double *ap, const double *rp, int32_t nlookup) {
+    BGUARD(h);
+    BTRY(h->e->set_fetm(nv, av, rv, np, ap, rp, nlookup));
+}
+
+int moldy_gpu_batch_set_state(moldy_batch *h, const double *x0, const double *y0, const double *z0,
+                              const double *b0, const double *mass) {
+    BGUARD(h);
+    BTRY(h->e->set_state(x0, y0, z0, b0, mass));
+}
+
+int moldy_gpu_batch_get_state(moldy_batch *h, double *x0, double *y0, double *z0) {
+    BGUARD(h);
+    BTRY(h->e->get_state(x0, y0, z0));
+}
+
+int moldy_gpu_batch_force(moldy_batch *h, double *out13) {
+    BGUARD(h);
+    BTRY(h->e->force(out13));
+}
+
+int moldy_gpu_batch_get_forces(moldy_batch *h, double *fx, double *fy, double *fz) {
+    BGUARD(h);
+    BTRY(h->e->get_array(h->e->f, 3, fx, fy, fz));
+}
+
+int moldy_gpu_batch_get_energies(moldy_batch *h, double *en_calc, double *en_force) {
+    BGUARD(h);
+    int rc = h->e->get_array(h->e->en_calc, 1, en_calc, nullptr, nullptr);
+    if (rc != MOLDY_OK) return rc;
+    return h->e->get_array(h->e->en_force, 1, en_force, nullptr, nullptr);
+}
+
+int moldy_gpu_batch_get_density(moldy_batch *h, double *rho, double *afrho, double *dafrho) {
+    BGUARD(h);
+    int rc = h->e->get_array(h->e->rho, 1, rho, nullptr, nullptr);
+    if (rc == MOLDY_OK) rc = h->e->get_array(h->e->afrho, 1, afrho, nullptr, nullptr);
+    if (rc == MOLDY_OK) rc = h->e->get_array(h->e->fp, 1, dafrho, nullptr, nullptr);
+    return rc;
+}
+
+int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, double fmax, double *out8) {
+    BGUARD(h);
+    BTRY(h->e->quench(maxfn, criterion, fmax, out8));
+}
+
+int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged) {
+    BGUARD(h);
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+        return moldy::set_last_error(MOLDY_ERR_INVALID, "lanes per atom must be 4, 8, 16 or 32");
+    if (staged < 0 || staged > moldy::kTileCapMax)
+        return moldy::set_last_error(MOLDY_ERR_INVALID, "staged candidates out of range");
+    h->e->lph = lanes;
+    h->e->cap = staged;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_launches(moldy_batch *h, int64_t *launches) {
+    BGUARD(h);
+    if (launches) *launches = h->e->launches;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_get_stream(moldy_batch *h, void **stream) {
+    BGUARD(h);
+    if (stream) *stream = (void *)h->e->stream;
+    return MOLDY_OK;
+}
+
+}  // extern "C"

@@ -234,6 +234,11 @@ void launch_count_screened(const DeviceState &d, const Params &p, unsigned long 
 size_t adjoint_smem_bytes(int nlookup);
 void launch_table_adjoint(const DeviceState &d, const AdjointArgs &a, double *grads, double *scr,
                           const double *gF, cudaStream_t s);
+int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, double2 **e2d, float2 **e2fd,
+                         Tables &t, double *rcull_out);
+int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv, int np,
+                      const double *ap, const double *rp, int uselookup, int nlookup);
+int set_last_error(int code, const std::string &msg);
 int fetm_knot_vjp(const HostTables &ht, const double *const g[6], double *g_av, double *g_rv,
                   double *g_ap, double *g_rp);
 

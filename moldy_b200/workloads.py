@@ -171,3 +171,22 @@ def config_adjoint(nconf: int = 256, n: int = 8, seed: int = 4,
         w.meta.update(config_temperature=t, strain=strain)
         out.append(w)
     return out
+
+
+def config_batch(nsys: int = 1024, seed: int = 3, n_range: tuple = (4, 16), sigma: float = 0.1,
+                 strain_amplitude: float = 0.02) -> list:
+    """Batched supercells: nsys bcc Fe systems of n^3 cells, n uniform in
+    n_range (inclusive), each with a symmetric strain whose components are
+    uniform in +/- strain_amplitude, Gaussian displacements sigma (A), at rest
+    and at a fixed box (ivol = 1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(nsys):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        strain = random_symmetric_strain(rng, strain_amplitude)
+        w = make_workload(n, sigma=sigma, temperature=0.0, ivol=1, nbrupdate=100,
+                          seed=int(rng.integers(1 << 30)), strain=strain,
+                          name=f"bcc_fe_{2 * n ** 3}_batch{c:04d}")
+        w.meta.update(strain=strain)
+        out.append(w)
+    return out
