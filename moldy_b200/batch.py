@@ -93,6 +93,13 @@ class MoldyBatch:
         check(self._L.moldy_gpu_batch_get_forces(self._h, *[_dp(a) for a in c]))
         return np.stack(c, axis=1)
 
+    def forces_into(self, fx, fy, fz):
+        """Fractional forces into three preallocated contiguous float64 arrays."""
+        for a in (fx, fy, fz):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (self.ntot,):
+                raise ValueError("forces_into needs contiguous float64 arrays of length ntot")
+        check(self._L.moldy_gpu_batch_get_forces(self._h, _dp(fx), _dp(fy), _dp(fz)))
+
     def energies(self):
         a, b = np.zeros(self.ntot), np.zeros(self.ntot)
         check(self._L.moldy_gpu_batch_get_energies(self._h, _dp(a), _dp(b)))
