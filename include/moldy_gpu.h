@@ -166,6 +166,16 @@ int moldy_gpu_md_steps(moldy_gpu *h, int32_t nsteps, moldy_thermo *thermo);
 /* dynamics_m::energy_calc (src/dynamics_m.F90:412-483): per-atom energy with
  * the exact pair function. */
 int moldy_gpu_energy_calc(moldy_gpu *h, double *en_atom);
+/* thermostat_m::scalev (src/thermostat_m.F90:317-395), the Nose-Hoover Euler
+ * thermostat.  moldy_gpu_set_thermostat sets simparam%nose and simparam%rqke
+ * (nose = 0: off, the default).  With nose > 0, moldy_gpu_md_steps calls
+ * scalev once per femtosecond of simulated time as the mdloop does
+ * (src/moldin.F90:828-835: a timer advanced by deltat against the constant
+ * 0.098227).  moldy_gpu_scalev calls it once now.  out4: nose, rqke, snhv
+ * (the accumulated scaling), the timer. */
+int moldy_gpu_set_thermostat(moldy_gpu *h, double nose, double rqke);
+int moldy_gpu_get_thermostat(moldy_gpu *h, double *out4);
+int moldy_gpu_scalev(moldy_gpu *h);
 /* Waits for all work queued on the handle's stream. */
 int moldy_gpu_synchronize(moldy_gpu *h);
 
@@ -180,7 +190,7 @@ int moldy_gpu_reset_kernel_stats(moldy_gpu *h);
  * family since the last reset; kernel ids are 0 .. MOLDY_KERNEL_FAMILIES-1. */
 int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64_t *launches);
 const char *moldy_gpu_kernel_name(int32_t kernel);
-#define MOLDY_KERNEL_FAMILIES 14
+#define MOLDY_KERNEL_FAMILIES 15
 
 /* kernel variants (no counterpart in the reference) -------------------------*/
 /* The screening, density and force passes are compiled in MOLDY_TUNE_VARIANTS

@@ -100,6 +100,9 @@ SIGNATURES = {
     "moldy_gpu_autotune": [H, ctypes.c_int32, D, I],
     "moldy_gpu_set_variants": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "moldy_gpu_get_list_stats": [H, D],
+    "moldy_gpu_set_thermostat": [H, ctypes.c_double, ctypes.c_double],
+    "moldy_gpu_get_thermostat": [H, D],
+    "moldy_gpu_scalev": [H],
     "moldy_gpu_table_gradients": [H, ctypes.c_double, D, D, D, D, D, D, D, D],
     "moldy_gpu_knot_gradients": [H, ctypes.c_double, D, D, D, D, D, D],
     "moldy_gpu_batch_create": [ctypes.c_int32, I, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(H)],
@@ -126,7 +129,7 @@ SIGNATURES = {
                                 ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 11,
 }
 NOALLOC_MAX_ATOMS = 262144
-KERNEL_FAMILIES = 14
+KERNEL_FAMILIES = 15
 TUNE_VARIANTS = 4
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}

@@ -81,7 +81,7 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
     "drift", "linkup", "relink", "build_nlist", "density", "screen", "forces",
-    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint"};
+    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint", "scalev"};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {
@@ -739,6 +739,13 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         ntcs[k] = ntc_;
         rbs[k] = rb ? 1 : 0;
         if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
+        // src/moldin.F90:828-835: scalev once per femtosecond of simulated time,
+        // with the mdloop's own constant for one femtosecond
+        thermotimer_ = thermotimer_ + prm.deltat;
+        if (thermotimer_ >= kFemtosecond) {
+            thermotimer_ = thermotimer_ - kFemtosecond;
+            if (nose_ > 0.0) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
+        }
     }
     CUDA_CHECK(cudaGetLastError(), "md_steps launch");
     CHECK(check_flags());
@@ -878,6 +885,31 @@ int Engine::knot_gradients(double gE, const double *gF, const double *gS, double
     const double *cg[6] = {g[0], g[1], g[2], g[3], g[4], g[5]};
     int rc = fetm_knot_vjp(ht, cg, g_av, g_rv, g_ap, g_rp);
     if (rc != MOLDY_OK) return fail(rc, "knot gradient contraction failed");
+    return MOLDY_OK;
+}
+
+int Engine::set_thermostat(double nose, double rqke) {
+    if (!(nose >= 0.0)) return fail(MOLDY_ERR_INVALID, "nose must be >= 0");
+    nose_ = nose;
+    rqke_ = rqke;
+    return MOLDY_OK;
+}
+
+int Engine::get_thermostat(double *out4) {
+    double v[2] = {0.0, 0.0};
+    CUDA_CHECK(cudaMemcpyAsync(&v[0], &d.box->snhv, sizeof(double), cudaMemcpyDeviceToHost, stream_), "snhv");
+    CUDA_CHECK(cudaMemcpyAsync(&v[1], &d.box->scalev_ke, sizeof(double), cudaMemcpyDeviceToHost, stream_), "ke");
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "thermostat");
+    out4[0] = nose_; out4[1] = rqke_; out4[2] = v[0]; out4[3] = thermotimer_;
+    return MOLDY_OK;
+}
+
+// one scalev call (src/thermostat_m.F90:317-395), whatever the timer
+int Engine::scalev() {
+    CHECK(check_ready());
+    if (nose_ > 0.0) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
+    CUDA_CHECK(cudaStreamSynchronize(stream_), "scalev");
+    CUDA_CHECK(cudaGetLastError(), "scalev");
     return MOLDY_OK;
 }
 
@@ -1165,6 +1197,22 @@ int moldy_gpu_knot_gradients(moldy_gpu *h, double g_energy, const double *g_forc
                              double *g_av, double *g_rv, double *g_ap, double *g_rp) {
     GUARD(h);
     TRY(h->e->knot_gradients(g_energy, g_force, g_stress, g_av, g_rv, g_ap, g_rp));
+}
+
+int moldy_gpu_set_thermostat(moldy_gpu *h, double nose, double rqke) {
+    GUARD(h);
+    TRY(h->e->set_thermostat(nose, rqke));
+}
+
+int moldy_gpu_get_thermostat(moldy_gpu *h, double *out4) {
+    GUARD(h);
+    if (!out4) return fail(MOLDY_ERR_INVALID, "null argument");
+    TRY(h->e->get_thermostat(out4));
+}
+
+int moldy_gpu_scalev(moldy_gpu *h) {
+    GUARD(h);
+    TRY(h->e->scalev());
 }
 
 int moldy_fetm_build_tables(int32_t nv, const double *av, const double *rv, int32_t np, const double *ap,

@@ -23,6 +23,7 @@ struct BoxState {
     double maxdisp;
     double npairs;                 // directed interacting pairs in the last density pass
     double bbuild[9];              // B0 when the intermediate list was built
+    double snhv, snhf, scalev_ke;  // Nose-Hoover scaling state of scalev and its last KE
     unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
     int32_t mid_builds;            // number of intermediate-list builds so far

@@ -270,6 +270,76 @@ void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStr
     k_finalize_therm<<<1, 256, 0, s>>>(p, d.box, d.partials, nblocks);
 }
 
+// ----------------------------------------------------------------- scalev --
+// scalev (src/thermostat_m.F90:317-395), the Nose-Hoover Euler thermostat:
+// remove the mean of x1 (over all atoms) from the movable atoms, measure their
+// kinetic energy, update snhv -= (ke - rqke) / (nose nm) and scale their x1
+// by 1 + snhv.  Atoms with Z = 0 or mass < 0.1 are not movable.
+__global__ void __launch_bounds__(256)
+k_scalev_mean(int nm, const double *__restrict__ x1, double *__restrict__ partials) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        v[0] += x1[a]; v[1] += x1[nm + a]; v[2] += x1[2 * nm + a];
+    }
+    block_partials<3>(v, partials, 0);
+}
+
+__global__ void __launch_bounds__(256)
+k_scalev_ke(Params p, const BoxState *__restrict__ box, const double *__restrict__ mean_part, int nblk,
+            double *__restrict__ x1, const double *__restrict__ mass, const int32_t *__restrict__ znum,
+            double *__restrict__ partials) {
+    __shared__ double s[3];
+    reduce_partials<3>(mean_part, nblk, s);
+    const int nm = p.nm;
+    const double fnm = (double)(float)nm;      // float(nm): default REAL
+    const double sx = s[0] / fnm, sy = s[1] / fnm, sz = s[2] / fnm;
+    const double *b = box->b0;
+    double v[1] = {0.0};
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        if (znum[a] == 0 || mass[a] < 0.1) continue;
+        double ux = x1[a] - sx, uy = x1[nm + a] - sy, uz = x1[2 * nm + a] - sz;
+        x1[a] = ux; x1[nm + a] = uy; x1[2 * nm + a] = uz;
+        double rx = b[0] * ux + b[3] * uy + b[6] * uz;
+        double ry = b[1] * ux + b[4] * uy + b[7] * uz;
+        double rz = b[2] * ux + b[5] * uy + b[8] * uz;
+        v[0] += mass[a] * (rx * rx + ry * ry + rz * rz);
+    }
+    block_partials<1>(v, partials, 0);
+}
+
+__global__ void __launch_bounds__(256)
+k_scalev_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ partials, int nblk, double nose,
+                double rqke) {
+    __shared__ double s[1];
+    reduce_partials<1>(partials, nblk, s);
+    if (threadIdx.x != 0) return;
+    BoxState &B = *box;
+    double ke = s[0] / (p.deltat * p.deltat) / 2.0;
+    // snhf keeps its previous value when ke is not positive
+    if (ke > 0.0) B.snhf = (ke - rqke) / (nose * (double)p.nm);
+    B.snhv = B.snhv - B.snhf;
+    B.scalev_ke = ke;
+}
+
+__global__ void __launch_bounds__(256)
+k_scalev_scale(int nm, const BoxState *__restrict__ box, double *__restrict__ x1, const double *__restrict__ mass,
+               const int32_t *__restrict__ znum) {
+    const double f = 1.0 + box->snhv;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        if (znum[a] == 0 || mass[a] < 0.1) continue;
+        x1[a] = x1[a] * f; x1[nm + a] = x1[nm + a] * f; x1[2 * nm + a] = x1[2 * nm + a] * f;
+    }
+}
+
+void launch_scalev(DeviceState &d, const Params &p, double nose, double rqke, cudaStream_t s) {
+    const int nb = grid_blocks(p.nm, kAtomThreads);
+    double *mean_part = d.partials, *ke_part = d.partials + (size_t)kMaxBlocks * kPartials;
+    k_scalev_mean<<<nb, kAtomThreads, 0, s>>>(p.nm, d.x1, mean_part);
+    k_scalev_ke<<<nb, kAtomThreads, 0, s>>>(p, d.box, mean_part, nb, d.x1, d.mass, d.znum, ke_part);
+    k_scalev_finish<<<1, kAtomThreads, 0, s>>>(p, d.box, ke_part, nb, nose, rqke);
+    k_scalev_scale<<<nb, kAtomThreads, 0, s>>>(p.nm, d.box, d.x1, d.mass, d.znum);
+}
+
 // ------------------------------------------------------------ energy_calc --
 // src/dynamics_m.F90:412-483: en_atom = F(rho) + half of each exact pair term
 __global__ void __launch_bounds__(256)

@@ -92,7 +92,7 @@ struct HostTables {
 // Kernel families timed by the optional per-kernel CUDA-event profiler.
 enum KernelId {
     K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_SCREEN, K_PAIR, K_FINALIZE,
-    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_ADJOINT, K_COUNT
+    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_ADJOINT, K_SCALEV, K_COUNT
 };
 extern const char *const kKernelNames[K_COUNT];
 
@@ -148,6 +148,10 @@ class Engine {
     int energy_calc(double *en_atom);
     int synchronize();
     int table_gradients(double gE, const double *gF, const double *gS, double *const g[6]);
+    // thermostat (thermostat_m): nose = 0 switches scalev off
+    int set_thermostat(double nose, double rqke);
+    int get_thermostat(double *out4);
+    int scalev();
     int knot_gradients(double gE, const double *gF, const double *gS, double *g_av, double *g_rv,
                        double *g_ap, double *g_rp);
     void set_ntc(int ntc) { ntc_ = ntc; }
@@ -156,7 +160,7 @@ class Engine {
     int device() const { return device_; }
     int precision() const { return precision_; }
     // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
-    int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
     int autotune(int nsteps, double *times_ms);
     // grows the compact list so that it holds the pairs a table cut of rcut
     // gives at the current atom density (and at least min_cap per side)
@@ -183,6 +187,8 @@ class Engine {
     bool potential_set_ = false;
     bool forces_current_ = false;   // force outputs match the state and tables
     double host_vol_ = 0.0;         // last box volume seen on the host
+    double nose_ = 0.0, rqke_ = 0.0; // scalev parameters (simparam%nose, simparam%rqke)
+    double thermotimer_ = 0.0;      // time since the last scalev (the mdloop's thermotimer)
     int active_overflow_ = 0;       // largest compact-list row of an overflowing evaluation
     double *part_embed_ = nullptr, *part_force_ = nullptr;   // slices of d.partials
     BoxState *host_box_ = nullptr;                            // pinned staging
@@ -195,6 +201,7 @@ constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
 constexpr int kOwnCap = 24;            // least own interacting pairs per atom in the compact list
 constexpr int kRevCap = 24;            // least reverse interacting pairs per atom
 constexpr int kMidCap = 40;            // half-list pairs per atom in the intermediate list
+constexpr double kFemtosecond = 0.098227;   // the mdloop's "fs" (src/moldin.F90:132), model time units
 constexpr double kMidSkin = 0.9;       // r_mid = table cut + kMidSkin (A), at most rnear
 constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
 constexpr int kFullTPA = 8;            // lanes per atom in the density and force passes
@@ -230,6 +237,7 @@ void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
+void launch_scalev(DeviceState &d, const Params &p, double nose, double rqke, cudaStream_t s);
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s);
 size_t adjoint_smem_bytes(int nlookup);
 void launch_table_adjoint(const DeviceState &d, const AdjointArgs &a, double *grads, double *scr,

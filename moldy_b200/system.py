@@ -288,6 +288,42 @@ class MoldySystem:
         keys = [f[0] for f in _lib.Thermo._fields_]
         return [{k: getattr(arr[i], k) for k in keys} for i in range(int(nsteps))]
 
+    def set_thermostat(self, nose: float, rqke: float):
+        """simparam%nose and simparam%rqke of scalev; nose = 0 switches it off."""
+        check(self._L.moldy_gpu_set_thermostat(self._h, float(nose), float(rqke)))
+
+    def thermostat(self) -> dict:
+        v = np.zeros(4)
+        check(self._L.moldy_gpu_get_thermostat(self._h, _dp(v)))
+        return {"nose": v[0], "rqke": v[1], "snhv": v[2], "thermotimer": v[3]}
+
+    def scalev(self):
+        check(self._L.moldy_gpu_scalev(self._h))
+
+    def strainloops(self, loops: int, nsteps: int, *, temprq: float, tempsp: float = 0.0, nose: float = 0.0,
+                    strx=None, thermo: bool = True):
+        """The strain-loop driver of moldin (src/moldin.F90:417-437): each loop
+        applies strx to B0 (when ivol != 0, keeping the old B0 in B2), raises
+        the required temperature by tempsp, sets rqke = 1.5 bk temprq (nm - 3),
+        then runs nsteps mdloop iterations with scalev (nose > 0).  Returns the
+        per-step thermodynamics (if asked) and the final temprq."""
+        from . import units
+        records = []
+        for _ in range(int(loops)):
+            if strx is not None and self.params.ivol != 0:
+                st = self.get_state()
+                b0 = np.asarray(strx, dtype=np.float64) @ st["b0"]
+                self.set_state(b0=b0, b2=st["b0"])
+            temprq = temprq + tempsp
+            rqke = 1.5 * units.BK * temprq * (self.nm - 3)
+            self.set_thermostat(nose, rqke)
+            r = self.md_steps(nsteps, thermo=thermo)
+            if thermo:
+                for rec in r:
+                    rec["temprq"] = temprq
+                records.extend(r)
+        return records, temprq
+
     def energy_calc(self) -> np.ndarray:
         e = np.zeros(self.nm)
         check(self._L.moldy_gpu_energy_calc(self._h, _dp(e)))

@@ -84,6 +84,9 @@ def _load():
         "orc_md_init": (ctypes.c_int, [vp]),
         "orc_md_step": (ctypes.c_int, [vp, _D]),
         "orc_quench": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D]),
+        "orc_set_thermostat": (None, [vp, ctypes.c_double, ctypes.c_double]),
+        "orc_get_thermostat": (None, [vp, _D]),
+        "orc_scalev": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -288,6 +291,17 @@ class Oracle:
             raise RuntimeError(f"oracle md_step status {st}")
         keys = ["ke", "pe", "te", "h", "th", "vol", "s1", "s2", "s3", "temp", "boxke", "ntc"]
         return dict(zip(keys, o.tolist()))
+
+    def set_thermostat(self, nose, rqke):
+        self._lib.orc_set_thermostat(self._h, float(nose), float(rqke))
+
+    def thermostat(self):
+        v = np.zeros(4)
+        self._lib.orc_get_thermostat(self._h, _dp(v))
+        return {"nose": v[0], "rqke": v[1], "snhv": v[2], "thermotimer": v[3]}
+
+    def scalev(self):
+        self._lib.orc_scalev(self._h)
 
     def quench(self, maxfn=1000, criterion=0, fmax=1e-4):
         """quench_m::quench (VA14CD + derivs).  criterion 0: the reference's

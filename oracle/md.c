@@ -702,7 +702,55 @@ int orc_md_init(orc_sys *s)
     return 0;
 }
 
-/* src/moldin.F90:752-791: one mdloop iteration without output/thermostat */
+/* scalev (src/thermostat_m.F90:317-395): Nose-Hoover Euler thermostat */
+void orc_scalev(orc_sys *s)
+{
+    if (!(s->nose > 0.0)) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0, s3 = 0.0;
+    for (int i = 1; i <= s->nm; ++i) {
+        sx = sx + s->x1[i];
+        sy = sy + s->y1[i];
+        sz = sz + s->z1[i];
+    }
+    const double fnm = (double)(float)s->nm; /* float(simparam%nm) */
+    sx = sx / fnm;
+    sy = sy / fnm;
+    sz = sz / fnm;
+    const double *b0 = s->b0;
+    for (int i = 1; i <= s->nm; ++i) {
+        if (s->atomic_number[i] == 0 || s->atomic_mass[i] < 0.1) continue;
+        s->x1[i] = s->x1[i] - sx;
+        s->y1[i] = s->y1[i] - sy;
+        s->z1[i] = s->z1[i] - sz;
+        double rx = M3(b0, 1, 1) * s->x1[i] + M3(b0, 1, 2) * s->y1[i] + M3(b0, 1, 3) * s->z1[i];
+        double ry = M3(b0, 2, 1) * s->x1[i] + M3(b0, 2, 2) * s->y1[i] + M3(b0, 2, 3) * s->z1[i];
+        double rz = M3(b0, 3, 1) * s->x1[i] + M3(b0, 3, 2) * s->y1[i] + M3(b0, 3, 3) * s->z1[i];
+        s3 = s3 + s->atomic_mass[i] * (rx * rx + ry * ry + rz * rz);
+    }
+    double ke = s3 / (s->deltat * s->deltat) / 2.0;
+    if (ke > 0.0) s->snhf = (ke - s->rqke) / (s->nose * (double)s->nm);
+    s->snhv = s->snhv - s->snhf;
+    for (int i = 1; i <= s->nm; ++i) {
+        if (s->atomic_number[i] == 0 || s->atomic_mass[i] < 0.1) continue;
+        s->x1[i] = s->x1[i] * (1.0 + s->snhv);
+        s->y1[i] = s->y1[i] * (1.0 + s->snhv);
+        s->z1[i] = s->z1[i] * (1.0 + s->snhv);
+    }
+}
+
+void orc_set_thermostat(orc_sys *s, double nose, double rqke)
+{
+    s->nose = nose;
+    s->rqke = rqke;
+}
+
+void orc_get_thermostat(const orc_sys *s, double *out4)
+{
+    out4[0] = s->nose; out4[1] = s->rqke; out4[2] = s->snhv; out4[3] = s->thermotimer;
+}
+
+/* src/moldin.F90:752-835: one mdloop iteration without output; scalev once
+ * per femtosecond (fs = 0.098227 model units, src/moldin.F90:132) */
 int orc_md_step(orc_sys *s, double *o)
 {
     int st = orc_velocityverlet(s);
@@ -718,6 +766,11 @@ int orc_md_step(orc_sys *s, double *o)
     double h = te + s->press * s->vol;
     double th = h + boxke;
     if (s->ntc == 0) orc_relink(s);
+    s->thermotimer = s->thermotimer + s->deltat;
+    if (s->thermotimer >= 0.098227) {
+        s->thermotimer = s->thermotimer - 0.098227;
+        if (s->nose != 0.0) orc_scalev(s);
+    }
     if (o) {
         o[0] = ke; o[1] = s->pe; o[2] = te; o[3] = h; o[4] = th; o[5] = s->vol;
         o[6] = s123[0]; o[7] = s123[1]; o[8] = s123[2]; o[9] = temp; o[10] = boxke;

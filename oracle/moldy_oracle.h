@@ -83,6 +83,10 @@ void orc_update_therm_avs(orc_sys *s, double *s123);  /* dynamics_m::update_ther
 void orc_energy_calc(orc_sys *s, double *en_atom);    /* dynamics_m::energy_calc */
 /* moldin strain-loop preparation: force, tgid, initial x2 and b2 */
 int orc_md_init(orc_sys *s);
+/* thermostat_m::scalev (src/thermostat_m.F90:317-395); nose = 0 is off */
+void orc_set_thermostat(orc_sys *s, double nose, double rqke);
+void orc_get_thermostat(const orc_sys *s, double *out4); /* nose, rqke, snhv, thermotimer */
+void orc_scalev(orc_sys *s);
 /* quench_m::quench with VA14CD and derivs (src/quench_m.F90:100-551); maxfn is
  * NSTEPS; criterion 0: gsumsq <= 5e-7 nm, 1: max real force <= fmax.
  * out8: f, pe, gsumsq, max |B0 f|, evaluations, iterations, iflag, status

@@ -47,6 +47,9 @@ struct orc_sys {
     double tginv[9], tgdot[9], tgid[9], fb[9];
     double vol, pe, ke;
 
+    /* thermostat_m (src/thermostat_m.F90:54-57) and the mdloop's thermotimer */
+    double nose, rqke, snhv, snhf, thermotimer;
+
     /* link cells and neighbour list */
     int *l0, *link, *ic;
     int *nlist, *numn;

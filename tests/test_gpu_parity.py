@@ -290,3 +290,43 @@ def test_md_hot_intermediate_list_rebuilds(oracle_mod, gpu_lib):
     assert np.max(np.abs(a - b)) < 1e-8 * np.max(np.abs(a))
     so, sg = o.get_state(), g.get_state()
     assert np.max(np.abs((sg["x0"] - so["x0"]) @ w.b0.T)) < 1e-7
+
+
+def test_scalev_thermostat_matches_oracle(gpu_lib, oracle_mod):
+    """mdloop with scalev (nose > 0) heating a 2000-atom NPT cell from 300 K
+    towards 900 K: the GPU trajectory follows the oracle's (thermo within 1e-9
+    relative over 60 steps), including snhv and the femtosecond timer."""
+    from moldy_b200 import MoldySystem, units
+    w = wl.make_workload(10, sigma=0.05, temperature=300.0, ivol=0, press_gpa=0.0, nbrupdate=20, seed=4)
+    rqke = 1.5 * units.BK * 900.0 * (w.nm - 3)
+    s = MoldySystem.from_workload(w)
+    s.linkup()
+    s.md_init()
+    s.set_thermostat(5.0, rqke)
+    g = s.md_steps(60)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=4)
+    o.md_init()
+    o.set_thermostat(5.0, rqke)
+    r = [o.md_step() for _ in range(60)]
+    for k in (0, 1, 2, 10, 30, 59):
+        for key in ("ke", "pe", "te", "th", "temp"):
+            assert abs(g[k][key] - r[k][key]) <= 1e-9 * abs(r[k][key]), (k, key, g[k][key], r[k][key])
+    tg, to = s.thermostat(), o.thermostat()
+    assert tg["snhv"] > 0.0          # kinetic energy below rqke: velocities scaled up
+    assert abs(tg["snhv"] - to["snhv"]) <= 1e-9 * abs(to["snhv"])
+    assert tg["thermotimer"] == to["thermotimer"]
+    s.close()
+
+
+def test_strainloops_ramp(gpu_lib):
+    """The strain-loop temperature ramp: each loop raises rqke; the cell heats."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(10, sigma=0.05, temperature=300.0, ivol=0, press_gpa=0.0, nbrupdate=20, seed=6)
+    s = MoldySystem.from_workload(w)
+    s.linkup()
+    s.md_init()
+    recs, t_end = s.strainloops(4, 50, temprq=300.0, tempsp=200.0, nose=2.0)
+    assert t_end == 1100.0 and len(recs) == 200
+    assert recs[-1]["temprq"] == 1100.0
+    assert np.mean([r["temp"] for r in recs[-20:]]) > np.mean([r["temp"] for r in recs[:20]]) + 100.0
+    s.close()
