@@ -58,9 +58,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0)
-    ap.add_argument("--workload", choices=["md", "batch", "adjoint"], default="md",
+    ap.add_argument("--workload", choices=["md", "batch", "adjoint", "liquid"], default="md",
                     help="md: the 2M-atom NPT step (headline); batch: 1024 supercells, force "
-                         "evaluations and the CG quench; adjoint: force-matching gradients")
+                         "evaluations and the CG quench; adjoint: force-matching gradients; liquid: "
+                         "the 1.024M-atom heating ramp 300 -> 2500 K with scalev")
     ap.add_argument("--nsys", type=int, default=1024, help="batch: number of supercells")
     ap.add_argument("--nconf", type=int, default=256, help="adjoint: number of configurations")
     return ap.parse_args()
@@ -696,6 +697,88 @@ def run_adjoint(args):
     return 0
 
 
+# ------------------------------------------------------------------ liquid --
+LIQ_METRIC = "atom-steps/s, 1.024M-atom bcc Fe heated 300 -> 2500 K (NPT, scalev every fs, nbrupdate 20)"
+
+
+def run_liquid(args):
+    import torch
+    from moldy_b200 import MoldySystem
+    from moldy_b200 import workloads as wl
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    w = wl.config_liquid(n=80, seed=5 + rank, temperature=300.0)
+    prec = "mixed" if args.precision in ("both", "mixed") else "fp64"
+    sysm = MoldySystem.from_workload(w, precision=prec, device=local_rank)
+    sysm.linkup()
+    sysm.md_init()
+    sysm.autotune(nreps=3)
+    stream = torch.cuda.ExternalStream(sysm.stream_handle(), device=local_rank)
+    loops, nose = 22, 10.0
+    per_loop = max(1, args.steps // loops) if args.steps != 1000 else 909
+    sysm.md_steps(max(args.warmup, 3), thermo=False)
+    sysm.reset_kernel_stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        recs, t_end = sysm.strainloops(loops, per_loop, temprq=300.0, tempsp=100.0, nose=nose, thermo=True)
+        e1.record(stream)
+        e1.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    nsteps = loops * per_loop
+    value = world * w.nm * nsteps / (ms / 1000.0)
+    launches = int(sum(n for _, n in sysm.kernel_stats().values()))
+    temps = [r["temp"] for r in recs]
+    # final segment without the thermostat: drift of the conserved quantity
+    # th = ke + pe + P V + box KE (per atom per ps), both precisions from the same state
+    drift = {}
+    if rank == 0 and not args.no_accuracy:
+        st = sysm.get_state()
+        for p2 in ("fp64", "mixed"):
+            s2 = MoldySystem.from_workload(w, precision=p2, device=local_rank)
+            s2.set_state(st["x0"], st["x1"], st["x2"], st["b0"], st["b1"], st["b2"], tgid=st["tgid"])
+            s2.linkup()
+            s2.md_init()
+            th = np.array([r["th"] for r in s2.md_steps(args.nve_steps)]) / w.nm
+            t = np.arange(len(th)) * (w.meta["dt_fs"] / 1000.0)
+            drift[p2] = {"slope_eV_per_atom_per_ps": float(np.polyfit(t, th, 1)[0]),
+                         "range_eV_per_atom": float(th.max() - th.min())}
+            s2.close()
+    sysm.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": LIQ_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": nsteps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / nsteps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": w.name, "atoms": w.nm, "loops": loops, "steps_per_loop": per_loop,
+                   "temprq_K": [300.0 + 100.0, t_end], "nose": nose, "nbrupdate": w.ntcm,
+                   "precision": prec, "ensemble": "NPT Parrinello-Rahman, P=0 GPa"},
+        "temperature_K": {"first_100_mean": float(np.mean(temps[:100])), "last_100_mean": float(np.mean(temps[-100:]))},
+        "final_segment_drift": drift, "clocks": clk.summary(), "gpu_launches": launches,
+        "e2e": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -704,6 +787,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "liquid":
+        return run_liquid(args)
     return run_ours(args)
 
 

@@ -113,6 +113,14 @@ int moldy_gpu_set_tables(moldy_gpu *h, int32_t nlookup, double rmin, double rmax
                          double rhomin, double rhomax, const double *vee,
                          const double *dvee, const double *phi, const double *dphi,
                          const double *emb, const double *demb);
+/* The Fe-Fe functions of the IRON_CARBON material module (src/iron_carbon.F90:
+ * Hepburn-Ackland Fe-C), tabulated as potential_set_lookup does over r in
+ * [0, 5.4] A and rho in [0, 10000] (lookup mode only; energy_calc and the knot
+ * gradients need the FETRANSMETAL forms and return MOLDY_ERR_UNSUPPORTED).
+ * moldy_ic_build_tables (no device needed) returns the same six tables. */
+int moldy_gpu_set_iron_carbon_fe(moldy_gpu *h, int32_t nlookup);
+int moldy_ic_build_tables(int32_t nlookup, double *vee, double *dvee, double *phi, double *dphi,
+                          double *emb, double *demb);
 /* Copies the six tables back (any pointer may be NULL). */
 int moldy_gpu_get_tables(moldy_gpu *h, double *vee, double *dvee, double *phi,
                          double *dphi, double *emb, double *demb);

@@ -364,6 +364,11 @@ int Engine::set_fetm(int nv, const double *av, const double *rv, int np, const d
     return upload_tables();
 }
 
+int Engine::set_iron_carbon(int nlookup) {
+    build_iron_carbon_tables(ht, nlookup);
+    return upload_tables();
+}
+
 int Engine::set_tables(int nlookup, double rmin, double rmax, double rhomin, double rhomax,
                        const double *vee, const double *dvee, const double *phi, const double *dphi,
                        const double *emb, const double *demb) {
@@ -1197,6 +1202,27 @@ int moldy_gpu_knot_gradients(moldy_gpu *h, double g_energy, const double *g_forc
                              double *g_av, double *g_rv, double *g_ap, double *g_rp) {
     GUARD(h);
     TRY(h->e->knot_gradients(g_energy, g_force, g_stress, g_av, g_rv, g_ap, g_rp));
+}
+
+int moldy_gpu_set_iron_carbon_fe(moldy_gpu *h, int32_t nlookup) {
+    GUARD(h);
+    TRY(h->e->set_iron_carbon(nlookup));
+}
+
+int moldy_ic_build_tables(int32_t nlookup, double *vee, double *dvee, double *phi, double *dphi, double *emb,
+                          double *demb) {
+    try {
+        if (nlookup < 2) return fail(MOLDY_ERR_INVALID, "nlookup < 2");
+        moldy::HostTables ht;
+        moldy::build_iron_carbon_tables(ht, nlookup);
+        double *out[6] = {vee, dvee, phi, dphi, emb, demb};
+        const std::vector<double> *src[6] = {&ht.vee, &ht.dvee, &ht.phi, &ht.dphi, &ht.emb, &ht.demb};
+        for (int k = 0; k < 6; ++k)
+            if (out[k]) std::memcpy(out[k], src[k]->data(), src[k]->size() * sizeof(double));
+        return MOLDY_OK;
+    } catch (...) {
+        return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
+    }
 }
 
 int moldy_gpu_set_thermostat(moldy_gpu *h, double nose, double rqke) {

@@ -122,6 +122,7 @@ class Engine {
 
     int set_fetm(int nv, const double *av, const double *rv, int np, const double *ap,
                  const double *rp, int uselookup, int nlookup);
+    int set_iron_carbon(int nlookup);
     int set_tables(int nlookup, double rmin, double rmax, double rhomin, double rhomax,
                    const double *vee, const double *dvee, const double *phi, const double *dphi,
                    const double *emb, const double *demb);
@@ -247,6 +248,7 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
 int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv, int np,
                       const double *ap, const double *rp, int uselookup, int nlookup);
 int set_last_error(int code, const std::string &msg);
+int build_iron_carbon_tables(HostTables &ht, int nlookup);
 int fetm_knot_vjp(const HostTables &ht, const double *const g[6], double *g_av, double *g_rv,
                   double *g_ap, double *g_rp);
 

@@ -271,4 +271,110 @@ int fetm_knot_vjp(const HostTables &ht, const double *const g[6], double *g_av, 
     return MOLDY_OK;
 }
 
+// ------------------------------------------------------- IRON_CARBON Fe-Fe --
+// The Fe-Fe functions of the IRON_CARBON material module (Hepburn-Ackland,
+// src/iron_carbon.F90): Biersack-Ziegler below 1 A, exp(cubic) join up to
+// 2.05 A (a default-REAL literal, as written), 13 cubic knots beyond
+// (118-266); phi a sum of 3 cubic knots (431-591); F(rho) = -sqrt(rho)
+// - 6.7314115586063e-4 rho^2 + 7.6514905604792e-8 rho^4, constant beyond
+// rho = 257 (599-696).  Tables over r in [0, 5.4] (pot_rmax, line 92).
+namespace {
+
+struct IronCarbonFe {
+    static constexpr double bierFe = 9734.159682000001;
+    static constexpr double b1 = 0.1818, x1 = -28.616172142695042, b2 = 0.5099, x2 = -8.42656844064423;
+    static constexpr double b3 = 0.2802, x3 = -3.6029549238411973, b4 = 0.02817, x4 = -1.8028188449897875;
+    static constexpr double j1 = 7.411957380630116, j2 = -0.6409989885339922;
+    static constexpr double j3 = -2.6049191728604733, j4 = 0.6263733940718166;
+    static constexpr double p1 = 4.2, p2 = 3.2, p3 = 2.4;
+    static constexpr double q1 = 0.47193527075943, q2 = 0.01471074009883, q3 = 11.68685940797;
+    static constexpr double rhocap = 257.0;
+    const double knot[13] = {5.3, 4.7, 4.2, 3.7, 3.3, 3.0, 2.8, 2.7, 2.6, 2.5, 2.4, 2.3, 2.2};
+    const double amp[13] = {-0.0030458824556234, -0.058531821042271, 0.35018615891957, -1.0260416933564,
+                            2.657740612828,      -2.3194358924605,   0.80656414937789, -0.77361294129713,
+                            4.2099676494795,     -2.4989799053251,   2.2077118733936,  15.738054058489,
+                            -27.444805994228};
+
+    static double step(double x) { return x < 0.0 ? 0.0 : 1.0; }
+    static bool spline(double r) { return r > (double)2.05f; }
+    static double joinexp(double r) { return std::exp(j1 + j2 * r + j3 * r * r + j4 * r * r * r); }
+
+    double vee(double r) const {
+        if (r < 1.0)
+            return (bierFe / r) * (b1 * std::exp(x1 * r) + b2 * std::exp(x2 * r) + b3 * std::exp(x3 * r) +
+                                   b4 * std::exp(x4 * r));
+        if (spline(r)) {
+            double v = 0.0;
+            for (int k = 0; k < 13; ++k) {
+                double d = knot[k] - r;
+                v = v + (step(d) * amp[k] * ((d * d) * d));
+            }
+            return v;
+        }
+        return joinexp(r);
+    }
+    double dvee(double r) const {
+        if (r < 1.0)
+            return -(bierFe / r) * ((1.0 / r - x1) * b1 * std::exp(x1 * r) + (1.0 / r - x2) * b2 * std::exp(x2 * r) +
+                                    (1.0 / r - x3) * b3 * std::exp(x3 * r) + (1.0 / r - x4) * b4 * std::exp(x4 * r));
+        if (spline(r)) {
+            double v = 0.0;
+            for (int k = 0; k < 13; ++k) {
+                double d = knot[k] - r;
+                v = v + (3.0 * step(d) * amp[k] * (d * d));
+            }
+            return -v;
+        }
+        return (j2 + 2.0 * j3 * r + 3.0 * j4 * r * r) * joinexp(r);
+    }
+    static double phi(double r) {
+        double d1 = p1 - r, d2 = p2 - r, d3 = p3 - r;
+        return step(d1) * q1 * ((d1 * d1) * d1) - step(d2) * q2 * ((d2 * d2) * d2) + step(d3) * q3 * ((d3 * d3) * d3);
+    }
+    static double dphi(double r) {
+        double d1 = p1 - r, d2 = p2 - r, d3 = p3 - r;
+        return -(3.0 * step(d1) * q1 * (d1 * d1) - 3.0 * step(d2) * q2 * (d2 * d2) + 3.0 * step(d3) * q3 * (d3 * d3));
+    }
+    static double embcore(double x) {
+        return (-1.0) * std::pow(x, 0.5) - (6.7314115586063e-4) * (x * x) + (7.6514905604792e-8) * ((x * x) * (x * x));
+    }
+    // the high-pressure correction of the reference has a zero amplitude
+    static double emb(double x) { return x > rhocap ? embcore(rhocap) : embcore(x); }
+    static double demb(double x) {
+        if (x <= 0.0 || x > rhocap) return 0.0;
+        return 0.5 * (-1.0) * std::pow(x, -0.5) - 2.0 * (6.7314115586063e-4) * x + 4.0 * (7.6514905604792e-8) * ((x * x) * x);
+    }
+};
+
+}  // namespace
+
+int build_iron_carbon_tables(HostTables &ht, int nlookup) {
+    if (nlookup < 2) nlookup = 5000;
+    IronCarbonFe f;
+    ht = HostTables();
+    ht.fetm = false;
+    ht.exact = false;
+    ht.nlookup = nlookup;
+    ht.rmin = 0.0; ht.rmax = 5.4; ht.rhomin = 0.0; ht.rhomax = 10000.0;
+    size_t n = (size_t)nlookup + 1;
+    ht.vee.assign(n, 0.0); ht.dvee.assign(n, 0.0); ht.phi.assign(n, 0.0); ht.dphi.assign(n, 0.0);
+    ht.emb.assign(n, 0.0); ht.demb.assign(n, 0.0);
+    double range = ht.rmax - ht.rmin, recipn = 1.0 / (double)nlookup;
+    for (int i = 0; i <= nlookup; ++i) {
+        double r = ht.rmin + (double)i * range * recipn;
+        ht.vee[i] = f.vee(r);
+        ht.dvee[i] = f.dvee(r);
+        ht.phi[i] = f.phi(r);
+        ht.dphi[i] = f.dphi(r);
+    }
+    double erange = ht.rhomax - ht.rhomin;
+    for (int i = 0; i <= nlookup; ++i) {
+        double rho = ht.rhomin + (double)i * erange * recipn;
+        ht.emb[i] = f.emb(rho);
+        ht.demb[i] = f.demb(rho);
+    }
+    ht.set = true;
+    return MOLDY_OK;
+}
+
 }  // namespace moldy

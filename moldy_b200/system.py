@@ -110,6 +110,11 @@ class MoldySystem:
         self.nlookup = int(nlookup)
         self.n_knots = (len(av), len(ap))
 
+    def set_up_iron_carbon(self, *, nlookup=5000):
+        """Fe-Fe functions of the IRON_CARBON module, lookup tables."""
+        check(self._L.moldy_gpu_set_iron_carbon_fe(self._h, int(nlookup)))
+        self.nlookup = int(nlookup)
+
     def set_tables(self, tables: dict, *, rmin=0.0, rmax=6.0, rhomin=0.0, rhomax=10000.0):
         t = {k: _f64(tables[k]) for k in ("vee", "dvee", "phi", "dphi", "emb", "demb")}
         n = len(t["vee"]) - 1

@@ -190,3 +190,115 @@ def config_batch(nsys: int = 1024, seed: int = 3, n_range: tuple = (4, 16), sigm
         w.meta.update(strain=strain)
         out.append(w)
     return out
+
+
+class ReferenceRandom:
+    """The reference's random number generator (src/random_m.F90): rstart
+    seeds the 97-entry lagged table, rand1 returns the next number in [0, 1).
+    The reference seeds it with rstart(97, 33, 21, 82) (src/moldin.F90:175)."""
+
+    def __init__(self, i=97, j=33, k=21, l=82):
+        u = [0.0] * 98
+        for ii in range(1, 98):
+            s, t = 0.0, 0.5
+            for _ in range(24):
+                m = ((i * j) % 179 * k) % 179
+                i, j, k = j, k, m
+                l = (53 * l + 1) % 169
+                if (l * m) % 64 >= 32:
+                    s = s + t
+                t = 0.5 * t
+            u[ii] = s
+        self.u = u
+        self.c = 362436.0 / 16777216.0
+        self.cd = 7654321.0 / 16777216.0
+        self.cm = 16777213.0 / 16777216.0
+        self.iu, self.ju = 97, 33
+
+    def rand1(self) -> float:
+        u = self.u
+        uni = u[self.iu] - u[self.ju]
+        if uni < 0.0:
+            uni = uni + 1.0
+        u[self.iu] = uni
+        self.iu -= 1
+        if self.iu == 0:
+            self.iu = 97
+        self.ju -= 1
+        if self.ju == 0:
+            self.ju = 97
+        self.c = self.c - self.cd
+        if self.c < 0.0:
+            self.c = self.c + self.cm
+        uni = uni - self.c
+        if uni < 0.0:
+            uni = uni + 1.0
+        return uni
+
+
+def setvel_reference(w: Workload, temprq: float, rng: ReferenceRandom | None = None) -> Workload:
+    """Initial velocities as the reference's setvel draws them
+    (src/thermostat_m.F90:201-256, with rqke = 1.5 bk temprq (nm - 1) from
+    src/thermostat_m.F90:97): uniform fractional components rand1() - 0.5 per
+    movable atom, the mass-weighted mean removed, scaled to rqke.  Box
+    velocities are only drawn for ivol >= 1 (not 4), which this does not do."""
+    if w.ivol >= 1 and w.ivol != 4:
+        raise ValueError("setvel_reference draws atom velocities only (ivol < 1 or ivol == 4)")
+    rng = rng or ReferenceRandom()
+    nm = w.nm
+    x1 = np.zeros((nm, 3))
+    mass = w.atomic_mass
+    movable = (w.atomic_number != 0) & (mass >= 0.1)
+    nmove = 0
+    for i in range(nm):
+        if not movable[i]:
+            continue
+        x1[i, 0] = rng.rand1() - 0.5
+        x1[i, 1] = rng.rand1() - 0.5
+        x1[i, 2] = rng.rand1() - 0.5
+        nmove += 1
+    sxyz = [0.0, 0.0, 0.0]
+    for d in range(3):
+        s = 0.0
+        for i in range(nm):
+            s = s + x1[i, d] * mass[i]
+        sxyz[d] = s / nmove
+    b0 = w.b0
+    s3 = 0.0
+    for i in range(nm):
+        if not movable[i]:
+            continue
+        for d in range(3):
+            x1[i, d] = x1[i, d] - sxyz[d] / mass[i]
+        rx = b0[0, 0] * x1[i, 0] + b0[0, 1] * x1[i, 1] + b0[0, 2] * x1[i, 2]
+        ry = b0[1, 0] * x1[i, 0] + b0[1, 1] * x1[i, 1] + b0[1, 2] * x1[i, 2]
+        rz = b0[2, 0] * x1[i, 0] + b0[2, 1] * x1[i, 1] + b0[2, 2] * x1[i, 2]
+        s3 = s3 + mass[i] * (rx * rx + ry * ry + rz * rz)
+    ke = s3 / w.deltat ** 2 / 2.0
+    rqke = 1.5 * units.BK * temprq * (nm - 1)
+    frac = float(np.sqrt(np.float32(np.float32(nmove) / np.float32(nm))))
+    scale = math.sqrt(rqke / ke) * frac
+    w2 = w.copy()
+    w2.x1 = x1 * scale
+    w2.meta.update(temperature=temprq, velocities="setvel (rand1)")
+    return w2
+
+
+def read_system_positions(n: int, rng: ReferenceRandom, dsp: float = 0.0, b0=None,
+                          basis=((0.0, 0.0, 0.0), (0.5, 0.5, 0.5))) -> np.ndarray:
+    """Fractional positions as read_system builds them (src/io_m.F90:221-248):
+    x0 = (rand1() - 1/2) dsp / B0(1,1) + (1/nt) (i0 + xb), three rand1 draws per
+    atom whatever dsp is, atoms in x-outer, z-inner, basis-innermost order."""
+    rt = 1.0 / n
+    b = np.asarray(b0) if b0 is not None else np.eye(3)
+    out = np.zeros((2 * n ** 3 if len(basis) == 2 else len(basis) * n ** 3, 3))
+    l = 0
+    for i0 in range(n):
+        for j0 in range(n):
+            for k0 in range(n):
+                for xb, yb, zb in basis:
+                    out[l, 0] = (rng.rand1() - 0.5) * dsp / b[0, 0] + rt * (i0 + xb)
+                    out[l, 1] = (rng.rand1() - 0.5) * dsp / b[1, 1] + rt * (j0 + yb)
+                    out[l, 2] = (rng.rand1() - 0.5) * dsp / b[2, 2] + rt * (k0 + zb)
+                    l += 1
+    return out

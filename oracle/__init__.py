@@ -58,6 +58,7 @@ def _load():
         "orc_get_max_threads": (ctypes.c_int, []),
         "orc_set_fetm": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, ctypes.c_int, _D, _D]),
         "orc_set_lookup": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "orc_set_iron_carbon": (ctypes.c_int, [vp]),
         "orc_get_tables": (None, [vp] + [_D] * 6),
         "orc_get_fetm_derived": (None, [vp, _D]),
         "orc_src": (ctypes.c_double, [vp, ctypes.c_int, ctypes.c_double]),
@@ -147,6 +148,10 @@ class Oracle:
         st = self._lib.orc_set_fetm(self._h, len(av), _dp(av), _dp(rv), len(ap), _dp(ap), _dp(rp))
         if st:
             raise RuntimeError(f"orc_set_fetm status {st}")
+
+    def set_iron_carbon(self):
+        """Fe-Fe functions of the IRON_CARBON module (src/iron_carbon.F90)."""
+        self._lib.orc_set_iron_carbon(self._h)
 
     def set_lookup(self, uselookup=True, nlookup=5000):
         st = self._lib.orc_set_lookup(self._h, int(bool(uselookup)), int(nlookup))

@@ -94,7 +94,7 @@ static double dexpjoin(double a1, double x1, double v1, double a2, double x2,
 }
 
 /* src/fetransmetal.F90:100-159 (vee_src), Fe-Fe branch */
-double orc_vee_src(const orc_sys *s, double r)
+static double fetm_vee_src(const orc_sys *s, double r)
 {
     double ans = 0.0;
     if (r > s->bier_cut2) {
@@ -112,7 +112,7 @@ double orc_vee_src(const orc_sys *s, double r)
 }
 
 /* src/fetransmetal.F90:167-219 (dvee_src) */
-double orc_dvee_src(const orc_sys *s, double r)
+static double fetm_dvee_src(const orc_sys *s, double r)
 {
     double ans = 0.0;
     if (r > s->bier_cut2) {
@@ -151,28 +151,44 @@ static double dphi_poly(const orc_sys *s, double r)
 }
 
 /* src/fetransmetal.F90:227-285 (phi_src): flat below the maximum of phi */
-double orc_phi_src(const orc_sys *s, double r)
+static double fetm_phi_src(const orc_sys *s, double r)
 {
     if (r < s->phi_cut1) return s->phi_cut2;
     return phi_poly(s, r);
 }
 
 /* src/fetransmetal.F90:293-366 (dphi_src) */
-double orc_dphi_src(const orc_sys *s, double r)
+static double fetm_dphi_src(const orc_sys *s, double r)
 {
     if (r < s->phi_cut1) return 0.0;
     return dphi_poly(s, r);
 }
 
 /* src/fetransmetal.F90:375-385 (emb_src) */
-double orc_emb_src(double rho) { return -(1.0 * sqrt(rho > 0.0 ? rho : 0.0)); }
+static double fetm_emb_src(double rho) { return -(1.0 * sqrt(rho > 0.0 ? rho : 0.0)); }
 
 /* src/fetransmetal.F90:394-404 (demb_src) */
-double orc_demb_src(double rho)
+static double fetm_demb_src(double rho)
 {
     double d = 0.0;
     if (rho > 0.0) d = -(0.5 / sqrt(rho));
     return d;
+}
+
+/* the material module in use: FETRANSMETAL (potential 0) or the Fe-Fe
+ * functions of IRON_CARBON (potential 1, ironcarbon.c) */
+double orc_vee_src(const orc_sys *s, double r) { return s->potential == 1 ? orc_ic_vee(r) : fetm_vee_src(s, r); }
+double orc_dvee_src(const orc_sys *s, double r) { return s->potential == 1 ? orc_ic_dvee(r) : fetm_dvee_src(s, r); }
+double orc_phi_src(const orc_sys *s, double r) { return s->potential == 1 ? orc_ic_phi(r) : fetm_phi_src(s, r); }
+double orc_dphi_src(const orc_sys *s, double r) { return s->potential == 1 ? orc_ic_dphi(r) : fetm_dphi_src(s, r); }
+double orc_emb_src(const orc_sys *s, double rho) { return s->potential == 1 ? orc_ic_emb(rho) : fetm_emb_src(rho); }
+double orc_demb_src(const orc_sys *s, double rho) { return s->potential == 1 ? orc_ic_demb(rho) : fetm_demb_src(rho); }
+
+int orc_set_iron_carbon(orc_sys *s)
+{
+    s->potential = 1;
+    s->fetm_set = 1;
+    return 0;
 }
 
 /* src/fetransmetal.F90:896-926 (phi_turn): bisection for the maximum of phi,
@@ -194,6 +210,7 @@ int orc_set_fetm(orc_sys *s, int nv, const double *av, const double *rv,
                  int np, const double *ap, const double *rp)
 {
     if (nv < 1 || nv > ORC_MAXCOEF || np < 1 || np > ORC_MAXCOEF) return 2;
+    s->potential = 0;
     s->nv = nv;
     s->np = np;
     for (int i = 0; i < nv; ++i) { s->av[i] = av[i]; s->rv[i] = rv[i]; }
@@ -218,6 +235,7 @@ int orc_set_fetm(orc_sys *s, int nv, const double *av, const double *rv,
     s->phi_cut1 = pc;
     s->phi_cut2 = orc_phi_src(s, pc);
     s->fetm_set = 1;
+    s->potential = 0;
     return 0;
 }
 
@@ -241,7 +259,8 @@ int orc_set_lookup(orc_sys *s, int uselookup, int nlookup)
     size_t n = (size_t)nlookup + 1;
     for (int k = 0; k < 6; ++k) s->tab[k] = (double *)calloc(n, sizeof(double));
 
-    s->vp_rmin = 0.0; s->vp_rmax = 6.0;
+    /* get_supported_potential_range: FETRANSMETAL 0..6, IRON_CARBON 0..5.4 (src/iron_carbon.F90:91-92) */
+    s->vp_rmin = 0.0; s->vp_rmax = s->potential == 1 ? 5.4 : 6.0;
     s->vp_range = s->vp_rmax - s->vp_rmin;
     s->vp_reciprange = 1.0 / s->vp_range;
     s->vp_recipnlkp = 1.0 / (double)nlookup;
@@ -260,8 +279,8 @@ int orc_set_lookup(orc_sys *s, int uselookup, int nlookup)
     s->e_recipstep = (double)nlookup / s->e_range;
     for (int i = 0; i <= nlookup; ++i) {
         double r = s->e_rmin + (double)i * s->e_range * s->e_recipnlkp;
-        s->tab[4][i] = orc_emb_src(r);
-        s->tab[5][i] = orc_demb_src(r);
+        s->tab[4][i] = orc_emb_src(s, r);
+        s->tab[5][i] = orc_demb_src(s, r);
     }
     return 0;
 }
@@ -307,8 +326,8 @@ double orc_src(const orc_sys *s, int which, double r)
     case 1: return orc_dvee_src(s, r);
     case 2: return orc_phi_src(s, r);
     case 3: return orc_dphi_src(s, r);
-    case 4: return orc_emb_src(r);
-    case 5: return orc_demb_src(r);
+    case 4: return orc_emb_src(s, r);
+    case 5: return orc_demb_src(s, r);
     }
     return 0.0;
 }
@@ -324,5 +343,5 @@ double orc_vee(const orc_sys *s, double r) { return s->uselookup ? orc_lookup_r(
 double orc_dvee(const orc_sys *s, double r) { return s->uselookup ? orc_lookup_r(s, s->tab[1], r) : orc_dvee_src(s, r); }
 double orc_phi(const orc_sys *s, double r) { return s->uselookup ? orc_lookup_r(s, s->tab[2], r) : orc_phi_src(s, r); }
 double orc_dphi(const orc_sys *s, double r) { return s->uselookup ? orc_lookup_r(s, s->tab[3], r) : orc_dphi_src(s, r); }
-double orc_emb(const orc_sys *s, double rho) { return s->uselookup ? orc_lookup_rho(s, s->tab[4], rho) : orc_emb_src(rho); }
-double orc_demb(const orc_sys *s, double rho) { return s->uselookup ? orc_lookup_rho(s, s->tab[5], rho) : orc_demb_src(rho); }
+double orc_emb(const orc_sys *s, double rho) { return s->uselookup ? orc_lookup_rho(s, s->tab[4], rho) : orc_emb_src(s, rho); }
+double orc_demb(const orc_sys *s, double rho) { return s->uselookup ? orc_lookup_rho(s, s->tab[5], rho) : orc_demb_src(s, rho); }

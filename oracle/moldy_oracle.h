@@ -42,6 +42,8 @@ int orc_set_fetm(orc_sys *s, int nv, const double *av, const double *rv,
 /* uselookup=1: build the six lookup_m tables with nlookup intervals
  * (r in [0,6], rho in [0,10000]); uselookup=0: exact *_src evaluation. */
 int orc_set_lookup(orc_sys *s, int uselookup, int nlookup);
+/* the Fe-Fe functions of the IRON_CARBON module (src/iron_carbon.F90) in place of FETRANSMETAL */
+int orc_set_iron_carbon(orc_sys *s);
 void orc_get_tables(const orc_sys *s, double *vee, double *dvee, double *phi,
                     double *dphi, double *emb, double *demb);
 void orc_get_fetm_derived(const orc_sys *s, double *out8);

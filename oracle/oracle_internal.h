@@ -25,6 +25,7 @@ struct orc_sys {
 
     /* FETRANSMETAL Fe-Fe data (src/fetransmetal.F90:70-90) */
     int nv, np, fetm_set;
+    int potential;   /* 0 FETRANSMETAL, 1 IRON_CARBON Fe-Fe */
     double av[ORC_MAXCOEF], rv[ORC_MAXCOEF], ap[ORC_MAXCOEF], rp[ORC_MAXCOEF];
     double p1, dp2, p3, dp4;
     double bier_cut1, bier_cut2, sc[4], phi_cut1, phi_cut2;
@@ -64,8 +65,14 @@ double orc_vee_src(const orc_sys *s, double r);
 double orc_dvee_src(const orc_sys *s, double r);
 double orc_phi_src(const orc_sys *s, double r);
 double orc_dphi_src(const orc_sys *s, double r);
-double orc_emb_src(double rho);
-double orc_demb_src(double rho);
+double orc_emb_src(const orc_sys *s, double rho);
+double orc_demb_src(const orc_sys *s, double rho);
+double orc_ic_vee(double r);
+double orc_ic_dvee(double r);
+double orc_ic_phi(double r);
+double orc_ic_dphi(double r);
+double orc_ic_emb(double rho);
+double orc_ic_demb(double rho);
 double orc_lookup_r(const orc_sys *s, const double *t, double r);
 double orc_lookup_rho(const orc_sys *s, const double *t, double rho);
 double orc_vee(const orc_sys *s, double r);

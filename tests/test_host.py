@@ -15,7 +15,7 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 def _declared_symbols():
     hdr = open(os.path.join(ROOT, "include", "moldy_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(moldy_(?:gpu|fetm)_[a-z_0-9]+)\s*\(", hdr)))
+    return sorted(set(re.findall(r"\b(moldy_(?:gpu|fetm|ic)_[a-z_0-9]+)\s*\(", hdr)))
 
 
 def test_library_exports_every_declared_symbol():
