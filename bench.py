@@ -173,14 +173,13 @@ def load_peaks():
 def kernel_bytes_per_atom(name, n_half, n_full, n_screen):
     """Algorithmic DRAM bytes per atom of one launch.
     n_half: mean half-list length; n_full: mean interacting (directed) pairs;
-    n_screen: mean list entries the screening pass reads (intermediate rows)."""
+    n_screen: mean intermediate-row entries the screening pass reads."""
     table = {
-        # screened row + count + own FP32 position + compact-list entries and counts
-        "screen": 4.0 * n_screen + 4 + 16 + 4.0 * n_full + 8,
-        # compact row + counts + own position, writes of (x,F') rho F F', old F', x1, mass, Z
-        "density": 4.0 * n_full + 8 + 32 + 32 + 24 + 8 + 24 + 8 + 4,
-        # compact row + counts + own (x,F') + mass, forces, x1 and x2 read+write, del2, Z
-        "forces": 4.0 * n_full + 8 + 32 + 8 + 24 + 48 + 48 + 8 + 4,
+        # intermediate row + count, compact-row writes + count, own position, pos2 write,
+        # rho/F/F' writes and old F', x1, mass, Z
+        "screen_density": 4.0 * n_screen + 4 + 4.0 * n_full + 4 + 32 + 32 + 24 + 8 + 24 + 8 + 4,
+        # compact row + count + own (x,F') + mass, forces, x1 and x2 read+write, del2, Z
+        "forces": 4.0 * n_full + 4 + 32 + 8 + 24 + 48 + 48 + 8 + 4,
         "drift": 32 + 48 + 32 + 16,
         "therm": 48 + 8 + 4,
         "build_nlist": 4.0 * n_half + 32 + 16,
@@ -272,10 +271,24 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     sysm.md_init()
     tune = sysm.autotune(nreps=5)
     stream = torch.cuda.ExternalStream(sysm.stream_handle(), device=local_rank)
+    # untimed: the intermediate-list skin that gives the shortest steps here
+    skin_ms = {}
+    for skin in (0.3, 0.45, 0.6, 0.9):
+        sysm.set_mid_skin(skin)
+        sysm.md_steps(20, thermo=False)
+        t0 = time.perf_counter()
+        sysm.md_steps(60, thermo=False)
+        sysm.synchronize()
+        skin_ms[skin] = (time.perf_counter() - t0) * 1000.0 / 60
+    best_skin = min(skin_ms, key=skin_ms.get)
+    sysm.set_mid_skin(best_skin)
+    tune["mid_skin_ms_per_step"] = skin_ms
+    tune["chosen"]["mid_skin_A"] = best_skin
     sysm.md_steps(max(args.warmup, 3), thermo=False)
     sysm.synchronize()
     sysm.reset_kernel_stats()
     sysm.set_profiling(True)
+    builds0 = sysm.list_stats()["mid_builds"]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
@@ -299,6 +312,7 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     lst = sysm.list_stats()
     n_full = lst["pairs"] / w.nm
     n_screen = lst["screened"] / w.nm
+    mid_builds_per_step = (lst["mid_builds"] - builds0) / args.steps
     dname, (dms, dlaunch) = max(stats.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = load_peaks()
     bpa = kernel_bytes_per_atom(dname, n_half, n_full, n_screen)
@@ -338,7 +352,7 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     sysm.close()
     return {"value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "stats": stats,
             "roofline": roofline, "e2e": e2e, "clocks": clk.summary(), "tune": tune,
-            "n_half": n_half, "n_full": n_full, "n_screen": n_screen}
+            "n_half": n_half, "n_full": n_full, "n_screen": n_screen, "mid_builds_per_step": mid_builds_per_step}
 
 
 def accuracy(w, local_rank, nve_steps):
@@ -424,7 +438,9 @@ def run_ours(args):
     if rank != 0:
         return 0
     extra = {"neighbours_half_mean": r["n_half"], "screened_entries_per_atom": r["n_screen"],
-             "interacting_pairs_per_atom": r["n_full"], "autotuned_variants": r["tune"]["chosen"]}
+             "interacting_pairs_per_atom": r["n_full"], "autotuned_variants": r["tune"]["chosen"],
+             "intermediate_list_builds_per_step": r["mid_builds_per_step"],
+             "mid_skin_ms_per_step": r["tune"].get("mid_skin_ms_per_step")}
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": r["ms_per_step"],

@@ -201,15 +201,23 @@ const char *moldy_gpu_kernel_name(int32_t kernel);
 #define MOLDY_KERNEL_FAMILIES 15
 
 /* kernel variants (no counterpart in the reference) -------------------------*/
-/* The screening, density and force passes are compiled in MOLDY_TUNE_VARIANTS
- * variants each (how many list entries a thread gathers before using them,
- * with or without L2 prefetches of the next atom's data).
+/* The screening-density pass and the force pass are compiled in
+ * MOLDY_TUNE_VARIANTS variants each: how many list entries a thread gathers
+ * before using them, with or without L2 prefetches of the next atom's data,
+ * and two or three resident blocks per SM (registers per thread).
  * moldy_gpu_autotune times every variant on the current configuration with
  * nreps force evaluations (positions, velocities, the rebuild counter and the
  * neighbour list are left unchanged) and keeps the fastest of each pass.
  * times_ms (3*MOLDY_TUNE_VARIANTS, may be NULL) receives the mean time per
- * launch; chosen (3, may be NULL) the selected variants. */
-#define MOLDY_TUNE_VARIANTS 4
+ * launch: screening-density, then zeros (the density pass is fused into it),
+ * then forces; chosen (3, may be NULL) the selected variants in that order.
+ * moldy_gpu_set_variants takes the same three numbers (the second is unused). */
+#define MOLDY_TUNE_VARIANTS 8
+/* Skin of the intermediate list (A, default 0.9): it holds the half-list pairs
+ * within min(rnear, table cut + skin) and is rebuilt on the device whenever
+ * the displacements since its build could bring an unlisted pair inside the
+ * cut.  Results do not depend on it; only the time per step does. */
+int moldy_gpu_set_mid_skin(moldy_gpu *h, double skin);
 int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
 int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
 /* out3[0]: directed interacting pairs (inside the table range) of the last

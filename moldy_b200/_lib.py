@@ -102,6 +102,7 @@ SIGNATURES = {
     "moldy_gpu_get_list_stats": [H, D],
     "moldy_gpu_set_iron_carbon_fe": [H, ctypes.c_int32],
     "moldy_ic_build_tables": [ctypes.c_int32, D, D, D, D, D, D],
+    "moldy_gpu_set_mid_skin": [H, ctypes.c_double],
     "moldy_gpu_set_thermostat": [H, ctypes.c_double, ctypes.c_double],
     "moldy_gpu_get_thermostat": [H, D],
     "moldy_gpu_scalev": [H],
@@ -132,7 +133,7 @@ SIGNATURES = {
 }
 NOALLOC_MAX_ATOMS = 262144
 KERNEL_FAMILIES = 15
-TUNE_VARIANTS = 4
+TUNE_VARIANTS = 8
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}
 

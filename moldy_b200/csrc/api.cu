@@ -80,7 +80,7 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
-    "drift", "linkup", "relink", "build_nlist", "density", "screen", "forces",
+    "drift", "linkup", "relink", "build_nlist", "density", "screen_density", "forces",
     "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint", "scalev"};
 
 cudaEvent_t Profiler::get() {
@@ -154,8 +154,8 @@ Engine::Engine(const moldy_params &p) {
     prm.nlcy = p.nlcy;
     prm.nlcz = p.nlcz;
     prm.ncell = 0;
-    prm.own_cap = kOwnCap;
-    prm.rev_cap = kRevCap;
+    prm.pair_cap = kPairCapMin;
+    prm.mid_cap = kMidCapMin;
     ntcm_ = p.ntcm;
     ntc_ = p.ntc;
     precision_ = p.precision;
@@ -169,7 +169,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
-                    d.own_cnt, d.rev_cnt, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -230,12 +230,11 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.numn, nm, "numn"));
     CHECK(dev_alloc(&d.posf, nm, "posf"));
     CHECK(dev_alloc(&d.pos2, nm, "pos2"));
-    CHECK(dev_alloc(&d.alist, nm * (size_t)(p.own_cap + p.rev_cap), "active list"));
-    CHECK(dev_alloc(&d.own_cnt, nm, "own_cnt"));
-    CHECK(dev_alloc(&d.mlist, nm * (size_t)kMidCap, "intermediate list"));
+    CHECK(dev_alloc(&d.alist, nm * (size_t)p.pair_cap, "compact list"));
+    CHECK(dev_alloc(&d.pair_cnt, nm, "pair_cnt"));
+    CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
     CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
-    CHECK(dev_alloc(&d.rev_cnt, nm, "rev_cnt"));
     CHECK(dev_alloc(&d.partials, 2 * (size_t)kMaxBlocks * kPartials, "partials"));
     CHECK(dev_alloc(&d.flags, 8, "flags"));
     CHECK(dev_alloc(&d.box, 1, "box"));
@@ -250,10 +249,9 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.numn, 0, nm * sizeof(int32_t)), "memset numn");
     CUDA_CHECK(cudaMemset(d.posf, 0, nm * sizeof(float4)), "memset posf");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
-    CUDA_CHECK(cudaMemset(d.own_cnt, 0, nm * sizeof(int32_t)), "memset own_cnt");
+    CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
     CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(double4)), "memset xbuild");
-    CUDA_CHECK(cudaMemset(d.rev_cnt, 0, nm * sizeof(int32_t)), "memset rev_cnt");
     CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
@@ -350,7 +348,7 @@ int Engine::upload_tables() {
     double rc = 0.0;
     CHECK(upload_device_tables(ht, &d.tab_r4, &d.tab_r4f, &d.tab_e2, &d.tab_e2f, tab, &rc));
     rcut = rc < 1e150 ? rc : prm.rnear;
-    rmid = std::min(prm.rnear, rcut + kMidSkin);
+    rmid = std::min(prm.rnear, rcut + mid_skin);
     potential_set_ = true;
     forces_current_ = false;
     return MOLDY_OK;
@@ -539,13 +537,18 @@ int Engine::check_flags() {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
         return fail(MOLDY_ERR_CAPACITY, "link-cell relink produced inconsistent cell counts");
     }
-    if (f[3]) {
+    if (f[3] || f[5]) {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
-        active_overflow_ = f[4];
-        return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[4]) +
-                                            " interacting neighbours on one side, more than the compact list holds (" +
-                                            std::to_string(prm.own_cap) + " own / " + std::to_string(prm.rev_cap) +
-                                            " reverse)");
+        active_overflow_ = f[3] ? f[4] : 0;
+        mid_overflow_ = f[5] ? f[6] : 0;
+        if (f[5]) mid_dirty_ = true;
+        if (f[3])
+            return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[4]) +
+                                                " interacting neighbours, more than the compact row holds (" +
+                                                std::to_string(prm.pair_cap) + ")");
+        return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[6]) +
+                                            " neighbours within r_mid, more than the intermediate row holds (" +
+                                            std::to_string(prm.mid_cap) + ")");
     }
     if (st) {
         cudaMemsetAsync(&d.box->status, 0, sizeof(int32_t), stream_);
@@ -592,8 +595,9 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     const bool rb = (ntc == 1 || !list_ready);
     // mode 1 (velocity Verlet) advances the box here, after the drift kernel;
     // force calls outside velocity Verlet always rebuild the intermediate list
-    LAUNCH(E, K_MID, 1, s,
-           launch_mid_decide(d, p, E.rmid, E.rcut, (mode == 1 && !rb) ? 0 : 1, mode == 1 ? 1 : 0, s));
+    const int force_mid = (mode == 1 && !rb && !E.mid_dirty()) ? 0 : 1;
+    E.clear_mid_dirty();
+    LAUNCH(E, K_MID, 1, s, launch_mid_decide(d, p, E.rmid, E.rcut, force_mid, mode == 1 ? 1 : 0, s));
     if (rb) {
         if (!cells_ready) { LAUNCH(E, K_LINKUP, 4, s, launch_linkup(d, p, s)); cells_ready = true; }
         LAUNCH(E, K_NLIST, 1, s, launch_build_nlist(d, p, s));
@@ -604,9 +608,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     int nbe = 0, nbf = 0;
-    LAUNCH(E, K_SCREEN, 1, s, launch_screen(d, p, E.tab, mixed, E.variant[K_SCREEN], s));
-    LAUNCH(E, K_DENSITY, 1, s,
-           nbe = launch_density_full(d, p, E.tab, mixed, E.variant[K_DENSITY], pe, s));
+    LAUNCH(E, K_SCREEN, 1, s, nbe = launch_screen_density(d, p, E.tab, mixed, E.variant[K_SCREEN], pe, s));
     LAUNCH(E, K_PAIR, 1, s,
            nbf = launch_forces(d, p, E.tab, mixed, mode == 1 ? 1 : 0, E.variant[K_PAIR], pf, s));
     LAUNCH(E, K_FINALIZE, 1, s, launch_finalize_force(d, p, pe, nbe, pf, nbf, mode, s));
@@ -649,12 +651,14 @@ int Engine::force(moldy_force_out *out) {
     for (int attempt = 0;; ++attempt) {
         bool rb = false;
         active_overflow_ = 0;
+        mid_overflow_ = 0;
         CHECK(force_device(&rb));
         int rc = fetch_force_out(out);
-        if (rc == MOLDY_ERR_CAPACITY && active_overflow_ > 0 && attempt < 2) {
+        if (rc == MOLDY_ERR_CAPACITY && (active_overflow_ > 0 || mid_overflow_ > 0) && attempt < 3) {
             // a force evaluation changes nothing but the rebuild counter and
-            // the lists: grow the compact list and evaluate again
-            CHECK(ensure_active_capacity(active_overflow_ + 8));
+            // the lists: grow the overflowing rows and evaluate again
+            CHECK(ensure_active_capacity(active_overflow_ > 0 ? active_overflow_ + 8 : 0,
+                                         mid_overflow_ > 0 ? mid_overflow_ + 16 : 0));
             ntc_ = ntc0;
             continue;
         }
@@ -665,22 +669,31 @@ int Engine::force(moldy_force_out *out) {
     }
 }
 
-int Engine::ensure_active_capacity(int min_cap) {
-    int need = std::max(kOwnCap, min_cap);
+int Engine::ensure_active_capacity(int min_pair, int min_mid) {
+    // pairs inside a radius: (4 pi / 3) r^3 n/V, with margin for fluctuations
+    auto expected = [&](double r) {
+        return (4.0 * M_PI / 3.0) * r * r * r * (double)prm.nm / host_vol_;
+    };
+    int need_pair = std::max(kPairCapMin, min_pair), need_mid = std::max(kMidCapMin, min_mid);
     if (host_vol_ > 0.0 && rcut > 0.0 && rcut < prm.rnear * 2.0) {
-        // pairs inside the cut, (4 pi / 3) rc^3 n/V, with margin: how they split
-        // between an atom's own row and its reverse entries depends on its
-        // place in the cell traversal, so either side may take nearly all
-        double full = (4.0 * M_PI / 3.0) * rcut * rcut * rcut * (double)prm.nm / host_vol_;
-        need = std::max(need, (int)std::ceil(1.25 * full + 8.0));
+        need_pair = std::max(need_pair, (int)std::ceil(1.25 * expected(rcut) + 8.0));
+        need_mid = std::max(need_mid, (int)std::ceil(1.25 * expected(rmid) + 16.0));
     }
-    need = std::min(need, std::max(2 * prm.nnbrs, kOwnCap));
-    if (need <= prm.own_cap && need <= prm.rev_cap) return MOLDY_OK;
-    if (d.alist) cudaFree(d.alist);
-    d.alist = nullptr;
-    CHECK(dev_alloc(&d.alist, (size_t)prm.nm * 2 * (size_t)need, "active list"));
-    prm.own_cap = need;
-    prm.rev_cap = need;
+    need_pair = std::min(need_pair, std::max(2 * prm.nnbrs, kPairCapMin));
+    need_mid = std::min(need_mid, std::max(2 * prm.nnbrs, kMidCapMin));
+    if (need_pair > prm.pair_cap) {
+        if (d.alist) cudaFree(d.alist);
+        d.alist = nullptr;
+        CHECK(dev_alloc(&d.alist, (size_t)prm.nm * (size_t)need_pair, "compact list"));
+        prm.pair_cap = need_pair;
+    }
+    if (need_mid > prm.mid_cap) {
+        if (d.mlist) cudaFree(d.mlist);
+        d.mlist = nullptr;
+        CHECK(dev_alloc(&d.mlist, (size_t)prm.nm * (size_t)need_mid, "intermediate list"));
+        prm.mid_cap = need_mid;
+        mid_dirty_ = true;
+    }
     return MOLDY_OK;
 }
 
@@ -792,14 +805,13 @@ int Engine::autotune(int nreps, double *times_ms) {
         list_ready_ = true;
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
-    const int fams[3] = {K_SCREEN, K_DENSITY, K_PAIR};
+    const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, 1, 0, stream_));
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
-        LAUNCH(*this, K_SCREEN, 1, stream_, launch_screen(d, prm, tab, mixed, variant[K_SCREEN], stream_));
-        LAUNCH(*this, K_DENSITY, 1, stream_,
-               launch_density_full(d, prm, tab, mixed, variant[K_DENSITY], pe, stream_));
+        LAUNCH(*this, K_SCREEN, 1, stream_,
+               launch_screen_density(d, prm, tab, mixed, variant[K_SCREEN], pe, stream_));
         LAUNCH(*this, K_PAIR, 1, stream_,
                launch_forces(d, prm, tab, mixed, 0, variant[K_PAIR], pf, stream_));
     };
@@ -807,7 +819,9 @@ int Engine::autotune(int nreps, double *times_ms) {
     CUDA_CHECK(cudaStreamSynchronize(stream_), "autotune");
     prof.harvest();
     prof.on = true;
-    for (int fi = 0; fi < 3; ++fi) {
+    if (times_ms)
+        for (int v = 0; v < kVariants; ++v) times_ms[kVariants + v] = 0.0;
+    for (int fi = 0; fi < 2; ++fi) {
         int fam = fams[fi], best = variant[fam];
         double best_ms = 1e300;
         for (int v = 0; v < kVariants; ++v) {
@@ -820,7 +834,7 @@ int Engine::autotune(int nreps, double *times_ms) {
             CUDA_CHECK(cudaStreamSynchronize(stream_), "autotune");
             prof.harvest();
             double ms = (prof.total_ms[fam] - t0) / nreps;
-            if (times_ms) times_ms[fi * kVariants + v] = ms;
+            if (times_ms) times_ms[(fi == 0 ? 0 : 2) * kVariants + v] = ms;
             if (ms < best_ms) { best_ms = ms; best = v; }
         }
         variant[fam] = best;
@@ -890,6 +904,16 @@ int Engine::knot_gradients(double gE, const double *gF, const double *gS, double
     const double *cg[6] = {g[0], g[1], g[2], g[3], g[4], g[5]};
     int rc = fetm_knot_vjp(ht, cg, g_av, g_rv, g_ap, g_rp);
     if (rc != MOLDY_OK) return fail(rc, "knot gradient contraction failed");
+    return MOLDY_OK;
+}
+
+// A thinner skin shortens the intermediate rows the screening pass walks every
+// step and makes their rebuilds (decided on the device) more frequent.
+int Engine::set_mid_skin(double skin) {
+    if (!(skin > 0.0) || !(skin <= 3.0)) return fail(MOLDY_ERR_INVALID, "skin must be in (0, 3] A");
+    mid_skin = skin;
+    if (rcut > 0.0) rmid = std::min(prm.rnear, rcut + mid_skin);
+    mid_dirty_ = true;
     return MOLDY_OK;
 }
 
@@ -1223,6 +1247,11 @@ int moldy_ic_build_tables(int32_t nlookup, double *vee, double *dvee, double *ph
     } catch (...) {
         return fail(MOLDY_ERR_CAPACITY, "host allocation failed");
     }
+}
+
+int moldy_gpu_set_mid_skin(moldy_gpu *h, double skin) {
+    GUARD(h);
+    TRY(h->e->set_mid_skin(skin));
 }
 
 int moldy_gpu_set_thermostat(moldy_gpu *h, double nose, double rqke) {

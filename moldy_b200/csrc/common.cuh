@@ -37,7 +37,7 @@ struct Params {
     double deltat, press, bdel2;
     int nm, nnbrs, ivol, atomstress;
     int nlcx, nlcy, nlcz, ncell;
-    int own_cap, rev_cap;    // compact-list entries per atom (own side, reverse side)
+    int pair_cap, mid_cap;   // entries per atom of the compact and the intermediate (full) rows
 };
 
 // Lookup-table description (lookup_m module data, src/lookup_m.F90:64-78).

@@ -40,12 +40,13 @@ struct DeviceState {
     float4 *posf = nullptr;
     // positions with F'(rho) in w, written by the density pass for the force pass
     double4 *pos2 = nullptr;
-    // compact full list of interacting pairs, entry-major: own entries
-    // (e * nm + i, e < own_cap), then reverse entries ((own_cap + e) * nm + i)
-    int32_t *alist = nullptr, *own_cnt = nullptr, *rev_cnt = nullptr;
-    // intermediate half list (pairs within r_mid when built), entry-major like
-    // nlist; mid_cnt < 0 marks an atom whose row overflowed (screen then reads
-    // its full half-list row); xbuild holds the positions at build time
+    // compact full list of the pairs inside the table cut, entry-major:
+    // entry e of atom i at alist[e * nm + i] (e < pair_cap), bit 31 set when
+    // j is in i's own half-list row; pair_cnt[i] entries
+    int32_t *alist = nullptr, *pair_cnt = nullptr;
+    // intermediate FULL list (half-list pairs within r_mid when built, entered
+    // in both rows, bit 31 on the owner's copy), entry-major; xbuild holds the
+    // positions at build time
     int32_t *mlist = nullptr, *mid_cnt = nullptr;
     double4 *xbuild = nullptr;
     // tables
@@ -74,6 +75,8 @@ struct AdjointArgs {
     double recipn;
     double gs[9], gE;
 };
+
+constexpr double kMidSkin = 0.9;       // default r_mid - table cut (A); r_mid is at most rnear
 
 // Host-side table data (potential_m / lookup_m).
 struct HostTables {
@@ -163,10 +166,12 @@ class Engine {
     // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
     int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
     int autotune(int nsteps, double *times_ms);
-    // grows the compact list so that it holds the pairs a table cut of rcut
-    // gives at the current atom density (and at least min_cap per side)
-    int ensure_active_capacity(int min_cap);
+    // sizes the compact and intermediate rows for the pairs inside rcut and
+    // r_mid at the current atom density (at least min_pair / min_mid entries)
+    int ensure_active_capacity(int min_pair, int min_mid = 0);
     double rmid = 0.0, rcut = 0.0;   // intermediate-list radius and table cut (A)
+    double mid_skin = kMidSkin;       // r_mid = min(rnear, rcut + mid_skin)
+    int set_mid_skin(double skin);
 
     DeviceState d;
     Params prm;
@@ -190,7 +195,13 @@ class Engine {
     double host_vol_ = 0.0;         // last box volume seen on the host
     double nose_ = 0.0, rqke_ = 0.0; // scalev parameters (simparam%nose, simparam%rqke)
     double thermotimer_ = 0.0;      // time since the last scalev (the mdloop's thermotimer)
-    int active_overflow_ = 0;       // largest compact-list row of an overflowing evaluation
+    int active_overflow_ = 0;       // largest compact row of an overflowing evaluation
+    int mid_overflow_ = 0;          // largest intermediate row of an overflowing build
+    bool mid_dirty_ = true;         // the intermediate list must be rebuilt before use
+  public:
+    bool mid_dirty() const { return mid_dirty_; }
+    void clear_mid_dirty() { mid_dirty_ = false; }
+  private:
     double *part_embed_ = nullptr, *part_force_ = nullptr;   // slices of d.partials
     BoxState *host_box_ = nullptr;                            // pinned staging
     int host_box_cap_ = 0;
@@ -199,11 +210,9 @@ class Engine {
 constexpr int kAtomThreads = 256;
 constexpr int kPairTPA = 8;            // threads per atom in the pair passes
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
-constexpr int kOwnCap = 24;            // least own interacting pairs per atom in the compact list
-constexpr int kRevCap = 24;            // least reverse interacting pairs per atom
-constexpr int kMidCap = 40;            // half-list pairs per atom in the intermediate list
+constexpr int kPairCapMin = 24;        // least compact-row entries per atom
+constexpr int kMidCapMin = 48;         // least intermediate-row entries per atom
 constexpr double kFemtosecond = 0.098227;   // the mdloop's "fs" (src/moldin.F90:132), model time units
-constexpr double kMidSkin = 0.9;       // r_mid = table cut + kMidSkin (A), at most rnear
 constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
 constexpr int kFullTPA = 8;            // lanes per atom in the density and force passes
 
@@ -221,11 +230,9 @@ void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
-constexpr int kVariants = 4;           // compiled variants per tunable pass
-void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                   cudaStream_t s);
-int launch_density_full(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                        double *partials, cudaStream_t s);
+constexpr int kVariants = 8;           // compiled variants per tunable pass
+int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
+                          double *partials, cudaStream_t s);
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s);
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,

@@ -3,27 +3,29 @@
 // The reference evaluates every pair of its half list twice per step (rhoset
 // and force, src/dynamics_m.F90:235-346, 524-569).  Only the pairs closer than
 // the last nonzero table node contribute (about 7 of the ~44 listed per atom
-// in bcc Fe at rnear = 6.3 A); the others add exact zeros.  So each step:
+// in bcc Fe at rnear = 6.3 A); the others add exact zeros.  The lists:
 //
-//  k_screen   walks each atom's half-list row, keeps the pairs inside the
-//             table range and writes them into a compact FULL list: j into
-//             i's own list (in row order) and i into j's reverse list (one
-//             int atomic per pair).  Both lists are entry-major like the half
-//             list, so one thread per atom reads contiguous rows.  In FP64 mode an FP32 distance with a
-//             margin that bounds its rounding error pre-selects candidates and
-//             the exact FP64 distance decides, so the kept set equals the set
-//             an all-FP64 test keeps.
-//  k_density  rho_i = sum_j phi(r_ij) over the compact full list (no atomics),
-//             then F(rho_i), F'(rho_i) (embed) and the kinetic stress tk.
-//  k_forces   f_i = sum_j dx_ij fp_ij over the same list (no atomics); energy
-//             and virial take half of every directed pair; the velocity-Verlet
-//             second half (src/quench_m.F90:606-622) is applied in the epilogue.
+//  intermediate  a FULL list (both directions) of the half-list pairs within
+//                r_mid = rcut + skin, rebuilt only when the displacements since
+//                its build could bring an unlisted pair inside the cut;
+//  compact       per step, the FULL list of pairs inside the table cut.
 //
-// Each pair is thus evaluated from both ends (2x the pair arithmetic of a half
-// list) but no floating-point atomic is issued, and all sums for one atom are
-// taken by one group of lanes.  MIXED = true runs distances, tables and pair
-// forces in FP32 (differences of FP64 positions rounded to FP32) and keeps
-// every accumulation, rho, F and F' in FP64.
+// Each step runs two passes, one thread per atom, no floating-point atomics:
+//
+//  k_screen_density  walks the atom's intermediate row, keeps the pairs inside
+//             the cut (exact FP64 distance in FP64 mode; FP32 with an error
+//             margin and an FP64 decision inside the margin in mixed mode),
+//             writes them to its compact row and sums rho_i = sum_j phi(r_ij);
+//             then embed, F'(rho) into pos2.w and the kinetic moment.
+//  k_forces   f_i = sum_j dx_ij fp_ij over the compact row; energy and virial
+//             take half of every directed pair; the velocity-Verlet second
+//             half (src/quench_m.F90:606-622) is applied in the epilogue.
+//
+// Entries carry the pair's direction in the reference's half list in bit 31
+// (set: j is in i's own row), which the per-atom stress of the reference
+// (own rows only) needs.  MIXED = true runs distances, tables and pair forces
+// in FP32 (differences of FP64 positions rounded to FP32) and keeps every
+// accumulation, rho, F and F' in FP64.
 #include "engine.h"
 
 namespace moldy {
@@ -77,176 +79,112 @@ __device__ float screen_radius2(const double *b, double rcull2) {
     return (float)(rs * rs);
 }
 
-// Keeps pair (a, j) iff its distance is inside the table range.  In FP64 mode
-// the FP32 distance decides outright when it is farther than the error bound
-// from the cut (rin2 .. rscreen2 is the only band that needs the FP64 test).
-template <bool MIXED, int B, bool PF>
-__global__ void __launch_bounds__(256)
-k_screen(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
-         const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
-         const int32_t *__restrict__ numn, const int32_t *__restrict__ mlist,
-         const int32_t *__restrict__ mid_cnt, int32_t *__restrict__ alist,
-         int32_t *__restrict__ own_cnt, int32_t *__restrict__ rev_cnt) {
+
+constexpr int32_t kOwnBit = (int32_t)0x80000000u;
+constexpr int32_t kIdMask = 0x7fffffff;
+
+// Keeps pair (a, j) iff its distance is inside the table range, sums rho_a,
+// embeds.  FP64: the exact distance decides.  Mixed: the FP32 distance decides
+// outside the band [rin, rscreen] around the cut, the FP64 one inside it.
+template <bool MIXED, bool EXACT, int B, bool PF, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
+                 double4 *__restrict__ pos2, const BoxState *__restrict__ box, const int32_t *__restrict__ mlist,
+                 const int32_t *__restrict__ mid_cnt, int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
+                 double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
+                 const double *__restrict__ x1, const double *__restrict__ mass,
+                 const int32_t *__restrict__ znum, double *__restrict__ partials, int32_t *__restrict__ flags) {
     __shared__ double sb[9];
     __shared__ float srs2, srin2;
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (MIXED && threadIdx.x == 0) {
         srs2 = screen_radius2(sb, t.rcull2);
-        // inner edge of the band: rcull minus the same error bound
         float rs = sqrtf(srs2), rc = (float)sqrt(t.rcull2);
         float rin = rc - (rs - rc);
         srin2 = (srs2 > 1e37f || rin <= 0.f) ? -1.f : rin * rin;
     }
     __syncthreads();
-    const float rscreen2 = MIXED ? t.rcull2f : srs2;
-    const float rin2 = srin2;
     double b[9];
     float bf[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bf[k] = (float)sb[k]; }
-    const int nm = p.nm;
-    const size_t stride = (size_t)nm;
-    const int astride = gridDim.x * blockDim.x;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += astride) {
-        if (PF && a + astride < nm) {   // next atom of this thread: its rows into L2
-            const int an = a + astride;
-#pragma unroll
-            for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
-            prefetch_l2(&mid_cnt[an]);
-            prefetch_l2(&posf[an]);
-        }
-        // the intermediate row (pairs within r_mid at its build), or the full
-        // half-list row when that row overflowed
-        const int mc = mid_cnt[a];
-        const int n = mc >= 0 ? mc : numn[a];
-        const int32_t *col = (mc >= 0 ? mlist : nlist) + a;
-        const float4 pf = posf[a];
-        int cnt = 0;
-        for (int k0 = 0; k0 < n; k0 += B) {
-            int jj[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (k0 + u < n) ? __ldg(&col[(size_t)(k0 + u) * stride]) : -1;
-            float4 qq[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = __ldg(&posf[jj[u] >= 0 ? jj[u] : a]);
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const int j = jj[u];
-                if (j < 0) continue;
-                float rx, ry, rz, r2, dx, dy, dz;
-                fsep<MIXED>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz,
-                            r2, dx, dy, dz);
-                if (r2 > rscreen2) continue;
-                bool keep = true;
-                if (!MIXED && !(r2 < rin2)) {
-                    const double4 pa = pos[a];
-                    const double4 qd = pos[j];
-                    double ex = pa.x - qd.x, ey = pa.y - qd.y, ez = pa.z - qd.z;
-                    min_image(p.ivol, ex, ey, ez);
-                    double sx = b[0] * ex + b[3] * ey + b[6] * ez;
-                    double sy = b[1] * ex + b[4] * ey + b[7] * ez;
-                    double sz = b[2] * ex + b[5] * ey + b[8] * ez;
-                    keep = (sx * sx + sy * sy + sz * sz) <= t.rcull2;
-                }
-                if (keep) {
-                    if (cnt < p.own_cap) alist[(size_t)cnt * stride + a] = j;
-                    ++cnt;
-                    int rs = atomicAdd(&rev_cnt[j], 1);
-                    if (rs < p.rev_cap) alist[((size_t)p.own_cap + rs) * stride + j] = a;
-                }
-            }
-        }
-        own_cnt[a] = cnt;
-    }
-}
-
-// the compact list of atom a: own entries 0..no-1 then reverse entries
-// 0..nr-1, stored entry-major at (e * nm + a) and ((own_cap + e) * nm + a)
-__device__ __forceinline__ void alist_counts(const Params &p, const int32_t *own_cnt, const int32_t *rev_cnt,
-                                             int a, int &no, int &nr, bool &over) {
-    no = own_cnt[a];
-    nr = rev_cnt[a];
-    over = no > p.own_cap || nr > p.rev_cap;
-    no = no < p.own_cap ? no : p.own_cap;
-    nr = nr < p.rev_cap ? nr : p.rev_cap;
-}
-
-__device__ __forceinline__ size_t alist_index(const Params &p, int e, int no, int a, int nm) {
-    return (size_t)(e < no ? e : p.own_cap + (e - no)) * (size_t)nm + a;
-}
-
-// -------------------------------------------------------------- density --
-// rho_i = sum phi over the compact row; embed; M = sum m x1 x1^T for kinten
-template <bool MIXED, bool EXACT, int B, bool PF>
-__global__ void __launch_bounds__(256)
-k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__restrict__ pos2,
-               const BoxState *__restrict__ box, const int32_t *__restrict__ alist,
-               const int32_t *__restrict__ own_cnt, const int32_t *__restrict__ rev_cnt,
-               double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
-               const double *__restrict__ x1, const double *__restrict__ mass,
-               const int32_t *__restrict__ znum, double *__restrict__ partials,
-               int32_t *__restrict__ flags) {
-    __shared__ double sb[9];
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    __syncthreads();
-    double b[9];
-    float bf[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bf[k] = (float)sb[k]; }
+    const float rscreen2 = MIXED ? srs2 : 0.f, rin2 = MIXED ? srin2 : 0.f;
     double v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = 0.0;
     const int nm = p.nm;
+    const size_t stride = (size_t)nm;
     const int astride = gridDim.x * blockDim.x;
+    int over = 0, over_max = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += astride) {
-        if (PF && a + astride < nm) {
+        if (PF && a + astride < nm) {   // next atom of this thread: its row and data into L2
             const int an = a + astride;
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                prefetch_l2(&alist[(size_t)u * nm + an]);
-                prefetch_l2(&alist[(size_t)(p.own_cap + u) * nm + an]);
-            }
-            prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos[an]);
-            prefetch_l2(&dafrho[an]); prefetch_l2(&mass[an]); prefetch_l2(&znum[an]);
-            prefetch_l2(&x1[an]); prefetch_l2(&x1[nm + an]); prefetch_l2(&x1[2 * nm + an]);
+            for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
+            prefetch_l2(&mid_cnt[an]);
+            prefetch_l2(MIXED ? (const void *)&posf[an] : (const void *)&pos[an]);
+            prefetch_l2(&dafrho[an]); prefetch_l2(&mass[an]);
         }
-        int no, nr;
-        bool over;
-        alist_counts(p, own_cnt, rev_cnt, a, no, nr, over);
-        v[7] += (double)(no + nr);
-        if (over) {
-            atomicExch(&flags[3], 1);
-            atomicMax(&flags[4], max(own_cnt[a], rev_cnt[a]));
-        }
+        const int mc = mid_cnt[a];
+        const int n = mc < p.mid_cap ? mc : p.mid_cap;
         const double4 pa = pos[a];
+        const float4 pf = MIXED ? posf[a] : make_float4(0.f, 0.f, 0.f, 0.f);
         double rho_a = 0.0;
-        const int ne = no + nr;
-        for (int e0 = 0; e0 < ne; e0 += B) {
-            int jj[B];
+        int cnt = 0;
+        for (int k0 = 0; k0 < n; k0 += B) {
+            int ee[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(p, e0 + u, no, a, nm)] : -1;
-            double4 qq[B];
+            for (int u = 0; u < B; ++u) ee[u] = (k0 + u < n) ? __ldg(&mlist[(size_t)(k0 + u) * stride + a]) : -1;
+            if (MIXED) {
+                float4 qq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = pos[jj[u] >= 0 ? jj[u] : a];
+                for (int u = 0; u < B; ++u) qq[u] = __ldg(&posf[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
 #pragma unroll
-            for (int u = 0; u < B; ++u) {
-                if (jj[u] < 0) continue;
-                double dx = pa.x - qq[u].x, dy = pa.y - qq[u].y, dz = pa.z - qq[u].z;
-                if (MIXED) {
-                    float rx, ry, rz, r2, fx, fy, fz;
-                    fsep<true>(bf, p.ivol, (float)dx, (float)dy, (float)dz, rx, ry, rz, r2, fx, fy, fz);
+                for (int u = 0; u < B; ++u) {
+                    if (ee[u] == -1) continue;
+                    float rx, ry, rz, r2, dx, dy, dz;
+                    fsep<true>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz, r2, dx, dy,
+                               dz);
+                    if (r2 > rscreen2) continue;
+                    if (!(r2 < rin2)) {   // inside the error band: the FP64 distance decides
+                        const double4 qd = pos[ee[u] & kIdMask];
+                        double ex = pa.x - qd.x, ey = pa.y - qd.y, ez = pa.z - qd.z;
+                        min_image(p.ivol, ex, ey, ez);
+                        double sx = b[0] * ex + b[3] * ey + b[6] * ez;
+                        double sy = b[1] * ex + b[4] * ey + b[7] * ez;
+                        double sz = b[2] * ex + b[5] * ey + b[8] * ez;
+                        if (!((sx * sx + sy * sy + sz * sz) <= t.rcull2)) continue;
+                    }
                     rho_a += (double)lookup_phif(t, sqrtf(r2));
-                } else {
+                    if (cnt < p.pair_cap) alist[(size_t)cnt * stride + a] = ee[u];
+                    ++cnt;
+                }
+            } else {
+                double4 qq[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) qq[u] = pos[ee[u] != -1 ? (ee[u] & kIdMask) : a];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if (ee[u] == -1) continue;
+                    double dx = pa.x - qq[u].x, dy = pa.y - qq[u].y, dz = pa.z - qq[u].z;
                     min_image(p.ivol, dx, dy, dz);
                     double rx = b[0] * dx + b[3] * dy + b[6] * dz;
                     double ry = b[1] * dx + b[4] * dy + b[7] * dz;
                     double rz = b[2] * dx + b[5] * dy + b[8] * dz;
-                    double r = sqrt(rx * rx + ry * ry + rz * rz);
+                    double r2 = rx * rx + ry * ry + rz * rz;
+                    if (!(r2 <= t.rcull2)) continue;
+                    double r = sqrt(r2);
                     rho_a += EXACT ? fetm_phi(t, r) : lookup_phi(t, r);
+                    if (cnt < p.pair_cap) alist[(size_t)cnt * stride + a] = ee[u];
+                    ++cnt;
                 }
             }
         }
+        pair_cnt[a] = cnt;
+        v[7] += (double)cnt;
+        if (cnt > p.pair_cap) { over = 1; over_max = max(over_max, cnt); }
+        if (mc > p.mid_cap) { over |= 2; over_max = max(over_max, mc); }
         // embed (src/potential_m.F90:148-169): rho <= 1e-40 keeps the old values
         double fd = dafrho[a];
         if (rho_a > 1e-40) {
@@ -266,17 +204,18 @@ k_density_full(Params p, Tables t, const double4 *__restrict__ pos, double4 *__r
             v[4] += m * ux * uy; v[5] += m * ux * uz; v[6] += m * uy * uz;
         }
     }
+    if (over & 1) { atomicExch(&flags[3], 1); atomicMax(&flags[4], over_max); }
+    if (over & 2) { atomicExch(&flags[5], 1); atomicMax(&flags[6], over_max); }
     block_partials<8>(v, partials, 0);
 }
 
 // --------------------------------------------------------------- forces --
 // f_i = sum dx fp over the compact row; pe and the virial moment
 // D = sum d d^T fp / 2 (tp = B0 D); mode 1 adds the velocity-Verlet second half
-template <bool MIXED, bool EXACT, int B, bool PF>
-__global__ void __launch_bounds__(256)
+template <bool MIXED, bool EXACT, int B, bool PF, bool STRESS, int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *__restrict__ box,
-         const int32_t *__restrict__ alist, const int32_t *__restrict__ own_cnt,
-         const int32_t *__restrict__ rev_cnt, const double *__restrict__ mass,
+         const int32_t *__restrict__ alist, const int32_t *__restrict__ pair_cnt, const double *__restrict__ mass,
          const int32_t *__restrict__ znum, const double *__restrict__ del2,
          double *__restrict__ f, double *__restrict__ x1, double *__restrict__ x2,
          double *__restrict__ stress, double *__restrict__ partials, int mode) {
@@ -299,36 +238,30 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
         if (PF && a + astride < nm) {
             const int an = a + astride;
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                prefetch_l2(&alist[(size_t)u * nm + an]);
-                prefetch_l2(&alist[(size_t)(p.own_cap + u) * nm + an]);
-            }
-            prefetch_l2(&own_cnt[an]); prefetch_l2(&rev_cnt[an]); prefetch_l2(&pos2[an]);
-            prefetch_l2(&mass[an]);
+            for (int u = 0; u < 8; ++u) prefetch_l2(&alist[(size_t)u * nm + an]);
+            prefetch_l2(&pair_cnt[an]); prefetch_l2(&pos2[an]); prefetch_l2(&mass[an]);
             if (mode == 1) {
                 prefetch_l2(&x1[an]); prefetch_l2(&x1[nm + an]); prefetch_l2(&x1[2 * nm + an]);
                 prefetch_l2(&x2[an]); prefetch_l2(&x2[nm + an]); prefetch_l2(&x2[2 * nm + an]);
                 prefetch_l2(&del2[an]); prefetch_l2(&znum[an]);
             }
         }
-        int no, nr;
-        bool over;
-        alist_counts(p, own_cnt, rev_cnt, a, no, nr, over);
+        int ne = pair_cnt[a];
+        ne = ne < p.pair_cap ? ne : p.pair_cap;
         const double4 pa = pos2[a];
         const double ma = mass[a];
         double fxa = 0.0, fya = 0.0, fza = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-        const int ne = no + nr;
         for (int e0 = 0; e0 < ne; e0 += B) {
-            int jj[B];
+            int ee[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (e0 + u < ne) ? alist[alist_index(p, e0 + u, no, a, nm)] : -1;
+            for (int u = 0; u < B; ++u) ee[u] = (e0 + u < ne) ? alist[(size_t)(e0 + u) * nm + a] : -1;
             double4 qq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = pos2[jj[u] >= 0 ? jj[u] : a];
+            for (int u = 0; u < B; ++u) qq[u] = pos2[ee[u] != -1 ? (ee[u] & kIdMask) : a];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
-                const int j = jj[u];
-                if (j < 0) continue;
+                if (ee[u] == -1) continue;
+                const int j = ee[u] & kIdMask;
                 const double4 q = qq[u];
                 double dx = pa.x - q.x, dy = pa.y - q.y, dz = pa.z - q.z;
                 double fp, vee, rx, ry, rz;
@@ -358,11 +291,11 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
                     v[1] += dx * dx * fp; v[2] += dy * dy * fp; v[3] += dz * dz * fp;
                     v[4] += dx * dy * fp; v[5] += dx * dz * fp; v[6] += dy * dz * fp;
                 }
-                if (p.atomstress && e0 + u < no) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
+                if (STRESS && (ee[u] & kOwnBit)) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
             }
         }
         f[a] = fxa; f[nm + a] = fya; f[2 * nm + a] = fza;
-        if (p.atomstress) { stress[a] = sx; stress[nm + a] = sy; stress[2 * nm + a] = sz; }
+        if (STRESS) { stress[a] = sx; stress[nm + a] = sy; stress[2 * nm + a] = sz; }
         if (mode == 1) {
             // velocity Verlet second half (src/quench_m.F90:606-622), previous tgid
             double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
@@ -437,6 +370,15 @@ __global__ void k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, 
     }
 }
 
+// The intermediate list is full: every half-list pair within r_mid (FP32
+// distance plus twice its error bound) is entered in both rows, the owner's
+// copy flagged.  Rows are filled through integer atomics on the counts, which
+// k_mid_clear zeroes first; both run only when k_mid_decide asked for a build.
+__global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ mid_cnt) {
+    if (!box->mid_rebuild) return;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) mid_cnt[a] = 0;
+}
+
 __global__ void __launch_bounds__(256)
 k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
@@ -459,13 +401,12 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
 #pragma unroll
     for (int k = 0; k < 9; ++k) bf[k] = (float)sb[k];
     const float keep2 = skeep2;
-    const int nm = p.nm;
+    const int nm = p.nm, cap = p.mid_cap;
     const size_t stride = (size_t)nm;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const int n = numn[a];
         const int32_t *col = nlist + a;
         const float4 pf = posf[a];
-        int cnt = 0;
 #pragma unroll 4
         for (int k = 0; k < n; ++k) {
             const int j = __ldg(&col[(size_t)k * stride]);
@@ -473,11 +414,12 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
             float rx, ry, rz, r2, dx, dy, dz;
             fsep<true>(bf, p.ivol, pf.x - q.x, pf.y - q.y, pf.z - q.z, rx, ry, rz, r2, dx, dy, dz);
             if (r2 <= keep2) {
-                if (cnt < kMidCap) mlist[(size_t)cnt * stride + a] = j;
-                ++cnt;
+                int sa = atomicAdd(&mid_cnt[a], 1);
+                if (sa < cap) mlist[(size_t)sa * stride + a] = j | kOwnBit;
+                int sj = atomicAdd(&mid_cnt[j], 1);
+                if (sj < cap) mlist[(size_t)sj * stride + j] = a;
             }
         }
-        mid_cnt[a] = cnt <= kMidCap ? cnt : -1;
         xbuild[a] = pos[a];
     }
 }
@@ -489,87 +431,82 @@ void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut
 
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
+    k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_cnt);
     k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist,
                                    d.mid_cnt, d.xbuild);
 }
 
 // ------------------------------------------------------------ launchers --
-// Variant v: bit 0 selects the batch of list entries whose gathers are issued
-// before any is used (screen {4, 8}, density and forces {2, 4}); bit 1 adds
-// L2 prefetches of the next atom's rows and per-atom data.
-void launch_screen(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                   cudaStream_t s) {
-    int nb = grid_blocks(p.nm, 256);
-    cudaMemsetAsync(d.rev_cnt, 0, sizeof(int32_t) * p.nm, s);
-#define SCREEN_ARGS p, t, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist, d.mid_cnt, d.alist, \
-                    d.own_cnt, d.rev_cnt
-#define SCREEN(B, PF)                                                                  \
-    do {                                                                               \
-        if (mixed) k_screen<true, B, PF><<<nb, 256, 0, s>>>(SCREEN_ARGS);              \
-        else k_screen<false, B, PF><<<nb, 256, 0, s>>>(SCREEN_ARGS);                   \
-    } while (0)
-    switch (variant) {
-    case 0: SCREEN(4, false); break;
-    case 1: SCREEN(8, false); break;
-    case 2: SCREEN(4, true); break;
-    default: SCREEN(8, true); break;
-    }
-#undef SCREEN
-#undef SCREEN_ARGS
+// Variant v (0..7): bit 0 selects the batch of list entries whose gathers are
+// issued before any is used (screen-density {4, 8}, forces {2, 4}); bit 1 adds
+// L2 prefetches of the next atom's rows and per-atom data; bit 2 asks for 3
+// resident blocks per SM instead of 2 (fewer registers per thread, more warps
+// to hide the gather latency).
+template <int B, bool PF, int MINB>
+static void sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials, int nb,
+                       cudaStream_t s) {
+#define SD_ARGS p, t, d.pos, d.posf, d.pos2, d.box, d.mlist, d.mid_cnt, d.alist, d.pair_cnt, d.rho, d.afrho, \
+                d.dafrho, d.x1, d.mass, d.znum, partials, d.flags
+    if (t.exact) k_screen_density<false, true, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
+    else if (mixed) k_screen_density<true, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
+    else k_screen_density<false, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
+#undef SD_ARGS
 }
 
-int launch_density_full(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                        double *partials, cudaStream_t s) {
+int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
+                          double *partials, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
-#define DENSITY_ARGS p, t, d.pos, d.pos2, d.box, d.alist, d.own_cnt, d.rev_cnt, d.rho, d.afrho, \
-                     d.dafrho, d.x1, d.mass, d.znum, partials, d.flags
-#define DENSITY(B, PF)                                                                          \
-    do {                                                                                        \
-        if (t.exact) k_density_full<false, true, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);       \
-        else if (mixed) k_density_full<true, false, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);    \
-        else k_density_full<false, false, B, PF><<<nb, 256, 0, s>>>(DENSITY_ARGS);              \
-    } while (0)
     switch (variant) {
-    case 0: DENSITY(2, false); break;
-    case 1: DENSITY(4, false); break;
-    case 2: DENSITY(2, true); break;
-    default: DENSITY(4, true); break;
+    case 0: sd_variant<4, false, 2>(d, p, t, mixed, partials, nb, s); break;
+    case 1: sd_variant<8, false, 2>(d, p, t, mixed, partials, nb, s); break;
+    case 2: sd_variant<4, true, 2>(d, p, t, mixed, partials, nb, s); break;
+    case 3: sd_variant<8, true, 2>(d, p, t, mixed, partials, nb, s); break;
+    case 4: sd_variant<4, false, 3>(d, p, t, mixed, partials, nb, s); break;
+    case 5: sd_variant<8, false, 3>(d, p, t, mixed, partials, nb, s); break;
+    case 6: sd_variant<4, true, 3>(d, p, t, mixed, partials, nb, s); break;
+    default: sd_variant<8, true, 3>(d, p, t, mixed, partials, nb, s); break;
     }
-#undef DENSITY
-#undef DENSITY_ARGS
     return nb;
+}
+
+template <int B, bool PF, bool STRESS, int MINB>
+static void forces_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode, double *partials,
+                           int nb, cudaStream_t s) {
+#define FORCE_ARGS p, t, d.pos2, d.box, d.alist, d.pair_cnt, d.mass, d.znum, d.del2, d.f, d.x1, d.x2, d.stress, \
+                   partials, mode
+    if (t.exact) k_forces<false, true, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
+    else if (mixed) k_forces<true, false, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
+    else k_forces<false, false, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
+#undef FORCE_ARGS
 }
 
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
-#define FORCE_ARGS p, t, d.pos2, d.box, d.alist, d.own_cnt, d.rev_cnt, d.mass, d.znum, d.del2, d.f, \
-                   d.x1, d.x2, d.stress, partials, mode
-#define FORCES(B, PF)                                                                        \
-    do {                                                                                     \
-        if (t.exact) k_forces<false, true, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);            \
-        else if (mixed) k_forces<true, false, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);         \
-        else k_forces<false, false, B, PF><<<nb, 256, 0, s>>>(FORCE_ARGS);                   \
-    } while (0)
-    switch (variant) {
-    case 0: FORCES(2, false); break;
-    case 1: FORCES(4, false); break;
-    case 2: FORCES(2, true); break;
-    default: FORCES(4, true); break;
+    if (p.atomstress) {
+        forces_variant<2, false, true, 2>(d, p, t, mixed, mode, partials, nb, s);
+        return nb;
     }
-#undef FORCES
-#undef FORCE_ARGS
+    switch (variant) {
+    case 0: forces_variant<2, false, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 1: forces_variant<4, false, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 2: forces_variant<2, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 3: forces_variant<4, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 4: forces_variant<2, false, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 5: forces_variant<4, false, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 6: forces_variant<2, true, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
+    default: forces_variant<4, true, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
+    }
     return nb;
 }
 
-// list entries the screening pass reads per step: the intermediate row, or
-// the half-list row of an atom whose intermediate row overflowed
+// list entries the screening pass reads per step (the full intermediate rows)
 __global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_cnt, const int32_t *__restrict__ numn,
                                  unsigned long long *__restrict__ out) {
     unsigned long long s = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         int mc = mid_cnt[a];
-        s += (unsigned long long)(mc >= 0 ? mc : numn[a]);
+        s += (unsigned long long)mc;
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(out, s);

@@ -351,16 +351,15 @@ class MoldySystem:
         check(self._L.moldy_gpu_reset_kernel_stats(self._h))
 
     def autotune(self, nreps: int = 5) -> dict:
-        """Times each compiled variant of the screening, density and force
+        """Times each compiled variant of the screening-density and force
         passes on the current configuration and keeps the fastest."""
         import numpy as _np
         t = _np.zeros(3 * _lib.TUNE_VARIANTS)
         ch = _np.zeros(3, dtype=_np.int32)
         check(self._L.moldy_gpu_autotune(self._h, int(nreps), _dp(t), _ip(ch)))
-        names = ("screen", "density", "forces")
-        return {"chosen": dict(zip(names, ch.tolist())),
-                "ms": {n: t[k * _lib.TUNE_VARIANTS:(k + 1) * _lib.TUNE_VARIANTS].tolist()
-                       for k, n in enumerate(names)}}
+        nv = _lib.TUNE_VARIANTS
+        return {"chosen": {"screen_density": int(ch[0]), "forces": int(ch[2])},
+                "ms": {"screen_density": t[0:nv].tolist(), "forces": t[2 * nv:3 * nv].tolist()}}
 
     def list_stats(self) -> dict:
         """Directed interacting pairs of the last force evaluation, the number
@@ -372,6 +371,10 @@ class MoldySystem:
 
     def pair_count(self) -> float:
         return self.list_stats()["pairs"]
+
+    def set_mid_skin(self, skin: float):
+        """Skin (A) of the intermediate list; a tuning knob, results unchanged."""
+        check(self._L.moldy_gpu_set_mid_skin(self._h, float(skin)))
 
     def set_variants(self, screen: int, density: int, forces: int):
         check(self._L.moldy_gpu_set_variants(self._h, int(screen), int(density), int(forces)))

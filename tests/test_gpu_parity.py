@@ -237,14 +237,14 @@ def test_kernel_variants_agree_and_autotune(oracle_mod, gpu_lib):
     g = MoldySystem.from_workload(w)
     g.force()
     f0 = g.forces()
-    for v in range(4):
-        g.set_variants(v, v, v)
+    for v in range(8):
+        g.set_variants(v, 0, v)
         g.force()
         assert rel_norm_err(g.forces(), f0) < 1e-13
     s0 = g.get_state()
     tune = g.autotune(nreps=2)
-    assert set(tune["chosen"]) == {"screen", "density", "forces"}
-    assert all(0 <= v < 4 for v in tune["chosen"].values())
+    assert set(tune["chosen"]) == {"screen_density", "forces"}
+    assert all(0 <= v < 8 for v in tune["chosen"].values())
     s1 = g.get_state()
     for k in ("x0", "x1", "x2", "b0", "b1"):
         assert np.array_equal(s0[k], s1[k]), k
@@ -330,3 +330,24 @@ def test_strainloops_ramp(gpu_lib):
     assert recs[-1]["temprq"] == 1100.0
     assert np.mean([r["temp"] for r in recs[-20:]]) > np.mean([r["temp"] for r in recs[:20]]) + 100.0
     s.close()
+
+
+def test_mid_skin_changes_no_result(gpu_lib):
+    """The intermediate-list skin is a tuning knob: a thin skin (frequent
+    device-decided rebuilds) and the default give the same trajectory."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(10, sigma=0.05, temperature=1500.0, ivol=0, seed=8, nbrupdate=50)
+    runs = []
+    for skin in (0.9, 0.25):
+        s = MoldySystem.from_workload(w)
+        s.set_mid_skin(skin)
+        s.linkup()
+        s.md_init()
+        th = s.md_steps(80)
+        runs.append((th, s.list_stats()["mid_builds"]))
+        s.close()
+    (a, na), (b, nb) = runs
+    assert nb > na                       # the thin skin was rebuilt more often
+    for k in (0, 40, 79):
+        for key in ("pe", "ke", "th"):
+            assert abs(a[k][key] - b[k][key]) <= 1e-10 * abs(a[k][key]), (k, key)
