@@ -273,7 +273,7 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     stream = torch.cuda.ExternalStream(sysm.stream_handle(), device=local_rank)
     # untimed: the intermediate-list skin that gives the shortest steps here
     skin_ms = {}
-    for skin in (0.3, 0.45, 0.6, 0.9):
+    for skin in (0.2, 0.3, 0.45, 0.9):
         sysm.set_mid_skin(skin)
         sysm.md_steps(20, thermo=False)
         t0 = time.perf_counter()

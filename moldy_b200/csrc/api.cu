@@ -169,7 +169,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
-                    d.pair_cnt, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.mlist, d.mid_own, d.mid_rev, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -233,9 +233,10 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.alist, nm * (size_t)p.pair_cap, "compact list"));
     CHECK(dev_alloc(&d.pair_cnt, nm, "pair_cnt"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
-    CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
+    CHECK(dev_alloc(&d.mid_own, nm, "mid_own"));
+    CHECK(dev_alloc(&d.mid_rev, nm, "mid_rev"));
     CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
-    CHECK(dev_alloc(&d.partials, 2 * (size_t)kMaxBlocks * kPartials, "partials"));
+    CHECK(dev_alloc(&d.partials, 3 * (size_t)kMaxBlocks * kPartials, "partials"));
     CHECK(dev_alloc(&d.flags, 8, "flags"));
     CHECK(dev_alloc(&d.box, 1, "box"));
     CUDA_CHECK(cudaMemset(d.pos, 0, nm * sizeof(double4)), "memset pos");
@@ -250,7 +251,8 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.posf, 0, nm * sizeof(float4)), "memset posf");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
     CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
-    CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
+    CUDA_CHECK(cudaMemset(d.mid_own, 0, nm * sizeof(int32_t)), "memset mid_own");
+    CUDA_CHECK(cudaMemset(d.mid_rev, 0, nm * sizeof(int32_t)), "memset mid_rev");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(double4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
@@ -607,11 +609,14 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, s));
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
+    double *pk = d.partials + 2 * (size_t)kMaxBlocks * kPartials;
     int nbe = 0, nbf = 0;
+    // kinten's moment: taken by the drift kernel in velocity Verlet
+    if (mode != 1) LAUNCH(E, K_DRIFT, 1, s, E.kin_blocks = launch_kinetic(d, p, pk, s));
     LAUNCH(E, K_SCREEN, 1, s, nbe = launch_screen_density(d, p, E.tab, mixed, E.variant[K_SCREEN], pe, s));
     LAUNCH(E, K_PAIR, 1, s,
            nbf = launch_forces(d, p, E.tab, mixed, mode == 1 ? 1 : 0, E.variant[K_PAIR], pf, s));
-    LAUNCH(E, K_FINALIZE, 1, s, launch_finalize_force(d, p, pe, nbe, pf, nbf, mode, s));
+    LAUNCH(E, K_FINALIZE, 1, s, launch_finalize_force(d, p, pe, nbe, pf, nbf, pk, E.kin_blocks, mode, s));
     if (rebuilt) *rebuilt = rb;
     return MOLDY_OK;
 }
@@ -700,7 +705,8 @@ int Engine::ensure_active_capacity(int min_pair, int min_mid) {
 int Engine::velocityverlet(moldy_force_out *out) {
     CHECK(check_ready());
     bool rb = false;
-    LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
+    LAUNCH(*this, K_DRIFT, 1, stream_,
+               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, stream_));
     CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
     CHECK(fetch_force_out(out));
     if (out) out->rebuilt = rb ? 1 : 0;
@@ -746,7 +752,8 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
     std::vector<int> ntcs(nsteps), rbs(nsteps);
     for (int k = 0; k < nsteps; ++k) {
         bool rb = false;
-        LAUNCH(*this, K_DRIFT, 1, stream_, launch_drift(d, prm, stream_));
+        LAUNCH(*this, K_DRIFT, 1, stream_,
+               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, stream_));
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
         int nb = 0;
         LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));

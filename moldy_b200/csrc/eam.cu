@@ -33,19 +33,21 @@ __device__ void reduce_partials(const double *__restrict__ part, int nblk, doubl
 // mode 0: force only; 1: velocity Verlet second half (box); 2: md_init
 __global__ void __launch_bounds__(256)
 k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
-                 int nblk_embed, const double *__restrict__ part_force, int nblk_force, int mode) {
-    __shared__ double se[8], sf[7];
-    reduce_partials<8>(part_embed, nblk_embed, se);
+                 int nblk_embed, const double *__restrict__ part_force, int nblk_force,
+                 const double *__restrict__ part_kin, int nblk_kin, int mode) {
+    __shared__ double se[2], sf[7], sk[6];
+    reduce_partials<2>(part_embed, nblk_embed, se);
     reduce_partials<7>(part_force, nblk_force, sf);
+    reduce_partials<6>(part_kin, nblk_kin, sk);
     if (threadIdx.x != 0) return;
     BoxState &B = *box;
     B.pe_emb = se[0];
     B.pe_pair = sf[0];
     B.pe = se[0] + sf[0];
-    B.npairs = se[7];
+    B.npairs = se[1];
     // symmetric moments (xx, yy, zz, xy, xz, yz) -> full 3x3
     double M[9], D[9];
-    M[0] = se[1]; M[4] = se[2]; M[8] = se[3]; M[3] = M[1] = se[4]; M[6] = M[2] = se[5]; M[7] = M[5] = se[6];
+    M[0] = sk[0]; M[4] = sk[1]; M[8] = sk[2]; M[3] = M[1] = sk[3]; M[6] = M[2] = sk[4]; M[7] = M[5] = sk[5];
     D[0] = sf[1]; D[4] = sf[2]; D[8] = sf[3]; D[3] = D[1] = sf[4]; D[6] = D[2] = sf[5]; D[7] = D[5] = sf[6];
     double dt2 = p.deltat * p.deltat;
     mat_mul(B.b0, D, B.tp);                       // tp(a,b) = sum r_a d_b fp, r = B0 d
@@ -79,8 +81,33 @@ k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict_
 }
 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
-                           const double *part_force, int nblk_force, int mode, cudaStream_t s) {
-    k_finalize_force<<<1, 256, 0, s>>>(p, d.box, part_embed, nblk_embed, part_force, nblk_force, mode);
+                           const double *part_force, int nblk_force, const double *part_kin, int nblk_kin,
+                           int mode, cudaStream_t s) {
+    k_finalize_force<<<1, 256, 0, s>>>(p, d.box, part_embed, nblk_embed, part_force, nblk_force, part_kin, nblk_kin,
+                                        mode);
+}
+
+// kinten's moment M = sum m x1 x1^T over atoms with a species
+// (src/thermostat_m.F90:138-157); tk = B0 M / dt^2 in k_finalize_force
+__device__ __forceinline__ void kin_moment(double (&v)[6], double m, double ux, double uy, double uz) {
+    v[0] += m * ux * ux; v[1] += m * uy * uy; v[2] += m * uz * uz;
+    v[3] += m * ux * uy; v[4] += m * ux * uz; v[5] += m * uy * uz;
+}
+
+__global__ void __launch_bounds__(256)
+k_kinetic(Params p, const double *__restrict__ x1, const double *__restrict__ mass,
+          const int32_t *__restrict__ znum, double *__restrict__ partials) {
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int nm = p.nm;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x)
+        if (znum[a] != 0) kin_moment(v, mass[a], x1[a], x1[nm + a], x1[2 * nm + a]);
+    block_partials<6>(v, partials, 0);
+}
+
+int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s) {
+    int nb = grid_blocks(p.nm, kAtomThreads);
+    k_kinetic<<<nb, kAtomThreads, 0, s>>>(p, d.x1, d.mass, d.znum, partials);
+    return nb;
 }
 
 // ------------------------------------------------------------- integrator --
@@ -90,7 +117,8 @@ void launch_finalize_force(DeviceState &d, const Params &p, const double *part_e
 __global__ void __launch_bounds__(256)
 k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
-        const double4 *__restrict__ xbuild) {
+        const double4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
+        double *__restrict__ kin_partials) {
     // every thread forms the post-drift box exactly as thread 0 stores it
     __shared__ double nb[9];
     if (threadIdx.x == 0) {
@@ -108,14 +136,15 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         for (int k = 0; k < 9; ++k) nb[k] = b0[k];
     }
     __syncthreads();
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
     double d2 = 0.0;
-    if (a < p.nm) {
-        const int nm = p.nm;
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int nm = p.nm;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        const double ex = x1[a], ey = x1[nm + a], ez = x1[2 * nm + a];
         double4 q = pos[a];
-        q.x = q.x + (x1[a] + x2[a]);
-        q.y = q.y + (x1[nm + a] + x2[nm + a]);
-        q.z = q.z + (x1[2 * nm + a] + x2[2 * nm + a]);
+        q.x = q.x + (ex + x2[a]);
+        q.y = q.y + (ey + x2[nm + a]);
+        q.z = q.z + (ez + x2[2 * nm + a]);
         pos[a] = q;
         posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
         double4 xb = xbuild[a];
@@ -123,8 +152,12 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         double rx = nb[0] * ux + nb[3] * uy + nb[6] * uz;
         double ry = nb[1] * ux + nb[4] * uy + nb[7] * uz;
         double rz = nb[2] * ux + nb[5] * uy + nb[8] * uz;
-        d2 = rx * rx + ry * ry + rz * rz;
+        d2 = fmax(d2, rx * rx + ry * ry + rz * rz);
+        // x1 is not changed by this half of the step: the kinetic moment of
+        // the coming force evaluation can be taken here
+        if (znum[a] != 0) kin_moment(v, mass[a], ex, ey, ez);
     }
+    block_partials<6>(v, kin_partials, 0);
     // block maximum, then one atomic per block (non-negative doubles order as their bits)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
@@ -140,9 +173,10 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
     // here can read a box another block has already moved
 }
 
-void launch_drift(DeviceState &d, const Params &p, cudaStream_t s) {
-    int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
-    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild);
+int launch_drift(DeviceState &d, const Params &p, double *kin_partials, cudaStream_t s) {
+    int nb = grid_blocks(p.nm, kAtomThreads);
+    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum, kin_partials);
+    return nb;
 }
 
 // moldin strain-loop preparation (src/moldin.F90:458-471): every atom with a

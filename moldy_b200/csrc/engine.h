@@ -47,7 +47,9 @@ struct DeviceState {
     // intermediate FULL list (half-list pairs within r_mid when built, entered
     // in both rows, bit 31 on the owner's copy), entry-major; xbuild holds the
     // positions at build time
-    int32_t *mlist = nullptr, *mid_cnt = nullptr;
+    // row of atom i: own entries in slots 0 .. mid_own[i]-1, reverse entries
+    // from the last slot down (mid_rev[i] of them)
+    int32_t *mlist = nullptr, *mid_own = nullptr, *mid_rev = nullptr;
     double4 *xbuild = nullptr;
     // tables
     double4 *tab_r4 = nullptr;
@@ -197,6 +199,9 @@ class Engine {
     double thermotimer_ = 0.0;      // time since the last scalev (the mdloop's thermotimer)
     int active_overflow_ = 0;       // largest compact row of an overflowing evaluation
     int mid_overflow_ = 0;          // largest intermediate row of an overflowing build
+  public:
+    int kin_blocks = 0;             // blocks whose kinetic-moment partials the last drift wrote
+  private:
     bool mid_dirty_ = true;         // the intermediate list must be rebuilt before use
   public:
     bool mid_dirty() const { return mid_dirty_; }
@@ -236,8 +241,10 @@ int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s);
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
-                           const double *part_force, int nblk_force, int mode, cudaStream_t s);
-void launch_drift(DeviceState &d, const Params &p, cudaStream_t s);
+                           const double *part_force, int nblk_force, const double *part_kin, int nblk_kin,
+                           int mode, cudaStream_t s);
+int launch_drift(DeviceState &d, const Params &p, double *kin_partials, cudaStream_t s);
+int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s);
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
                        int apply_box, cudaStream_t s);
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s);

@@ -16,7 +16,8 @@
 //             the cut (exact FP64 distance in FP64 mode; FP32 with an error
 //             margin and an FP64 decision inside the margin in mixed mode),
 //             writes them to its compact row and sums rho_i = sum_j phi(r_ij);
-//             then embed, F'(rho) into pos2.w and the kinetic moment.
+//             then embed and F'(rho) into pos2.w.  (The kinetic moment of
+//             kinten is taken by the drift kernel, or k_kinetic outside MD.)
 //  k_forces   f_i = sum_j dx_ij fp_ij over the compact row; energy and virial
 //             take half of every directed pair; the velocity-Verlet second
 //             half (src/quench_m.F90:606-622) is applied in the epilogue.
@@ -83,6 +84,20 @@ __device__ float screen_radius2(const double *b, double rcull2) {
 constexpr int32_t kOwnBit = (int32_t)0x80000000u;
 constexpr int32_t kIdMask = 0x7fffffff;
 
+// The exact FP64 test r^2 <= rcull^2 for a pair whose FP32 distance lies in
+// the error band around the cut (rare: kept out of line, so its registers do
+// not count against the screening loop)
+__device__ __noinline__ bool inside_cut_fp64(const double4 *__restrict__ pos, int a, int j, const double *b,
+                                             int ivol, double rcull2) {
+    const double4 pa = pos[a], qd = pos[j];
+    double ex = pa.x - qd.x, ey = pa.y - qd.y, ez = pa.z - qd.z;
+    min_image(ivol, ex, ey, ez);
+    double sx = b[0] * ex + b[3] * ey + b[6] * ez;
+    double sy = b[1] * ex + b[4] * ey + b[7] * ez;
+    double sz = b[2] * ex + b[5] * ey + b[8] * ez;
+    return (sx * sx + sy * sy + sz * sz) <= rcull2;
+}
+
 // Keeps pair (a, j) iff its distance is inside the table range, sums rho_a,
 // embeds.  FP64: the exact distance decides.  Mixed: the FP32 distance decides
 // outside the band [rin, rscreen] around the cut, the FP64 one inside it.
@@ -90,10 +105,10 @@ template <bool MIXED, bool EXACT, int B, bool PF, int MINB>
 __global__ void __launch_bounds__(256, MINB)
 k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
                  double4 *__restrict__ pos2, const BoxState *__restrict__ box, const int32_t *__restrict__ mlist,
-                 const int32_t *__restrict__ mid_cnt, int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
+                 const int32_t *__restrict__ mid_own, const int32_t *__restrict__ mid_rev,
+                 int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
                  double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
-                 const double *__restrict__ x1, const double *__restrict__ mass,
-                 const int32_t *__restrict__ znum, double *__restrict__ partials, int32_t *__restrict__ flags) {
+                 double *__restrict__ partials, int32_t *__restrict__ flags) {
     __shared__ double sb[9];
     __shared__ float srs2, srin2;
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
@@ -108,11 +123,9 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
     double b[9];
     float bf[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bf[k] = (float)sb[k]; }
+    for (int k = 0; k < 9; ++k) { b[k] = MIXED ? 0.0 : sb[k]; bf[k] = (float)sb[k]; }
     const float rscreen2 = MIXED ? srs2 : 0.f, rin2 = MIXED ? srin2 : 0.f;
-    double v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = 0.0;
+    double v[2] = {0.0, 0.0};   // embedding energy, directed pairs
     const int nm = p.nm;
     const size_t stride = (size_t)nm;
     const int astride = gridDim.x * blockDim.x;
@@ -122,20 +135,25 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
             const int an = a + astride;
 #pragma unroll
             for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
-            prefetch_l2(&mid_cnt[an]);
+            prefetch_l2(&mid_own[an]); prefetch_l2(&mid_rev[an]);
             prefetch_l2(MIXED ? (const void *)&posf[an] : (const void *)&pos[an]);
-            prefetch_l2(&dafrho[an]); prefetch_l2(&mass[an]);
+            prefetch_l2(&dafrho[an]);
         }
-        const int mc = mid_cnt[a];
+        const int n_own = mid_own[a];
+        const int mc = n_own + mid_rev[a];
         const int n = mc < p.mid_cap ? mc : p.mid_cap;
-        const double4 pa = pos[a];
+        const int rev_base = p.mid_cap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
+        const double4 pa = MIXED ? make_double4(0.0, 0.0, 0.0, 0.0) : pos[a];
         const float4 pf = MIXED ? posf[a] : make_float4(0.f, 0.f, 0.f, 0.f);
         double rho_a = 0.0;
         int cnt = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
             int ee[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) ee[u] = (k0 + u < n) ? __ldg(&mlist[(size_t)(k0 + u) * stride + a]) : -1;
+            for (int u = 0; u < B; ++u) {
+                const int k = k0 + u;
+                ee[u] = (k < n) ? __ldg(&mlist[(size_t)(k < n_own ? k : rev_base - k) * stride + a]) : -1;
+            }
             if (MIXED) {
                 float4 qq[B];
 #pragma unroll
@@ -147,15 +165,8 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
                     fsep<true>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz, r2, dx, dy,
                                dz);
                     if (r2 > rscreen2) continue;
-                    if (!(r2 < rin2)) {   // inside the error band: the FP64 distance decides
-                        const double4 qd = pos[ee[u] & kIdMask];
-                        double ex = pa.x - qd.x, ey = pa.y - qd.y, ez = pa.z - qd.z;
-                        min_image(p.ivol, ex, ey, ez);
-                        double sx = b[0] * ex + b[3] * ey + b[6] * ez;
-                        double sy = b[1] * ex + b[4] * ey + b[7] * ez;
-                        double sz = b[2] * ex + b[5] * ey + b[8] * ez;
-                        if (!((sx * sx + sy * sy + sz * sz) <= t.rcull2)) continue;
-                    }
+                    // inside the error band: the FP64 distance decides
+                    if (!(r2 < rin2) && !inside_cut_fp64(pos, a, ee[u] & kIdMask, sb, p.ivol, t.rcull2)) continue;
                     rho_a += (double)lookup_phif(t, sqrtf(r2));
                     if (cnt < p.pair_cap) alist[(size_t)cnt * stride + a] = ee[u];
                     ++cnt;
@@ -182,7 +193,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
             }
         }
         pair_cnt[a] = cnt;
-        v[7] += (double)cnt;
+        v[1] += (double)cnt;
         if (cnt > p.pair_cap) { over = 1; over_max = max(over_max, cnt); }
         if (mc > p.mid_cap) { over |= 2; over_max = max(over_max, mc); }
         // embed (src/potential_m.F90:148-169): rho <= 1e-40 keeps the old values
@@ -195,18 +206,12 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
             v[0] += e.x;
         }
         rho[a] = rho_a;
-        pos2[a] = make_double4(pa.x, pa.y, pa.z, fd);
-        // kinten (src/thermostat_m.F90:138-157) as tk = B0 M / dt^2, M = sum m x1 x1^T
-        if (znum[a] != 0) {
-            double m = mass[a];
-            double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
-            v[1] += m * ux * ux; v[2] += m * uy * uy; v[3] += m * uz * uz;
-            v[4] += m * ux * uy; v[5] += m * ux * uz; v[6] += m * uy * uz;
-        }
+        const double4 pw = MIXED ? pos[a] : pa;
+        pos2[a] = make_double4(pw.x, pw.y, pw.z, fd);
     }
     if (over & 1) { atomicExch(&flags[3], 1); atomicMax(&flags[4], over_max); }
     if (over & 2) { atomicExch(&flags[5], 1); atomicMax(&flags[6], over_max); }
-    block_partials<8>(v, partials, 0);
+    block_partials<2>(v, partials, 0);
 }
 
 // --------------------------------------------------------------- forces --
@@ -371,19 +376,22 @@ __global__ void k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, 
 }
 
 // The intermediate list is full: every half-list pair within r_mid (FP32
-// distance plus twice its error bound) is entered in both rows, the owner's
-// copy flagged.  Rows are filled through integer atomics on the counts, which
-// k_mid_clear zeroes first; both run only when k_mid_decide asked for a build.
-__global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ mid_cnt) {
+// distance plus twice its error bound) is entered in both rows.  The owner
+// writes its own entries from the first slot with a local count (flagged in
+// bit 31); the partner's copy goes from the last slot down through a returned
+// integer atomic on mid_rev, which k_mid_clear zeroes first.  Both run only
+// when k_mid_decide asked for a build.
+__global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ mid_rev) {
     if (!box->mid_rebuild) return;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) mid_cnt[a] = 0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) mid_rev[a] = 0;
 }
 
 __global__ void __launch_bounds__(256)
 k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
             const int32_t *__restrict__ numn, int32_t *__restrict__ mlist,
-            int32_t *__restrict__ mid_cnt, double4 *__restrict__ xbuild) {
+            int32_t *__restrict__ mid_own, int32_t *__restrict__ mid_rev, double4 *__restrict__ xbuild) {
+    constexpr int B = 8;
     __shared__ double sb[9];
     __shared__ float skeep2;
     __shared__ int sneed;
@@ -407,19 +415,31 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
         const int n = numn[a];
         const int32_t *col = nlist + a;
         const float4 pf = posf[a];
-#pragma unroll 4
-        for (int k = 0; k < n; ++k) {
-            const int j = __ldg(&col[(size_t)k * stride]);
-            const float4 q = __ldg(&posf[j]);
-            float rx, ry, rz, r2, dx, dy, dz;
-            fsep<true>(bf, p.ivol, pf.x - q.x, pf.y - q.y, pf.z - q.z, rx, ry, rz, r2, dx, dy, dz);
-            if (r2 <= keep2) {
-                int sa = atomicAdd(&mid_cnt[a], 1);
-                if (sa < cap) mlist[(size_t)sa * stride + a] = j | kOwnBit;
-                int sj = atomicAdd(&mid_cnt[j], 1);
-                if (sj < cap) mlist[(size_t)sj * stride + j] = a;
+        int own = 0;
+        for (int k0 = 0; k0 < n; k0 += B) {
+            int jj[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) jj[u] = (k0 + u < n) ? __ldg(&col[(size_t)(k0 + u) * stride]) : -1;
+            float4 qq[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) qq[u] = __ldg(&posf[jj[u] >= 0 ? jj[u] : a]);
+            int slot[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                slot[u] = -1;
+                if (jj[u] < 0) continue;
+                float rx, ry, rz, r2, dx, dy, dz;
+                fsep<true>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz, r2, dx, dy, dz);
+                if (!(r2 <= keep2)) { jj[u] = -1; continue; }
+                if (own < cap) mlist[(size_t)own * stride + a] = jj[u] | kOwnBit;
+                ++own;
+                slot[u] = atomicAdd(&mid_rev[jj[u]], 1);   // issued together, used below
             }
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (slot[u] >= 0 && slot[u] < cap) mlist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
         }
+        mid_own[a] = own;
         xbuild[a] = pos[a];
     }
 }
@@ -431,9 +451,9 @@ void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut
 
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
-    k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_cnt);
+    k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_rev);
     k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist,
-                                   d.mid_cnt, d.xbuild);
+                                   d.mid_own, d.mid_rev, d.xbuild);
 }
 
 // ------------------------------------------------------------ launchers --
@@ -445,8 +465,8 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t
 template <int B, bool PF, int MINB>
 static void sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials, int nb,
                        cudaStream_t s) {
-#define SD_ARGS p, t, d.pos, d.posf, d.pos2, d.box, d.mlist, d.mid_cnt, d.alist, d.pair_cnt, d.rho, d.afrho, \
-                d.dafrho, d.x1, d.mass, d.znum, partials, d.flags
+#define SD_ARGS p, t, d.pos, d.posf, d.pos2, d.box, d.mlist, d.mid_own, d.mid_rev, d.alist, d.pair_cnt, d.rho, d.afrho, \
+                d.dafrho, partials, d.flags
     if (t.exact) k_screen_density<false, true, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
     else if (mixed) k_screen_density<true, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
     else k_screen_density<false, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
@@ -501,12 +521,11 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
 }
 
 // list entries the screening pass reads per step (the full intermediate rows)
-__global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_cnt, const int32_t *__restrict__ numn,
+__global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_own, const int32_t *__restrict__ mid_rev,
                                  unsigned long long *__restrict__ out) {
     unsigned long long s = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        int mc = mid_cnt[a];
-        s += (unsigned long long)mc;
+        s += (unsigned long long)(mid_own[a] + mid_rev[a]);
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
@@ -514,7 +533,7 @@ __global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_cnt, co
 
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s) {
     cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
-    k_count_screened<<<grid_blocks(p.nm, kAtomThreads), kAtomThreads, 0, s>>>(p.nm, d.mid_cnt, d.numn, out);
+    k_count_screened<<<grid_blocks(p.nm, kAtomThreads), kAtomThreads, 0, s>>>(p.nm, d.mid_own, d.mid_rev, out);
 }
 
 }  // namespace moldy
