@@ -192,11 +192,15 @@ __global__ void k_bin_sort(int ncell, const int32_t *__restrict__ cell_start, in
 }
 
 // ------------------------------------------------------------ tile passes --
-// rho_i (rhoset), then F and F' (embed, src/potential_m.F90:148-169)
+// The tile screen finds, for every home atom of a cell, the candidates
+// inside the cut and writes their cell-order slots into the atom's compact
+// row (entry-major, alist[e * ntot + slot]) in candidate order.  LPH lanes
+// serve one home atom: they test LPH candidates at a time and place the hits
+// with one warp ballot, so no lane waits on another's pair arithmetic.
 template <int LPH>
 __global__ void __launch_bounds__(32 * kTileWarps)
-k_tile_density(TileArgs a, Tables t, double *__restrict__ sfp, double *__restrict__ rho_out,
-               double *__restrict__ afrho_out, double *__restrict__ fp_out) {
+k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, int32_t *__restrict__ cnt_out,
+              int32_t *__restrict__ flags) {
     __shared__ double4 tpos[kTileWarps][kTileCap];
     __shared__ int tidx[kTileWarps][kTileCap];
     __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
@@ -212,117 +216,144 @@ k_tile_density(TileArgs a, Tables t, double *__restrict__ sfp, double *__restric
     for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
     const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
     const int g = lane / LPH, gl = lane % LPH;
+    const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
+    const unsigned below = (1u << lane) - 1u;
+    int overflow = 0;
     for (int hb = h0; hb < h1; hb += 32 / LPH) {
         const int hs = hb + g;
-        double rho = 0.0;
-        if (hs < h1) {
-            const double4 ph = a.spos[hs];
-            for (int k = gl; k < total; k += LPH) {
-                double4 p; double fpk; int slot;
+        const bool live = hs < h1;
+        const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
+        int cnt = 0;
+        // every lane of the warp runs the same number of rounds (ballots are warp-wide)
+        for (int k0 = 0; k0 < total; k0 += LPH) {
+            const int k = k0 + gl;
+            bool hit = false;
+            int slot = -1;
+            if (live && k < total) {
+                double4 p; double fpk;
                 candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
-                if (slot == hs) continue;
-                double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-                dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-                double ux, uy, uz;
-                pair_u(b, dx, dy, dz, ux, uy, uz);
-                double r2 = ux * ux + uy * uy + uz * uz;
-                if (r2 >= a.rc2) continue;
-                rho += density_func(t, sqrt(r2));
+                if (slot != hs) {
+                    double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                    double ux, uy, uz;
+                    pair_u(b, dx, dy, dz, ux, uy, uz);
+                    hit = (ux * ux + uy * uy + uz * uz) < a.rc2;
+                }
             }
-        }
-        rho = group_sum<LPH>(rho);
-        if (hs < h1 && gl == 0) {
-            double f = 0.0, fd = 0.0;
-            if (rho > 1e-40) {
-                double2 e = embed_funcs(t, rho);
-                f = e.x; fd = e.y;
+            const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
+            if (hit) {
+                const int e = cnt + __popc(m & below);
+                if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
             }
-            sfp[hs] = fd;
-            const int at = a.sorted[hs];
-            rho_out[at] = rho;
-            afrho_out[at] = f;
-            fp_out[at] = fd;
+            cnt += __popc(m);
         }
+        if (live && gl == 0) {
+            cnt_out[hs] = cnt;
+            if (cnt > pair_cap) overflow = max(overflow, cnt);
+        }
+    }
+    if (overflow) { atomicExch(&flags[0], 1); atomicMax(&flags[1], overflow); }
+}
+
+// rho_i over the compact row (rhoset), then F and F' (embed,
+// src/potential_m.F90:148-169); one thread per atom in cell order
+__global__ void __launch_bounds__(256)
+k_cl_density(TileArgs a, Tables t, const int32_t *__restrict__ nslots_ptr, int ntot, int pair_cap,
+             const int32_t *__restrict__ alist,
+             const int32_t *__restrict__ cnt, double *__restrict__ sfp, double *__restrict__ rho_out,
+             double *__restrict__ afrho_out, double *__restrict__ fp_out, const int32_t *__restrict__ slot_sys) {
+    const int nslots = *nslots_ptr;   // atoms binned this evaluation
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < nslots; hs += gridDim.x * blockDim.x) {
+        const BSys &S = a.sys[slot_sys[hs]];
+        const double *b = S.b0;
+        const double4 ph = a.spos[hs];
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
+        double rho = 0.0;
+        for (int e = 0; e < n; ++e) {
+            const double4 p = a.spos[alist[(size_t)e * ntot + hs]];
+            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+            double ux, uy, uz;
+            pair_u(b, dx, dy, dz, ux, uy, uz);
+            rho += density_func(t, sqrt(ux * ux + uy * uy + uz * uz));
+        }
+        double f = 0.0, fd = 0.0;
+        if (rho > 1e-40) {
+            double2 e2 = embed_funcs(t, rho);
+            f = e2.x; fd = e2.y;
+        }
+        sfp[hs] = fd;
+        const int at = a.sorted[hs];
+        rho_out[at] = rho;
+        afrho_out[at] = f;
+        fp_out[at] = fd;
     }
 }
 
-// Forces on each home atom (the pair loop of force(), src/dynamics_m.F90:232-318),
+// Forces on each atom (the pair loop of force(), src/dynamics_m.F90:232-318),
 // its energy_calc energy F + sum V_src/2 (src/dynamics_m.F90:412-483), the
 // force-routine energy F + sum V/2, and with VIR the per-atom virial
-// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1.
-template <int LPH, bool VIR>
-__global__ void __launch_bounds__(32 * kTileWarps)
-k_tile_forces(TileArgs a, Tables t, const double *__restrict__ afrho, double *__restrict__ fout,
-              double *__restrict__ en_calc, double *__restrict__ en_force, double *__restrict__ vir) {
-    __shared__ double4 tpos[kTileWarps][kTileCap];
-    __shared__ double tfp[kTileWarps][kTileCap];
-    __shared__ int tidx[kTileWarps][kTileCap];
-    __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * kTileWarps + w;
-    if (c >= a.ncell) return;
-    const BSys &S = a.sys[a.cell_sys[c]];
-    if (!S.active) return;
-    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
-    if (h1 == h0) return;
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
-    const int total = stage_tile<true>(a, S, c, tpos[w], tfp[w], tidx[w], tpre[w], tcs[w]);
-    const int g = lane / LPH, gl = lane % LPH;
-    for (int hb = h0; hb < h1; hb += 32 / LPH) {
-        const int hs = hb + g;
+// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1; one thread per atom.
+template <bool VIR>
+__global__ void __launch_bounds__(256)
+k_cl_forces(TileArgs a, Tables t, const int32_t *__restrict__ nslots_ptr, int ntot, int pair_cap,
+            const int32_t *__restrict__ alist,
+            const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ afrho,
+            double *__restrict__ fout, double *__restrict__ en_calc, double *__restrict__ en_force,
+            double *__restrict__ vir) {
+    const int nslots = *nslots_ptr;
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < nslots; hs += gridDim.x * blockDim.x) {
+        const BSys &S = a.sys[slot_sys[hs]];
+        const double *b = S.b0;
+        const double4 ph = a.spos[hs];
+        const double fph = a.sfp[hs];
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
         double fx = 0.0, fy = 0.0, fz = 0.0, ec = 0.0, ef = 0.0;
         double v[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) v[k] = 0.0;
-        if (hs < h1) {
-            const double4 ph = a.spos[hs];
-            const double fph = a.sfp[hs];
-            for (int k = gl; k < total; k += LPH) {
-                double4 p; double fpk; int slot;
-                candidate<true>(a, k, tpos[w], tfp[w], tidx[w], tpre[w], tcs[w], p, fpk, slot);
-                if (slot == hs) continue;
-                double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-                dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-                double ux, uy, uz;
-                pair_u(b, dx, dy, dz, ux, uy, uz);
-                double r2 = ux * ux + uy * uy + uz * uz;
-                if (r2 >= a.rc2) continue;
-                double r = sqrt(r2);
-                double4 q = pair_funcs(t, r);     // V, V', phi, phi'
-                double rr = 1.0 / r;
-                double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
-                fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-                ef += 0.5 * q.x;
-                ec += 0.5 * fetm_vee(t, r);
-                if (VIR && (ph.w + p.w) > 0.1) {
-                    double hf = 0.5 * fpair;
-                    v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
-                    v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
-                    v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
-                }
+        for (int e = 0; e < n; ++e) {
+            const int j = alist[(size_t)e * ntot + hs];
+            const double4 p = a.spos[j];
+            const double fpk = a.sfp[j];
+            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+            double ux, uy, uz;
+            pair_u(b, dx, dy, dz, ux, uy, uz);
+            double r = sqrt(ux * ux + uy * uy + uz * uz);
+            double4 q = pair_funcs(t, r);     // V, V', phi, phi'
+            double rr = 1.0 / r;
+            double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
+            fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+            ef += 0.5 * q.x;
+            ec += 0.5 * fetm_vee(t, r);
+            if (VIR && (ph.w + p.w) > 0.1) {
+                double hf = 0.5 * fpair;
+                v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
+                v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
+                v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
             }
         }
-        fx = group_sum<LPH>(fx); fy = group_sum<LPH>(fy); fz = group_sum<LPH>(fz);
-        ec = group_sum<LPH>(ec); ef = group_sum<LPH>(ef);
+        const int at = a.sorted[hs];
+        fout[3 * (size_t)at] = fx;
+        fout[3 * (size_t)at + 1] = fy;
+        fout[3 * (size_t)at + 2] = fz;
+        en_calc[at] = afrho[at] + ec;
+        en_force[at] = afrho[at] + ef;
         if (VIR) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) v[k] = group_sum<LPH>(v[k]);
-        }
-        if (hs < h1 && gl == 0) {
-            const int at = a.sorted[hs];
-            fout[3 * (size_t)at] = fx;
-            fout[3 * (size_t)at + 1] = fy;
-            fout[3 * (size_t)at + 2] = fz;
-            en_calc[at] = afrho[at] + ec;
-            en_force[at] = afrho[at] + ef;
-            if (VIR) {
-#pragma unroll
-                for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
-            }
+            for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
         }
     }
+}
+
+// system of each cell-order slot (the slot's atom's system)
+__global__ void k_slot_sys(const int32_t *__restrict__ nslots_ptr, const int32_t *__restrict__ sorted,
+                           const int32_t *__restrict__ atom_sys, int32_t *__restrict__ slot_sys) {
+    int hs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (hs < *nslots_ptr) slot_sys[hs] = atom_sys[sorted[hs]];
 }
 
 // ------------------------------------------------------ block reductions --
@@ -659,6 +690,8 @@ class BatchEngine {
     double *X = nullptr, *mass = nullptr, *f = nullptr, *rho = nullptr, *afrho = nullptr, *fp = nullptr;
     double *en_calc = nullptr, *en_force = nullptr, *vir = nullptr, *sfp = nullptr, *sysout = nullptr;
     double *cgv = nullptr;              // G, D, GS, XX, GG, DR, DGR (3*ntot each)
+    int32_t *alist = nullptr, *pcnt = nullptr, *slot_sys = nullptr, *flags = nullptr;
+    int pair_cap = 48;                  // compact-row entries per atom
     double4 *spos = nullptr;
     CgState *cg = nullptr;
     double4 *tab_r4 = nullptr;
@@ -683,6 +716,7 @@ class BatchEngine {
     int get_array(const double *dev, int stride, double *a, double *b, double *c);
     void queue_evaluation(bool with_vir);
     int ready();
+    int take_overflow();
 };
 
 #define BCHECK(call)                                                      \
@@ -717,7 +751,7 @@ BatchEngine::~BatchEngine() {
     if (graph) cudaGraphExecDestroy(graph);
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, mass,
                     f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
-                    tab_r4f, tab_e2f, stage};
+                    tab_r4f, tab_e2f, stage, alist, pcnt, slot_sys, flags};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -771,6 +805,11 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCHECK(balloc(&cgv, 7 * 3 * nt, "CG vectors"));
     BCHECK(balloc(&cg, n, "CG state"));
     BCHECK(balloc(&stage, 3 * nt, "staging"));
+    BCHECK(balloc(&alist, nt * (size_t)pair_cap, "compact list"));
+    BCHECK(balloc(&pcnt, nt, "compact counts"));
+    BCHECK(balloc(&slot_sys, nt, "slot systems"));
+    BCHECK(balloc(&flags, 2, "flags"));
+    BCUDA(cudaMemset(flags, 0, 2 * sizeof(int32_t)), "flags");
     BCUDA(cudaMallocHost((void **)&host_active, sizeof(int)), "pinned");
     std::vector<int32_t> as(nt);
     for (int s = 0; s < n; ++s)
@@ -879,12 +918,17 @@ int BatchEngine::ready() {
 template <int LPH>
 static void launch_tiles(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
     const int nb = (E.ncell + kTileWarps - 1) / kTileWarps;
-    k_tile_density<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.sfp, E.rho, E.afrho, E.fp);
+    const int nbs = grid_blocks(E.ntot, 256);
+    k_tile_screen<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.ntot, E.pair_cap, E.alist, E.pcnt, E.flags);
+    const int32_t *nslots = E.cell_start + E.ncell;
+    k_cl_density<<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho, E.afrho,
+                                     E.fp, E.slot_sys);
     if (with_vir)
-        k_tile_forces<LPH, true><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.afrho, E.f, E.en_calc, E.en_force, E.vir);
+        k_cl_forces<true><<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.slot_sys,
+                                              E.afrho, E.f, E.en_calc, E.en_force, E.vir);
     else
-        k_tile_forces<LPH, false><<<nb, 32 * kTileWarps, 0, s>>>(a, E.tab, E.afrho, E.f, E.en_calc, E.en_force,
-                                                                  E.vir);
+        k_cl_forces<false><<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.slot_sys,
+                                               E.afrho, E.f, E.en_calc, E.en_force, E.vir);
 }
 
 // binning and the two tile passes for the systems marked active
@@ -897,6 +941,7 @@ void BatchEngine::queue_evaluation(bool with_vir) {
     cudaMemsetAsync(cursor, 0, sizeof(int32_t) * ncell, s);
     k_bin_fill<<<nb, 256, 0, s>>>(ntot, cell_of, cell_start, cursor, sorted);
     k_bin_sort<<<nbc, 256, 0, s>>>(ncell, cell_start, sorted, X, mass, spos);
+    k_slot_sys<<<nb, 256, 0, s>>>(cell_start + ncell, sorted, atom_sys, slot_sys);
     TileArgs a;
     a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
     a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
@@ -906,20 +951,41 @@ void BatchEngine::queue_evaluation(bool with_vir) {
         case 32: launch_tiles<32>(*this, a, with_vir, s); break;
         default: launch_tiles<8>(*this, a, with_vir, s); break;
     }
-    launches += 6;
+    launches += 8;
+}
+
+// compact-row overflow of the last evaluations: grows the rows (the caller
+// evaluates again) and returns the largest row seen, or 0
+int BatchEngine::take_overflow() {
+    int32_t h[2] = {0, 0};
+    if (cudaMemcpy(h, flags, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (!h[0]) return 0;
+    cudaMemset(flags, 0, sizeof(h));
+    int need = h[1] + 8;
+    if (alist) cudaFree(alist);
+    alist = nullptr;
+    if (balloc(&alist, (size_t)ntot * (size_t)need, "compact list") != MOLDY_OK) return -1;
+    pair_cap = need;
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    return h[1];
 }
 
 int BatchEngine::force(double *out13) {
     BCHECK(ready());
-    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1);
-    queue_evaluation(true);
-    k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
-    launches += 2;
+    for (int attempt = 0;; ++attempt) {
+        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1);
+        queue_evaluation(true);
+        k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+        launches += 2;
+        BCUDA(cudaStreamSynchronize(stream), "batch force");
+        BCUDA(cudaGetLastError(), "batch force");
+        int ov = take_overflow();
+        if (ov < 0) return set_last_error(MOLDY_ERR_CUDA, "compact list re-allocation failed");
+        if (ov == 0) break;
+        if (attempt >= 2) return set_last_error(MOLDY_ERR_CAPACITY, "compact list keeps overflowing");
+    }
     if (out13)
-        BCUDA(cudaMemcpyAsync(out13, sysout, 13 * (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost, stream),
-              "results");
-    BCUDA(cudaStreamSynchronize(stream), "batch force");
-    BCUDA(cudaGetLastError(), "batch force");
+        BCUDA(cudaMemcpy(out13, sysout, 13 * (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost), "results");
     return MOLDY_OK;
 }
 
@@ -978,14 +1044,14 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
             return set_last_error(MOLDY_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
         }
         graph_lph = lph; graph_cap = cap; graph_maxfn = maxfn; graph_criterion = criterion; graph_fmax = fmax;
-        launches -= 6;   // captured, not run; counted per replay below
+        launches -= 8;   // captured, not run; counted per replay below
     }
     // VA14CD evaluates at most maxfn times; a few rounds more let every
     // system reach its return
     const int rounds = maxfn + 8;
     for (int r = 0; r < rounds; ++r) {
         BCUDA(cudaGraphLaunch(graph, s), "graph launch");
-        launches += 7;
+        launches += 9;
         if ((r & 7) == 7 || r == rounds - 1) {
             BCUDA(cudaMemcpyAsync(host_active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s), "counter");
             BCUDA(cudaStreamSynchronize(s), "quench");
@@ -1009,6 +1075,11 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
     // leave every system active for later force calls
     k_set_active<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, sys, 1);
     BCUDA(cudaStreamSynchronize(s), "quench");
+    int ov = take_overflow();
+    if (ov != 0)
+        return set_last_error(MOLDY_ERR_CAPACITY, "an atom had " + std::to_string(ov) +
+                                                      " neighbours inside the cut, more than a compact row held; "
+                                                      "the rows have been grown, quench again");
     if (unfinished) return set_last_error(MOLDY_ERR_CAPACITY, std::to_string(unfinished) + " systems did not finish");
     return MOLDY_OK;
 }
