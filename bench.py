@@ -529,16 +529,32 @@ def run_batch(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    # untimed: choose the tile shape (lanes per home atom) on this batch
+    boxes = [w.b0 for w in ws]
+
+    def build_and_force():
+        b.set_state(b0=boxes)          # new boxes: every list is built at the next evaluation
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.force()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # untimed: choose the tile shape (lanes per home atom) on evaluations that
+    # build every list
     tune = {}
     for lanes in (4, 8, 16, 32):
         b.set_tiles(lanes, 256)
-        b.force()
-        tune[lanes] = timed(b.force, 3)
+        build_and_force()
+        tune[lanes] = min(build_and_force() for _ in range(3))
     best = min(tune, key=tune.get)
     b.set_tiles(best, 256)
     for _ in range(max(args.warmup, 3)):
         b.force()
+    # evaluations with every list current (the positions do not move between
+    # them; in a quench or MD run lists are kept until an atom moved half the skin)
     steps = max(1, min(args.steps, 200))
     l0 = b.launches()
     with ClockSampler(local_rank) as clk:
@@ -551,41 +567,55 @@ def run_batch(args):
     launches = b.launches() - l0
     ntot_all = sum(w.nm for w in ws_all)
     value = ntot_all / (ms_max / 1000.0)
+    build_ms = max_over_ranks(float(np.median([build_and_force() for _ in range(5)])))
 
     # end to end: positions from pinned host memory, one evaluation, forces and
     # per-system results back, every step
     x = torch.empty((b.ntot, 3), dtype=torch.float64, pin_memory=True).numpy()
     x[:] = b.get_state()
-    boxes = [w.b0 for w in ws]
-    fr = [torch.empty(b.ntot, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+
+    fxyz = torch.empty((b.ntot, 3), dtype=torch.float64, pin_memory=True).numpy()
 
     def e2e_step():
-        b.set_state(x, boxes)
+        b.set_positions(x)
         b.force()
-        b.forces_into(*fr)
+        b.forces_xyz_into(fxyz)
 
     e2e_ms = max_over_ranks(timed(e2e_step, min(steps, 20)))
-    h2d = 24 * b.ntot + 72 * len(ws)
+    h2d = 24 * b.ntot
     d2h = 24 * b.ntot + 104 * len(ws)
 
     # the quench of every supercell to max |F| <= 1e-4 eV/A (criterion of the
-    # benchmark) from the starting positions
-    b.set_state(x, boxes)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    q = b.quench(maxfn=2000, criterion=1, fmax=1e-4)
-    e1.record(stream)
-    e1.synchronize()
-    qms = max_over_ranks(e0.elapsed_time(e1))
+    # benchmark) from the starting positions; untimed sweep of the list skin,
+    # then a fresh timed quench with the best
+    def run_quench(skin):
+        b.set_skin(skin)
+        b.set_state(x, boxes)
+        st0 = b.list_stats()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        q = b.quench(maxfn=2000, criterion=1, fmax=1e-4)
+        e1.record(stream)
+        e1.synchronize()
+        st1 = b.list_stats()
+        return q, max_over_ranks(e0.elapsed_time(e1)), st1["builds"] - st0["builds"], \
+            st1["evaluations"] - st0["evaluations"]
+
+    skin_ms = {}
+    for sk in (0.0, 0.3, 0.6):
+        skin_ms[sk] = run_quench(sk)[1]
+    best_skin = min(skin_ms, key=skin_ms.get)
+    q, qms, qbuilds, qevals = run_quench(best_skin)
     rounds = int(q["nfev"].max())
     quench = {"seconds": qms / 1000.0, "systems": int(len(ws_all)), "converged": int((q["iflag"] == 0).sum()),
               "cg_error_returns": int((q["iflag"] == 2).sum()), "max_function_values": rounds,
               "median_function_values": float(np.median(q["nfev"])),
               "systems_per_s": len(ws_all) / (qms / 1000.0),
               "atom_evals_per_s": float((q["nfev"] * b.natoms).sum()) * world / (qms / 1000.0),
-              "max_force_eV_per_A": float(q["fmax"].max())}
+              "max_force_eV_per_A": float(q["fmax"].max()), "skin_A": best_skin, "skin_sweep_ms": skin_ms,
+              "list_builds_per_system_evaluation": qbuilds / max(qevals, 1)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = batch_cpu_baseline(ws_all, args.cpu_seconds)
@@ -600,6 +630,8 @@ def run_batch(args):
         "data": "synthetic (seeded strained bcc Fe supercells, Gaussian displacements 0.1 A)",
         "config": {"workload": f"{len(ws_all)} bcc Fe supercells, n ~ U{{4..16}}, strain +/-2%",
                    "atoms": ntot_all, "tile_lanes_per_atom": best, "tile_autotune_ms": tune,
+                   "timed_step": "one evaluation of every system with its list current",
+                   "evaluation_with_every_list_built_ms": build_ms,
                    "parallelism": f"supercells sharded over {world} rank(s) by atom count",
                    "l2": "per-evaluation working set (positions, cell order, forces, energies, virial) "
                          "> 126 MB L2"},

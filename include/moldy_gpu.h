@@ -297,6 +297,10 @@ int moldy_gpu_batch_get_state(moldy_batch *h, double *x0, double *y0, double *z0
 int moldy_gpu_batch_force(moldy_batch *h, double *out13);
 /* fractional forces, per-atom energies (energy_calc; force routine), rho/F/F' */
 int moldy_gpu_batch_get_forces(moldy_batch *h, double *fx, double *fy, double *fz);
+/* Interleaved forms: xyz[3i..3i+2] are atom i's fractional position or
+ * fractional force (the layout of quench_m's x vector), one copy each way. */
+int moldy_gpu_batch_set_positions(moldy_batch *h, const double *xyz);
+int moldy_gpu_batch_get_forces_xyz(moldy_batch *h, double *fxyz);
 int moldy_gpu_batch_get_energies(moldy_batch *h, double *en_calc, double *en_force);
 int moldy_gpu_batch_get_density(moldy_batch *h, double *rho, double *afrho, double *dafrho);
 /* Conjugate-gradient quench of every system with at most maxfn function values
@@ -313,6 +317,14 @@ int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, dou
  * candidates a warp stages in shared memory (0..256, default 256; the rest are
  * read from global memory). */
 int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
+/* Verlet skin of the per-system lists (default 0.3 A): a system's list holds
+ * the pairs within rcut + skin (less where its box is narrower than twice
+ * that) and is rebuilt once one of its atoms has moved more than half the
+ * skin since the last build, or after its box changed.  0 rebuilds at every
+ * evaluation in which an atom moved. */
+int moldy_gpu_batch_set_skin(moldy_batch *h, double skin);
+/* out2[0]: system list builds so far; out2[1]: system evaluations so far. */
+int moldy_gpu_batch_list_stats(moldy_batch *h, int64_t *out2);
 /* Kernel launches queued so far by this handle; its cudaStream_t. */
 int moldy_gpu_batch_launches(moldy_batch *h, int64_t *launches);
 int moldy_gpu_batch_get_stream(moldy_batch *h, void **stream);

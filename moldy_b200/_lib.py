@@ -116,9 +116,13 @@ SIGNATURES = {
     "moldy_gpu_batch_force": [H, D],
     "moldy_gpu_batch_get_forces": [H, D, D, D],
     "moldy_gpu_batch_get_energies": [H, D, D],
+    "moldy_gpu_batch_set_positions": [H, D],
+    "moldy_gpu_batch_get_forces_xyz": [H, D],
     "moldy_gpu_batch_get_density": [H, D, D, D],
     "moldy_gpu_batch_quench": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, D],
     "moldy_gpu_batch_set_tiles": [H, ctypes.c_int32, ctypes.c_int32],
+    "moldy_gpu_batch_set_skin": [H, ctypes.c_double],
+    "moldy_gpu_batch_list_stats": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_get_stream": [H, ctypes.POINTER(ctypes.c_void_p)],
     "moldy_fetm_build_tables": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,

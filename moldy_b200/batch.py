@@ -74,6 +74,22 @@ class MoldyBatch:
         m = None if mass is None else _f64(mass)
         check(self._L.moldy_gpu_batch_set_state(self._h, *[_dp(c) for c in cols], _dp(bb), _dp(m)))
 
+    def set_positions(self, xyz):
+        """(ntot, 3) C-contiguous float64 fractional positions in one copy
+        (pinned host memory copies fastest)."""
+        a = self._xyz(xyz)
+        check(self._L.moldy_gpu_batch_set_positions(self._h, _dp(a)))
+
+    def forces_xyz_into(self, out):
+        """Fractional forces into a preallocated (ntot, 3) C-contiguous float64 array."""
+        check(self._L.moldy_gpu_batch_get_forces_xyz(self._h, _dp(self._xyz(out))))
+
+    def _xyz(self, a):
+        if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous \
+                or a.shape != (self.ntot, 3):
+            raise ValueError("needs a C-contiguous float64 array of shape (ntot, 3)")
+        return a
+
     def get_state(self) -> np.ndarray:
         c = [np.zeros(self.ntot) for _ in range(3)]
         check(self._L.moldy_gpu_batch_get_state(self._h, *[_dp(a) for a in c]))
@@ -122,6 +138,16 @@ class MoldyBatch:
 
     def set_tiles(self, lanes=8, staged=256):
         check(self._L.moldy_gpu_batch_set_tiles(self._h, int(lanes), int(staged)))
+
+    def set_skin(self, skin=0.3):
+        """Verlet skin of the per-system lists (A); 0 rebuilds whenever an atom moved."""
+        check(self._L.moldy_gpu_batch_set_skin(self._h, float(skin)))
+
+    def list_stats(self) -> dict:
+        """System list builds and system evaluations since creation."""
+        v = (ctypes.c_int64 * 2)()
+        check(self._L.moldy_gpu_batch_list_stats(self._h, v))
+        return {"builds": int(v[0]), "evaluations": int(v[1])}
 
     def launches(self) -> int:
         v = ctypes.c_int64(0)

@@ -6,23 +6,30 @@
 // (src/quench_m.F90:100-551) at a fixed box.
 //
 // Layout.  Atoms of all systems are concatenated, each system's in the
-// reference's order.  Every evaluation bins the atoms of the systems that
-// need one into a per-system grid of cells at least the interaction range
-// wide (in each direction, perpendicular to the cell faces), sorts each cell
-// by atom index, and copies positions into cell order.  One warp owns one
-// cell: it stages the atoms of the 27 (fewer for grids under 3 cells)
-// surrounding cells in shared memory and evaluates every pair of a home atom
-// with its lanes, reducing with shuffles.  Each pair is evaluated from both
-// ends, so there are no atomics and every sum has a fixed order.
+// reference's order, and system s owns the slots [atom0, atom0 + nm) of the
+// cell order too, so one system's list can be rebuilt without moving another
+// system's.  A system's cells are at least its list radius rv = rc + skin wide
+// (perpendicular to the cell faces).
+//
+// Lists.  One block per system checks the largest displacement since the
+// system's last build; past half the skin (or after a box change) the same
+// block bins, scans, fills and sorts the system's cells, and every evaluated
+// system copies its positions into cell order.  For a rebuilt system one warp
+// per cell stages the 27 (fewer for grids under 3 cells) surrounding cells in
+// shared memory and writes each home atom's compact row of the candidates
+// inside rv.  The density and force passes run one thread per atom over its
+// row and keep the pairs inside rc.  Each pair is evaluated from both ends, so
+// there are no atomics and every sum has a fixed order.
 //
 // Pairs.  The reference sums over its Verlet list (pairs within rnear at the
 // last rebuild); every pair beyond the table cut contributes exactly zero, so
-// a complete set of the pairs inside the cut gives the same sums.  The tiles
-// find every pair within the cut at every evaluation.
+// a complete set of the pairs inside the cut gives the same sums.  A pair
+// inside rc now was inside rv at the last build while no atom has moved more
+// than half the skin since.
 //
 // The quench keeps VA14CD's state per system in device memory.  One block per
 // system runs the state machine between function evaluations; a round is the
-// binning, the two tile passes and one control launch, captured once in a
+// list check, the tile passes and one control launch, captured once in a
 // CUDA graph and replayed until every system has finished.
 #include <algorithm>
 #include <cmath>
@@ -38,13 +45,18 @@ namespace {
 constexpr int kTileWarps = 4;     // cells (warps) per block
 constexpr int kTileCap = 256;     // staged candidates per warp
 constexpr int kCgThreads = 256;   // control block
+constexpr int kPrepThreads = 256; // list check and binning block
 
 struct BSys {
     int atom0, nm, cell0, ncell;
     int nc[3], nst[3];            // cells per dimension; stencil offsets per dimension (1, 2 or 3)
     int active;                   // evaluated in the next round
+    int rebuild;                  // list rebuilt in this evaluation (set by k_prepare)
+    int stale;                    // list invalid: rebuild at the next evaluation
     int pad;
     double b0[9], tg[9], vol;
+    double rv2;                   // squared list radius
+    double hs2;                   // squared half skin: rebuild once an atom moved farther
 };
 
 // VA14CD state of one system (src/quench_m.F90:323-551)
@@ -143,219 +155,6 @@ __device__ __forceinline__ double group_sum(double v) {
     return v;
 }
 
-// ---------------------------------------------------------------- binning --
-__global__ void k_bin(int ntot, const double *__restrict__ X, const int32_t *__restrict__ atom_sys,
-                      const BSys *__restrict__ sys, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= ntot) return;
-    const BSys &S = sys[atom_sys[a]];
-    if (!S.active) { cell_of[a] = -1; return; }
-    int ic[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double x = X[3 * (size_t)a + d];
-        double u = x - floor(x);
-        int c = (int)(u * (double)S.nc[d]);
-        ic[d] = c < 0 ? 0 : (c >= S.nc[d] ? S.nc[d] - 1 : c);
-    }
-    int c = S.cell0 + ic[0] + S.nc[0] * (ic[1] + S.nc[1] * ic[2]);
-    cell_of[a] = c;
-    atomicAdd(&cell_count[c], 1);
-}
-
-__global__ void k_bin_fill(int ntot, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ cell_start,
-                           int32_t *__restrict__ cursor, int32_t *__restrict__ sorted) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= ntot) return;
-    int c = cell_of[a];
-    if (c < 0) return;
-    int k = atomicAdd(&cursor[c], 1);
-    sorted[cell_start[c] + k] = a;
-}
-
-// ascending atom order inside each cell, then positions and masses in cell order
-__global__ void k_bin_sort(int ncell, const int32_t *__restrict__ cell_start, int32_t *__restrict__ sorted,
-                           const double *__restrict__ X, const double *__restrict__ mass,
-                           double4 *__restrict__ spos) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    int s0 = cell_start[c], s1 = cell_start[c + 1];
-    for (int i = s0 + 1; i < s1; ++i) {
-        int v = sorted[i], j = i - 1;
-        while (j >= s0 && sorted[j] > v) { sorted[j + 1] = sorted[j]; --j; }
-        sorted[j + 1] = v;
-    }
-    for (int i = s0; i < s1; ++i) {
-        int a = sorted[i];
-        spos[i] = make_double4(X[3 * (size_t)a], X[3 * (size_t)a + 1], X[3 * (size_t)a + 2], mass[a]);
-    }
-}
-
-// ------------------------------------------------------------ tile passes --
-// The tile screen finds, for every home atom of a cell, the candidates
-// inside the cut and writes their cell-order slots into the atom's compact
-// row (entry-major, alist[e * ntot + slot]) in candidate order.  LPH lanes
-// serve one home atom: they test LPH candidates at a time and place the hits
-// with one warp ballot, so no lane waits on another's pair arithmetic.
-template <int LPH>
-__global__ void __launch_bounds__(32 * kTileWarps)
-k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, int32_t *__restrict__ cnt_out,
-              int32_t *__restrict__ flags) {
-    __shared__ double4 tpos[kTileWarps][kTileCap];
-    __shared__ int tidx[kTileWarps][kTileCap];
-    __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * kTileWarps + w;
-    if (c >= a.ncell) return;
-    const BSys &S = a.sys[a.cell_sys[c]];
-    if (!S.active) return;
-    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
-    if (h1 == h0) return;
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
-    const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
-    const int g = lane / LPH, gl = lane % LPH;
-    const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
-    const unsigned below = (1u << lane) - 1u;
-    int overflow = 0;
-    for (int hb = h0; hb < h1; hb += 32 / LPH) {
-        const int hs = hb + g;
-        const bool live = hs < h1;
-        const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
-        int cnt = 0;
-        // every lane of the warp runs the same number of rounds (ballots are warp-wide)
-        for (int k0 = 0; k0 < total; k0 += LPH) {
-            const int k = k0 + gl;
-            bool hit = false;
-            int slot = -1;
-            if (live && k < total) {
-                double4 p; double fpk;
-                candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
-                if (slot != hs) {
-                    double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-                    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-                    double ux, uy, uz;
-                    pair_u(b, dx, dy, dz, ux, uy, uz);
-                    hit = (ux * ux + uy * uy + uz * uz) < a.rc2;
-                }
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
-            if (hit) {
-                const int e = cnt + __popc(m & below);
-                if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
-            }
-            cnt += __popc(m);
-        }
-        if (live && gl == 0) {
-            cnt_out[hs] = cnt;
-            if (cnt > pair_cap) overflow = max(overflow, cnt);
-        }
-    }
-    if (overflow) { atomicExch(&flags[0], 1); atomicMax(&flags[1], overflow); }
-}
-
-// rho_i over the compact row (rhoset), then F and F' (embed,
-// src/potential_m.F90:148-169); one thread per atom in cell order
-__global__ void __launch_bounds__(256)
-k_cl_density(TileArgs a, Tables t, const int32_t *__restrict__ nslots_ptr, int ntot, int pair_cap,
-             const int32_t *__restrict__ alist,
-             const int32_t *__restrict__ cnt, double *__restrict__ sfp, double *__restrict__ rho_out,
-             double *__restrict__ afrho_out, double *__restrict__ fp_out, const int32_t *__restrict__ slot_sys) {
-    const int nslots = *nslots_ptr;   // atoms binned this evaluation
-    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < nslots; hs += gridDim.x * blockDim.x) {
-        const BSys &S = a.sys[slot_sys[hs]];
-        const double *b = S.b0;
-        const double4 ph = a.spos[hs];
-        int n = cnt[hs];
-        n = n < pair_cap ? n : pair_cap;
-        double rho = 0.0;
-        for (int e = 0; e < n; ++e) {
-            const double4 p = a.spos[alist[(size_t)e * ntot + hs]];
-            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-            double ux, uy, uz;
-            pair_u(b, dx, dy, dz, ux, uy, uz);
-            rho += density_func(t, sqrt(ux * ux + uy * uy + uz * uz));
-        }
-        double f = 0.0, fd = 0.0;
-        if (rho > 1e-40) {
-            double2 e2 = embed_funcs(t, rho);
-            f = e2.x; fd = e2.y;
-        }
-        sfp[hs] = fd;
-        const int at = a.sorted[hs];
-        rho_out[at] = rho;
-        afrho_out[at] = f;
-        fp_out[at] = fd;
-    }
-}
-
-// Forces on each atom (the pair loop of force(), src/dynamics_m.F90:232-318),
-// its energy_calc energy F + sum V_src/2 (src/dynamics_m.F90:412-483), the
-// force-routine energy F + sum V/2, and with VIR the per-atom virial
-// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1; one thread per atom.
-template <bool VIR>
-__global__ void __launch_bounds__(256)
-k_cl_forces(TileArgs a, Tables t, const int32_t *__restrict__ nslots_ptr, int ntot, int pair_cap,
-            const int32_t *__restrict__ alist,
-            const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ afrho,
-            double *__restrict__ fout, double *__restrict__ en_calc, double *__restrict__ en_force,
-            double *__restrict__ vir) {
-    const int nslots = *nslots_ptr;
-    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < nslots; hs += gridDim.x * blockDim.x) {
-        const BSys &S = a.sys[slot_sys[hs]];
-        const double *b = S.b0;
-        const double4 ph = a.spos[hs];
-        const double fph = a.sfp[hs];
-        int n = cnt[hs];
-        n = n < pair_cap ? n : pair_cap;
-        double fx = 0.0, fy = 0.0, fz = 0.0, ec = 0.0, ef = 0.0;
-        double v[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = 0.0;
-        for (int e = 0; e < n; ++e) {
-            const int j = alist[(size_t)e * ntot + hs];
-            const double4 p = a.spos[j];
-            const double fpk = a.sfp[j];
-            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-            double ux, uy, uz;
-            pair_u(b, dx, dy, dz, ux, uy, uz);
-            double r = sqrt(ux * ux + uy * uy + uz * uz);
-            double4 q = pair_funcs(t, r);     // V, V', phi, phi'
-            double rr = 1.0 / r;
-            double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
-            fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-            ef += 0.5 * q.x;
-            ec += 0.5 * fetm_vee(t, r);
-            if (VIR && (ph.w + p.w) > 0.1) {
-                double hf = 0.5 * fpair;
-                v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
-                v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
-                v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
-            }
-        }
-        const int at = a.sorted[hs];
-        fout[3 * (size_t)at] = fx;
-        fout[3 * (size_t)at + 1] = fy;
-        fout[3 * (size_t)at + 2] = fz;
-        en_calc[at] = afrho[at] + ec;
-        en_force[at] = afrho[at] + ef;
-        if (VIR) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
-        }
-    }
-}
-
-// system of each cell-order slot (the slot's atom's system)
-__global__ void k_slot_sys(const int32_t *__restrict__ nslots_ptr, const int32_t *__restrict__ sorted,
-                           const int32_t *__restrict__ atom_sys, int32_t *__restrict__ slot_sys) {
-    int hs = blockIdx.x * blockDim.x + threadIdx.x;
-    if (hs < *nslots_ptr) slot_sys[hs] = atom_sys[sorted[hs]];
-}
-
 // ------------------------------------------------------ block reductions --
 // fixed-order sum over the block, returned to every thread
 __device__ double block_sum(double v, double *sh) {
@@ -386,6 +185,276 @@ __device__ double block_max(double v, double *sh) {
     }
     __syncthreads();
     return sh[32];
+}
+
+// ------------------------------------------------------ lists and binning --
+// One block per system.  An evaluated system whose list is stale, or one of
+// whose atoms moved more than half the skin since the last build (a pair can
+// only come inside rc after that), rebuilds: its atoms are binned into its
+// cells, the cell sizes scanned into slot ranges starting at atom0, every
+// cell filled and sorted by atom index.  Every evaluated system then copies
+// its positions and masses into cell order.
+__global__ void __launch_bounds__(kPrepThreads)
+k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__restrict__ mass,
+          double *__restrict__ Xb, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
+          int32_t *__restrict__ cell_start, int32_t *__restrict__ cursor, int32_t *__restrict__ sorted,
+          double4 *__restrict__ spos, unsigned long long *__restrict__ stats) {
+    __shared__ double sh[33];
+    __shared__ int wsum[kPrepThreads / 32];
+    BSys &S = sys[blockIdx.x];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+    if (!S.active) {
+        if (tid == 0) S.rebuild = 0;
+        return;
+    }
+    const int a0 = S.atom0, nm = S.nm;
+    int rebuild = S.stale;
+    if (!rebuild) {
+        double m = 0.0;
+        for (int i = tid; i < nm; i += nt) {
+            const size_t a = 3 * (size_t)(a0 + i);
+            double rx, ry, rz;
+            pair_u(S.b0, X[a] - Xb[a], X[a + 1] - Xb[a + 1], X[a + 2] - Xb[a + 2], rx, ry, rz);
+            m = fmax(m, rx * rx + ry * ry + rz * rz);
+        }
+        rebuild = block_max(m, sh) > S.hs2;
+    }
+    __syncthreads();   // every thread has read S.stale
+    if (tid == 0) {
+        S.rebuild = rebuild;
+        S.stale = 0;
+        atomicAdd(&stats[1], 1ULL);
+        if (rebuild) atomicAdd(&stats[0], 1ULL);
+    }
+    if (rebuild) {
+        for (int i = tid; i < nm; i += nt) {
+            const int a = a0 + i;
+            int ic[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double x = X[3 * (size_t)a + d];
+                Xb[3 * (size_t)a + d] = x;
+                const double u = x - floor(x);
+                const int c = (int)(u * (double)S.nc[d]);
+                ic[d] = c < 0 ? 0 : (c >= S.nc[d] ? S.nc[d] - 1 : c);
+            }
+            const int c = S.cell0 + ic[0] + S.nc[0] * (ic[1] + S.nc[1] * ic[2]);
+            cell_of[a] = c;
+            atomicAdd(&cell_count[c], 1);
+        }
+        __syncthreads();
+        // exclusive scan of the cell sizes; the counts are taken (and zeroed
+        // for the next build) with atomics, which read them where they were added
+        int carry = a0;
+        for (int c0 = 0; c0 < S.ncell; c0 += nt) {
+            const int cl = c0 + tid;
+            const int v = cl < S.ncell ? atomicExch(&cell_count[S.cell0 + cl], 0) : 0;
+            int inc = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (lane == 31) wsum[w] = inc;
+            __syncthreads();
+            if (w == 0) {
+                int x = lane < nw ? wsum[lane] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (lane < nw) wsum[lane] = x;
+            }
+            __syncthreads();
+            if (cl < S.ncell) {
+                cell_start[S.cell0 + cl] = carry + (w > 0 ? wsum[w - 1] : 0) + inc - v;
+                cursor[S.cell0 + cl] = 0;
+            }
+            carry += wsum[nw - 1];
+            __syncthreads();
+        }
+        for (int i = tid; i < nm; i += nt) {
+            const int a = a0 + i, c = cell_of[a];
+            sorted[cell_start[c] + atomicAdd(&cursor[c], 1)] = a;
+        }
+        __syncthreads();
+        // ascending atom order inside each cell
+        for (int cl = tid; cl < S.ncell; cl += nt) {
+            const int c = S.cell0 + cl;
+            const int s0 = cell_start[c], s1 = cl + 1 < S.ncell ? cell_start[c + 1] : a0 + nm;
+            for (int i = s0 + 1; i < s1; ++i) {
+                const int v = sorted[i];
+                int j = i - 1;
+                while (j >= s0 && sorted[j] > v) { sorted[j + 1] = sorted[j]; --j; }
+                sorted[j + 1] = v;
+            }
+        }
+        __syncthreads();
+    }
+    for (int hs = a0 + tid; hs < a0 + nm; hs += nt) {
+        const int a = sorted[hs];
+        spos[hs] = make_double4(X[3 * (size_t)a], X[3 * (size_t)a + 1], X[3 * (size_t)a + 2], mass[a]);
+    }
+}
+
+// ------------------------------------------------------------ tile passes --
+// The tile screen finds, for every home atom of a cell of a rebuilt system,
+// the candidates inside the list radius and writes their cell-order slots
+// into the atom's compact row (entry-major, alist[e * ntot + slot]) in
+// candidate order.  LPH lanes
+// serve one home atom: they test LPH candidates at a time and place the hits
+// with one warp ballot, so no lane waits on another's pair arithmetic.
+template <int LPH>
+__global__ void __launch_bounds__(32 * kTileWarps)
+k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, int32_t *__restrict__ cnt_out,
+              int32_t *__restrict__ flags) {
+    __shared__ double4 tpos[kTileWarps][kTileCap];
+    __shared__ int tidx[kTileWarps][kTileCap];
+    __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kTileWarps + w;
+    if (c >= a.ncell) return;
+    const BSys &S = a.sys[a.cell_sys[c]];
+    if (!S.rebuild) return;
+    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
+    if (h1 == h0) return;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
+    const double rv2 = S.rv2;
+    const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
+    const int g = lane / LPH, gl = lane % LPH;
+    const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
+    const unsigned below = (1u << lane) - 1u;
+    int overflow = 0;
+    for (int hb = h0; hb < h1; hb += 32 / LPH) {
+        const int hs = hb + g;
+        const bool live = hs < h1;
+        const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
+        int cnt = 0;
+        // every lane of the warp runs the same number of rounds (ballots are warp-wide)
+        for (int k0 = 0; k0 < total; k0 += LPH) {
+            const int k = k0 + gl;
+            bool hit = false;
+            int slot = -1;
+            if (live && k < total) {
+                double4 p; double fpk;
+                candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
+                if (slot != hs) {
+                    double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                    double ux, uy, uz;
+                    pair_u(b, dx, dy, dz, ux, uy, uz);
+                    hit = (ux * ux + uy * uy + uz * uz) < rv2;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
+            if (hit) {
+                const int e = cnt + __popc(m & below);
+                if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
+            }
+            cnt += __popc(m);
+        }
+        if (live && gl == 0) {
+            cnt_out[hs] = cnt;
+            if (cnt > pair_cap) overflow = max(overflow, cnt);
+        }
+    }
+    if (overflow) { atomicExch(&flags[0], 1); atomicMax(&flags[1], overflow); }
+}
+
+// rho_i over the pairs of the compact row inside rc (rhoset), then F and F'
+// (embed, src/potential_m.F90:148-169); one thread per atom in cell order
+__global__ void __launch_bounds__(256)
+k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
+             const int32_t *__restrict__ cnt, double *__restrict__ sfp, double *__restrict__ rho_out,
+             double *__restrict__ afrho_out, double *__restrict__ fp_out, const int32_t *__restrict__ slot_sys) {
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
+        const BSys &S = a.sys[slot_sys[hs]];
+        if (!S.active) continue;
+        const double *b = S.b0;
+        const double4 ph = a.spos[hs];
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
+        double rho = 0.0;
+        for (int e = 0; e < n; ++e) {
+            const double4 p = a.spos[alist[(size_t)e * ntot + hs]];
+            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+            double ux, uy, uz;
+            pair_u(b, dx, dy, dz, ux, uy, uz);
+            const double r2 = ux * ux + uy * uy + uz * uz;
+            if (r2 < a.rc2) rho += density_func(t, sqrt(r2));
+        }
+        double f = 0.0, fd = 0.0;
+        if (rho > 1e-40) {
+            double2 e2 = embed_funcs(t, rho);
+            f = e2.x; fd = e2.y;
+        }
+        sfp[hs] = fd;
+        const int at = a.sorted[hs];
+        rho_out[at] = rho;
+        afrho_out[at] = f;
+        fp_out[at] = fd;
+    }
+}
+
+// Forces on each atom (the pair loop of force(), src/dynamics_m.F90:232-318),
+// its energy_calc energy F + sum V_src/2 (src/dynamics_m.F90:412-483), the
+// force-routine energy F + sum V/2, and with VIR the per-atom virial
+// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1; one thread per atom.
+template <bool VIR>
+__global__ void __launch_bounds__(256)
+k_cl_forces(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
+            const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ afrho,
+            double *__restrict__ fout, double *__restrict__ en_calc, double *__restrict__ en_force,
+            double *__restrict__ vir) {
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
+        const BSys &S = a.sys[slot_sys[hs]];
+        if (!S.active) continue;
+        const double *b = S.b0;
+        const double4 ph = a.spos[hs];
+        const double fph = a.sfp[hs];
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
+        double fx = 0.0, fy = 0.0, fz = 0.0, ec = 0.0, ef = 0.0;
+        double v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = 0.0;
+        for (int e = 0; e < n; ++e) {
+            const int j = alist[(size_t)e * ntot + hs];
+            const double4 p = a.spos[j];
+            const double fpk = a.sfp[j];
+            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+            double ux, uy, uz;
+            pair_u(b, dx, dy, dz, ux, uy, uz);
+            const double r2 = ux * ux + uy * uy + uz * uz;
+            if (!(r2 < a.rc2)) continue;
+            double r = sqrt(r2);
+            double4 q = pair_funcs(t, r);     // V, V', phi, phi'
+            double rr = 1.0 / r;
+            double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
+            fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+            ef += 0.5 * q.x;
+            ec += 0.5 * fetm_vee(t, r);
+            if (VIR && (ph.w + p.w) > 0.1) {
+                double hf = 0.5 * fpair;
+                v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
+                v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
+                v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
+            }
+        }
+        const int at = a.sorted[hs];
+        fout[3 * (size_t)at] = fx;
+        fout[3 * (size_t)at + 1] = fy;
+        fout[3 * (size_t)at + 2] = fz;
+        en_calc[at] = afrho[at] + ec;
+        en_force[at] = afrho[at] + ef;
+        if (VIR) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
+        }
+    }
 }
 
 // per-system sums of one evaluation: pe (energy_calc), pe (force), virial,
@@ -660,9 +729,12 @@ __global__ void k_unpack(int ntot, const double *__restrict__ X, double *__restr
     x[a] = X[3 * (size_t)a]; y[a] = X[3 * (size_t)a + 1]; z[a] = X[3 * (size_t)a + 2];
 }
 
-__global__ void k_set_active(int nsys, BSys *sys, int v) {
+// marks every system active (v) and, with stale, its list invalid
+__global__ void k_set_active(int nsys, BSys *sys, int v, int stale) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < nsys) sys[s].active = v;
+    if (s >= nsys) return;
+    sys[s].active = v;
+    if (stale) sys[s].stale = 1;
 }
 
 }  // namespace
@@ -681,16 +753,18 @@ class BatchEngine {
     HostTables ht;
     Tables tab;
     double rcut = 0.0;
-    bool potential_set = false, state_set = false;
+    double skin = 0.3;                  // list radius rcut + skin (less where a box is too narrow)
+    bool potential_set = false, state_set = false, boxes_set = false, pos_set = false;
     cudaStream_t stream = nullptr;
     // device buffers
     BSys *sys = nullptr;
     int32_t *atom_sys = nullptr, *cell_sys = nullptr, *cell_of = nullptr, *cell_count = nullptr;
     int32_t *cell_start = nullptr, *cursor = nullptr, *sorted = nullptr, *n_active = nullptr;
-    double *X = nullptr, *mass = nullptr, *f = nullptr, *rho = nullptr, *afrho = nullptr, *fp = nullptr;
+    double *X = nullptr, *Xb = nullptr, *mass = nullptr, *f = nullptr, *rho = nullptr, *afrho = nullptr, *fp = nullptr;
     double *en_calc = nullptr, *en_force = nullptr, *vir = nullptr, *sfp = nullptr, *sysout = nullptr;
     double *cgv = nullptr;              // G, D, GS, XX, GG, DR, DGR (3*ntot each)
-    int32_t *alist = nullptr, *pcnt = nullptr, *slot_sys = nullptr, *flags = nullptr;
+    int32_t *alist = nullptr, *pcnt = nullptr, *flags = nullptr;
+    unsigned long long *stats = nullptr;   // system list builds, system evaluations
     int pair_cap = 48;                  // compact-row entries per atom
     double4 *spos = nullptr;
     CgState *cg = nullptr;
@@ -710,10 +784,13 @@ class BatchEngine {
     int set_fetm(int nv, const double *av, const double *rv, int np, const double *ap, const double *rp,
                  int nlookup);
     int set_state(const double *x0, const double *y0, const double *z0, const double *b0, const double *m);
+    int layout();
+    int set_skin(double sk);
     int get_state(double *x0, double *y0, double *z0);
     int force(double *out13);
     int quench(int maxfn, int criterion, double fmax, double *out8);
     int get_array(const double *dev, int stride, double *a, double *b, double *c);
+    int copy_xyz(double *dev, const double *src, double *dst);
     void queue_evaluation(bool with_vir);
     int ready();
     int take_overflow();
@@ -749,9 +826,9 @@ static int balloc(T **p, size_t n, const char *what) {
 BatchEngine::~BatchEngine() {
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
-    void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, mass,
-                    f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
-                    tab_r4f, tab_e2f, stage, alist, pcnt, slot_sys, flags};
+    void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
+                    mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
+                    tab_r4f, tab_e2f, stage, alist, pcnt, flags, stats};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -791,6 +868,7 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCHECK(balloc(&sorted, nt, "sorted"));
     BCHECK(balloc(&n_active, 1, "n_active"));
     BCHECK(balloc(&X, 3 * nt, "X"));
+    BCHECK(balloc(&Xb, 3 * nt, "build positions"));
     BCHECK(balloc(&mass, nt, "mass"));
     BCHECK(balloc(&f, 3 * nt, "f"));
     BCHECK(balloc(&rho, nt, "rho"));
@@ -807,9 +885,10 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCHECK(balloc(&stage, 3 * nt, "staging"));
     BCHECK(balloc(&alist, nt * (size_t)pair_cap, "compact list"));
     BCHECK(balloc(&pcnt, nt, "compact counts"));
-    BCHECK(balloc(&slot_sys, nt, "slot systems"));
     BCHECK(balloc(&flags, 2, "flags"));
     BCUDA(cudaMemset(flags, 0, 2 * sizeof(int32_t)), "flags");
+    BCHECK(balloc(&stats, 2, "list statistics"));
+    BCUDA(cudaMemset(stats, 0, 2 * sizeof(unsigned long long)), "list statistics");
     BCUDA(cudaMallocHost((void **)&host_active, sizeof(int)), "pinned");
     std::vector<int32_t> as(nt);
     for (int s = 0; s < n; ++s)
@@ -834,6 +913,7 @@ int BatchEngine::set_fetm(int nv, const double *av, const double *rv, int np, co
     if (!(r > 0.0) || r > 1e100) return set_last_error(MOLDY_ERR_UNSUPPORTED, "tables without a finite cut");
     rcut = r;
     potential_set = true;
+    if (boxes_set) return layout();
     return MOLDY_OK;
 }
 
@@ -849,9 +929,6 @@ int BatchEngine::set_state(const double *x0, const double *y0, const double *z0,
     }
     if (m) BCUDA(cudaMemcpyAsync(mass, m, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "mass");
     if (b0) {
-        // per-system cell grids: at least rcut wide perpendicular to each face
-        int cell = 0;
-        std::vector<int32_t> csys;
         for (int s = 0; s < nsys; ++s) {
             BSys &S = hsys[s];
             const double *b = b0 + 9 * (size_t)s;
@@ -866,46 +943,89 @@ int BatchEngine::set_state(const double *x0, const double *y0, const double *z0,
                     for (int k = 0; k < 3; ++k) t += b[k + 3 * i] * b[k + 3 * j];
                     S.tg[i + 3 * j] = t;
                 }
-            for (int d = 0; d < 3; ++d) {
-                const double *p = b + 3 * ((d + 1) % 3), *q = b + 3 * ((d + 2) % 3);
-                double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
-                double w = std::fabs(vol) / std::sqrt(cx * cx + cy * cy + cz * cz);
-                if (!(w > 2.0 * rcut))
-                    return set_last_error(MOLDY_ERR_INVALID, "system " + std::to_string(s) +
-                                                                 ": box narrower than twice the interaction range");
-                int nc = (int)std::floor(w / rcut);
-                nc = std::max(1, std::min(nc, 1024));
-                S.nc[d] = nc;
-                S.nst[d] = nc >= 3 ? 3 : nc;
-            }
-            S.atom0 = atom0[s];
-            S.nm = natoms[s];
-            S.cell0 = cell;
-            S.ncell = S.nc[0] * S.nc[1] * S.nc[2];
-            S.active = 1;
-            cell += S.ncell;
-            csys.insert(csys.end(), S.ncell, s);
         }
-        if (cell != ncell) {
-            void *bufs[] = {cell_sys, cell_count, cell_start, cursor};
-            for (void *bp : bufs)
-                if (bp) cudaFree(bp);
-            cell_sys = cell_count = cell_start = cursor = nullptr;
-            ncell = cell;
-            BCHECK(balloc(&cell_sys, ncell, "cell_sys"));
-            BCHECK(balloc(&cell_count, ncell, "cell_count"));
-            BCHECK(balloc(&cell_start, ncell + 1, "cell_start"));
-            BCHECK(balloc(&cursor, ncell, "cursor"));
-            if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
-        }
-        BCUDA(cudaMemcpyAsync(cell_sys, csys.data(), csys.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream),
-              "cell_sys");
-        BCUDA(cudaMemcpyAsync(sys, hsys.data(), nsys * sizeof(BSys), cudaMemcpyHostToDevice, stream), "systems");
-        BCUDA(cudaStreamSynchronize(stream), "set_state");
+        boxes_set = true;
+        BCHECK(layout());
     }
-    if (x0 && y0 && z0 && b0) state_set = true;
+    if (x0 && y0 && z0) pos_set = true;
+    state_set = pos_set && boxes_set;
     BCUDA(cudaStreamSynchronize(stream), "set_state");
     BCUDA(cudaGetLastError(), "set_state");
+    return MOLDY_OK;
+}
+
+// Per-system list radius and cell grid from the boxes: rv = rcut + skin,
+// less where a box is narrower than 2 rv (every pair inside rv must have a
+// unique minimum image), and cells at least rv wide perpendicular to each
+// face.  Every list is marked stale.
+int BatchEngine::layout() {
+    int cell = 0;
+    std::vector<int32_t> csys;
+    for (int s = 0; s < nsys; ++s) {
+        BSys &S = hsys[s];
+        const double *b = S.b0;
+        double w[3];
+        for (int d = 0; d < 3; ++d) {
+            const double *p = b + 3 * ((d + 1) % 3), *q = b + 3 * ((d + 2) % 3);
+            double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
+            w[d] = std::fabs(S.vol) / std::sqrt(cx * cx + cy * cy + cz * cz);
+            if (!(w[d] > 2.0 * rcut))
+                return set_last_error(MOLDY_ERR_INVALID, "system " + std::to_string(s) +
+                                                             ": box narrower than twice the interaction range");
+        }
+        const double wmin = std::min(w[0], std::min(w[1], w[2]));
+        const double rv = std::max(rcut, std::min(rcut + skin, 0.5 * wmin * (1.0 - 1e-9)));
+        const double half = 0.5 * (rv - rcut);
+        S.rv2 = rv * rv;
+        // a small margin keeps rounding in the displacement from hiding a crossing
+        S.hs2 = half * half * (1.0 - 1e-6);
+        for (int d = 0; d < 3; ++d) {
+            int nc = (int)std::floor(w[d] / rv);
+            nc = std::max(1, std::min(nc, 1024));
+            S.nc[d] = nc;
+            S.nst[d] = nc >= 3 ? 3 : nc;
+        }
+        S.atom0 = atom0[s];
+        S.nm = natoms[s];
+        S.cell0 = cell;
+        S.ncell = S.nc[0] * S.nc[1] * S.nc[2];
+        S.active = 1;
+        S.rebuild = 0;
+        S.stale = 1;
+        cell += S.ncell;
+        csys.insert(csys.end(), S.ncell, s);
+    }
+    if (cell != ncell) {
+        void *bufs[] = {cell_sys, cell_count, cell_start, cursor};
+        for (void *bp : bufs)
+            if (bp) cudaFree(bp);
+        cell_sys = cell_count = cell_start = cursor = nullptr;
+        ncell = cell;
+        BCHECK(balloc(&cell_sys, ncell, "cell_sys"));
+        BCHECK(balloc(&cell_count, ncell, "cell_count"));
+        BCHECK(balloc(&cell_start, ncell + 1, "cell_start"));
+        BCHECK(balloc(&cursor, ncell, "cursor"));
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    }
+    BCUDA(cudaMemsetAsync(cell_count, 0, ncell * sizeof(int32_t), stream), "cell_count");
+    // every build writes atom0 as the first slot of a system's first cell, and
+    // the end of a system's last cell is the next system's first slot
+    std::vector<int32_t> cs(ncell + 1, 0);
+    for (int s = 0; s < nsys; ++s) cs[hsys[s].cell0] = atom0[s];
+    cs[ncell] = ntot;
+    BCUDA(cudaMemcpyAsync(cell_start, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream),
+          "cell_start");
+    BCUDA(cudaMemcpyAsync(cell_sys, csys.data(), csys.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream),
+          "cell_sys");
+    BCUDA(cudaMemcpyAsync(sys, hsys.data(), nsys * sizeof(BSys), cudaMemcpyHostToDevice, stream), "systems");
+    BCUDA(cudaStreamSynchronize(stream), "layout");
+    return MOLDY_OK;
+}
+
+int BatchEngine::set_skin(double sk) {
+    if (!(sk >= 0.0) || sk > 10.0) return set_last_error(MOLDY_ERR_INVALID, "skin must be in [0, 10]");
+    skin = sk;
+    if (boxes_set) return layout();
     return MOLDY_OK;
 }
 
@@ -920,28 +1040,22 @@ static void launch_tiles(const BatchEngine &E, const TileArgs &a, bool with_vir,
     const int nb = (E.ncell + kTileWarps - 1) / kTileWarps;
     const int nbs = grid_blocks(E.ntot, 256);
     k_tile_screen<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.ntot, E.pair_cap, E.alist, E.pcnt, E.flags);
-    const int32_t *nslots = E.cell_start + E.ncell;
-    k_cl_density<<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho, E.afrho,
-                                     E.fp, E.slot_sys);
+    // a system's slots are its atoms' index range, so atom_sys is the slot's system
+    k_cl_density<<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho, E.afrho, E.fp,
+                                     E.atom_sys);
     if (with_vir)
-        k_cl_forces<true><<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.slot_sys,
-                                              E.afrho, E.f, E.en_calc, E.en_force, E.vir);
+        k_cl_forces<true><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys, E.afrho,
+                                              E.f, E.en_calc, E.en_force, E.vir);
     else
-        k_cl_forces<false><<<nbs, 256, 0, s>>>(a, E.tab, nslots, E.ntot, E.pair_cap, E.alist, E.pcnt, E.slot_sys,
-                                               E.afrho, E.f, E.en_calc, E.en_force, E.vir);
+        k_cl_forces<false><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys, E.afrho,
+                                               E.f, E.en_calc, E.en_force, E.vir);
 }
 
-// binning and the two tile passes for the systems marked active
+// list check (and rebuild) and the tile passes for the systems marked active
 void BatchEngine::queue_evaluation(bool with_vir) {
     cudaStream_t s = stream;
-    const int nb = (ntot + 255) / 256, nbc = (ncell + 255) / 256;
-    cudaMemsetAsync(cell_count, 0, sizeof(int32_t) * ncell, s);
-    k_bin<<<nb, 256, 0, s>>>(ntot, X, atom_sys, sys, cell_of, cell_count);
-    launch_exclusive_scan(cell_count, cell_start, ncell, s);
-    cudaMemsetAsync(cursor, 0, sizeof(int32_t) * ncell, s);
-    k_bin_fill<<<nb, 256, 0, s>>>(ntot, cell_of, cell_start, cursor, sorted);
-    k_bin_sort<<<nbc, 256, 0, s>>>(ncell, cell_start, sorted, X, mass, spos);
-    k_slot_sys<<<nb, 256, 0, s>>>(cell_start + ncell, sorted, atom_sys, slot_sys);
+    k_prepare<<<nsys, kPrepThreads, 0, s>>>(sys, X, mass, Xb, cell_of, cell_count, cell_start, cursor, sorted, spos,
+                                           stats);
     TileArgs a;
     a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
     a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
@@ -951,11 +1065,12 @@ void BatchEngine::queue_evaluation(bool with_vir) {
         case 32: launch_tiles<32>(*this, a, with_vir, s); break;
         default: launch_tiles<8>(*this, a, with_vir, s); break;
     }
-    launches += 8;
+    launches += 4;
 }
 
-// compact-row overflow of the last evaluations: grows the rows (the caller
-// evaluates again) and returns the largest row seen, or 0
+// compact-row overflow of the last evaluations: grows the rows, marks every
+// list stale (the caller evaluates again) and returns the largest row seen,
+// or 0
 int BatchEngine::take_overflow() {
     int32_t h[2] = {0, 0};
     if (cudaMemcpy(h, flags, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
@@ -967,13 +1082,15 @@ int BatchEngine::take_overflow() {
     if (balloc(&alist, (size_t)ntot * (size_t)need, "compact list") != MOLDY_OK) return -1;
     pair_cap = need;
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 1);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
     return h[1];
 }
 
 int BatchEngine::force(double *out13) {
     BCHECK(ready());
     for (int attempt = 0;; ++attempt) {
-        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1);
+        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
         queue_evaluation(true);
         k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
         launches += 2;
@@ -1006,6 +1123,19 @@ int BatchEngine::get_array(const double *dev, int stride, double *a, double *b, 
 }
 
 int BatchEngine::get_state(double *x0, double *y0, double *z0) { return get_array(X, 3, x0, y0, z0); }
+
+// interleaved x(3i-2..3i) straight to or from the device arrays
+int BatchEngine::copy_xyz(double *dev, const double *src, double *dst) {
+    const size_t bytes = 3 * (size_t)ntot * sizeof(double);
+    if (src) {
+        BCUDA(cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, stream), "positions");
+        pos_set = true;
+        state_set = pos_set && boxes_set;
+    }
+    if (dst) BCUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, stream), "copy back");
+    BCUDA(cudaStreamSynchronize(stream), "interleaved copy");
+    return MOLDY_OK;
+}
 
 int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
     BCHECK(ready());
@@ -1044,14 +1174,14 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
             return set_last_error(MOLDY_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
         }
         graph_lph = lph; graph_cap = cap; graph_maxfn = maxfn; graph_criterion = criterion; graph_fmax = fmax;
-        launches -= 8;   // captured, not run; counted per replay below
+        launches -= 4;   // captured, not run; counted per replay below
     }
     // VA14CD evaluates at most maxfn times; a few rounds more let every
     // system reach its return
     const int rounds = maxfn + 8;
     for (int r = 0; r < rounds; ++r) {
         BCUDA(cudaGraphLaunch(graph, s), "graph launch");
-        launches += 9;
+        launches += 5;
         if ((r & 7) == 7 || r == rounds - 1) {
             BCUDA(cudaMemcpyAsync(host_active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s), "counter");
             BCUDA(cudaStreamSynchronize(s), "quench");
@@ -1073,7 +1203,7 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
         }
     }
     // leave every system active for later force calls
-    k_set_active<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, sys, 1);
+    k_set_active<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, sys, 1, 0);
     BCUDA(cudaStreamSynchronize(s), "quench");
     int ov = take_overflow();
     if (ov != 0)
@@ -1153,6 +1283,19 @@ int moldy_gpu_batch_get_forces(moldy_batch *h, double *fx, double *fy, double *f
     BTRY(h->e->get_array(h->e->f, 3, fx, fy, fz));
 }
 
+int moldy_gpu_batch_set_positions(moldy_batch *h, const double *xyz) {
+    BGUARD(h);
+    if (!h->e->potential_set) return moldy::set_last_error(MOLDY_ERR_ORDER, "set the potential before the state");
+    if (!xyz) return moldy::set_last_error(MOLDY_ERR_INVALID, "null positions");
+    BTRY(h->e->copy_xyz(h->e->X, xyz, nullptr));
+}
+
+int moldy_gpu_batch_get_forces_xyz(moldy_batch *h, double *fxyz) {
+    BGUARD(h);
+    if (!fxyz) return moldy::set_last_error(MOLDY_ERR_INVALID, "null output");
+    BTRY(h->e->copy_xyz(h->e->f, nullptr, fxyz));
+}
+
 int moldy_gpu_batch_get_energies(moldy_batch *h, double *en_calc, double *en_force) {
     BGUARD(h);
     int rc = h->e->get_array(h->e->en_calc, 1, en_calc, nullptr, nullptr);
@@ -1181,6 +1324,25 @@ int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged) {
         return moldy::set_last_error(MOLDY_ERR_INVALID, "staged candidates out of range");
     h->e->lph = lanes;
     h->e->cap = staged;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_skin(moldy_batch *h, double skin) {
+    BGUARD(h);
+    BTRY(h->e->set_skin(skin));
+}
+
+int moldy_gpu_batch_list_stats(moldy_batch *h, int64_t *out2) {
+    BGUARD(h);
+    if (!out2) return moldy::set_last_error(MOLDY_ERR_INVALID, "null output");
+    unsigned long long v[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(v, h->e->stats, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return moldy::set_last_error(MOLDY_ERR_CUDA, std::string("list statistics: ") + cudaGetErrorString(e));
+    }
+    out2[0] = (int64_t)v[0];
+    out2[1] = (int64_t)v[1];
     return MOLDY_OK;
 }
 

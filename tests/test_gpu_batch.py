@@ -49,14 +49,16 @@ def test_batch_force_matches_oracle(gpu_lib, oracle_mod, tiles):
     b.close()
 
 
-@pytest.mark.parametrize("maxfn", [3, 8, 17])
-def test_batch_quench_path_matches_oracle(gpu_lib, oracle_mod, maxfn):
+@pytest.mark.parametrize("maxfn,skin", [(3, 0.3), (8, 0.3), (17, 0.3), (17, 0.0), (17, 1.0)])
+def test_batch_quench_path_matches_oracle(gpu_lib, oracle_mod, maxfn, skin):
     """The first maxfn function values of VA14CD: with an unreachable force
     bound both the device state machine and the oracle stop at maxfn with
     iflag 1 at the best point so far; f agrees to 1e-11 and the positions to
-    1e-9 A, so both took the same steps."""
+    1e-9 A, so both took the same steps.  Skins 0 (a build at every
+    evaluation), 0.3 and 1 A (lists kept through the line searches)."""
     ws = mixed_systems([4, 5, 6, 4, 7], seed=5)
     b = MoldyBatch.from_workloads(ws)
+    b.set_skin(skin)
     q = b.quench(maxfn=maxfn, criterion=1, fmax=1e-12)
     xs = b.split(b.get_state())
     for s, w in enumerate(ws):
@@ -139,3 +141,70 @@ def test_batch_rejects_narrow_box(gpu_lib):
     w = wl.make_workload(2, sigma=0.0, temperature=0.0, ivol=1)
     with pytest.raises(MoldyError):
         MoldyBatch.from_workloads([w])
+
+
+def test_batch_list_kept_until_half_skin(gpu_lib, oracle_mod):
+    """A system's list is kept while its atoms stay within half the skin of
+    their positions at the last build, and rebuilt (that system alone) once
+    one atom moves farther; the results match the oracle at every step."""
+    ws = mixed_systems([4, 5, 6, 4], seed=21)
+    b = MoldyBatch.from_workloads(ws)
+    b.set_skin(0.4)
+    b.force()
+    assert b.list_stats() == {"builds": 4, "evaluations": 4}
+    rng = np.random.default_rng(4)
+    x0 = [w.x0.copy() for w in ws]
+
+    def move(s, cart):
+        return np.linalg.solve(ws[s].b0, cart.T).T
+
+    # every atom of every system moves by less than 0.15 A: no build
+    xs = [x0[s] + move(s, rng.uniform(-0.08, 0.08, size=(ws[s].nm, 3))) for s in range(4)]
+    b.set_state(np.concatenate(xs))
+    b.force()
+    assert b.list_stats() == {"builds": 4, "evaluations": 8}
+    f = b.split(b.forces())
+    for s, w in enumerate(ws):
+        w2 = w.copy()
+        w2.x0 = xs[s]
+        o, _ = oracle_eval(oracle_mod, w2)
+        assert rel_norm_err(f[s], o.forces()) <= 1e-10, s
+    # one atom of system 2 moves 0.25 A from its built position: that system rebuilds
+    xs[2] = xs[2].copy()
+    xs[2][7] = x0[2][7] + move(2, np.array([[0.25, 0.0, 0.0]]))[0]
+    b.set_state(np.concatenate(xs))
+    out = b.force()
+    assert b.list_stats() == {"builds": 5, "evaluations": 12}
+    f = b.split(b.forces())
+    for s, w in enumerate(ws):
+        w2 = w.copy()
+        w2.x0 = xs[s]
+        o, en = oracle_eval(oracle_mod, w2)
+        assert rel_norm_err(f[s], o.forces()) <= 1e-10, s
+        assert abs(out["pe_calc"][s] - en.sum()) <= 1e-10 * abs(en.sum())
+    # a new box rebuilds every list
+    b.set_state(b0=[w.b0 for w in ws])
+    b.force()
+    assert b.list_stats()["builds"] == 9
+    b.close()
+
+
+def test_batch_interleaved_copies(gpu_lib):
+    """set_positions / forces_xyz_into carry the same numbers as the
+    per-component calls."""
+    ws = mixed_systems([4, 5], seed=2)
+    b = MoldyBatch.from_workloads(ws)
+    b.force()
+    f1 = b.forces()
+    x = np.ascontiguousarray(np.concatenate([w.x0 for w in ws]))
+    x[3] += 1e-3
+    b.set_positions(x)
+    assert np.array_equal(b.get_state(), x)
+    b.force()
+    f2 = np.empty_like(f1)
+    b.forces_xyz_into(f2)
+    assert np.array_equal(f2, b.forces())
+    assert not np.array_equal(f1, f2)
+    with pytest.raises(ValueError):
+        b.set_positions(x[:, :2])
+    b.close()
