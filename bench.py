@@ -55,6 +55,7 @@ def parse_args():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--nve-steps", type=int, default=1000)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-quench", action="store_true", help="batch: skip the quench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0)
@@ -530,6 +531,11 @@ def run_batch(args):
         return float(t.item())
 
     boxes = [w.b0 for w in ws]
+    raw = np.zeros(13 * len(ws))
+
+    def force():
+        # the C-ABI call with its preallocated result array (no Python post-processing)
+        b.force_into(raw)
 
     def build_and_force():
         b.set_state(b0=boxes)          # new boxes: every list is built at the next evaluation
@@ -544,6 +550,8 @@ def run_batch(args):
 
     # untimed: choose the tile shape (lanes per home atom) on evaluations that
     # build every list
+    prec = "fp64" if args.precision == "fp64" else "mixed"
+    b.set_precision(prec)
     tune = {}
     for lanes in (4, 8, 16, 32):
         b.set_tiles(lanes, 256)
@@ -551,6 +559,17 @@ def run_batch(args):
         tune[lanes] = min(build_and_force() for _ in range(3))
     best = min(tune, key=tune.get)
     b.set_tiles(best, 256)
+    # untimed: row entries gathered at a time by the per-atom passes, per precision
+    gather_ms, best_gather = {}, {}
+    for p in ("fp64", "mixed"):
+        b.set_precision(p)
+        for g in (1, 2, 4):
+            b.set_gather(g)
+            b.force()
+            gather_ms[f"{p}/{g}"] = timed(force, 5)
+        best_gather[p] = min((1, 2, 4), key=lambda g: gather_ms[f"{p}/{g}"])
+    b.set_precision(prec)
+    b.set_gather(best_gather[prec])
     for _ in range(max(args.warmup, 3)):
         b.force()
     # evaluations with every list current (the positions do not move between
@@ -560,7 +579,7 @@ def run_batch(args):
     with ClockSampler(local_rank) as clk:
         if world > 1:
             torch.distributed.barrier()
-        ms = timed(b.force, steps)
+        ms = timed(force, steps)
         if world > 1:
             torch.distributed.barrier()
     ms_max = max_over_ranks(ms)
@@ -568,6 +587,32 @@ def run_batch(args):
     ntot_all = sum(w.nm for w in ws_all)
     value = ntot_all / (ms_max / 1000.0)
     build_ms = max_over_ranks(float(np.median([build_and_force() for _ in range(5)])))
+
+    # the other precision on the same lists, and the mixed path's errors
+    # against the FP64 path (real forces, energy_calc energy per atom, stress)
+    def snapshot():
+        out = b.force()
+        return b.split(b.forces()), out
+    other = "fp64" if prec == "mixed" else "mixed"
+    b.set_precision(other)
+    b.set_gather(best_gather[other])
+    b.force()
+    other_ms = max_over_ranks(timed(force, min(steps, 50)))
+    res = {p_: None for p_ in ("fp64", "mixed")}
+    res[other] = snapshot()
+    b.set_precision(prec)
+    b.set_gather(best_gather[prec])
+    res[prec] = snapshot()
+    (f64, o64), (fmx, omx) = res["fp64"], res["mixed"]
+    d = np.concatenate([(x - y) @ w.b0.T for w, x, y in zip(ws, fmx, f64)])
+    accuracy = {
+        "vs": "FP64 GPU path (bit-matched to the oracle at 1e-10)",
+        "force_rms_eV_per_A": float(np.sqrt(np.mean(np.sum(d * d, axis=1)))),
+        "force_max_eV_per_A": float(np.max(np.linalg.norm(d, axis=1))),
+        "pe_calc_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe_calc"] - o64["pe_calc"]) / b.natoms)),
+        "pe_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe"] - o64["pe"]) / b.natoms)),
+        "stress_max_abs_GPa": float(np.max(np.abs(omx["tp"] - o64["tp"]) / o64["vol"][:, None, None]) * 160.2176),
+    }
 
     # end to end: positions from pinned host memory, one evaluation, forces and
     # per-system results back, every step
@@ -578,12 +623,14 @@ def run_batch(args):
 
     def e2e_step():
         b.set_positions(x)
-        b.force()
+        force()
         b.forces_xyz_into(fxyz)
 
-    e2e_ms = max_over_ranks(timed(e2e_step, min(steps, 20)))
-    h2d = 24 * b.ntot
-    d2h = 24 * b.ntot + 104 * len(ws)
+    e2e = None
+    if not args.no_e2e:
+        e2e_ms = max_over_ranks(timed(e2e_step, min(steps, 20)))
+        e2e = {"value": ntot_all / (e2e_ms / 1000.0), "unit": "atom-evals/s", "h2d_bytes_per_step": 24 * b.ntot,
+               "d2h_bytes_per_step": 24 * b.ntot + 104 * len(ws), "ms": e2e_ms}
 
     # the quench of every supercell to max |F| <= 1e-4 eV/A (criterion of the
     # benchmark) from the starting positions; untimed sweep of the list skin,
@@ -603,19 +650,26 @@ def run_batch(args):
         return q, max_over_ranks(e0.elapsed_time(e1)), st1["builds"] - st0["builds"], \
             st1["evaluations"] - st0["evaluations"]
 
-    skin_ms = {}
-    for sk in (0.0, 0.3, 0.6):
-        skin_ms[sk] = run_quench(sk)[1]
-    best_skin = min(skin_ms, key=skin_ms.get)
-    q, qms, qbuilds, qevals = run_quench(best_skin)
-    rounds = int(q["nfev"].max())
-    quench = {"seconds": qms / 1000.0, "systems": int(len(ws_all)), "converged": int((q["iflag"] == 0).sum()),
-              "cg_error_returns": int((q["iflag"] == 2).sum()), "max_function_values": rounds,
-              "median_function_values": float(np.median(q["nfev"])),
-              "systems_per_s": len(ws_all) / (qms / 1000.0),
-              "atom_evals_per_s": float((q["nfev"] * b.natoms).sum()) * world / (qms / 1000.0),
-              "max_force_eV_per_A": float(q["fmax"].max()), "skin_A": best_skin, "skin_sweep_ms": skin_ms,
-              "list_builds_per_system_evaluation": qbuilds / max(qevals, 1)}
+    quench = None
+    if not args.no_quench:
+        skin_ms = {}
+        b.set_gather(best_gather["fp64"])
+        for sk in (0.0, 0.3, 0.6):
+            skin_ms[sk] = run_quench(sk)[1]
+        best_skin = min(skin_ms, key=skin_ms.get)
+        # the quench evaluates in FP64 (its line search compares energies below
+        # FP32 resolution) with the FP64 passes' best gather
+        q, qms, qbuilds, qevals = run_quench(best_skin)
+        b.set_gather(best_gather[prec])
+        rounds = int(q["nfev"].max())
+        quench = {"seconds": qms / 1000.0, "systems": int(len(ws_all)), "converged": int((q["iflag"] == 0).sum()),
+                  "cg_error_returns": int((q["iflag"] == 2).sum()), "max_function_values": rounds,
+                  "median_function_values": float(np.median(q["nfev"])),
+                  "systems_per_s": len(ws_all) / (qms / 1000.0),
+                  "atom_evals_per_s": float((q["nfev"] * b.natoms).sum()) * world / (qms / 1000.0),
+                  "max_force_eV_per_A": float(q["fmax"].max()), "skin_A": best_skin, "skin_sweep_ms": skin_ms,
+                  "list_builds_per_system_evaluation": qbuilds / max(qevals, 1),
+                  "precision": "fp64 (line search needs it; force() runs " + prec + ")"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = batch_cpu_baseline(ws_all, args.cpu_seconds)
@@ -626,18 +680,20 @@ def run_batch(args):
     line = {
         "metric": BATCH_METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": world, "steps": steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_max, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 arithmetic / f64 accumulate" if prec == "mixed" else "f64",
         "data": "synthetic (seeded strained bcc Fe supercells, Gaussian displacements 0.1 A)",
         "config": {"workload": f"{len(ws_all)} bcc Fe supercells, n ~ U{{4..16}}, strain +/-2%",
                    "atoms": ntot_all, "tile_lanes_per_atom": best, "tile_autotune_ms": tune,
                    "timed_step": "one evaluation of every system with its list current",
+                   "precision": prec, "gather_tune_ms": gather_ms, "gather": best_gather[prec],
+                   f"{other}_ms_per_step": other_ms,
                    "evaluation_with_every_list_built_ms": build_ms,
                    "parallelism": f"supercells sharded over {world} rank(s) by atom count",
                    "l2": "per-evaluation working set (positions, cell order, forces, energies, virial) "
                          "> 126 MB L2"},
-        "e2e": {"value": ntot_all / (e2e_ms / 1000.0), "unit": "atom-evals/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms": e2e_ms},
-        "quench": quench, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+        "e2e": e2e,
+        "quench": quench, "accuracy": accuracy, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
     return 0

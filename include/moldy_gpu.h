@@ -317,6 +317,16 @@ int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, dou
  * candidates a warp stages in shared memory (0..256, default 256; the rest are
  * read from global memory). */
 int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
+/* Precision of the per-atom density and force passes of moldy_gpu_batch_force:
+ * 0 all FP64 (default); 1 mixed: separations, distances, table interpolation
+ * and pair forces in FP32 from FP64 position differences, every sum in FP64,
+ * and energy_calc's exact pair energy at the FP64 distance.  The quench always
+ * evaluates in FP64: its line search compares energies that differ in the
+ * seventh digit, below what FP32 distances resolve. */
+int moldy_gpu_batch_set_precision(moldy_batch *h, int32_t mixed);
+/* Row entries one thread gathers before it evaluates them in the per-atom
+ * passes: 1, 2 or 4 (default 4).  Results do not depend on it. */
+int moldy_gpu_batch_set_gather(moldy_batch *h, int32_t entries);
 /* Verlet skin of the per-system lists (default 0.3 A): a system's list holds
  * the pairs within rcut + skin (less where its box is narrower than twice
  * that) and is rebuilt once one of its atoms has moved more than half the

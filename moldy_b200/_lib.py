@@ -122,6 +122,8 @@ SIGNATURES = {
     "moldy_gpu_batch_quench": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, D],
     "moldy_gpu_batch_set_tiles": [H, ctypes.c_int32, ctypes.c_int32],
     "moldy_gpu_batch_set_skin": [H, ctypes.c_double],
+    "moldy_gpu_batch_set_precision": [H, ctypes.c_int32],
+    "moldy_gpu_batch_set_gather": [H, ctypes.c_int32],
     "moldy_gpu_batch_list_stats": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_get_stream": [H, ctypes.POINTER(ctypes.c_void_p)],

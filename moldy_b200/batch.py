@@ -104,6 +104,15 @@ class MoldyBatch:
         return {"pe_calc": o[:, 0].copy(), "pe": o[:, 1].copy(), "fmax": o[:, 2].copy(), "vol": o[:, 3].copy(),
                 "tp": np.stack([_mat_from_f(o[s, 4:13]) for s in range(self.nsys)])}
 
+    def force_into(self, out):
+        """One evaluation of every system with its per-system results written
+        raw into a preallocated contiguous float64 array of 13 * nsys: pe_calc,
+        pe, fmax, vol and tp (column-major 3x3) per system."""
+        if not isinstance(out, np.ndarray) or out.dtype != np.float64 or not out.flags.c_contiguous \
+                or out.size != 13 * self.nsys:
+            raise ValueError("needs a contiguous float64 array of 13 * nsys")
+        check(self._L.moldy_gpu_batch_force(self._h, _dp(out)))
+
     def forces(self) -> np.ndarray:
         c = [np.zeros(self.ntot) for _ in range(3)]
         check(self._L.moldy_gpu_batch_get_forces(self._h, *[_dp(a) for a in c]))
@@ -138,6 +147,18 @@ class MoldyBatch:
 
     def set_tiles(self, lanes=8, staged=256):
         check(self._L.moldy_gpu_batch_set_tiles(self._h, int(lanes), int(staged)))
+
+    def set_precision(self, precision="fp64"):
+        """"fp64" or "mixed" (FP32 separations, tables and pair forces, FP64
+        sums) for the density and force passes of :meth:`force`.  The quench
+        always evaluates in FP64, as its line search needs."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision is 'fp64' or 'mixed'")
+        check(self._L.moldy_gpu_batch_set_precision(self._h, 1 if precision == "mixed" else 0))
+
+    def set_gather(self, entries=4):
+        """Row entries a thread gathers at a time in the per-atom passes (1, 2, 4)."""
+        check(self._L.moldy_gpu_batch_set_gather(self._h, int(entries)))
 
     def set_skin(self, skin=0.3):
         """Verlet skin of the per-system lists (A); 0 rebuilds whenever an atom moved."""

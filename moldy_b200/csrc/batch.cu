@@ -21,6 +21,10 @@
 // row and keep the pairs inside rc.  Each pair is evaluated from both ends, so
 // there are no atomics and every sum has a fixed order.
 //
+// Tables.  The batch always runs in lookup mode (uselookup = .true.): the
+// passes interpolate the tables directly; energy_calc's exact pair function
+// is the one analytic evaluation.
+//
 // Pairs.  The reference sums over its Verlet list (pairs within rnear at the
 // last rebuild); every pair beyond the table cut contributes exactly zero, so
 // a complete set of the pairs inside the cut gives the same sums.  A pair
@@ -44,7 +48,7 @@ namespace {
 
 constexpr int kTileWarps = 4;     // cells (warps) per block
 constexpr int kTileCap = 256;     // staged candidates per warp
-constexpr int kCgThreads = 256;   // control block
+constexpr int kCgThreads = 512;   // control block
 constexpr int kPrepThreads = 256; // list check and binning block
 
 struct BSys {
@@ -198,9 +202,11 @@ __global__ void __launch_bounds__(kPrepThreads)
 k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__restrict__ mass,
           double *__restrict__ Xb, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
           int32_t *__restrict__ cell_start, int32_t *__restrict__ cursor, int32_t *__restrict__ sorted,
-          double4 *__restrict__ spos, unsigned long long *__restrict__ stats) {
+          double4 *__restrict__ spos, unsigned long long *__restrict__ stats, int32_t *__restrict__ todo,
+          int32_t *__restrict__ ntodo) {
     __shared__ double sh[33];
     __shared__ int wsum[kPrepThreads / 32];
+    __shared__ int todo0;
     BSys &S = sys[blockIdx.x];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
     if (!S.active) {
@@ -224,7 +230,10 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
         S.rebuild = rebuild;
         S.stale = 0;
         atomicAdd(&stats[1], 1ULL);
-        if (rebuild) atomicAdd(&stats[0], 1ULL);
+        if (rebuild) {
+            atomicAdd(&stats[0], 1ULL);
+            todo0 = atomicAdd(ntodo, S.ncell);
+        }
     }
     if (rebuild) {
         for (int i = tid; i < nm; i += nt) {
@@ -277,9 +286,10 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
             sorted[cell_start[c] + atomicAdd(&cursor[c], 1)] = a;
         }
         __syncthreads();
-        // ascending atom order inside each cell
+        // ascending atom order inside each cell; the cells join the tile screen's work
         for (int cl = tid; cl < S.ncell; cl += nt) {
             const int c = S.cell0 + cl;
+            todo[todo0 + cl] = c;
             const int s0 = cell_start[c], s1 = cl + 1 < S.ncell ? cell_start[c + 1] : a0 + nm;
             for (int i = s0 + 1; i < s1; ++i) {
                 const int v = sorted[i];
@@ -306,88 +316,140 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
 template <int LPH>
 __global__ void __launch_bounds__(32 * kTileWarps)
 k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, int32_t *__restrict__ cnt_out,
-              int32_t *__restrict__ flags) {
+              int32_t *__restrict__ flags, const int32_t *__restrict__ todo, const int32_t *__restrict__ ntodo) {
     __shared__ double4 tpos[kTileWarps][kTileCap];
     __shared__ int tidx[kTileWarps][kTileCap];
     __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * kTileWarps + w;
-    if (c >= a.ncell) return;
-    const BSys &S = a.sys[a.cell_sys[c]];
-    if (!S.rebuild) return;
-    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
-    if (h1 == h0) return;
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
-    const double rv2 = S.rv2;
-    const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
     const int g = lane / LPH, gl = lane % LPH;
     const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
     const unsigned below = (1u << lane) - 1u;
+    const int nwork = *ntodo;
     int overflow = 0;
-    for (int hb = h0; hb < h1; hb += 32 / LPH) {
-        const int hs = hb + g;
-        const bool live = hs < h1;
-        const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
-        int cnt = 0;
-        // every lane of the warp runs the same number of rounds (ballots are warp-wide)
-        for (int k0 = 0; k0 < total; k0 += LPH) {
-            const int k = k0 + gl;
-            bool hit = false;
-            int slot = -1;
-            if (live && k < total) {
-                double4 p; double fpk;
-                candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
-                if (slot != hs) {
-                    double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-                    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-                    double ux, uy, uz;
-                    pair_u(b, dx, dy, dz, ux, uy, uz);
-                    hit = (ux * ux + uy * uy + uz * uz) < rv2;
+    // one warp per cell of the rebuilt systems (warp-uniform loop)
+    for (int t = blockIdx.x * kTileWarps + w; t < nwork; t += gridDim.x * kTileWarps) {
+        const int c = todo[t];
+        const BSys &S = a.sys[a.cell_sys[c]];
+        const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
+        if (h1 == h0) continue;
+        double b[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
+        const double rv2 = S.rv2;
+        const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
+        for (int hb = h0; hb < h1; hb += 32 / LPH) {
+            const int hs = hb + g;
+            const bool live = hs < h1;
+            const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
+            int cnt = 0;
+            // every lane of the warp runs the same number of rounds (ballots are warp-wide)
+            for (int k0 = 0; k0 < total; k0 += LPH) {
+                const int k = k0 + gl;
+                bool hit = false;
+                int slot = -1;
+                if (live && k < total) {
+                    double4 p; double fpk;
+                    candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
+                    if (slot != hs) {
+                        double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                        dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                        double ux, uy, uz;
+                        pair_u(b, dx, dy, dz, ux, uy, uz);
+                        hit = (ux * ux + uy * uy + uz * uz) < rv2;
+                    }
                 }
+                const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
+                if (hit) {
+                    const int e = cnt + __popc(m & below);
+                    if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
+                }
+                cnt += __popc(m);
             }
-            const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
-            if (hit) {
-                const int e = cnt + __popc(m & below);
-                if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
+            if (live && gl == 0) {
+                cnt_out[hs] = cnt;
+                if (cnt > pair_cap) overflow = max(overflow, cnt);
             }
-            cnt += __popc(m);
         }
-        if (live && gl == 0) {
-            cnt_out[hs] = cnt;
-            if (cnt > pair_cap) overflow = max(overflow, cnt);
-        }
+        __syncwarp();   // the next cell restages the warp's tile
     }
     if (overflow) { atomicExch(&flags[0], 1); atomicMax(&flags[1], overflow); }
 }
 
+__device__ __forceinline__ void pair_uf(const float *b, float dx, float dy, float dz, float &ux, float &uy,
+                                        float &uz) {
+    ux = b[0] * dx + b[3] * dy + b[6] * dz;
+    uy = b[1] * dx + b[4] * dy + b[7] * dz;
+    uz = b[2] * dx + b[5] * dy + b[8] * dz;
+}
+
+// fractional difference to the nearest image (round is Fortran NINT)
+__device__ __forceinline__ void frac_diff(const double4 &p, const double4 &q, double &dx, double &dy, double &dz) {
+    dx = p.x - q.x; dy = p.y - q.y; dz = p.z - q.z;
+    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+}
+
 // rho_i over the pairs of the compact row inside rc (rhoset), then F and F'
-// (embed, src/potential_m.F90:148-169); one thread per atom in cell order
+// (embed, src/potential_m.F90:148-169), and the atom's energy_calc energy
+// F + sum V_src/2 with the exact pair function at the FP64 distance
+// (src/dynamics_m.F90:412-483); one thread per atom in cell order, which
+// gathers B row entries before it evaluates them.  MIXED takes rho's
+// separation B0 d, distance and table interpolation in FP32 from the FP64
+// difference and sums rho_i in FP64.  Entries are summed in row order at
+// every B.
+template <bool MIXED, int B>
 __global__ void __launch_bounds__(256)
 k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
              const int32_t *__restrict__ cnt, double *__restrict__ sfp, double *__restrict__ rho_out,
-             double *__restrict__ afrho_out, double *__restrict__ fp_out, const int32_t *__restrict__ slot_sys) {
+             double *__restrict__ afrho_out, double *__restrict__ fp_out, double *__restrict__ en_calc,
+             const int32_t *__restrict__ slot_sys, int32_t *__restrict__ ntodo) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *ntodo = 0;   // the tile screen before this pass has read it
+    const float rc2f = (float)a.rc2;
     for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
         const BSys &S = a.sys[slot_sys[hs]];
         if (!S.active) continue;
-        const double *b = S.b0;
+        double b[9];
+        float bf[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { b[k] = S.b0[k]; bf[k] = (float)b[k]; }
         const double4 ph = a.spos[hs];
         int n = cnt[hs];
         n = n < pair_cap ? n : pair_cap;
-        double rho = 0.0;
-        for (int e = 0; e < n; ++e) {
-            const double4 p = a.spos[alist[(size_t)e * ntot + hs]];
-            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-            double ux, uy, uz;
-            pair_u(b, dx, dy, dz, ux, uy, uz);
-            const double r2 = ux * ux + uy * uy + uz * uz;
-            if (r2 < a.rc2) rho += density_func(t, sqrt(r2));
+        double rho = 0.0, ec = 0.0;
+        for (int e0 = 0; e0 < n; e0 += B) {
+            int jj[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) jj[u] = e0 + u < n ? alist[(size_t)(e0 + u) * ntot + hs] : hs;
+            double4 pp[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) pp[u] = a.spos[jj[u]];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                if (e0 + u >= n) continue;
+                double dx, dy, dz;
+                frac_diff(ph, pp[u], dx, dy, dz);
+                if (MIXED) {
+                    float ux, uy, uz;
+                    pair_uf(bf, (float)dx, (float)dy, (float)dz, ux, uy, uz);
+                    const float r2 = ux * ux + uy * uy + uz * uz;
+                    if (!(r2 < rc2f)) continue;
+                    rho += (double)lookup_phif(t, sqrtf(r2));
+                    double vx, vy, vz;
+                    pair_u(b, dx, dy, dz, vx, vy, vz);
+                    ec += 0.5 * fetm_vee(t, sqrt(vx * vx + vy * vy + vz * vz));
+                } else {
+                    double ux, uy, uz;
+                    pair_u(b, dx, dy, dz, ux, uy, uz);
+                    const double r2 = ux * ux + uy * uy + uz * uz;
+                    if (!(r2 < a.rc2)) continue;
+                    const double r = sqrt(r2);
+                    rho += lookup_phi(t, r);
+                    ec += 0.5 * fetm_vee(t, r);
+                }
+            }
         }
         double f = 0.0, fd = 0.0;
         if (rho > 1e-40) {
-            double2 e2 = embed_funcs(t, rho);
+            double2 e2 = lookup_e2(t, rho);
             f = e2.x; fd = e2.y;
         }
         sfp[hs] = fd;
@@ -395,64 +457,89 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
         rho_out[at] = rho;
         afrho_out[at] = f;
         fp_out[at] = fd;
+        en_calc[at] = f + ec;
     }
 }
 
 // Forces on each atom (the pair loop of force(), src/dynamics_m.F90:232-318),
-// its energy_calc energy F + sum V_src/2 (src/dynamics_m.F90:412-483), the
-// force-routine energy F + sum V/2, and with VIR the per-atom virial
-// sum u d^T fp / 2 over pairs with m_i + m_j > 0.1; one thread per atom.
-template <bool VIR>
+// its force-routine energy F + sum V/2, and with VIR the symmetric per-atom
+// moment S = sum d d^T fp / 2 over pairs with m_i + m_j > 0.1 (stored xx, yy,
+// zz, xy, xz, yz), from which the virial sum (B0 d) d^T fp / 2 is B0 S; one
+// thread per atom, B row entries gathered at a time.  MIXED takes the
+// separation, the table interpolation and the pair force in FP32 and sums in
+// FP64.
+template <bool MIXED, int B, bool VIR>
 __global__ void __launch_bounds__(256)
 k_cl_forces(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
             const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ afrho,
-            double *__restrict__ fout, double *__restrict__ en_calc, double *__restrict__ en_force,
-            double *__restrict__ vir) {
+            double *__restrict__ fout, double *__restrict__ en_force, double *__restrict__ vir) {
+    const float rc2f = (float)a.rc2;
     for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
         const BSys &S = a.sys[slot_sys[hs]];
         if (!S.active) continue;
-        const double *b = S.b0;
+        double b[9];
+        float bf[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { b[k] = S.b0[k]; bf[k] = (float)b[k]; }
         const double4 ph = a.spos[hs];
         const double fph = a.sfp[hs];
         int n = cnt[hs];
         n = n < pair_cap ? n : pair_cap;
-        double fx = 0.0, fy = 0.0, fz = 0.0, ec = 0.0, ef = 0.0;
-        double v[9];
+        double fx = 0.0, fy = 0.0, fz = 0.0, ef = 0.0;
+        double v[6];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = 0.0;
-        for (int e = 0; e < n; ++e) {
-            const int j = alist[(size_t)e * ntot + hs];
-            const double4 p = a.spos[j];
-            const double fpk = a.sfp[j];
-            double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-            dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-            double ux, uy, uz;
-            pair_u(b, dx, dy, dz, ux, uy, uz);
-            const double r2 = ux * ux + uy * uy + uz * uz;
-            if (!(r2 < a.rc2)) continue;
-            double r = sqrt(r2);
-            double4 q = pair_funcs(t, r);     // V, V', phi, phi'
-            double rr = 1.0 / r;
-            double fpair = -q.y * rr - (q.w * fph + q.w * fpk) * rr;
-            fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-            ef += 0.5 * q.x;
-            ec += 0.5 * fetm_vee(t, r);
-            if (VIR && (ph.w + p.w) > 0.1) {
-                double hf = 0.5 * fpair;
-                v[0] += ux * dx * hf; v[1] += uy * dx * hf; v[2] += uz * dx * hf;
-                v[3] += ux * dy * hf; v[4] += uy * dy * hf; v[5] += uz * dy * hf;
-                v[6] += ux * dz * hf; v[7] += uy * dz * hf; v[8] += uz * dz * hf;
+        for (int k = 0; k < 6; ++k) v[k] = 0.0;
+        for (int e0 = 0; e0 < n; e0 += B) {
+            int jj[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) jj[u] = e0 + u < n ? alist[(size_t)(e0 + u) * ntot + hs] : hs;
+            double4 pp[B];
+            double fq[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) { pp[u] = a.spos[jj[u]]; fq[u] = a.sfp[jj[u]]; }
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                if (e0 + u >= n) continue;
+                double dx, dy, dz;
+                frac_diff(ph, pp[u], dx, dy, dz);
+                double fpair, vee;
+                if (MIXED) {
+                    float uxf, uyf, uzf;
+                    pair_uf(bf, (float)dx, (float)dy, (float)dz, uxf, uyf, uzf);
+                    const float r2 = uxf * uxf + uyf * uyf + uzf * uzf;
+                    if (!(r2 < rc2f)) continue;
+                    const float r = sqrtf(r2), rr = 1.0f / r;
+                    const float4 q = lookup_r4f(t, r);
+                    fpair = (double)(-(q.y + q.w * ((float)fph + (float)fq[u])) * rr);
+                    vee = (double)q.x;
+                } else {
+                    double ux, uy, uz;
+                    pair_u(b, dx, dy, dz, ux, uy, uz);
+                    const double r2 = ux * ux + uy * uy + uz * uz;
+                    if (!(r2 < a.rc2)) continue;
+                    const double r = sqrt(r2);
+                    const double4 q = lookup_r4(t, r);     // V, V', phi, phi'
+                    const double rr = 1.0 / r;
+                    fpair = -q.y * rr - (q.w * fph + q.w * fq[u]) * rr;
+                    vee = q.x;
+                }
+                fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+                ef += 0.5 * vee;
+                if (VIR && (ph.w + pp[u].w) > 0.1) {
+                    const double hf = 0.5 * fpair;
+                    v[0] += dx * dx * hf; v[1] += dy * dy * hf; v[2] += dz * dz * hf;
+                    v[3] += dx * dy * hf; v[4] += dx * dz * hf; v[5] += dy * dz * hf;
+                }
             }
         }
         const int at = a.sorted[hs];
         fout[3 * (size_t)at] = fx;
         fout[3 * (size_t)at + 1] = fy;
         fout[3 * (size_t)at + 2] = fz;
-        en_calc[at] = afrho[at] + ec;
         en_force[at] = afrho[at] + ef;
         if (VIR) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) vir[9 * (size_t)at + k] = v[k];
+            for (int k = 0; k < 6; ++k) vir[6 * (size_t)at + k] = v[k];
         }
     }
 }
@@ -464,13 +551,13 @@ k_sys_reduce(const BSys *__restrict__ sys, const double *__restrict__ en_calc, c
              const double *__restrict__ vir, const double *__restrict__ f, int with_vir, double *__restrict__ out) {
     __shared__ double sh[33];
     const BSys &S = sys[blockIdx.x];
-    double ec = 0.0, ef = 0.0, fm = 0.0, v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double ec = 0.0, ef = 0.0, fm = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
     for (int i = threadIdx.x; i < S.nm; i += blockDim.x) {
         const int at = S.atom0 + i;
         ec += en_calc[at];
         ef += en_force[at];
         if (with_vir)
-            for (int k = 0; k < 9; ++k) v[k] += vir[9 * (size_t)at + k];
+            for (int k = 0; k < 6; ++k) v[k] += vir[6 * (size_t)at + k];
         double gx = f[3 * (size_t)at], gy = f[3 * (size_t)at + 1], gz = f[3 * (size_t)at + 2];
         double rx, ry, rz;
         pair_u(S.b0, gx, gy, gz, rx, ry, rz);
@@ -481,7 +568,13 @@ k_sys_reduce(const BSys *__restrict__ sys, const double *__restrict__ en_calc, c
     o[1] = block_sum(ef, sh);
     o[2] = block_max(fm, sh);
     o[3] = S.vol;
-    for (int k = 0; k < 9; ++k) o[4 + k] = with_vir ? block_sum(v[k], sh) : 0.0;
+    // virial B0 S from the summed symmetric moment S
+    double sm[6];
+    for (int k = 0; k < 6; ++k) sm[k] = with_vir ? block_sum(v[k], sh) : 0.0;
+    const double S9[9] = {sm[0], sm[3], sm[4], sm[3], sm[1], sm[5], sm[4], sm[5], sm[2]};   // S(c, b) at c + 3b
+    for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb)
+            o[4 + a + 3 * bb] = S.b0[a] * S9[3 * bb] + S.b0[a + 3] * S9[1 + 3 * bb] + S.b0[a + 6] * S9[2 + 3 * bb];
     if (threadIdx.x == 0)
         for (int k = 0; k < 13; ++k) out[13 * (size_t)blockIdx.x + k] = o[k];
 }
@@ -494,7 +587,8 @@ struct CgVecs {
     double *X, *G, *D, *GS, *XX, *GG, *DR, *DGR;
 };
 
-// One block per system.  On entry after an evaluation it finishes derivs
+// One block per system, the largest systems first (order).  On entry after
+// an evaluation it finishes derivs
 // (pe = sum of energy_calc energies, g = -tg f, f = pe + press vol) and runs
 // VA14CD until it needs the next function value (it then leaves x set and
 // marks the system active) or returns (the system is done).  Scalars are
@@ -503,10 +597,11 @@ struct CgVecs {
 __global__ void __launch_bounds__(kCgThreads)
 k_cg(BSys *__restrict__ sys, CgState *__restrict__ cg, CgVecs v, const double *__restrict__ fvec,
      const double *__restrict__ en_calc, double press, int maxfn, int criterion, double fmax_tol,
-     int *__restrict__ n_active) {
+     int *__restrict__ n_active, const int32_t *__restrict__ order) {
     __shared__ double sh[33];
-    BSys &S = sys[blockIdx.x];
-    CgState st = cg[blockIdx.x];
+    const int sid = order[blockIdx.x];
+    BSys &S = sys[sid];
+    CgState st = cg[sid];
     if (st.done) return;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int n = 3 * S.nm;            // atom variables; the nine box variables stay 0 in g and d
@@ -529,6 +624,7 @@ k_cg(BSys *__restrict__ sys, CgState *__restrict__ cg, CgVecs v, const double *_
         // derivs (src/quench_m.F90:215-313) for the evaluation just made
         double pe = 0.0, fm = 0.0;
         const double *tg = S.tg;
+        #pragma unroll 4
         for (int i = tid; i < S.nm; i += nt) {
             const size_t at = (size_t)S.atom0 + i;
             pe += en_calc[at];
@@ -555,17 +651,20 @@ L30:
     if (++guard > 100000) { st.iflag = 4; goto DONE; }
     if (st.maxfnk >= st.maxfnc) goto L50;
     st.f = st.fmin;
+    #pragma unroll 4
     for (int i = tid; i < n; i += nt) { X[i] = XX[i]; G[i] = GG[i]; }
     __syncthreads();
 L50:
     if (st.iflag > 0) goto DONE;
     if (st.itcrs <= nref) goto L70;
+    #pragma unroll 4
     for (int i = tid; i < n; i += nt) D[i] = -G[i];
     __syncthreads();
 L70:
     st.iterc = st.iterc + 1;
     {
         double s = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) { GS[i] = G[i]; s += D[i] * G[i]; }
         st.dginit = block_sum(s, sh);
     }
@@ -584,6 +683,7 @@ L170:
     c = st.xnew - st.xmin;
     {
         double s = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) {
             X[i] = XX[i] + c * D[i];
             s += fabs(X[i] - XX[i]);
@@ -600,6 +700,7 @@ L190_AFTER:
     if (st.maxfnc <= 1) goto L210;
     {
         double s = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) s += D[i] * G[i];
         st.gnew = block_sum(s, sh);
     }
@@ -610,6 +711,7 @@ L210:
     st.maxfnk = st.maxfnc;
     {
         double s = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) s += G[i] * G[i];
         st.gsumsq = block_sum(s, sh);
     }
@@ -621,6 +723,7 @@ L250:
     goto L30;
 L270:
     if (st.maxfnk < st.maxfnc) goto L300;
+    #pragma unroll 4
     for (int i = tid; i < n; i += nt) { XX[i] = X[i]; GG[i] = G[i]; }
     __syncthreads();
     if (st.maxfnc <= 1) goto L10;
@@ -628,6 +731,7 @@ L270:
     if (st.gm <= st.dginit) goto L310;
     {
         double s = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) s += GS[i] * G[i];
         st.ggstar = block_sum(s, sh);
     }
@@ -675,12 +779,14 @@ L390:
     if (fabs(st.ggstar) >= 0.2 * st.gsumsq) goto L420;
     {
         double s1 = 0.0, s2 = 0.0;
+        #pragma unroll 4
         for (int i = tid; i < n; i += nt) { s1 += GG[i] * DGR[i]; s2 += GG[i] * DR[i]; }
         gamma = block_sum(s1, sh);
         c = block_sum(s2, sh);
     }
     gamma = gamma / st.gamden;
     if (fabs(st.beta * st.gm + gamma * c) >= 0.2 * st.gsumsq) goto L420;
+    #pragma unroll 4
     for (int i = tid; i < n; i += nt) D[i] = -GG[i] + st.beta * D[i] + gamma * DR[i];
     __syncthreads();
     st.itcrs = st.itcrs + 1;
@@ -688,6 +794,7 @@ L390:
 L420:
     st.itcrs = 2;
     st.gamden = st.gm - st.dginit;
+    #pragma unroll 4
     for (int i = tid; i < n; i += nt) {
         DR[i] = D[i];
         DGR[i] = GG[i] - GS[i];
@@ -700,7 +807,7 @@ CALLF:
     __syncthreads();
     if (tid == 0) {
         st.label = 1;
-        cg[blockIdx.x] = st;
+        cg[sid] = st;
         S.active = 1;
         atomicAdd(n_active, 1);
     }
@@ -709,7 +816,7 @@ DONE:
     __syncthreads();
     if (tid == 0) {
         st.done = 1;
-        cg[blockIdx.x] = st;
+        cg[sid] = st;
         S.active = 0;
     }
 }
@@ -746,7 +853,10 @@ class BatchEngine {
   public:
     int nsys = 0, ntot = 0, ncell = 0, device = 0;
     double press = 0.0;
-    int lph = 8;                        // lanes per home atom in the tile passes
+    int lph = 8;                        // lanes per home atom in the tile screen
+    int gather = 4;                     // row entries a thread gathers at a time in the per-atom passes
+    bool mixed = false;                 // FP32 separations, tables and pair forces in the per-atom passes
+    int nsm = 148;
     int cap = kTileCap;                 // staged candidates per warp
     std::vector<int> natoms, atom0;
     std::vector<BSys> hsys;
@@ -765,6 +875,8 @@ class BatchEngine {
     double *cgv = nullptr;              // G, D, GS, XX, GG, DR, DGR (3*ntot each)
     int32_t *alist = nullptr, *pcnt = nullptr, *flags = nullptr;
     unsigned long long *stats = nullptr;   // system list builds, system evaluations
+    int32_t *todo = nullptr, *ntodo = nullptr;   // cells of the systems rebuilt in this evaluation
+    int32_t *cg_order = nullptr;                 // systems by descending size
     int pair_cap = 48;                  // compact-row entries per atom
     double4 *spos = nullptr;
     CgState *cg = nullptr;
@@ -775,7 +887,7 @@ class BatchEngine {
     double *stage = nullptr;            // host-to-device staging (3*ntot)
     int *host_active = nullptr;         // pinned
     cudaGraphExec_t graph = nullptr;
-    int graph_lph = -1, graph_cap = -1, graph_maxfn = -1, graph_criterion = -1;
+    int graph_lph = -1, graph_cap = -1, graph_maxfn = -1, graph_criterion = -1, graph_gather = -1;
     double graph_fmax = -1.0;
     long long launches = 0;
 
@@ -791,7 +903,7 @@ class BatchEngine {
     int quench(int maxfn, int criterion, double fmax, double *out8);
     int get_array(const double *dev, int stride, double *a, double *b, double *c);
     int copy_xyz(double *dev, const double *src, double *dst);
-    void queue_evaluation(bool with_vir);
+    void queue_evaluation(bool with_vir, bool use_mixed);
     int ready();
     int take_overflow();
 };
@@ -828,7 +940,7 @@ BatchEngine::~BatchEngine() {
     if (graph) cudaGraphExecDestroy(graph);
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
                     mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
-                    tab_r4f, tab_e2f, stage, alist, pcnt, flags, stats};
+                    tab_r4f, tab_e2f, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -848,6 +960,7 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCUDA(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
     if (prop.major != 10) return set_last_error(MOLDY_ERR_NO_DEVICE, "kernels are built for sm_100a only");
     device = dev;
+    nsm = prop.multiProcessorCount;
     nsys = n;
     press = p;
     natoms.assign(na, na + n);
@@ -876,7 +989,7 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCHECK(balloc(&fp, nt, "fp"));
     BCHECK(balloc(&en_calc, nt, "en_calc"));
     BCHECK(balloc(&en_force, nt, "en_force"));
-    BCHECK(balloc(&vir, 9 * nt, "virial"));
+    BCHECK(balloc(&vir, 6 * nt, "virial moments"));
     BCHECK(balloc(&sfp, nt, "sfp"));
     BCHECK(balloc(&spos, nt, "spos"));
     BCHECK(balloc(&sysout, 13 * (size_t)n, "system results"));
@@ -888,12 +1001,19 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCHECK(balloc(&flags, 2, "flags"));
     BCUDA(cudaMemset(flags, 0, 2 * sizeof(int32_t)), "flags");
     BCHECK(balloc(&stats, 2, "list statistics"));
+    BCHECK(balloc(&ntodo, 1, "screen work count"));
+    BCUDA(cudaMemset(ntodo, 0, sizeof(int32_t)), "screen work count");
     BCUDA(cudaMemset(stats, 0, 2 * sizeof(unsigned long long)), "list statistics");
     BCUDA(cudaMallocHost((void **)&host_active, sizeof(int)), "pinned");
     std::vector<int32_t> as(nt);
     for (int s = 0; s < n; ++s)
         for (int i = 0; i < na[s]; ++i) as[atom0[s] + i] = s;
     BCUDA(cudaMemcpy(atom_sys, as.data(), nt * sizeof(int32_t), cudaMemcpyHostToDevice), "atom_sys");
+    std::vector<int32_t> ord(n);
+    for (int k = 0; k < n; ++k) ord[k] = k;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return na[x] > na[y]; });
+    BCHECK(balloc(&cg_order, n, "system order"));
+    BCUDA(cudaMemcpy(cg_order, ord.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "system order");
     std::vector<double> m(nt, 55.845);
     BCUDA(cudaMemcpy(mass, m.data(), nt * sizeof(double), cudaMemcpyHostToDevice), "mass");
     hsys.assign(n, BSys());
@@ -996,11 +1116,12 @@ int BatchEngine::layout() {
         csys.insert(csys.end(), S.ncell, s);
     }
     if (cell != ncell) {
-        void *bufs[] = {cell_sys, cell_count, cell_start, cursor};
+        void *bufs[] = {cell_sys, cell_count, cell_start, cursor, todo};
         for (void *bp : bufs)
             if (bp) cudaFree(bp);
-        cell_sys = cell_count = cell_start = cursor = nullptr;
+        cell_sys = cell_count = cell_start = cursor = todo = nullptr;
         ncell = cell;
+        BCHECK(balloc(&todo, ncell, "screen work"));
         BCHECK(balloc(&cell_sys, ncell, "cell_sys"));
         BCHECK(balloc(&cell_count, ncell, "cell_count"));
         BCHECK(balloc(&cell_start, ncell + 1, "cell_start"));
@@ -1036,35 +1157,55 @@ int BatchEngine::ready() {
 }
 
 template <int LPH>
-static void launch_tiles(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
-    const int nb = (E.ncell + kTileWarps - 1) / kTileWarps;
+static void launch_screen(const BatchEngine &E, const TileArgs &a, cudaStream_t s) {
+    // a persistent grid over the cells of the rebuilt systems (6 blocks of
+    // 37 KB shared memory fit one SM)
+    const int nb = std::max(1, std::min((E.ncell + kTileWarps - 1) / kTileWarps, 6 * E.nsm));
+    k_tile_screen<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.ntot, E.pair_cap, E.alist, E.pcnt, E.flags, E.todo,
+                                                     E.ntodo);
+}
+
+template <bool MIXED, int B>
+static void launch_passes(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
     const int nbs = grid_blocks(E.ntot, 256);
-    k_tile_screen<LPH><<<nb, 32 * kTileWarps, 0, s>>>(a, E.ntot, E.pair_cap, E.alist, E.pcnt, E.flags);
     // a system's slots are its atoms' index range, so atom_sys is the slot's system
-    k_cl_density<<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho, E.afrho, E.fp,
-                                     E.atom_sys);
+    k_cl_density<MIXED, B><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho,
+                                               E.afrho, E.fp, E.en_calc, E.atom_sys, E.ntodo);
     if (with_vir)
-        k_cl_forces<true><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys, E.afrho,
-                                              E.f, E.en_calc, E.en_force, E.vir);
+        k_cl_forces<MIXED, B, true><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys,
+                                                        E.afrho, E.f, E.en_force, E.vir);
     else
-        k_cl_forces<false><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys, E.afrho,
-                                               E.f, E.en_calc, E.en_force, E.vir);
+        k_cl_forces<MIXED, B, false><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys,
+                                                         E.afrho, E.f, E.en_force, E.vir);
+}
+
+template <bool MIXED>
+static void launch_passes_b(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
+    switch (E.gather) {
+        case 1: launch_passes<MIXED, 1>(E, a, with_vir, s); break;
+        case 2: launch_passes<MIXED, 2>(E, a, with_vir, s); break;
+        default: launch_passes<MIXED, 4>(E, a, with_vir, s); break;
+    }
 }
 
 // list check (and rebuild) and the tile passes for the systems marked active
-void BatchEngine::queue_evaluation(bool with_vir) {
+void BatchEngine::queue_evaluation(bool with_vir, bool use_mixed) {
     cudaStream_t s = stream;
     k_prepare<<<nsys, kPrepThreads, 0, s>>>(sys, X, mass, Xb, cell_of, cell_count, cell_start, cursor, sorted, spos,
-                                           stats);
+                                           stats, todo, ntodo);
     TileArgs a;
     a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
     a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
     switch (lph) {
-        case 4: launch_tiles<4>(*this, a, with_vir, s); break;
-        case 16: launch_tiles<16>(*this, a, with_vir, s); break;
-        case 32: launch_tiles<32>(*this, a, with_vir, s); break;
-        default: launch_tiles<8>(*this, a, with_vir, s); break;
+        case 4: launch_screen<4>(*this, a, s); break;
+        case 16: launch_screen<16>(*this, a, s); break;
+        case 32: launch_screen<32>(*this, a, s); break;
+        default: launch_screen<8>(*this, a, s); break;
     }
+    if (use_mixed)
+        launch_passes_b<true>(*this, a, with_vir, s);
+    else
+        launch_passes_b<false>(*this, a, with_vir, s);
     launches += 4;
 }
 
@@ -1091,7 +1232,7 @@ int BatchEngine::force(double *out13) {
     BCHECK(ready());
     for (int attempt = 0;; ++attempt) {
         k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
-        queue_evaluation(true);
+        queue_evaluation(true, mixed);
         k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
         launches += 2;
         BCUDA(cudaStreamSynchronize(stream), "batch force");
@@ -1149,17 +1290,22 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
     BCUDA(cudaMemsetAsync(cg, 0, nsys * sizeof(CgState), s), "CG state");
     BCUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s), "counter");
     // first pass: every system asks for its first function value
-    k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active);
+    k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active,
+                                         cg_order);
     launches += 1;
     BCUDA(cudaGetLastError(), "quench start");
     // one round: evaluate the active systems, then advance every state machine
-    if (!graph || graph_lph != lph || graph_cap != cap || graph_maxfn != maxfn || graph_criterion != criterion || graph_fmax != fmax) {
+    if (!graph || graph_lph != lph || graph_cap != cap || graph_maxfn != maxfn || graph_criterion != criterion ||
+        graph_fmax != fmax || graph_gather != gather) {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         cudaGraph_t g = nullptr;
         BCUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
-        queue_evaluation(false);
+        // FP64 passes: the line search compares energies that differ in the
+        // seventh digit, below the rounding of FP32 distances
+        queue_evaluation(false, false);
         cudaMemsetAsync(n_active, 0, sizeof(int), s);
-        k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active);
+        k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active,
+                                         cg_order);
         cudaError_t e = cudaStreamEndCapture(s, &g);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -1174,6 +1320,7 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
             return set_last_error(MOLDY_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
         }
         graph_lph = lph; graph_cap = cap; graph_maxfn = maxfn; graph_criterion = criterion; graph_fmax = fmax;
+        graph_gather = gather;
         launches -= 4;   // captured, not run; counted per replay below
     }
     // VA14CD evaluates at most maxfn times; a few rounds more let every
@@ -1324,6 +1471,21 @@ int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged) {
         return moldy::set_last_error(MOLDY_ERR_INVALID, "staged candidates out of range");
     h->e->lph = lanes;
     h->e->cap = staged;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_precision(moldy_batch *h, int32_t mixed) {
+    BGUARD(h);
+    if (mixed != 0 && mixed != 1) return moldy::set_last_error(MOLDY_ERR_INVALID, "mixed must be 0 or 1");
+    h->e->mixed = mixed == 1;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_gather(moldy_batch *h, int32_t entries) {
+    BGUARD(h);
+    if (entries != 1 && entries != 2 && entries != 4)
+        return moldy::set_last_error(MOLDY_ERR_INVALID, "row entries gathered at a time must be 1, 2 or 4");
+    h->e->gather = entries;
     return MOLDY_OK;
 }
 

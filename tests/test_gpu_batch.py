@@ -207,4 +207,75 @@ def test_batch_interleaved_copies(gpu_lib):
     assert not np.array_equal(f1, f2)
     with pytest.raises(ValueError):
         b.set_positions(x[:, :2])
+    out = b.force()
+    raw = np.zeros(13 * b.nsys)
+    b.force_into(raw)
+    raw = raw.reshape(b.nsys, 13)
+    assert np.array_equal(raw[:, 0], out["pe_calc"]) and np.array_equal(raw[:, 1], out["pe"])
+    assert np.array_equal(raw[:, 4:13].reshape(b.nsys, 3, 3).transpose(0, 2, 1), out["tp"])
     b.close()
+
+
+def test_batch_gather_bit_identical(gpu_lib):
+    """Row entries gathered 1, 2 or 4 at a time are summed in the same order:
+    forces, energies, densities and the per-system virial are bit-identical."""
+    ws = mixed_systems([4, 6, 5], seed=8)
+    b = MoldyBatch.from_workloads(ws)
+    res = []
+    for g in (1, 2, 4):
+        b.set_gather(g)
+        out = b.force()
+        res.append((b.forces(), *b.energies(), b.density()["rho"], out["tp"], out["pe_calc"]))
+    for other in res[1:]:
+        for x, y in zip(res[0], other):
+            assert np.array_equal(x, y)
+    with pytest.raises(Exception):
+        b.set_gather(3)
+    b.close()
+
+
+def real_force_rms(ws, fa, fb):
+    d = np.concatenate([(x - y) @ w.b0.T for w, x, y in zip(ws, fa, fb)])
+    return float(np.sqrt(np.mean(np.sum(d * d, axis=1))))
+
+
+def test_batch_mixed_accuracy(gpu_lib, oracle_mod):
+    """Mixed precision (FP32 separations, tables and pair forces, FP64 sums)
+    against the oracle, at the accuracy gate of the mixed path: real-force RMS
+    error <= 1e-5 eV/A, both energies within 1e-6 eV/atom, rho within 1e-6
+    and the virial within 1e-5 relative.  (An FP32 distance carries about
+    2e-7 A of rounding, which the tables pass on to rho and F(rho).)"""
+    ws = mixed_systems([4, 5, 6, 7, 9], seed=13)
+    b = MoldyBatch.from_workloads(ws)
+    b.set_precision("mixed")
+    for g in (1, 4):
+        b.set_gather(g)
+        out = b.force()
+        f = b.split(b.forces())
+        rho = b.split(b.density()["rho"])
+        fo_all = []
+        for s, w in enumerate(ws):
+            o, en = oracle_eval(oracle_mod, w)
+            fo = o.force_out()
+            fo_all.append(o.forces())
+            assert rel_norm_err(rho[s], o.density()["rho"]) <= 1e-6, s
+            assert abs(out["pe_calc"][s] - en.sum()) <= 1e-6 * w.nm, s
+            assert abs(out["pe"][s] - fo["pe"]) <= 1e-6 * w.nm, s
+            assert rel_norm_err(out["tp"][s], fo["tp"]) <= 1e-5, s
+        assert real_force_rms(ws, f, fo_all) <= 1e-5
+    b.close()
+
+
+def test_batch_quench_stays_fp64(gpu_lib):
+    """The quench evaluates in FP64 whatever force() uses: with mixed
+    precision set, its results are bit-identical to the FP64 quench's."""
+    ws = mixed_systems([4, 5, 6], seed=5)
+    out = []
+    for p in ("fp64", "mixed"):
+        b = MoldyBatch.from_workloads(ws)
+        b.set_precision(p)
+        q = b.quench(maxfn=40, criterion=1, fmax=1e-4)
+        out.append((q["f"], q["nfev"], b.get_state()))
+        b.close()
+    for x, y in zip(*out):
+        assert np.array_equal(x, y)
