@@ -198,7 +198,7 @@ int moldy_gpu_reset_kernel_stats(moldy_gpu *h);
  * family since the last reset; kernel ids are 0 .. MOLDY_KERNEL_FAMILIES-1. */
 int moldy_gpu_kernel_stats(moldy_gpu *h, int32_t kernel, double *total_ms, int64_t *launches);
 const char *moldy_gpu_kernel_name(int32_t kernel);
-#define MOLDY_KERNEL_FAMILIES 15
+#define MOLDY_KERNEL_FAMILIES 16
 
 /* kernel variants (no counterpart in the reference) -------------------------*/
 /* The screening-density pass and the force pass are compiled in
@@ -264,6 +264,32 @@ int moldy_fetm_knot_vjp(int32_t nv, const double *av, const double *rv, int32_t 
                         const double *g_vee, const double *g_dvee, const double *g_phi,
                         const double *g_dphi, const double *g_emb, const double *g_demb,
                         double *g_av, double *g_rv, double *g_ap, double *g_rp);
+
+/* analysis_m::rdf (src/analysis_m.F90:497-760) at the current device state.
+ *
+ * moldy_gpu_rdf: pair-distance histogram hist[(ibin * nspec + si) * nspec + sj]
+ * for ibin = int(r * binsperangstrom) in 0..maxbin (bin 0 holds the pairs the
+ * reference would write out of bounds).  mode 0 bins the half neighbour list
+ * as it stands, pairs with rsq <= (maxbin/binsperangstrom)**2 in integer
+ * division (analysis_m.F90:580-608); mode 1 bins every pair of atoms, the
+ * older form of the routine that wrote the reference's shipped rdf.dat
+ * (every box width must exceed 2 (maxbin+1)/binsperangstrom).  species[nm]
+ * holds each atom's 0-based species index (atomic_index - 1), NULL for one
+ * species; atoms with atomic number 0 are vacancies and are skipped.
+ * natoms[nspec] counts the non-vacancy atoms, *nclose the pairs closer than
+ * 2 A (the routine's warning); either may be NULL.
+ *
+ * moldy_gpu_ackland_jones: per-atom class aj (0 unknown, 1 bcc, 2 fcc, 3 hcp,
+ * 4 icosahedral), coordination nn and, unless NULL, the eight bond-angle
+ * counts chi[8 i + k] (analysis_m.F90:644-757), for neighbours within
+ * rsq <= 1.45 rn[si * nspec + sj]^2 (rn: the fourth-neighbour radii the
+ * routine estimates from the histogram, analysis_m.F90:619-637).  mode 0
+ * takes the full list from the half list, mode 1 every atom.  Fails with
+ * MOLDY_ERR_CAPACITY when an atom has more than 64 such neighbours. */
+int moldy_gpu_rdf(moldy_gpu *h, int32_t mode, int32_t maxbin, int32_t binsperangstrom, const int32_t *species,
+                  int32_t nspec, uint64_t *hist, int64_t *natoms, int64_t *nclose);
+int moldy_gpu_ackland_jones(moldy_gpu *h, int32_t mode, const int32_t *species, int32_t nspec, const double *rn,
+                            int32_t *aj, int32_t *nn, int32_t *chi);
 
 /* batched supercells (no counterpart in the reference's API) ----------------*/
 /* Many independent systems of uneven size (strained or perturbed replicas)

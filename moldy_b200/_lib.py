@@ -108,6 +108,9 @@ SIGNATURES = {
     "moldy_gpu_scalev": [H],
     "moldy_gpu_table_gradients": [H, ctypes.c_double, D, D, D, D, D, D, D, D],
     "moldy_gpu_knot_gradients": [H, ctypes.c_double, D, D, D, D, D, D],
+    "moldy_gpu_rdf": [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, I, ctypes.c_int32,
+                      ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+    "moldy_gpu_ackland_jones": [H, ctypes.c_int32, I, ctypes.c_int32, D, I, I, I],
     "moldy_gpu_batch_create": [ctypes.c_int32, I, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(H)],
     "moldy_gpu_batch_destroy": [H],
     "moldy_gpu_batch_set_fetm_fe": [H, ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32],
@@ -138,7 +141,7 @@ SIGNATURES = {
                                 ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 11,
 }
 NOALLOC_MAX_ATOMS = 262144
-KERNEL_FAMILIES = 15
+KERNEL_FAMILIES = 16
 TUNE_VARIANTS = 8
 _RESTYPE = {"moldy_gpu_last_error": ctypes.c_char_p, "moldy_gpu_version": ctypes.c_char_p,
             "moldy_gpu_kernel_name": ctypes.c_char_p}

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmoldy_gpu.so")
-SOURCES = ["api.cu", "cells.cu", "nlist.cu", "eam.cu", "pairs.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "tables.cpp"]
+SOURCES = ["api.cu", "cells.cu", "nlist.cu", "eam.cu", "pairs.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "rdf.cu", "tables.cpp"]
 HEADERS = ["common.cuh", "engine.h"]
 
 NVCC_FLAGS = [

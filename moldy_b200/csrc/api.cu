@@ -81,7 +81,7 @@ __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__
 // ---------------------------------------------------------------- Profiler --
 const char *const kKernelNames[K_COUNT] = {
     "drift", "linkup", "relink", "build_nlist", "density", "screen_density", "forces",
-    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint", "scalev"};
+    "finalize_force", "mid_list", "therm", "finalize_therm", "energy_calc", "md_init_x2", "adjoint", "scalev", "rdf"};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {
@@ -1121,6 +1121,18 @@ int moldy_gpu_md_steps(moldy_gpu *h, int32_t nsteps, moldy_thermo *thermo) {
 int moldy_gpu_energy_calc(moldy_gpu *h, double *en_atom) { GUARD(h); TRY(h->e->energy_calc(en_atom)); }
 
 int moldy_gpu_synchronize(moldy_gpu *h) { GUARD(h); TRY(h->e->synchronize()); }
+
+int moldy_gpu_rdf(moldy_gpu *h, int32_t mode, int32_t maxbin, int32_t binsperangstrom, const int32_t *species,
+                  int32_t nspec, uint64_t *hist, int64_t *natoms, int64_t *nclose) {
+    GUARD(h);
+    TRY(h->e->rdf(mode, maxbin, binsperangstrom, species, nspec, hist, natoms, nclose));
+}
+
+int moldy_gpu_ackland_jones(moldy_gpu *h, int32_t mode, const int32_t *species, int32_t nspec, const double *rn,
+                            int32_t *aj, int32_t *nn, int32_t *chi) {
+    GUARD(h);
+    TRY(h->e->ackland_jones(mode, species, nspec, rn, aj, nn, chi));
+}
 
 int moldy_gpu_get_stream(moldy_gpu *h, void **stream) {
     GUARD(h);

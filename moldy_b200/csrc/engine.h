@@ -97,7 +97,7 @@ struct HostTables {
 // Kernel families timed by the optional per-kernel CUDA-event profiler.
 enum KernelId {
     K_DRIFT = 0, K_LINKUP, K_RELINK, K_NLIST, K_DENSITY, K_SCREEN, K_PAIR, K_FINALIZE,
-    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_ADJOINT, K_SCALEV, K_COUNT
+    K_MID, K_THERM, K_THERM_FIN, K_ENERGY, K_MDINIT, K_ADJOINT, K_SCALEV, K_RDF, K_COUNT
 };
 extern const char *const kKernelNames[K_COUNT];
 
@@ -158,6 +158,12 @@ class Engine {
     int set_thermostat(double nose, double rqke);
     int get_thermostat(double *out4);
     int scalev();
+    // analysis_m::rdf (src/analysis_m.F90:497-760): pair histogram, then the
+    // Ackland-Jones classification with the fourth-neighbour radii rn
+    int rdf(int mode, int maxbin, int bpa, const int32_t *species, int nspec, uint64_t *hist, int64_t *natoms,
+            int64_t *nclose);
+    int ackland_jones(int mode, const int32_t *species, int nspec, const double *rn, int32_t *aj, int32_t *nn,
+                      int32_t *chi);
     int knot_gradients(double gE, const double *gF, const double *gS, double *g_av, double *g_rv,
                        double *g_ap, double *g_rp);
     void set_ntc(int ntc) { ntc_ = ntc; }

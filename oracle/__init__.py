@@ -33,6 +33,7 @@ _lib = None
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_longlong)
 
 
 def build(force: bool = False) -> str:
@@ -88,6 +89,9 @@ def _load():
         "orc_set_thermostat": (None, [vp, ctypes.c_double, ctypes.c_double]),
         "orc_get_thermostat": (None, [vp, _D]),
         "orc_scalev": (None, [vp]),
+        "orc_rdf": (None, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I, ctypes.c_int, _L, _L, _L]),
+        "orc_rdf_rneighbour": (None, [_L, _L, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]),
+        "orc_ackland_jones": (None, [vp, ctypes.c_int, _I, ctypes.c_int, _D, _I, _I, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -95,6 +99,10 @@ def _load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def _lp(a):
+    return a.ctypes.data_as(_L)
 
 
 def _dp(a):
@@ -316,6 +324,47 @@ class Oracle:
         if st:
             raise RuntimeError(f"oracle quench status {st}")
         return _quench_dict(o)
+
+
+    # analysis_m::rdf ------------------------------------------------------
+    def _spec(self, spec):
+        if spec is None:
+            spec = np.zeros(self.nm, dtype=np.int32)
+        return np.ascontiguousarray(spec, dtype=np.int32)
+
+    def rdf(self, maxbin=500, binsperangstrom=50, mode=0, spec=None, nspec=1):
+        """Pair histogram hist[ibin, si, sj] (ibin 0..maxbin), natoms per
+        species and the count of pairs closer than 2 A.  mode 0: half-list
+        pairs (the current routine); 1: every pair (its older form)."""
+        sp = self._spec(spec)
+        h = np.zeros((maxbin + 1) * nspec * nspec, dtype=np.int64)
+        na = np.zeros(nspec, dtype=np.int64)
+        nc = np.zeros(1, dtype=np.int64)
+        self._lib.orc_rdf(self._h, int(mode), int(maxbin), int(binsperangstrom), _ip(sp), int(nspec), _lp(h),
+                          _lp(na), _lp(nc))
+        return {"hist": h.reshape(maxbin + 1, nspec, nspec), "natoms": na, "nclose": int(nc[0])}
+
+    @staticmethod
+    def rneighbour(hist, natoms, binsperangstrom=50):
+        _load()
+        h = np.ascontiguousarray(hist, dtype=np.int64)
+        nspec = h.shape[1]
+        rn = np.zeros(nspec * nspec)
+        _lib.orc_rdf_rneighbour(_lp(h), _lp(np.ascontiguousarray(natoms, dtype=np.int64)), h.shape[0] - 1,
+                                int(binsperangstrom), nspec, _dp(rn))
+        return rn.reshape(nspec, nspec)
+
+    def ackland_jones(self, rn, mode=0, spec=None):
+        """Per-atom Ackland-Jones class (0 unknown, 1 bcc, 2 fcc, 3 hcp, 4
+        icosahedral), coordination nn and the eight bond-angle counts chi."""
+        sp = self._spec(spec)
+        rn = np.ascontiguousarray(rn, dtype=np.float64)
+        nspec = rn.shape[0]
+        aj = np.zeros(self.nm, dtype=np.int32)
+        nn = np.zeros(self.nm, dtype=np.int32)
+        chi = np.zeros(8 * self.nm, dtype=np.int32)
+        self._lib.orc_ackland_jones(self._h, int(mode), _ip(sp), nspec, _dp(rn), _ip(aj), _ip(nn), _ip(chi))
+        return {"aj": aj, "nn": nn, "chi": chi.reshape(self.nm, 8)}
 
 
 def _quench_dict(o8):

@@ -97,6 +97,14 @@ int orc_quench(orc_sys *s, int maxfn, int criterion, double fmax, double *out8);
 /* one mdloop iteration: velocityverlet, update_therm_avs, thermo, relink.
  * out12 = ke, pe, te, h, th, vol, s1, s2, s3, temperature, boxke, ntc */
 int orc_md_step(orc_sys *s, double *out12);
+/* analysis_m::rdf (src/analysis_m.F90:497-760).  mode 0: half-list pairs;
+ * mode 1: every pair j < i.  spec[nm]: 0-based species index per atom.
+ * hist[((ibin * nspec) + si) * nspec + sj], ibin 0..maxbin. */
+void orc_rdf(const orc_sys *s, int mode, int maxbin, int bpa, const int *spec, int nspec, long long *hist,
+             long long *natoms, long long *nclose);
+void orc_rdf_rneighbour(const long long *hist, const long long *natoms, int maxbin, int bpa, int nspec, double *rn);
+void orc_ackland_jones(const orc_sys *s, int mode, const int *spec, int nspec, const double *rn, int *aj, int *nn,
+                       int *chi);
 
 #ifdef __cplusplus
 }
