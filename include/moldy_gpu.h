@@ -285,7 +285,7 @@ int moldy_fetm_knot_vjp(int32_t nv, const double *av, const double *rv, int32_t 
  * rsq <= 1.45 rn[si * nspec + sj]^2 (rn: the fourth-neighbour radii the
  * routine estimates from the histogram, analysis_m.F90:619-637).  mode 0
  * takes the full list from the half list, mode 1 every atom.  Fails with
- * MOLDY_ERR_CAPACITY when an atom has more than 64 such neighbours. */
+ * MOLDY_ERR_CAPACITY when an atom has more than 32 such neighbours. */
 int moldy_gpu_rdf(moldy_gpu *h, int32_t mode, int32_t maxbin, int32_t binsperangstrom, const int32_t *species,
                   int32_t nspec, uint64_t *hist, int64_t *natoms, int64_t *nclose);
 int moldy_gpu_ackland_jones(moldy_gpu *h, int32_t mode, const int32_t *species, int32_t nspec, const double *rn,

@@ -170,7 +170,7 @@ Engine::~Engine() {
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
                     d.pair_cnt, d.mlist, d.mid_own, d.mid_rev, d.xbuild, d.tab_r4, d.tab_e2,
-                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj};
+                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_box_) cudaFreeHost(host_box_);

@@ -36,6 +36,9 @@ struct DeviceState {
     // neighbour list (neighbourlist_m), entry-major: entry k of atom i at
     // nlist[k*nm + i], 0-based atom ids
     int32_t *nlist = nullptr, *numn = nullptr;
+    // scratch of the structure analysis (rdf.cu), grown on demand
+    void *rdf = nullptr;
+    size_t rdf_bytes = 0;
     // FP32 mirror of the positions (written by drift) for the screening pass
     float4 *posf = nullptr;
     // positions with F'(rho) in w, written by the density pass for the force pass

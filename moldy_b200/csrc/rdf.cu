@@ -32,7 +32,7 @@ namespace moldy {
 namespace {
 
 constexpr int kRdfThreads = 256;
-constexpr int kNearCap = 64;          // neighbours inside the Ackland-Jones cutoff per atom
+constexpr int kNearCap = 32;          // neighbours inside the Ackland-Jones cutoff per atom
 constexpr int kMaxSpecies = 8;
 constexpr int kSmemHistBytes = 48 * 1024;
 
@@ -107,7 +107,10 @@ __device__ void init_block(const HistArgs &a, unsigned int *sh, unsigned int *sc
     __syncthreads();
 }
 
-// mode 0: the half-list rows (src/analysis_m.F90:580-608)
+// mode 0: the half-list rows (src/analysis_m.F90:580-608).  The lanes of a
+// warp walk their rows in step; lanes whose pairs fall in the same bin are
+// grouped with __match_any_sync and one of them adds the group's count, since
+// the pairs of neighbouring atoms crowd into the same few shell bins.
 template <bool SMEM>
 __global__ void __launch_bounds__(kRdfThreads)
 k_rdf_list(HistArgs a, const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn) {
@@ -115,14 +118,50 @@ k_rdf_list(HistArgs a, const int32_t *__restrict__ nlist, const int32_t *__restr
     __shared__ double b[9];
     __shared__ unsigned int sclose, snat[kMaxSpecies];
     init_block<SMEM>(a, sh, &sclose, b, snat);
+    const int lane = threadIdx.x & 31;
     unsigned int close = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nm; i += gridDim.x * blockDim.x) {
-        if (a.znum[i] == 0) continue;
-        atomicAdd(&snat[species_of(a.spec, i)], 1u);
-        const double4 pi = a.pos[i];
-        const int si = species_of(a.spec, i);
-        const int n = numn[i];
-        for (int k = 0; k < n; ++k) bin_pair<SMEM>(a, b, sh, pi, si, nlist[(size_t)k * a.nm + i], true, close);
+    // block-uniform loop: every lane takes part in every __match_any_sync
+    for (int base = blockIdx.x * blockDim.x; base < a.nm; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;
+        const bool live = i < a.nm && a.znum[i] != 0;
+        const int si = live ? species_of(a.spec, i) : 0;
+        if (live) atomicAdd(&snat[si], 1u);
+        const double4 pi = live ? a.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const int n = live ? numn[i] : 0;
+        const int nmax = __reduce_max_sync(0xffffffffu, n);
+        // four row entries gathered before they are evaluated
+        for (int k0 = 0; k0 < nmax; k0 += 4) {
+            int jj[4];
+            double4 pp[4];
+            int zz[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) jj[u] = k0 + u < n ? nlist[(size_t)(k0 + u) * a.nm + i] : -1;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = jj[u] >= 0 ? jj[u] : 0;
+                pp[u] = a.pos[j];
+                zz[u] = a.znum[j];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (k0 + u >= nmax) break;                 // warp-uniform
+                int key = -1;
+                if (jj[u] >= 0 && zz[u] != 0) {
+                    const double rsq = pair_sep2(b, a.ivol, pi, pp[u]);
+                    if (!(rsq > a.rsqmax)) {
+                        const double r = __dsqrt_rn(rsq);
+                        const int ibin = (int)__dmul_rn(r, (double)a.bpa);
+                        if (r <= 2.0) close += 1;
+                        if (ibin <= a.maxbin) key = (ibin * a.nspec + si) * a.nspec + species_of(a.spec, jj[u]);
+                    }
+                }
+                const unsigned int m = __match_any_sync(0xffffffffu, key);
+                if (key >= 0 && lane == __ffs(m) - 1) {
+                    if (SMEM) atomicAdd(&sh[key], (unsigned int)__popc(m));
+                    else atomicAdd(&a.hist[key], (unsigned long long)__popc(m));
+                }
+            }
+        }
     }
     flush_hist<SMEM>(a, sh, close, &sclose, snat);
 }
@@ -210,18 +249,13 @@ struct AjArgs {
     int nm, ivol, nspec;
     double thr[kMaxSpecies * kMaxSpecies];   // 1.45 rn(si,sj)^2 with the single-precision 1.45
     int32_t *ncount, *near;                  // near[i * kNearCap + k]
-    double *nrsq;
     int32_t *flags;                          // [0]: an atom had more than kNearCap neighbours
 };
 
-__device__ __forceinline__ void near_add(const AjArgs &a, int i, int j, double rsq) {
+__device__ __forceinline__ void near_add(const AjArgs &a, int i, int j) {
     const int k = atomicAdd(&a.ncount[i], 1);
-    if (k < kNearCap) {
-        a.near[(size_t)i * kNearCap + k] = j;
-        a.nrsq[(size_t)i * kNearCap + k] = rsq;
-    } else {
-        atomicExch(&a.flags[0], 1);
-    }
+    if (k < kNearCap) a.near[(size_t)i * kNearCap + k] = j;
+    else atomicExch(&a.flags[0], 1);
 }
 
 // mode 0: the full list of analysis_m.F90:562-578 from the half-list rows
@@ -239,8 +273,8 @@ k_aj_near_list(AjArgs a, const int32_t *__restrict__ nlist, const int32_t *__res
             const int sj = species_of(a.spec, j);
             // the same rsq from either end: the image rule and the rounding are symmetric
             const double rsq = pair_sep2(b, a.ivol, pi, a.pos[j]);
-            if (!(rsq > a.thr[si * a.nspec + sj])) near_add(a, i, j, rsq);
-            if (!(rsq > a.thr[sj * a.nspec + si])) near_add(a, j, i, rsq);
+            if (!(rsq > a.thr[si * a.nspec + sj])) near_add(a, i, j);
+            if (!(rsq > a.thr[sj * a.nspec + si])) near_add(a, j, i);
         }
     }
 }
@@ -257,7 +291,7 @@ k_aj_near_all(AjArgs a, Grid g) {
         for_stencil(g, pi, [&](int j) {
             if (j == i) return;
             const double rsq = pair_sep2(b, a.ivol, pi, a.pos[j]);
-            if (!(rsq > a.thr[si * a.nspec + species_of(a.spec, j)])) near_add(a, i, j, rsq);
+            if (!(rsq > a.thr[si * a.nspec + species_of(a.spec, j)])) near_add(a, i, j);
         });
     }
 }
@@ -309,7 +343,10 @@ k_aj_classify(AjArgs a, int32_t *__restrict__ aj, int32_t *__restrict__ nnout, i
         n = n < kNearCap ? n : kNearCap;
         int chi[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         const int32_t *nb = a.near + (size_t)i * kNearCap;
-        const double *nr = a.nrsq + (size_t)i * kNearCap;
+        const double4 pi = a.pos[i];
+        // rsq from the centre, as the routine computes it (x0(i) - x0(j))
+        double nr[kNearCap];
+        for (int p = 0; p < n; ++p) nr[p] = pair_sep2(b, a.ivol, pi, a.pos[nb[p]]);
         for (int p = 0; p < n; ++p) {
             const int j = nb[p];
             const double rsqj = nr[p];
@@ -336,24 +373,6 @@ k_aj_classify(AjArgs a, int32_t *__restrict__ aj, int32_t *__restrict__ nnout, i
 // --------------------------------------------------------------- host side
 namespace {
 
-struct DevBuf {
-    void *p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-};
-
-template <typename T>
-int rdf_alloc(DevBuf &b, size_t n, const char *what) {
-    cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        b.p = nullptr;
-        return set_last_error(MOLDY_ERR_CUDA, std::string("cudaMalloc ") + what + ": " + cudaGetErrorString(e));
-    }
-    return MOLDY_OK;
-}
-
 #define RCHECK(x)                                                             \
     do {                                                                      \
         int rc_ = (x);                                                        \
@@ -368,20 +387,47 @@ int rdf_alloc(DevBuf &b, size_t n, const char *what) {
         }                                                                     \
     } while (0)
 
+// Carves 256-byte aligned pieces out of the engine's analysis scratch.
+struct Carve {
+    size_t off = 0;
+    char *base = nullptr;
+    template <typename T>
+    T *take(size_t n) {
+        off = (off + 255) & ~(size_t)255;
+        T *p = base ? (T *)(base + off) : nullptr;
+        off += std::max<size_t>(n, 1) * sizeof(T);
+        return p;
+    }
+};
+
+int reserve(DeviceState &d, size_t bytes) {
+    if (bytes <= d.rdf_bytes) return MOLDY_OK;
+    if (d.rdf) cudaFree(d.rdf);
+    d.rdf = nullptr;
+    d.rdf_bytes = 0;
+    cudaError_t e = cudaMalloc(&d.rdf, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        d.rdf = nullptr;
+        return set_last_error(MOLDY_ERR_CUDA, std::string("cudaMalloc analysis scratch: ") + cudaGetErrorString(e));
+    }
+    d.rdf_bytes = bytes;
+    return MOLDY_OK;
+}
+
 // Cell grid at least radius/2 wide per direction (5 cells per direction in
 // the stencil, all of them where fewer); every pair inside radius must have
 // one image only, so each box width must exceed 2 radius.
-int build_grid(const double *b0, int nm, const double4 *pos, double radius, cudaStream_t s, Grid &g,
-               DevBuf &start, DevBuf &atoms, DevBuf &scratch) {
-    double vol = b0[0] * (b0[4] * b0[8] - b0[7] * b0[5]) + b0[1] * (b0[5] * b0[6] - b0[3] * b0[8]) +
-                 b0[2] * (b0[3] * b0[7] - b0[4] * b0[6]);
+int grid_shape(const double *b0, double radius, Grid &g) {
+    const double vol = b0[0] * (b0[4] * b0[8] - b0[7] * b0[5]) + b0[1] * (b0[5] * b0[6] - b0[3] * b0[8]) +
+                       b0[2] * (b0[3] * b0[7] - b0[4] * b0[6]);
     long long ncell = 1;
     for (int d = 0; d < 3; ++d) {
         const double *p = b0 + 3 * ((d + 1) % 3), *q = b0 + 3 * ((d + 2) % 3);
         const double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
         const double w = std::fabs(vol) / std::sqrt(cx * cx + cy * cy + cz * cz);
         if (!(w > 2.0 * radius))
-            return set_last_error(MOLDY_ERR_INVALID, "box narrower than twice the largest binned pair distance");
+            return set_last_error(MOLDY_ERR_INVALID, "box narrower than twice the largest pair distance analysed");
         int n = (int)std::floor(w / (0.5 * radius));
         n = std::max(1, std::min(n, 512));
         g.nc[d] = n;
@@ -390,27 +436,42 @@ int build_grid(const double *b0, int nm, const double4 *pos, double radius, cuda
         ncell *= n;
     }
     g.ncell = (int)ncell;
-    RCHECK(rdf_alloc<int32_t>(start, ncell + 1, "RDF cells"));
-    RCHECK(rdf_alloc<int32_t>(atoms, nm, "RDF cell atoms"));
-    RCHECK(rdf_alloc<int32_t>(scratch, (size_t)nm + 2 * ncell, "RDF cell scratch"));
-    int32_t *cell_of = (int32_t *)scratch.p, *count = cell_of + nm, *cursor = count + ncell;
-    RCUDA(cudaMemsetAsync(count, 0, 2 * ncell * sizeof(int32_t), s), "RDF cells");
-    const int nb = (nm + 255) / 256;
-    k_grid_count<<<nb, 256, 0, s>>>(nm, pos, g, cell_of, count);
-    launch_exclusive_scan(count, (int32_t *)start.p, g.ncell, s);
-    k_grid_fill<<<nb, 256, 0, s>>>(nm, cell_of, (const int32_t *)start.p, cursor, (int32_t *)atoms.p);
-    g.start = (const int32_t *)start.p;
-    g.atoms = (const int32_t *)atoms.p;
     return MOLDY_OK;
 }
 
-int upload_species(const int32_t *species, int nm, int nspec, cudaStream_t s, DevBuf &buf) {
-    if (!species) return MOLDY_OK;
-    for (int i = 0; i < nm; ++i)
-        if (species[i] < 0 || species[i] >= nspec)
-            return set_last_error(MOLDY_ERR_INVALID, "species index of atom " + std::to_string(i) + " out of range");
-    RCHECK(rdf_alloc<int32_t>(buf, nm, "species"));
-    RCUDA(cudaMemcpyAsync(buf.p, species, nm * sizeof(int32_t), cudaMemcpyHostToDevice, s), "species");
+void grid_take(Carve &c, Grid &g, int nm, int32_t **cell_of, int32_t **count, int32_t **cursor) {
+    g.start = c.take<int32_t>((size_t)g.ncell + 1);
+    g.atoms = c.take<int32_t>(nm);
+    *cell_of = c.take<int32_t>(nm);
+    *count = c.take<int32_t>(2 * (size_t)g.ncell);
+    *cursor = *count + g.ncell;
+}
+
+int grid_fill(Grid &g, int nm, const double4 *pos, int32_t *cell_of, int32_t *count, int32_t *cursor,
+              cudaStream_t s) {
+    RCUDA(cudaMemsetAsync(count, 0, 2 * (size_t)g.ncell * sizeof(int32_t), s), "analysis cells");
+    const int nb = (nm + 255) / 256;
+    k_grid_count<<<nb, 256, 0, s>>>(nm, pos, g, cell_of, count);
+    launch_exclusive_scan(count, (int32_t *)g.start, g.ncell, s);
+    k_grid_fill<<<nb, 256, 0, s>>>(nm, cell_of, g.start, cursor, (int32_t *)g.atoms);
+    return MOLDY_OK;
+}
+
+int check_species(const int32_t *species, int nm, int nspec) {
+    if (nspec < 1 || nspec > kMaxSpecies || (!species && nspec != 1))
+        return set_last_error(MOLDY_ERR_INVALID, "nspec out of range (1..8; 1 without a species array)");
+    if (species)
+        for (int i = 0; i < nm; ++i)
+            if (species[i] < 0 || species[i] >= nspec)
+                return set_last_error(MOLDY_ERR_INVALID, "species index of atom " + std::to_string(i) + " out of range");
+    return MOLDY_OK;
+}
+
+int host_box(const DeviceState &d, cudaStream_t s, double *b0) {
+    BoxState hb;
+    RCUDA(cudaMemcpyAsync(&hb, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "box");
+    RCUDA(cudaStreamSynchronize(s), "box");
+    for (int k = 0; k < 9; ++k) b0[k] = hb.b0[k];
     return MOLDY_OK;
 }
 
@@ -420,24 +481,40 @@ int Engine::rdf(int mode, int maxbin, int bpa, const int32_t *species, int nspec
                 int64_t *nclose) {
     RCHECK(check_ready());
     if (mode != 0 && mode != 1) return set_last_error(MOLDY_ERR_INVALID, "rdf mode is 0 (neighbour list) or 1 (all pairs)");
-    if (maxbin < 1 || maxbin > 1000000 || bpa < 1) return set_last_error(MOLDY_ERR_INVALID, "maxbin and binsperangstrom >= 1");
-    if (nspec < 1 || nspec > kMaxSpecies || (!species && nspec != 1))
-        return set_last_error(MOLDY_ERR_INVALID, "nspec out of range (1..8; 1 without a species array)");
+    if (maxbin < 1 || maxbin > 1000000 || bpa < 1)
+        return set_last_error(MOLDY_ERR_INVALID, "maxbin and binsperangstrom >= 1");
     if (!hist) return set_last_error(MOLDY_ERR_INVALID, "null histogram");
     if (mode == 0 && !list_ready_) return set_last_error(MOLDY_ERR_ORDER, "the neighbour list has not been built");
-    cudaStream_t s = stream_;
     const int nm = prm.nm;
+    RCHECK(check_species(species, nm, nspec));
+    cudaStream_t s = stream_;
     const size_t nh = (size_t)(maxbin + 1) * nspec * nspec;
-    DevBuf dh, dsp, start, atoms, scratch;
-    RCHECK(rdf_alloc<unsigned long long>(dh, nh + nspec + 1, "RDF histogram"));
-    RCUDA(cudaMemsetAsync(dh.p, 0, (nh + nspec + 1) * sizeof(unsigned long long), s), "RDF histogram");
-    RCHECK(upload_species(species, nm, nspec, s, dsp));
+    Grid g;
+    if (mode == 1) {
+        double b0[9];
+        RCHECK(host_box(d, s, b0));
+        RCHECK(grid_shape(b0, (double)(maxbin + 1) / (double)bpa, g));
+    }
+    // size the scratch, then carve it
+    int32_t *cell_of = nullptr, *count = nullptr, *cursor = nullptr;
+    Carve c;
+    c.take<unsigned long long>(nh + nspec + 1);
+    if (species) c.take<int32_t>(nm);
+    if (mode == 1) grid_take(c, g, nm, &cell_of, &count, &cursor);
+    RCHECK(reserve(d, c.off));
+    c = Carve();
+    c.base = (char *)d.rdf;
+    unsigned long long *dh = c.take<unsigned long long>(nh + nspec + 1);
+    int32_t *dsp = species ? c.take<int32_t>(nm) : nullptr;
+    if (mode == 1) grid_take(c, g, nm, &cell_of, &count, &cursor);
+    RCUDA(cudaMemsetAsync(dh, 0, (nh + nspec + 1) * sizeof(unsigned long long), s), "analysis histogram");
+    if (species) RCUDA(cudaMemcpyAsync(dsp, species, nm * sizeof(int32_t), cudaMemcpyHostToDevice, s), "species");
     HistArgs a;
-    a.pos = d.pos; a.box = d.box; a.znum = d.znum; a.spec = (const int32_t *)dsp.p;
+    a.pos = d.pos; a.box = d.box; a.znum = d.znum; a.spec = dsp;
     a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec; a.maxbin = maxbin; a.bpa = bpa;
     const int q = maxbin / bpa;
     a.rsqmax = (double)(q * q);
-    a.hist = (unsigned long long *)dh.p; a.natoms = a.hist + nh; a.nclose = a.natoms + nspec;
+    a.hist = dh; a.natoms = dh + nh; a.nclose = a.natoms + nspec;
     const size_t smem = nh * sizeof(unsigned int);
     const bool use_smem = smem <= (size_t)kSmemHistBytes;
     const int nb = std::max(1, std::min((nm + kRdfThreads - 1) / kRdfThreads, 4 * 148));
@@ -446,18 +523,14 @@ int Engine::rdf(int mode, int maxbin, int bpa, const int32_t *species, int nspec
         else k_rdf_list<false><<<nb, kRdfThreads, 0, s>>>(a, d.nlist, d.numn);
         prof.launches[K_RDF] += 1;
     } else {
-        BoxState hb;
-        RCUDA(cudaMemcpyAsync(&hb, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "box");
-        RCUDA(cudaStreamSynchronize(s), "box");
-        Grid g;
-        RCHECK(build_grid(hb.b0, nm, d.pos, (double)(maxbin + 1) / (double)bpa, s, g, start, atoms, scratch));
+        RCHECK(grid_fill(g, nm, d.pos, cell_of, count, cursor, s));
         if (use_smem) k_rdf_all<true><<<nb, kRdfThreads, smem, s>>>(a, g);
         else k_rdf_all<false><<<nb, kRdfThreads, 0, s>>>(a, g);
         prof.launches[K_RDF] += 4;
     }
     std::vector<unsigned long long> h(nh + nspec + 1);
-    RCUDA(cudaMemcpyAsync(h.data(), dh.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
-          "RDF histogram");
+    RCUDA(cudaMemcpyAsync(h.data(), dh, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+          "analysis histogram");
     RCUDA(cudaStreamSynchronize(s), "rdf");
     RCUDA(cudaGetLastError(), "rdf");
     for (size_t k = 0; k < nh; ++k) hist[k] = h[k];
@@ -471,58 +544,70 @@ int Engine::ackland_jones(int mode, const int32_t *species, int nspec, const dou
                           int32_t *chi) {
     RCHECK(check_ready());
     if (mode != 0 && mode != 1) return set_last_error(MOLDY_ERR_INVALID, "mode is 0 (neighbour list) or 1 (all atoms)");
-    if (nspec < 1 || nspec > kMaxSpecies || (!species && nspec != 1))
-        return set_last_error(MOLDY_ERR_INVALID, "nspec out of range (1..8; 1 without a species array)");
     if (!rn || !aj || !nn) return set_last_error(MOLDY_ERR_INVALID, "null argument");
     if (mode == 0 && !list_ready_) return set_last_error(MOLDY_ERR_ORDER, "the neighbour list has not been built");
-    cudaStream_t s = stream_;
     const int nm = prm.nm;
+    RCHECK(check_species(species, nm, nspec));
+    cudaStream_t s = stream_;
     AjArgs a;
     double rmax = 0.0;
     for (int k = 0; k < nspec * nspec; ++k) {
-        if (!(rn[k] >= 0.0) || !std::isfinite(rn[k])) return set_last_error(MOLDY_ERR_INVALID, "rn must be finite and >= 0");
+        if (!(rn[k] >= 0.0) || !std::isfinite(rn[k]))
+            return set_last_error(MOLDY_ERR_INVALID, "rn must be finite and >= 0");
         a.thr[k] = (double)1.45f * (rn[k] * rn[k]);
         rmax = std::max(rmax, std::sqrt(a.thr[k]));
     }
-    DevBuf dsp, cnt, nb, nr, dflag, daj, dnn, dchi, start, atoms, scratch;
-    RCHECK(upload_species(species, nm, nspec, s, dsp));
-    RCHECK(rdf_alloc<int32_t>(cnt, nm, "AJ counts"));
-    RCHECK(rdf_alloc<int32_t>(nb, (size_t)nm * kNearCap, "AJ neighbours"));
-    RCHECK(rdf_alloc<double>(nr, (size_t)nm * kNearCap, "AJ distances"));
-    RCHECK(rdf_alloc<int32_t>(dflag, 1, "AJ flag"));
-    RCHECK(rdf_alloc<int32_t>(daj, (size_t)nm * 10, "AJ results"));
-    RCUDA(cudaMemsetAsync(cnt.p, 0, nm * sizeof(int32_t), s), "AJ counts");
-    RCUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int32_t), s), "AJ flag");
-    a.pos = d.pos; a.box = d.box; a.spec = (const int32_t *)dsp.p;
+    Grid g;
+    if (mode == 1) {
+        double b0[9];
+        RCHECK(host_box(d, s, b0));
+        RCHECK(grid_shape(b0, std::max(rmax, 1e-3), g));
+    }
+    int32_t *cell_of = nullptr, *count = nullptr, *cursor = nullptr;
+    Carve c;
+    c.take<int32_t>(nm);                                 // species
+    c.take<int32_t>(nm);                                 // neighbour counts
+    c.take<int32_t>((size_t)nm * kNearCap);              // neighbours
+    c.take<int32_t>(1);                                  // flag
+    c.take<int32_t>((size_t)nm * 10);                    // aj, nn, chi
+    if (mode == 1) grid_take(c, g, nm, &cell_of, &count, &cursor);
+    RCHECK(reserve(d, c.off));
+    c = Carve();
+    c.base = (char *)d.rdf;
+    int32_t *dsp = c.take<int32_t>(nm);
+    a.ncount = c.take<int32_t>(nm);
+    a.near = c.take<int32_t>((size_t)nm * kNearCap);
+    a.flags = c.take<int32_t>(1);
+    int32_t *o = c.take<int32_t>((size_t)nm * 10);
+    if (mode == 1) grid_take(c, g, nm, &cell_of, &count, &cursor);
+    if (species) RCUDA(cudaMemcpyAsync(dsp, species, nm * sizeof(int32_t), cudaMemcpyHostToDevice, s), "species");
+    RCUDA(cudaMemsetAsync(a.ncount, 0, nm * sizeof(int32_t), s), "analysis counts");
+    RCUDA(cudaMemsetAsync(a.flags, 0, sizeof(int32_t), s), "analysis flag");
+    a.pos = d.pos; a.box = d.box; a.spec = species ? dsp : nullptr;
     a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec;
-    a.ncount = (int32_t *)cnt.p; a.near = (int32_t *)nb.p; a.nrsq = (double *)nr.p; a.flags = (int32_t *)dflag.p;
     const int blocks = std::max(1, std::min((nm + kRdfThreads - 1) / kRdfThreads, 8 * 148));
     if (mode == 0) {
         k_aj_near_list<<<blocks, kRdfThreads, 0, s>>>(a, d.nlist, d.numn);
         prof.launches[K_RDF] += 1;
     } else {
-        BoxState hb;
-        RCUDA(cudaMemcpyAsync(&hb, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "box");
-        RCUDA(cudaStreamSynchronize(s), "box");
-        Grid g;
-        RCHECK(build_grid(hb.b0, nm, d.pos, std::max(rmax, 1e-3), s, g, start, atoms, scratch));
+        RCHECK(grid_fill(g, nm, d.pos, cell_of, count, cursor, s));
         k_aj_near_all<<<blocks, kRdfThreads, 0, s>>>(a, g);
         prof.launches[K_RDF] += 4;
     }
-    int32_t *o = (int32_t *)daj.p;
-    k_aj_classify<<<blocks, kRdfThreads, 0, s>>>(a, o, o + nm, o + 2 * (size_t)nm);
+    k_aj_classify<<<blocks, kRdfThreads, 0, s>>>(a, o, o + nm, chi ? o + 2 * (size_t)nm : nullptr);
     prof.launches[K_RDF] += 1;
     int32_t flag = 0;
-    RCUDA(cudaMemcpyAsync(&flag, dflag.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "AJ flag");
-    RCUDA(cudaMemcpyAsync(aj, o, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "AJ classes");
-    RCUDA(cudaMemcpyAsync(nn, o + nm, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "AJ coordination");
-    if (chi) RCUDA(cudaMemcpyAsync(chi, o + 2 * (size_t)nm, 8 * (size_t)nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-                   "AJ angles");
+    RCUDA(cudaMemcpyAsync(&flag, a.flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "analysis flag");
+    RCUDA(cudaMemcpyAsync(aj, o, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "classes");
+    RCUDA(cudaMemcpyAsync(nn, o + nm, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "coordination");
+    if (chi)
+        RCUDA(cudaMemcpyAsync(chi, o + 2 * (size_t)nm, 8 * (size_t)nm * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+              "angle counts");
     RCUDA(cudaStreamSynchronize(s), "ackland_jones");
     RCUDA(cudaGetLastError(), "ackland_jones");
     if (flag)
         return set_last_error(MOLDY_ERR_CAPACITY, "an atom has more than " + std::to_string(kNearCap) +
-                                            " neighbours inside the Ackland-Jones cutoff");
+                                                      " neighbours inside the Ackland-Jones cutoff");
     return MOLDY_OK;
 }
 
