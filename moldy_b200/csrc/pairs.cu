@@ -477,8 +477,8 @@ int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool
                           double *partials, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
     switch (variant) {
-    case 0: sd_variant<4, false, 2>(d, p, t, mixed, partials, nb, s); break;
-    case 1: sd_variant<8, false, 2>(d, p, t, mixed, partials, nb, s); break;
+    case 0: sd_variant<4, true, 4>(d, p, t, mixed, partials, nb, s); break;
+    case 1: sd_variant<8, true, 4>(d, p, t, mixed, partials, nb, s); break;
     case 2: sd_variant<4, true, 2>(d, p, t, mixed, partials, nb, s); break;
     case 3: sd_variant<8, true, 2>(d, p, t, mixed, partials, nb, s); break;
     case 4: sd_variant<4, false, 3>(d, p, t, mixed, partials, nb, s); break;
@@ -508,8 +508,8 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
         return nb;
     }
     switch (variant) {
-    case 0: forces_variant<2, false, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 1: forces_variant<4, false, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 0: forces_variant<2, true, false, 4>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 1: forces_variant<4, true, false, 4>(d, p, t, mixed, mode, partials, nb, s); break;
     case 2: forces_variant<2, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
     case 3: forces_variant<4, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
     case 4: forces_variant<2, false, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
