@@ -716,9 +716,7 @@ int Engine::velocityverlet(moldy_force_out *out) {
 
 int Engine::update_therm_avs(double *s123) {
     CHECK(check_ready());
-    int nb = 0;
-    LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));
-    LAUNCH(*this, K_THERM_FIN, 1, stream_, launch_finalize_therm(d, prm, nb, stream_));
+    LAUNCH(*this, K_THERM, 2, stream_, launch_therm(d, prm, true, stream_));
     if (!host_box_) {
         CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * 4), "pinned staging");
         host_box_cap_ = 4;
@@ -755,9 +753,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         LAUNCH(*this, K_DRIFT, 1, stream_,
                kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, stream_));
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
-        int nb = 0;
-        LAUNCH(*this, K_THERM, 1, stream_, nb = launch_therm(d, prm, stream_));
-        LAUNCH(*this, K_THERM_FIN, 1, stream_, launch_finalize_therm(d, prm, nb, stream_));
+        LAUNCH(*this, K_THERM, 1, stream_, launch_therm(d, prm, false, stream_));
         if (thermo)
             CUDA_CHECK(cudaMemcpyAsync(host_box_ + k, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost,
                                        stream_), "thermo");

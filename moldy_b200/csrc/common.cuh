@@ -24,11 +24,12 @@ struct BoxState {
     double npairs;                 // directed interacting pairs in the last density pass
     double bbuild[9];              // B0 when the intermediate list was built
     double snhv, snhf, scalev_ke;  // Nose-Hoover scaling state of scalev and its last KE
+    double th_tgid[9], th_cof[9];  // tg^-1 tgdot and cof(B0)/vol of the box k_therm sees
     unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
     int32_t mid_builds;            // number of intermediate-list builds so far
     int32_t status;                // nonzero: singular box in a device-side inversion
-    int32_t pad;
+    int32_t therm_ticket;          // blocks of k_therm done (the last one finalizes)
 };
 
 // Per-launch constant parameters.

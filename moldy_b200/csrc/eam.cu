@@ -5,28 +5,32 @@
 
 namespace moldy {
 
-// Sums NV partial columns over nblk blocks in a fixed order into out[NV].
-template <int NV>
+__device__ void therm_prep(const Params &p, BoxState &B);
+
+// Sums NV partial columns over nblk blocks in a fixed order into out[NV];
+// CG reads them through L2 (partials other blocks of the same launch wrote).
+template <int NV, bool CG = false>
 __device__ void reduce_partials(const double *__restrict__ part, int nblk, double *out) {
-    __shared__ double sm[256][NV];
+    __shared__ double sm[32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
     for (int bidx = threadIdx.x; bidx < nblk; bidx += blockDim.x)
 #pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k] += part[(size_t)bidx * kPartials + k];
+        for (int k = 0; k < NV; ++k) acc[k] += CG ? __ldcg(&part[(size_t)bidx * kPartials + k]) : part[(size_t)bidx * kPartials + k];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) sm[threadIdx.x][k] = acc[k];
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w)
-#pragma unroll
-            for (int k = 0; k < NV; ++k) sm[threadIdx.x][k] += sm[threadIdx.x + w][k];
-        __syncthreads();
+    for (int k = 0; k < NV; ++k) {
+        const double w = warp_sum(acc[k]);
+        if (lane == 0) sm[warp][k] = w;
     }
-    if (threadIdx.x == 0)
+    __syncthreads();
+    if (warp == 0)
 #pragma unroll
-        for (int k = 0; k < NV; ++k) out[k] = sm[0][k];
+        for (int k = 0; k < NV; ++k) {
+            const double w = warp_sum(lane < nw ? sm[lane][k] : 0.0);
+            if (lane == 0) out[k] = w;
+        }
     __syncthreads();
 }
 
@@ -78,6 +82,7 @@ k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict_
         mat_mul(B.tginv, B.tgdot, B.tgid);
         for (int k = 0; k < 9; ++k) B.b2[k] = p.bdel2 * B.fb[k];
     }
+    therm_prep(p, B);       // for the update_therm_avs that follows
 }
 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
@@ -224,38 +229,58 @@ __device__ bool therm_box(const Params &p, const BoxState &B, double *tg, double
     return ok;
 }
 
+// The box quantities k_therm needs, from the box after the force call:
+// tgid = tg^-1 tgdot of the new B1 and cof(B0)/vol (the b0_xxdet ... of
+// update_therm_avs); computed once, by one thread.
+__device__ void therm_prep(const Params &p, BoxState &B) {
+    double tg[9], tgdot[9], tginv[9], tgid[9], vol;
+    therm_box(p, B, tg, tgdot, tginv, tgid, vol);
+    const double *b = B.b0;
+    double *d = B.th_cof;        // row-major as in the reference's names
+    for (int k = 0; k < 9; ++k) B.th_tgid[k] = tgid[k];
+    d[0] = (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) / vol;
+    d[1] = (MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1)) / vol;
+    d[2] = (MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2)) / vol;
+    d[3] = (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) / vol;
+    d[4] = (MAT(b, 1, 1) * MAT(b, 3, 3) - MAT(b, 1, 3) * MAT(b, 3, 1)) / vol;
+    d[5] = (MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2)) / vol;
+    d[6] = (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3)) / vol;
+    d[7] = (MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3)) / vol;
+    d[8] = (MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 1, 2) * MAT(b, 2, 1)) / vol;
+}
+
+__global__ void k_therm_prep(Params p, BoxState *__restrict__ box) { therm_prep(p, *box); }
+
+// update_therm_avs (src/dynamics_m.F90:649-734): s1 = sum |F|^2, s2 = sum
+// |F|^4, s3 = sum m |B0 x1|^2 over the atoms with a species.  The last block
+// to finish reduces every block's partials in a fixed order and derives the
+// mdloop quantities (src/moldin.F90:760-790).
 __global__ void __launch_bounds__(256)
-k_therm(Params p, const BoxState *__restrict__ box, const double *__restrict__ x1,
+k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
         const double *__restrict__ x2, const double *__restrict__ mass,
         const int32_t *__restrict__ znum, double *__restrict__ partials) {
     __shared__ double sh[9 + 9 + 9];   // tgid, b0, cof(b0)/vol
-    if (threadIdx.x == 0) {
-        double tg[9], tgdot[9], tginv[9], tgid[9], vol;
-        therm_box(p, *box, tg, tgdot, tginv, tgid, vol);
-        const double *b = box->b0;
-        for (int k = 0; k < 9; ++k) { sh[k] = tgid[k]; sh[9 + k] = b[k]; }
-        double *d = sh + 18;   // b0_xxdet ... stored row-major as in the reference names
-        d[0] = (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) / vol;
-        d[1] = (MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1)) / vol;
-        d[2] = (MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2)) / vol;
-        d[3] = (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) / vol;
-        d[4] = (MAT(b, 1, 1) * MAT(b, 3, 3) - MAT(b, 1, 3) * MAT(b, 3, 1)) / vol;
-        d[5] = (MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2)) / vol;
-        d[6] = (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3)) / vol;
-        d[7] = (MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3)) / vol;
-        d[8] = (MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 1, 2) * MAT(b, 2, 1)) / vol;
+    __shared__ bool last;
+    if (threadIdx.x < 9) {
+        sh[threadIdx.x] = box->th_tgid[threadIdx.x];
+        sh[9 + threadIdx.x] = box->b0[threadIdx.x];
+        sh[18 + threadIdx.x] = box->th_cof[threadIdx.x];
     }
     __syncthreads();
     double v[3] = {0.0, 0.0, 0.0};
     const int nm = p.nm;
     const double *t = sh, *b = sh + 9, *d = sh + 18;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        if (znum[a] == 0) continue;
-        double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
+        // every load issued before the species test, so none waits on it
+        const int z = znum[a];
+        const double ux = x1[a], uy = x1[nm + a], uz = x1[2 * nm + a];
+        const double wx = x2[a], wy = x2[nm + a], wz = x2[2 * nm + a];
+        const double ma = mass[a];
+        if (z == 0) continue;
         double sxi = t[0] * ux + t[3] * uy + t[6] * uz;
         double syi = t[1] * ux + t[4] * uy + t[7] * uz;
         double szi = t[2] * ux + t[5] * uy + t[8] * uz;
-        double fxp = 2.0 * x2[a] + sxi, fyp = 2.0 * x2[nm + a] + syi, fzp = 2.0 * x2[2 * nm + a] + szi;
+        double fxp = 2.0 * wx + sxi, fyp = 2.0 * wy + syi, fzp = 2.0 * wz + szi;
         double fx = d[0] * fxp + d[1] * fyp + d[2] * fzp;
         double fy = d[3] * fxp + d[4] * fyp + d[5] * fzp;
         double fz = d[6] * fxp + d[7] * fyp + d[8] * fzp;
@@ -265,31 +290,27 @@ k_therm(Params p, const BoxState *__restrict__ box, const double *__restrict__ x
         double rx = b[0] * ux + b[3] * uy + b[6] * uz;
         double ry = b[1] * ux + b[4] * uy + b[7] * uz;
         double rz = b[2] * ux + b[5] * uy + b[8] * uz;
-        v[2] += mass[a] * (rx * rx + ry * ry + rz * rz);
+        v[2] += ma * (rx * rx + ry * ry + rz * rz);
     }
     block_partials<3>(v, partials, 0);
-}
-
-int launch_therm(DeviceState &d, const Params &p, cudaStream_t s) {
-    int nblocks = grid_blocks(p.nm, kAtomThreads);
-    k_therm<<<nblocks, kAtomThreads, 0, s>>>(p, d.box, d.x1, d.x2, d.mass, d.znum, d.partials);
-    return nblocks;
-}
-
-// reduces the thermo partials and derives the mdloop quantities
-// (src/moldin.F90:760-790)
-__global__ void __launch_bounds__(256)
-k_finalize_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ partials, int nblk) {
-    __shared__ double s[3];
-    reduce_partials<3>(partials, nblk, s);
+    if (threadIdx.x == 0) {
+        __threadfence();                                 // this block's partials before its ticket
+        last = atomicAdd(&box->therm_ticket, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double s3[3];
+    reduce_partials<3, true>(partials, gridDim.x, s3);
     if (threadIdx.x != 0) return;
     BoxState &B = *box;
+    B.therm_ticket = 0;
     double vol;
     if (!therm_box(p, B, B.tg, B.tgdot, B.tginv, B.tgid, vol)) B.status = MOLDY_ERR_SINGULAR_BOX;
     B.vol = vol;
-    B.s1 = s[0]; B.s2 = s[1]; B.s3 = s[2];
+    B.s1 = s3[0]; B.s2 = s3[1]; B.s3 = s3[2];
     const double bk = 1.3806504e-23 / 1.602176487e-19;
-    B.ke = s[2] / (p.deltat * p.deltat) / 2.0;
+    B.ke = s3[2] / (p.deltat * p.deltat) / 2.0;
     B.temp = B.ke / (1.5 * bk * (double)p.nm);
     double boxke = 0.0;
     for (int i = 1; i <= 3; ++i)
@@ -300,9 +321,16 @@ k_finalize_therm(Params p, BoxState *__restrict__ box, const double *__restrict_
     B.th = B.h + boxke;
 }
 
-void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s) {
-    k_finalize_therm<<<1, 256, 0, s>>>(p, d.box, d.partials, nblocks);
+// prep: compute the box quantities first (the call does not follow a force
+// evaluation that left them)
+int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s) {
+    if (prep) k_therm_prep<<<1, 1, 0, s>>>(p, d.box);
+    int nblocks = grid_blocks(p.nm, kAtomThreads);
+    k_therm<<<nblocks, kAtomThreads, 0, s>>>(p, d.box, d.x1, d.x2, d.mass, d.znum, d.partials);
+    return nblocks;
 }
+
+
 
 // ----------------------------------------------------------------- scalev --
 // scalev (src/thermostat_m.F90:317-395), the Nose-Hoover Euler thermostat:

@@ -258,8 +258,9 @@ void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut
                        int apply_box, cudaStream_t s);
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
-int launch_therm(DeviceState &d, const Params &p, cudaStream_t s);
-void launch_finalize_therm(DeviceState &d, const Params &p, int nblocks, cudaStream_t s);
+// update_therm_avs with the thermo finalization in its last block; prep
+// when the call does not directly follow a force evaluation
+int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s);
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
 void launch_scalev(DeviceState &d, const Params &p, double nose, double rqke, cudaStream_t s);
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s);
