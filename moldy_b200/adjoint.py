@@ -122,6 +122,73 @@ class EAMKnots(torch.autograd.Function):
         return (None, None) + tuple(_t(g[k]) for k in KNOT_NAMES)
 
 
+def _force_matching_share(system, coeffs, nlookup, configs, refs, w_force, w_stress):
+    """Loss and summed table gradients of some configurations on one system."""
+    system.set_up_fetm(coeffs, uselookup=True, nlookup=int(nlookup))
+    loss = 0.0
+    acc = {k: np.zeros(int(nlookup) + 1) for k in TABLE_NAMES}
+    for (x0, b0), (f_ref, s_ref) in zip(configs, refs):
+        system.set_state(x0=x0, b0=b0)
+        _, f, sig, _ = _evaluate(system)
+        df = f - np.asarray(f_ref, dtype=np.float64)
+        ds = sig - np.asarray(s_ref, dtype=np.float64)
+        loss += w_force * float((df * df).sum()) + w_stress * float((ds * ds).sum())
+        g = system.table_gradients(0.0, 2.0 * w_force * df, 2.0 * w_stress * ds)
+        for k in TABLE_NAMES:
+            acc[k] += g[k]
+    return loss, acc
+
+
+class ForceMatchingKnots(torch.autograd.Function):
+    """The force-matching loss of many configurations,
+    sum_c w_force |F_c - F_c^ref|^2 + w_stress |sigma_c - sigma_c^ref|^2, as a
+    function of the Fe-Fe knots.  The loss is a scalar, so its gradient is
+    formed in the forward pass: the tables are built once per system, each
+    configuration is evaluated once and its table gradients summed, and one
+    contraction with d(table)/d(knot) gives dL/d(knot); backward scales it.
+
+    ``apply(systems, configs, refs, w_force, w_stress, nlookup, av, rv, ap,
+    rp)``; systems is one MoldySystem or a list of them (each on its own CUDA
+    stream): with k systems, host threads evaluate configuration c on system
+    c mod k, so their launches and copies overlap, and the shares are summed
+    in system order.  configs[c] = (x0 [nm,3] fractional, b0 3x3), refs[c] =
+    (F_ref [nm,3] real forces, sigma_ref 3x3)."""
+
+    @staticmethod
+    def forward(ctx, systems, configs, refs, w_force, w_stress, nlookup, av, rv, ap, rp):
+        coeffs = FeFeCoefficients(*(_f64(t.detach().cpu().numpy()) for t in (av, rv, ap, rp)))
+        systems = list(systems) if isinstance(systems, (list, tuple)) else [systems]
+        k = len(systems)
+        shares = [(systems[t], coeffs, nlookup, configs[t::k], refs[t::k], w_force, w_stress) for t in range(k)]
+        if k == 1:
+            results = [_force_matching_share(*shares[0])]
+        else:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(max_workers=k) as pool:
+                results = list(pool.map(lambda a: _force_matching_share(*a), shares))
+        loss = 0.0
+        acc = {name: np.zeros(int(nlookup) + 1) for name in TABLE_NAMES}
+        for l, g in results:
+            loss += l
+            for name in TABLE_NAMES:
+                acc[name] += g[name]
+        kg = fetm_knot_vjp(coeffs, acc, int(nlookup))
+        ctx.grads = [torch.as_tensor(kg[name]) for name in KNOT_NAMES]
+        return torch.tensor(loss, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, g):
+        return (None,) * 6 + tuple(g * t for t in ctx.grads)
+
+
+def force_matching_knots(systems, configs, refs, knots: dict, *, w_force=1.0, w_stress=1.0, nlookup: int = 5000):
+    """Scalar force-matching loss of many configurations on one system or a
+    list of systems, differentiable in the knots dict {av, rv, ap, rp} of
+    torch tensors (ForceMatchingKnots)."""
+    return ForceMatchingKnots.apply(systems, configs, refs, float(w_force), float(w_stress), int(nlookup),
+                                    *[knots[k] for k in KNOT_NAMES])
+
+
 def eam_tables(system, tables: dict, ranges=(0.0, 6.0, 0.0, 10000.0)):
     """(E, F, sigma) differentiable in the tables dict of torch tensors."""
     return EAMTables.apply(system, tuple(ranges), *[tables[k] for k in TABLE_NAMES])

@@ -176,6 +176,12 @@ class MoldySystem:
                     b0=_mat_from_f(mats[0]), b1=_mat_from_f(mats[1]), b2=_mat_from_f(mats[2]),
                     tgid=_mat_from_f(mats[3]))
 
+    def box(self) -> np.ndarray:
+        """B0 alone (columns are box vectors)."""
+        m = np.zeros(9)
+        check(self._L.moldy_gpu_get_state(self._h, *([None] * 9), _dp(m), None, None, None))
+        return _mat_from_f(m)
+
     def forces(self) -> np.ndarray:
         f = [np.zeros(self.nm) for _ in range(3)]
         check(self._L.moldy_gpu_get_forces(self._h, *[_dp(a) for a in f]))
@@ -237,7 +243,7 @@ class MoldySystem:
         F = B0 f and sigma(i,j) = -sum_k b0(j,k) tp(i,k) / vol."""
         if out is None:
             out = self.force()
-        b0 = self.get_state()["b0"]
+        b0 = self.box()
         f = self.forces() @ b0.T
         sigma = -(out["tp"] @ b0.T) / out["vol"]
         return out["pe"], f, sigma

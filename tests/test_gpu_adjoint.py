@@ -205,6 +205,48 @@ def test_force_matching_autograd_knots(gpu_lib):
     s.close()
 
 
+def test_fused_force_matching_equals_per_configuration_autograd(gpu_lib):
+    """ForceMatchingKnots (tables built once, each configuration evaluated
+    once, the gradient formed in the forward pass) gives the loss and the
+    knot gradient of the per-configuration EAMKnots path within 1e-11, with
+    weights, and scales its gradient by the incoming one."""
+    configs = [fm_config(60 + c, n=6, sigma=0.1) for c in range(3)]
+    s = MoldySystem.from_workload(configs[0], uselookup=True)
+    refs = []
+    for w in configs:
+        s.set_state(x0=w.x0, b0=w.b0)
+        _, f0, s0 = gpu_eval(s, coeffs=FE_FE)
+        refs.append((f0 + 1e-3, s0 * 1.01))
+    rng = np.random.default_rng(5)
+    base = {k: np.asarray(getattr(FE_FE, k)) * (1 + 1e-3 * rng.normal(size=len(getattr(FE_FE, k))))
+            for k in adj.KNOT_NAMES}
+    th1 = {k: torch.tensor(v, requires_grad=True) for k, v in base.items()}
+    total = torch.zeros((), dtype=torch.float64)
+    for w, (f0, s0) in zip(configs, refs):
+        s.set_state(x0=w.x0, b0=w.b0)
+        _, f, sig = adj.eam_knots(s, th1)
+        total = total + 0.7 * ((f - torch.as_tensor(f0)) ** 2).sum() + 2.0 * ((sig - torch.as_tensor(s0)) ** 2).sum()
+    total.backward()
+    th2 = {k: torch.tensor(v, requires_grad=True) for k, v in base.items()}
+    fused = adj.force_matching_knots(s, [(w.x0, w.b0) for w in configs], refs, th2, w_force=0.7, w_stress=2.0)
+    (3.0 * fused).backward()
+    assert abs(fused.item() - total.item()) <= 1e-11 * abs(total.item())
+    for k in adj.KNOT_NAMES:
+        a, b = th1[k].grad.numpy(), th2[k].grad.numpy() / 3.0
+        assert np.max(np.abs(a - b)) <= 1e-11 * np.linalg.norm(a), (k, a, b)
+    # two systems driven from two host threads: the same loss and gradient
+    s2 = MoldySystem.from_workload(configs[0], uselookup=True)
+    th3 = {k: torch.tensor(v, requires_grad=True) for k, v in base.items()}
+    par = adj.force_matching_knots([s, s2], [(w.x0, w.b0) for w in configs], refs, th3, w_force=0.7, w_stress=2.0)
+    par.backward()
+    assert abs(par.item() - total.item()) <= 1e-11 * abs(total.item())
+    for k in adj.KNOT_NAMES:
+        a, b = th1[k].grad.numpy(), th3[k].grad.numpy()
+        assert np.max(np.abs(a - b)) <= 1e-11 * np.linalg.norm(a), (k, a, b)
+    s2.close()
+    s.close()
+
+
 def test_table_autograd_matches_reference(case):
     """EAMTables backward equals torch autograd of the restated forward."""
     w, o, s = case["w"], case["o"], case["s"]
