@@ -677,12 +677,17 @@ def run_batch(args):
         # FP32 resolution) with the FP64 passes' best gather
         q, qms, qbuilds, qevals = run_quench(best_skin)
         b.set_gather(best_gather[prec])
+        # every rank's systems, at their global indices (one all-gather)
+        from moldy_b200.batch import gather_system_results
+        shards = shard_configs([w.nm for w in ws_all], world)
+        q = gather_system_results({k: q[k] for k in ("iflag", "fmax", "nfev", "f")}, shards, len(ws_all))
+        natoms_all = np.array([w.nm for w in ws_all])
         rounds = int(q["nfev"].max())
         quench = {"seconds": qms / 1000.0, "systems": int(len(ws_all)), "converged": int((q["iflag"] == 0).sum()),
                   "cg_error_returns": int((q["iflag"] == 2).sum()), "max_function_values": rounds,
                   "median_function_values": float(np.median(q["nfev"])),
                   "systems_per_s": len(ws_all) / (qms / 1000.0),
-                  "atom_evals_per_s": float((q["nfev"] * b.natoms).sum()) * world / (qms / 1000.0),
+                  "atom_evals_per_s": float((q["nfev"] * natoms_all).sum()) / (qms / 1000.0),
                   "max_force_eV_per_A": float(q["fmax"].max()), "skin_A": best_skin, "skin_sweep_ms": skin_ms,
                   "list_builds_per_system_evaluation": qbuilds / max(qevals, 1),
                   "precision": "fp64 (line search needs it; force() runs " + prec + ")"}

@@ -183,3 +183,45 @@ class MoldyBatch:
     def split(self, arr):
         """Per-system views of a concatenated per-atom array."""
         return [arr[self.offsets[s]:self.offsets[s + 1]] for s in range(self.nsys)]
+
+
+def gather_system_results(local: dict, assignment, nsys: int, group=None) -> dict:
+    """Per-system results of a batch sharded over ranks, on every rank.
+
+    ``local`` maps names to this rank's arrays, first dimension = its
+    systems in the order of ``assignment[rank]`` (``adjoint.shard_configs``
+    gives such an assignment); ``assignment[r]`` lists the global indices of
+    rank r's systems.  One all_gather of a packed float64 tensor per rank
+    (padded to the largest shard; on the GPU under NCCL, on the host under
+    gloo) places every system's row at its global index.  Without an
+    initialised process group the local arrays are the whole batch."""
+    import torch
+    import torch.distributed as dist
+    names = sorted(local)
+    if not (dist.is_available() and dist.is_initialized()):
+        return {k: np.asarray(local[k]) for k in names}
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    mine = list(assignment[rank])
+    arrs = [np.asarray(local[k], dtype=np.float64).reshape(len(mine), -1) for k in names]
+    widths = [a.shape[1] for a in arrs]
+    width = int(sum(widths))
+    rows = max(len(a) for a in assignment)
+    device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    buf = torch.zeros((rows, width), dtype=torch.float64, device=device)
+    if mine:
+        buf[:len(mine)] = torch.from_numpy(np.concatenate(arrs, axis=1)).to(device)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    out = {}
+    off = 0
+    for k, wdt, a in zip(names, widths, arrs):
+        full = np.zeros((nsys, wdt))
+        for r in range(world):
+            p = parts[r].cpu().numpy()
+            for i, sidx in enumerate(assignment[r]):
+                full[sidx] = p[i, off:off + wdt]
+        shape = np.asarray(local[k]).shape[1:]
+        out[k] = full.reshape((nsys,) + tuple(shape))
+        off += wdt
+    return out
