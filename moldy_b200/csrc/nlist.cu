@@ -1,12 +1,15 @@
 // nlist.cu -- the hybrid Verlet half list (update_neighbourlist,
 // src/neighbourlist_m.F90:103-276) built on the GPU.
 //
-// One warp owns one atom i.  It walks the 14 cells of the reference's half
-// stencil in the reference's order (dz in {0,+1}; at dz=0 dy in {0,+1}; at
-// dz=0,dy=0 dx in {0,+1}; otherwise dx,dy in {-1,0,+1}), and inside each cell
-// the atoms in chain order; in i's own cell only the atoms after i.  Lanes
+// One block owns one link cell.  It stages the atoms of the 14 cells of the
+// reference's half stencil in shared memory, in the reference's order (dz in
+// {0,+1}; at dz=0 dy in {0,+1}; at dz=0,dy=0 dx in {0,+1}; otherwise dx,dy in
+// {-1,0,+1}), each cell's atoms in chain order, the home cell first.  Each
+// warp then takes home atoms i in turn and walks the staged candidates from
+// the one after i: the rest of i's own cell, then the other 13 cells.  Lanes
 // test 32 candidates at a time and a ballot appends the accepted ones in
-// order, so NLIST(:, i) matches the reference entry for entry.  The list is
+// order, so NLIST(:, i) matches the reference entry for entry.  Candidates
+// past the staging capacity are read from global memory.  The list is
 // stored entry-major (entry k of atom i at k*nm + i) so that the per-step
 // passes, one thread per atom, read it in contiguous 128-byte rows; the export
 // transposes it to the reference's NLIST(nnbrs, nm).  The distance
@@ -26,69 +29,97 @@ __constant__ int8_t c_stencil[14][3] = {
 
 __device__ __forceinline__ int wrap(int j, int n) { return j < 0 ? j + n : (j >= n ? j - n : j); }
 
-__global__ void __launch_bounds__(256)
+constexpr int kNlStage = 640;   // staged candidates per home cell
+constexpr int kNlWarps = 4;
+
+__global__ void __launch_bounds__(32 * kNlWarps)
 k_build_nlist(Params p, const double4 *__restrict__ pos, const BoxState *__restrict__ box,
-              const int32_t *__restrict__ ic, const int32_t *__restrict__ cell_pos,
               const int32_t *__restrict__ cell_start, const int32_t *__restrict__ cell_count,
               const int32_t *__restrict__ cell_atoms, int32_t *__restrict__ nlist,
               int32_t *__restrict__ numn, int32_t *__restrict__ flags) {
+    __shared__ double sx[kNlStage], sy[kNlStage], sz[kNlStage];
+    __shared__ int sj[kNlStage];
+    __shared__ int sbase[15], sstart[14];
     __shared__ double sb[9];
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
+    const int c = blockIdx.x;
+    const int L0 = cell_count[c];
+    if (L0 == 0) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid < 9) sb[tid] = box->b0[tid];
+    if (tid < 14) {
+        const int cx = c % p.nlcx, cy = (c / p.nlcx) % p.nlcy, cz = c / (p.nlcx * p.nlcy);
+        const int jx = wrap(cx + c_stencil[tid][0], p.nlcx);
+        const int jy = wrap(cy + c_stencil[tid][1], p.nlcy);
+        const int jz = wrap(cz + c_stencil[tid][2], p.nlcz);
+        const int jp = jx + p.nlcx * (jy + p.nlcy * jz);
+        sstart[tid] = cell_start[jp];
+        sbase[tid + 1] = cell_count[jp];
+    }
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (a >= p.nm) return;
+    if (tid == 0) {
+        sbase[0] = 0;
+        for (int k = 1; k <= 14; ++k) sbase[k] += sbase[k - 1];
+    }
+    __syncthreads();
+    const int total = sbase[14];
+    const int staged = total < kNlStage ? total : kNlStage;
+    for (int k = tid; k < staged; k += blockDim.x) {
+        int s = 0;
+        while (sbase[s + 1] <= k) ++s;
+        const int j = cell_atoms[sstart[s] + (k - sbase[s])];
+        const double4 pj = pos[j];
+        sx[k] = pj.x; sy[k] = pj.y; sz[k] = pj.z; sj[k] = j;
+    }
+    __syncthreads();
     double b[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) b[k] = sb[k];
-    const int c = ic[a];
-    const int q = cell_pos[a];
-    const int cx = c % p.nlcx, cy = (c / p.nlcx) % p.nlcy, cz = c / (p.nlcx * p.nlcy);
-    const double4 pa = pos[a];
-    int count = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int s = 0; s < 14; ++s) {
-        int jx = wrap(cx + c_stencil[s][0], p.nlcx);
-        int jy = wrap(cy + c_stencil[s][1], p.nlcy);
-        int jz = wrap(cz + c_stencil[s][2], p.nlcz);
-        int jp = jx + p.nlcx * (jy + p.nlcy * jz);
-        int L = cell_count[jp];
-        const int32_t *seg = cell_atoms + cell_start[jp];
-        int k0 = (jp == c) ? q + 1 : 0;
-        for (int k = k0; k < L; k += 32) {
-            int kk = k + lane;
+    // home atom q sits at staged slot q (the home cell is staged first)
+    for (int q = w; q < L0; q += kNlWarps) {
+        const int a = cell_atoms[sstart[0] + q];
+        const double4 pa = pos[a];
+        int count = 0;
+        for (int k0 = q + 1; k0 < total; k0 += 32) {
+            const int kk = k0 + lane;
             bool take = false;
             int j = 0;
-            if (kk < L) {
-                j = seg[kk];
-                double4 pj = pos[j];
-                double dx = __dsub_rn(pa.x, pj.x), dy = __dsub_rn(pa.y, pj.y), dz = __dsub_rn(pa.z, pj.z);
+            if (kk < total) {
+                double qx, qy, qz;
+                if (kk < staged) {
+                    qx = sx[kk]; qy = sy[kk]; qz = sz[kk]; j = sj[kk];
+                } else {
+                    int s = 0;
+                    while (sbase[s + 1] <= kk) ++s;
+                    j = cell_atoms[sstart[s] + (kk - sbase[s])];
+                    const double4 pj = pos[j];
+                    qx = pj.x; qy = pj.y; qz = pj.z;
+                }
+                double dx = __dsub_rn(pa.x, qx), dy = __dsub_rn(pa.y, qy), dz = __dsub_rn(pa.z, qz);
                 min_image(p.ivol, dx, dy, dz);
-                double r = realsep_exact(b, dx, dy, dz);
+                const double r = realsep_exact(b, dx, dy, dz);
                 take = r < p.rnear;
             }
-            unsigned bal = __ballot_sync(0xffffffffu, take);
+            const unsigned bal = __ballot_sync(0xffffffffu, take);
             if (take) {
-                int slot = count + __popc(bal & lt);
+                const int slot = count + __popc(bal & lt);
                 if (slot < p.nnbrs) nlist[(size_t)slot * p.nm + a] = j;
             }
             count += __popc(bal);
         }
-    }
-    if (lane == 0) {
-        numn[a] = count < p.nnbrs ? count : p.nnbrs;
-        if (count > p.nnbrs) {
-            atomicExch(&flags[0], 1);
-            atomicMax(&flags[2], a + 1);
+        if (lane == 0) {
+            numn[a] = count < p.nnbrs ? count : p.nnbrs;
+            if (count > p.nnbrs) {
+                atomicExch(&flags[0], 1);
+                atomicMax(&flags[2], a + 1);
+            }
         }
     }
 }
 
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s) {
-    long long threads = (long long)p.nm * 32;
-    int nb = (int)((threads + 255) / 256);
-    k_build_nlist<<<nb, 256, 0, s>>>(p, d.pos, d.box, d.ic, d.cell_pos, d.cell_start, d.cell_count,
-                                     d.cell_atoms, d.nlist, d.numn, d.flags);
+    k_build_nlist<<<p.ncell, 32 * kNlWarps, 0, s>>>(p, d.pos, d.box, d.cell_start, d.cell_count, d.cell_atoms,
+                                                     d.nlist, d.numn, d.flags);
 }
 
 // NLIST(nnbrs, nm) with 1-based entries; unused slots are zero
