@@ -297,11 +297,13 @@ int moldy_gpu_ackland_jones(moldy_gpu *h, int32_t mode, const int32_t *species, 
  * are concatenated, each system's in the reference's order.  Per system the
  * results are those of force() + energy_calc() (src/dynamics_m.F90:135-483)
  * in lookup mode, and the quench is quench_m::quench with VA14CD and derivs
- * (src/quench_m.F90:100-551) at a fixed box (ivol = 1).  Pairs are found by
- * neighbour-cell tiles at every evaluation (all pairs inside the table cut),
- * not by the Verlet list; beyond the cut every pair contributes zero, so the
- * sums are those of a complete list.  Each box must be wider than twice the
- * interaction range in every direction (MOLDY_ERR_INVALID otherwise). */
+ * (src/quench_m.F90:100-551) at a fixed box (ivol = 1).  Each system keeps
+ * its own list of the pairs within rcut + skin, found by neighbour-cell tiles
+ * and rebuilt on the device once one of its atoms has moved half the skin
+ * (moldy_gpu_batch_set_skin); the passes keep the pairs inside the table cut,
+ * and beyond it every pair contributes zero, so the sums are those of a
+ * complete list.  Each box must be wider than twice the interaction range in
+ * every direction (MOLDY_ERR_INVALID otherwise). */
 typedef struct moldy_batch moldy_batch;
 int moldy_gpu_batch_create(int32_t nsys, const int32_t *natoms, double press, int32_t device,
                            moldy_batch **out);
@@ -339,9 +341,9 @@ int moldy_gpu_batch_get_density(moldy_batch *h, double *rho, double *afrho, doub
  * the returned points (moldy_gpu_batch_get_state). */
 int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, double fmax,
                            double *out8);
-/* Tile shape: lanes per home atom (4, 8, 16 or 32; default 8) and how many
- * candidates a warp stages in shared memory (0..256, default 256; the rest are
- * read from global memory). */
+/* Tile shape of the list builds: lanes per home atom (4, 8, 16 or 32; default
+ * 8) and how many candidates a warp stages in shared memory (0..256, default
+ * 256; the rest are read from global memory). */
 int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
 /* Precision of the per-atom density and force passes of moldy_gpu_batch_force:
  * 0 all FP64 (default); 1 mixed: separations, distances, table interpolation
