@@ -170,7 +170,7 @@ Engine::~Engine() {
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
                     d.pair_cnt, d.mlist, d.mid_own, d.mid_rev, d.xbuild, d.tab_r4, d.tab_e2,
-                    d.tab_r4f, d.tab_e2f, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
+                    d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_box_) cudaFreeHost(host_box_);
@@ -273,6 +273,7 @@ int Engine::check_ready() {
 // at and beyond which every pair contributes exactly zero (exact mode: the
 // largest knot), times 1 + 1e-12; 1e150 when the tables never reach zero.
 int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, double2 **e2d, float2 **e2fd,
+                         void **auxd,
                          Tables &t, double *rcull_out) {
     int n = h.nlookup;
     int cut = n + 1;
@@ -282,10 +283,19 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
     }
     int nr = (cut <= n - 1) ? cut + 2 : n + 1;
     std::vector<double4> r4(nr);
-    std::vector<float4> r4f(nr);
+    // FP32 nodes in pairs (node k, node k+1) so that one 32-byte load brings
+    // both ends of an interval; the density tables keep phi_k, phi_k+1 side by side
+    std::vector<float4> r4f(2 * (size_t)nr, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<double2> phi2(nr, make_double2(0.0, 0.0));
+    std::vector<float2> phi2f(nr, make_float2(0.f, 0.f));
     for (int i = 0; i < nr; ++i) {
         r4[i] = make_double4(h.vee[i], h.dvee[i], h.phi[i], h.dphi[i]);
-        r4f[i] = make_float4((float)h.vee[i], (float)h.dvee[i], (float)h.phi[i], (float)h.dphi[i]);
+        const float4 q = make_float4((float)h.vee[i], (float)h.dvee[i], (float)h.phi[i], (float)h.dphi[i]);
+        r4f[2 * (size_t)i] = q;
+        if (i > 0) r4f[2 * (size_t)i - 1] = q;
+        phi2[i].x = h.phi[i];
+        phi2f[i].x = (float)h.phi[i];
+        if (i > 0) { phi2[i - 1].y = h.phi[i]; phi2f[i - 1].y = (float)h.phi[i]; }
     }
     std::vector<double2> e2(n + 1);
     std::vector<float2> e2f(n + 1);
@@ -293,20 +303,29 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
         e2[i] = make_double2(h.emb[i], h.demb[i]);
         e2f[i] = make_float2((float)h.emb[i], (float)h.demb[i]);
     }
-    void *old[] = {*r4d, *e2d, *r4fd, *e2fd};
+    void *old[] = {*r4d, *e2d, *r4fd, *e2fd, *auxd};
     for (void *b : old)
         if (b) cudaFree(b);
-    *r4d = nullptr; *e2d = nullptr; *r4fd = nullptr; *e2fd = nullptr;
+    *r4d = nullptr; *e2d = nullptr; *r4fd = nullptr; *e2fd = nullptr; *auxd = nullptr;
     CHECK(dev_alloc(r4d, nr, "tables"));
-    CHECK(dev_alloc(r4fd, nr, "tables"));
+    CHECK(dev_alloc(r4fd, 2 * (size_t)nr, "tables"));
+    // phi2 (nr double2), then phi2f (nr float2)
+    unsigned char *aux = nullptr;
+    CHECK(dev_alloc(&aux, (size_t)nr * (sizeof(double2) + sizeof(float2)), "tables"));
+    *auxd = aux;
     CHECK(dev_alloc(e2d, n + 1, "tables"));
     CHECK(dev_alloc(e2fd, n + 1, "tables"));
     CUDA_CHECK(cudaMemcpy(*r4d, r4.data(), nr * sizeof(double4), cudaMemcpyHostToDevice), "tables");
-    CUDA_CHECK(cudaMemcpy(*r4fd, r4f.data(), nr * sizeof(float4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(*r4fd, r4f.data(), 2 * (size_t)nr * sizeof(float4), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(aux, phi2.data(), nr * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+    CUDA_CHECK(cudaMemcpy(aux + nr * sizeof(double2), phi2f.data(), nr * sizeof(float2), cudaMemcpyHostToDevice),
+               "tables");
     CUDA_CHECK(cudaMemcpy(*e2d, e2.data(), (n + 1) * sizeof(double2), cudaMemcpyHostToDevice), "tables");
     CUDA_CHECK(cudaMemcpy(*e2fd, e2f.data(), (n + 1) * sizeof(float2), cudaMemcpyHostToDevice), "tables");
 
     t.r4 = *r4d; t.e2 = *e2d; t.r4f = *r4fd; t.e2f = *e2fd;
+    t.phi2 = reinterpret_cast<const double2 *>(aux);
+    t.phi2f = reinterpret_cast<const float2 *>(aux + nr * sizeof(double2));
     t.nlookup = n;
     t.nr = nr;
     t.idx_cut = cut;
@@ -348,7 +367,7 @@ int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 
 int Engine::upload_tables() {
     double rc = 0.0;
-    CHECK(upload_device_tables(ht, &d.tab_r4, &d.tab_r4f, &d.tab_e2, &d.tab_e2f, tab, &rc));
+    CHECK(upload_device_tables(ht, &d.tab_r4, &d.tab_r4f, &d.tab_e2, &d.tab_e2f, &d.tab_aux, tab, &rc));
     rcut = rc < 1e150 ? rc : prm.rnear;
     rmid = std::min(prm.rnear, rcut + mid_skin);
     potential_set_ = true;
@@ -599,7 +618,12 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     // force calls outside velocity Verlet always rebuild the intermediate list
     const int force_mid = (mode == 1 && !rb && !E.mid_dirty()) ? 0 : 1;
     E.clear_mid_dirty();
-    LAUNCH(E, K_MID, 1, s, launch_mid_decide(d, p, E.rmid, E.rcut, force_mid, mode == 1 ? 1 : 0, s));
+    LAUNCH(E, K_MID, 1, s,
+           launch_mid_decide(d, p, E.rmid, E.rcut, force_mid, mode == 1 ? 1 : 0, E.therm_blocks, s));
+    if (E.therm_blocks > 0 && E.therm_dst)   // the deferred thermo record, before the box algebra below
+        CUDA_CHECK(cudaMemcpyAsync(E.therm_dst, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "thermo");
+    E.therm_blocks = 0;
+    E.therm_dst = nullptr;
     if (rb) {
         if (!cells_ready) { LAUNCH(E, K_LINKUP, 4, s, launch_linkup(d, p, s)); cells_ready = true; }
         LAUNCH(E, K_NLIST, 1, s, launch_build_nlist(d, p, s));
@@ -706,7 +730,7 @@ int Engine::velocityverlet(moldy_force_out *out) {
     CHECK(check_ready());
     bool rb = false;
     LAUNCH(*this, K_DRIFT, 1, stream_,
-               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, stream_));
+               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, false, stream_));
     CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
     CHECK(fetch_force_out(out));
     if (out) out->rebuilt = rb ? 1 : 0;
@@ -748,25 +772,40 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         host_box_cap_ = nsteps;
     }
     std::vector<int> ntcs(nsteps), rbs(nsteps);
+    // update_therm_avs of step k reads x1 and x2 as step k's force evaluation
+    // left them.  Unless scalev changes x1 first, or k is the last step, it is
+    // deferred into the drift kernel of step k + 1, which reads both anyway,
+    // and finished by the k_mid_decide that follows it.
+    bool therm_pending = false;
     for (int k = 0; k < nsteps; ++k) {
         bool rb = false;
         LAUNCH(*this, K_DRIFT, 1, stream_,
-               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, stream_));
+               kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, therm_pending,
+                                         stream_));
+        if (therm_pending) {
+            therm_blocks = kin_blocks;
+            therm_dst = thermo ? host_box_ + k - 1 : nullptr;
+        }
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
-        LAUNCH(*this, K_THERM, 1, stream_, launch_therm(d, prm, false, stream_));
-        if (thermo)
-            CUDA_CHECK(cudaMemcpyAsync(host_box_ + k, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost,
-                                       stream_), "thermo");
         ntcs[k] = ntc_;
         rbs[k] = rb ? 1 : 0;
-        if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
         // src/moldin.F90:828-835: scalev once per femtosecond of simulated time,
         // with the mdloop's own constant for one femtosecond
         thermotimer_ = thermotimer_ + prm.deltat;
+        bool scalev = false;
         if (thermotimer_ >= kFemtosecond) {
             thermotimer_ = thermotimer_ - kFemtosecond;
-            if (nose_ > 0.0) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
+            scalev = nose_ > 0.0;
         }
+        therm_pending = !(scalev || k == nsteps - 1);
+        if (!therm_pending) {
+            LAUNCH(*this, K_THERM, 1, stream_, launch_therm(d, prm, false, stream_));
+            if (thermo)
+                CUDA_CHECK(cudaMemcpyAsync(host_box_ + k, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost,
+                                           stream_), "thermo");
+        }
+        if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
+        if (scalev) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
     }
     CUDA_CHECK(cudaGetLastError(), "md_steps launch");
     CHECK(check_flags());
@@ -809,7 +848,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, 1, 0, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, 1, 0, 0, stream_));
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {

@@ -421,7 +421,7 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
             for (int u = 0; u < B; ++u) jj[u] = e0 + u < n ? alist[(size_t)(e0 + u) * ntot + hs] : hs;
             double4 pp[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) pp[u] = a.spos[jj[u]];
+            for (int u = 0; u < B; ++u) pp[u] = ldg4(&a.spos[jj[u]]);
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 if (e0 + u >= n) continue;
@@ -496,7 +496,7 @@ k_cl_forces(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restr
             double4 pp[B];
             double fq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) { pp[u] = a.spos[jj[u]]; fq[u] = a.sfp[jj[u]]; }
+            for (int u = 0; u < B; ++u) { pp[u] = ldg4(&a.spos[jj[u]]); fq[u] = a.sfp[jj[u]]; }
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 if (e0 + u >= n) continue;
@@ -884,6 +884,7 @@ class BatchEngine {
     double2 *tab_e2 = nullptr;
     float4 *tab_r4f = nullptr;
     float2 *tab_e2f = nullptr;
+    void *tab_aux = nullptr;
     double *stage = nullptr;            // host-to-device staging (3*ntot)
     int *host_active = nullptr;         // pinned
     cudaGraphExec_t graph = nullptr;
@@ -940,7 +941,7 @@ BatchEngine::~BatchEngine() {
     if (graph) cudaGraphExecDestroy(graph);
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
                     mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
-                    tab_r4f, tab_e2f, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order};
+                    tab_r4f, tab_e2f, tab_aux, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -1026,7 +1027,7 @@ int BatchEngine::set_fetm(int nv, const double *av, const double *rv, int np, co
     int rc = build_fetm_tables(ht, nv, av, rv, np, ap, rp, 1, nlookup);
     if (rc != MOLDY_OK) return set_last_error(rc, "FETRANSMETAL set-up failed");
     double rcull = 0.0;
-    BCHECK(upload_device_tables(ht, &tab_r4, &tab_r4f, &tab_e2, &tab_e2f, tab, &rcull));
+    BCHECK(upload_device_tables(ht, &tab_r4, &tab_r4f, &tab_e2, &tab_e2f, &tab_aux, tab, &rcull));
     // every pair beyond the table cut and the pair function's knots contributes zero
     double r = rcull < 1e150 ? rcull : 0.0;
     for (int i = 0; i < nv; ++i) r = std::max(r, rv[i] * (1.0 + 1e-12));

@@ -29,7 +29,7 @@ struct BoxState {
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
     int32_t mid_builds;            // number of intermediate-list builds so far
     int32_t status;                // nonzero: singular box in a device-side inversion
-    int32_t therm_ticket;          // blocks of k_therm done (the last one finalizes)
+    int32_t pad2;
 };
 
 // Per-launch constant parameters.
@@ -45,8 +45,10 @@ struct Params {
 struct Tables {
     const double4 *r4;      // per node (vee, dvee, phi, dphi), nodes 0..nr-1
     const double2 *e2;      // per node (emb, demb), nodes 0..nlookup
-    const float4 *r4f;      // FP32 copy of r4 for the mixed path
+    const float4 *r4f;      // FP32 copy of r4 for the mixed path, node pairs: [2k] = node k, [2k+1] = node k+1
     const float2 *e2f;
+    const double2 *phi2;    // per node k (phi_k, phi_k+1): one load per density lookup
+    const float2 *phi2f;
     int nlookup;            // intervals
     int nr;                 // stored r nodes (culled tail removed)
     int idx_cut;            // first node from which all r tables are zero
@@ -94,11 +96,20 @@ __device__ __forceinline__ int cell_coord(double x, int nlc) {
     return (int)__dmul_rn(__dadd_rn(__dsub_rn(x, round(x)), hmeps), (double)nlc);
 }
 
-// read-only (non-coherent) 32-byte load as two 16-byte halves
+// Read-only (non-coherent) 32-byte loads as one 256-bit request (sm_100).
+// The address must be 32-byte aligned: every double4 array and the paired
+// float4 table are cudaMalloc'd arrays of 32-byte elements.  The data must
+// not be written while the kernel runs.
 __device__ __forceinline__ double4 ldg4(const double4 *p) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    double2 lo = __ldg(q), hi = __ldg(q + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
+    double4 v;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void ldg8f(const float4 *p, float4 &a, float4 &b) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
 }
 
 // ---------------------------------------------------------- table lookup --
@@ -130,7 +141,8 @@ __device__ __forceinline__ double lookup_phi(const Tables &t, double r) {
     idx = idx < 0 ? 0 : idx;
     double rlow = t.vp_rmin + (t.vp_range * (double)idx) * t.vp_recipnlkp;
     double dr = (r - rlow) * t.vp_recipstep;
-    return __ldg(&t.r4[idx].z) * (1.0 - dr) + __ldg(&t.r4[idx + 1].z) * dr;
+    const double2 v = __ldg(&t.phi2[idx]);
+    return v.x * (1.0 - dr) + v.y * dr;
 }
 
 // get_value_from_lookup_emb (src/lookup_m.F90:356-394) for (emb, demb)
@@ -152,8 +164,8 @@ __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
     if (idx >= t.nr - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
     idx = idx < 0 ? 0 : idx;
     float dr = r * (float)t.vp_recipstep - (float)idx;
-    float4 a = __ldg(&t.r4f[idx]);
-    float4 b = __ldg(&t.r4f[idx + 1]);
+    float4 a, b;
+    ldg8f(&t.r4f[2 * idx], a, b);
     return make_float4(fmaf(b.x - a.x, dr, a.x), fmaf(b.y - a.y, dr, a.y),
                        fmaf(b.z - a.z, dr, a.z), fmaf(b.w - a.w, dr, a.w));
 }
@@ -163,9 +175,8 @@ __device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
     if (idx >= t.nr - 1) return 0.f;
     idx = idx < 0 ? 0 : idx;
     float dr = r * (float)t.vp_recipstep - (float)idx;
-    float a = __ldg(&t.r4f[idx].z);
-    float b = __ldg(&t.r4f[idx + 1].z);
-    return fmaf(b - a, dr, a);
+    const float2 v = __ldg(&t.phi2f[idx]);
+    return fmaf(v.y - v.x, dr, v.x);
 }
 
 // ------------------------------------------------ exact FETRANSMETAL Fe-Fe --
@@ -334,6 +345,14 @@ __device__ __forceinline__ void mat_mul(const double *a, const double *b, double
     }
 }
 
+// Frobenius norm of a 3x3 matrix
+__device__ __forceinline__ double frob(const double *m) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s += m[k] * m[k];
+    return sqrt(s);
+}
+
 // ------------------------------------------------------------ reductions --
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -362,6 +381,33 @@ __device__ __forceinline__ void block_partials(double (&v)[NV], double *partials
             if (lane == 0) partials[(size_t)blockIdx.x * kPartials + off + k] = s;
         }
     }
+    __syncthreads();
+}
+
+// Sums NV partial columns over nblk blocks in a fixed order into out[NV];
+// CG reads them through L2 (partials other blocks of the same launch wrote).
+template <int NV, bool CG = false>
+__device__ __forceinline__ void reduce_partials(const double *__restrict__ part, int nblk, double *out) {
+    __shared__ double sm[32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int bidx = threadIdx.x; bidx < nblk; bidx += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += CG ? __ldcg(&part[(size_t)bidx * kPartials + k]) : part[(size_t)bidx * kPartials + k];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double w = warp_sum(acc[k]);
+        if (lane == 0) sm[warp][k] = w;
+    }
+    __syncthreads();
+    if (warp == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double w = warp_sum(lane < nw ? sm[lane][k] : 0.0);
+            if (lane == 0) out[k] = w;
+        }
     __syncthreads();
 }
 

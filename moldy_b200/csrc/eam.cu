@@ -5,46 +5,52 @@
 
 namespace moldy {
 
-__device__ void therm_prep(const Params &p, BoxState &B);
-
-// Sums NV partial columns over nblk blocks in a fixed order into out[NV];
-// CG reads them through L2 (partials other blocks of the same launch wrote).
-template <int NV, bool CG = false>
-__device__ void reduce_partials(const double *__restrict__ part, int nblk, double *out) {
-    __shared__ double sm[32][NV];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    double acc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    for (int bidx = threadIdx.x; bidx < nblk; bidx += blockDim.x)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k] += CG ? __ldcg(&part[(size_t)bidx * kPartials + k]) : part[(size_t)bidx * kPartials + k];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        const double w = warp_sum(acc[k]);
-        if (lane == 0) sm[warp][k] = w;
-    }
-    __syncthreads();
-    if (warp == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            const double w = warp_sum(lane < nw ? sm[lane][k] : 0.0);
-            if (lane == 0) out[k] = w;
-        }
-    __syncthreads();
-}
+__device__ void therm_prep(const Params &p, const double *b0, const double *b1, BoxState &B);
 
 // mode 0: force only; 1: velocity Verlet second half (box); 2: md_init
 __global__ void __launch_bounds__(256)
 k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
                  int nblk_embed, const double *__restrict__ part_force, int nblk_force,
                  const double *__restrict__ part_kin, int nblk_kin, int mode) {
-    __shared__ double se[2], sf[7], sk[6];
-    reduce_partials<2>(part_embed, nblk_embed, se);
-    reduce_partials<7>(part_force, nblk_force, sf);
-    reduce_partials<6>(part_kin, nblk_kin, sk);
+    // the three sets of block partials in one pass: each thread issues the
+    // loads of all three before adding (per set, the same order as
+    // reduce_partials)
+    __shared__ double sm[8][15], sr[15];
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    const int nmax = max(nblk_embed, max(nblk_force, nblk_kin));
+    for (int b = threadIdx.x; b < nmax; b += blockDim.x) {
+        double e[15];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) e[k] = b < nblk_embed ? part_embed[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) e[2 + k] = b < nblk_force ? part_force[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) e[9 + k] = b < nblk_kin ? part_kin[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 15; ++k) acc[k] += e[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        const double w = warp_sum(acc[k]);
+        if (lane == 0) sm[warp][k] = w;
+    }
+    __syncthreads();
+    if (warp == 0 && lane < 15) {
+        double w = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) w += sm[q][lane];
+        sr[lane] = w;
+    }
+    __syncthreads();
     if (threadIdx.x != 0) return;
+    const double *se = sr, *sf = sr + 2, *sk = sr + 9;
+    // the box algebra runs on register copies and is stored once at the end
     BoxState &B = *box;
+    double b0[9], b1[9], b2[9], tp[9], tk[9], tc[9], tg[9], tgdot[9], fb[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { b0[k] = B.b0[k]; b1[k] = B.b1[k]; b2[k] = B.b2[k]; }
     B.pe_emb = se[0];
     B.pe_pair = sf[0];
     B.pe = se[0] + sf[0];
@@ -54,35 +60,52 @@ k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict_
     M[0] = sk[0]; M[4] = sk[1]; M[8] = sk[2]; M[3] = M[1] = sk[3]; M[6] = M[2] = sk[4]; M[7] = M[5] = sk[5];
     D[0] = sf[1]; D[4] = sf[2]; D[8] = sf[3]; D[3] = D[1] = sf[4]; D[6] = D[2] = sf[5]; D[7] = D[5] = sf[6];
     double dt2 = p.deltat * p.deltat;
-    mat_mul(B.b0, D, B.tp);                       // tp(a,b) = sum r_a d_b fp, r = B0 d
-    mat_mul(B.b0, M, B.tk);                       // tk(a,b) = sum m (B0 x1)_a x1_b
-    for (int k = 0; k < 9; ++k) B.tk[k] = B.tk[k] / dt2;
-    mat_cofactor(B.b0, B.tc);
-    for (int k = 0; k < 9; ++k) { B.tgdot[k] = 0.0; B.tg[k] = 0.0; }
+    mat_mul(b0, D, tp);                           // tp(a,b) = sum r_a d_b fp, r = B0 d
+    mat_mul(b0, M, tk);                           // tk(a,b) = sum m (B0 x1)_a x1_b
+#pragma unroll
+    for (int k = 0; k < 9; ++k) tk[k] = tk[k] / dt2;
+    mat_cofactor(b0, tc);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { tgdot[k] = 0.0; tg[k] = 0.0; }
+#pragma unroll
     for (int i = 1; i <= 3; ++i)
+#pragma unroll
         for (int k = 1; k <= 3; ++k)
+#pragma unroll
             for (int j = 1; j <= 3; ++j) {
-                MAT(B.tg, i, j) = MAT(B.tg, i, j) + MAT(B.b0, k, i) * MAT(B.b0, k, j);
-                MAT(B.tgdot, i, j) = MAT(B.tgdot, i, j) + MAT(B.b0, k, i) * MAT(B.b1, k, j) +
-                                     MAT(B.b1, k, i) * MAT(B.b0, k, j);
+                MAT(tg, i, j) = MAT(tg, i, j) + MAT(b0, k, i) * MAT(b0, k, j);
+                MAT(tgdot, i, j) = MAT(tgdot, i, j) + MAT(b0, k, i) * MAT(b1, k, j) + MAT(b1, k, i) * MAT(b0, k, j);
             }
-    B.vol = mat_volume(B.b0);
-    for (int k = 0; k < 9; ++k) B.fb[k] = B.tk[k] + B.tp[k] - p.press * B.tc[k];
+    const double vol = mat_volume(b0);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fb[k] = tk[k] + tp[k] - p.press * tc[k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        B.tp[k] = tp[k]; B.tk[k] = tk[k]; B.tc[k] = tc[k]; B.tg[k] = tg[k]; B.tgdot[k] = tgdot[k]; B.fb[k] = fb[k];
+    }
+    B.vol = vol;
     if (mode == 1) {
         if (p.ivol < 1) {
-            for (int k = 0; k < 9; ++k) B.b2[k] = p.bdel2 * B.fb[k];
-            for (int k = 0; k < 9; ++k) B.b1[k] = B.b1[k] + B.b2[k];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b2[k] = p.bdel2 * fb[k];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b1[k] = b1[k] + b2[k];
         }
         if (p.ivol == 4) {
-            MAT(B.b2, 3, 3) = p.bdel2 * MAT(B.fb, 3, 3);
-            for (int k = 0; k < 9; ++k) B.b1[k] = B.b1[k] + B.b2[k];
+            MAT(b2, 3, 3) = p.bdel2 * MAT(fb, 3, 3);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b1[k] = b1[k] + b2[k];
         }
     } else if (mode == 2) {
-        if (!mat_invert(B.tg, B.tginv)) { B.status = MOLDY_ERR_SINGULAR_BOX; return; }
-        mat_mul(B.tginv, B.tgdot, B.tgid);
-        for (int k = 0; k < 9; ++k) B.b2[k] = p.bdel2 * B.fb[k];
+        double tginv[9], tgid[9];
+        if (!mat_invert(tg, tginv)) { B.status = MOLDY_ERR_SINGULAR_BOX; return; }
+        mat_mul(tginv, tgdot, tgid);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { B.tginv[k] = tginv[k]; B.tgid[k] = tgid[k]; b2[k] = p.bdel2 * fb[k]; }
     }
-    therm_prep(p, B);       // for the update_therm_avs that follows
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { B.b1[k] = b1[k]; B.b2[k] = b2[k]; }
+    therm_prep(p, b0, b1, B);       // for the update_therm_avs that follows
 }
 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
@@ -115,17 +138,195 @@ int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream
     return nb;
 }
 
+// ---------------------------------------------------------- thermo sums ----
+// update_therm_avs (src/dynamics_m.F90:649-734): tg, tgdot (ivol != 1),
+// tgid = tg^-1 tgdot, vol, and per-atom s1 = sum |F|^2, s2 = sum |F|^4,
+// s3 = sum m |B0 x1|^2.
+__device__ __forceinline__ bool therm_box(const Params &p, const double *b0, const double *b1, double *tg,
+                                          double *tgdot, double *tginv, double *tgid, double &vol) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { tg[k] = 0.0; tgdot[k] = 0.0; }
+#pragma unroll
+    for (int i = 1; i <= 3; ++i)
+#pragma unroll
+        for (int k = 1; k <= 3; ++k)
+#pragma unroll
+            for (int j = 1; j <= 3; ++j) {
+                MAT(tg, i, j) = MAT(tg, i, j) + MAT(b0, k, i) * MAT(b0, k, j);
+                if (p.ivol != 1)
+                    MAT(tgdot, i, j) = MAT(tgdot, i, j) + MAT(b1, k, i) * MAT(b0, k, j) +
+                                       MAT(b0, k, i) * MAT(b1, k, j);
+            }
+    bool ok = mat_invert(tg, tginv);
+    mat_mul(tginv, tgdot, tgid);
+    vol = mat_volume(b0);
+    return ok;
+}
+
+// The box quantities k_therm needs, from the box after the force call:
+// tgid = tg^-1 tgdot of the new B1 and cof(B0)/vol (the b0_xxdet ... of
+// update_therm_avs); computed once, by one thread, from register copies of
+// B0 and B1.
+__device__ void therm_prep(const Params &p, const double *b, const double *b1, BoxState &B) {
+    double tg[9], tgdot[9], tginv[9], tgid[9], vol, d[9];   // d row-major as in the reference's names
+    therm_box(p, b, b1, tg, tgdot, tginv, tgid, vol);
+    d[0] = (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) / vol;
+    d[1] = (MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1)) / vol;
+    d[2] = (MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2)) / vol;
+    d[3] = (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) / vol;
+    d[4] = (MAT(b, 1, 1) * MAT(b, 3, 3) - MAT(b, 1, 3) * MAT(b, 3, 1)) / vol;
+    d[5] = (MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2)) / vol;
+    d[6] = (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3)) / vol;
+    d[7] = (MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3)) / vol;
+    d[8] = (MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 1, 2) * MAT(b, 2, 1)) / vol;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { B.th_tgid[k] = tgid[k]; B.th_cof[k] = d[k]; }
+}
+
+__global__ void k_therm_prep(Params p, BoxState *__restrict__ box) {
+    double b0[9], b1[9];
+    for (int k = 0; k < 9; ++k) { b0[k] = box->b0[k]; b1[k] = box->b1[k]; }
+    therm_prep(p, b0, b1, *box);
+}
+
+// update_therm_avs (src/dynamics_m.F90:649-734), one atom's terms: s1 += |F|^2,
+// s2 += |F|^4, s3 += m |B0 x1|^2, with F = cof(B0)/vol (2 x2 + tgid x1); t, b, d
+// are tgid, B0 and cof(B0)/vol in shared memory, read at every use (volatile)
+// rather than held in 54 registers across the atom loop, which would halve the
+// resident warps of the streaming kernels that call this.  The caller skips
+// atoms without a species.
+__device__ __forceinline__ void therm_terms(double (&v)[3], const volatile double *t, const volatile double *b,
+                                            const volatile double *d,
+                                            double ma, double ux, double uy, double uz, double wx, double wy,
+                                            double wz) {
+    double sxi = t[0] * ux + t[3] * uy + t[6] * uz;
+    double syi = t[1] * ux + t[4] * uy + t[7] * uz;
+    double szi = t[2] * ux + t[5] * uy + t[8] * uz;
+    double fxp = 2.0 * wx + sxi, fyp = 2.0 * wy + syi, fzp = 2.0 * wz + szi;
+    double fx = d[0] * fxp + d[1] * fyp + d[2] * fzp;
+    double fy = d[3] * fxp + d[4] * fyp + d[5] * fzp;
+    double fz = d[6] * fxp + d[7] * fyp + d[8] * fzp;
+    double f2 = fx * fx + fy * fy + fz * fz;
+    v[0] += f2;
+    v[1] += f2 * f2;
+    double rx = b[0] * ux + b[3] * uy + b[6] * uz;
+    double ry = b[1] * ux + b[4] * uy + b[7] * uz;
+    double rz = b[2] * ux + b[5] * uy + b[8] * uz;
+    v[2] += ma * (rx * rx + ry * ry + rz * rz);
+}
+
+// The mdloop quantities (src/moldin.F90:760-790) from the three sums of
+// update_therm_avs (s3 = s1, s2, s3), by one thread.  The box has not moved
+// since the force evaluation that ended the step.
+__device__ void therm_store(const Params &p, BoxState &B, const double *s3) {
+    double b0[9], b1[9], tg[9], tgdot[9], tginv[9], tgid[9], vol;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { b0[k] = B.b0[k]; b1[k] = B.b1[k]; }
+    if (!therm_box(p, b0, b1, tg, tgdot, tginv, tgid, vol)) B.status = MOLDY_ERR_SINGULAR_BOX;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { B.tg[k] = tg[k]; B.tgdot[k] = tgdot[k]; B.tginv[k] = tginv[k]; B.tgid[k] = tgid[k]; }
+    B.vol = vol;
+    B.s1 = s3[0]; B.s2 = s3[1]; B.s3 = s3[2];
+    const double bk = 1.3806504e-23 / 1.602176487e-19;
+    B.ke = s3[2] / (p.deltat * p.deltat) / 2.0;
+    B.temp = B.ke / (1.5 * bk * (double)p.nm);
+    double boxke = 0.0;
+    for (int i = 1; i <= 3; ++i)
+        for (int j = 1; j <= 3; ++j) boxke = boxke + (MAT(b1, i, j) * MAT(b1, i, j)) / p.bdel2;
+    B.boxke = boxke;
+    B.te = B.ke + B.pe;
+    B.h = B.te + p.press * B.vol;
+    B.th = B.h + boxke;
+}
+
+// Every block's three partial sums of update_therm_avs, in block order, and
+// the quantities derived from them (one block)
+__global__ void __launch_bounds__(256)
+k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ partials, int nblk) {
+    __shared__ double s3[3];
+    reduce_partials<3>(partials, nblk, s3);
+    if (threadIdx.x == 0) therm_store(p, *box, s3);
+}
+
+// ------------------------------------------------ intermediate-list check --
+// therm_nblk > 0: first finish the update_therm_avs that the drift kernel
+// took for the step that has just ended (its block partials), before the box
+// moves.
+__global__ void __launch_bounds__(256)
+k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, int force, int apply_box,
+             const double *__restrict__ therm_partials, int therm_nblk) {
+    if (therm_nblk > 0) {
+        __shared__ double s3[3];
+        reduce_partials<3>(therm_partials, therm_nblk, s3);
+        if (threadIdx.x == 0) therm_store(p, *box, s3);
+    }
+    if (threadIdx.x != 0) return;
+    BoxState &B = *box;
+    // register copies; the box is stored back once
+    double b0[9], b1[9], b2[9], bb[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { b0[k] = B.b0[k]; b1[k] = B.b1[k]; b2[k] = B.b2[k]; bb[k] = B.bbuild[k]; }
+    if (apply_box) {   // velocityverlet box half (src/quench_m.F90:582-589)
+        if (p.ivol == 4) {
+            MAT(b1, 3, 3) = MAT(b1, 3, 3) + MAT(b2, 3, 3);
+            MAT(b0, 3, 3) = MAT(b0, 3, 3) + MAT(b1, 3, 3);
+        }
+        if (p.ivol < 1) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b1[k] = b1[k] + b2[k];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b0[k] = b0[k] + b1[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { B.b0[k] = b0[k]; B.b1[k] = b1[k]; }
+    }
+    double md = sqrt(__longlong_as_double((long long)B.maxdisp2));
+    B.maxdisp2 = 0ull;
+    double eps = 2.0e-6 * frob(b0) + 1.0e-4;
+    double db[9], inv[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) db[k] = b0[k] - bb[k];
+    bool ok = mat_invert(bb, inv);
+    double dmax = ok ? p.rnear * frob(inv) : 1e300;
+    double shrink = 2.0 * md + frob(db) * dmax;
+    int need = force || !ok || !(shrink < rmid - eps - (rcut + eps));
+    B.mid_rebuild = need;
+    if (need) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) B.bbuild[k] = b0[k];
+        B.mid_builds += 1;
+    }
+}
+
+void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
+                       int apply_box, int therm_nblk, cudaStream_t s) {
+    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, force, apply_box, d.partials, therm_nblk);
+}
+
 // ------------------------------------------------------------- integrator --
 // velocityverlet first half (src/quench_m.F90:574-589): x1_dt2 = x1 + x2;
 // x0 += x1_dt2.  The box half (b1 += b2; b0 += b1 for ivol < 1, zz only for
 // ivol 4) is applied by k_mid_decide, which runs next.
+//
+// THERM: the update_therm_avs of the previous step is taken here too.  x1 and
+// x2 are read unchanged from the force evaluation that ended that step, the
+// box has not yet moved, and the grid is k_therm's, so the sums are k_therm's
+// to the last bit.  The block partials go to therm_partials; k_mid_decide,
+// which runs next, finishes them.
+template <bool THERM>
 __global__ void __launch_bounds__(256)
 k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
         const double4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
-        double *__restrict__ kin_partials) {
+        double *__restrict__ kin_partials, double *__restrict__ therm_partials) {
     // every thread forms the post-drift box exactly as thread 0 stores it
     __shared__ double nb[9];
+    __shared__ double sh[THERM ? 27 : 1];   // tgid, b0, cof(b0)/vol of the previous step
+    if (THERM && threadIdx.x < 9) {
+        sh[threadIdx.x] = box->th_tgid[threadIdx.x];
+        sh[9 + threadIdx.x] = box->b0[threadIdx.x];
+        sh[18 + threadIdx.x] = box->th_cof[threadIdx.x];
+    }
     if (threadIdx.x == 0) {
         const BoxState &B = *box;
         double b1[9], b0[9];
@@ -143,24 +344,31 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
     __syncthreads();
     double d2 = 0.0;
     double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double vt[3] = {0.0, 0.0, 0.0};
     const int nm = p.nm;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const double ex = x1[a], ey = x1[nm + a], ez = x1[2 * nm + a];
+        const double wx = x2[a], wy = x2[nm + a], wz = x2[2 * nm + a];
         double4 q = pos[a];
-        q.x = q.x + (ex + x2[a]);
-        q.y = q.y + (ey + x2[nm + a]);
-        q.z = q.z + (ez + x2[2 * nm + a]);
+        q.x = q.x + (ex + wx);
+        q.y = q.y + (ey + wy);
+        q.z = q.z + (ez + wz);
         pos[a] = q;
         posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
         double4 xb = xbuild[a];
         double ux = q.x - xb.x, uy = q.y - xb.y, uz = q.z - xb.z;
-        double rx = nb[0] * ux + nb[3] * uy + nb[6] * uz;
-        double ry = nb[1] * ux + nb[4] * uy + nb[7] * uz;
-        double rz = nb[2] * ux + nb[5] * uy + nb[8] * uz;
+        const volatile double *bv = nb;   // read per use, not held in registers
+        double rx = bv[0] * ux + bv[3] * uy + bv[6] * uz;
+        double ry = bv[1] * ux + bv[4] * uy + bv[7] * uz;
+        double rz = bv[2] * ux + bv[5] * uy + bv[8] * uz;
         d2 = fmax(d2, rx * rx + ry * ry + rz * rz);
         // x1 is not changed by this half of the step: the kinetic moment of
         // the coming force evaluation can be taken here
-        if (znum[a] != 0) kin_moment(v, mass[a], ex, ey, ez);
+        if (znum[a] != 0) {
+            const double ma = mass[a];
+            kin_moment(v, ma, ex, ey, ez);
+            if (THERM) therm_terms(vt, sh, sh + 9, sh + 18, ma, ex, ey, ez, wx, wy, wz);
+        }
     }
     block_partials<6>(v, kin_partials, 0);
     // block maximum, then one atomic per block (non-negative doubles order as their bits)
@@ -174,13 +382,20 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
         atomicMax(&box->maxdisp2, (unsigned long long)__double_as_longlong(m));
     }
+    // the sums are finished by k_mid_decide, which runs next
+    if (THERM) block_partials<3>(vt, therm_partials, 0);
     // the box itself is advanced afterwards by k_mid_decide, so that no block
     // here can read a box another block has already moved
 }
 
-int launch_drift(DeviceState &d, const Params &p, double *kin_partials, cudaStream_t s) {
+int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s) {
     int nb = grid_blocks(p.nm, kAtomThreads);
-    k_drift<<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum, kin_partials);
+    if (therm)
+        k_drift<true><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+                                                  kin_partials, d.partials);
+    else
+        k_drift<false><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+                                                   kin_partials, nullptr);
     return nb;
 }
 
@@ -208,59 +423,14 @@ void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s) {
     k_md_init_x2<<<nb, kAtomThreads, 0, s>>>(p, d.box, d.f, d.x1, d.x2, d.del2);
 }
 
-// ---------------------------------------------------------- thermo sums ----
-// update_therm_avs (src/dynamics_m.F90:649-734): tg, tgdot (ivol != 1),
-// tgid = tg^-1 tgdot, vol, and per-atom s1 = sum |F|^2, s2 = sum |F|^4,
-// s3 = sum m |B0 x1|^2.
-__device__ bool therm_box(const Params &p, const BoxState &B, double *tg, double *tgdot,
-                          double *tginv, double *tgid, double &vol) {
-    for (int k = 0; k < 9; ++k) { tg[k] = 0.0; tgdot[k] = 0.0; }
-    for (int i = 1; i <= 3; ++i)
-        for (int k = 1; k <= 3; ++k)
-            for (int j = 1; j <= 3; ++j) {
-                MAT(tg, i, j) = MAT(tg, i, j) + MAT(B.b0, k, i) * MAT(B.b0, k, j);
-                if (p.ivol != 1)
-                    MAT(tgdot, i, j) = MAT(tgdot, i, j) + MAT(B.b1, k, i) * MAT(B.b0, k, j) +
-                                       MAT(B.b0, k, i) * MAT(B.b1, k, j);
-            }
-    bool ok = mat_invert(tg, tginv);
-    mat_mul(tginv, tgdot, tgid);
-    vol = mat_volume(B.b0);
-    return ok;
-}
-
-// The box quantities k_therm needs, from the box after the force call:
-// tgid = tg^-1 tgdot of the new B1 and cof(B0)/vol (the b0_xxdet ... of
-// update_therm_avs); computed once, by one thread.
-__device__ void therm_prep(const Params &p, BoxState &B) {
-    double tg[9], tgdot[9], tginv[9], tgid[9], vol;
-    therm_box(p, B, tg, tgdot, tginv, tgid, vol);
-    const double *b = B.b0;
-    double *d = B.th_cof;        // row-major as in the reference's names
-    for (int k = 0; k < 9; ++k) B.th_tgid[k] = tgid[k];
-    d[0] = (MAT(b, 2, 2) * MAT(b, 3, 3) - MAT(b, 2, 3) * MAT(b, 3, 2)) / vol;
-    d[1] = (MAT(b, 2, 3) * MAT(b, 3, 1) - MAT(b, 3, 3) * MAT(b, 2, 1)) / vol;
-    d[2] = (MAT(b, 2, 1) * MAT(b, 3, 2) - MAT(b, 3, 1) * MAT(b, 2, 2)) / vol;
-    d[3] = (MAT(b, 3, 2) * MAT(b, 1, 3) - MAT(b, 1, 2) * MAT(b, 3, 3)) / vol;
-    d[4] = (MAT(b, 1, 1) * MAT(b, 3, 3) - MAT(b, 1, 3) * MAT(b, 3, 1)) / vol;
-    d[5] = (MAT(b, 3, 1) * MAT(b, 1, 2) - MAT(b, 1, 1) * MAT(b, 3, 2)) / vol;
-    d[6] = (MAT(b, 1, 2) * MAT(b, 2, 3) - MAT(b, 2, 2) * MAT(b, 1, 3)) / vol;
-    d[7] = (MAT(b, 1, 3) * MAT(b, 2, 1) - MAT(b, 1, 1) * MAT(b, 2, 3)) / vol;
-    d[8] = (MAT(b, 1, 1) * MAT(b, 2, 2) - MAT(b, 1, 2) * MAT(b, 2, 1)) / vol;
-}
-
-__global__ void k_therm_prep(Params p, BoxState *__restrict__ box) { therm_prep(p, *box); }
-
-// update_therm_avs (src/dynamics_m.F90:649-734): s1 = sum |F|^2, s2 = sum
-// |F|^4, s3 = sum m |B0 x1|^2 over the atoms with a species.  The last block
-// to finish reduces every block's partials in a fixed order and derives the
-// mdloop quantities (src/moldin.F90:760-790).
+// update_therm_avs over the atoms with a species, after a force evaluation
+// (therm_prep has left tgid and cof(B0)/vol in the box state); block partials
+// only, finished by k_therm_finish
 __global__ void __launch_bounds__(256)
 k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
         const double *__restrict__ x2, const double *__restrict__ mass,
         const int32_t *__restrict__ znum, double *__restrict__ partials) {
     __shared__ double sh[9 + 9 + 9];   // tgid, b0, cof(b0)/vol
-    __shared__ bool last;
     if (threadIdx.x < 9) {
         sh[threadIdx.x] = box->th_tgid[threadIdx.x];
         sh[9 + threadIdx.x] = box->b0[threadIdx.x];
@@ -269,7 +439,6 @@ k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
     __syncthreads();
     double v[3] = {0.0, 0.0, 0.0};
     const int nm = p.nm;
-    const double *t = sh, *b = sh + 9, *d = sh + 18;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         // every load issued before the species test, so none waits on it
         const int z = znum[a];
@@ -277,48 +446,9 @@ k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
         const double wx = x2[a], wy = x2[nm + a], wz = x2[2 * nm + a];
         const double ma = mass[a];
         if (z == 0) continue;
-        double sxi = t[0] * ux + t[3] * uy + t[6] * uz;
-        double syi = t[1] * ux + t[4] * uy + t[7] * uz;
-        double szi = t[2] * ux + t[5] * uy + t[8] * uz;
-        double fxp = 2.0 * wx + sxi, fyp = 2.0 * wy + syi, fzp = 2.0 * wz + szi;
-        double fx = d[0] * fxp + d[1] * fyp + d[2] * fzp;
-        double fy = d[3] * fxp + d[4] * fyp + d[5] * fzp;
-        double fz = d[6] * fxp + d[7] * fyp + d[8] * fzp;
-        double f2 = fx * fx + fy * fy + fz * fz;
-        v[0] += f2;
-        v[1] += f2 * f2;
-        double rx = b[0] * ux + b[3] * uy + b[6] * uz;
-        double ry = b[1] * ux + b[4] * uy + b[7] * uz;
-        double rz = b[2] * ux + b[5] * uy + b[8] * uz;
-        v[2] += ma * (rx * rx + ry * ry + rz * rz);
+        therm_terms(v, sh, sh + 9, sh + 18, ma, ux, uy, uz, wx, wy, wz);
     }
     block_partials<3>(v, partials, 0);
-    if (threadIdx.x == 0) {
-        __threadfence();                                 // this block's partials before its ticket
-        last = atomicAdd(&box->therm_ticket, 1) == (int)gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    __shared__ double s3[3];
-    reduce_partials<3, true>(partials, gridDim.x, s3);
-    if (threadIdx.x != 0) return;
-    BoxState &B = *box;
-    B.therm_ticket = 0;
-    double vol;
-    if (!therm_box(p, B, B.tg, B.tgdot, B.tginv, B.tgid, vol)) B.status = MOLDY_ERR_SINGULAR_BOX;
-    B.vol = vol;
-    B.s1 = s3[0]; B.s2 = s3[1]; B.s3 = s3[2];
-    const double bk = 1.3806504e-23 / 1.602176487e-19;
-    B.ke = s3[2] / (p.deltat * p.deltat) / 2.0;
-    B.temp = B.ke / (1.5 * bk * (double)p.nm);
-    double boxke = 0.0;
-    for (int i = 1; i <= 3; ++i)
-        for (int j = 1; j <= 3; ++j) boxke = boxke + (MAT(B.b1, i, j) * MAT(B.b1, i, j)) / p.bdel2;
-    B.boxke = boxke;
-    B.te = B.ke + B.pe;
-    B.h = B.te + p.press * B.vol;
-    B.th = B.h + boxke;
 }
 
 // prep: compute the box quantities first (the call does not follow a force
@@ -327,10 +457,9 @@ int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s) {
     if (prep) k_therm_prep<<<1, 1, 0, s>>>(p, d.box);
     int nblocks = grid_blocks(p.nm, kAtomThreads);
     k_therm<<<nblocks, kAtomThreads, 0, s>>>(p, d.box, d.x1, d.x2, d.mass, d.znum, d.partials);
+    k_therm_finish<<<1, kAtomThreads, 0, s>>>(p, d.box, d.partials, nblocks);
     return nblocks;
 }
-
-
 
 // ----------------------------------------------------------------- scalev --
 // scalev (src/thermostat_m.F90:317-395), the Nose-Hoover Euler thermostat:

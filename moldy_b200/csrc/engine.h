@@ -59,6 +59,7 @@ struct DeviceState {
     double2 *tab_e2 = nullptr;
     float4 *tab_r4f = nullptr;
     float2 *tab_e2f = nullptr;
+    void *tab_aux = nullptr;               // phi2 / phi2f node-pair tables
     // reductions, flags and box state
     double *partials = nullptr;
     int32_t *flags = nullptr;     // [0] neighbour overflow, [1] relink inconsistency,
@@ -210,6 +211,8 @@ class Engine {
     int mid_overflow_ = 0;          // largest intermediate row of an overflowing build
   public:
     int kin_blocks = 0;             // blocks whose kinetic-moment partials the last drift wrote
+    int therm_blocks = 0;           // > 0: the last drift took update_therm_avs, for k_mid_decide to finish
+    BoxState *therm_dst = nullptr;  // pinned slot for that step's thermo record (or none)
   private:
     bool mid_dirty_ = true;         // the intermediate list must be rebuilt before use
   public:
@@ -222,13 +225,10 @@ class Engine {
 };
 
 constexpr int kAtomThreads = 256;
-constexpr int kPairTPA = 8;            // threads per atom in the pair passes
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
 constexpr int kPairCapMin = 24;        // least compact-row entries per atom
 constexpr int kMidCapMin = 48;         // least intermediate-row entries per atom
 constexpr double kFemtosecond = 0.098227;   // the mdloop's "fs" (src/moldin.F90:132), model time units
-constexpr int kScreenTPA = 8;          // lanes per atom in the screening pass
-constexpr int kFullTPA = 8;            // lanes per atom in the density and force passes
 
 inline int grid_blocks(long long work, int threads) {
     long long nb = (work + threads - 1) / threads;
@@ -252,10 +252,13 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
                            const double *part_force, int nblk_force, const double *part_kin, int nblk_kin,
                            int mode, cudaStream_t s);
-int launch_drift(DeviceState &d, const Params &p, double *kin_partials, cudaStream_t s);
+// therm: also take the update_therm_avs of the step that ended with the last
+// force evaluation (x1 and x2 unchanged since)
+int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s);
 int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s);
+// therm_nblk > 0: finish the drift kernel's deferred update_therm_avs first
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
-                       int apply_box, cudaStream_t s);
+                       int apply_box, int therm_nblk, cudaStream_t s);
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 // update_therm_avs with the thermo finalization in its last block; prep
@@ -268,6 +271,7 @@ size_t adjoint_smem_bytes(int nlookup);
 void launch_table_adjoint(const DeviceState &d, const AdjointArgs &a, double *grads, double *scr,
                           const double *gF, cudaStream_t s);
 int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, double2 **e2d, float2 **e2fd,
+                         void **auxd,
                          Tables &t, double *rcull_out);
 int build_fetm_tables(HostTables &ht, int nv, const double *av, const double *rv, int np,
                       const double *ap, const double *rp, int uselookup, int nlookup);

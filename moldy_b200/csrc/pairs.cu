@@ -174,7 +174,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
             } else {
                 double4 qq[B];
 #pragma unroll
-                for (int u = 0; u < B; ++u) qq[u] = pos[ee[u] != -1 ? (ee[u] & kIdMask) : a];
+                for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
 #pragma unroll
                 for (int u = 0; u < B; ++u) {
                     if (ee[u] == -1) continue;
@@ -262,7 +262,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
             for (int u = 0; u < B; ++u) ee[u] = (e0 + u < ne) ? alist[(size_t)(e0 + u) * nm + a] : -1;
             double4 qq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = pos2[ee[u] != -1 ? (ee[u] & kIdMask) : a];
+            for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos2[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 if (ee[u] == -1) continue;
@@ -338,43 +338,9 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
 // |B0_build^-1|_F bounding the fractional separation of any listed pair.  The
 // list is rebuilt before that bound reaches the screening radius, and after
 // every half-list rebuild and every force call outside velocity Verlet, so
-// the screen keeps exactly the pairs a walk over the whole half list keeps.
-__device__ double frob(const double *m) {
-    double s = 0.0;
-    for (int k = 0; k < 9; ++k) s += m[k] * m[k];
-    return sqrt(s);
-}
-
-__global__ void k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut,
-                             int force, int apply_box) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    BoxState &B = *box;
-    if (apply_box) {   // velocityverlet box half (src/quench_m.F90:582-589)
-        if (p.ivol == 4) {
-            MAT(B.b1, 3, 3) = MAT(B.b1, 3, 3) + MAT(B.b2, 3, 3);
-            MAT(B.b0, 3, 3) = MAT(B.b0, 3, 3) + MAT(B.b1, 3, 3);
-        }
-        if (p.ivol < 1) {
-            for (int k = 0; k < 9; ++k) B.b1[k] = B.b1[k] + B.b2[k];
-            for (int k = 0; k < 9; ++k) B.b0[k] = B.b0[k] + B.b1[k];
-        }
-    }
-    double md = sqrt(__longlong_as_double((long long)B.maxdisp2));
-    B.maxdisp2 = 0ull;
-    double eps = 2.0e-6 * frob(B.b0) + 1.0e-4;
-    double db[9], inv[9];
-    for (int k = 0; k < 9; ++k) db[k] = B.b0[k] - B.bbuild[k];
-    bool ok = mat_invert(B.bbuild, inv);
-    double dmax = ok ? p.rnear * frob(inv) : 1e300;
-    double shrink = 2.0 * md + frob(db) * dmax;
-    int need = force || !ok || !(shrink < rmid - eps - (rcut + eps));
-    B.mid_rebuild = need;
-    if (need) {
-        for (int k = 0; k < 9; ++k) B.bbuild[k] = B.b0[k];
-        B.mid_builds += 1;
-    }
-}
-
+// the screen keeps exactly the pairs a walk over the whole half list keeps
+// (k_mid_decide applies the rule).
+//
 // The intermediate list is full: every half-list pair within r_mid (FP32
 // distance plus twice its error bound) is entered in both rows.  The owner
 // writes its own entries from the first slot with a local count (flagged in
@@ -444,11 +410,6 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
     }
 }
 
-void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
-                       int apply_box, cudaStream_t s) {
-    k_mid_decide<<<1, 32, 0, s>>>(p, d.box, rmid, rcut, force, apply_box);
-}
-
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
     k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_rev);
@@ -462,62 +423,82 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t
 // L2 prefetches of the next atom's rows and per-atom data; bit 2 asks for 3
 // resident blocks per SM instead of 2 (fewer registers per thread, more warps
 // to hide the gather latency).
+// One wave of resident blocks for the kernel (at 256 threads): every block
+// then runs the same number of grid-stride iterations (to within one), and no
+// partly filled last wave idles the SMs.  Computed once per instantiation.
+template <typename K>
+static int one_wave(K kernel) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+    const long long w = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+    return (int)(w < kMaxBlocks ? w : kMaxBlocks);
+}
+
+#define LAUNCH_WAVE(KERNEL, NB, S, ...)                      \
+    do {                                                     \
+        static const int wave_ = one_wave(KERNEL);           \
+        NB = NB < wave_ ? NB : wave_;                        \
+        KERNEL<<<NB, 256, 0, S>>>(__VA_ARGS__);              \
+    } while (0)
+
 template <int B, bool PF, int MINB>
-static void sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials, int nb,
-                       cudaStream_t s) {
+static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials,
+                      cudaStream_t s) {
 #define SD_ARGS p, t, d.pos, d.posf, d.pos2, d.box, d.mlist, d.mid_own, d.mid_rev, d.alist, d.pair_cnt, d.rho, d.afrho, \
                 d.dafrho, partials, d.flags
-    if (t.exact) k_screen_density<false, true, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
-    else if (mixed) k_screen_density<true, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
-    else k_screen_density<false, false, B, PF, MINB><<<nb, 256, 0, s>>>(SD_ARGS);
+    int nb = grid_blocks(p.nm, 256);
+    if (t.exact) LAUNCH_WAVE((k_screen_density<false, true, B, PF, MINB>), nb, s, SD_ARGS);
+    else if (mixed) LAUNCH_WAVE((k_screen_density<true, false, B, PF, MINB>), nb, s, SD_ARGS);
+    else LAUNCH_WAVE((k_screen_density<false, false, B, PF, MINB>), nb, s, SD_ARGS);
 #undef SD_ARGS
+    return nb;
 }
 
 int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
                           double *partials, cudaStream_t s) {
-    int nb = grid_blocks(p.nm, 256);
     switch (variant) {
-    case 0: sd_variant<4, true, 4>(d, p, t, mixed, partials, nb, s); break;
-    case 1: sd_variant<8, true, 4>(d, p, t, mixed, partials, nb, s); break;
-    case 2: sd_variant<4, true, 2>(d, p, t, mixed, partials, nb, s); break;
-    case 3: sd_variant<8, true, 2>(d, p, t, mixed, partials, nb, s); break;
-    case 4: sd_variant<4, false, 3>(d, p, t, mixed, partials, nb, s); break;
-    case 5: sd_variant<8, false, 3>(d, p, t, mixed, partials, nb, s); break;
-    case 6: sd_variant<4, true, 3>(d, p, t, mixed, partials, nb, s); break;
-    default: sd_variant<8, true, 3>(d, p, t, mixed, partials, nb, s); break;
+    case 0: return sd_variant<4, true, 4>(d, p, t, mixed, partials, s);
+    case 1: return sd_variant<8, true, 4>(d, p, t, mixed, partials, s);
+    case 2: return sd_variant<4, true, 2>(d, p, t, mixed, partials, s);
+    case 3: return sd_variant<8, true, 2>(d, p, t, mixed, partials, s);
+    case 4: return sd_variant<4, false, 3>(d, p, t, mixed, partials, s);
+    case 5: return sd_variant<8, false, 3>(d, p, t, mixed, partials, s);
+    case 6: return sd_variant<4, true, 3>(d, p, t, mixed, partials, s);
+    default: return sd_variant<8, true, 3>(d, p, t, mixed, partials, s);
     }
-    return nb;
 }
 
 template <int B, bool PF, bool STRESS, int MINB>
-static void forces_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode, double *partials,
-                           int nb, cudaStream_t s) {
+static int forces_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode, double *partials,
+                          cudaStream_t s) {
 #define FORCE_ARGS p, t, d.pos2, d.box, d.alist, d.pair_cnt, d.mass, d.znum, d.del2, d.f, d.x1, d.x2, d.stress, \
                    partials, mode
-    if (t.exact) k_forces<false, true, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
-    else if (mixed) k_forces<true, false, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
-    else k_forces<false, false, B, PF, STRESS, MINB><<<nb, 256, 0, s>>>(FORCE_ARGS);
+    int nb = grid_blocks(p.nm, 256);
+    if (t.exact) LAUNCH_WAVE((k_forces<false, true, B, PF, STRESS, MINB>), nb, s, FORCE_ARGS);
+    else if (mixed) LAUNCH_WAVE((k_forces<true, false, B, PF, STRESS, MINB>), nb, s, FORCE_ARGS);
+    else LAUNCH_WAVE((k_forces<false, false, B, PF, STRESS, MINB>), nb, s, FORCE_ARGS);
 #undef FORCE_ARGS
+    return nb;
 }
 
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s) {
-    int nb = grid_blocks(p.nm, 256);
-    if (p.atomstress) {
-        forces_variant<2, false, true, 2>(d, p, t, mixed, mode, partials, nb, s);
-        return nb;
-    }
+    if (p.atomstress) return forces_variant<2, false, true, 2>(d, p, t, mixed, mode, partials, s);
     switch (variant) {
-    case 0: forces_variant<2, true, false, 4>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 1: forces_variant<4, true, false, 4>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 2: forces_variant<2, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 3: forces_variant<4, true, false, 2>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 4: forces_variant<2, false, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 5: forces_variant<4, false, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
-    case 6: forces_variant<2, true, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
-    default: forces_variant<4, true, false, 3>(d, p, t, mixed, mode, partials, nb, s); break;
+    case 0: return forces_variant<2, true, false, 4>(d, p, t, mixed, mode, partials, s);
+    case 1: return forces_variant<4, true, false, 4>(d, p, t, mixed, mode, partials, s);
+    case 2: return forces_variant<2, true, false, 2>(d, p, t, mixed, mode, partials, s);
+    case 3: return forces_variant<4, true, false, 2>(d, p, t, mixed, mode, partials, s);
+    case 4: return forces_variant<2, false, false, 3>(d, p, t, mixed, mode, partials, s);
+    case 5: return forces_variant<4, false, false, 3>(d, p, t, mixed, mode, partials, s);
+    case 6: return forces_variant<2, true, false, 3>(d, p, t, mixed, mode, partials, s);
+    default: return forces_variant<4, true, false, 3>(d, p, t, mixed, mode, partials, s);
     }
-    return nb;
 }
 
 // list entries the screening pass reads per step (the full intermediate rows)
