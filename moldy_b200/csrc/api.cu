@@ -56,7 +56,7 @@ int dev_alloc(T **p, size_t n, const char *what) {
 
 __global__ void k_pack_pos(int nm, const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, int mask, double4 *__restrict__ pos,
-                           float4 *__restrict__ posf) {
+                           int4 *__restrict__ posq) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nm) return;
     double4 p = pos[a];
@@ -64,7 +64,7 @@ __global__ void k_pack_pos(int nm, const double *__restrict__ x, const double *_
     if (mask & 2) p.y = y[a];
     if (mask & 4) p.z = z[a];
     pos[a] = p;
-    posf[a] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    posq[a] = make_int4(fix32(p.x), fix32(p.y), fix32(p.z), 0);
 }
 
 __global__ void k_unpack_pos(int nm, const double4 *__restrict__ pos, double *__restrict__ xyz) {
@@ -168,7 +168,7 @@ Engine::~Engine() {
     void *bufs[] = {d.pos, d.x1, d.x2, d.f, d.rho, d.afrho, d.dafrho, d.stress, d.mass, d.del2,
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
-                    d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posf, d.pos2, d.alist,
+                    d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
                     d.pair_cnt, d.mlist, d.mid_own, d.mid_rev, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
@@ -228,7 +228,8 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.cell_atoms2, nm, "cell_atoms2"));
     CHECK(dev_alloc(&d.nlist, nm * (size_t)p.nnbrs, "nlist"));
     CHECK(dev_alloc(&d.numn, nm, "numn"));
-    CHECK(dev_alloc(&d.posf, nm, "posf"));
+    CHECK(dev_alloc(&d.posq, nm, "posq"));
+    CHECK(dev_alloc(&d.posq2, nm, "posq2"));
     CHECK(dev_alloc(&d.pos2, nm, "pos2"));
     CHECK(dev_alloc(&d.alist, nm * (size_t)p.pair_cap, "compact list"));
     CHECK(dev_alloc(&d.pair_cnt, nm, "pair_cnt"));
@@ -248,7 +249,8 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.dafrho, 0, nm * sizeof(double)), "memset dafrho");
     CUDA_CHECK(cudaMemset(d.stress, 0, 3 * nm * sizeof(double)), "memset stress");
     CUDA_CHECK(cudaMemset(d.numn, 0, nm * sizeof(int32_t)), "memset numn");
-    CUDA_CHECK(cudaMemset(d.posf, 0, nm * sizeof(float4)), "memset posf");
+    CUDA_CHECK(cudaMemset(d.posq, 0, nm * sizeof(int4)), "memset posq");
+    CUDA_CHECK(cudaMemset(d.posq2, 0, nm * sizeof(int4)), "memset posq2");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
     CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
     CUDA_CHECK(cudaMemset(d.mid_own, 0, nm * sizeof(int32_t)), "memset mid_own");
@@ -353,6 +355,7 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
     double rc = rcull < 1e150 ? rcull * (1.0 + 1.0e-12) : 1.0e150;
     t.rcull2 = rc * rc;
     t.rcull2f = (float)(rc * rc * (1.0 + 1.0e-6));
+    t.recipstep_f = (float)t.vp_recipstep;
     t.nv = h.nv; t.np = h.np;
     for (int i = 0; i < 8; ++i) { t.av[i] = h.av[i]; t.rv[i] = h.rv[i]; t.ap[i] = h.ap[i]; t.rp[i] = h.rp[i]; }
     t.bier_cut1 = h.bier_cut1; t.bier_cut2 = h.bier_cut2;
@@ -428,7 +431,7 @@ int Engine::set_state(const double *x0, const double *y0, const double *z0, cons
         if (z0) CUDA_CHECK(cudaMemcpyAsync(tmp + 2 * nm, z0, nb, cudaMemcpyHostToDevice, s), "set z0");
         int mask = (x0 ? 1 : 0) | (y0 ? 2 : 0) | (z0 ? 4 : 0);
         k_pack_pos<<<(prm.nm + 255) / 256, 256, 0, s>>>(prm.nm, tmp, tmp + nm, tmp + 2 * nm, mask, d.pos,
-                                                         d.posf);
+                                                         d.posq);
     }
     const double *v1[3] = {x1, y1, z1}, *v2[3] = {x2, y2, z2};
     for (int k = 0; k < 3; ++k) {

@@ -57,6 +57,7 @@ struct Tables {
     double e_rmin, e_rmax, e_range, e_reciprange, e_recipnlkp, e_recipstep;
     double rcull2;          // pairs with r^2 above this contribute exactly zero
     float rcull2f;
+    float recipstep_f;      // (float) vp_recipstep: node coordinate of r in the FP32 lookups
     // FETRANSMETAL Fe-Fe analytic data for exact mode / energy_calc
     int nv, np;
     double av[8], rv[8], ap[8], rp[8];
@@ -112,6 +113,39 @@ __device__ __forceinline__ void ldg8f(const float4 *p, float4 &a, float4 &b) {
         : "l"(p));
 }
 
+// ------------------------------------------------------- fixed point --
+// Fractional coordinates in 32-bit fixed point: one box length is 2^32 units,
+// so the difference of two coordinates taken in 32-bit integer arithmetic
+// wraps to the minimum image of a periodic direction by itself (within half a
+// box; the quantisation is 2^-33 box lengths).  Used by the mixed-precision
+// pair passes of fully periodic boxes.
+constexpr double kFixScale = 4294967296.0;               // 2^32
+constexpr double kFixUnit = 1.0 / 4294967296.0;          // 2^-32
+
+__device__ __forceinline__ int32_t fix32(double x) {
+    return (int32_t)(uint32_t)(unsigned long long)__double2ll_rn(x * kFixScale);
+}
+
+// A 32-bit integer as a float, rounded once to nearest, without the
+// conversion unit: the upper 20 and the lower 12 bits are each made exact
+// floats by adding them to the bit pattern of a power-of-two bias, then joined
+// by one fused multiply-add.
+__device__ __forceinline__ float fix_to_float(int32_t d) {
+    const int32_t hi = d >> 12;                                            // [-2^19, 2^19)
+    const int32_t lo = d & 0xfff;                                          // [0, 4096)
+    const float fhi = __int_as_float(0x4b400000 + hi) - 12582912.0f;      // bias 1.5 * 2^23
+    const float flo = __int_as_float(0x4b000000 + lo) - 8388608.0f;       // bias 2^23
+    return fmaf(fhi, 4096.0f, flo);
+}
+
+// floor(x) of 0 <= x < 2^23 as an integer and as a float, from one round-down
+// addition (no conversion unit)
+__device__ __forceinline__ int floor_small(float x, float &fl) {
+    const float b = __fadd_rd(fminf(x, 8388607.0f), 8388608.0f);
+    fl = b - 8388608.0f;
+    return __float_as_int(b) - 0x4b000000;
+}
+
 // ---------------------------------------------------------- table lookup --
 // get_value_from_lookup_veephi (src/lookup_m.F90:307-346) for the four r tables
 // at once; returns (vee, dvee, phi, dphi).
@@ -159,11 +193,14 @@ __device__ __forceinline__ double2 lookup_e2(const Tables &t, double rho) {
 }
 
 // FP32 variants for the mixed path (index arithmetic in FP32 as well)
+// FP32 lookups for the mixed path (r >= 0): the interval and its fraction
+// come from one multiply and a floor on the FMA pipe
 __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
-    int idx = (int)(((float)t.nlookup * r) * (float)t.vp_reciprange);
+    const float x = r * t.recipstep_f;
+    float fl;
+    const int idx = floor_small(x, fl);
     if (idx >= t.nr - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
-    idx = idx < 0 ? 0 : idx;
-    float dr = r * (float)t.vp_recipstep - (float)idx;
+    const float dr = x - fl;
     float4 a, b;
     ldg8f(&t.r4f[2 * idx], a, b);
     return make_float4(fmaf(b.x - a.x, dr, a.x), fmaf(b.y - a.y, dr, a.y),
@@ -171,10 +208,11 @@ __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
 }
 
 __device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
-    int idx = (int)(((float)t.nlookup * r) * (float)t.vp_reciprange);
+    const float x = r * t.recipstep_f;
+    float fl;
+    const int idx = floor_small(x, fl);
     if (idx >= t.nr - 1) return 0.f;
-    idx = idx < 0 ? 0 : idx;
-    float dr = r * (float)t.vp_recipstep - (float)idx;
+    const float dr = x - fl;
     const float2 v = __ldg(&t.phi2f[idx]);
     return fmaf(v.y - v.x, dr, v.x);
 }

@@ -315,7 +315,7 @@ void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut
 // which runs next, finishes them.
 template <bool THERM>
 __global__ void __launch_bounds__(256)
-k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
+k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
         const double4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
         double *__restrict__ kin_partials, double *__restrict__ therm_partials) {
@@ -354,7 +354,7 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
         q.y = q.y + (ey + wy);
         q.z = q.z + (ez + wz);
         pos[a] = q;
-        posf[a] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+        posq[a] = make_int4(fix32(q.x), fix32(q.y), fix32(q.z), 0);
         double4 xb = xbuild[a];
         double ux = q.x - xb.x, uy = q.y - xb.y, uz = q.z - xb.z;
         const volatile double *bv = nb;   // read per use, not held in registers
@@ -391,10 +391,10 @@ k_drift(Params p, double4 *__restrict__ pos, float4 *__restrict__ posf,
 int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s) {
     int nb = grid_blocks(p.nm, kAtomThreads);
     if (therm)
-        k_drift<true><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+        k_drift<true><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
                                                   kin_partials, d.partials);
     else
-        k_drift<false><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posf, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+        k_drift<false><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
                                                    kin_partials, nullptr);
     return nb;
 }

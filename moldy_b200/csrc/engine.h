@@ -39,9 +39,11 @@ struct DeviceState {
     // scratch of the structure analysis (rdf.cu), grown on demand
     void *rdf = nullptr;
     size_t rdf_bytes = 0;
-    // FP32 mirror of the positions (written by drift) for the screening pass
-    float4 *posf = nullptr;
-    // positions with F'(rho) in w, written by the density pass for the force pass
+    // fixed-point fractional positions (2^32 units per box length; written with
+    // pos) for the mixed screening pass; posq2 adds F'(rho) as a float in w for
+    // the mixed force pass
+    int4 *posq = nullptr, *posq2 = nullptr;
+    // positions with F'(rho) in w, written by the density pass for the FP64 force pass
     double4 *pos2 = nullptr;
     // compact full list of the pairs inside the table cut, entry-major:
     // entry e of atom i at alist[e * nm + i] (e < pair_cap), bit 31 set when

@@ -38,10 +38,11 @@ __device__ __forceinline__ void prefetch_l2(const void *ptr) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
 }
 
-template <bool MIXED>
-__device__ __forceinline__ void fsep(const float *bf, int ivol, float dx, float dy, float dz,
-                                     float &rx, float &ry, float &rz, float &r2,
-                                     float &odx, float &ody, float &odz) {
+// Squared FP32 distance of an FP64 fractional difference (any box): the
+// difference rounded to FP32 (off by at most 2^-24 |dx|), the minimum image by
+// rintf in the periodic directions.
+__device__ __forceinline__ float sep2_f32(const float *bf, int ivol, double dxd, double dyd, double dzd) {
+    float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
     if (ivol == 0 || ivol == 1 || ivol == 4) {
         dx -= rintf(dx); dy -= rintf(dy); dz -= rintf(dz);
     } else if (ivol == 2) {
@@ -49,11 +50,30 @@ __device__ __forceinline__ void fsep(const float *bf, int ivol, float dx, float 
     } else if (ivol == 5) {
         dz -= rintf(dz);
     }
-    rx = fmaf(bf[6], dz, fmaf(bf[3], dy, bf[0] * dx));
-    ry = fmaf(bf[7], dz, fmaf(bf[4], dy, bf[1] * dx));
-    rz = fmaf(bf[8], dz, fmaf(bf[5], dy, bf[2] * dx));
-    r2 = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
-    odx = dx; ody = dy; odz = dz;
+    const float rx = fmaf(bf[6], dz, fmaf(bf[3], dy, bf[0] * dx));
+    const float ry = fmaf(bf[7], dz, fmaf(bf[4], dy, bf[1] * dx));
+    const float rz = fmaf(bf[8], dz, fmaf(bf[5], dy, bf[2] * dx));
+    return fmaf(rz, rz, fmaf(ry, ry, rx * rx));
+}
+
+// Separation of two atoms from their fixed-point coordinates (fully periodic
+// box): the 32-bit differences are the minimum image; bs is B0 per fixed-point
+// unit.  Returns r^2 and the Cartesian separation, all FP32.
+__device__ __forceinline__ float fix_sep(const float *bs, const int4 &qa, const int4 &qj, float &rx, float &ry,
+                                         float &rz, float &dx, float &dy, float &dz) {
+    dx = fix_to_float((int32_t)((uint32_t)qa.x - (uint32_t)qj.x));
+    dy = fix_to_float((int32_t)((uint32_t)qa.y - (uint32_t)qj.y));
+    dz = fix_to_float((int32_t)((uint32_t)qa.z - (uint32_t)qj.z));
+    rx = fmaf(bs[6], dz, fmaf(bs[3], dy, bs[0] * dx));
+    ry = fmaf(bs[7], dz, fmaf(bs[4], dy, bs[1] * dx));
+    rz = fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx));
+    return fmaf(rz, rz, fmaf(ry, ry, rx * rx));
+}
+
+__device__ __forceinline__ float fix_sep(const float *bs, const int4 &qa, const int4 &qj, float &rx, float &ry,
+                                         float &rz) {
+    float dx, dy, dz;
+    return fix_sep(bs, qa, qj, rx, ry, rz, dx, dy, dz);
 }
 
 // --------------------------------------------------------------- screen --
@@ -103,8 +123,9 @@ __device__ __noinline__ bool inside_cut_fp64(const double4 *__restrict__ pos, in
 // outside the band [rin, rscreen] around the cut, the FP64 one inside it.
 template <bool MIXED, bool EXACT, int B, bool PF, int MINB>
 __global__ void __launch_bounds__(256, MINB)
-k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
-                 double4 *__restrict__ pos2, const BoxState *__restrict__ box, const int32_t *__restrict__ mlist,
+k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
+                 double4 *__restrict__ pos2, int4 *__restrict__ posq2, const BoxState *__restrict__ box,
+                 const int32_t *__restrict__ mlist,
                  const int32_t *__restrict__ mid_own, const int32_t *__restrict__ mid_rev,
                  int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
                  double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
@@ -121,9 +142,9 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
     }
     __syncthreads();
     double b[9];
-    float bf[9];
+    float bs[9];   // B0 in A per fixed-point unit (mixed)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) { b[k] = MIXED ? 0.0 : sb[k]; bf[k] = (float)sb[k]; }
+    for (int k = 0; k < 9; ++k) { b[k] = MIXED ? 0.0 : sb[k]; bs[k] = (float)(sb[k] * kFixUnit); }
     const float rscreen2 = MIXED ? srs2 : 0.f, rin2 = MIXED ? srin2 : 0.f;
     double v[2] = {0.0, 0.0};   // embedding energy, directed pairs
     const int nm = p.nm;
@@ -136,7 +157,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
 #pragma unroll
             for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
             prefetch_l2(&mid_own[an]); prefetch_l2(&mid_rev[an]);
-            prefetch_l2(MIXED ? (const void *)&posf[an] : (const void *)&pos[an]);
+            prefetch_l2(MIXED ? (const void *)&posq[an] : (const void *)&pos[an]);
             prefetch_l2(&dafrho[an]);
         }
         const int n_own = mid_own[a];
@@ -144,7 +165,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
         const int n = mc < p.mid_cap ? mc : p.mid_cap;
         const int rev_base = p.mid_cap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
         const double4 pa = MIXED ? make_double4(0.0, 0.0, 0.0, 0.0) : pos[a];
-        const float4 pf = MIXED ? posf[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int4 qa = MIXED ? posq[a] : make_int4(0, 0, 0, 0);
         double rho_a = 0.0;
         int cnt = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
@@ -155,19 +176,18 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
                 ee[u] = (k < n) ? __ldg(&mlist[(size_t)(k < n_own ? k : rev_base - k) * stride + a]) : -1;
             }
             if (MIXED) {
-                float4 qq[B];
+                int4 qq[B];
 #pragma unroll
-                for (int u = 0; u < B; ++u) qq[u] = __ldg(&posf[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
+                for (int u = 0; u < B; ++u) qq[u] = __ldg(&posq[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
 #pragma unroll
                 for (int u = 0; u < B; ++u) {
                     if (ee[u] == -1) continue;
-                    float rx, ry, rz, r2, dx, dy, dz;
-                    fsep<true>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz, r2, dx, dy,
-                               dz);
+                    float rx, ry, rz;
+                    const float r2 = fix_sep(bs, qa, qq[u], rx, ry, rz);
                     if (r2 > rscreen2) continue;
                     // inside the error band: the FP64 distance decides
                     if (!(r2 < rin2) && !inside_cut_fp64(pos, a, ee[u] & kIdMask, sb, p.ivol, t.rcull2)) continue;
-                    rho_a += (double)lookup_phif(t, sqrtf(r2));
+                    rho_a += (double)lookup_phif(t, r2 * rsqrtf(r2));
                     if (cnt < p.pair_cap) alist[(size_t)cnt * stride + a] = ee[u];
                     ++cnt;
                 }
@@ -206,8 +226,8 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
             v[0] += e.x;
         }
         rho[a] = rho_a;
-        const double4 pw = MIXED ? pos[a] : pa;
-        pos2[a] = make_double4(pw.x, pw.y, pw.z, fd);
+        if (MIXED) posq2[a] = make_int4(qa.x, qa.y, qa.z, __float_as_int((float)fd));
+        else pos2[a] = make_double4(pa.x, pa.y, pa.z, fd);
     }
     if (over & 1) { atomicExch(&flags[3], 1); atomicMax(&flags[4], over_max); }
     if (over & 2) { atomicExch(&flags[5], 1); atomicMax(&flags[6], over_max); }
@@ -219,7 +239,8 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const floa
 // D = sum d d^T fp / 2 (tp = B0 D); mode 1 adds the velocity-Verlet second half
 template <bool MIXED, bool EXACT, int B, bool PF, bool STRESS, int MINB>
 __global__ void __launch_bounds__(256, MINB)
-k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *__restrict__ box,
+k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__restrict__ posq2,
+         const BoxState *__restrict__ box,
          const int32_t *__restrict__ alist, const int32_t *__restrict__ pair_cnt, const double *__restrict__ mass,
          const int32_t *__restrict__ znum, const double *__restrict__ del2,
          double *__restrict__ f, double *__restrict__ x1, double *__restrict__ x2,
@@ -231,9 +252,9 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
     }
     __syncthreads();
     double b[9];
-    float bf[9];
+    float bs[9];   // B0 in A per fixed-point unit (mixed)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bf[k] = (float)sb[k]; }
+    for (int k = 0; k < 9; ++k) { b[k] = sb[k]; bs[k] = (float)(sb[k] * kFixUnit); }
     double v[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) v[k] = 0.0;
@@ -244,7 +265,8 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
             const int an = a + astride;
 #pragma unroll
             for (int u = 0; u < 8; ++u) prefetch_l2(&alist[(size_t)u * nm + an]);
-            prefetch_l2(&pair_cnt[an]); prefetch_l2(&pos2[an]); prefetch_l2(&mass[an]);
+            prefetch_l2(&pair_cnt[an]); prefetch_l2(MIXED ? (const void *)&posq2[an] : (const void *)&pos2[an]);
+            prefetch_l2(&mass[an]);
             if (mode == 1) {
                 prefetch_l2(&x1[an]); prefetch_l2(&x1[nm + an]); prefetch_l2(&x1[2 * nm + an]);
                 prefetch_l2(&x2[an]); prefetch_l2(&x2[nm + an]); prefetch_l2(&x2[2 * nm + an]);
@@ -253,50 +275,80 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const BoxState *_
         }
         int ne = pair_cnt[a];
         ne = ne < p.pair_cap ? ne : p.pair_cap;
-        const double4 pa = pos2[a];
         const double ma = mass[a];
         double fxa = 0.0, fya = 0.0, fza = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int e0 = 0; e0 < ne; e0 += B) {
-            int ee[B];
+        if constexpr (MIXED) {
+            // fixed-point separations, FP32 geometry, tables and pair forces;
+            // forces summed in FP64, the atom's energy and virial moments in
+            // FP32 over its row and in FP64 over atoms
+            const int4 qa = posq2[a];
+            const float fa = __int_as_float(qa.w);
+            double gx = 0.0, gy = 0.0, gz = 0.0;   // sum of d fp, fixed-point units
+            float ve = 0.f, w0 = 0.f, w1 = 0.f, w2 = 0.f, w3 = 0.f, w4 = 0.f, w5 = 0.f;
+            float tx = 0.f, ty = 0.f, tz = 0.f;
+            for (int e0 = 0; e0 < ne; e0 += B) {
+                int ee[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) ee[u] = (e0 + u < ne) ? alist[(size_t)(e0 + u) * nm + a] : -1;
-            double4 qq[B];
+                for (int u = 0; u < B; ++u) ee[u] = (e0 + u < ne) ? alist[(size_t)(e0 + u) * nm + a] : -1;
+                int4 qq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos2[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
+                for (int u = 0; u < B; ++u) qq[u] = __ldg(&posq2[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
 #pragma unroll
-            for (int u = 0; u < B; ++u) {
-                if (ee[u] == -1) continue;
-                const int j = ee[u] & kIdMask;
-                const double4 q = qq[u];
-                double dx = pa.x - q.x, dy = pa.y - q.y, dz = pa.z - q.z;
-                double fp, vee, rx, ry, rz;
-                if (MIXED) {
-                    float frx, fry, frz, r2, ex, ey, ez;
-                    fsep<true>(bf, p.ivol, (float)dx, (float)dy, (float)dz, frx, fry, frz, r2, ex, ey, ez);
-                    float r = sqrtf(r2), rr = 1.0f / r;
-                    float4 tv = lookup_r4f(t, r);
-                    fp = (double)(-(tv.y + tv.w * ((float)pa.w + (float)q.w)) * rr);
-                    vee = (double)tv.x;
-                    dx = (double)ex; dy = (double)ey; dz = (double)ez;
-                    rx = (double)frx; ry = (double)fry; rz = (double)frz;
-                } else {
+                for (int u = 0; u < B; ++u) {
+                    if (ee[u] == -1) continue;
+                    const int j = ee[u] & kIdMask;
+                    float rx, ry, rz, dx, dy, dz;
+                    const float r2 = fix_sep(bs, qa, qq[u], rx, ry, rz, dx, dy, dz);
+                    const float rr = rsqrtf(r2);
+                    const float4 tv = lookup_r4f(t, r2 * rr);    // vee, dvee, phi, dphi
+                    const float fp = -(tv.y + tv.w * (fa + __int_as_float(qq[u].w))) * rr;
+                    const float dfx = dx * fp, dfy = dy * fp, dfz = dz * fp;
+                    gx += (double)dfx; gy += (double)dfy; gz += (double)dfz;
+                    ve += tv.x;
+                    if (ma > 0.1 || ma + mass[j] > 0.1) {
+                        w0 = fmaf(dx, dfx, w0); w1 = fmaf(dy, dfy, w1); w2 = fmaf(dz, dfz, w2);
+                        w3 = fmaf(dx, dfy, w3); w4 = fmaf(dx, dfz, w4); w5 = fmaf(dy, dfz, w5);
+                    }
+                    if (STRESS && (ee[u] & kOwnBit)) { tx = fmaf(rx, fp, tx); ty = fmaf(ry, fp, ty); tz = fmaf(rz, fp, tz); }
+                }
+            }
+            fxa = gx * kFixUnit; fya = gy * kFixUnit; fza = gz * kFixUnit;
+            const double u2 = kFixUnit * kFixUnit;
+            v[0] += (double)ve;
+            v[1] += (double)w0 * u2; v[2] += (double)w1 * u2; v[3] += (double)w2 * u2;
+            v[4] += (double)w3 * u2; v[5] += (double)w4 * u2; v[6] += (double)w5 * u2;
+            sx = (double)tx; sy = (double)ty; sz = (double)tz;
+        } else {
+            const double4 pa = pos2[a];
+            for (int e0 = 0; e0 < ne; e0 += B) {
+                int ee[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) ee[u] = (e0 + u < ne) ? alist[(size_t)(e0 + u) * nm + a] : -1;
+                double4 qq[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos2[ee[u] != -1 ? (ee[u] & kIdMask) : a]);
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if (ee[u] == -1) continue;
+                    const int j = ee[u] & kIdMask;
+                    const double4 q = qq[u];
+                    double dx = pa.x - q.x, dy = pa.y - q.y, dz = pa.z - q.z;
                     min_image(p.ivol, dx, dy, dz);
-                    rx = b[0] * dx + b[3] * dy + b[6] * dz;
-                    ry = b[1] * dx + b[4] * dy + b[7] * dz;
-                    rz = b[2] * dx + b[5] * dy + b[8] * dz;
-                    double r = sqrt(rx * rx + ry * ry + rz * rz);
-                    double rr = 1.0 / r;
-                    double4 tv = EXACT ? pair_funcs(t, r) : lookup_r4(t, r);    // vee, dvee, phi, dphi
-                    fp = -tv.y * rr - (tv.w * pa.w + tv.w * q.w) * rr;
-                    vee = tv.x;
+                    const double rx = b[0] * dx + b[3] * dy + b[6] * dz;
+                    const double ry = b[1] * dx + b[4] * dy + b[7] * dz;
+                    const double rz = b[2] * dx + b[5] * dy + b[8] * dz;
+                    const double r = sqrt(rx * rx + ry * ry + rz * rz);
+                    const double rr = 1.0 / r;
+                    const double4 tv = EXACT ? pair_funcs(t, r) : lookup_r4(t, r);    // vee, dvee, phi, dphi
+                    const double fp = -tv.y * rr - (tv.w * pa.w + tv.w * q.w) * rr;
+                    fxa += dx * fp; fya += dy * fp; fza += dz * fp;
+                    v[0] += tv.x;
+                    if (ma > 0.1 || ma + mass[j] > 0.1) {
+                        v[1] += dx * dx * fp; v[2] += dy * dy * fp; v[3] += dz * dz * fp;
+                        v[4] += dx * dy * fp; v[5] += dx * dz * fp; v[6] += dy * dz * fp;
+                    }
+                    if (STRESS && (ee[u] & kOwnBit)) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
                 }
-                fxa += dx * fp; fya += dy * fp; fza += dz * fp;
-                v[0] += vee;
-                if (ma > 0.1 || ma + mass[j] > 0.1) {
-                    v[1] += dx * dx * fp; v[2] += dy * dy * fp; v[3] += dz * dz * fp;
-                    v[4] += dx * dy * fp; v[5] += dx * dz * fp; v[6] += dy * dz * fp;
-                }
-                if (STRESS && (ee[u] & kOwnBit)) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
             }
         }
         f[a] = fxa; f[nm + a] = fya; f[2 * nm + a] = fza;
@@ -353,7 +405,7 @@ __global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *_
 }
 
 __global__ void __launch_bounds__(256)
-k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4 *__restrict__ posf,
+k_mid_build(Params p, double rmid, const double4 *__restrict__ pos,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
             const int32_t *__restrict__ numn, int32_t *__restrict__ mlist,
             int32_t *__restrict__ mid_own, int32_t *__restrict__ mid_rev, double4 *__restrict__ xbuild) {
@@ -380,22 +432,21 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const int n = numn[a];
         const int32_t *col = nlist + a;
-        const float4 pf = posf[a];
+        const double4 pa = pos[a];
         int own = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
             int jj[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) jj[u] = (k0 + u < n) ? __ldg(&col[(size_t)(k0 + u) * stride]) : -1;
-            float4 qq[B];
+            double4 qq[B];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = __ldg(&posf[jj[u] >= 0 ? jj[u] : a]);
+            for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos[jj[u] >= 0 ? jj[u] : a]);
             int slot[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 slot[u] = -1;
                 if (jj[u] < 0) continue;
-                float rx, ry, rz, r2, dx, dy, dz;
-                fsep<true>(bf, p.ivol, pf.x - qq[u].x, pf.y - qq[u].y, pf.z - qq[u].z, rx, ry, rz, r2, dx, dy, dz);
+                const float r2 = sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
                 if (!(r2 <= keep2)) { jj[u] = -1; continue; }
                 if (own < cap) mlist[(size_t)own * stride + a] = jj[u] | kOwnBit;
                 ++own;
@@ -413,7 +464,7 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const float4
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
     int nb = grid_blocks(p.nm, 256);
     k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_rev);
-    k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.posf, d.box, d.nlist, d.numn, d.mlist,
+    k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.box, d.nlist, d.numn, d.mlist,
                                    d.mid_own, d.mid_rev, d.xbuild);
 }
 
@@ -449,8 +500,8 @@ static int one_wave(K kernel) {
 template <int B, bool PF, int MINB>
 static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials,
                       cudaStream_t s) {
-#define SD_ARGS p, t, d.pos, d.posf, d.pos2, d.box, d.mlist, d.mid_own, d.mid_rev, d.alist, d.pair_cnt, d.rho, d.afrho, \
-                d.dafrho, partials, d.flags
+#define SD_ARGS p, t, d.pos, d.posq, d.pos2, d.posq2, d.box, d.mlist, d.mid_own, d.mid_rev, d.alist, d.pair_cnt, \
+                d.rho, d.afrho, d.dafrho, partials, d.flags
     int nb = grid_blocks(p.nm, 256);
     if (t.exact) LAUNCH_WAVE((k_screen_density<false, true, B, PF, MINB>), nb, s, SD_ARGS);
     else if (mixed) LAUNCH_WAVE((k_screen_density<true, false, B, PF, MINB>), nb, s, SD_ARGS);
@@ -459,8 +510,13 @@ static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mix
     return nb;
 }
 
+// The mixed passes take the minimum image from fixed-point differences, which
+// needs a box periodic in all three directions; other boxes run in FP64.
+static inline bool mixed_applies(const Params &p) { return p.ivol == 0 || p.ivol == 1 || p.ivol == 4; }
+
 int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
                           double *partials, cudaStream_t s) {
+    mixed = mixed && mixed_applies(p);
     switch (variant) {
     case 0: return sd_variant<4, true, 4>(d, p, t, mixed, partials, s);
     case 1: return sd_variant<8, true, 4>(d, p, t, mixed, partials, s);
@@ -476,8 +532,8 @@ int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool
 template <int B, bool PF, bool STRESS, int MINB>
 static int forces_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode, double *partials,
                           cudaStream_t s) {
-#define FORCE_ARGS p, t, d.pos2, d.box, d.alist, d.pair_cnt, d.mass, d.znum, d.del2, d.f, d.x1, d.x2, d.stress, \
-                   partials, mode
+#define FORCE_ARGS p, t, d.pos2, d.posq2, d.box, d.alist, d.pair_cnt, d.mass, d.znum, d.del2, d.f, d.x1, d.x2, \
+                   d.stress, partials, mode
     int nb = grid_blocks(p.nm, 256);
     if (t.exact) LAUNCH_WAVE((k_forces<false, true, B, PF, STRESS, MINB>), nb, s, FORCE_ARGS);
     else if (mixed) LAUNCH_WAVE((k_forces<true, false, B, PF, STRESS, MINB>), nb, s, FORCE_ARGS);
@@ -488,6 +544,7 @@ static int forces_variant(DeviceState &d, const Params &p, const Tables &t, bool
 
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s) {
+    mixed = mixed && mixed_applies(p);
     if (p.atomstress) return forces_variant<2, false, true, 2>(d, p, t, mixed, mode, partials, s);
     switch (variant) {
     case 0: return forces_variant<2, true, false, 4>(d, p, t, mixed, mode, partials, s);
