@@ -122,8 +122,10 @@ __device__ __forceinline__ void ldg8f(const float4 *p, float4 &a, float4 &b) {
 constexpr double kFixScale = 4294967296.0;               // 2^32
 constexpr double kFixUnit = 1.0 / 4294967296.0;          // 2^-32
 
+// round(x 2^32) mod 2^32 (ties to even) for |x| < 2^19: one fused multiply-add
+// against the bias 1.5 * 2^52 leaves the integer in the low mantissa bits
 __device__ __forceinline__ int32_t fix32(double x) {
-    return (int32_t)(uint32_t)(unsigned long long)__double2ll_rn(x * kFixScale);
+    return __double2loint(fma(x, kFixScale, 6755399441055744.0));
 }
 
 // A 32-bit integer as a float, rounded once to nearest, without the

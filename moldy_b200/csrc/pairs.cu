@@ -31,6 +31,30 @@
 
 namespace moldy {
 
+// One wave of resident blocks for the kernel (at 256 threads): every block
+// then runs the same number of grid-stride iterations (to within one), and no
+// partly filled last wave idles the SMs.  Computed once per instantiation.
+template <typename K>
+static int one_wave(K kernel) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+    const long long w = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+    return (int)(w < kMaxBlocks ? w : kMaxBlocks);
+}
+
+#define LAUNCH_WAVE(KERNEL, NB, S, ...)                      \
+    do {                                                     \
+        static const int wave_ = one_wave(KERNEL);           \
+        NB = NB < wave_ ? NB : wave_;                        \
+        KERNEL<<<NB, 256, 0, S>>>(__VA_ARGS__);              \
+    } while (0)
+
+
 
 // L2 prefetch of one address (no register result; the address is always
 // inside an allocated buffer)
@@ -404,8 +428,9 @@ __global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *_
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) mid_rev[a] = 0;
 }
 
+template <bool FIX>
 __global__ void __launch_bounds__(256)
-k_mid_build(Params p, double rmid, const double4 *__restrict__ pos,
+k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
             const int32_t *__restrict__ numn, int32_t *__restrict__ mlist,
             int32_t *__restrict__ mid_own, int32_t *__restrict__ mid_rev, double4 *__restrict__ xbuild) {
@@ -423,9 +448,9 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos,
         skeep2 = screen_radius2(sb, rmid * rmid) > 1e37f ? 3.0e38f : keep * keep;
     }
     __syncthreads();
-    float bf[9];
+    float bf[9];   // B0, per fixed-point unit when FIX
 #pragma unroll
-    for (int k = 0; k < 9; ++k) bf[k] = (float)sb[k];
+    for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
     const float keep2 = skeep2;
     const int nm = p.nm, cap = p.mid_cap;
     const size_t stride = (size_t)nm;
@@ -433,20 +458,27 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos,
         const int n = numn[a];
         const int32_t *col = nlist + a;
         const double4 pa = pos[a];
+        const int4 qa = FIX ? posq[a] : make_int4(0, 0, 0, 0);
         int own = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
             int jj[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) jj[u] = (k0 + u < n) ? __ldg(&col[(size_t)(k0 + u) * stride]) : -1;
-            double4 qq[B];
+            double4 qq[FIX ? 1 : B];
+            int4 qi[FIX ? B : 1];
 #pragma unroll
-            for (int u = 0; u < B; ++u) qq[u] = ldg4(&pos[jj[u] >= 0 ? jj[u] : a]);
+            for (int u = 0; u < B; ++u) {
+                if (FIX) qi[u] = __ldg(&posq[jj[u] >= 0 ? jj[u] : a]);
+                else qq[u] = ldg4(&pos[jj[u] >= 0 ? jj[u] : a]);
+            }
             int slot[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 slot[u] = -1;
                 if (jj[u] < 0) continue;
-                const float r2 = sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
+                float rx, ry, rz;
+                const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
+                                     : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
                 if (!(r2 <= keep2)) { jj[u] = -1; continue; }
                 if (own < cap) mlist[(size_t)own * stride + a] = jj[u] | kOwnBit;
                 ++own;
@@ -457,15 +489,23 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos,
                 if (slot[u] >= 0 && slot[u] < cap) mlist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
         }
         mid_own[a] = own;
-        xbuild[a] = pos[a];
+        xbuild[a] = pa;
     }
 }
 
+// fixed-point separations in a fully periodic box, FP64 differences otherwise;
+// both launches exit at once when no build was decided, so their grids are one
+// resident wave
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
+    int nc = grid_blocks(p.nm, 256);
+    LAUNCH_WAVE(k_mid_clear, nc, s, d.box, p.nm, d.mid_rev);
     int nb = grid_blocks(p.nm, 256);
-    k_mid_clear<<<nb, 256, 0, s>>>(d.box, p.nm, d.mid_rev);
-    k_mid_build<<<nb, 256, 0, s>>>(p, rmid, d.pos, d.box, d.nlist, d.numn, d.mlist,
-                                   d.mid_own, d.mid_rev, d.xbuild);
+    if (p.ivol == 0 || p.ivol == 1 || p.ivol == 4)
+        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.mlist, d.mid_own,
+                    d.mid_rev, d.xbuild);
+    else
+        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.mlist, d.mid_own,
+                    d.mid_rev, d.xbuild);
 }
 
 // ------------------------------------------------------------ launchers --
@@ -474,29 +514,6 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t
 // L2 prefetches of the next atom's rows and per-atom data; bit 2 asks for 3
 // resident blocks per SM instead of 2 (fewer registers per thread, more warps
 // to hide the gather latency).
-// One wave of resident blocks for the kernel (at 256 threads): every block
-// then runs the same number of grid-stride iterations (to within one), and no
-// partly filled last wave idles the SMs.  Computed once per instantiation.
-template <typename K>
-static int one_wave(K kernel) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess) {
-        cudaGetLastError();
-        per_sm = 0;
-    }
-    const long long w = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
-    return (int)(w < kMaxBlocks ? w : kMaxBlocks);
-}
-
-#define LAUNCH_WAVE(KERNEL, NB, S, ...)                      \
-    do {                                                     \
-        static const int wave_ = one_wave(KERNEL);           \
-        NB = NB < wave_ ? NB : wave_;                        \
-        KERNEL<<<NB, 256, 0, S>>>(__VA_ARGS__);              \
-    } while (0)
-
 template <int B, bool PF, int MINB>
 static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials,
                       cudaStream_t s) {
