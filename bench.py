@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both",
                     help="both: the mixed path is the headline value, the FP64 path is timed beside it")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--skins", default=None,
+                    help="md: intermediate/outer list skins in A (e.g. 0.15/0.8) instead of the sweep")
     ap.add_argument("--nve-steps", type=int, default=1000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-quench", action="store_true", help="batch: skip the quench")
@@ -273,25 +275,33 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     sysm.md_init()
     tune = sysm.autotune(nreps=5)
     stream = torch.cuda.ExternalStream(sysm.stream_handle(), device=local_rank)
-    # untimed: the intermediate-list skin that gives the shortest steps here
+    # untimed: the intermediate- and outer-list skins that give the shortest
+    # steps here (outer rebuilds are rare, so each pair runs 100 steps)
     skin_ms = {}
-    for skin in (0.2, 0.3, 0.45, 0.9):
-        sysm.set_mid_skin(skin)
-        sysm.md_steps(20, thermo=False)
+    grid = [tuple(float(x) for x in args.skins.split("/"))] if args.skins else \
+        [(mid, out) for mid in (0.1, 0.15, 0.2) for out in (0.6, 0.8, 1.0)]
+    for mid, out in grid:
+        sysm.set_mid_skin(mid)
+        sysm.set_outer_skin(out)
+        sysm.md_steps(10, thermo=False)
         t0 = time.perf_counter()
-        sysm.md_steps(60, thermo=False)
+        sysm.md_steps(100, thermo=False)
         sysm.synchronize()
-        skin_ms[skin] = (time.perf_counter() - t0) * 1000.0 / 60
-    best_skin = min(skin_ms, key=skin_ms.get)
-    sysm.set_mid_skin(best_skin)
-    tune["mid_skin_ms_per_step"] = skin_ms
-    tune["chosen"]["mid_skin_A"] = best_skin
+        skin_ms[f"{mid}/{out}"] = (time.perf_counter() - t0) * 1000.0 / 100
+    best = min(skin_ms, key=skin_ms.get)
+    best_mid, best_out = (float(x) for x in best.split("/"))
+    sysm.set_mid_skin(best_mid)
+    sysm.set_outer_skin(best_out)
+    tune["list_skins_ms_per_step"] = skin_ms
+    tune["chosen"]["mid_skin_A"] = best_mid
+    tune["chosen"]["outer_skin_A"] = best_out
     sysm.md_steps(max(args.warmup, 3), thermo=False)
     sysm.synchronize()
     # the timed steps run without the per-launch events of the profiler
     # (launch counts are kept either way)
     sysm.reset_kernel_stats()
     builds0 = sysm.list_stats()["mid_builds"]
+    obuilds0 = sysm.outer_builds()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
@@ -309,6 +319,7 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     ms_max = max_over_ranks(ms)
     value = world * w.nm * args.steps / (ms_max / 1000.0)
     lst_timed = sysm.list_stats()
+    out_builds_per_step = (sysm.outer_builds() - obuilds0) / args.steps
     # then a profiled stretch: per-kernel CUDA-event times on the library's stream
     prof_steps = min(args.steps, 300)
     sysm.reset_kernel_stats()
@@ -366,7 +377,8 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     sysm.close()
     return {"value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "stats": stats,
             "roofline": roofline, "e2e": e2e, "clocks": clk.summary(), "tune": tune,
-            "n_half": n_half, "n_full": n_full, "n_screen": n_screen, "mid_builds_per_step": mid_builds_per_step}
+            "n_half": n_half, "n_full": n_full, "n_screen": n_screen, "mid_builds_per_step": mid_builds_per_step,
+            "out_builds_per_step": out_builds_per_step}
 
 
 def accuracy(w, local_rank, nve_steps):
@@ -455,7 +467,8 @@ def run_ours(args):
     extra = {"neighbours_half_mean": r["n_half"], "screened_entries_per_atom": r["n_screen"],
              "interacting_pairs_per_atom": r["n_full"], "autotuned_variants": r["tune"]["chosen"],
              "intermediate_list_builds_per_step": r["mid_builds_per_step"],
-             "mid_skin_ms_per_step": r["tune"].get("mid_skin_ms_per_step")}
+             "outer_list_builds_per_step": r["out_builds_per_step"],
+             "list_skins_ms_per_step": r["tune"].get("list_skins_ms_per_step")}
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": r["ms_per_step"],

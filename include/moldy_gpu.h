@@ -213,18 +213,25 @@ const char *moldy_gpu_kernel_name(int32_t kernel);
  * then forces; chosen (3, may be NULL) the selected variants in that order.
  * moldy_gpu_set_variants takes the same three numbers (the second is unused). */
 #define MOLDY_TUNE_VARIANTS 8
-/* Skin of the intermediate list (A, default 0.9): it holds the half-list pairs
+/* Skin of the intermediate list (A, default 0.3): it holds the half-list pairs
  * within min(rnear, table cut + skin) and is rebuilt on the device whenever
  * the displacements since its build could bring an unlisted pair inside the
- * cut.  Results do not depend on it; only the time per step does. */
+ * cut.  It is filtered from the outer list, the half-list pairs within
+ * min(rnear, table cut + max(outer skin, skin + 0.4)) (outer skin default
+ * 1.0 A), which is rebuilt from the half list whenever the displacements since
+ * its own build could bring an unlisted pair within the intermediate radius.
+ * Results depend on neither skin; only the time per step does. */
 int moldy_gpu_set_mid_skin(moldy_gpu *h, double skin);
+int moldy_gpu_set_outer_skin(moldy_gpu *h, double skin);
+/* builds of the outer list so far */
+int moldy_gpu_get_outer_builds(moldy_gpu *h, int32_t *builds);
 int moldy_gpu_autotune(moldy_gpu *h, int32_t nreps, double *times_ms, int32_t *chosen);
 int moldy_gpu_set_variants(moldy_gpu *h, int32_t screen, int32_t density, int32_t forces);
 /* out3[0]: directed interacting pairs (inside the table range) of the last
  * force evaluation, twice the contributing half-list pairs; out3[1]: how many
- * times the intermediate list (half-list pairs within the table cut + 0.9 A)
+ * times the intermediate list (half-list pairs within the table cut + skin)
  * has been built; out3[2]: list entries the screening pass reads per step
- * (the intermediate rows, or the half-list row where one overflowed). */
+ * (the intermediate rows). */
 int moldy_gpu_get_list_stats(moldy_gpu *h, double *out3);
 
 /* adjoint (no counterpart in the reference) ---------------------------------*/

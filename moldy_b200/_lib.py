@@ -103,6 +103,8 @@ SIGNATURES = {
     "moldy_gpu_set_iron_carbon_fe": [H, ctypes.c_int32],
     "moldy_ic_build_tables": [ctypes.c_int32, D, D, D, D, D, D],
     "moldy_gpu_set_mid_skin": [H, ctypes.c_double],
+    "moldy_gpu_set_outer_skin": [H, ctypes.c_double],
+    "moldy_gpu_get_outer_builds": [H, ctypes.POINTER(ctypes.c_int32)],
     "moldy_gpu_set_thermostat": [H, ctypes.c_double, ctypes.c_double],
     "moldy_gpu_get_thermostat": [H, D],
     "moldy_gpu_scalev": [H],

@@ -156,6 +156,7 @@ Engine::Engine(const moldy_params &p) {
     prm.ncell = 0;
     prm.pair_cap = kPairCapMin;
     prm.mid_cap = kMidCapMin;
+    prm.out_cap = kOutCapMin;
     ntcm_ = p.ntcm;
     ntc_ = p.ntc;
     precision_ = p.precision;
@@ -169,7 +170,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
-                    d.pair_cnt, d.mlist, d.mid_own, d.mid_rev, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.olist, d.out_own, d.out_rev, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -233,12 +234,15 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.pos2, nm, "pos2"));
     CHECK(dev_alloc(&d.alist, nm * (size_t)p.pair_cap, "compact list"));
     CHECK(dev_alloc(&d.pair_cnt, nm, "pair_cnt"));
+    CHECK(dev_alloc(&d.olist, nm * (size_t)p.out_cap, "outer list"));
+    CHECK(dev_alloc(&d.out_own, nm, "out_own"));
+    CHECK(dev_alloc(&d.out_rev, nm, "out_rev"));
+    CHECK(dev_alloc(&d.xout, nm, "xout"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
-    CHECK(dev_alloc(&d.mid_own, nm, "mid_own"));
-    CHECK(dev_alloc(&d.mid_rev, nm, "mid_rev"));
+    CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
     CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
     CHECK(dev_alloc(&d.partials, 3 * (size_t)kMaxBlocks * kPartials, "partials"));
-    CHECK(dev_alloc(&d.flags, 8, "flags"));
+    CHECK(dev_alloc(&d.flags, 12, "flags"));
     CHECK(dev_alloc(&d.box, 1, "box"));
     CUDA_CHECK(cudaMemset(d.pos, 0, nm * sizeof(double4)), "memset pos");
     CUDA_CHECK(cudaMemset(d.x1, 0, 3 * nm * sizeof(double)), "memset x1");
@@ -253,10 +257,11 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.posq2, 0, nm * sizeof(int4)), "memset posq2");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
     CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
-    CUDA_CHECK(cudaMemset(d.mid_own, 0, nm * sizeof(int32_t)), "memset mid_own");
-    CUDA_CHECK(cudaMemset(d.mid_rev, 0, nm * sizeof(int32_t)), "memset mid_rev");
+    CUDA_CHECK(cudaMemset(d.out_own, 0, nm * sizeof(int32_t)), "memset out_own");
+    CUDA_CHECK(cudaMemset(d.out_rev, 0, nm * sizeof(int32_t)), "memset out_rev");
+    CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(double4)), "memset xbuild");
-    CUDA_CHECK(cudaMemset(d.flags, 0, 8 * sizeof(int32_t)), "memset flags");
+    CUDA_CHECK(cudaMemset(d.flags, 0, 12 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
     return MOLDY_OK;
@@ -372,7 +377,7 @@ int Engine::upload_tables() {
     double rc = 0.0;
     CHECK(upload_device_tables(ht, &d.tab_r4, &d.tab_r4f, &d.tab_e2, &d.tab_e2f, &d.tab_aux, tab, &rc));
     rcut = rc < 1e150 ? rc : prm.rnear;
-    rmid = std::min(prm.rnear, rcut + mid_skin);
+    set_list_radii();
     potential_set_ = true;
     forces_current_ = false;
     return MOLDY_OK;
@@ -543,7 +548,7 @@ int Engine::get_linkcells(int32_t *l0, int32_t *link, int32_t *ic) {
 }
 
 int Engine::check_flags() {
-    int32_t f[8];
+    int32_t f[12];
     CUDA_CHECK(cudaMemcpyAsync(f, d.flags, sizeof(f), cudaMemcpyDeviceToHost, stream_), "flags");
     int32_t st = 0;
     CUDA_CHECK(cudaMemcpyAsync(&st, &d.box->status, sizeof(st), cudaMemcpyDeviceToHost, stream_), "flags");
@@ -561,11 +566,16 @@ int Engine::check_flags() {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
         return fail(MOLDY_ERR_CAPACITY, "link-cell relink produced inconsistent cell counts");
     }
-    if (f[3] || f[5]) {
+    if (f[3] || f[5] || f[8]) {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
         active_overflow_ = f[3] ? f[4] : 0;
         mid_overflow_ = f[5] ? f[6] : 0;
-        if (f[5]) mid_dirty_ = true;
+        out_overflow_ = f[8] ? f[9] : 0;
+        if (f[5] || f[8]) mid_dirty_ = true;
+        if (f[8] && !f[3] && !f[5])
+            return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[9]) +
+                                                " neighbours within r_out, more than the outer row holds (" +
+                                                std::to_string(prm.out_cap) + ")");
         if (f[3])
             return fail(MOLDY_ERR_CAPACITY, "an atom has " + std::to_string(f[4]) +
                                                 " interacting neighbours, more than the compact row holds (" +
@@ -622,7 +632,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     const int force_mid = (mode == 1 && !rb && !E.mid_dirty()) ? 0 : 1;
     E.clear_mid_dirty();
     LAUNCH(E, K_MID, 1, s,
-           launch_mid_decide(d, p, E.rmid, E.rcut, force_mid, mode == 1 ? 1 : 0, E.therm_blocks, s));
+           launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, mode == 1 ? 1 : 0, E.therm_blocks, s));
     if (E.therm_blocks > 0 && E.therm_dst)   // the deferred thermo record, before the box algebra below
         CUDA_CHECK(cudaMemcpyAsync(E.therm_dst, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "thermo");
     E.therm_blocks = 0;
@@ -633,7 +643,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
         list_ready = true;
     }
     if (ntc == ntcm) ntc = 0;
-    LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, s));
+    LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, E.rout, s));
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     double *pk = d.partials + 2 * (size_t)kMaxBlocks * kPartials;
@@ -684,13 +694,16 @@ int Engine::force(moldy_force_out *out) {
         bool rb = false;
         active_overflow_ = 0;
         mid_overflow_ = 0;
+        out_overflow_ = 0;
         CHECK(force_device(&rb));
         int rc = fetch_force_out(out);
-        if (rc == MOLDY_ERR_CAPACITY && (active_overflow_ > 0 || mid_overflow_ > 0) && attempt < 3) {
+        if (rc == MOLDY_ERR_CAPACITY && (active_overflow_ > 0 || mid_overflow_ > 0 || out_overflow_ > 0) &&
+            attempt < 3) {
             // a force evaluation changes nothing but the rebuild counter and
             // the lists: grow the overflowing rows and evaluate again
             CHECK(ensure_active_capacity(active_overflow_ > 0 ? active_overflow_ + 8 : 0,
-                                         mid_overflow_ > 0 ? mid_overflow_ + 16 : 0));
+                                         mid_overflow_ > 0 ? mid_overflow_ + 16 : 0,
+                                         out_overflow_ > 0 ? out_overflow_ + 16 : 0));
             ntc_ = ntc0;
             continue;
         }
@@ -701,18 +714,28 @@ int Engine::force(moldy_force_out *out) {
     }
 }
 
-int Engine::ensure_active_capacity(int min_pair, int min_mid) {
+int Engine::ensure_active_capacity(int min_pair, int min_mid, int min_out) {
     // pairs inside a radius: (4 pi / 3) r^3 n/V, with margin for fluctuations
     auto expected = [&](double r) {
         return (4.0 * M_PI / 3.0) * r * r * r * (double)prm.nm / host_vol_;
     };
     int need_pair = std::max(kPairCapMin, min_pair), need_mid = std::max(kMidCapMin, min_mid);
+    int need_out = std::max(kOutCapMin, min_out);
     if (host_vol_ > 0.0 && rcut > 0.0 && rcut < prm.rnear * 2.0) {
         need_pair = std::max(need_pair, (int)std::ceil(1.25 * expected(rcut) + 8.0));
         need_mid = std::max(need_mid, (int)std::ceil(1.25 * expected(rmid) + 16.0));
+        need_out = std::max(need_out, (int)std::ceil(1.25 * expected(rout) + 16.0));
     }
     need_pair = std::min(need_pair, std::max(2 * prm.nnbrs, kPairCapMin));
     need_mid = std::min(need_mid, std::max(2 * prm.nnbrs, kMidCapMin));
+    need_out = std::min(need_out, std::max(2 * prm.nnbrs, kOutCapMin));
+    if (need_out > prm.out_cap) {
+        if (d.olist) cudaFree(d.olist);
+        d.olist = nullptr;
+        CHECK(dev_alloc(&d.olist, (size_t)prm.nm * (size_t)need_out, "outer list"));
+        prm.out_cap = need_out;
+        mid_dirty_ = true;
+    }
     if (need_pair > prm.pair_cap) {
         if (d.alist) cudaFree(d.alist);
         d.alist = nullptr;
@@ -851,8 +874,8 @@ int Engine::autotune(int nreps, double *times_ms) {
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, 1, 0, 0, stream_));
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
         LAUNCH(*this, K_SCREEN, 1, stream_,
@@ -957,9 +980,27 @@ int Engine::knot_gradients(double gE, const double *gF, const double *gS, double
 int Engine::set_mid_skin(double skin) {
     if (!(skin > 0.0) || !(skin <= 3.0)) return fail(MOLDY_ERR_INVALID, "skin must be in (0, 3] A");
     mid_skin = skin;
-    if (rcut > 0.0) rmid = std::min(prm.rnear, rcut + mid_skin);
+    set_list_radii();
     mid_dirty_ = true;
     return MOLDY_OK;
+}
+
+// The outer list is filtered into the intermediate list at each of its
+// rebuilds and is itself rebuilt from the half list only when the
+// displacements since its build could bring an unlisted pair within r_mid:
+// a thicker outer skin makes those rebuilds rarer and its rows longer.
+int Engine::set_out_skin(double skin) {
+    if (!(skin > 0.0) || !(skin <= 3.0)) return fail(MOLDY_ERR_INVALID, "skin must be in (0, 3] A");
+    out_skin = skin;
+    set_list_radii();
+    mid_dirty_ = true;
+    return MOLDY_OK;
+}
+
+void Engine::set_list_radii() {
+    if (!(rcut > 0.0)) return;
+    rmid = std::min(prm.rnear, rcut + mid_skin);
+    rout = std::min(prm.rnear, rcut + std::max(out_skin, mid_skin + 0.4));
 }
 
 int Engine::set_thermostat(double nose, double rqke) {
@@ -1309,6 +1350,22 @@ int moldy_ic_build_tables(int32_t nlookup, double *vee, double *dvee, double *ph
 int moldy_gpu_set_mid_skin(moldy_gpu *h, double skin) {
     GUARD(h);
     TRY(h->e->set_mid_skin(skin));
+}
+
+int moldy_gpu_set_outer_skin(moldy_gpu *h, double skin) {
+    GUARD(h);
+    TRY(h->e->set_out_skin(skin));
+}
+
+int moldy_gpu_get_outer_builds(moldy_gpu *h, int32_t *builds) {
+    GUARD(h);
+    if (!builds) return fail(MOLDY_ERR_INVALID, "null argument");
+    moldy::Engine &E = *h->e;
+    cudaStream_t st = E.stream_ref();
+    cudaError_t e = cudaMemcpyAsync(builds, &E.d.box->out_builds, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return moldy::cuda_fail(e, "get_outer_builds");
+    return MOLDY_OK;
 }
 
 int moldy_gpu_set_thermostat(moldy_gpu *h, double nose, double rqke) {

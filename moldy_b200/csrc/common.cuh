@@ -25,10 +25,14 @@ struct BoxState {
     double bbuild[9];              // B0 when the intermediate list was built
     double snhv, snhf, scalev_ke;  // Nose-Hoover scaling state of scalev and its last KE
     double th_tgid[9], th_cof[9];  // tg^-1 tgdot and cof(B0)/vol of the box k_therm sees
+    double bout[9];                // B0 when the outer list was built
     unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
+    unsigned long long outdisp2;   // max |B0 (x - x_out)|^2 at the last intermediate build (double bits)
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
     int32_t mid_builds;            // number of intermediate-list builds so far
     int32_t status;                // nonzero: singular box in a device-side inversion
+    int32_t out_rebuild;           // 1: the outer list is rebuilt this step
+    int32_t out_builds;            // number of outer-list builds so far
     int32_t pad2;
 };
 
@@ -39,6 +43,7 @@ struct Params {
     int nm, nnbrs, ivol, atomstress;
     int nlcx, nlcy, nlcz, ncell;
     int pair_cap, mid_cap;   // entries per atom of the compact and the intermediate (full) rows
+    int out_cap;             // entries per atom of the outer (full) rows
 };
 
 // Lookup-table description (lookup_m module data, src/lookup_m.F90:64-78).

@@ -253,8 +253,8 @@ k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ 
 // took for the step that has just ended (its block partials), before the box
 // moves.
 __global__ void __launch_bounds__(256)
-k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, int force, int apply_box,
-             const double *__restrict__ therm_partials, int therm_nblk) {
+k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
+             int apply_box, const double *__restrict__ therm_partials, int therm_nblk) {
     if (therm_nblk > 0) {
         __shared__ double s3[3];
         reduce_partials<3>(therm_partials, therm_nblk, s3);
@@ -290,17 +290,38 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, int
     double dmax = ok ? p.rnear * frob(inv) : 1e300;
     double shrink = 2.0 * md + frob(db) * dmax;
     int need = force || !ok || !(shrink < rmid - eps - (rcut + eps));
-    B.mid_rebuild = need;
+    int need_out = 0;
     if (need) {
+        // The intermediate list is filtered from the outer list, which must
+        // then hold every pair within r_mid: a pair left out of it was farther
+        // than r_out - eps at its build, and each atom has moved since then by
+        // at most its displacement at the last intermediate build (outdisp2)
+        // plus its displacement since (md).
+        double bo[9], dbo[9], invo[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { bo[k] = B.bout[k]; dbo[k] = b0[k] - bo[k]; }
+        const bool oko = mat_invert(bo, invo);
+        const double dmaxo = oko ? p.rnear * frob(invo) : 1e300;
+        const double dout = sqrt(__longlong_as_double((long long)B.outdisp2)) + md;
+        const double shrink_out = 2.0 * dout + frob(dbo) * dmaxo;
+        need_out = force || !oko || !(shrink_out < rout - eps - (rmid + 2.0 * eps));
 #pragma unroll
         for (int k = 0; k < 9; ++k) B.bbuild[k] = b0[k];
         B.mid_builds += 1;
+        B.outdisp2 = 0ull;   // measured again by the intermediate build
+        if (need_out) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) B.bout[k] = b0[k];
+            B.out_builds += 1;
+        }
     }
+    B.mid_rebuild = need;
+    B.out_rebuild = need_out;
 }
 
-void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
+void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
                        int apply_box, int therm_nblk, cudaStream_t s) {
-    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, force, apply_box, d.partials, therm_nblk);
+    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk);
 }
 
 // ------------------------------------------------------------- integrator --

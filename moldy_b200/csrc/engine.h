@@ -49,12 +49,17 @@ struct DeviceState {
     // entry e of atom i at alist[e * nm + i] (e < pair_cap), bit 31 set when
     // j is in i's own half-list row; pair_cnt[i] entries
     int32_t *alist = nullptr, *pair_cnt = nullptr;
-    // intermediate FULL list (half-list pairs within r_mid when built, entered
-    // in both rows, bit 31 on the owner's copy), entry-major; xbuild holds the
-    // positions at build time
-    // row of atom i: own entries in slots 0 .. mid_own[i]-1, reverse entries
-    // from the last slot down (mid_rev[i] of them)
-    int32_t *mlist = nullptr, *mid_own = nullptr, *mid_rev = nullptr;
+    // outer FULL list: the half-list pairs within r_out = r_cut + outer skin
+    // when built, entered in both rows (bit 31 on the owner's copy),
+    // entry-major; row of atom i: own entries in slots 0 .. out_own[i]-1,
+    // reverse entries from the last slot down (out_rev[i] of them); xout holds
+    // the positions at build time
+    int32_t *olist = nullptr, *out_own = nullptr, *out_rev = nullptr;
+    double4 *xout = nullptr;
+    // intermediate FULL list: the outer-list pairs within r_mid = r_cut + skin
+    // when built, entry-major, mid_cnt[i] entries from slot 0 (bit 31 kept);
+    // xbuild holds the positions at build time
+    int32_t *mlist = nullptr, *mid_cnt = nullptr;
     double4 *xbuild = nullptr;
     // tables
     double4 *tab_r4 = nullptr;
@@ -65,7 +70,9 @@ struct DeviceState {
     // reductions, flags and box state
     double *partials = nullptr;
     int32_t *flags = nullptr;     // [0] neighbour overflow, [1] relink inconsistency,
-                                  // [2] overflow atom, [3] active-list overflow, [4] its count
+                                  // [2] overflow atom, [3] active-list overflow, [4] its count,
+                                  // [5] intermediate-row overflow, [6] its count,
+                                  // [8] outer-row overflow, [9] its count
     BoxState *box = nullptr;
     int32_t *scan_tmp = nullptr;
     // adjoint (allocated on first use): full tables and their gradients
@@ -84,7 +91,8 @@ struct AdjointArgs {
     double gs[9], gE;
 };
 
-constexpr double kMidSkin = 0.9;       // default r_mid - table cut (A); r_mid is at most rnear
+constexpr double kMidSkin = 0.3;       // default r_mid - table cut (A); r_mid is at most rnear
+constexpr double kOutSkin = 1.0;       // default r_out - table cut (A); r_out is at most rnear
 
 // Host-side table data (potential_m / lookup_m).
 struct HostTables {
@@ -180,12 +188,17 @@ class Engine {
     // kernel variant per tunable family (K_SCREEN, K_DENSITY, K_PAIR)
     int variant[K_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
     int autotune(int nsteps, double *times_ms);
-    // sizes the compact and intermediate rows for the pairs inside rcut and
-    // r_mid at the current atom density (at least min_pair / min_mid entries)
-    int ensure_active_capacity(int min_pair, int min_mid = 0);
+    // sizes the compact, intermediate and outer rows for the pairs inside
+    // rcut, r_mid and r_out at the current atom density (at least min_pair /
+    // min_mid / min_out entries)
+    int ensure_active_capacity(int min_pair, int min_mid = 0, int min_out = 0);
     double rmid = 0.0, rcut = 0.0;   // intermediate-list radius and table cut (A)
+    double rout = 0.0;                // outer-list radius (A)
     double mid_skin = kMidSkin;       // r_mid = min(rnear, rcut + mid_skin)
+    double out_skin = kOutSkin;       // r_out = min(rnear, rcut + max(out_skin, mid_skin + 0.4))
     int set_mid_skin(double skin);
+    int set_out_skin(double skin);
+    void set_list_radii();
 
     DeviceState d;
     Params prm;
@@ -211,6 +224,7 @@ class Engine {
     double thermotimer_ = 0.0;      // time since the last scalev (the mdloop's thermotimer)
     int active_overflow_ = 0;       // largest compact row of an overflowing evaluation
     int mid_overflow_ = 0;          // largest intermediate row of an overflowing build
+    int out_overflow_ = 0;          // largest outer row of an overflowing build
   public:
     int kin_blocks = 0;             // blocks whose kinetic-moment partials the last drift wrote
     int therm_blocks = 0;           // > 0: the last drift took update_therm_avs, for k_mid_decide to finish
@@ -229,7 +243,8 @@ class Engine {
 constexpr int kAtomThreads = 256;
 constexpr int kMaxBlocks = 148 * 8;    // grid-stride kernels: 8 blocks per SM
 constexpr int kPairCapMin = 24;        // least compact-row entries per atom
-constexpr int kMidCapMin = 48;         // least intermediate-row entries per atom
+constexpr int kMidCapMin = 32;         // least intermediate-row entries per atom
+constexpr int kOutCapMin = 48;         // least outer-row entries per atom
 constexpr double kFemtosecond = 0.098227;   // the mdloop's "fs" (src/moldin.F90:132), model time units
 
 inline int grid_blocks(long long work, int threads) {
@@ -259,9 +274,11 @@ void launch_finalize_force(DeviceState &d, const Params &p, const double *part_e
 int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s);
 int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s);
 // therm_nblk > 0: finish the drift kernel's deferred update_therm_avs first
-void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, int force,
+void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
                        int apply_box, int therm_nblk, cudaStream_t s);
-void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s);
+// the outer list from the half list when k_mid_decide asked for it, then the
+// intermediate list from the outer list when it asked for that
+void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 // update_therm_avs with the thermo finalization in its last block; prep
 // when the call does not directly follow a force evaluation

@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256, MINB)
 k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
                  double4 *__restrict__ pos2, int4 *__restrict__ posq2, const BoxState *__restrict__ box,
                  const int32_t *__restrict__ mlist,
-                 const int32_t *__restrict__ mid_own, const int32_t *__restrict__ mid_rev,
+                 const int32_t *__restrict__ mid_cnt,
                  int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
                  double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
                  double *__restrict__ partials, int32_t *__restrict__ flags) {
@@ -180,14 +180,12 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
             const int an = a + astride;
 #pragma unroll
             for (int u = 0; u < 16; ++u) prefetch_l2(&mlist[(size_t)u * stride + an]);
-            prefetch_l2(&mid_own[an]); prefetch_l2(&mid_rev[an]);
+            prefetch_l2(&mid_cnt[an]);
             prefetch_l2(MIXED ? (const void *)&posq[an] : (const void *)&pos[an]);
             prefetch_l2(&dafrho[an]);
         }
-        const int n_own = mid_own[a];
-        const int mc = n_own + mid_rev[a];
+        const int mc = mid_cnt[a];
         const int n = mc < p.mid_cap ? mc : p.mid_cap;
-        const int rev_base = p.mid_cap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
         const double4 pa = MIXED ? make_double4(0.0, 0.0, 0.0, 0.0) : pos[a];
         const int4 qa = MIXED ? posq[a] : make_int4(0, 0, 0, 0);
         double rho_a = 0.0;
@@ -197,7 +195,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 const int k = k0 + u;
-                ee[u] = (k < n) ? __ldg(&mlist[(size_t)(k < n_own ? k : rev_base - k) * stride + a]) : -1;
+                ee[u] = (k < n) ? __ldg(&mlist[(size_t)k * stride + a]) : -1;
             }
             if (MIXED) {
                 int4 qq[B];
@@ -405,8 +403,8 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
     block_partials<7>(v, partials, 0);
 }
 
-// ------------------------------------------------------ intermediate list --
-// The screen walks, per atom, the half-list pairs that were within
+// ------------------------------------------------ outer and intermediate --
+// The screen walks, per atom, a FULL intermediate row: the pairs within
 // r_mid = r_cut + skin when the intermediate list was last built.  A pair
 // left out was farther than r_mid - eps then (eps bounds the FP32 distance
 // error); since then its distance can have shrunk by at most
@@ -417,42 +415,49 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
 // the screen keeps exactly the pairs a walk over the whole half list keeps
 // (k_mid_decide applies the rule).
 //
-// The intermediate list is full: every half-list pair within r_mid (FP32
-// distance plus twice its error bound) is entered in both rows.  The owner
-// writes its own entries from the first slot with a local count (flagged in
-// bit 31); the partner's copy goes from the last slot down through a returned
-// integer atomic on mid_rev, which k_mid_clear zeroes first.  Both run only
-// when k_mid_decide asked for a build.
-__global__ void k_mid_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ mid_rev) {
-    if (!box->mid_rebuild) return;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) mid_rev[a] = 0;
+// The intermediate list is filtered from the outer list (half-list pairs
+// within r_out = r_cut + outer skin, both directions), which k_mid_decide has
+// rebuilt from the half list whenever the displacements since its own build
+// could bring an unlisted pair within r_mid.  The outer build enters every
+// kept half-list pair in both rows: the owner writes its own entries from the
+// first slot (flagged in bit 31); the partner's copy goes from the last slot
+// down through a returned integer atomic on out_rev, which k_out_clear zeroes
+// first.  The intermediate build then writes each atom's row from its own
+// outer row alone, with no atomics.  Each kernel returns at once when
+// k_mid_decide asked for no build.
+__global__ void k_out_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ out_rev) {
+    if (!box->out_rebuild) return;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) out_rev[a] = 0;
+}
+
+// FP32 keep radius^2 of a list of radius r: r plus twice the FP32 distance
+// error bound, or every pair when the box is too small for the FP32 screen
+__device__ float keep_radius2(const double *sb, double r) {
+    const float keep = (float)(r + 2.0 * (2.0e-6 * frob(sb) + 1.0e-4));
+    return screen_radius2(sb, r * r) > 1e37f ? 3.0e38f : keep * keep;
 }
 
 template <bool FIX>
 __global__ void __launch_bounds__(256)
-k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
+k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
-            const int32_t *__restrict__ numn, int32_t *__restrict__ mlist,
-            int32_t *__restrict__ mid_own, int32_t *__restrict__ mid_rev, double4 *__restrict__ xbuild) {
+            const int32_t *__restrict__ numn, int32_t *__restrict__ olist,
+            int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, double4 *__restrict__ xout) {
     constexpr int B = 8;
     __shared__ double sb[9];
     __shared__ float skeep2;
     __shared__ int sneed;
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    if (threadIdx.x == 0) sneed = box->mid_rebuild;
+    if (threadIdx.x == 0) sneed = box->out_rebuild;
     __syncthreads();
     if (!sneed) return;
-    if (threadIdx.x == 0) {
-        float keep = (float)(rmid + 2.0 * (2.0e-6 * frob(sb) + 1.0e-4));
-        // when a box is too small for the FP32 screen, keep every listed pair
-        skeep2 = screen_radius2(sb, rmid * rmid) > 1e37f ? 3.0e38f : keep * keep;
-    }
+    if (threadIdx.x == 0) skeep2 = keep_radius2(sb, rout);
     __syncthreads();
     float bf[9];   // B0, per fixed-point unit when FIX
 #pragma unroll
     for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
     const float keep2 = skeep2;
-    const int nm = p.nm, cap = p.mid_cap;
+    const int nm = p.nm, cap = p.out_cap;
     const size_t stride = (size_t)nm;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const int n = numn[a];
@@ -480,32 +485,126 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
                 const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
                                      : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
                 if (!(r2 <= keep2)) { jj[u] = -1; continue; }
-                if (own < cap) mlist[(size_t)own * stride + a] = jj[u] | kOwnBit;
+                if (own < cap) olist[(size_t)own * stride + a] = jj[u] | kOwnBit;
                 ++own;
-                slot[u] = atomicAdd(&mid_rev[jj[u]], 1);   // issued together, used below
+                slot[u] = atomicAdd(&out_rev[jj[u]], 1);   // issued together, used below
             }
 #pragma unroll
             for (int u = 0; u < B; ++u)
-                if (slot[u] >= 0 && slot[u] < cap) mlist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
+                if (slot[u] >= 0 && slot[u] < cap) olist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
         }
-        mid_own[a] = own;
-        xbuild[a] = pa;
+        out_own[a] = own;
+        xout[a] = pa;
     }
 }
 
+// The intermediate rows from the outer rows; also the largest displacement
+// since the outer build (outdisp2) for the next decision, and the overflow of
+// an outer row (flags 8, 9).  An intermediate row longer than mid_cap keeps
+// its true count in mid_cnt; the screening pass reports it.
+template <bool FIX>
+__global__ void __launch_bounds__(256)
+k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
+            BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_own,
+            const int32_t *__restrict__ out_rev, const double4 *__restrict__ xout, int32_t *__restrict__ mlist,
+            int32_t *__restrict__ mid_cnt, double4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
+    constexpr int B = 8;
+    __shared__ double sb[9];
+    __shared__ float skeep2;
+    __shared__ int sneed;
+    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
+    if (threadIdx.x == 0) sneed = box->mid_rebuild;
+    __syncthreads();
+    if (!sneed) return;
+    if (threadIdx.x == 0) skeep2 = keep_radius2(sb, rmid);
+    __syncthreads();
+    float bf[9];   // B0, per fixed-point unit when FIX
+#pragma unroll
+    for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
+    const float keep2 = skeep2;
+    const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
+    const size_t stride = (size_t)nm;
+    double d2 = 0.0;
+    int over = 0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        const int n_own = out_own[a];
+        const int nt = n_own + out_rev[a];
+        if (nt > ocap) over = max(over, nt);
+        const int n = nt < ocap ? nt : ocap;
+        const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
+        const double4 pa = pos[a];
+        const int4 qa = FIX ? posq[a] : make_int4(0, 0, 0, 0);
+        int cnt = 0;
+        for (int k0 = 0; k0 < n; k0 += B) {
+            int ee[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int k = k0 + u;
+                ee[u] = k < n ? __ldg(&olist[(size_t)(k < n_own ? k : rev_base - k) * stride + a]) : -1;
+            }
+            double4 qq[FIX ? 1 : B];
+            int4 qi[FIX ? B : 1];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int j = ee[u] != -1 ? (ee[u] & kIdMask) : a;
+                if (FIX) qi[u] = __ldg(&posq[j]);
+                else qq[u] = ldg4(&pos[j]);
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                if (ee[u] == -1) continue;
+                float rx, ry, rz;
+                const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
+                                     : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
+                if (!(r2 <= keep2)) continue;
+                if (cnt < mcap) mlist[(size_t)cnt * stride + a] = ee[u];
+                ++cnt;
+            }
+        }
+        mid_cnt[a] = cnt;
+        xbuild[a] = pa;
+        const double4 xo = xout[a];
+        const double ux = pa.x - xo.x, uy = pa.y - xo.y, uz = pa.z - xo.z;
+        const double rx = sb[0] * ux + sb[3] * uy + sb[6] * uz;
+        const double ry = sb[1] * ux + sb[4] * uy + sb[7] * uz;
+        const double rz = sb[2] * ux + sb[5] * uy + sb[8] * uz;
+        d2 = fmax(d2, rx * rx + ry * ry + rz * rz);
+    }
+    // block maximum, then one atomic per block (non-negative doubles order as their bits)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    __shared__ double wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+        atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong(m));
+    }
+    if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
+}
+
 // fixed-point separations in a fully periodic box, FP64 differences otherwise;
-// both launches exit at once when no build was decided, so their grids are one
+// the launches exit at once when no build was decided, so their grids are one
 // resident wave
-void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t s) {
+void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s) {
+    const bool fix = p.ivol == 0 || p.ivol == 1 || p.ivol == 4;
     int nc = grid_blocks(p.nm, 256);
-    LAUNCH_WAVE(k_mid_clear, nc, s, d.box, p.nm, d.mid_rev);
-    int nb = grid_blocks(p.nm, 256);
-    if (p.ivol == 0 || p.ivol == 1 || p.ivol == 4)
-        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.mlist, d.mid_own,
-                    d.mid_rev, d.xbuild);
+    LAUNCH_WAVE(k_out_clear, nc, s, d.box, p.nm, d.out_rev);
+    int no = grid_blocks(p.nm, 256);
+    if (fix)
+        LAUNCH_WAVE(k_out_build<true>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
+                    d.out_rev, d.xout);
     else
-        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.mlist, d.mid_own,
-                    d.mid_rev, d.xbuild);
+        LAUNCH_WAVE(k_out_build<false>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
+                    d.out_rev, d.xout);
+    int nb = grid_blocks(p.nm, 256);
+    if (fix)
+        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_rev, d.xout,
+                    d.mlist, d.mid_cnt, d.xbuild, d.flags);
+    else
+        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_rev, d.xout,
+                    d.mlist, d.mid_cnt, d.xbuild, d.flags);
 }
 
 // ------------------------------------------------------------ launchers --
@@ -517,7 +616,7 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, cudaStream_t
 template <int B, bool PF, int MINB>
 static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials,
                       cudaStream_t s) {
-#define SD_ARGS p, t, d.pos, d.posq, d.pos2, d.posq2, d.box, d.mlist, d.mid_own, d.mid_rev, d.alist, d.pair_cnt, \
+#define SD_ARGS p, t, d.pos, d.posq, d.pos2, d.posq2, d.box, d.mlist, d.mid_cnt, d.alist, d.pair_cnt, \
                 d.rho, d.afrho, d.dafrho, partials, d.flags
     int nb = grid_blocks(p.nm, 256);
     if (t.exact) LAUNCH_WAVE((k_screen_density<false, true, B, PF, MINB>), nb, s, SD_ARGS);
@@ -576,11 +675,11 @@ int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, 
 }
 
 // list entries the screening pass reads per step (the full intermediate rows)
-__global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_own, const int32_t *__restrict__ mid_rev,
+__global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_cnt,
                                  unsigned long long *__restrict__ out) {
     unsigned long long s = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        s += (unsigned long long)(mid_own[a] + mid_rev[a]);
+        s += (unsigned long long)mid_cnt[a];
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
@@ -588,7 +687,7 @@ __global__ void k_count_screened(int nm, const int32_t *__restrict__ mid_own, co
 
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s) {
     cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
-    k_count_screened<<<grid_blocks(p.nm, kAtomThreads), kAtomThreads, 0, s>>>(p.nm, d.mid_own, d.mid_rev, out);
+    k_count_screened<<<grid_blocks(p.nm, kAtomThreads), kAtomThreads, 0, s>>>(p.nm, d.mid_cnt, out);
 }
 
 }  // namespace moldy

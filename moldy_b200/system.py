@@ -382,6 +382,16 @@ class MoldySystem:
         """Skin (A) of the intermediate list; a tuning knob, results unchanged."""
         check(self._L.moldy_gpu_set_mid_skin(self._h, float(skin)))
 
+    def set_outer_skin(self, skin: float):
+        """Skin (A) of the outer list the intermediate list is filtered from;
+        a tuning knob, results unchanged."""
+        check(self._L.moldy_gpu_set_outer_skin(self._h, float(skin)))
+
+    def outer_builds(self) -> int:
+        n = ctypes.c_int32(0)
+        check(self._L.moldy_gpu_get_outer_builds(self._h, ctypes.byref(n)))
+        return int(n.value)
+
     def set_variants(self, screen: int, density: int, forces: int):
         check(self._L.moldy_gpu_set_variants(self._h, int(screen), int(density), int(forces)))
 
