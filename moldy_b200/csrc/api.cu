@@ -260,7 +260,8 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.out_own, 0, nm * sizeof(int32_t)), "memset out_own");
     CUDA_CHECK(cudaMemset(d.out_rev, 0, nm * sizeof(int32_t)), "memset out_rev");
     CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
-    CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(double4)), "memset xbuild");
+    CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(int4)), "memset xbuild");
+    CUDA_CHECK(cudaMemset(d.xout, 0, nm * sizeof(int4)), "memset xout");
     CUDA_CHECK(cudaMemset(d.flags, 0, 12 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));

@@ -26,6 +26,7 @@ struct BoxState {
     double snhv, snhf, scalev_ke;  // Nose-Hoover scaling state of scalev and its last KE
     double th_tgid[9], th_cof[9];  // tg^-1 tgdot and cof(B0)/vol of the box k_therm sees
     double bout[9];                // B0 when the outer list was built
+    double dmax_mid, dmax_out;     // rnear |B_build^-1|_F of those builds (0: none)
     unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
     unsigned long long outdisp2;   // max |B0 (x - x_out)|^2 at the last intermediate build (double bits)
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step
@@ -143,6 +144,20 @@ __device__ __forceinline__ float fix_to_float(int32_t d) {
     const float fhi = __int_as_float(0x4b400000 + hi) - 12582912.0f;      // bias 1.5 * 2^23
     const float flo = __int_as_float(0x4b000000 + lo) - 8388608.0f;       // bias 2^23
     return fmaf(fhi, 4096.0f, flo);
+}
+
+// |B0 (x - x_ref)|^2 from fixed-point coordinates (any box: displacements
+// since a list build are far below half a box, so the 32-bit difference is
+// the displacement itself); bs is B0 per fixed-point unit.  Off from the FP64
+// value by less than 1e-6 A^2 for any displacement a list build allows.
+__device__ __forceinline__ float fix_disp2(const float *bs, const int4 &q, const int4 &ref) {
+    const float dx = fix_to_float((int32_t)((uint32_t)q.x - (uint32_t)ref.x));
+    const float dy = fix_to_float((int32_t)((uint32_t)q.y - (uint32_t)ref.y));
+    const float dz = fix_to_float((int32_t)((uint32_t)q.z - (uint32_t)ref.z));
+    const float rx = fmaf(bs[6], dz, fmaf(bs[3], dy, bs[0] * dx));
+    const float ry = fmaf(bs[7], dz, fmaf(bs[4], dy, bs[1] * dx));
+    const float rz = fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx));
+    return fmaf(rz, rz, fmaf(ry, ry, rx * rx));
 }
 
 // floor(x) of 0 <= x < 2^23 as an integer and as a float, from one round-down

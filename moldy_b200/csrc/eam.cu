@@ -7,6 +7,17 @@ namespace moldy {
 
 __device__ void therm_prep(const Params &p, const double *b0, const double *b1, BoxState &B);
 
+int stream_blocks(int nm) {
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
+    const int nb = grid_blocks(nm, kAtomThreads);
+    return nb < 4 * sms ? nb : 4 * sms;
+}
+
 // mode 0: force only; 1: velocity Verlet second half (box); 2: md_init
 __global__ void __launch_bounds__(256)
 k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
@@ -133,7 +144,7 @@ k_kinetic(Params p, const double *__restrict__ x1, const double *__restrict__ ma
 }
 
 int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s) {
-    int nb = grid_blocks(p.nm, kAtomThreads);
+    int nb = stream_blocks(p.nm);
     k_kinetic<<<nb, kAtomThreads, 0, s>>>(p, d.x1, d.mass, d.znum, partials);
     return nb;
 }
@@ -280,16 +291,19 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
 #pragma unroll
         for (int k = 0; k < 9; ++k) { B.b0[k] = b0[k]; B.b1[k] = b1[k]; }
     }
-    double md = sqrt(__longlong_as_double((long long)B.maxdisp2));
+    // displacements are measured in FP32 from fixed-point positions: the
+    // factor and the offset cover their rounding
+    double md = sqrt(__longlong_as_double((long long)B.maxdisp2)) * (1.0 + 1.0e-5) + 1.0e-6;
     B.maxdisp2 = 0ull;
     double eps = 2.0e-6 * frob(b0) + 1.0e-4;
-    double db[9], inv[9];
+    // dmax = rnear |B_build^-1|_F bounds the fractional separation of a listed
+    // pair; it is stored with each build (0: none yet, or a singular box)
+    double db[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) db[k] = b0[k] - bb[k];
-    bool ok = mat_invert(bb, inv);
-    double dmax = ok ? p.rnear * frob(inv) : 1e300;
+    const double dmax = B.dmax_mid;
     double shrink = 2.0 * md + frob(db) * dmax;
-    int need = force || !ok || !(shrink < rmid - eps - (rcut + eps));
+    int need = force || !(dmax > 0.0) || !(shrink < rmid - eps - (rcut + eps));
     int need_out = 0;
     if (need) {
         // The intermediate list is filtered from the outer list, which must
@@ -297,21 +311,24 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
         // than r_out - eps at its build, and each atom has moved since then by
         // at most its displacement at the last intermediate build (outdisp2)
         // plus its displacement since (md).
-        double bo[9], dbo[9], invo[9];
+        double dbo[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { bo[k] = B.bout[k]; dbo[k] = b0[k] - bo[k]; }
-        const bool oko = mat_invert(bo, invo);
-        const double dmaxo = oko ? p.rnear * frob(invo) : 1e300;
-        const double dout = sqrt(__longlong_as_double((long long)B.outdisp2)) + md;
+        for (int k = 0; k < 9; ++k) dbo[k] = b0[k] - B.bout[k];
+        const double dmaxo = B.dmax_out;
+        const double dout = sqrt(__longlong_as_double((long long)B.outdisp2)) * (1.0 + 1.0e-5) + 1.0e-6 + md;
         const double shrink_out = 2.0 * dout + frob(dbo) * dmaxo;
-        need_out = force || !oko || !(shrink_out < rout - eps - (rmid + 2.0 * eps));
+        need_out = force || !(dmaxo > 0.0) || !(shrink_out < rout - eps - (rmid + 2.0 * eps));
+        double inv[9];
+        const double dnew = mat_invert(b0, inv) ? p.rnear * frob(inv) : 0.0;
 #pragma unroll
         for (int k = 0; k < 9; ++k) B.bbuild[k] = b0[k];
+        B.dmax_mid = dnew;
         B.mid_builds += 1;
         B.outdisp2 = 0ull;   // measured again by the intermediate build
         if (need_out) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) B.bout[k] = b0[k];
+            B.dmax_out = dnew;
             B.out_builds += 1;
         }
     }
@@ -338,10 +355,10 @@ template <bool THERM>
 __global__ void __launch_bounds__(256)
 k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
-        const double4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
+        const int4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
         double *__restrict__ kin_partials, double *__restrict__ therm_partials) {
     // every thread forms the post-drift box exactly as thread 0 stores it
-    __shared__ double nb[9];
+    __shared__ float nbs[9];   // that box per fixed-point unit
     __shared__ double sh[THERM ? 27 : 1];   // tgid, b0, cof(b0)/vol of the previous step
     if (THERM && threadIdx.x < 9) {
         sh[threadIdx.x] = box->th_tgid[threadIdx.x];
@@ -360,10 +377,10 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
             for (int k = 0; k < 9; ++k) b1[k] = b1[k] + B.b2[k];
             for (int k = 0; k < 9; ++k) b0[k] = b0[k] + b1[k];
         }
-        for (int k = 0; k < 9; ++k) nb[k] = b0[k];
+        for (int k = 0; k < 9; ++k) nbs[k] = (float)(b0[k] * kFixUnit);
     }
     __syncthreads();
-    double d2 = 0.0;
+    float d2 = 0.f;
     double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     double vt[3] = {0.0, 0.0, 0.0};
     const int nm = p.nm;
@@ -375,14 +392,9 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
         q.y = q.y + (ey + wy);
         q.z = q.z + (ez + wz);
         pos[a] = q;
-        posq[a] = make_int4(fix32(q.x), fix32(q.y), fix32(q.z), 0);
-        double4 xb = xbuild[a];
-        double ux = q.x - xb.x, uy = q.y - xb.y, uz = q.z - xb.z;
-        const volatile double *bv = nb;   // read per use, not held in registers
-        double rx = bv[0] * ux + bv[3] * uy + bv[6] * uz;
-        double ry = bv[1] * ux + bv[4] * uy + bv[7] * uz;
-        double rz = bv[2] * ux + bv[5] * uy + bv[8] * uz;
-        d2 = fmax(d2, rx * rx + ry * ry + rz * rz);
+        const int4 qn = make_int4(fix32(q.x), fix32(q.y), fix32(q.z), 0);
+        posq[a] = qn;
+        d2 = fmaxf(d2, fix_disp2(nbs, qn, xbuild[a]));
         // x1 is not changed by this half of the step: the kinetic moment of
         // the coming force evaluation can be taken here
         if (znum[a] != 0) {
@@ -394,14 +406,14 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
     block_partials<6>(v, kin_partials, 0);
     // block maximum, then one atomic per block (non-negative doubles order as their bits)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-    __shared__ double wmax[8];
+    for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    __shared__ float wmax[8];
     if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
-        atomicMax(&box->maxdisp2, (unsigned long long)__double_as_longlong(m));
+        float m = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+        atomicMax(&box->maxdisp2, (unsigned long long)__double_as_longlong((double)m));
     }
     // the sums are finished by k_mid_decide, which runs next
     if (THERM) block_partials<3>(vt, therm_partials, 0);
@@ -410,7 +422,7 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
 }
 
 int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s) {
-    int nb = grid_blocks(p.nm, kAtomThreads);
+    int nb = stream_blocks(p.nm);
     if (therm)
         k_drift<true><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
                                                   kin_partials, d.partials);
@@ -476,7 +488,7 @@ k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
 // evaluation that left them)
 int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s) {
     if (prep) k_therm_prep<<<1, 1, 0, s>>>(p, d.box);
-    int nblocks = grid_blocks(p.nm, kAtomThreads);
+    int nblocks = stream_blocks(p.nm);
     k_therm<<<nblocks, kAtomThreads, 0, s>>>(p, d.box, d.x1, d.x2, d.mass, d.znum, d.partials);
     k_therm_finish<<<1, kAtomThreads, 0, s>>>(p, d.box, d.partials, nblocks);
     return nblocks;

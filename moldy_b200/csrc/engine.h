@@ -55,12 +55,12 @@ struct DeviceState {
     // reverse entries from the last slot down (out_rev[i] of them); xout holds
     // the positions at build time
     int32_t *olist = nullptr, *out_own = nullptr, *out_rev = nullptr;
-    double4 *xout = nullptr;
+    int4 *xout = nullptr;                  // fixed-point (posq) snapshot
     // intermediate FULL list: the outer-list pairs within r_mid = r_cut + skin
     // when built, entry-major, mid_cnt[i] entries from slot 0 (bit 31 kept);
     // xbuild holds the positions at build time
     int32_t *mlist = nullptr, *mid_cnt = nullptr;
-    double4 *xbuild = nullptr;
+    int4 *xbuild = nullptr;                // fixed-point (posq) snapshot
     // tables
     double4 *tab_r4 = nullptr;
     double2 *tab_e2 = nullptr;
@@ -246,6 +246,12 @@ constexpr int kPairCapMin = 24;        // least compact-row entries per atom
 constexpr int kMidCapMin = 32;         // least intermediate-row entries per atom
 constexpr int kOutCapMin = 48;         // least outer-row entries per atom
 constexpr double kFemtosecond = 0.098227;   // the mdloop's "fs" (src/moldin.F90:132), model time units
+
+// Grid of the streaming per-atom kernels that leave block partials (drift,
+// kinetic moment, thermo sums): 4 blocks of 256 per SM, one resident wave, so
+// the one-block reductions that follow read few partials.  The same for all
+// of them, so the fused and the separate thermo sums agree to the bit.
+int stream_blocks(int nm);
 
 inline int grid_blocks(long long work, int threads) {
     long long nb = (work + threads - 1) / threads;

@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(256)
 k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
             const int32_t *__restrict__ numn, int32_t *__restrict__ olist,
-            int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, double4 *__restrict__ xout) {
+            int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, int4 *__restrict__ xout) {
     constexpr int B = 8;
     __shared__ double sb[9];
     __shared__ float skeep2;
@@ -463,7 +463,7 @@ k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *
         const int n = numn[a];
         const int32_t *col = nlist + a;
         const double4 pa = pos[a];
-        const int4 qa = FIX ? posq[a] : make_int4(0, 0, 0, 0);
+        const int4 qa = posq[a];
         int own = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
             int jj[B];
@@ -494,7 +494,7 @@ k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *
                 if (slot[u] >= 0 && slot[u] < cap) olist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
         }
         out_own[a] = own;
-        xout[a] = pa;
+        xout[a] = qa;
     }
 }
 
@@ -506,8 +506,8 @@ template <bool FIX>
 __global__ void __launch_bounds__(256)
 k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_own,
-            const int32_t *__restrict__ out_rev, const double4 *__restrict__ xout, int32_t *__restrict__ mlist,
-            int32_t *__restrict__ mid_cnt, double4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
+            const int32_t *__restrict__ out_rev, const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
+            int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
     constexpr int B = 8;
     __shared__ double sb[9];
     __shared__ float skeep2;
@@ -524,7 +524,10 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
     const float keep2 = skeep2;
     const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
     const size_t stride = (size_t)nm;
-    double d2 = 0.0;
+    float bq[9];   // B0 per fixed-point unit, for the displacement
+#pragma unroll
+    for (int k = 0; k < 9; ++k) bq[k] = (float)(sb[k] * kFixUnit);
+    float d2 = 0.f;
     int over = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const int n_own = out_own[a];
@@ -533,7 +536,7 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
         const int n = nt < ocap ? nt : ocap;
         const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
         const double4 pa = pos[a];
-        const int4 qa = FIX ? posq[a] : make_int4(0, 0, 0, 0);
+        const int4 qa = posq[a];
         int cnt = 0;
         for (int k0 = 0; k0 < n; k0 += B) {
             int ee[B];
@@ -562,24 +565,19 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
             }
         }
         mid_cnt[a] = cnt;
-        xbuild[a] = pa;
-        const double4 xo = xout[a];
-        const double ux = pa.x - xo.x, uy = pa.y - xo.y, uz = pa.z - xo.z;
-        const double rx = sb[0] * ux + sb[3] * uy + sb[6] * uz;
-        const double ry = sb[1] * ux + sb[4] * uy + sb[7] * uz;
-        const double rz = sb[2] * ux + sb[5] * uy + sb[8] * uz;
-        d2 = fmax(d2, rx * rx + ry * ry + rz * rz);
+        xbuild[a] = qa;
+        d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
     }
     // block maximum, then one atomic per block (non-negative doubles order as their bits)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-    __shared__ double wmax[8];
+    for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    __shared__ float wmax[8];
     if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
-        atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong(m));
+        float m = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+        atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong((double)m));
     }
     if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
 }
