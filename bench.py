@@ -174,19 +174,22 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def kernel_bytes_per_atom(name, n_half, n_full, n_screen):
+def kernel_bytes_per_atom(name, n_half, n_full, n_screen, mixed=True):
     """Algorithmic DRAM bytes per atom of one launch.
     n_half: mean half-list length; n_full: mean interacting (directed) pairs;
-    n_screen: mean intermediate-row entries the screening pass reads."""
+    n_screen: mean intermediate-row entries the screening pass reads; mixed:
+    the fixed-point position records (16 bytes) instead of the FP64 ones (32)."""
+    own = 16 if mixed else 32
     table = {
-        # intermediate row + count, compact-row writes + count, own position, pos2 write,
-        # rho/F/F' writes and old F', x1, mass, Z
-        "screen_density": 4.0 * n_screen + 4 + 4.0 * n_full + 4 + 32 + 32 + 24 + 8 + 24 + 8 + 4,
-        # compact row + count + own (x,F') + mass, forces, x1 and x2 read+write, del2, Z
-        "forces": 4.0 * n_full + 4 + 32 + 8 + 24 + 48 + 48 + 8 + 4,
-        "drift": 32 + 48 + 32 + 16,
+        # intermediate row + count, own position, old F'; compact-row writes + count,
+        # rho/F/F' writes, position record with F'
+        "screen_density": 4.0 * n_screen + 4 + own + 8 + 4.0 * n_full + 4 + 24 + own,
+        # compact row + count, own position record, mass; forces; x1 and x2 read + write, del2, Z
+        "forces": 4.0 * n_full + 4 + own + 8 + 24 + 48 + 48 + 8 + 4,
+        # pos read + write, x1, x2, build snapshot (fixed point), mass, Z, fixed-point positions
+        "drift": 64 + 48 + 16 + 8 + 4 + 16,
         "therm": 48 + 8 + 4,
-        "build_nlist": 4.0 * n_half + 32 + 16,
+        "build_nlist": 4.0 * n_half + 4 + 32 + 16,
     }
     return table.get(name)
 
@@ -339,7 +342,7 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     mid_builds_per_step = (lst_timed["mid_builds"] - builds0) / args.steps
     dname, (dms, dlaunch) = max(stats.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = load_peaks()
-    bpa = kernel_bytes_per_atom(dname, n_half, n_full, n_screen)
+    bpa = kernel_bytes_per_atom(dname, n_half, n_full, n_screen, mixed=(precision == "mixed"))
     roofline = None
     if bpa is not None and dlaunch > 0:
         achieved = bpa * w.nm / (dms / 1000.0 / dlaunch) / 1e9

@@ -170,7 +170,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
-                    d.pair_cnt, d.olist, d.out_own, d.out_rev, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.olist, d.out_own, d.out_rev, d.out_nrev, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -237,6 +237,7 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.olist, nm * (size_t)p.out_cap, "outer list"));
     CHECK(dev_alloc(&d.out_own, nm, "out_own"));
     CHECK(dev_alloc(&d.out_rev, nm, "out_rev"));
+    CHECK(dev_alloc(&d.out_nrev, nm, "out_nrev"));
     CHECK(dev_alloc(&d.xout, nm, "xout"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
@@ -259,6 +260,7 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
     CUDA_CHECK(cudaMemset(d.out_own, 0, nm * sizeof(int32_t)), "memset out_own");
     CUDA_CHECK(cudaMemset(d.out_rev, 0, nm * sizeof(int32_t)), "memset out_rev");
+    CUDA_CHECK(cudaMemset(d.out_nrev, 0, nm * sizeof(int32_t)), "memset out_nrev");
     CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(int4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.xout, 0, nm * sizeof(int4)), "memset xout");

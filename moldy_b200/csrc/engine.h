@@ -54,7 +54,9 @@ struct DeviceState {
     // entry-major; row of atom i: own entries in slots 0 .. out_own[i]-1,
     // reverse entries from the last slot down (out_rev[i] of them); xout holds
     // the positions at build time
-    int32_t *olist = nullptr, *out_own = nullptr, *out_rev = nullptr;
+    // (out_rev counts the reverse entries during a build and is zero
+    // otherwise; out_nrev keeps the count after it)
+    int32_t *olist = nullptr, *out_own = nullptr, *out_rev = nullptr, *out_nrev = nullptr;
     int4 *xout = nullptr;                  // fixed-point (posq) snapshot
     // intermediate FULL list: the outer-list pairs within r_mid = r_cut + skin
     // when built, entry-major, mid_cnt[i] entries from slot 0 (bit 31 kept);

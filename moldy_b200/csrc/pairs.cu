@@ -27,6 +27,8 @@
 // (own rows only) needs.  MIXED = true runs distances, tables and pair forces
 // in FP32 (differences of FP64 positions rounded to FP32) and keeps every
 // accumulation, rho, F and F' in FP64.
+#include <climits>
+
 #include "engine.h"
 
 namespace moldy {
@@ -421,14 +423,10 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
 // could bring an unlisted pair within r_mid.  The outer build enters every
 // kept half-list pair in both rows: the owner writes its own entries from the
 // first slot (flagged in bit 31); the partner's copy goes from the last slot
-// down through a returned integer atomic on out_rev, which k_out_clear zeroes
-// first.  The intermediate build then writes each atom's row from its own
-// outer row alone, with no atomics.  Each kernel returns at once when
-// k_mid_decide asked for no build.
-__global__ void k_out_clear(const BoxState *__restrict__ box, int nm, int32_t *__restrict__ out_rev) {
-    if (!box->out_rebuild) return;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) out_rev[a] = 0;
-}
+// down through a returned integer atomic on out_rev (zero before each build);
+// k_out_finish then sorts each reverse segment.  The intermediate build writes
+// each atom's row from its own outer row alone, with no atomics.  Each kernel
+// returns at once when k_mid_decide asked for no build.
 
 // FP32 keep radius^2 of a list of radius r: r plus twice the FP32 distance
 // error bound, or every pair when the box is too small for the FP32 screen
@@ -498,6 +496,78 @@ k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *
     }
 }
 
+// Ascending sort of a register array by a bitonic network (all indices known
+// at compile time, so the array stays in registers)
+constexpr int kSortNet = 32;
+template <int N>
+__device__ __forceinline__ void sort_net(int (&v)[N]) {
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int lo = min(v[i], v[l]), hi = max(v[i], v[l]);
+                    if ((i & k) == 0) { v[i] = lo; v[l] = hi; }
+                    else { v[i] = hi; v[l] = lo; }
+                }
+            }
+}
+
+// After an outer build: each atom's reverse entries, placed in the order the
+// atomics were served, are sorted by atom index (its own entries are in
+// half-list order), so the lists below and the sums over their rows are the
+// same run after run; the reverse count moves to out_nrev and out_rev is
+// zeroed for the next build.
+__global__ void __launch_bounds__(256)
+k_out_finish(const BoxState *__restrict__ box, int nm, int ocap, int32_t *__restrict__ olist,
+             const int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, int32_t *__restrict__ out_nrev) {
+    if (!box->out_rebuild) return;
+    const size_t stride = (size_t)nm;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
+        const int n_own = out_own[a], n_rev = out_rev[a];
+        out_rev[a] = 0;
+        out_nrev[a] = n_rev;
+        const int nt = n_own + n_rev;
+        const int n = nt < ocap ? nt : ocap;
+        const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
+        const int nr = n - n_own;
+        if (nr <= 1) continue;
+        if (nr <= 16) {
+            int rv[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                rv[k] = k < nr ? olist[(size_t)(rev_base - n_own - k) * stride + a] : INT_MAX;
+            sort_net(rv);
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (k < nr) olist[(size_t)(rev_base - n_own - k) * stride + a] = rv[k];
+        } else if (nr <= kSortNet) {
+            int rv[kSortNet];
+#pragma unroll
+            for (int k = 0; k < kSortNet; ++k)
+                rv[k] = k < nr ? olist[(size_t)(rev_base - n_own - k) * stride + a] : INT_MAX;
+            sort_net(rv);
+#pragma unroll
+            for (int k = 0; k < kSortNet; ++k)
+                if (k < nr) olist[(size_t)(rev_base - n_own - k) * stride + a] = rv[k];
+        } else {
+            for (int k = n_own + 1; k < n; ++k) {   // insertion sort in place
+                const int e = olist[(size_t)(rev_base - k) * stride + a];
+                int m = k - 1;
+                for (; m >= n_own; --m) {
+                    const int f = olist[(size_t)(rev_base - m) * stride + a];
+                    if (f <= e) break;
+                    olist[(size_t)(rev_base - m - 1) * stride + a] = f;
+                }
+                olist[(size_t)(rev_base - m - 1) * stride + a] = e;
+            }
+        }
+    }
+}
+
 // The intermediate rows from the outer rows; also the largest displacement
 // since the outer build (outdisp2) for the next decision, and the overflow of
 // an outer row (flags 8, 9).  An intermediate row longer than mid_cap keeps
@@ -506,7 +576,7 @@ template <bool FIX>
 __global__ void __launch_bounds__(256)
 k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_own,
-            const int32_t *__restrict__ out_rev, const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
+            const int32_t *__restrict__ out_nrev, const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
             int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
     constexpr int B = 8;
     __shared__ double sb[9];
@@ -531,7 +601,7 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
     int over = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const int n_own = out_own[a];
-        const int nt = n_own + out_rev[a];
+        const int nt = n_own + out_nrev[a];
         if (nt > ocap) over = max(over, nt);
         const int n = nt < ocap ? nt : ocap;
         const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
@@ -587,8 +657,6 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
 // resident wave
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s) {
     const bool fix = p.ivol == 0 || p.ivol == 1 || p.ivol == 4;
-    int nc = grid_blocks(p.nm, 256);
-    LAUNCH_WAVE(k_out_clear, nc, s, d.box, p.nm, d.out_rev);
     int no = grid_blocks(p.nm, 256);
     if (fix)
         LAUNCH_WAVE(k_out_build<true>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
@@ -596,12 +664,14 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout,
     else
         LAUNCH_WAVE(k_out_build<false>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
                     d.out_rev, d.xout);
+    int nf = grid_blocks(p.nm, 256);
+    LAUNCH_WAVE(k_out_finish, nf, s, d.box, p.nm, p.out_cap, d.olist, d.out_own, d.out_rev, d.out_nrev);
     int nb = grid_blocks(p.nm, 256);
     if (fix)
-        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_rev, d.xout,
+        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_nrev, d.xout,
                     d.mlist, d.mid_cnt, d.xbuild, d.flags);
     else
-        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_rev, d.xout,
+        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_nrev, d.xout,
                     d.mlist, d.mid_cnt, d.xbuild, d.flags);
 }
 

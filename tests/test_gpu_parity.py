@@ -351,3 +351,95 @@ def test_mid_skin_changes_no_result(gpu_lib):
     for k in (0, 40, 79):
         for key in ("pe", "ke", "th"):
             assert abs(a[k][key] - b[k][key]) <= 1e-10 * abs(a[k][key]), (k, key)
+
+
+def test_outer_skin_changes_no_result(gpu_lib):
+    """The outer-list skin is a tuning knob too: a thin outer skin (outer
+    rebuilds decided on the device from the displacement since its build)
+    and a thick one give the same trajectory."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(10, sigma=0.05, temperature=1500.0, ivol=0, seed=8, nbrupdate=200)
+    runs = []
+    for out in (2.0, 0.45):
+        s = MoldySystem.from_workload(w)
+        s.set_mid_skin(0.05)
+        s.set_outer_skin(out)
+        s.linkup()
+        s.md_init()
+        th = s.md_steps(80)
+        runs.append((th, s.outer_builds(), s.list_stats()["mid_builds"]))
+        s.close()
+    (a, oa, ma), (b, ob, mb) = runs
+    assert ob > oa >= 1 and ma > 3 and mb > 3
+    for k in (0, 40, 79):
+        for key in ("pe", "ke", "th"):
+            assert abs(a[k][key] - b[k][key]) <= 1e-10 * abs(a[k][key]), (k, key)
+
+
+def test_md_hot_outer_list_rebuilds(oracle_mod, gpu_lib):
+    """3000 K with thin skins and no half-list rebuild in 60 steps: the outer
+    list is rebuilt from its displacement bound several times, and the
+    trajectory follows the oracle, which walks the whole half list."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(8, sigma=0.1, temperature=3000.0, ivol=1, seed=13, nbrupdate=200)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=1)
+    g = MoldySystem.from_workload(w)
+    g.set_mid_skin(0.05)
+    g.set_outer_skin(0.45)
+    o.md_init()
+    g.md_init()
+    th_o = [o.md_step() for _ in range(60)]
+    th_g = g.md_steps(60)
+    assert g.outer_builds() >= 3
+    a = np.array([t["pe"] for t in th_o])
+    b = np.array([t["pe"] for t in th_g])
+    assert np.max(np.abs(a - b)) < 1e-8 * np.max(np.abs(a))
+    so, sg = o.get_state(), g.get_state()
+    assert np.max(np.abs((sg["x0"] - so["x0"]) @ w.b0.T)) < 1e-7
+
+
+@pytest.mark.parametrize("ivol", [2, 5])
+def test_partly_periodic_box_mixed_runs_fp64(oracle_mod, gpu_lib, ivol):
+    """A box periodic in only some directions (ivol 2: x and y; ivol 5: z):
+    the fixed-point minimum image of the mixed passes does not apply, so the
+    mixed engine evaluates in FP64 and matches the FP64 engine bit for bit,
+    and both match the oracle."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(8, sigma=0.05, temperature=600.0, ivol=ivol, seed=21)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=4)
+    o.force()
+    fo = o.force_out()
+    res = []
+    for prec in ("mixed", "fp64"):
+        g = MoldySystem.from_workload(w, precision=prec)
+        out = g.force()
+        res.append((g.forces(), out))
+        g.close()
+    (fm, om), (fd, od) = res
+    assert np.array_equal(fm, fd) and om["pe"] == od["pe"]
+    assert rel_norm_err(fd, o.forces()) <= 1e-10
+    assert abs(od["pe"] - fo["pe"]) <= 1e-10 * abs(fo["pe"])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_md_bit_reproducible(gpu_lib, prec):
+    """Two runs of the same MD (thin skins: several outer and intermediate
+    rebuilds, whose reverse entries are placed by integer atomics and then
+    sorted) end in the same state bit for bit."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(8, sigma=0.1, temperature=2000.0, ivol=0, seed=17, nbrupdate=200)
+    states = []
+    for _ in range(2):
+        s = MoldySystem.from_workload(w, precision=prec)
+        s.set_mid_skin(0.05)
+        s.set_outer_skin(0.45)
+        s.linkup()
+        s.md_init()
+        s.md_steps(40)
+        assert s.outer_builds() >= 2
+        states.append((s.get_state(), s.forces()))
+        s.close()
+    (a, fa), (b, fb) = states
+    for k in ("x0", "x1", "x2", "b0", "b1"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(fa, fb)
