@@ -323,6 +323,34 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
     value = world * w.nm * args.steps / (ms_max / 1000.0)
     lst_timed = sysm.list_stats()
     out_builds_per_step = (sysm.outer_builds() - obuilds0) / args.steps
+    # end to end through the C ABI, right after the timed steps: host state in,
+    # the same K steps with their per-step thermo records, host state out.  An
+    # untimed pass of the same call first sizes the pinned thermo staging.
+    e2e = None
+    if with_e2e:
+        sysm.md_steps(args.steps, thermo=True)
+        sysm.synchronize()
+        st = sysm.get_state()
+        pin = [torch.empty(w.nm, dtype=torch.float64, pin_memory=True).numpy() for _ in range(12)]
+        for k, name in enumerate(("x0", "x1", "x2")):
+            for c in range(3):
+                pin[3 * k + c][:] = st[name][:, c]
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sysm.set_state_soa(*pin[:9], b0=st["b0"], b1=st["b1"], b2=st["b2"])
+        sysm.md_steps(args.steps, thermo=True)
+        sysm.get_state_soa(pin[:9], forces=pin[9:12])
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        h2d = 9 * 8 * w.nm + 3 * 72
+        d2h = 12 * 8 * w.nm + args.steps * 104 + 4 * 72
+        e2e = {"value": world * w.nm * args.steps / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "ms": ems}
+
     # then a profiled stretch: per-kernel CUDA-event times on the library's stream
     prof_steps = min(args.steps, 300)
     sysm.reset_kernel_stats()
@@ -355,28 +383,6 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
                     "traffic": traffic, "algorithmic_bytes_per_launch": bpa * w.nm,
                     "avg_launch_ms": dms / dlaunch, "share_of_step": dms / prof_ms,
                     "profiled_steps": prof_steps}
-    e2e = None
-    if with_e2e:
-        st = sysm.get_state()
-        pin = [torch.empty(w.nm, dtype=torch.float64, pin_memory=True).numpy() for _ in range(12)]
-        for k, name in enumerate(("x0", "x1", "x2")):
-            for c in range(3):
-                pin[3 * k + c][:] = st[name][:, c]
-        barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        sysm.set_state_soa(*pin[:9], b0=st["b0"], b1=st["b1"], b2=st["b2"])
-        sysm.md_steps(args.steps, thermo=True)
-        sysm.get_state_soa(pin[:9], forces=pin[9:12])
-        e1.record(stream)
-        e1.synchronize()
-        barrier()
-        ems = max_over_ranks(e0.elapsed_time(e1))
-        h2d = 9 * 8 * w.nm + 3 * 72
-        d2h = 12 * 8 * w.nm + args.steps * 104 + 4 * 72
-        e2e = {"value": world * w.nm * args.steps / (ems / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "ms": ems}
     sysm.close()
     return {"value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "stats": stats,
             "roofline": roofline, "e2e": e2e, "clocks": clk.summary(), "tune": tune,
@@ -486,6 +492,14 @@ def run_ours(args):
                         f"{min(args.steps, 300)} steps after the timed ones",
         "autotune_ms_per_launch": r["tune"]["ms"],
     }
+    # the whole step against the fixed per-atom-step figure of the reference's
+    # algorithm (x, v, a and F' read and written, two passes over the int32
+    # half list: 160 + 8 n_half bytes), the same for both precisions
+    peak, peak_kind = load_peaks()
+    step_bytes = 160.0 + 8.0 * r["n_half"]
+    line["step_roofline"] = {"bound": "hbm", "bytes_per_atom_step": step_bytes,
+                             "achieved": step_bytes * r["value"] / 1e9, "peak": peak, "peak_kind": peak_kind,
+                             "unit": "GB/s", "frac": step_bytes * r["value"] / 1e9 / peak}
     if "fp64" in runs and head != "fp64":
         f = runs["fp64"]
         line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],

@@ -175,6 +175,8 @@ Engine::~Engine() {
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_box_) cudaFreeHost(host_box_);
+    if (host_rec_) cudaFreeHost(host_rec_);
+    if (d.thermo_rec) cudaFree(d.thermo_rec);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -635,11 +637,10 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     const int force_mid = (mode == 1 && !rb && !E.mid_dirty()) ? 0 : 1;
     E.clear_mid_dirty();
     LAUNCH(E, K_MID, 1, s,
-           launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, mode == 1 ? 1 : 0, E.therm_blocks, s));
-    if (E.therm_blocks > 0 && E.therm_dst)   // the deferred thermo record, before the box algebra below
-        CUDA_CHECK(cudaMemcpyAsync(E.therm_dst, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost, s), "thermo");
+           launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, mode == 1 ? 1 : 0, E.therm_blocks,
+                             E.therm_rec, s));
     E.therm_blocks = 0;
-    E.therm_dst = nullptr;
+    E.therm_rec = nullptr;
     if (rb) {
         if (!cells_ready) { LAUNCH(E, K_LINKUP, 4, s, launch_linkup(d, p, s)); cells_ready = true; }
         LAUNCH(E, K_NLIST, 1, s, launch_build_nlist(d, p, s));
@@ -769,7 +770,7 @@ int Engine::velocityverlet(moldy_force_out *out) {
 
 int Engine::update_therm_avs(double *s123) {
     CHECK(check_ready());
-    LAUNCH(*this, K_THERM, 2, stream_, launch_therm(d, prm, true, stream_));
+    LAUNCH(*this, K_THERM, 2, stream_, launch_therm(d, prm, true, nullptr, stream_));
     if (!host_box_) {
         CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * 4), "pinned staging");
         host_box_cap_ = 4;
@@ -794,11 +795,20 @@ int Engine::md_init(moldy_force_out *out) {
 int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
     CHECK(check_ready());
     if (nsteps < 0) return fail(MOLDY_ERR_INVALID, "nsteps < 0");
-    if (thermo && host_box_cap_ < nsteps) {
-        if (host_box_) cudaFreeHost(host_box_);
-        host_box_ = nullptr;
-        CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * nsteps), "pinned staging");
-        host_box_cap_ = nsteps;
+    // per-step thermo records are written on the device and copied back once
+    if (thermo && d.thermo_cap < nsteps) {
+        if (d.thermo_rec) cudaFree(d.thermo_rec);
+        d.thermo_rec = nullptr;
+        d.thermo_cap = 0;
+        CHECK(dev_alloc(&d.thermo_rec, (size_t)kThermoRec * nsteps, "thermo records"));
+        d.thermo_cap = nsteps;
+    }
+    if (thermo && host_rec_cap_ < nsteps) {
+        if (host_rec_) cudaFreeHost(host_rec_);
+        host_rec_ = nullptr;
+        host_rec_cap_ = 0;
+        CUDA_CHECK(cudaMallocHost((void **)&host_rec_, sizeof(double) * kThermoRec * nsteps), "pinned staging");
+        host_rec_cap_ = nsteps;
     }
     std::vector<int> ntcs(nsteps), rbs(nsteps);
     // update_therm_avs of step k reads x1 and x2 as step k's force evaluation
@@ -813,7 +823,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
                                          stream_));
         if (therm_pending) {
             therm_blocks = kin_blocks;
-            therm_dst = thermo ? host_box_ + k - 1 : nullptr;
+            therm_rec = thermo ? d.thermo_rec + (size_t)kThermoRec * (k - 1) : nullptr;
         }
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
         ntcs[k] = ntc_;
@@ -827,23 +837,23 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
             scalev = nose_ > 0.0;
         }
         therm_pending = !(scalev || k == nsteps - 1);
-        if (!therm_pending) {
-            LAUNCH(*this, K_THERM, 1, stream_, launch_therm(d, prm, false, stream_));
-            if (thermo)
-                CUDA_CHECK(cudaMemcpyAsync(host_box_ + k, d.box, sizeof(BoxState), cudaMemcpyDeviceToHost,
-                                           stream_), "thermo");
-        }
+        if (!therm_pending)
+            LAUNCH(*this, K_THERM, 1, stream_,
+                   launch_therm(d, prm, false, thermo ? d.thermo_rec + (size_t)kThermoRec * k : nullptr, stream_));
         if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
         if (scalev) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
     }
     CUDA_CHECK(cudaGetLastError(), "md_steps launch");
+    if (thermo && nsteps > 0)
+        CUDA_CHECK(cudaMemcpyAsync(host_rec_, d.thermo_rec, sizeof(double) * kThermoRec * nsteps,
+                                   cudaMemcpyDeviceToHost, stream_), "thermo");
     CHECK(check_flags());
     if (thermo) {
         for (int k = 0; k < nsteps; ++k) {
-            const BoxState &B = host_box_[k];
+            const double *r = host_rec_ + (size_t)kThermoRec * k;
             moldy_thermo &t = thermo[k];
-            t.ke = B.ke; t.pe = B.pe; t.te = B.te; t.h = B.h; t.th = B.th; t.vol = B.vol;
-            t.s1 = B.s1; t.s2 = B.s2; t.s3 = B.s3; t.temp = B.temp; t.boxke = B.boxke;
+            t.ke = r[0]; t.pe = r[1]; t.te = r[2]; t.h = r[3]; t.th = r[4]; t.vol = r[5];
+            t.s1 = r[6]; t.s2 = r[7]; t.s3 = r[8]; t.temp = r[9]; t.boxke = r[10];
             t.ntc = ntcs[k]; t.rebuilt = rbs[k];
         }
     }
@@ -877,7 +887,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, nullptr, stream_));
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {

@@ -229,7 +229,9 @@ __device__ __forceinline__ void therm_terms(double (&v)[3], const volatile doubl
 // The mdloop quantities (src/moldin.F90:760-790) from the three sums of
 // update_therm_avs (s3 = s1, s2, s3), by one thread.  The box has not moved
 // since the force evaluation that ended the step.
-__device__ void therm_store(const Params &p, BoxState &B, const double *s3) {
+// rec (may be null): the step's thermo record, kThermoRec doubles in the order
+// of moldy_thermo (ke, pe, te, h, th, vol, s1, s2, s3, temp, boxke)
+__device__ void therm_store(const Params &p, BoxState &B, const double *s3, double *rec) {
     double b0[9], b1[9], tg[9], tgdot[9], tginv[9], tgid[9], vol;
 #pragma unroll
     for (int k = 0; k < 9; ++k) { b0[k] = B.b0[k]; b1[k] = B.b1[k]; }
@@ -248,15 +250,20 @@ __device__ void therm_store(const Params &p, BoxState &B, const double *s3) {
     B.te = B.ke + B.pe;
     B.h = B.te + p.press * B.vol;
     B.th = B.h + boxke;
+    if (rec) {
+        rec[0] = B.ke; rec[1] = B.pe; rec[2] = B.te; rec[3] = B.h; rec[4] = B.th; rec[5] = B.vol;
+        rec[6] = B.s1; rec[7] = B.s2; rec[8] = B.s3; rec[9] = B.temp; rec[10] = B.boxke;
+    }
 }
 
 // Every block's three partial sums of update_therm_avs, in block order, and
 // the quantities derived from them (one block)
 __global__ void __launch_bounds__(256)
-k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ partials, int nblk) {
+k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ partials, int nblk,
+               double *__restrict__ rec) {
     __shared__ double s3[3];
     reduce_partials<3>(partials, nblk, s3);
-    if (threadIdx.x == 0) therm_store(p, *box, s3);
+    if (threadIdx.x == 0) therm_store(p, *box, s3, rec);
 }
 
 // ------------------------------------------------ intermediate-list check --
@@ -265,11 +272,11 @@ k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ 
 // moves.
 __global__ void __launch_bounds__(256)
 k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
-             int apply_box, const double *__restrict__ therm_partials, int therm_nblk) {
+             int apply_box, const double *__restrict__ therm_partials, int therm_nblk, double *__restrict__ rec) {
     if (therm_nblk > 0) {
         __shared__ double s3[3];
         reduce_partials<3>(therm_partials, therm_nblk, s3);
-        if (threadIdx.x == 0) therm_store(p, *box, s3);
+        if (threadIdx.x == 0) therm_store(p, *box, s3, rec);
     }
     if (threadIdx.x != 0) return;
     BoxState &B = *box;
@@ -337,8 +344,8 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
 }
 
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, cudaStream_t s) {
-    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk);
+                       int apply_box, int therm_nblk, double *rec, cudaStream_t s) {
+    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk, rec);
 }
 
 // ------------------------------------------------------------- integrator --
@@ -486,11 +493,11 @@ k_therm(Params p, BoxState *__restrict__ box, const double *__restrict__ x1,
 
 // prep: compute the box quantities first (the call does not follow a force
 // evaluation that left them)
-int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s) {
+int launch_therm(DeviceState &d, const Params &p, bool prep, double *rec, cudaStream_t s) {
     if (prep) k_therm_prep<<<1, 1, 0, s>>>(p, d.box);
     int nblocks = stream_blocks(p.nm);
     k_therm<<<nblocks, kAtomThreads, 0, s>>>(p, d.box, d.x1, d.x2, d.mass, d.znum, d.partials);
-    k_therm_finish<<<1, kAtomThreads, 0, s>>>(p, d.box, d.partials, nblocks);
+    k_therm_finish<<<1, kAtomThreads, 0, s>>>(p, d.box, d.partials, nblocks, rec);
     return nblocks;
 }
 

@@ -69,6 +69,9 @@ struct DeviceState {
     float4 *tab_r4f = nullptr;
     float2 *tab_e2f = nullptr;
     void *tab_aux = nullptr;               // phi2 / phi2f node-pair tables
+    // per-step thermo records of an md_steps call (kThermoRec doubles each), grown on demand
+    double *thermo_rec = nullptr;
+    int thermo_cap = 0;
     // reductions, flags and box state
     double *partials = nullptr;
     int32_t *flags = nullptr;     // [0] neighbour overflow, [1] relink inconsistency,
@@ -230,7 +233,7 @@ class Engine {
   public:
     int kin_blocks = 0;             // blocks whose kinetic-moment partials the last drift wrote
     int therm_blocks = 0;           // > 0: the last drift took update_therm_avs, for k_mid_decide to finish
-    BoxState *therm_dst = nullptr;  // pinned slot for that step's thermo record (or none)
+    double *therm_rec = nullptr;    // device slot for that step's thermo record (or none)
   private:
     bool mid_dirty_ = true;         // the intermediate list must be rebuilt before use
   public:
@@ -240,6 +243,8 @@ class Engine {
     double *part_embed_ = nullptr, *part_force_ = nullptr;   // slices of d.partials
     BoxState *host_box_ = nullptr;                            // pinned staging
     int host_box_cap_ = 0;
+    double *host_rec_ = nullptr;                              // pinned thermo records
+    int host_rec_cap_ = 0;
 };
 
 constexpr int kAtomThreads = 256;
@@ -283,14 +288,16 @@ int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool the
 int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s);
 // therm_nblk > 0: finish the drift kernel's deferred update_therm_avs first
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, cudaStream_t s);
+                       int apply_box, int therm_nblk, double *rec, cudaStream_t s);
 // the outer list from the half list when k_mid_decide asked for it, then the
 // intermediate list from the outer list when it asked for that
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s);
 void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 // update_therm_avs with the thermo finalization in its last block; prep
 // when the call does not directly follow a force evaluation
-int launch_therm(DeviceState &d, const Params &p, bool prep, cudaStream_t s);
+// rec: where the step's thermo record goes (kThermoRec doubles, device; may be null)
+int launch_therm(DeviceState &d, const Params &p, bool prep, double *rec, cudaStream_t s);
+constexpr int kThermoRec = 11;
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
 void launch_scalev(DeviceState &d, const Params &p, double nose, double rqke, cudaStream_t s);
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s);

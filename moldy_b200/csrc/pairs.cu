@@ -521,7 +521,7 @@ __device__ __forceinline__ void sort_net(int (&v)[N]) {
 // half-list order), so the lists below and the sums over their rows are the
 // same run after run; the reverse count moves to out_nrev and out_rev is
 // zeroed for the next build.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_out_finish(const BoxState *__restrict__ box, int nm, int ocap, int32_t *__restrict__ olist,
              const int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, int32_t *__restrict__ out_nrev) {
     if (!box->out_rebuild) return;
