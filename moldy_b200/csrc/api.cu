@@ -654,7 +654,9 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     int nbe = 0, nbf = 0;
     // kinten's moment: taken by the drift kernel in velocity Verlet
     if (mode != 1) LAUNCH(E, K_DRIFT, 1, s, E.kin_blocks = launch_kinetic(d, p, pk, s));
-    LAUNCH(E, K_SCREEN, 1, s, nbe = launch_screen_density(d, p, E.tab, mixed, E.variant[K_SCREEN], pe, s));
+    LAUNCH(E, K_SCREEN, 1, s,
+           nbe = launch_screen_density(d, p, E.tab, mixed, E.variant[K_SCREEN], pe, s, !E.skip_rho));
+    E.skip_rho = false;
     LAUNCH(E, K_PAIR, 1, s,
            nbf = launch_forces(d, p, E.tab, mixed, mode == 1 ? 1 : 0, E.variant[K_PAIR], pf, s));
     LAUNCH(E, K_FINALIZE, 1, s, launch_finalize_force(d, p, pe, nbe, pf, nbf, pk, E.kin_blocks, mode, s));
@@ -825,6 +827,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
             therm_blocks = kin_blocks;
             therm_rec = thermo ? d.thermo_rec + (size_t)kThermoRec * (k - 1) : nullptr;
         }
+        skip_rho = k < nsteps - 1;   // rho is read only after the last step
         CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
         ntcs[k] = ntc_;
         rbs[k] = rb ? 1 : 0;

@@ -232,6 +232,7 @@ class Engine {
     int out_overflow_ = 0;          // largest outer row of an overflowing build
   public:
     int kin_blocks = 0;             // blocks whose kinetic-moment partials the last drift wrote
+    bool skip_rho = false;          // the next evaluation need not store rho (an inner md_steps step)
     int therm_blocks = 0;           // > 0: the last drift took update_therm_avs, for k_mid_decide to finish
     double *therm_rec = nullptr;    // device slot for that step's thermo record (or none)
   private:
@@ -275,8 +276,10 @@ void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0,
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
 constexpr int kVariants = 8;           // compiled variants per tunable pass
+// store_rho false: rho is not written (no caller reads it before the next
+// evaluation overwrites it: the inner steps of an md_steps call)
 int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                          double *partials, cudaStream_t s);
+                          double *partials, cudaStream_t s, bool store_rho = true);
 int launch_forces(DeviceState &d, const Params &p, const Tables &t, bool mixed, int mode,
                   int variant, double *partials, cudaStream_t s);
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,

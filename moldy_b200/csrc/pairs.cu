@@ -155,7 +155,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
                  const int32_t *__restrict__ mid_cnt,
                  int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
                  double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
-                 double *__restrict__ partials, int32_t *__restrict__ flags) {
+                 double *__restrict__ partials, int32_t *__restrict__ flags, int store_rho) {
     __shared__ double sb[9];
     __shared__ float srs2, srin2;
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
@@ -241,15 +241,17 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
         if (cnt > p.pair_cap) { over = 1; over_max = max(over_max, cnt); }
         if (mc > p.mid_cap) { over |= 2; over_max = max(over_max, mc); }
         // embed (src/potential_m.F90:148-169): rho <= 1e-40 keeps the old values
-        double fd = dafrho[a];
+        double fd;
         if (rho_a > 1e-40) {
             double2 e = EXACT ? embed_funcs(t, rho_a) : lookup_e2(t, rho_a);
             afrho[a] = e.x;
             dafrho[a] = e.y;
             fd = e.y;
             v[0] += e.x;
+        } else {
+            fd = dafrho[a];
         }
-        rho[a] = rho_a;
+        if (store_rho) rho[a] = rho_a;
         if (MIXED) posq2[a] = make_int4(qa.x, qa.y, qa.z, __float_as_int((float)fd));
         else pos2[a] = make_double4(pa.x, pa.y, pa.z, fd);
     }
@@ -683,9 +685,9 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout,
 // to hide the gather latency).
 template <int B, bool PF, int MINB>
 static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mixed, double *partials,
-                      cudaStream_t s) {
+                      int store_rho, cudaStream_t s) {
 #define SD_ARGS p, t, d.pos, d.posq, d.pos2, d.posq2, d.box, d.mlist, d.mid_cnt, d.alist, d.pair_cnt, \
-                d.rho, d.afrho, d.dafrho, partials, d.flags
+                d.rho, d.afrho, d.dafrho, partials, d.flags, store_rho
     int nb = grid_blocks(p.nm, 256);
     if (t.exact) LAUNCH_WAVE((k_screen_density<false, true, B, PF, MINB>), nb, s, SD_ARGS);
     else if (mixed) LAUNCH_WAVE((k_screen_density<true, false, B, PF, MINB>), nb, s, SD_ARGS);
@@ -699,17 +701,17 @@ static int sd_variant(DeviceState &d, const Params &p, const Tables &t, bool mix
 static inline bool mixed_applies(const Params &p) { return p.ivol == 0 || p.ivol == 1 || p.ivol == 4; }
 
 int launch_screen_density(DeviceState &d, const Params &p, const Tables &t, bool mixed, int variant,
-                          double *partials, cudaStream_t s) {
+                          double *partials, cudaStream_t s, bool store_rho) {
     mixed = mixed && mixed_applies(p);
     switch (variant) {
-    case 0: return sd_variant<4, true, 4>(d, p, t, mixed, partials, s);
-    case 1: return sd_variant<8, true, 4>(d, p, t, mixed, partials, s);
-    case 2: return sd_variant<4, true, 2>(d, p, t, mixed, partials, s);
-    case 3: return sd_variant<8, true, 2>(d, p, t, mixed, partials, s);
-    case 4: return sd_variant<4, false, 3>(d, p, t, mixed, partials, s);
-    case 5: return sd_variant<8, false, 3>(d, p, t, mixed, partials, s);
-    case 6: return sd_variant<4, true, 3>(d, p, t, mixed, partials, s);
-    default: return sd_variant<8, true, 3>(d, p, t, mixed, partials, s);
+    case 0: return sd_variant<4, true, 4>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 1: return sd_variant<8, true, 4>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 2: return sd_variant<4, true, 2>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 3: return sd_variant<8, true, 2>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 4: return sd_variant<4, false, 3>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 5: return sd_variant<8, false, 3>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    case 6: return sd_variant<4, true, 3>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
+    default: return sd_variant<8, true, 3>(d, p, t, mixed, partials, store_rho ? 1 : 0, s);
     }
 }
 
