@@ -181,9 +181,9 @@ def kernel_bytes_per_atom(name, n_half, n_full, n_screen, mixed=True):
     the fixed-point position records (16 bytes) instead of the FP64 ones (32)."""
     own = 16 if mixed else 32
     table = {
-        # intermediate row + count, own position, old F'; compact-row writes + count,
-        # rho/F/F' writes, position record with F'
-        "screen_density": 4.0 * n_screen + 4 + own + 8 + 4.0 * n_full + 4 + 24 + own,
+        # intermediate row + count, own position; compact-row writes + count, F and F'
+        # writes, position record with F' (rho is stored on the last step of a call only)
+        "screen_density": 4.0 * n_screen + 4 + own + 4.0 * n_full + 4 + 16 + own,
         # compact row + count, own position record, mass; forces; x1 and x2 read + write, del2, Z
         "forces": 4.0 * n_full + 4 + own + 8 + 24 + 48 + 48 + 8 + 4,
         # pos read + write, x1, x2, build snapshot (fixed point), mass, Z, fixed-point positions
