@@ -647,7 +647,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
         list_ready = true;
     }
     if (ntc == ntcm) ntc = 0;
-    LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, E.rout, s));
+    LAUNCH(E, K_MID, 3, s, launch_mid_build(d, p, E.rmid, E.rout, s));   // outer build, finish, filter
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     double *pk = d.partials + 2 * (size_t)kMaxBlocks * kPartials;
@@ -772,7 +772,7 @@ int Engine::velocityverlet(moldy_force_out *out) {
 
 int Engine::update_therm_avs(double *s123) {
     CHECK(check_ready());
-    LAUNCH(*this, K_THERM, 2, stream_, launch_therm(d, prm, true, nullptr, stream_));
+    LAUNCH(*this, K_THERM, 3, stream_, launch_therm(d, prm, true, nullptr, stream_));   // prep, sums, finish
     if (!host_box_) {
         CUDA_CHECK(cudaMallocHost((void **)&host_box_, sizeof(BoxState) * 4), "pinned staging");
         host_box_cap_ = 4;
@@ -841,7 +841,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         }
         therm_pending = !(scalev || k == nsteps - 1);
         if (!therm_pending)
-            LAUNCH(*this, K_THERM, 1, stream_,
+            LAUNCH(*this, K_THERM, 2, stream_,
                    launch_therm(d, prm, false, thermo ? d.thermo_rec + (size_t)kThermoRec * k : nullptr, stream_));
         if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
         if (scalev) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
@@ -891,7 +891,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, nullptr, stream_));
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
+    LAUNCH(*this, K_MID, 3, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
         LAUNCH(*this, K_SCREEN, 1, stream_,
