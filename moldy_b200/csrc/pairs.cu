@@ -5,9 +5,13 @@
 // the last nonzero table node contribute (about 7 of the ~44 listed per atom
 // in bcc Fe at rnear = 6.3 A); the others add exact zeros.  The lists:
 //
-//  intermediate  a FULL list (both directions) of the half-list pairs within
-//                r_mid = rcut + skin, rebuilt only when the displacements since
-//                its build could bring an unlisted pair inside the cut;
+//  outer         a FULL list (both directions) of the half-list pairs within
+//                r_out = rcut + outer skin, rebuilt from the half list only when
+//                the displacements since its build could bring an unlisted
+//                pair within r_mid;
+//  intermediate  the outer-list pairs within r_mid = rcut + skin, rebuilt
+//                (filtered from the outer rows) only when the displacements
+//                since its build could bring an unlisted pair inside the cut;
 //  compact       per step, the FULL list of pairs inside the table cut.
 //
 // Each step runs two passes, one thread per atom, no floating-point atomics:
@@ -16,8 +20,9 @@
 //             the cut (exact FP64 distance in FP64 mode; FP32 with an error
 //             margin and an FP64 decision inside the margin in mixed mode),
 //             writes them to its compact row and sums rho_i = sum_j phi(r_ij);
-//             then embed and F'(rho) into pos2.w.  (The kinetic moment of
-//             kinten is taken by the drift kernel, or k_kinetic outside MD.)
+//             then embed and F'(rho) into pos2.w / posq2.w.  (The kinetic
+//             moment of kinten is taken by the drift kernel, or k_kinetic
+//             outside MD.)
 //  k_forces   f_i = sum_j dx_ij fp_ij over the compact row; energy and virial
 //             take half of every directed pair; the velocity-Verlet second
 //             half (src/quench_m.F90:606-622) is applied in the epilogue.
@@ -25,8 +30,9 @@
 // Entries carry the pair's direction in the reference's half list in bit 31
 // (set: j is in i's own row), which the per-atom stress of the reference
 // (own rows only) needs.  MIXED = true runs distances, tables and pair forces
-// in FP32 (differences of FP64 positions rounded to FP32) and keeps every
-// accumulation, rho, F and F' in FP64.
+// in FP32 from 32-bit fixed-point positions (whose integer differences are
+// the minimum image) and keeps rho, F, F', the forces and every sum over atoms
+// in FP64.
 #include <climits>
 
 #include "engine.h"
