@@ -366,6 +366,8 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
     t.rcull2 = rc * rc;
     t.rcull2f = (float)(rc * rc * (1.0 + 1.0e-6));
     t.recipstep_f = (float)t.vp_recipstep;
+    t.xoff_f = (float)(-h.rmin * t.vp_recipstep);
+    t.tail_f = r4f[2 * (size_t)(nr - 1)];
     t.nv = h.nv; t.np = h.np;
     for (int i = 0; i < 8; ++i) { t.av[i] = h.av[i]; t.rv[i] = h.rv[i]; t.ap[i] = h.ap[i]; t.rp[i] = h.rp[i]; }
     t.bier_cut1 = h.bier_cut1; t.bier_cut2 = h.bier_cut2;

@@ -64,6 +64,9 @@ struct Tables {
     double rcull2;          // pairs with r^2 above this contribute exactly zero
     float rcull2f;
     float recipstep_f;      // (float) vp_recipstep: node coordinate of r in the FP32 lookups
+    float xoff_f;           // (float) (-vp_rmin * vp_recipstep): node coordinate = r * recipstep_f + xoff_f
+    float4 tail_f;          // FP32 (vee, dvee, phi, dphi) of the last stored node nr - 1: the
+                            // value for r >= rmax (node nlookup) or beyond the culled tail (zero)
     // FETRANSMETAL Fe-Fe analytic data for exact mode / energy_calc
     int nv, np;
     double av[8], rv[8], ap[8], rp[8];
@@ -214,14 +217,18 @@ __device__ __forceinline__ double2 lookup_e2(const Tables &t, double rho) {
     return make_double2(a.x * w + b.x * dr, a.y * w + b.y * dr);
 }
 
-// FP32 variants for the mixed path (index arithmetic in FP32 as well)
-// FP32 lookups for the mixed path (r >= 0): the interval and its fraction
-// come from one multiply and a floor on the FMA pipe
+// FP32 lookups for the mixed path, in FP32 index arithmetic.  As
+// get_value_from_lookup_veephi (src/lookup_m.F90:322-340): the node
+// coordinate x = (r - rmin) n / range comes from one fused multiply-add and
+// its interval from a floor on the FMA pipe; at and beyond the last stored
+// node (r >= rmax: node nlookup; a culled table: its first all-zero node) the
+// value is that node's.  Below rmin the first interval is extrapolated, as
+// the FP64 lookups do (the reference reads out of bounds there).
 __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
-    const float x = r * t.recipstep_f;
+    const float x = fmaf(r, t.recipstep_f, t.xoff_f);
     float fl;
-    const int idx = floor_small(x, fl);
-    if (idx >= t.nr - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const int idx = floor_small(fmaxf(x, 0.f), fl);
+    if (idx >= t.nr - 1) return t.tail_f;
     const float dr = x - fl;
     float4 a, b;
     ldg8f(&t.r4f[2 * idx], a, b);
@@ -230,10 +237,10 @@ __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
 }
 
 __device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
-    const float x = r * t.recipstep_f;
+    const float x = fmaf(r, t.recipstep_f, t.xoff_f);
     float fl;
-    const int idx = floor_small(x, fl);
-    if (idx >= t.nr - 1) return 0.f;
+    const int idx = floor_small(fmaxf(x, 0.f), fl);
+    if (idx >= t.nr - 1) return t.tail_f.z;
     const float dr = x - fl;
     const float2 v = __ldg(&t.phi2f[idx]);
     return fmaf(v.y - v.x, dr, v.x);

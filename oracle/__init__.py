@@ -60,6 +60,7 @@ def _load():
         "orc_set_fetm": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, ctypes.c_int, _D, _D]),
         "orc_set_lookup": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "orc_set_iron_carbon": (ctypes.c_int, [vp]),
+        "orc_set_tables": (ctypes.c_int, [vp, ctypes.c_int] + [ctypes.c_double] * 4 + [_D] * 6),
         "orc_get_tables": (None, [vp] + [_D] * 6),
         "orc_get_fetm_derived": (None, [vp, _D]),
         "orc_src": (ctypes.c_double, [vp, ctypes.c_int, ctypes.c_double]),
@@ -166,6 +167,17 @@ class Oracle:
         if st:
             raise RuntimeError(f"orc_set_lookup status {st}")
         self.nlookup = int(nlookup)
+
+    def set_tables(self, tables, rmin=0.0, rmax=6.0, rhomin=0.0, rhomax=10000.0):
+        """A caller's own lookup_m tables (dict of vee, dvee, phi, dphi, emb,
+        demb with nlookup + 1 nodes each) over [rmin, rmax] and [rhomin, rhomax]."""
+        t = [_f64(tables[k]) for k in ("vee", "dvee", "phi", "dphi", "emb", "demb")]
+        n = len(t[0]) - 1
+        st = self._lib.orc_set_tables(self._h, n, float(rmin), float(rmax), float(rhomin), float(rhomax),
+                                      *[_dp(a) for a in t])
+        if st:
+            raise RuntimeError(f"orc_set_tables status {st}")
+        self.nlookup = n
 
     def tables(self):
         n = self.nlookup + 1

@@ -285,6 +285,38 @@ int orc_set_lookup(orc_sys *s, int uselookup, int nlookup)
     return 0;
 }
 
+/* Tables handed over by a caller in the lookup_m layout (src/lookup_m.F90:64-78):
+ * nlookup intervals over [rmin, rmax] for vee, dvee, phi, dphi and over
+ * [rhomin, rhomax] for emb, demb; the reciprocal ranges are formed as
+ * calculate_lookup_table_* does (src/lookup_m.F90:161-251). */
+int orc_set_tables(orc_sys *s, int nlookup, double rmin, double rmax, double rhomin, double rhomax,
+                   const double *vee, const double *dvee, const double *phi, const double *dphi,
+                   const double *emb, const double *demb)
+{
+    if (nlookup < 2) return 2;
+    if (!(rmax > rmin) || !(rhomax > rhomin)) return 3;
+    orc_free_tables(s);
+    size_t n = (size_t)nlookup + 1;
+    const double *src[6] = {vee, dvee, phi, dphi, emb, demb};
+    for (int k = 0; k < 6; ++k) {
+        s->tab[k] = (double *)malloc(n * sizeof(double));
+        memcpy(s->tab[k], src[k], n * sizeof(double));
+    }
+    s->uselookup = 1;
+    s->nlookup = nlookup;
+    s->vp_rmin = rmin; s->vp_rmax = rmax;
+    s->vp_range = rmax - rmin;
+    s->vp_reciprange = 1.0 / s->vp_range;
+    s->vp_recipnlkp = 1.0 / (double)nlookup;
+    s->vp_recipstep = (double)nlookup / s->vp_range;
+    s->e_rmin = rhomin; s->e_rmax = rhomax;
+    s->e_range = rhomax - rhomin;
+    s->e_reciprange = 1.0 / s->e_range;
+    s->e_recipnlkp = 1.0 / (double)nlookup;
+    s->e_recipstep = (double)nlookup / s->e_range;
+    return 0;
+}
+
 void orc_free_tables(orc_sys *s)
 {
     for (int k = 0; k < 6; ++k) { free(s->tab[k]); s->tab[k] = NULL; }

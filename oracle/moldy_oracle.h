@@ -42,6 +42,11 @@ int orc_set_fetm(orc_sys *s, int nv, const double *av, const double *rv,
 /* uselookup=1: build the six lookup_m tables with nlookup intervals
  * (r in [0,6], rho in [0,10000]); uselookup=0: exact *_src evaluation. */
 int orc_set_lookup(orc_sys *s, int uselookup, int nlookup);
+/* a caller's own lookup_m tables (nlookup + 1 nodes each, r in [rmin, rmax],
+ * rho in [rhomin, rhomax]); switches to lookup mode.  Returns 0 on success. */
+int orc_set_tables(orc_sys *s, int nlookup, double rmin, double rmax, double rhomin, double rhomax,
+                   const double *vee, const double *dvee, const double *phi, const double *dphi,
+                   const double *emb, const double *demb);
 /* the Fe-Fe functions of the IRON_CARBON module (src/iron_carbon.F90) in place of FETRANSMETAL */
 int orc_set_iron_carbon(orc_sys *s);
 void orc_get_tables(const orc_sys *s, double *vee, double *dvee, double *phi,

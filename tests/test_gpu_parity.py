@@ -68,6 +68,26 @@ def test_strained_box_neighbour_list_exact(oracle_mod, gpu_lib):
     assert np.array_equal(nlo[mask], nlg[mask])
 
 
+def test_neighbour_list_exact_beyond_staging(oracle_mod, gpu_lib):
+    """3^3 link cells over a 2000-atom box: about 74 atoms per cell, so a half
+    stencil holds about 1040 candidates, beyond the 640 the builder stages in
+    shared memory; the rest are read from global memory.  NLIST/NUMN are
+    still identical entry by entry."""
+    w = wl.make_workload(10, sigma=0.1, temperature=0.0, seed=14)
+    w.nlc = (3, 3, 3)
+    o, g = _pair(oracle_mod, gpu_lib, w)
+    g.linkup()
+    counts = np.bincount(g.linkcells(27)[2] - 1, minlength=27)
+    assert counts.min() * 14 > 640
+    assert o.update_neighbourlist() == 0
+    g.update_neighbourlist()
+    nlo, nno = o.nlist()
+    nlg, nng = g.neighbour_list()
+    assert np.array_equal(nno, nng)
+    for i in range(w.nm):
+        assert np.array_equal(nlo[i, :nno[i]], nlg[i, :nng[i]]), i
+
+
 @pytest.mark.parametrize("n", [8, 30])
 def test_relink_chain_order_exact(oracle_mod, gpu_lib, n):
     """relink replays the reference's chain surgery: same l0/link after moves,
@@ -148,6 +168,52 @@ def test_set_tables_drop_in(oracle_mod, gpu_lib):
     g.set_state(w.x0, w.x1, w.x2, w.b0, w.b1, w.b2, w.atomic_number, w.atomic_mass, w.del2)
     g.force()
     assert rel_norm_err(g.forces(), o.forces()) < FP64_TOL
+
+
+def _offset_tables(o, nlookup, rmin, rmax):
+    """Caller tables over [rmin, rmax] from the analytic FETRANSMETAL Fe-Fe
+    functions: rmin > 0, and since rmax lies inside the cut, the last node is
+    nonzero, so every pair beyond rmax takes T(nlookup) (src/lookup_m.F90:322-340)."""
+    r = rmin + np.arange(nlookup + 1) * ((rmax - rmin) / nlookup)
+    t = {k: np.array([o.src(i, x) for x in r]) for i, k in enumerate(("vee", "dvee", "phi", "dphi"))}
+    full = o.tables()
+    t["emb"], t["demb"] = full["emb"], full["demb"]
+    return t
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_set_tables_offset_range_nonzero_tail(oracle_mod, gpu_lib, precision):
+    """Caller tables with rmin = 1.2 A and rmax = 3.2 A (inside the 3.73 A cut,
+    so the last node is nonzero and every listed pair out to rnear contributes):
+    FP64 within 1e-10 of the oracle; mixed within the accuracy gate (real-force
+    RMS <= 1e-5 eV/A, pe <= 1e-6 eV/atom, stress <= 1e-4 GPa)."""
+    from moldy_b200 import MoldySystem
+    from moldy_b200 import units
+    w = wl.make_workload(6, sigma=0.08, temperature=0.0, seed=9)
+    o = oracle_mod.from_workload(w, uselookup=True, threads=1)
+    rmin, rmax = 1.2, 3.2
+    tabs = _offset_tables(o, 5000, rmin, rmax)
+    assert min(abs(tabs[k][-1]) for k in ("vee", "dvee", "phi", "dphi")) > 1e-3
+    o.set_tables(tabs, rmin=rmin, rmax=rmax)
+    o.force()
+    oo = o.force_out()
+    g = MoldySystem(w.nm, rnear=w.rnear, deltat=w.deltat, ivol=w.ivol, ntcm=w.ntcm, nlc=w.nlc,
+                    precision=precision)
+    g.set_tables(tabs, rmin=rmin, rmax=rmax)
+    g.set_state(w.x0, w.x1, w.x2, w.b0, w.b1, w.b2, w.atomic_number, w.atomic_mass, w.del2)
+    go = g.force()
+    if precision == "fp64":
+        assert rel_norm_err(g.forces(), o.forces()) < FP64_TOL
+        assert rel_norm_err(g.density()["rho"], o.density()["rho"]) < FP64_TOL
+        assert abs(go["pe"] - oo["pe"]) < FP64_TOL * abs(oo["pe"])
+        assert rel_norm_err(go["tp"], oo["tp"]) < FP64_TOL
+        return
+    df = real_forces(g.forces(), w.b0) - real_forces(o.forces(), w.b0)
+    rms = float(np.sqrt(np.mean(np.sum(df * df, axis=1))))
+    assert rms <= 1e-5, rms
+    assert abs(go["pe"] - oo["pe"]) / w.nm < 1e-6
+    sig = lambda fo: -(w.b0 @ (fo["tp"]).T).T / fo["vol"] * units.PRESS_TO_GPA
+    assert np.max(np.abs(sig(go) - sig(oo))) < 1e-4
 
 
 def test_md_trajectory_nve_100_steps(oracle_mod, gpu_lib):
