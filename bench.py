@@ -390,33 +390,71 @@ def time_path(args, w, precision, local_rank, barrier, max_over_ranks, with_e2e)
             "out_builds_per_step": out_builds_per_step}
 
 
+def _errors(f, pe, sig, f_ref, pe_ref, sig_ref, nm):
+    df = f - f_ref
+    return {"force_rms_err_eV_per_A": float(np.sqrt(np.mean(np.sum(df * df, axis=1)))),
+            "force_max_err_eV_per_A": float(np.max(np.linalg.norm(df, axis=1))),
+            "pe_err_eV_per_atom": abs(pe - pe_ref) / nm,
+            "stress_max_err_GPa": float(np.max(np.abs(sig - sig_ref))) * 160.21766}
+
+
 def accuracy(w, local_rank, nve_steps):
-    """Mixed against FP64 on the same 2M-atom state: real-force RMS error, pe
-    and stress differences; and the total-energy drift of an NVE run of the
-    same lattice (te = ke + pe per atom, least-squares slope per ps)."""
+    """On the same 2M-atom state: the mixed path against the FP64 path, and both
+    against the oracle (the C restatement of the reference, all host threads):
+    real-force RMS and max errors, pe and stress differences, and whether the
+    half list NLIST/NUMN is identical entry by entry.  Then the total-energy
+    drift of an NVE run of the same lattice (te = ke + pe per atom,
+    least-squares slope per ps) with the lookup tables in both precisions, and
+    with the analytic pair functions (uselookup = 0, FP64)."""
+    import oracle
     from moldy_b200 import MoldySystem
     from moldy_b200 import workloads as wl
     out = {}
     res = {}
+    nl_gpu = None
     for prec in ("fp64", "mixed"):
         s = MoldySystem.from_workload(w, precision=prec, device=local_rank)
         s.linkup()
         fo = s.force()
         b0 = s.get_state()["b0"]
         res[prec] = (s.forces() @ b0.T, fo["pe"], -(fo["tp"] @ b0.T) / fo["vol"])
+        if prec == "fp64":
+            nl_gpu = s.neighbour_list()
         s.close()
-    df = res["mixed"][0] - res["fp64"][0]
-    out["force_rms_err_eV_per_A"] = float(np.sqrt(np.mean(np.sum(df * df, axis=1))))
-    out["force_max_err_eV_per_A"] = float(np.max(np.linalg.norm(df, axis=1)))
-    out["pe_err_eV_per_atom"] = abs(res["mixed"][1] - res["fp64"][1]) / w.nm
-    out["stress_max_err_GPa"] = float(np.max(np.abs(res["mixed"][2] - res["fp64"][2]))) * 160.21766
+    out.update(_errors(*res["mixed"], *res["fp64"], w.nm))
+    # against the oracle on the same state
+    oracle.build()
+    nth = oracle.max_threads()
+    o = oracle.from_workload(w, uselookup=True, threads=nth)
+    t0 = time.perf_counter()
+    o.force()
+    t_o = time.perf_counter() - t0
+    oo = o.force_out()
+    ref = (o.forces() @ w.b0.T, oo["pe"], -(oo["tp"] @ w.b0.T) / oo["vol"])
+    nlo, nno = o.nlist()
+    o.close()
+    mask = np.arange(w.nnbrs, dtype=np.int32)[None, :] < nno[:, None]
+    nl_same = bool(np.array_equal(nno, nl_gpu[1]) and np.array_equal(np.where(mask, nlo, 0), nl_gpu[0]))
+    del nlo, mask
+    fr = np.linalg.norm(ref[0])
+    out["vs_oracle"] = {
+        "oracle": f"C restatement of the reference, FP64, {nth} OpenMP threads, {t_o:.2f} s for linkup, "
+                  "half-list build and force",
+        "neighbour_list_identical": nl_same,
+        "half_list_entries": int(nno.sum()),
+        "fp64": {**_errors(*res["fp64"], *ref, w.nm),
+                 "force_rel_norm_err": float(np.linalg.norm(res["fp64"][0] - ref[0]) / fr)},
+        "mixed": {**_errors(*res["mixed"], *ref, w.nm),
+                  "force_rel_norm_err": float(np.linalg.norm(res["mixed"][0] - ref[0]) / fr)},
+    }
     if nve_steps > 0:
         wn = wl.make_workload(w.meta["n"], sigma=0.05, temperature=300.0, ivol=1, nbrupdate=100, seed=5,
                               name="bcc_fe_nve_300K")
         dt_ps = wn.meta["dt_fs"] / 1000.0
         drift = {}
-        for prec in ("fp64", "mixed"):
-            s = MoldySystem.from_workload(wn, precision=prec, device=local_rank)
+        for prec, lookup in (("fp64", True), ("mixed", True), ("fp64_exact", False)):
+            s = MoldySystem.from_workload(wn, precision=prec.split("_")[0], uselookup=lookup,
+                                          device=local_rank)
             s.linkup()
             s.md_init()
             th = s.md_steps(nve_steps, thermo=True)
@@ -425,6 +463,9 @@ def accuracy(w, local_rank, nve_steps):
             slope = float(np.polyfit(t, te, 1)[0])
             drift[prec] = {"slope_eV_per_atom_per_ps": slope, "te_range_eV_per_atom": float(te.max() - te.min())}
             s.close()
+        drift["fp64_exact"]["note"] = ("analytic pair functions (uselookup = 0): the tabulated dvee is not "
+                                       "the derivative of the interpolated vee, which the lookup runs' "
+                                       "drift reflects")
         out["nve_drift"] = {"workload": f"{wn.nm}-atom bcc Fe NVE, 300 K, {nve_steps} steps of 1 fs",
                             **drift,
                             "mixed_minus_fp64_eV_per_atom_per_ps": drift["mixed"]["slope_eV_per_atom_per_ps"] -

@@ -389,8 +389,13 @@ int moldy_gpu_batch_get_stream(moldy_batch *h, void **stream);
  * is queued on `stream` (a cudaStream_t, NULL = legacy default stream) and
  * the call returns after it finishes.  The first call on each device looks
  * up the array's device address; make that first call before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU race
- * and give wrong results. */
+ * capture; the cached address belongs to the device's primary context, so a
+ * device reset or a caller-made context between calls is not supported.
+ * Every call shares the array: calls that overlap on the GPU race and give
+ * wrong results.  Unlike embed (src/potential_m.F90:162), an atom with
+ * rho <= 1e-40 gets F = F' = 0 (the array may hold another system's F').
+ * A NUMN count outside 0..nnbrs or an NLIST entry outside 1..nm returns
+ * MOLDY_ERR_INVALID (the row is clamped, the entry skipped). */
 #define MOLDY_NOALLOC_MAX_ATOMS 262144
 int moldy_gpu_force_noalloc(int32_t nm, int32_t nnbrs, int32_t ivol,
                             const double *x0, const double *y0, const double *z0,

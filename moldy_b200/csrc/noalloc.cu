@@ -18,7 +18,15 @@
 // The host cannot use the array's name as a device address (on the host it
 // names a stand-in object), so the first call on each device looks the
 // address up with cudaGetSymbolAddress, with that device current, and caches
-// it.  That first call should come before any stream capture.
+// it.  That first call should come before any stream capture.  The cached
+// address belongs to the device's primary context: a caller that resets the
+// device (cudaDeviceReset) or runs in a context of its own between calls
+// would get a stale address, and is not supported.
+//
+// One deliberate difference from embed (src/potential_m.F90:148-169): an
+// atom with rho <= 1e-40 gets F = 0 and F'(rho) = 0 here, where the reference
+// skips it and keeps its F' from an earlier call.  The array's previous
+// contents may belong to another system, so they are not used.
 #include <mutex>
 
 #include "engine.h"
@@ -104,7 +112,10 @@ __global__ void __launch_bounds__(256) k_na_density(NaArgs a, NaTables t, double
         double rho_i = 0.0;
         if (active) {
             int n = a.numn[g];
-            n = n < 0 ? 0 : (n > a.nnbrs ? a.nnbrs : n);
+            if (n < 0 || n > a.nnbrs) {   // malformed NUMN: record it, use the clamped count
+                if (l == 0) status[1] = 1.0;
+                n = n < 0 ? 0 : a.nnbrs;
+            }
             const int32_t *row = a.nlist + (size_t)g * a.nnbrs;
             for (int k = l; k < n; k += kNaTPA) {
                 int j = row[k] - 1;
@@ -301,13 +312,18 @@ int force_noalloc(int nm, int nnbrs, int ivol, const double *x0, const double *y
         err = std::string("launch: ") + cudaGetErrorString(e);
         return MOLDY_ERR_CUDA;
     }
-    double status = 0.0;
-    if ((e = cudaMemcpyAsync(&status, scratch + kOffStatus, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+    double status[2] = {0.0, 0.0};
+    if ((e = cudaMemcpyAsync(status, scratch + kOffStatus, 2 * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess) {
         err = std::string("synchronize: ") + cudaGetErrorString(e);
         return MOLDY_ERR_CUDA;
     }
-    if (status != 0.0) {
+    if (status[1] != 0.0) {
+        err = "NUMN holds a count outside 0..nnbrs (those rows were clamped)";
+        return MOLDY_ERR_INVALID;
+    }
+    if (status[0] != 0.0) {
         err = "neighbour list holds an atom index outside 1..nm (those pairs were skipped)";
         return MOLDY_ERR_INVALID;
     }
