@@ -352,6 +352,19 @@ int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, dou
  * 8) and how many candidates a warp stages in shared memory (0..256, default
  * 256; the rest are read from global memory). */
 int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
+/* Chooses, on the live configuration, the lanes per home atom of the tile
+ * screen (4, 8, 16, 32; timed on evaluations that rebuild every list) and the
+ * row entries gathered at a time by the per-atom passes (1, 2, 4; timed with
+ * current lists), nreps evaluations each in the current precision, and keeps
+ * the fastest.  times_ms (7 doubles, may be NULL) receives the mean times in
+ * that order, chosen (2 int32, may be NULL) lanes and entries.  Results do not
+ * depend on either choice; positions and boxes are unchanged. */
+int moldy_gpu_batch_autotune(moldy_batch *h, int32_t nreps, double *times_ms, int32_t *chosen);
+/* One evaluation of every system (as moldy_gpu_batch_force) with its four
+ * launches timed by CUDA events on the batch's stream: the list check, the
+ * tile screen, the density pass and the force pass, into ms4 (ms);
+ * rebuild = 1 rebuilds every list first. */
+int moldy_gpu_batch_kernel_times(moldy_batch *h, int32_t rebuild, double *ms4);
 /* Precision of the per-atom density and force passes of moldy_gpu_batch_force:
  * 0 all FP64 (default); 1 mixed: separations, distances, table interpolation
  * and pair forces in FP32 from FP64 position differences, every sum in FP64,
@@ -359,6 +372,30 @@ int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
  * evaluates in FP64: its line search compares energies that differ in the
  * seventh digit, below what FP32 distances resolve. */
 int moldy_gpu_batch_set_precision(moldy_batch *h, int32_t mixed);
+/* Whether moldy_gpu_batch_force also forms energy_calc's per-atom energies
+ * (src/dynamics_m.F90:412-483, the exact pair function at every pair inside
+ * the cut): 1 (default) yes; 0 no, and the energy_calc sums and
+ * moldy_gpu_batch_get_energies' en_calc read zero.  The force routine's
+ * energy, the forces and the virial do not depend on it; the quench always
+ * forms them, since derivs (src/quench_m.F90:215-323) takes its energy from
+ * energy_calc. */
+int moldy_gpu_batch_set_energy_calc(moldy_batch *h, int32_t enable);
+/* Force matching over all systems of a batch (no counterpart in the
+ * reference; it differentiates what write_energy_forces_stress prints,
+ * src/dynamics_m.F90:588-619).  set_references takes the reference real
+ * forces (3 * ntot doubles, interleaved x, y, z per atom, atom order) and
+ * stresses (9 doubles per system, sigma(i,j) at i + 3 j, in the model units
+ * of moldy_gpu_batch_force's tp: sigma(i,j) = -sum_k b0(j,k) tp(i,k) / vol).  force_matching then runs one FP64 evaluation of
+ * every system, writes each system's loss
+ *   L_s = w_force sum_i |F_i - F_i^ref|^2 + w_stress |sigma_s - sigma_s^ref|^2
+ * into loss[nsys], and dL/d(table) of sum_s L_s into table_grads[6 * (nlookup
+ * + 1)] (vee, dvee, phi, dphi, emb, demb; vee and emb get none, the loss holds
+ * no energy).  Pairs inside the table cut enter, which carries every node
+ * below the cut and every knot derivative (moldy_fetm_knot_vjp contracts the
+ * table gradients to the knots). */
+int moldy_gpu_batch_set_references(moldy_batch *h, const double *fref_xyz, const double *sref);
+int moldy_gpu_batch_force_matching(moldy_batch *h, double w_force, double w_stress, double *loss,
+                                   double *table_grads);
 /* Row entries one thread gathers before it evaluates them in the per-atom
  * passes: 1, 2 or 4 (default 4).  Results do not depend on it. */
 int moldy_gpu_batch_set_gather(moldy_batch *h, int32_t entries);

@@ -128,6 +128,11 @@ SIGNATURES = {
     "moldy_gpu_batch_set_tiles": [H, ctypes.c_int32, ctypes.c_int32],
     "moldy_gpu_batch_set_skin": [H, ctypes.c_double],
     "moldy_gpu_batch_set_precision": [H, ctypes.c_int32],
+    "moldy_gpu_batch_set_energy_calc": [H, ctypes.c_int32],
+    "moldy_gpu_batch_autotune": [H, ctypes.c_int32, D, I],
+    "moldy_gpu_batch_kernel_times": [H, ctypes.c_int32, D],
+    "moldy_gpu_batch_set_references": [H, D, D],
+    "moldy_gpu_batch_force_matching": [H, ctypes.c_double, ctypes.c_double, D, D],
     "moldy_gpu_batch_set_gather": [H, ctypes.c_int32],
     "moldy_gpu_batch_list_stats": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],

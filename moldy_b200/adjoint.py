@@ -181,6 +181,38 @@ class ForceMatchingKnots(torch.autograd.Function):
         return (None,) * 6 + tuple(g * t for t in ctx.grads)
 
 
+class BatchForceMatchingKnots(torch.autograd.Function):
+    """The force-matching loss of every configuration held by a
+    :class:`moldy_b200.MoldyBatch` (its references set with
+    ``set_references``), as a function of the Fe-Fe knots.  The forward builds
+    the tables from the knots, runs one FP64 evaluation of all systems, forms
+    the loss and the table gradients on the device (moldy_gpu_batch_force_matching)
+    and contracts them with d(table)/d(knot) on the host; backward scales the
+    stored gradient.  ``apply(batch, w_force, w_stress, nlookup, av, rv, ap, rp)``."""
+
+    @staticmethod
+    def forward(ctx, batch, w_force, w_stress, nlookup, av, rv, ap, rp):
+        coeffs = FeFeCoefficients(*(_f64(t.detach().cpu().numpy()) for t in (av, rv, ap, rp)))
+        batch.set_up_fetm(coeffs, nlookup=int(nlookup))
+        loss, tg = batch.force_matching(w_force, w_stress)
+        kg = fetm_knot_vjp(coeffs, tg, int(nlookup))
+        ctx.grads = [torch.as_tensor(kg[name]) for name in KNOT_NAMES]
+        ctx.loss_per_system = loss
+        return torch.tensor(float(loss.sum()), dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, g):
+        return (None,) * 4 + tuple(g * t for t in ctx.grads)
+
+
+def batch_force_matching_knots(batch, knots: dict, *, w_force=1.0, w_stress=1.0, nlookup: int = 5000):
+    """Scalar force-matching loss of every configuration of a MoldyBatch,
+    differentiable in the knots dict {av, rv, ap, rp} of torch tensors
+    (BatchForceMatchingKnots)."""
+    return BatchForceMatchingKnots.apply(batch, float(w_force), float(w_stress), int(nlookup),
+                                         *[knots[k] for k in KNOT_NAMES])
+
+
 def force_matching_knots(systems, configs, refs, knots: dict, *, w_force=1.0, w_stress=1.0, nlookup: int = 5000):
     """Scalar force-matching loss of many configurations on one system or a
     list of systems, differentiable in the knots dict {av, rv, ap, rp} of

@@ -60,6 +60,7 @@ class MoldyBatch:
         av, rv, ap, rp = (_f64(v) for v in (coeffs.av, coeffs.rv, coeffs.ap, coeffs.rp))
         check(self._L.moldy_gpu_batch_set_fetm_fe(self._h, len(av), _dp(av), _dp(rv), len(ap), _dp(ap), _dp(rp),
                                                   int(nlookup)))
+        self.nlookup = int(nlookup)
 
     def set_state(self, x0=None, b0=None, mass=None):
         """x0: (ntot, 3) fractional positions; b0: nsys 3x3 boxes (columns are
@@ -155,6 +156,50 @@ class MoldyBatch:
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision is 'fp64' or 'mixed'")
         check(self._L.moldy_gpu_batch_set_precision(self._h, 1 if precision == "mixed" else 0))
+
+    def autotune(self, nreps: int = 3) -> dict:
+        """Chooses the tile lanes per home atom and the gather width on the
+        live configuration (moldy_gpu_batch_autotune); returns the mean
+        evaluation times (ms) and the choice."""
+        t = np.zeros(7)
+        ch = (ctypes.c_int32 * 2)()
+        check(self._L.moldy_gpu_batch_autotune(self._h, int(nreps), _dp(t), ch))
+        return {"lanes_ms": dict(zip((4, 8, 16, 32), t[:4].tolist())),
+                "gather_ms": dict(zip((1, 2, 4), t[4:].tolist())),
+                "chosen": {"lanes": int(ch[0]), "gather": int(ch[1])}}
+
+    def set_references(self, f_ref, sigma_ref):
+        """Reference real forces (one (nm_s, 3) array per system, or one (ntot, 3)
+        array in atom order) and stresses ((nsys, 3, 3), sigma(i,j) =
+        -sum_k b0(j,k) tp(i,k) / vol, model units) for :meth:`force_matching`."""
+        f = np.ascontiguousarray(np.concatenate(f_ref) if isinstance(f_ref, (list, tuple)) else f_ref,
+                                 dtype=np.float64).reshape(self.ntot, 3)
+        sg = np.asarray(sigma_ref, dtype=np.float64).reshape(self.nsys, 3, 3)
+        sref = np.ascontiguousarray(np.stack([m.ravel(order="F") for m in sg]))
+        check(self._L.moldy_gpu_batch_set_references(self._h, _dp(f), _dp(sref)))
+
+    def force_matching(self, w_force=1.0, w_stress=1.0):
+        """One FP64 evaluation of every system: the per-system force-matching
+        loss against the references and dL/d(table) of their sum (dict of the
+        six tables; vee and emb get none)."""
+        loss = np.zeros(self.nsys)
+        nb = self.nlookup + 1
+        g = np.zeros(6 * nb)
+        check(self._L.moldy_gpu_batch_force_matching(self._h, float(w_force), float(w_stress), _dp(loss), _dp(g)))
+        names = ("vee", "dvee", "phi", "dphi", "emb", "demb")
+        return loss, {k: g[i * nb:(i + 1) * nb].copy() for i, k in enumerate(names)}
+
+    def kernel_times(self, rebuild=False) -> dict:
+        """One evaluation with its four launches timed (ms): the list check,
+        the tile screen, the density pass and the force pass."""
+        t = np.zeros(4)
+        check(self._L.moldy_gpu_batch_kernel_times(self._h, 1 if rebuild else 0, _dp(t)))
+        return dict(zip(("prepare", "tile_screen", "density", "forces"), t.tolist()))
+
+    def set_energy_calc(self, enable=True):
+        """Whether force() also forms energy_calc's per-atom energies (the
+        exact pair function; default on).  The quench always forms them."""
+        check(self._L.moldy_gpu_batch_set_energy_calc(self._h, 1 if enable else 0))
 
     def set_gather(self, entries=4):
         """Row entries a thread gathers at a time in the per-atom passes (1, 2, 4)."""

@@ -170,7 +170,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
-                    d.pair_cnt, d.olist, d.out_own, d.out_rev, d.out_nrev, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.olist, d.out_cnt, d.rlist, d.numr, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -237,9 +237,9 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.alist, nm * (size_t)p.pair_cap, "compact list"));
     CHECK(dev_alloc(&d.pair_cnt, nm, "pair_cnt"));
     CHECK(dev_alloc(&d.olist, nm * (size_t)p.out_cap, "outer list"));
-    CHECK(dev_alloc(&d.out_own, nm, "out_own"));
-    CHECK(dev_alloc(&d.out_rev, nm, "out_rev"));
-    CHECK(dev_alloc(&d.out_nrev, nm, "out_nrev"));
+    CHECK(dev_alloc(&d.out_cnt, nm, "out_cnt"));
+    CHECK(dev_alloc(&d.rlist, nm * (size_t)p.nnbrs, "reverse half rows"));
+    CHECK(dev_alloc(&d.numr, nm, "numr"));
     CHECK(dev_alloc(&d.xout, nm, "xout"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
@@ -260,9 +260,8 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.posq2, 0, nm * sizeof(int4)), "memset posq2");
     CUDA_CHECK(cudaMemset(d.pos2, 0, nm * sizeof(double4)), "memset pos2");
     CUDA_CHECK(cudaMemset(d.pair_cnt, 0, nm * sizeof(int32_t)), "memset pair_cnt");
-    CUDA_CHECK(cudaMemset(d.out_own, 0, nm * sizeof(int32_t)), "memset out_own");
-    CUDA_CHECK(cudaMemset(d.out_rev, 0, nm * sizeof(int32_t)), "memset out_rev");
-    CUDA_CHECK(cudaMemset(d.out_nrev, 0, nm * sizeof(int32_t)), "memset out_nrev");
+    CUDA_CHECK(cudaMemset(d.out_cnt, 0, nm * sizeof(int32_t)), "memset out_cnt");
+    CUDA_CHECK(cudaMemset(d.numr, 0, nm * sizeof(int32_t)), "memset numr");
     CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(int4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.xout, 0, nm * sizeof(int4)), "memset xout");
@@ -572,6 +571,12 @@ int Engine::check_flags() {
     if (f[1]) {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
         return fail(MOLDY_ERR_CAPACITY, "link-cell relink produced inconsistent cell counts");
+    }
+    if (f[10]) {
+        cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);
+        return fail(MOLDY_ERR_NEIGHBOUR_OVERFLOW, "an atom appears in the half-list rows of " +
+                                                      std::to_string(f[11]) + " atoms, more than nnbrs (" +
+                                                      std::to_string(prm.nnbrs) + "): increase nnbrs");
     }
     if (f[3] || f[5] || f[8]) {
         cudaMemsetAsync(d.flags, 0, sizeof(f), stream_);

@@ -396,7 +396,7 @@ __device__ __forceinline__ void frac_diff(const double4 &p, const double4 &q, do
 // separation B0 d, distance and table interpolation in FP32 from the FP64
 // difference and sums rho_i in FP64.  Entries are summed in row order at
 // every B.
-template <bool MIXED, int B>
+template <bool MIXED, int B, bool ECALC>
 __global__ void __launch_bounds__(256)
 k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
              const int32_t *__restrict__ cnt, double *__restrict__ sfp, double *__restrict__ rho_out,
@@ -433,9 +433,11 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
                     const float r2 = ux * ux + uy * uy + uz * uz;
                     if (!(r2 < rc2f)) continue;
                     rho += (double)lookup_phif(t, sqrtf(r2));
-                    double vx, vy, vz;
-                    pair_u(b, dx, dy, dz, vx, vy, vz);
-                    ec += 0.5 * fetm_vee(t, sqrt(vx * vx + vy * vy + vz * vz));
+                    if (ECALC) {
+                        double vx, vy, vz;
+                        pair_u(b, dx, dy, dz, vx, vy, vz);
+                        ec += 0.5 * fetm_vee(t, sqrt(vx * vx + vy * vy + vz * vz));
+                    }
                 } else {
                     double ux, uy, uz;
                     pair_u(b, dx, dy, dz, ux, uy, uz);
@@ -443,7 +445,7 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
                     if (!(r2 < a.rc2)) continue;
                     const double r = sqrt(r2);
                     rho += lookup_phi(t, r);
-                    ec += 0.5 * fetm_vee(t, r);
+                    if (ECALC) ec += 0.5 * fetm_vee(t, r);
                 }
             }
         }
@@ -457,7 +459,7 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
         rho_out[at] = rho;
         afrho_out[at] = f;
         fp_out[at] = fd;
-        en_calc[at] = f + ec;
+        if (ECALC) en_calc[at] = f + ec;
     }
 }
 
@@ -582,6 +584,205 @@ k_sys_reduce(const BSys *__restrict__ sys, const double *__restrict__ en_calc, c
 // --------------------------------------------------------- CG control --
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// --------------------------------------------------------- force matching --
+// The force-matching loss of one evaluation of every system against
+// reference real forces and stresses, and its adjoint with respect to the six
+// lookup tables (no counterpart in the reference).  The differentiated
+// quantities are those write_energy_forces_stress prints
+// (src/dynamics_m.F90:588-619): F = B0 f and sigma(i,j) = -sum_k b0(j,k)
+// tp(i,k) / vol.  With dL/dF_i = gF_i and dL/dsigma_s = G_s, per pair (i,j)
+// inside the table cut, u = B0 d, r = |u|:
+//   lam_ij = (gF_i - gF_j) . u - u^T G_s u / vol_s  [m_i + m_j > 0.1]   (= dL/dfp_ij)
+//   mu_i = dL/dF'_i = sum_j -lam_ij DP(r_ij) / r_ij
+//   nu_i = dL/drho_i = mu_i De'(rho_i)          (slope of the interpolant)
+//   dL/dDV(r) = -lam / r,  dL/dDP(r) = -lam (F'_i + F'_j) / r,  dL/dP(r) = nu_i + nu_j,
+//   dL/dDe(rho_i) = mu_i,  dL/dV = dL/dEm = 0 (the loss holds no energy),
+// each table node receiving its interpolation weight times these.  Every row
+// holds both directions, so each atom forms its own mu and nu from its row,
+// with no atomics; a table histogram takes each pair once (from the lower
+// slot).  Only pairs inside the table cut enter: they carry every table
+// node below the cut, and with it every knot derivative (the Fe-Fe forms and
+// their knot derivatives vanish at and beyond the largest knot).  rho comes
+// from the forward pass (per atom), F' from its cell-order copy.
+
+// Loss and dL/dF, dL/dsigma of one evaluation; one block per system.  gF
+// goes to cell order (slot hs) for the pair passes.
+__global__ void __launch_bounds__(kCgThreads)
+k_fm_loss(const BSys *__restrict__ sys, const double *__restrict__ f, const double *__restrict__ fref,
+          const double *__restrict__ sref, const double *__restrict__ sysout, const int32_t *__restrict__ sorted,
+          double wf, double ws, double *__restrict__ gF, double *__restrict__ gS, double *__restrict__ loss) {
+    __shared__ double sh[33];
+    const BSys &S = sys[blockIdx.x];
+    double lf = 0.0;
+    for (int hs = S.atom0 + threadIdx.x; hs < S.atom0 + S.nm; hs += blockDim.x) {
+        const size_t at = 3 * (size_t)sorted[hs];
+        double fx, fy, fz;
+        pair_u(S.b0, f[at], f[at + 1], f[at + 2], fx, fy, fz);
+        const double dx = fx - fref[at], dy = fy - fref[at + 1], dz = fz - fref[at + 2];
+        lf += dx * dx + dy * dy + dz * dz;
+        gF[3 * (size_t)hs] = 2.0 * wf * dx;
+        gF[3 * (size_t)hs + 1] = 2.0 * wf * dy;
+        gF[3 * (size_t)hs + 2] = 2.0 * wf * dz;
+    }
+    lf = block_sum(lf, sh);
+    if (threadIdx.x == 0) {
+        const double *o = sysout + 13 * (size_t)blockIdx.x;
+        const double *tp = o + 4;
+        double ls = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double sg = 0.0;
+                for (int k = 0; k < 3; ++k) sg -= S.b0[j + 3 * k] * tp[i + 3 * k];
+                sg /= o[3];
+                const double d = sg - sref[9 * (size_t)blockIdx.x + i + 3 * j];
+                ls += d * d;
+                gS[9 * (size_t)blockIdx.x + i + 3 * j] = 2.0 * ws * d;
+            }
+        loss[blockIdx.x] = wf * lf + ws * ls;
+    }
+}
+
+// index and weights of the lookup_m interpolation (src/lookup_m.F90:322-341)
+// below the table end
+__device__ __forceinline__ int fm_weights(double x, double xmin, double range, double recipr, double recipn,
+                                          double recips, int n, double &w1) {
+    int idx = (int)(((double)n * (x - xmin)) * recipr);
+    idx = idx < 0 ? 0 : (idx > n - 1 ? n - 1 : idx);
+    const double xlow = xmin + (range * (double)idx) * recipn;
+    w1 = (x - xlow) * recips;
+    return idx;
+}
+
+__device__ __forceinline__ void fm_hist(double *h, int k, double c, double w1) {
+    atomicAdd(&h[k], c * (1.0 - w1));
+    atomicAdd(&h[k + 1], c * w1);
+}
+
+__device__ __forceinline__ void fm_flush(const double *h, double *g, int nb) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const double v = h[k];
+        if (v != 0.0) atomicAdd(&g[k], v);
+    }
+}
+
+// the pair geometry of slot hs and row entry j: u = B0 d, r; false beyond the cut
+__device__ __forceinline__ bool fm_pair(const BSys &S, const double4 &ph, const double4 &pj, double rc2,
+                                        double &ux, double &uy, double &uz, double &r) {
+    double dx, dy, dz;
+    frac_diff(ph, pj, dx, dy, dz);
+    pair_u(S.b0, dx, dy, dz, ux, uy, uz);
+    const double r2 = ux * ux + uy * uy + uz * uz;
+    if (!(r2 < rc2)) return false;
+    r = sqrt(r2);
+    return true;
+}
+
+// lam per pair; mu_i; dL/d dvee and dL/d dphi
+__global__ void __launch_bounds__(256)
+k_fm_pairs_a(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
+             const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ gF,
+             const double *__restrict__ gS, double *__restrict__ mu, double *__restrict__ g_dvee,
+             double *__restrict__ g_dphi, int nbr) {
+    extern __shared__ double sh[];
+    double *hdv = sh, *hdp = sh + nbr;
+    for (int k = threadIdx.x; k < 2 * nbr; k += blockDim.x) sh[k] = 0.0;
+    __syncthreads();
+    const double rmin = t.vp_rmin, range = t.vp_range, recipr = t.vp_reciprange, recipn = t.vp_recipnlkp,
+                 recips = t.vp_recipstep;
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
+        const int s = slot_sys[hs];
+        const BSys &S = a.sys[s];
+        const double4 ph = a.spos[hs];
+        const double fph = a.sfp[hs];
+        const double gx = gF[3 * (size_t)hs], gy = gF[3 * (size_t)hs + 1], gz = gF[3 * (size_t)hs + 2];
+        const double *G = gS + 9 * (size_t)s;
+        const double ivol = 1.0 / S.vol;
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
+        double m = 0.0;
+        for (int e = 0; e < n; ++e) {
+            const int j = alist[(size_t)e * ntot + hs];
+            const double4 pj = a.spos[j];
+            double ux, uy, uz, r;
+            if (!fm_pair(S, ph, pj, a.rc2, ux, uy, uz, r)) continue;
+            double w1;
+            const int q = fm_weights(r, rmin, range, recipr, recipn, recips, t.nlookup, w1);
+            const double dp = t.r4[q].w * (1.0 - w1) + t.r4[q + 1].w * w1;
+            double lam = (gx - gF[3 * (size_t)j]) * ux + (gy - gF[3 * (size_t)j + 1]) * uy +
+                         (gz - gF[3 * (size_t)j + 2]) * uz;
+            if (ph.w + pj.w > 0.1)
+                lam -= ivol * (ux * (G[0] * ux + G[3] * uy + G[6] * uz) + uy * (G[1] * ux + G[4] * uy + G[7] * uz) +
+                               uz * (G[2] * ux + G[5] * uy + G[8] * uz));
+            const double rr = 1.0 / r;
+            m -= lam * dp * rr;
+            if (hs < j) {
+                fm_hist(hdv, q, -lam * rr, w1);
+                fm_hist(hdp, q, -lam * (fph + a.sfp[j]) * rr, w1);
+            }
+        }
+        mu[hs] = m;
+    }
+    fm_flush(hdv, g_dvee, nbr);
+    fm_flush(hdp, g_dphi, nbr);
+}
+
+// nu_i = mu_i De'(rho_i) and dL/d demb per atom
+__global__ void __launch_bounds__(256)
+k_fm_atoms(Tables t, int ntot, const int32_t *__restrict__ sorted, const double *__restrict__ rho,
+           const double *__restrict__ mu, double *__restrict__ nu, double *__restrict__ g_demb) {
+    extern __shared__ double sh[];
+    const int nb = t.nlookup + 1;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) sh[k] = 0.0;
+    __syncthreads();
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
+        const double r = rho[sorted[hs]];
+        double v = 0.0;
+        if (r > 1e-40) {
+            if (r >= t.e_rmax) {
+                atomicAdd(&sh[t.nlookup], mu[hs]);   // the last node alone, zero slope
+            } else {
+                double w1;
+                const int q = fm_weights(r, t.e_rmin, t.e_range, t.e_reciprange, t.e_recipnlkp, t.e_recipstep,
+                                         t.nlookup, w1);
+                v = mu[hs] * (t.e2[q + 1].y - t.e2[q].y) * t.e_recipstep;
+                fm_hist(sh, q, mu[hs], w1);
+            }
+        }
+        nu[hs] = v;
+    }
+    fm_flush(sh, g_demb, nb);
+}
+
+// dL/d phi = nu_i + nu_j per pair
+__global__ void __launch_bounds__(256)
+k_fm_pairs_c(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restrict__ alist,
+             const int32_t *__restrict__ cnt, const int32_t *__restrict__ slot_sys, const double *__restrict__ nu,
+             double *__restrict__ g_phi, int nbr) {
+    extern __shared__ double sh[];
+    for (int k = threadIdx.x; k < nbr; k += blockDim.x) sh[k] = 0.0;
+    __syncthreads();
+    for (int hs = blockIdx.x * blockDim.x + threadIdx.x; hs < ntot; hs += gridDim.x * blockDim.x) {
+        const BSys &S = a.sys[slot_sys[hs]];
+        const double4 ph = a.spos[hs];
+        const double nui = nu[hs];
+        int n = cnt[hs];
+        n = n < pair_cap ? n : pair_cap;
+        for (int e = 0; e < n; ++e) {
+            const int j = alist[(size_t)e * ntot + hs];
+            if (!(hs < j)) continue;
+            double ux, uy, uz, r;
+            if (!fm_pair(S, ph, a.spos[j], a.rc2, ux, uy, uz, r)) continue;
+            double w1;
+            const int q = fm_weights(r, t.vp_rmin, t.vp_range, t.vp_reciprange, t.vp_recipnlkp, t.vp_recipstep,
+                                     t.nlookup, w1);
+            fm_hist(sh, q, nui + nu[j], w1);
+        }
+    }
+    fm_flush(sh, g_phi, nbr);
+}
+
 
 struct CgVecs {
     double *X, *G, *D, *GS, *XX, *GG, *DR, *DGR;
@@ -902,9 +1103,24 @@ class BatchEngine {
     int get_state(double *x0, double *y0, double *z0);
     int force(double *out13);
     int quench(int maxfn, int criterion, double fmax, double *out8);
+    int autotune(int nreps, double *times_ms, int32_t *chosen);
+    // force matching: references (device), dL/dF in cell order, dL/dsigma,
+    // per-system loss, mu, nu and the six table gradients; allocated on first use
+    double *fm_fref = nullptr, *fm_sref = nullptr, *fm_gF = nullptr, *fm_gS = nullptr, *fm_loss = nullptr;
+    double *fm_mu = nullptr, *fm_nu = nullptr, *fm_grads = nullptr;
+    int fm_nb = 0;
+    bool fm_refs = false;
+    int set_references(const double *fref_xyz, const double *sref);
+    int force_matching(double wf, double ws, double *loss, double *grads);
     int get_array(const double *dev, int stride, double *a, double *b, double *c);
     int copy_xyz(double *dev, const double *src, double *dst);
-    void queue_evaluation(bool with_vir, bool use_mixed);
+    // ecalc: also energy_calc's per-atom energies (exact pair function), which
+    // the quench needs and a plain force evaluation only when asked
+    // ev (5 events, may be null): recorded before k_prepare, the tile screen,
+    // the density pass and the force pass, and after the force pass
+    void queue_evaluation(bool with_vir, bool use_mixed, bool ecalc, cudaEvent_t *ev = nullptr);
+    int kernel_times(int rebuild, double *ms4);
+    bool ecalc = true;                  // moldy_gpu_batch_force computes energy_calc's energies
     int ready();
     int take_overflow();
 };
@@ -941,7 +1157,8 @@ BatchEngine::~BatchEngine() {
     if (graph) cudaGraphExecDestroy(graph);
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
                     mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
-                    tab_r4f, tab_e2f, tab_aux, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order};
+                    tab_r4f, tab_e2f, tab_aux, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order,
+                    fm_fref, fm_sref, fm_gF, fm_gS, fm_loss, fm_mu, fm_nu, fm_grads};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -1167,11 +1384,17 @@ static void launch_screen(const BatchEngine &E, const TileArgs &a, cudaStream_t 
 }
 
 template <bool MIXED, int B>
-static void launch_passes(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
+static void launch_passes(const BatchEngine &E, const TileArgs &a, bool with_vir, bool ecalc, cudaStream_t s,
+                          cudaEvent_t *ev) {
     const int nbs = grid_blocks(E.ntot, 256);
     // a system's slots are its atoms' index range, so atom_sys is the slot's system
-    k_cl_density<MIXED, B><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp, E.rho,
-                                               E.afrho, E.fp, E.en_calc, E.atom_sys, E.ntodo);
+    if (ecalc)
+        k_cl_density<MIXED, B, true><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp,
+                                                         E.rho, E.afrho, E.fp, E.en_calc, E.atom_sys, E.ntodo);
+    else
+        k_cl_density<MIXED, B, false><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.sfp,
+                                                          E.rho, E.afrho, E.fp, E.en_calc, E.atom_sys, E.ntodo);
+    if (ev) cudaEventRecord(ev[3], s);
     if (with_vir)
         k_cl_forces<MIXED, B, true><<<nbs, 256, 0, s>>>(a, E.tab, E.ntot, E.pair_cap, E.alist, E.pcnt, E.atom_sys,
                                                         E.afrho, E.f, E.en_force, E.vir);
@@ -1181,19 +1404,22 @@ static void launch_passes(const BatchEngine &E, const TileArgs &a, bool with_vir
 }
 
 template <bool MIXED>
-static void launch_passes_b(const BatchEngine &E, const TileArgs &a, bool with_vir, cudaStream_t s) {
+static void launch_passes_b(const BatchEngine &E, const TileArgs &a, bool with_vir, bool ecalc, cudaStream_t s,
+                            cudaEvent_t *ev) {
     switch (E.gather) {
-        case 1: launch_passes<MIXED, 1>(E, a, with_vir, s); break;
-        case 2: launch_passes<MIXED, 2>(E, a, with_vir, s); break;
-        default: launch_passes<MIXED, 4>(E, a, with_vir, s); break;
+        case 1: launch_passes<MIXED, 1>(E, a, with_vir, ecalc, s, ev); break;
+        case 2: launch_passes<MIXED, 2>(E, a, with_vir, ecalc, s, ev); break;
+        default: launch_passes<MIXED, 4>(E, a, with_vir, ecalc, s, ev); break;
     }
 }
 
 // list check (and rebuild) and the tile passes for the systems marked active
-void BatchEngine::queue_evaluation(bool with_vir, bool use_mixed) {
+void BatchEngine::queue_evaluation(bool with_vir, bool use_mixed, bool ecalc, cudaEvent_t *ev) {
     cudaStream_t s = stream;
+    if (ev) cudaEventRecord(ev[0], s);
     k_prepare<<<nsys, kPrepThreads, 0, s>>>(sys, X, mass, Xb, cell_of, cell_count, cell_start, cursor, sorted, spos,
                                            stats, todo, ntodo);
+    if (ev) cudaEventRecord(ev[1], s);
     TileArgs a;
     a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
     a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
@@ -1203,10 +1429,12 @@ void BatchEngine::queue_evaluation(bool with_vir, bool use_mixed) {
         case 32: launch_screen<32>(*this, a, s); break;
         default: launch_screen<8>(*this, a, s); break;
     }
+    if (ev) cudaEventRecord(ev[2], s);
     if (use_mixed)
-        launch_passes_b<true>(*this, a, with_vir, s);
+        launch_passes_b<true>(*this, a, with_vir, ecalc, s, ev);
     else
-        launch_passes_b<false>(*this, a, with_vir, s);
+        launch_passes_b<false>(*this, a, with_vir, ecalc, s, ev);
+    if (ev) cudaEventRecord(ev[4], s);
     launches += 4;
 }
 
@@ -1233,7 +1461,8 @@ int BatchEngine::force(double *out13) {
     BCHECK(ready());
     for (int attempt = 0;; ++attempt) {
         k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
-        queue_evaluation(true, mixed);
+        if (!ecalc) BCUDA(cudaMemsetAsync(en_calc, 0, (size_t)ntot * sizeof(double), stream), "en_calc");
+        queue_evaluation(true, mixed, ecalc);
         k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
         launches += 2;
         BCUDA(cudaStreamSynchronize(stream), "batch force");
@@ -1245,6 +1474,169 @@ int BatchEngine::force(double *out13) {
     }
     if (out13)
         BCUDA(cudaMemcpy(out13, sysout, 13 * (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost), "results");
+    return MOLDY_OK;
+}
+
+// Chooses the tile shape and the gather width on the live configuration:
+// the lanes per home atom of the tile screen (4, 8, 16, 32) by evaluations
+// that rebuild every list, then the row entries gathered at a time by the
+// per-atom passes (1, 2, 4) by evaluations with current lists, each the mean
+// of nreps evaluations in the current precision.  times_ms (7 values) gets
+// those means in that order, chosen (2 values) the choice.  Positions and
+// boxes are left as they were; the lists are current afterwards.
+int BatchEngine::autotune(int nreps, double *times_ms, int32_t *chosen) {
+    BCHECK(ready());
+    if (nreps < 1) nreps = 1;
+    cudaEvent_t e0, e1;
+    BCUDA(cudaEventCreate(&e0), "event");
+    BCUDA(cudaEventCreate(&e1), "event");
+    auto evaluate = [&](bool rebuild) {
+        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, rebuild ? 1 : 0);
+        queue_evaluation(true, mixed, ecalc);
+        k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+        launches += 3;
+    };
+    auto timed = [&](bool rebuild) -> double {
+        double total = 0.0;
+        for (int r = 0; r < nreps; ++r) {
+            if (rebuild) k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 1);
+            cudaEventRecord(e0, stream);
+            evaluate(false);
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            total += ms;
+        }
+        return total / nreps;
+    };
+    const int lanes[4] = {4, 8, 16, 32}, gathers[3] = {1, 2, 4};
+    double t[7];
+    evaluate(true);   // rows sized before timing
+    BCUDA(cudaStreamSynchronize(stream), "autotune");
+    if (take_overflow() < 0) return set_last_error(MOLDY_ERR_CUDA, "compact list re-allocation failed");
+    int bl = 0;
+    for (int k = 0; k < 4; ++k) {
+        lph = lanes[k];
+        t[k] = timed(true);
+        if (t[k] < t[bl]) bl = k;
+    }
+    lph = lanes[bl];
+    evaluate(true);
+    int bg = 0;
+    for (int k = 0; k < 3; ++k) {
+        gather = gathers[k];
+        t[4 + k] = timed(false);
+        if (t[4 + k] < t[4 + bg]) bg = k;
+    }
+    gather = gathers[bg];
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BCUDA(cudaStreamSynchronize(stream), "autotune");
+    BCUDA(cudaGetLastError(), "autotune");
+    if (take_overflow() != 0) return set_last_error(MOLDY_ERR_CAPACITY, "compact rows grew during tuning; run again");
+    if (times_ms) for (int k = 0; k < 7; ++k) times_ms[k] = t[k];
+    if (chosen) { chosen[0] = lph; chosen[1] = gather; }
+    return MOLDY_OK;
+}
+
+// Reference real forces (interleaved x, y, z per atom, atom order) and
+// stresses (9 per system, sigma(i,j) at i + 3 j) for force_matching.
+int BatchEngine::set_references(const double *fref_xyz, const double *sref) {
+    if (!fref_xyz || !sref) return set_last_error(MOLDY_ERR_INVALID, "null reference array");
+    const size_t nt = (size_t)ntot;
+    if (!fm_fref) {
+        BCHECK(balloc(&fm_fref, 3 * nt, "reference forces"));
+        BCHECK(balloc(&fm_sref, 9 * (size_t)nsys, "reference stresses"));
+        BCHECK(balloc(&fm_gF, 3 * nt, "dL/dF"));
+        BCHECK(balloc(&fm_gS, 9 * (size_t)nsys, "dL/dsigma"));
+        BCHECK(balloc(&fm_loss, nsys, "loss"));
+        BCHECK(balloc(&fm_mu, nt, "mu"));
+        BCHECK(balloc(&fm_nu, nt, "nu"));
+    }
+    BCUDA(cudaMemcpyAsync(fm_fref, fref_xyz, 3 * nt * sizeof(double), cudaMemcpyHostToDevice, stream), "references");
+    BCUDA(cudaMemcpyAsync(fm_sref, sref, 9 * (size_t)nsys * sizeof(double), cudaMemcpyHostToDevice, stream),
+          "references");
+    BCUDA(cudaStreamSynchronize(stream), "references");
+    fm_refs = true;
+    return MOLDY_OK;
+}
+
+// One FP64 evaluation of every system, the loss
+//   L_s = w_f sum_i |F_i - F_i^ref|^2 + w_s |sigma_s - sigma_s^ref|^2
+// per system into loss[nsys], and dL/d(table) of L = sum_s L_s into
+// grads[6 (nlookup + 1)] (vee, dvee, phi, dphi, emb, demb).
+int BatchEngine::force_matching(double wf, double ws, double *loss, double *grads) {
+    BCHECK(ready());
+    if (!fm_refs) return set_last_error(MOLDY_ERR_ORDER, "set the references first (moldy_gpu_batch_set_references)");
+    const int n = tab.nlookup, nb = n + 1, nbr = tab.nr;
+    if (fm_nb != nb) {
+        if (fm_grads) cudaFree(fm_grads);
+        fm_grads = nullptr;
+        BCHECK(balloc(&fm_grads, 6 * (size_t)nb, "table gradients"));
+        fm_nb = nb;
+    }
+    // the forward in FP64, energy_calc not needed
+    for (int attempt = 0;; ++attempt) {
+        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+        queue_evaluation(true, false, false);
+        k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+        launches += 2;
+        BCUDA(cudaStreamSynchronize(stream), "force matching");
+        int ov = take_overflow();
+        if (ov < 0) return set_last_error(MOLDY_ERR_CUDA, "compact list re-allocation failed");
+        if (ov == 0) break;
+        if (attempt >= 2) return set_last_error(MOLDY_ERR_CAPACITY, "compact list keeps overflowing");
+    }
+    cudaStream_t s = stream;
+    k_fm_loss<<<nsys, kCgThreads, 0, s>>>(sys, f, fm_fref, fm_sref, sysout, sorted, wf, ws, fm_gF, fm_gS, fm_loss);
+    BCUDA(cudaMemsetAsync(fm_grads, 0, 6 * (size_t)nb * sizeof(double), s), "table gradients");
+    TileArgs a;
+    a.sys = sys; a.cell_sys = cell_sys; a.cell_start = cell_start; a.sorted = sorted;
+    a.spos = spos; a.sfp = sfp; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
+    const size_t smem_r = 2 * (size_t)nbr * sizeof(double), smem_e = (size_t)nb * sizeof(double);
+    BCUDA(cudaFuncSetAttribute(k_fm_pairs_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r), "smem");
+    BCUDA(cudaFuncSetAttribute(k_fm_atoms, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_e), "smem");
+    BCUDA(cudaFuncSetAttribute(k_fm_pairs_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_r / 2)),
+          "smem");
+    // histogram kernels: two blocks per SM, so each flush serves many atoms
+    const int g = std::min(grid_blocks(ntot, 256), 2 * nsm);
+    // vee and emb get no gradient: the loss holds no energy
+    double *gdv = fm_grads + nb, *gp = fm_grads + 2 * nb, *gdp = fm_grads + 3 * nb, *gde = fm_grads + 5 * nb;
+    k_fm_pairs_a<<<g, 256, smem_r, s>>>(a, tab, ntot, pair_cap, alist, pcnt, atom_sys, fm_gF, fm_gS, fm_mu, gdv, gdp,
+                                       nbr);
+    k_fm_atoms<<<g, 256, smem_e, s>>>(tab, ntot, sorted, rho, fm_mu, fm_nu, gde);
+    k_fm_pairs_c<<<g, 256, smem_r / 2, s>>>(a, tab, ntot, pair_cap, alist, pcnt, atom_sys, fm_nu, gp, nbr);
+    launches += 4;
+    BCUDA(cudaGetLastError(), "force matching launch");
+    if (loss) BCUDA(cudaMemcpyAsync(loss, fm_loss, (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost, s), "loss");
+    if (grads)
+        BCUDA(cudaMemcpyAsync(grads, fm_grads, 6 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, s), "grads");
+    BCUDA(cudaStreamSynchronize(s), "force matching");
+    return MOLDY_OK;
+}
+
+// The four launches of one evaluation of every system, timed with CUDA
+// events on the batch's stream: the list check (k_prepare), the tile screen,
+// the density pass and the force pass, in ms; rebuild = 1 rebuilds every
+// list first.  The per-system reduction is not included.
+int BatchEngine::kernel_times(int rebuild, double *ms4) {
+    BCHECK(ready());
+    cudaEvent_t ev[5];
+    for (auto &e : ev) BCUDA(cudaEventCreate(&e), "event");
+    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, rebuild ? 1 : 0);
+    queue_evaluation(true, mixed, ecalc, ev);
+    k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+    launches += 2;
+    BCUDA(cudaStreamSynchronize(stream), "kernel times");
+    for (int k = 0; k < 4; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        if (ms4) ms4[k] = ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (take_overflow() != 0) return set_last_error(MOLDY_ERR_CAPACITY, "compact rows grew; time again");
     return MOLDY_OK;
 }
 
@@ -1303,7 +1695,7 @@ int BatchEngine::quench(int maxfn, int criterion, double fmax, double *out8) {
         BCUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
         // FP64 passes: the line search compares energies that differ in the
         // seventh digit, below the rounding of FP32 distances
-        queue_evaluation(false, false);
+        queue_evaluation(false, false, true);
         cudaMemsetAsync(n_active, 0, sizeof(int), s);
         k_cg<<<nsys, kCgThreads, 0, s>>>(sys, cg, v, f, en_calc, press, maxfn, criterion, fmax, n_active,
                                          cg_order);
@@ -1472,6 +1864,33 @@ int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged) {
         return moldy::set_last_error(MOLDY_ERR_INVALID, "staged candidates out of range");
     h->e->lph = lanes;
     h->e->cap = staged;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_autotune(moldy_batch *h, int32_t nreps, double *times_ms, int32_t *chosen) {
+    BGUARD(h);
+    BTRY(h->e->autotune(nreps, times_ms, chosen));
+}
+
+int moldy_gpu_batch_set_references(moldy_batch *h, const double *fref_xyz, const double *sref) {
+    BGUARD(h);
+    BTRY(h->e->set_references(fref_xyz, sref));
+}
+
+int moldy_gpu_batch_force_matching(moldy_batch *h, double w_force, double w_stress, double *loss,
+                                   double *table_grads) {
+    BGUARD(h);
+    BTRY(h->e->force_matching(w_force, w_stress, loss, table_grads));
+}
+
+int moldy_gpu_batch_kernel_times(moldy_batch *h, int32_t rebuild, double *ms4) {
+    BGUARD(h);
+    BTRY(h->e->kernel_times(rebuild, ms4));
+}
+
+int moldy_gpu_batch_set_energy_calc(moldy_batch *h, int32_t enable) {
+    BGUARD(h);
+    h->e->ecalc = enable != 0;
     return MOLDY_OK;
 }
 

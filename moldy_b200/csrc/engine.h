@@ -34,8 +34,10 @@ struct DeviceState {
     int32_t *ic_new = nullptr, *arr_count = nullptr, *arr_start = nullptr, *arr_list = nullptr;
     int32_t *work = nullptr, *new_count = nullptr, *new_start = nullptr, *cell_atoms2 = nullptr;
     // neighbour list (neighbourlist_m), entry-major: entry k of atom i at
-    // nlist[k*nm + i], 0-based atom ids
+    // nlist[k*nm + i], 0-based atom ids; rlist/numr hold each atom's reverse
+    // half row (the atoms j with i in row(j)), written by the same build
     int32_t *nlist = nullptr, *numn = nullptr;
+    int32_t *rlist = nullptr, *numr = nullptr;
     // scratch of the structure analysis (rdf.cu), grown on demand
     void *rdf = nullptr;
     size_t rdf_bytes = 0;
@@ -51,12 +53,10 @@ struct DeviceState {
     int32_t *alist = nullptr, *pair_cnt = nullptr;
     // outer FULL list: the half-list pairs within r_out = r_cut + outer skin
     // when built, entered in both rows (bit 31 on the owner's copy),
-    // entry-major; row of atom i: own entries in slots 0 .. out_own[i]-1,
-    // reverse entries from the last slot down (out_rev[i] of them); xout holds
-    // the positions at build time
-    // (out_rev counts the reverse entries during a build and is zero
-    // otherwise; out_nrev keeps the count after it)
-    int32_t *olist = nullptr, *out_own = nullptr, *out_rev = nullptr, *out_nrev = nullptr;
+    // entry-major; row of atom i: its own entries (half-list order), then its
+    // reverse entries (reverse-row order), out_cnt[i] in all; xout holds the
+    // positions at build time
+    int32_t *olist = nullptr, *out_cnt = nullptr;
     int4 *xout = nullptr;                  // fixed-point (posq) snapshot
     // intermediate FULL list: the outer-list pairs within r_mid = r_cut + skin
     // when built, entry-major, mid_cnt[i] entries from slot 0 (bit 31 kept);
@@ -77,7 +77,8 @@ struct DeviceState {
     int32_t *flags = nullptr;     // [0] neighbour overflow, [1] relink inconsistency,
                                   // [2] overflow atom, [3] active-list overflow, [4] its count,
                                   // [5] intermediate-row overflow, [6] its count,
-                                  // [8] outer-row overflow, [9] its count
+                                  // [8] outer-row overflow, [9] its count,
+                                  // [10] reverse half-row overflow, [11] its count
     BoxState *box = nullptr;
     int32_t *scan_tmp = nullptr;
     // adjoint (allocated on first use): full tables and their gradients

@@ -23,17 +23,19 @@
 //             then embed and F'(rho) into pos2.w / posq2.w.  (The kinetic
 //             moment of kinten is taken by the drift kernel, or k_kinetic
 //             outside MD.)
-//  k_forces   f_i = sum_j dx_ij fp_ij over the compact row; energy and virial
-//             take half of every directed pair; the velocity-Verlet second
-//             half (src/quench_m.F90:606-622) is applied in the epilogue.
+//  k_forces   f_i = sum_j dx_ij fp_ij over the compact row; the pair energy
+//             and the virial take each pair once, from the copy in its
+//             owner's row (bit 31); the velocity-Verlet second half
+//             (src/quench_m.F90:606-622) is applied in the epilogue.
 //
 // Entries carry the pair's direction in the reference's half list in bit 31
 // (set: j is in i's own row), which the per-atom stress of the reference
 // (own rows only) needs.  MIXED = true runs distances, tables and pair forces
 // in FP32 from 32-bit fixed-point positions (whose integer differences are
-// the minimum image) and keeps rho, F, F', the forces and every sum over atoms
-// in FP64.
-#include <climits>
+// the minimum image) and keeps rho, F, F', the forces, the energy, the virial
+// and every other sum in FP64: each pair's FP32 terms are converted once and
+// accumulated in FP64.
+#include <type_traits>
 
 #include "engine.h"
 
@@ -267,8 +269,34 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
 }
 
 // --------------------------------------------------------------- forces --
-// f_i = sum dx fp over the compact row; pe and the virial moment
-// D = sum d d^T fp / 2 (tp = B0 D); mode 1 adds the velocity-Verlet second half
+// v[1..6] += s * sym(a (x) b) in the order xx, yy, zz, xy, xz, yz
+__device__ __forceinline__ void add_sym(double *v, double ax, double ay, double az, double bx, double by,
+                                        double bz, double s) {
+    v[1] += s * (ax * bx);
+    v[2] += s * (ay * by);
+    v[3] += s * (az * bz);
+    v[4] += (0.5 * s) * (ax * by + ay * bx);
+    v[5] += (0.5 * s) * (ax * bz + az * bx);
+    v[6] += (0.5 * s) * (ay * bz + az * by);
+}
+
+// f_i = sum_j g_ij over the compact row, g_ij = d_ij fp_ij; pe and the
+// virial moment D = sum over pairs d d^T fp (tp = B0 D, pairs with
+// m_i + m_j <= 0.1 left out, src/dynamics_m.F90:287); mode 1 adds the
+// velocity-Verlet second half.
+//
+// D is formed from per-atom FP64 quantities instead of a per-pair sum: with
+// d_ij = x_i - x_j - m_ij (m_ij the periodic image the minimum-image
+// convention picks) and g_ji = -g_ij,
+//   sum_pairs d_ij (x) g_ij = sum_i x_i (x) f_i - sum_pairs m_ij (x) g_ij,
+// and D is symmetric, so sym(x_i (x) f_i) is accumulated per atom and
+// sym(m_ij (x) g_ij) / 2 subtracted on both ends of the pairs that cross a
+// periodic boundary (a few percent); a pair the mass filter leaves out has
+// its whole sym((x_i - x_j) (x) g_ij) / 2 removed the same way.  The two
+// ends compute g_ij bit for bit with opposite signs, so this is the pair sum
+// up to FP64 rounding of the per-atom terms, and it needs no per-pair
+// conversion to FP64 in the mixed pass.  The pair energy is summed from the
+// copy in the owner's row.
 template <bool MIXED, bool EXACT, int B, bool PF, bool STRESS, int MINB>
 __global__ void __launch_bounds__(256, MINB)
 k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__restrict__ posq2,
@@ -278,11 +306,28 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
          double *__restrict__ f, double *__restrict__ x1, double *__restrict__ x2,
          double *__restrict__ stress, double *__restrict__ partials, int mode) {
     __shared__ double sb[9], stg[9];
+    __shared__ int slim[3];
     if (threadIdx.x < 9) {
         sb[threadIdx.x] = box->b0[threadIdx.x];
         stg[threadIdx.x] = box->tgid[threadIdx.x];
     }
     __syncthreads();
+    if (MIXED && threadIdx.x == 0) {
+        // a pair inside the cut spans at most M_d = rcull |row d of B0^-1|
+        // box lengths in direction d; an atom whose fixed-point coordinates
+        // all lie within 2^31 - M_d of zero has no pair whose 32-bit
+        // difference wraps (crosses a periodic boundary)
+        double bi[9];
+        const bool ok = mat_invert(sb, bi);
+        for (int d = 0; d < 3; ++d) {
+            const double rn = sqrt(MAT(bi, d + 1, 1) * MAT(bi, d + 1, 1) + MAT(bi, d + 1, 2) * MAT(bi, d + 1, 2) +
+                                   MAT(bi, d + 1, 3) * MAT(bi, d + 1, 3));
+            const double m = sqrt(t.rcull2) * rn * (1.0 + 1e-6) * kFixScale + 4.0;
+            slim[d] = (ok && m < 2147483000.0) ? (int)(2147483647.0 - m) : -1;
+        }
+    }
+    __syncthreads();
+    const int limx = slim[0], limy = slim[1], limz = slim[2];
     double b[9];
     float bs[9];   // B0 in A per fixed-point unit (mixed)
 #pragma unroll
@@ -311,13 +356,18 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
         double fxa = 0.0, fya = 0.0, fza = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
         if constexpr (MIXED) {
             // fixed-point separations, FP32 geometry, tables and pair forces;
-            // forces summed in FP64, the atom's energy and virial moments in
-            // FP32 over its row and in FP64 over atoms
+            // forces, pair energy and virial accumulate in FP64
             const int4 qa = posq2[a];
             const float fa = __int_as_float(qa.w);
-            double gx = 0.0, gy = 0.0, gz = 0.0;   // sum of d fp, fixed-point units
-            float ve = 0.f, w0 = 0.f, w1 = 0.f, w2 = 0.f, w3 = 0.f, w4 = 0.f, w5 = 0.f;
+            double gx = 0.0, gy = 0.0, gz = 0.0;   // sum of g = d fp, fixed-point units
             float tx = 0.f, ty = 0.f, tz = 0.f;
+            // CORR: the pairs that wrap or that the mass filter leaves out are
+            // corrected; a warp takes that path when one of its atoms lies near
+            // a face (limits above) or has m <= 0.1
+            const bool slow = !(ma > 0.1) || qa.x > limx || qa.x < -limx || qa.y > limy || qa.y < -limy ||
+                              qa.z > limz || qa.z < -limz;
+            auto row = [&](auto corr) {
+            constexpr bool CORR = decltype(corr)::value;
             for (int e0 = 0; e0 < ne; e0 += B) {
                 int ee[B];
 #pragma unroll
@@ -329,29 +379,52 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
                 for (int u = 0; u < B; ++u) {
                     if (ee[u] == -1) continue;
                     const int j = ee[u] & kIdMask;
-                    float rx, ry, rz, dx, dy, dz;
-                    const float r2 = fix_sep(bs, qa, qq[u], rx, ry, rz, dx, dy, dz);
+                    const int4 qj = qq[u];
+                    // 32-bit differences: the minimum image (wrapping past half a box)
+                    const int32_t ex = (int32_t)((uint32_t)qa.x - (uint32_t)qj.x);
+                    const int32_t ey = (int32_t)((uint32_t)qa.y - (uint32_t)qj.y);
+                    const int32_t ez = (int32_t)((uint32_t)qa.z - (uint32_t)qj.z);
+                    const float dx = fix_to_float(ex), dy = fix_to_float(ey), dz = fix_to_float(ez);
+                    const float rx = fmaf(bs[6], dz, fmaf(bs[3], dy, bs[0] * dx));
+                    const float ry = fmaf(bs[7], dz, fmaf(bs[4], dy, bs[1] * dx));
+                    const float rz = fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx));
+                    const float r2 = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
                     const float rr = rsqrtf(r2);
                     const float4 tv = lookup_r4f(t, r2 * rr);    // vee, dvee, phi, dphi
-                    const float fp = -(tv.y + tv.w * (fa + __int_as_float(qq[u].w))) * rr;
+                    const float fp = -(tv.y + tv.w * (fa + __int_as_float(qj.w))) * rr;
                     const float dfx = dx * fp, dfy = dy * fp, dfz = dz * fp;
                     gx += (double)dfx; gy += (double)dfy; gz += (double)dfz;
-                    ve += tv.x;
-                    if (ma > 0.1 || ma + mass[j] > 0.1) {
-                        w0 = fmaf(dx, dfx, w0); w1 = fmaf(dy, dfy, w1); w2 = fmaf(dz, dfz, w2);
-                        w3 = fmaf(dx, dfy, w3); w4 = fmaf(dx, dfz, w4); w5 = fmaf(dy, dfz, w5);
+                    if (ee[u] & kOwnBit) {   // the owner's copy carries the pair energy
+                        v[0] += (double)tv.x;
+                        if (STRESS) { tx = fmaf(rx, fp, tx); ty = fmaf(ry, fp, ty); tz = fmaf(rz, fp, tz); }
                     }
-                    if (STRESS && (ee[u] & kOwnBit)) { tx = fmaf(rx, fp, tx); ty = fmaf(ry, fp, ty); tz = fmaf(rz, fp, tz); }
+                    if constexpr (CORR) {
+                        // sign bit set: that difference wrapped (a periodic image, m = +-1)
+                        const int32_t wx = (qa.x ^ qj.x) & (qa.x ^ ex), wy = (qa.y ^ qj.y) & (qa.y ^ ey),
+                                      wz = (qa.z ^ qj.z) & (qa.z ^ ez);
+                        const bool excluded = !(ma > 0.1 || ma + mass[j] > 0.1);
+                        if ((wx | wy | wz) < 0 || excluded) {
+                            // c = m 2^32 (the image), or q_a - q_j exactly when excluded
+                            double cx = wx < 0 ? (qa.x >= 0 ? kFixScale : -kFixScale) : 0.0;
+                            double cy = wy < 0 ? (qa.y >= 0 ? kFixScale : -kFixScale) : 0.0;
+                            double cz = wz < 0 ? (qa.z >= 0 ? kFixScale : -kFixScale) : 0.0;
+                            if (excluded) { cx += (double)ex; cy += (double)ey; cz += (double)ez; }
+                            add_sym(v, cx, cy, cz, (double)dfx, (double)dfy, (double)dfz, -0.5);
+                        }
+                    }
                 }
             }
+            };
+            if (__any_sync(__activemask(), slow)) row(std::true_type{});
+            else row(std::false_type{});
+            add_sym(v, (double)qa.x, (double)qa.y, (double)qa.z, gx, gy, gz, 1.0);
             fxa = gx * kFixUnit; fya = gy * kFixUnit; fza = gz * kFixUnit;
-            const double u2 = kFixUnit * kFixUnit;
-            v[0] += (double)ve;
-            v[1] += (double)w0 * u2; v[2] += (double)w1 * u2; v[3] += (double)w2 * u2;
-            v[4] += (double)w3 * u2; v[5] += (double)w4 * u2; v[6] += (double)w5 * u2;
             sx = (double)tx; sy = (double)ty; sz = (double)tz;
         } else {
             const double4 pa = pos2[a];
+            // periodic directions of min_image: all for ivol 0, 1, 4; x and y for 2; z for 5
+            const bool pxy = p.ivol == 0 || p.ivol == 1 || p.ivol == 4 || p.ivol == 2;
+            const bool pz = p.ivol == 0 || p.ivol == 1 || p.ivol == 4 || p.ivol == 5;
             for (int e0 = 0; e0 < ne; e0 += B) {
                 int ee[B];
 #pragma unroll
@@ -364,8 +437,10 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
                     if (ee[u] == -1) continue;
                     const int j = ee[u] & kIdMask;
                     const double4 q = qq[u];
-                    double dx = pa.x - q.x, dy = pa.y - q.y, dz = pa.z - q.z;
-                    min_image(p.ivol, dx, dy, dz);
+                    // the minimum image as min_image takes it, keeping the image m
+                    const double ux = pa.x - q.x, uy = pa.y - q.y, uz = pa.z - q.z;
+                    const double mx = pxy ? round(ux) : 0.0, my = pxy ? round(uy) : 0.0, mz = pz ? round(uz) : 0.0;
+                    const double dx = __dsub_rn(ux, mx), dy = __dsub_rn(uy, my), dz = __dsub_rn(uz, mz);
                     const double rx = b[0] * dx + b[3] * dy + b[6] * dz;
                     const double ry = b[1] * dx + b[4] * dy + b[7] * dz;
                     const double rz = b[2] * dx + b[5] * dy + b[8] * dz;
@@ -373,15 +448,21 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
                     const double rr = 1.0 / r;
                     const double4 tv = EXACT ? pair_funcs(t, r) : lookup_r4(t, r);    // vee, dvee, phi, dphi
                     const double fp = -tv.y * rr - (tv.w * pa.w + tv.w * q.w) * rr;
-                    fxa += dx * fp; fya += dy * fp; fza += dz * fp;
-                    v[0] += tv.x;
-                    if (ma > 0.1 || ma + mass[j] > 0.1) {
-                        v[1] += dx * dx * fp; v[2] += dy * dy * fp; v[3] += dz * dz * fp;
-                        v[4] += dx * dy * fp; v[5] += dx * dz * fp; v[6] += dy * dz * fp;
+                    const double gxp = dx * fp, gyp = dy * fp, gzp = dz * fp;
+                    fxa += gxp; fya += gyp; fza += gzp;
+                    if (ee[u] & kOwnBit) {   // the owner's copy carries the pair energy
+                        v[0] += tv.x;
+                        if (STRESS) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
                     }
-                    if (STRESS && (ee[u] & kOwnBit)) { sx += rx * fp; sy += ry * fp; sz += rz * fp; }
+                    const bool excluded = !(ma > 0.1 || ma + mass[j] > 0.1);
+                    if (mx != 0.0 || my != 0.0 || mz != 0.0 || excluded) {
+                        // c = m, or x_a - x_j when excluded (ux = dx + mx exactly)
+                        add_sym(v, excluded ? ux : mx, excluded ? uy : my, excluded ? uz : mz, gxp, gyp, gzp,
+                                -0.5);
+                    }
                 }
             }
+            add_sym(v, pa.x, pa.y, pa.z, fxa, fya, fza, 1.0);
         }
         f[a] = fxa; f[nm + a] = fya; f[2 * nm + a] = fza;
         if (STRESS) { stress[a] = sx; stress[nm + a] = sy; stress[2 * nm + a] = sz; }
@@ -407,9 +488,11 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
             x1[a] = hx + wx; x1[nm + a] = hy + wy; x1[2 * nm + a] = hz + wz;
         }
     }
-    // every directed pair carries half of the pair energy and virial
+    if (MIXED) {   // the virial moments were summed in fixed-point units^2
 #pragma unroll
-    for (int k = 0; k < 7; ++k) v[k] *= 0.5;
+        for (int k = 1; k < 7; ++k) v[k] *= kFixUnit * kFixUnit;
+    }
+    // v[1..6] is D; every directed pair entered half of it
     block_partials<7>(v, partials, 0);
 }
 
@@ -428,13 +511,14 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
 // The intermediate list is filtered from the outer list (half-list pairs
 // within r_out = r_cut + outer skin, both directions), which k_mid_decide has
 // rebuilt from the half list whenever the displacements since its own build
-// could bring an unlisted pair within r_mid.  The outer build enters every
-// kept half-list pair in both rows: the owner writes its own entries from the
-// first slot (flagged in bit 31); the partner's copy goes from the last slot
-// down through a returned integer atomic on out_rev (zero before each build);
-// k_out_finish then sorts each reverse segment.  The intermediate build writes
-// each atom's row from its own outer row alone, with no atomics.  Each kernel
-// returns at once when k_mid_decide asked for no build.
+// could bring an unlisted pair within r_mid.  The outer build walks, per atom,
+// its own half-list row and its reverse half row (the atoms whose rows hold
+// it, written by the half-list build) and keeps the pairs within r_out: own
+// entries first (flagged in bit 31, in half-list order), then the reverse
+// ones in reverse-row order.  Each atom writes only its own row, so there are
+// no atomics and every row is the same from run to run.  The intermediate
+// build filters each atom's outer row the same way.  Each kernel returns at
+// once when k_mid_decide asked for no build.
 
 // FP32 keep radius^2 of a list of radius r: r plus twice the FP32 distance
 // error bound, or every pair when the box is too small for the FP32 screen
@@ -443,13 +527,48 @@ __device__ float keep_radius2(const double *sb, double r) {
     return screen_radius2(sb, r * r) > 1e37f ? 3.0e38f : keep * keep;
 }
 
+// Appends to atom a's row (entries kept in [cnt, cap)) the entries of one
+// source row (n entries, entry-major with stride nm) whose FP32 distance is
+// within keep2; own = bit 31 to set on the kept entries.
+template <bool FIX, int B>
+__device__ __forceinline__ int filter_row(const Params &p, const int32_t *__restrict__ src, int n, int a,
+                                          const double4 &pa, const int4 &qa, const double4 *__restrict__ pos,
+                                          const int4 *__restrict__ posq, const float *bf, float keep2,
+                                          int32_t own, int32_t *__restrict__ dst, int cap, int cnt) {
+    const size_t stride = (size_t)p.nm;
+    for (int k0 = 0; k0 < n; k0 += B) {
+        int ee[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) ee[u] = (k0 + u < n) ? __ldg(&src[(size_t)(k0 + u) * stride + a]) : -1;
+        double4 qq[FIX ? 1 : B];
+        int4 qi[FIX ? B : 1];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int j = ee[u] != -1 ? (ee[u] & kIdMask) : a;
+            if (FIX) qi[u] = __ldg(&posq[j]);
+            else qq[u] = ldg4(&pos[j]);
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            if (ee[u] == -1) continue;
+            float rx, ry, rz;
+            const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
+                                 : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
+            if (!(r2 <= keep2)) continue;
+            if (cnt < cap) dst[(size_t)cnt * stride + a] = ee[u] | own;
+            ++cnt;
+        }
+    }
+    return cnt;
+}
+
 template <bool FIX>
 __global__ void __launch_bounds__(256)
 k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
             const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
-            const int32_t *__restrict__ numn, int32_t *__restrict__ olist,
-            int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, int4 *__restrict__ xout) {
-    constexpr int B = 8;
+            const int32_t *__restrict__ numn, const int32_t *__restrict__ rlist,
+            const int32_t *__restrict__ numr, int32_t *__restrict__ olist,
+            int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, int32_t *__restrict__ flags) {
     __shared__ double sb[9];
     __shared__ float skeep2;
     __shared__ int sneed;
@@ -464,129 +583,29 @@ k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *
     for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
     const float keep2 = skeep2;
     const int nm = p.nm, cap = p.out_cap;
-    const size_t stride = (size_t)nm;
+    int over = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const int n = numn[a];
-        const int32_t *col = nlist + a;
         const double4 pa = pos[a];
         const int4 qa = posq[a];
-        int own = 0;
-        for (int k0 = 0; k0 < n; k0 += B) {
-            int jj[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) jj[u] = (k0 + u < n) ? __ldg(&col[(size_t)(k0 + u) * stride]) : -1;
-            double4 qq[FIX ? 1 : B];
-            int4 qi[FIX ? B : 1];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                if (FIX) qi[u] = __ldg(&posq[jj[u] >= 0 ? jj[u] : a]);
-                else qq[u] = ldg4(&pos[jj[u] >= 0 ? jj[u] : a]);
-            }
-            int slot[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                slot[u] = -1;
-                if (jj[u] < 0) continue;
-                float rx, ry, rz;
-                const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
-                                     : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
-                if (!(r2 <= keep2)) { jj[u] = -1; continue; }
-                if (own < cap) olist[(size_t)own * stride + a] = jj[u] | kOwnBit;
-                ++own;
-                slot[u] = atomicAdd(&out_rev[jj[u]], 1);   // issued together, used below
-            }
-#pragma unroll
-            for (int u = 0; u < B; ++u)
-                if (slot[u] >= 0 && slot[u] < cap) olist[(size_t)(cap - 1 - slot[u]) * stride + jj[u]] = a;
-        }
-        out_own[a] = own;
+        int cnt = filter_row<FIX, 8>(p, nlist, numn[a], a, pa, qa, pos, posq, bf, keep2, kOwnBit, olist, cap, 0);
+        cnt = filter_row<FIX, 8>(p, rlist, numr[a], a, pa, qa, pos, posq, bf, keep2, 0, olist, cap, cnt);
+        out_cnt[a] = cnt;
+        if (cnt > cap) over = max(over, cnt);
         xout[a] = qa;
     }
-}
-
-// Ascending sort of a register array by a bitonic network (all indices known
-// at compile time, so the array stays in registers)
-constexpr int kSortNet = 32;
-template <int N>
-__device__ __forceinline__ void sort_net(int (&v)[N]) {
-#pragma unroll
-    for (int k = 2; k <= N; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const int lo = min(v[i], v[l]), hi = max(v[i], v[l]);
-                    if ((i & k) == 0) { v[i] = lo; v[l] = hi; }
-                    else { v[i] = hi; v[l] = lo; }
-                }
-            }
-}
-
-// After an outer build: each atom's reverse entries, placed in the order the
-// atomics were served, are sorted by atom index (its own entries are in
-// half-list order), so the lists below and the sums over their rows are the
-// same run after run; the reverse count moves to out_nrev and out_rev is
-// zeroed for the next build.
-__global__ void __launch_bounds__(256, 4)
-k_out_finish(const BoxState *__restrict__ box, int nm, int ocap, int32_t *__restrict__ olist,
-             const int32_t *__restrict__ out_own, int32_t *__restrict__ out_rev, int32_t *__restrict__ out_nrev) {
-    if (!box->out_rebuild) return;
-    const size_t stride = (size_t)nm;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const int n_own = out_own[a], n_rev = out_rev[a];
-        out_rev[a] = 0;
-        out_nrev[a] = n_rev;
-        const int nt = n_own + n_rev;
-        const int n = nt < ocap ? nt : ocap;
-        const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
-        const int nr = n - n_own;
-        if (nr <= 1) continue;
-        if (nr <= 16) {
-            int rv[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k)
-                rv[k] = k < nr ? olist[(size_t)(rev_base - n_own - k) * stride + a] : INT_MAX;
-            sort_net(rv);
-#pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if (k < nr) olist[(size_t)(rev_base - n_own - k) * stride + a] = rv[k];
-        } else if (nr <= kSortNet) {
-            int rv[kSortNet];
-#pragma unroll
-            for (int k = 0; k < kSortNet; ++k)
-                rv[k] = k < nr ? olist[(size_t)(rev_base - n_own - k) * stride + a] : INT_MAX;
-            sort_net(rv);
-#pragma unroll
-            for (int k = 0; k < kSortNet; ++k)
-                if (k < nr) olist[(size_t)(rev_base - n_own - k) * stride + a] = rv[k];
-        } else {
-            for (int k = n_own + 1; k < n; ++k) {   // insertion sort in place
-                const int e = olist[(size_t)(rev_base - k) * stride + a];
-                int m = k - 1;
-                for (; m >= n_own; --m) {
-                    const int f = olist[(size_t)(rev_base - m) * stride + a];
-                    if (f <= e) break;
-                    olist[(size_t)(rev_base - m - 1) * stride + a] = f;
-                }
-                olist[(size_t)(rev_base - m - 1) * stride + a] = e;
-            }
-        }
-    }
+    if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
 }
 
 // The intermediate rows from the outer rows; also the largest displacement
-// since the outer build (outdisp2) for the next decision, and the overflow of
-// an outer row (flags 8, 9).  An intermediate row longer than mid_cap keeps
-// its true count in mid_cnt; the screening pass reports it.
+// since the outer build (outdisp2) for the next decision.  An intermediate
+// row longer than mid_cap keeps its true count in mid_cnt; the screening pass
+// reports it.
 template <bool FIX>
 __global__ void __launch_bounds__(256)
 k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
-            BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_own,
-            const int32_t *__restrict__ out_nrev, const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
-            int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
-    constexpr int B = 8;
+            BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_cnt,
+            const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
+            int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild) {
     __shared__ double sb[9];
     __shared__ float skeep2;
     __shared__ int sneed;
@@ -601,48 +620,16 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
     for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
     const float keep2 = skeep2;
     const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
-    const size_t stride = (size_t)nm;
     float bq[9];   // B0 per fixed-point unit, for the displacement
 #pragma unroll
     for (int k = 0; k < 9; ++k) bq[k] = (float)(sb[k] * kFixUnit);
     float d2 = 0.f;
-    int over = 0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const int n_own = out_own[a];
-        const int nt = n_own + out_nrev[a];
-        if (nt > ocap) over = max(over, nt);
+        const int nt = out_cnt[a];
         const int n = nt < ocap ? nt : ocap;
-        const int rev_base = ocap - 1 + n_own;   // entry k >= n_own sits in slot rev_base - k
         const double4 pa = pos[a];
         const int4 qa = posq[a];
-        int cnt = 0;
-        for (int k0 = 0; k0 < n; k0 += B) {
-            int ee[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const int k = k0 + u;
-                ee[u] = k < n ? __ldg(&olist[(size_t)(k < n_own ? k : rev_base - k) * stride + a]) : -1;
-            }
-            double4 qq[FIX ? 1 : B];
-            int4 qi[FIX ? B : 1];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const int j = ee[u] != -1 ? (ee[u] & kIdMask) : a;
-                if (FIX) qi[u] = __ldg(&posq[j]);
-                else qq[u] = ldg4(&pos[j]);
-            }
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                if (ee[u] == -1) continue;
-                float rx, ry, rz;
-                const float r2 = FIX ? fix_sep(bf, qa, qi[u], rx, ry, rz)
-                                     : sep2_f32(bf, p.ivol, pa.x - qq[u].x, pa.y - qq[u].y, pa.z - qq[u].z);
-                if (!(r2 <= keep2)) continue;
-                if (cnt < mcap) mlist[(size_t)cnt * stride + a] = ee[u];
-                ++cnt;
-            }
-        }
-        mid_cnt[a] = cnt;
+        mid_cnt[a] = filter_row<FIX, 8>(p, olist, n, a, pa, qa, pos, posq, bf, keep2, 0, mlist, mcap, 0);
         xbuild[a] = qa;
         d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
     }
@@ -657,7 +644,6 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
         atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong((double)m));
     }
-    if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
 }
 
 // fixed-point separations in a fully periodic box, FP64 differences otherwise;
@@ -667,20 +653,18 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout,
     const bool fix = p.ivol == 0 || p.ivol == 1 || p.ivol == 4;
     int no = grid_blocks(p.nm, 256);
     if (fix)
-        LAUNCH_WAVE(k_out_build<true>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
-                    d.out_rev, d.xout);
+        LAUNCH_WAVE(k_out_build<true>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist, d.numr,
+                    d.olist, d.out_cnt, d.xout, d.flags);
     else
-        LAUNCH_WAVE(k_out_build<false>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.olist, d.out_own,
-                    d.out_rev, d.xout);
-    int nf = grid_blocks(p.nm, 256);
-    LAUNCH_WAVE(k_out_finish, nf, s, d.box, p.nm, p.out_cap, d.olist, d.out_own, d.out_rev, d.out_nrev);
+        LAUNCH_WAVE(k_out_build<false>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist, d.numr,
+                    d.olist, d.out_cnt, d.xout, d.flags);
     int nb = grid_blocks(p.nm, 256);
     if (fix)
-        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_nrev, d.xout,
-                    d.mlist, d.mid_cnt, d.xbuild, d.flags);
+        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_cnt, d.xout,
+                    d.mlist, d.mid_cnt, d.xbuild);
     else
-        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_own, d.out_nrev, d.xout,
-                    d.mlist, d.mid_cnt, d.xbuild, d.flags);
+        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_cnt, d.xout,
+                    d.mlist, d.mid_cnt, d.xbuild);
 }
 
 // ------------------------------------------------------------ launchers --

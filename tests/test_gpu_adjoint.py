@@ -293,3 +293,61 @@ def test_adjoint_order_and_mode_errors(gpu_lib):
         x.table_gradients(1.0)
     assert ei.value.code == 7
     x.close()
+
+
+def test_batch_force_matching_equals_single_system_path(gpu_lib):
+    """The batched force matching (every configuration in one MoldyBatch: one
+    FP64 evaluation, the loss and the table adjoint on the device) gives the
+    loss and the knot gradient of ForceMatchingKnots (one MoldySystem per
+    configuration size, summed) within 1e-10 and 1e-8 (the pair sets are the
+    same, the summation orders are not), on configurations of uneven size, and
+    matches central differences (h = 1e-6) of its own loss within 1e-6."""
+    from moldy_b200 import MoldyBatch
+    configs = [fm_config(80 + c, n=n, sigma=0.1) for c, n in enumerate((6, 5, 6, 7, 5))]
+    by_size = {}
+    for c, w in enumerate(configs):
+        by_size.setdefault(w.nm, []).append(c)
+    systems = {nm: MoldySystem.from_workload(configs[cs[0]], uselookup=True) for nm, cs in by_size.items()}
+    refs = [None] * len(configs)
+    for nm, cs in by_size.items():
+        for c in cs:
+            w = configs[c]
+            systems[nm].set_state(x0=w.x0, b0=w.b0)
+            _, f0, s0 = gpu_eval(systems[nm], coeffs=FE_FE)
+            refs[c] = (f0 + 1e-3, s0 * 1.01)
+    rng = np.random.default_rng(6)
+    base = {k: np.asarray(getattr(FE_FE, k)) * (1 + 1e-3 * rng.normal(size=len(getattr(FE_FE, k))))
+            for k in adj.KNOT_NAMES}
+    th1 = {k: torch.tensor(v, requires_grad=True) for k, v in base.items()}
+    single = torch.zeros((), dtype=torch.float64)
+    for nm, cs in by_size.items():
+        single = single + adj.force_matching_knots(systems[nm], [(configs[c].x0, configs[c].b0) for c in cs],
+                                                   [refs[c] for c in cs], th1, w_force=0.7, w_stress=2.0)
+    single.backward()
+    for sys_ in systems.values():
+        sys_.close()
+    b = MoldyBatch.from_workloads(configs)
+    b.set_references([f for f, _ in refs], [sg for _, sg in refs])
+    th2 = {k: torch.tensor(v, requires_grad=True) for k, v in base.items()}
+    batched = adj.batch_force_matching_knots(b, th2, w_force=0.7, w_stress=2.0)
+    batched.backward()
+    assert abs(batched.item() - single.item()) <= 1e-10 * abs(single.item())
+    for k in adj.KNOT_NAMES:
+        a, g = th1[k].grad.numpy(), th2[k].grad.numpy()
+        assert np.max(np.abs(a - g)) <= 1e-8 * np.linalg.norm(a), (k, a, g)
+
+    def loss_of(th):
+        return adj.batch_force_matching_knots(b, th, w_force=0.7, w_stress=2.0).item()
+
+    h = 1e-6
+    for name in adj.KNOT_NAMES:
+        g = th2[name].grad.numpy()
+        fd = np.zeros_like(g)
+        for k in range(len(g)):
+            tp = {n: torch.tensor(base[n]) for n in adj.KNOT_NAMES}
+            tm = {n: torch.tensor(base[n]) for n in adj.KNOT_NAMES}
+            tp[name][k] += h
+            tm[name][k] -= h
+            fd[k] = (loss_of(tp) - loss_of(tm)) / (2 * h)
+        assert np.max(np.abs(fd - g)) <= 1e-6 * np.linalg.norm(g), (name, fd, g)
+    b.close()

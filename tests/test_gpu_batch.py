@@ -279,3 +279,32 @@ def test_batch_quench_stays_fp64(gpu_lib):
         b.close()
     for x, y in zip(*out):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_autotune_and_energy_calc_switch(gpu_lib, precision):
+    """moldy_gpu_batch_autotune picks a lanes/gather pair from its sets and
+    changes no result: forces, pe and the virial after it equal, bit for bit,
+    those of the default tiles.  With energy_calc switched off the energy_calc
+    sums read zero and everything else is again bit-identical."""
+    ws = mixed_systems([4, 5, 6, 7, 9, 4, 5], seed=21)
+    b = MoldyBatch.from_workloads(ws)
+    b.set_precision(precision)
+    out0 = b.force()
+    f0 = b.forces()
+    tune = b.autotune(nreps=2)
+    assert tune["chosen"]["lanes"] in (4, 8, 16, 32) and tune["chosen"]["gather"] in (1, 2, 4)
+    assert all(t > 0 for t in tune["lanes_ms"].values()) and all(t > 0 for t in tune["gather_ms"].values())
+    out1 = b.force()
+    assert np.array_equal(b.forces(), f0)
+    for k in ("pe_calc", "pe", "tp", "vol"):
+        assert np.array_equal(out1[k], out0[k]), k
+    b.set_energy_calc(False)
+    out2 = b.force()
+    assert np.array_equal(b.forces(), f0)
+    assert np.all(out2["pe_calc"] == 0.0) and np.all(b.energies()[0] == 0.0)
+    for k in ("pe", "tp", "vol"):
+        assert np.array_equal(out2[k], out0[k]), k
+    b.set_energy_calc(True)
+    assert np.array_equal(b.force()["pe_calc"], out0["pe_calc"])
+    b.close()

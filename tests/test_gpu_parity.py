@@ -68,17 +68,20 @@ def test_strained_box_neighbour_list_exact(oracle_mod, gpu_lib):
     assert np.array_equal(nlo[mask], nlg[mask])
 
 
-def test_neighbour_list_exact_beyond_staging(oracle_mod, gpu_lib):
-    """3^3 link cells over a 2000-atom box: about 74 atoms per cell, so a half
-    stencil holds about 1040 candidates, beyond the 640 the builder stages in
-    shared memory; the rest are read from global memory.  NLIST/NUMN are
-    still identical entry by entry."""
-    w = wl.make_workload(10, sigma=0.1, temperature=0.0, seed=14)
-    w.nlc = (3, 3, 3)
+@pytest.mark.parametrize("n,nlc", [(10, 3), (10, 4), (12, 4)])
+def test_neighbour_list_exact_beyond_staging(oracle_mod, gpu_lib, n, nlc):
+    """Few, crowded link cells: 31 to 74 atoms per cell, so the 27 cells
+    around a home cell hold more than the 640 candidates the builder stages in
+    shared memory (the rest are read from global memory), and home cells of
+    more than 32 atoms take several rounds of lanes; 3 cells per direction use
+    the fixed-point pre-test, 4 the cell-relative one.  NLIST/NUMN are still
+    identical entry by entry."""
+    w = wl.make_workload(n, sigma=0.1, temperature=0.0, seed=14)
+    w.nlc = (nlc, nlc, nlc)
     o, g = _pair(oracle_mod, gpu_lib, w)
     g.linkup()
-    counts = np.bincount(g.linkcells(27)[2] - 1, minlength=27)
-    assert counts.min() * 14 > 640
+    counts = np.bincount(g.linkcells(nlc ** 3)[2] - 1, minlength=nlc ** 3)
+    assert counts.min() * 27 > 640
     assert o.update_neighbourlist() == 0
     g.update_neighbourlist()
     nlo, nno = o.nlist()
