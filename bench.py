@@ -554,7 +554,7 @@ def run_ours(args):
 
 
 # ------------------------------------------------------------------- batch --
-BATCH_METRIC = ("atom-evals/s, 1024 bcc Fe supercells of 128-8192 atoms: force + energy_calc + "
+BATCH_METRIC = ("atom-evals/s, 1024 bcc Fe supercells of 128-8192 atoms: energy + forces + "
                 "virial per system")
 
 
@@ -635,28 +635,20 @@ def run_batch(args):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    # untimed: choose the tile shape (lanes per home atom) on evaluations that
-    # build every list
+    # untimed: the library's tuner picks the tile lanes (on list-building
+    # evaluations) and the gather width (lists current), per precision; the
+    # timed evaluations form the force routine's energy, forces and virial,
+    # energy_calc's exact energies (the quench's) are timed separately
     prec = "fp64" if args.precision == "fp64" else "mixed"
-    b.set_precision(prec)
-    tune = {}
-    for lanes in (4, 8, 16, 32):
-        b.set_tiles(lanes, 256)
-        build_and_force()
-        tune[lanes] = min(build_and_force() for _ in range(3))
-    best = min(tune, key=tune.get)
-    b.set_tiles(best, 256)
-    # untimed: row entries gathered at a time by the per-atom passes, per precision
-    gather_ms, best_gather = {}, {}
+    b.set_energy_calc(False)
+    tunes = {}
     for p in ("fp64", "mixed"):
         b.set_precision(p)
-        for g in (1, 2, 4):
-            b.set_gather(g)
-            b.force()
-            gather_ms[f"{p}/{g}"] = timed(force, 5)
-        best_gather[p] = min((1, 2, 4), key=lambda g: gather_ms[f"{p}/{g}"])
+        tunes[p] = b.autotune(nreps=3)
     b.set_precision(prec)
-    b.set_gather(best_gather[prec])
+    b.set_tiles(tunes[prec]["chosen"]["lanes"], 256)
+    b.set_gather(tunes[prec]["chosen"]["gather"])
+    best_gather = {p: tunes[p]["chosen"]["gather"] for p in tunes}
     for _ in range(max(args.warmup, 3)):
         b.force()
     # evaluations with every list current (the positions do not move between
@@ -674,6 +666,27 @@ def run_batch(args):
     ntot_all = sum(w.nm for w in ws_all)
     value = ntot_all / (ms_max / 1000.0)
     build_ms = max_over_ranks(float(np.median([build_and_force() for _ in range(5)])))
+    # per-kernel times of an evaluation with current lists, and the same
+    # evaluation with energy_calc's energies
+    kt = [b.kernel_times() for _ in range(5)]
+    ktimes = {k: float(np.median([t[k] for t in kt])) for k in kt[0]}
+    # the dominant pass against its algorithmic bytes per atom: the compact
+    # row (4 n + 4), the atom's cell-order record (32) and, density: F' into
+    # cell order plus rho, F, F' (32); forces: its F' (8), F read (8), the
+    # force (24), the force-routine energy (8) and the six virial moments (48)
+    n_row = b.row_entries() / b.ntot
+    bpa = {"density": 4 * n_row + 4 + 32 + 32, "forces": 4 * n_row + 4 + 32 + 8 + 8 + 24 + 8 + 48}
+    dom = max(("density", "forces"), key=lambda k: ktimes[k])
+    peak, peak_kind = load_peaks()
+    achieved = bpa[dom] * b.ntot / (ktimes[dom] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "algorithmic_bytes_per_launch": bpa[dom] * b.ntot, "avg_launch_ms": ktimes[dom]}
+    b.set_energy_calc(True)
+    b.force()
+    ecalc_ms = max_over_ranks(timed(force, min(steps, 50)))
+    b.set_energy_calc(False)
+    b.force()
 
     # the other precision on the same lists, and the mixed path's errors
     # against the FP64 path (real forces, energy_calc energy per atom, stress)
@@ -685,6 +698,7 @@ def run_batch(args):
     b.set_gather(best_gather[other])
     b.force()
     other_ms = max_over_ranks(timed(force, min(steps, 50)))
+    b.set_energy_calc(True)   # the accuracy comparison includes energy_calc's energies
     res = {p_: None for p_ in ("fp64", "mixed")}
     res[other] = snapshot()
     b.set_precision(prec)
@@ -776,16 +790,20 @@ def run_batch(args):
         "dtype": "f32 arithmetic / f64 accumulate" if prec == "mixed" else "f64",
         "data": "synthetic (seeded strained bcc Fe supercells, Gaussian displacements 0.1 A)",
         "config": {"workload": f"{len(ws_all)} bcc Fe supercells, n ~ U{{4..16}}, strain +/-2%",
-                   "atoms": ntot_all, "tile_lanes_per_atom": best, "tile_autotune_ms": tune,
-                   "timed_step": "one evaluation of every system with its list current",
-                   "precision": prec, "gather_tune_ms": gather_ms, "gather": best_gather[prec],
-                   f"{other}_ms_per_step": other_ms,
+                   "atoms": ntot_all, "tile_lanes_per_atom": tunes[prec]["chosen"]["lanes"],
+                   "gather": best_gather[prec], "autotune": tunes,
+                   "timed_step": "one evaluation of every system with its list current: the force "
+                                 "routine's energy, forces and virial (energy_calc off)",
+                   "precision": prec, f"{other}_ms_per_step": other_ms,
+                   "with_energy_calc_ms_per_step": ecalc_ms,
                    "evaluation_with_every_list_built_ms": build_ms,
+                   "kernel_ms": ktimes, "row_entries_per_atom": n_row,
                    "parallelism": f"supercells sharded over {world} rank(s) by atom count",
                    "l2": "per-evaluation working set (positions, cell order, forces, energies, virial) "
                          "> 126 MB L2"},
         "e2e": e2e,
         "quench": quench, "accuracy": accuracy, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+        "roofline": roofline,
     }
     print(json.dumps(line), flush=True)
     return 0

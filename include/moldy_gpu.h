@@ -407,6 +407,9 @@ int moldy_gpu_batch_set_gather(moldy_batch *h, int32_t entries);
 int moldy_gpu_batch_set_skin(moldy_batch *h, double skin);
 /* out2[0]: system list builds so far; out2[1]: system evaluations so far. */
 int moldy_gpu_batch_list_stats(moldy_batch *h, int64_t *out2);
+/* Entries of the compact rows (the pairs within each system's list radius,
+ * both directions) summed over all atoms, as the last evaluation left them. */
+int moldy_gpu_batch_row_entries(moldy_batch *h, int64_t *total);
 /* Kernel launches queued so far by this handle; its cudaStream_t. */
 int moldy_gpu_batch_launches(moldy_batch *h, int64_t *launches);
 int moldy_gpu_batch_get_stream(moldy_batch *h, void **stream);

@@ -135,6 +135,7 @@ SIGNATURES = {
     "moldy_gpu_batch_force_matching": [H, ctypes.c_double, ctypes.c_double, D, D],
     "moldy_gpu_batch_set_gather": [H, ctypes.c_int32],
     "moldy_gpu_batch_list_stats": [H, ctypes.POINTER(ctypes.c_int64)],
+    "moldy_gpu_batch_row_entries": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_get_stream": [H, ctypes.POINTER(ctypes.c_void_p)],
     "moldy_fetm_build_tables": [ctypes.c_int32, D, D, ctypes.c_int32, D, D, ctypes.c_int32,

@@ -215,6 +215,13 @@ class MoldyBatch:
         check(self._L.moldy_gpu_batch_list_stats(self._h, v))
         return {"builds": int(v[0]), "evaluations": int(v[1])}
 
+    def row_entries(self) -> int:
+        """Compact-row entries summed over all atoms (pairs within the list
+        radius, both directions), as the last evaluation left them."""
+        v = ctypes.c_int64(0)
+        check(self._L.moldy_gpu_batch_row_entries(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def launches(self) -> int:
         v = ctypes.c_int64(0)
         check(self._L.moldy_gpu_batch_launches(self._h, ctypes.byref(v)))

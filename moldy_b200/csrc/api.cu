@@ -834,10 +834,6 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
             therm_blocks = kin_blocks;
             therm_rec = thermo ? d.thermo_rec + (size_t)kThermoRec * (k - 1) : nullptr;
         }
-        skip_rho = k < nsteps - 1;   // rho is read only after the last step
-        CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
-        ntcs[k] = ntc_;
-        rbs[k] = rb ? 1 : 0;
         // src/moldin.F90:828-835: scalev once per femtosecond of simulated time,
         // with the mdloop's own constant for one femtosecond
         thermotimer_ = thermotimer_ + prm.deltat;
@@ -846,6 +842,10 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
             thermotimer_ = thermotimer_ - kFemtosecond;
             scalev = nose_ > 0.0;
         }
+        skip_rho = k < nsteps - 1;   // rho is read only after the last step
+        CHECK(queue_force(*this, 1, ntc_, ntcm_, cells_ready_, list_ready_, &rb, stream_));
+        ntcs[k] = ntc_;
+        rbs[k] = rb ? 1 : 0;
         therm_pending = !(scalev || k == nsteps - 1);
         if (!therm_pending)
             LAUNCH(*this, K_THERM, 2, stream_,

@@ -1914,6 +1914,22 @@ int moldy_gpu_batch_set_skin(moldy_batch *h, double skin) {
     BTRY(h->e->set_skin(skin));
 }
 
+int moldy_gpu_batch_row_entries(moldy_batch *h, int64_t *total) {
+    BGUARD(h);
+    if (!total) return moldy::set_last_error(MOLDY_ERR_INVALID, "null output");
+    const int nt = h->e->ntot;
+    std::vector<int32_t> c(nt);
+    cudaError_t e = cudaMemcpy(c.data(), h->e->pcnt, nt * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return moldy::set_last_error(MOLDY_ERR_CUDA, std::string("row entries: ") + cudaGetErrorString(e));
+    }
+    long long t = 0;
+    for (int k = 0; k < nt; ++k) t += std::min(c[k], h->e->pair_cap);
+    *total = (int64_t)t;
+    return MOLDY_OK;
+}
+
 int moldy_gpu_batch_list_stats(moldy_batch *h, int64_t *out2) {
     BGUARD(h);
     if (!out2) return moldy::set_last_error(MOLDY_ERR_INVALID, "null output");

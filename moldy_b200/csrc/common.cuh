@@ -137,17 +137,10 @@ __device__ __forceinline__ int32_t fix32(double x) {
     return __double2loint(fma(x, kFixScale, 6755399441055744.0));
 }
 
-// A 32-bit integer as a float, rounded once to nearest, without the
-// conversion unit: the upper 20 and the lower 12 bits are each made exact
-// floats by adding them to the bit pattern of a power-of-two bias, then joined
-// by one fused multiply-add.
-__device__ __forceinline__ float fix_to_float(int32_t d) {
-    const int32_t hi = d >> 12;                                            // [-2^19, 2^19)
-    const int32_t lo = d & 0xfff;                                          // [0, 4096)
-    const float fhi = __int_as_float(0x4b400000 + hi) - 12582912.0f;      // bias 1.5 * 2^23
-    const float flo = __int_as_float(0x4b000000 + lo) - 8388608.0f;       // bias 2^23
-    return fmaf(fhi, 4096.0f, flo);
-}
+// A 32-bit integer as a float, rounded once to nearest (ties to even): the
+// conversion instruction, whose throughput the pair passes measured to be
+// no limit (about 7 % faster than forming it on the FMA pipe)
+__device__ __forceinline__ float fix_to_float(int32_t d) { return __int2float_rn(d); }
 
 // |B0 (x - x_ref)|^2 from fixed-point coordinates (any box: displacements
 // since a list build are far below half a box, so the 32-bit difference is

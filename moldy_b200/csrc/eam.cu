@@ -359,7 +359,7 @@ void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut
 // to the last bit.  The block partials go to therm_partials; k_mid_decide,
 // which runs next, finishes them.
 template <bool THERM>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)   // the grid is 4 blocks per SM (stream_blocks): one wave
 k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
         const int4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
@@ -394,7 +394,7 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const double ex = x1[a], ey = x1[nm + a], ez = x1[2 * nm + a];
         const double wx = x2[a], wy = x2[nm + a], wz = x2[2 * nm + a];
-        double4 q = pos[a];
+    double4 q = pos[a];
         q.x = q.x + (ex + wx);
         q.y = q.y + (ey + wy);
         q.z = q.z + (ez + wz);

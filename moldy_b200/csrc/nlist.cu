@@ -76,8 +76,7 @@ __device__ double stencil_reach(const double *b, int nlcx, int nlcy, int nlcz) {
 
 // Shared state of one block's candidate tests
 struct NlStage {
-    const int *sj;          // staged atom ids
-    const int4 *sqc;        // staged fixed-point or cell-relative positions
+    const int4 *sqc;        // staged fixed-point or cell-relative positions, atom id in w
     const int *sbase, *sstart;
     const int32_t *cell_atoms;
     const int4 *posq;
@@ -110,7 +109,7 @@ __device__ __forceinline__ bool nl_take(const NlStage &S, int kk, const double4 
     int4 qj = make_int4(0, 0, 0, 0);
     const bool staged = kk < S.staged;
     if (staged) {
-        j = S.sj[kk];
+        j = S.sqc[kk].w;
     } else {
         int s = 0;
         while (S.sbase[s + 1] <= kk) ++s;
@@ -163,10 +162,10 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
               const int32_t *__restrict__ cell_atoms, int32_t *__restrict__ nlist,
               int32_t *__restrict__ numn, int32_t *__restrict__ rlist, int32_t *__restrict__ numr,
               int32_t *__restrict__ flags) {
-    __shared__ int sj[kNlStage];
-    // fixed-point positions (fixed-point form) or cell-relative Cartesian
-    // positions as float4 bits (cell-relative form)
-    __shared__ int4 sqc[PERIODIC ? kNlStage : 1];
+    // per staged candidate: its fixed-point position (fixed-point form) or its
+    // cell-relative Cartesian position as float bits (cell-relative form) in
+    // x, y, z, and its atom id in w
+    __shared__ int4 sqc[kNlStage];
     __shared__ int sbase[28], sstart[27];
     __shared__ double sb[9];
     const int c = blockIdx.x;
@@ -214,13 +213,13 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     for (int k = lane; k < staged; k += 32) {
         int sc = 0;
         while (sbase[sc + 1] <= k) ++sc;
-        sj[k] = cell_atoms[sstart[sc] + (k - sbase[sc])];
+        sqc[k].w = cell_atoms[sstart[sc] + (k - sbase[sc])];
     }
     __syncwarp();
+    if (PERIODIC) {
 #pragma unroll 4
-    for (int k = lane; k < staged; k += 32) {
-        const int j = sj[k];
-        if (PERIODIC) {
+        for (int k = lane; k < staged; k += 32) {
+            const int j = sqc[k].w;
             const int4 qj = posq[j];
             if (rel) {
                 const float dx = __int2float_rn((int32_t)((uint32_t)qj.x - (uint32_t)cen.x));
@@ -228,15 +227,22 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
                 const float dz = __int2float_rn((int32_t)((uint32_t)qj.z - (uint32_t)cen.z));
                 sqc[k] = make_int4(__float_as_int(fmaf(bs[6], dz, fmaf(bs[3], dy, bs[0] * dx))),
                                    __float_as_int(fmaf(bs[7], dz, fmaf(bs[4], dy, bs[1] * dx))),
-                                   __float_as_int(fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx))), 0);
+                                   __float_as_int(fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx))), j);
             } else {
-                sqc[k] = qj;
+                sqc[k] = make_int4(qj.x, qj.y, qj.z, j);
             }
         }
     }
+    // records past the staged candidates, up to the next multiple of 32: far
+    // away, so the chunked walk below needs no bound check
+    if (PERIODIC && rel) {
+        const int pad_end = (staged + 31) & ~31;
+        for (int k = staged + lane; k < pad_end && k < kNlStage; k += 32)
+            sqc[k] = make_int4(__float_as_int(1.0e30f), __float_as_int(1.0e30f), __float_as_int(1.0e30f), -1);
+    }
     __syncwarp();
     NlStage S;
-    S.sj = sj; S.sqc = sqc; S.sbase = sbase; S.sstart = sstart; S.cell_atoms = cell_atoms;
+    S.sqc = sqc; S.sbase = sbase; S.sstart = sstart; S.cell_atoms = cell_atoms;
     S.posq = posq; S.pos = pos; S.bs = bs; S.b = sb; S.staged = staged; S.ivol = p.ivol; S.rnear = p.rnear;
     S.rlo2 = (float)((p.rnear - kNlBand) * (p.rnear - kNlBand));
     S.rhi2 = (float)((p.rnear + kNlBand) * (p.rnear + kNlBand));
@@ -251,45 +257,58 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
         if (PERIODIC && live) qa = q < staged ? sqc[q] : posq[a];
         const bool rel_a = rel && q < staged;
         const float ax = __int_as_float(qa.x), ay = __int_as_float(qa.y), az = __int_as_float(qa.z);
+        // every append below is predicated, with no branch: entry n of a row
+        // sits at n * nm + a (entry-major)
         int nf = 0, nr = 0;
-        int32_t *frow = nlist + a, *rrow = rlist + a;
-        // staged candidates, read by every lane at once
+        const int cap = p.nnbrs;
+        auto append = [&](bool take, bool fwd, int j) {
+            const int n = fwd ? nf : nr;
+            int32_t *base = fwd ? nlist : rlist;
+            if (take && n < cap) base[(size_t)n * nm + a] = j;
+            nf += (take && fwd) ? 1 : 0;
+            nr += (take && !fwd) ? 1 : 0;
+        };
         int kk = 0;
         if (rel && min(L0, q0 + 32) <= staged) {   // cell relative, every live lane's atom staged
-#pragma unroll 4
-            for (; kk < staged; ++kk) {
-                const int4 cq = sqc[kk];
-                const int j = sj[kk];
-                const float rx = ax - __int_as_float(cq.x), ry = ay - __int_as_float(cq.y),
-                            rz = az - __int_as_float(cq.z);
-                const float r2 = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
-                bool take = live && kk != q && r2 < S.rlo2;
-                if (live && kk != q && !take && !(r2 > S.rhi2)) take = nl_exact(pos, sb, p.ivol, p.rnear, pa, j);
-                if (take) {
-                    if (kk > q && kk < fwd_end) {
-                        if (nf < p.nnbrs) frow[(size_t)nf * nm] = j;
-                        ++nf;
-                    } else {
-                        if (nr < p.nnbrs) rrow[(size_t)nr * nm] = j;
-                        ++nr;
-                    }
+            // 32 candidates at a time: every lane tests its home atom against
+            // each (a shared-memory broadcast) into a keep mask and a mask of
+            // those in the band around rnear, then appends its kept ones in
+            // order, so the append work is paid per kept pair only
+            for (int k0 = 0; k0 < staged; k0 += 32) {
+                unsigned tm = 0u, um = 0u;
+#pragma unroll
+                for (int b = 0; b < 32; ++b) {
+                    const int4 cq = sqc[k0 + b];
+                    const float rx = ax - __int_as_float(cq.x), ry = ay - __int_as_float(cq.y),
+                                rz = az - __int_as_float(cq.z);
+                    const float r2 = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
+                    tm |= (r2 < S.rlo2 ? 1u : 0u) << b;
+                    um |= (r2 <= S.rhi2 ? 1u : 0u) << b;
+                }
+                um &= ~tm;                                   // in the band: the exact test decides
+                const unsigned self = (q >= k0 && q < k0 + 32) ? (1u << (q - k0)) : 0u;
+                tm = live ? tm & ~self : 0u;
+                um = live ? um & ~self : 0u;
+                while (um) {
+                    const int b = __ffs(um) - 1;
+                    um &= um - 1;
+                    if (nl_exact(pos, sb, p.ivol, p.rnear, pa, sqc[k0 + b].w)) tm |= 1u << b;
+                }
+                while (tm) {
+                    const int b = __ffs(tm) - 1;
+                    tm &= tm - 1;
+                    const int c = k0 + b;
+                    append(true, c > q && c < fwd_end, sqc[c].w);
                 }
             }
+            kk = staged;
         }
         // the rest: candidates beyond the staging, every candidate of the
         // fixed-point form and of boxes not periodic in all three directions
         for (; kk < total; ++kk) {
             int j = 0;
             const bool take = live && kk != q && nl_take<PERIODIC>(S, kk, pa, qa, rel_a, rel, cen, j);
-            if (take) {
-                if (kk > q && kk < fwd_end) {
-                    if (nf < p.nnbrs) frow[(size_t)nf * nm] = j;
-                    ++nf;
-                } else {
-                    if (nr < p.nnbrs) rrow[(size_t)nr * nm] = j;
-                    ++nr;
-                }
-            }
+            append(take, kk > q && kk < fwd_end, j);
         }
         if (live) {
             numn[a] = nf < p.nnbrs ? nf : p.nnbrs;

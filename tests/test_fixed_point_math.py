@@ -1,15 +1,16 @@
 """The bit-level arithmetic the mixed pair passes rely on, restated in numpy
-and checked on the host (moldy_b200/csrc/common.cuh: fix32, fix_to_float,
-floor_small):
+and checked on the host (moldy_b200/csrc/common.cuh: fix32, floor_small;
+moldy_b200/csrc/pairs.cu: the wrap test of the virial corrections):
 
 * fix32(x) = round-to-nearest-even(x * 2^32) mod 2^32 through one fused
   multiply-add against the bias 1.5 * 2^52;
-* fix_to_float(d): the upper 20 and lower 12 bits of an int32 made exact
-  floats by power-of-two biases and joined by one fused multiply-add equal
-  float(d) rounded once to nearest;
 * floor_small(x): one round-down addition of 2^23 gives floor(x) for
   0 <= x < 2^23;
-* the 32-bit difference of two fixed-point coordinates is the minimum image."""
+* the 32-bit difference of two fixed-point coordinates is the minimum image;
+* ((qa ^ qj) & (qa ^ e)) < 0, e the wrapped 32-bit difference qa - qj, flags
+  exactly the differences that wrapped, the image being m = +1 for qa >= 0 and
+  -1 otherwise (qa - qj = e + m 2^32), and no pair within M of an atom wraps
+  when |qa| <= 2^31 - 1 - M."""
 import numpy as np
 
 RNG = np.random.default_rng(7)
@@ -19,25 +20,30 @@ def bits_f32(u):
     return np.asarray(u, dtype=np.uint32).view(np.float32)
 
 
-def fix_to_float(d):
-    d = np.asarray(d, dtype=np.int32)
-    hi = (d >> 12).astype(np.int64)
-    lo = (d & 0xFFF).astype(np.int64)
-    fhi = bits_f32((0x4B400000 + hi).astype(np.uint32)).astype(np.float64) - 12582912.0
-    flo = bits_f32((0x4B000000 + lo).astype(np.uint32)).astype(np.float64) - 8388608.0
-    # fhi*4096 + flo is exact in float64; the fused multiply-add rounds it once to float32
-    return (fhi * 4096.0 + flo).astype(np.float32)
-
-
 def fix32(x):
     y = np.asarray(x, dtype=np.float64) * 4294967296.0 + 6755399441055744.0   # exact product, one rounding
     return (y.view(np.uint64) & np.uint64(0xFFFFFFFF)).astype(np.uint32).view(np.int32)
 
 
-def test_fix_to_float_is_one_rounding():
-    d = np.concatenate([RNG.integers(-2**31, 2**31, size=2_000_000, dtype=np.int64),
-                        [-2**31, 2**31 - 1, 0, 1, -1, 4095, 4096, -4096, 2**24 + 1, -(2**24 + 1)]]).astype(np.int32)
-    assert np.array_equal(fix_to_float(d), d.astype(np.float32))
+def test_wrap_flag_and_image():
+    qa = RNG.integers(-2**31, 2**31, size=2_000_000, dtype=np.int64)
+    qj = RNG.integers(-2**31, 2**31, size=2_000_000, dtype=np.int64)
+    exact = qa - qj
+    e = ((exact + 2**31) % 2**32 - 2**31)                     # the 32-bit difference
+    a32, j32, e32 = (v.astype(np.int32) for v in (qa, qj, e))
+    flag = ((a32 ^ j32) & (a32 ^ e32)) < 0
+    assert np.array_equal(flag, exact != e)
+    m = np.where(qa >= 0, 1, -1)
+    assert np.array_equal((exact - e)[flag], (m * 2**32)[flag])
+
+
+def test_no_wrap_away_from_the_faces():
+    M = 56_000_000                                            # a pair's span, fixed-point units
+    lim = 2**31 - 1 - M
+    qa = RNG.integers(-lim, lim + 1, size=1_000_000, dtype=np.int64)
+    d = RNG.integers(-M, M + 1, size=1_000_000, dtype=np.int64)
+    qj = qa - d                                               # the partner's true image
+    assert np.all((qj >= -2**31) & (qj < 2**31))              # stored without wrapping: qa - qj = d
 
 
 def test_fix32_rounds_to_nearest_mod_2_32():

@@ -307,4 +307,8 @@ def test_batch_autotune_and_energy_calc_switch(gpu_lib, precision):
         assert np.array_equal(out2[k], out0[k]), k
     b.set_energy_calc(True)
     assert np.array_equal(b.force()["pe_calc"], out0["pe_calc"])
+    kt = b.kernel_times(rebuild=True)
+    assert set(kt) == {"prepare", "tile_screen", "density", "forces"} and all(v > 0 for v in kt.values())
+    assert np.array_equal(b.forces(), f0)
+    assert 10 * b.ntot < b.row_entries() < 40 * b.ntot
     b.close()
