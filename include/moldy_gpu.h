@@ -154,6 +154,12 @@ int moldy_gpu_get_linkcells(moldy_gpu *h, int32_t *l0, int32_t *link, int32_t *i
 int moldy_gpu_update_neighbourlist(moldy_gpu *h);
 /* NLIST(nnbrs, nm) and NUMN(nm), entries 1-based, same order as the reference. */
 int moldy_gpu_get_neighbourlist(moldy_gpu *h, int32_t *nlist, int32_t *numn);
+/* The transpose of that list, as the same build writes it: row i holds the
+ * atoms j with i in NLIST(:, j) -- i's own link cell before i, then the 13
+ * cells of the mirror half stencil (offsets negated, in reverse order), each
+ * cell in chain order.  Same layout as moldy_gpu_get_neighbourlist.  No
+ * reference counterpart: the reference walks only the half list. */
+int moldy_gpu_get_reverse_list(moldy_gpu *h, int32_t *rlist, int32_t *numr);
 
 /* the hot path --------------------------------------------------------------*/
 /* dynamics_m::force (src/dynamics_m.F90:135-401): rebuild schedule (ntc),

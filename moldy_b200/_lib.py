@@ -85,6 +85,7 @@ SIGNATURES = {
     "moldy_gpu_get_linkcells": [H, I, I, I],
     "moldy_gpu_update_neighbourlist": [H],
     "moldy_gpu_get_neighbourlist": [H, I, I],
+    "moldy_gpu_get_reverse_list": [H, I, I],
     "moldy_gpu_force": [H, ctypes.POINTER(ForceOut)],
     "moldy_gpu_velocityverlet": [H, ctypes.POINTER(ForceOut)],
     "moldy_gpu_update_therm_avs": [H, D],

@@ -612,20 +612,21 @@ int Engine::update_neighbourlist() {
     return check_flags();
 }
 
-int Engine::get_neighbourlist(int32_t *nlist, int32_t *numn) {
+int Engine::get_neighbourlist(int32_t *nlist, int32_t *numn, bool reverse) {
     if (!list_ready_) return fail(MOLDY_ERR_ORDER, "neighbour list not built");
+    const int32_t *rows = reverse ? d.rlist : d.nlist, *cnt = reverse ? d.numr : d.numn;
     size_t ne = (size_t)prm.nm * prm.nnbrs;
     if (nlist) {
         int32_t *tmp = nullptr;
         CHECK(dev_alloc(&tmp, ne, "nlist export"));
-        launch_export_nlist(d, prm, tmp, stream_);
+        launch_export_nlist(rows, cnt, prm, tmp, stream_);
         cudaError_t e = cudaMemcpyAsync(nlist, tmp, ne * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
         cudaFree(tmp);
         if (e != cudaSuccess) return cuda_fail(e, "get_neighbourlist");
     }
     if (numn) {
-        CUDA_CHECK(cudaMemcpyAsync(numn, d.numn, prm.nm * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "numn");
+        CUDA_CHECK(cudaMemcpyAsync(numn, cnt, prm.nm * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "numn");
         CUDA_CHECK(cudaStreamSynchronize(stream_), "numn");
     }
     return MOLDY_OK;
@@ -1205,6 +1206,11 @@ int moldy_gpu_update_neighbourlist(moldy_gpu *h) { GUARD(h); TRY(h->e->update_ne
 int moldy_gpu_get_neighbourlist(moldy_gpu *h, int32_t *nlist, int32_t *numn) {
     GUARD(h);
     TRY(h->e->get_neighbourlist(nlist, numn));
+}
+
+int moldy_gpu_get_reverse_list(moldy_gpu *h, int32_t *rlist, int32_t *numr) {
+    GUARD(h);
+    TRY(h->e->get_neighbourlist(rlist, numr, true));
 }
 
 int moldy_gpu_force(moldy_gpu *h, moldy_force_out *out) { GUARD(h); TRY(h->e->force(out)); }

@@ -165,7 +165,7 @@ class Engine {
     int relink();
     int get_linkcells(int32_t *l0, int32_t *link, int32_t *ic);
     int update_neighbourlist();
-    int get_neighbourlist(int32_t *nlist, int32_t *numn);
+    int get_neighbourlist(int32_t *nlist, int32_t *numn, bool reverse = false);
     int force(moldy_force_out *out);
     int velocityverlet(moldy_force_out *out);
     int update_therm_avs(double *s123);
@@ -275,7 +275,8 @@ void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t 
 void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0, int32_t *link,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
-void launch_export_nlist(const DeviceState &d, const Params &p, int32_t *out, cudaStream_t s);
+// rows (entry-major, counts cnt) as NLIST(nnbrs, nm), 1-based, unused slots zero
+void launch_export_nlist(const int32_t *rows, const int32_t *cnt, const Params &p, int32_t *out, cudaStream_t s);
 constexpr int kVariants = 8;           // compiled variants per tunable pass
 // store_rho false: rho is not written (no caller reads it before the next
 // evaluation overwrites it: the inner steps of an md_steps call)

@@ -224,6 +224,15 @@ class MoldySystem:
         check(self._L.moldy_gpu_get_neighbourlist(self._h, _ip(nl), _ip(nn)))
         return nl.reshape(self.nm, self.nnbrs), nn
 
+    def reverse_list(self):
+        """(rlist[nm, nnbrs] 1-based, numr[nm]): row i holds the atoms j whose
+        neighbour-list rows hold i, i's own link cell first, then the mirror
+        half stencil, each cell in chain order."""
+        nl = np.zeros(self.nm * self.nnbrs, dtype=np.int32)
+        nn = np.zeros(self.nm, dtype=np.int32)
+        check(self._L.moldy_gpu_get_reverse_list(self._h, _ip(nl), _ip(nn)))
+        return nl.reshape(self.nm, self.nnbrs), nn
+
     # ------------------------------------------------------------ hot path
     @staticmethod
     def _force_dict(o: _lib.ForceOut) -> dict:

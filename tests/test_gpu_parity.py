@@ -91,6 +91,72 @@ def test_neighbour_list_exact_beyond_staging(oracle_mod, gpu_lib, n, nlc):
         assert np.array_equal(nlo[i, :nno[i]], nlg[i, :nng[i]]), i
 
 
+# (dx, dy, dz) of the 13 cells of the half stencil after the home cell, in
+# the reference's loop order (src/neighbourlist_m.F90:103-276); the reverse
+# rows walk their negations
+_HALF = [(1, 0, 0), (-1, 1, 0), (0, 1, 0), (1, 1, 0), (-1, -1, 1), (0, -1, 1), (1, -1, 1),
+         (-1, 0, 1), (0, 0, 1), (1, 0, 1), (-1, 1, 1), (0, 1, 1), (1, 1, 1)]
+
+
+def _expected_reverse_rows(g, w, nlc):
+    """The transpose of NLIST, each row ordered as the build stages its
+    candidates: the own cell (chain order) before the atom, then the mirror
+    cells -offset(1) ... -offset(13), each in chain order."""
+    ncell = nlc[0] * nlc[1] * nlc[2]
+    l0, link, ic = g.linkcells(ncell)
+    chain = np.zeros(w.nm, dtype=np.int64)
+    for c in range(ncell):
+        # the chain is circular: the last atom links back to the head
+        a, k = l0[c], 0
+        while a and k < w.nm:
+            chain[a - 1] = k
+            k += 1
+            a = link[a - 1]
+            if a == l0[c]:
+                break
+    cell = ic - 1
+    cxyz = np.stack([cell % nlc[0], (cell // nlc[0]) % nlc[1], cell // (nlc[0] * nlc[1])], axis=1)
+    mirror = {}
+    for k, (dx, dy, dz) in enumerate(_HALF):
+        mirror[((-dx) % nlc[0], (-dy) % nlc[1], (-dz) % nlc[2])] = 1 + k
+    nl, nn = g.neighbour_list()
+    rows = [[] for _ in range(w.nm)]
+    for j in range(w.nm):
+        for i in nl[j, :nn[j]] - 1:
+            rows[i].append(j)
+    out = []
+    for i in range(w.nm):
+        def key(j, i=i):
+            off = tuple(int(v) for v in (cxyz[j] - cxyz[i]) % np.array(nlc))
+            return (0 if off == (0, 0, 0) else mirror[off], chain[j])
+        out.append(sorted(rows[i], key=key))
+    return out
+
+
+@pytest.mark.parametrize("n,nlc,strain", [(10, None, False), (9, None, True), (10, 3, False), (12, 4, False)])
+def test_reverse_rows_are_the_ordered_transpose(gpu_lib, n, nlc, strain):
+    """The reverse rows the build writes beside NLIST hold, for every atom i,
+    exactly the atoms j with i in NLIST(:, j), in staging order; covers the
+    cell-relative pre-test (default cells, a strained box), the fixed-point
+    one (3 cells per direction) and candidates beyond the staging (12^3 bcc in
+    4^3 cells)."""
+    rng = np.random.default_rng(21)
+    w = wl.make_workload(n, sigma=0.1, temperature=0.0, seed=22,
+                         strain=wl.random_symmetric_strain(rng, 0.02) if strain else None)
+    if nlc is not None:
+        w.nlc = (nlc, nlc, nlc)
+    from moldy_b200 import MoldySystem
+    g = MoldySystem.from_workload(w, precision="mixed")
+    g.linkup()
+    g.update_neighbourlist()
+    exp = _expected_reverse_rows(g, w, tuple(w.nlc))
+    rl, nr = g.reverse_list()
+    assert np.array_equal(nr, [len(r) for r in exp])
+    for i in range(w.nm):
+        assert np.array_equal(rl[i, :nr[i]] - 1, exp[i]), i
+    g.close()
+
+
 @pytest.mark.parametrize("n", [8, 30])
 def test_relink_chain_order_exact(oracle_mod, gpu_lib, n):
     """relink replays the reference's chain surgery: same l0/link after moves,
@@ -493,8 +559,7 @@ def test_partly_periodic_box_mixed_runs_fp64(oracle_mod, gpu_lib, ivol):
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_md_bit_reproducible(gpu_lib, prec):
     """Two runs of the same MD (thin skins: several outer and intermediate
-    rebuilds, whose reverse entries are placed by integer atomics and then
-    sorted) end in the same state bit for bit."""
+    list rebuilds) end in the same state bit for bit."""
     from moldy_b200 import MoldySystem
     w = wl.make_workload(8, sigma=0.1, temperature=2000.0, ivol=0, seed=17, nbrupdate=200)
     states = []
