@@ -675,13 +675,31 @@ def run_batch(args):
     # cell order plus rho, F, F' (32); forces: its F' (8), F read (8), the
     # force (24), the force-routine energy (8) and the six virial moments (48)
     n_row = b.row_entries() / b.ntot
-    bpa = {"density": 4 * n_row + 4 + 32 + 32, "forces": 4 * n_row + 4 + 32 + 8 + 8 + 24 + 8 + 48}
-    dom = max(("density", "forces"), key=lambda k: ktimes[k])
     peak, peak_kind = load_peaks()
-    achieved = bpa[dom] * b.ntot / (ktimes[dom] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                "algorithmic_bytes_per_launch": bpa[dom] * b.ntot, "avg_launch_ms": ktimes[dom]}
+    persistent = b.persistent_applies()
+    eval_ms = None
+    if persistent:
+        # the timed evaluations are one persistent launch each: its bytes per
+        # atom are the compact row and count read by both passes (2 (4 n + 4)),
+        # the positions and cell order read into the records (24 + 4), the cell
+        # order again per pass (8), rho, F, F' out (24), F read back (8), the
+        # force (24) and the force-routine energy (8) out
+        et = [b.eval_times() for _ in range(5)]
+        eval_ms = {k: float(np.median([t[k] for t in et])) for k in ("current", "rebuilt")}
+        bpa_p = 8 * n_row + 8 + 28 + 8 + 24 + 8 + 24 + 8
+        achieved = bpa_p * b.ntot / (eval_ms["current"] / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": "batch_eval (persistent: list check, records in shared memory, "
+                                              "density, forces, per-system sums)",
+                    "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": bpa_p * b.ntot,
+                    "avg_launch_ms": eval_ms["current"]}
+    else:
+        bpa = {"density": 4 * n_row + 4 + 32 + 32, "forces": 4 * n_row + 4 + 32 + 8 + 8 + 24 + 8 + 48}
+        dom = max(("density", "forces"), key=lambda k: ktimes[k])
+        achieved = bpa[dom] * b.ntot / (ktimes[dom] / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "algorithmic_bytes_per_launch": bpa[dom] * b.ntot, "avg_launch_ms": ktimes[dom]}
     b.set_energy_calc(True)
     b.force()
     ecalc_ms = max_over_ranks(timed(force, min(steps, 50)))
@@ -698,22 +716,37 @@ def run_batch(args):
     b.set_gather(best_gather[other])
     b.force()
     other_ms = max_over_ranks(timed(force, min(steps, 50)))
-    b.set_energy_calc(True)   # the accuracy comparison includes energy_calc's energies
+    # the timed path (energy_calc off: the persistent launch in mixed
+    # precision where it applies) against the FP64 path, then the per-pass
+    # path with energy_calc's energies
+    def errors(res_):
+        (f64, o64), (fmx, omx) = res_["fp64"], res_["mixed"]
+        d = np.concatenate([(x - y) @ w.b0.T for w, x, y in zip(ws, fmx, f64)])
+        return {
+            "force_rms_eV_per_A": float(np.sqrt(np.mean(np.sum(d * d, axis=1)))),
+            "force_max_eV_per_A": float(np.max(np.linalg.norm(d, axis=1))),
+            "pe_calc_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe_calc"] - o64["pe_calc"]) / b.natoms)),
+            "pe_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe"] - o64["pe"]) / b.natoms)),
+            "stress_max_abs_GPa": float(np.max(np.abs(omx["tp"] - o64["tp"]) / o64["vol"][:, None, None])
+                                        * 160.2176),
+        }
     res = {p_: None for p_ in ("fp64", "mixed")}
     res[other] = snapshot()
     b.set_precision(prec)
     b.set_gather(best_gather[prec])
     res[prec] = snapshot()
-    (f64, o64), (fmx, omx) = res["fp64"], res["mixed"]
-    d = np.concatenate([(x - y) @ w.b0.T for w, x, y in zip(ws, fmx, f64)])
-    accuracy = {
-        "vs": "FP64 GPU path (bit-matched to the oracle at 1e-10)",
-        "force_rms_eV_per_A": float(np.sqrt(np.mean(np.sum(d * d, axis=1)))),
-        "force_max_eV_per_A": float(np.max(np.linalg.norm(d, axis=1))),
-        "pe_calc_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe_calc"] - o64["pe_calc"]) / b.natoms)),
-        "pe_max_abs_eV_per_atom": float(np.max(np.abs(omx["pe"] - o64["pe"]) / b.natoms)),
-        "stress_max_abs_GPa": float(np.max(np.abs(omx["tp"] - o64["tp"]) / o64["vol"][:, None, None]) * 160.2176),
-    }
+    accuracy = {"vs": "FP64 GPU path (bit-matched to the oracle at 1e-10)",
+                "timed_path": {"persistent": b.persistent_applies(), **errors(res)}}
+    b.set_energy_calc(True)
+    res = {p_: None for p_ in ("fp64", "mixed")}
+    b.set_precision(other)
+    b.set_gather(best_gather[other])
+    res[other] = snapshot()
+    b.set_precision(prec)
+    b.set_gather(best_gather[prec])
+    res[prec] = snapshot()
+    accuracy["per_pass_with_energy_calc"] = errors(res)
+    b.set_energy_calc(False)
 
     # end to end: positions from pinned host memory, one evaluation, forces and
     # per-system results back, every step
@@ -797,7 +830,9 @@ def run_batch(args):
                    "precision": prec, f"{other}_ms_per_step": other_ms,
                    "with_energy_calc_ms_per_step": ecalc_ms,
                    "evaluation_with_every_list_built_ms": build_ms,
-                   "kernel_ms": ktimes, "row_entries_per_atom": n_row,
+                   "persistent_evaluation": persistent, "atom_lanes": tunes[prec]["chosen"].get("atom_lanes"),
+                   "persistent_eval_ms": eval_ms,
+                   "per_pass_kernel_ms": ktimes, "row_entries_per_atom": n_row,
                    "parallelism": f"supercells sharded over {world} rank(s) by atom count",
                    "l2": "per-evaluation working set (positions, cell order, forces, energies, virial) "
                          "> 126 MB L2"},

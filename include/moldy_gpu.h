@@ -359,18 +359,41 @@ int moldy_gpu_batch_quench(moldy_batch *h, int32_t maxfn, int32_t criterion, dou
  * 256; the rest are read from global memory). */
 int moldy_gpu_batch_set_tiles(moldy_batch *h, int32_t lanes, int32_t staged);
 /* Chooses, on the live configuration, the lanes per home atom of the tile
- * screen (4, 8, 16, 32; timed on evaluations that rebuild every list) and the
+ * screen (4, 8, 16, 32; timed on evaluations that rebuild every list), the
  * row entries gathered at a time by the per-atom passes (1, 2, 4; timed with
- * current lists), nreps evaluations each in the current precision, and keeps
- * the fastest.  times_ms (7 doubles, may be NULL) receives the mean times in
- * that order, chosen (2 int32, may be NULL) lanes and entries.  Results do not
- * depend on either choice; positions and boxes are unchanged. */
+ * current lists) and, where the persistent evaluation applies, its lanes per
+ * atom (1, 2, 4; timed with current lists), nreps evaluations each in the
+ * current precision, and keeps the fastest.  times_ms (10 doubles, may be
+ * NULL) receives the mean times in that order (the last three 0 where the
+ * persistent evaluation does not apply), chosen (3 int32, may be NULL) the
+ * tile lanes, the entries and the lanes per atom (0: not tuned).  Results do
+ * not depend on the tile lanes or the entries; the lanes per atom change the
+ * order of each atom's FP64 sums.  Positions and boxes are unchanged. */
 int moldy_gpu_batch_autotune(moldy_batch *h, int32_t nreps, double *times_ms, int32_t *chosen);
 /* One evaluation of every system (as moldy_gpu_batch_force) with its four
  * launches timed by CUDA events on the batch's stream: the list check, the
  * tile screen, the density pass and the force pass, into ms4 (ms);
  * rebuild = 1 rebuilds every list first. */
 int moldy_gpu_batch_kernel_times(moldy_batch *h, int32_t rebuild, double *ms4);
+/* The persistent evaluation: moldy_gpu_batch_force evaluates every system in
+ * one launch (k_batch_eval) when the precision is mixed, energy_calc is off,
+ * every atom is heavier than 0.05 and the largest system's records (16 bytes
+ * per atom) fit in one block's shared memory.  A resident grid of blocks
+ * takes the systems in descending size from a device queue; per system the
+ * block checks (and rebuilds) the list, stages the atoms in shared memory as
+ * fixed-point records and runs the density and force passes with `lanes`
+ * lanes per atom, then the per-system sums.  enable = 0 keeps the per-pass
+ * launches (default 1). */
+int moldy_gpu_batch_set_persistent(moldy_batch *h, int32_t enable);
+/* Lanes per atom in the persistent evaluation's passes: 1, 2 or 4 (default 2;
+ * moldy_gpu_batch_autotune chooses). */
+int moldy_gpu_batch_set_atom_lanes(moldy_batch *h, int32_t lanes);
+/* *applies = 1 when moldy_gpu_batch_force runs the persistent evaluation. */
+int moldy_gpu_batch_persistent_applies(moldy_batch *h, int32_t *applies);
+/* Device times (ms) of the persistent evaluation: ms2[0] with every list
+ * current, ms2[1] with every list rebuilt in the same launch.
+ * MOLDY_ERR_UNSUPPORTED where it does not apply. */
+int moldy_gpu_batch_eval_times(moldy_batch *h, double *ms2);
 /* Precision of the per-atom density and force passes of moldy_gpu_batch_force:
  * 0 all FP64 (default); 1 mixed: separations, distances, table interpolation
  * and pair forces in FP32 from FP64 position differences, every sum in FP64,

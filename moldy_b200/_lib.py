@@ -135,6 +135,10 @@ SIGNATURES = {
     "moldy_gpu_batch_set_references": [H, D, D],
     "moldy_gpu_batch_force_matching": [H, ctypes.c_double, ctypes.c_double, D, D],
     "moldy_gpu_batch_set_gather": [H, ctypes.c_int32],
+    "moldy_gpu_batch_set_persistent": [H, ctypes.c_int32],
+    "moldy_gpu_batch_set_atom_lanes": [H, ctypes.c_int32],
+    "moldy_gpu_batch_persistent_applies": [H, I],
+    "moldy_gpu_batch_eval_times": [H, D],
     "moldy_gpu_batch_list_stats": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_row_entries": [H, ctypes.POINTER(ctypes.c_int64)],
     "moldy_gpu_batch_launches": [H, ctypes.POINTER(ctypes.c_int64)],

@@ -158,15 +158,41 @@ class MoldyBatch:
         check(self._L.moldy_gpu_batch_set_precision(self._h, 1 if precision == "mixed" else 0))
 
     def autotune(self, nreps: int = 3) -> dict:
-        """Chooses the tile lanes per home atom and the gather width on the
-        live configuration (moldy_gpu_batch_autotune); returns the mean
-        evaluation times (ms) and the choice."""
-        t = np.zeros(7)
-        ch = (ctypes.c_int32 * 2)()
+        """Chooses the tile lanes per home atom, the gather width and, where
+        the persistent evaluation applies, its lanes per atom on the live
+        configuration (moldy_gpu_batch_autotune); returns the mean evaluation
+        times (ms) and the choice (atom_lanes 0: not tuned)."""
+        t = np.zeros(10)
+        ch = (ctypes.c_int32 * 3)()
         check(self._L.moldy_gpu_batch_autotune(self._h, int(nreps), _dp(t), ch))
-        return {"lanes_ms": dict(zip((4, 8, 16, 32), t[:4].tolist())),
-                "gather_ms": dict(zip((1, 2, 4), t[4:].tolist())),
-                "chosen": {"lanes": int(ch[0]), "gather": int(ch[1])}}
+        out = {"lanes_ms": dict(zip((4, 8, 16, 32), t[:4].tolist())),
+               "gather_ms": dict(zip((1, 2, 4), t[4:7].tolist())),
+               "chosen": {"lanes": int(ch[0]), "gather": int(ch[1]), "atom_lanes": int(ch[2])}}
+        if ch[2]:
+            out["atom_lanes_ms"] = dict(zip((1, 2, 4), t[7:].tolist()))
+        return out
+
+    def set_persistent(self, enable: bool = True):
+        """Whether :meth:`force` may evaluate every system in one persistent
+        launch (mixed precision, energy_calc off, every atom heavier than 0.05)."""
+        check(self._L.moldy_gpu_batch_set_persistent(self._h, 1 if enable else 0))
+
+    def set_atom_lanes(self, lanes: int):
+        """Lanes per atom (1, 2, 4) of the persistent evaluation's passes."""
+        check(self._L.moldy_gpu_batch_set_atom_lanes(self._h, int(lanes)))
+
+    def persistent_applies(self) -> bool:
+        """True when :meth:`force` runs the persistent evaluation."""
+        v = ctypes.c_int32(0)
+        check(self._L.moldy_gpu_batch_persistent_applies(self._h, ctypes.byref(v)))
+        return bool(v.value)
+
+    def eval_times(self) -> dict:
+        """Device times (ms) of the persistent evaluation with every list
+        current and with every list rebuilt in the same launch."""
+        t = np.zeros(2)
+        check(self._L.moldy_gpu_batch_eval_times(self._h, _dp(t)))
+        return {"current": float(t[0]), "rebuilt": float(t[1])}
 
     def set_references(self, f_ref, sigma_ref):
         """Reference real forces (one (nm_s, 3) array per system, or one (ntot, 3)

@@ -198,25 +198,26 @@ __device__ double block_max(double v, double *sh) {
 // cells, the cell sizes scanned into slot ranges starting at atom0, every
 // cell filled and sorted by atom index.  Every evaluated system then copies
 // its positions and masses into cell order.
-__global__ void __launch_bounds__(kPrepThreads)
-k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__restrict__ mass,
-          double *__restrict__ Xb, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
-          int32_t *__restrict__ cell_start, int32_t *__restrict__ cursor, int32_t *__restrict__ sorted,
-          double4 *__restrict__ spos, unsigned long long *__restrict__ stats, int32_t *__restrict__ todo,
-          int32_t *__restrict__ ntodo) {
+// The list check and rebuild of one active system by the whole block (any
+// block size up to 1024); todo, when given, receives the rebuilt cells for
+// the tile screen.  Every atom's cell-order copy goes to spos when all_spos,
+// else only a rebuilt system's (the tile screen reads it).  Returns whether
+// the system was rebuilt (the same in every thread).
+__device__ int prepare_system(BSys &S, const double *__restrict__ X, const double *__restrict__ mass,
+                              double *__restrict__ Xb, int32_t *__restrict__ cell_of,
+                              int32_t *__restrict__ cell_count, int32_t *__restrict__ cell_start,
+                              int32_t *__restrict__ cursor, int32_t *__restrict__ sorted,
+                              double4 *__restrict__ spos, unsigned long long *__restrict__ stats,
+                              int32_t *__restrict__ todo, int32_t *__restrict__ ntodo, bool all_spos) {
     __shared__ double sh[33];
-    __shared__ int wsum[kPrepThreads / 32];
+    __shared__ int wsum[32];
     __shared__ int todo0;
-    BSys &S = sys[blockIdx.x];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-    if (!S.active) {
-        if (tid == 0) S.rebuild = 0;
-        return;
-    }
     const int a0 = S.atom0, nm = S.nm;
     int rebuild = S.stale;
     if (!rebuild) {
         double m = 0.0;
+#pragma unroll 4
         for (int i = tid; i < nm; i += nt) {
             const size_t a = 3 * (size_t)(a0 + i);
             double rx, ry, rz;
@@ -232,7 +233,7 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
         atomicAdd(&stats[1], 1ULL);
         if (rebuild) {
             atomicAdd(&stats[0], 1ULL);
-            todo0 = atomicAdd(ntodo, S.ncell);
+            if (todo) todo0 = atomicAdd(ntodo, S.ncell);
         }
     }
     if (rebuild) {
@@ -289,7 +290,7 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
         // ascending atom order inside each cell; the cells join the tile screen's work
         for (int cl = tid; cl < S.ncell; cl += nt) {
             const int c = S.cell0 + cl;
-            todo[todo0 + cl] = c;
+            if (todo) todo[todo0 + cl] = c;
             const int s0 = cell_start[c], s1 = cl + 1 < S.ncell ? cell_start[c + 1] : a0 + nm;
             for (int i = s0 + 1; i < s1; ++i) {
                 const int v = sorted[i];
@@ -300,10 +301,29 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
         }
         __syncthreads();
     }
-    for (int hs = a0 + tid; hs < a0 + nm; hs += nt) {
-        const int a = sorted[hs];
-        spos[hs] = make_double4(X[3 * (size_t)a], X[3 * (size_t)a + 1], X[3 * (size_t)a + 2], mass[a]);
+    if (rebuild || all_spos) {
+        for (int hs = a0 + tid; hs < a0 + nm; hs += nt) {
+            const int a = sorted[hs];
+            spos[hs] = make_double4(X[3 * (size_t)a], X[3 * (size_t)a + 1], X[3 * (size_t)a + 2], mass[a]);
+        }
     }
+    __syncthreads();
+    return rebuild;
+}
+
+__global__ void __launch_bounds__(kPrepThreads)
+k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__restrict__ mass,
+          double *__restrict__ Xb, int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
+          int32_t *__restrict__ cell_start, int32_t *__restrict__ cursor, int32_t *__restrict__ sorted,
+          double4 *__restrict__ spos, unsigned long long *__restrict__ stats, int32_t *__restrict__ todo,
+          int32_t *__restrict__ ntodo) {
+    BSys &S = sys[blockIdx.x];
+    if (!S.active) {
+        if (threadIdx.x == 0) S.rebuild = 0;
+        return;
+    }
+    prepare_system(S, X, mass, Xb, cell_of, cell_count, cell_start, cursor, sorted, spos, stats, todo, ntodo,
+                   true);
 }
 
 // ------------------------------------------------------------ tile passes --
@@ -313,6 +333,62 @@ k_prepare(BSys *__restrict__ sys, const double *__restrict__ X, const double *__
 // candidate order.  LPH lanes
 // serve one home atom: they test LPH candidates at a time and place the hits
 // with one warp ballot, so no lane waits on another's pair arithmetic.
+// The compact rows of the home atoms of cell c by one warp, with the warp's
+// tile (tp, ti: cap entries; pre, cs: 28); returns the longest row seen when
+// it exceeds pair_cap, else 0.
+template <int LPH>
+__device__ int screen_cell(const TileArgs &a, int c, int ntot, int pair_cap, int32_t *__restrict__ alist,
+                           int32_t *__restrict__ cnt_out, double4 *tp, int *ti, int *pre, int *cs) {
+    const int lane = threadIdx.x & 31;
+    const int g = lane / LPH, gl = lane % LPH;
+    const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
+    const unsigned below = (1u << lane) - 1u;
+    int overflow = 0;
+    const BSys &S = a.sys[a.cell_sys[c]];
+    const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
+    if (h1 == h0) return 0;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
+    const double rv2 = S.rv2;
+    const int total = stage_tile<false>(a, S, c, tp, nullptr, ti, pre, cs);
+    for (int hb = h0; hb < h1; hb += 32 / LPH) {
+        const int hs = hb + g;
+        const bool live = hs < h1;
+        const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
+        int cnt = 0;
+        // every lane of the warp runs the same number of rounds (ballots are warp-wide)
+        for (int k0 = 0; k0 < total; k0 += LPH) {
+            const int k = k0 + gl;
+            bool hit = false;
+            int slot = -1;
+            if (live && k < total) {
+                double4 p; double fpk;
+                candidate<false>(a, k, tp, nullptr, ti, pre, cs, p, fpk, slot);
+                if (slot != hs) {
+                    double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
+                    dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
+                    double ux, uy, uz;
+                    pair_u(b, dx, dy, dz, ux, uy, uz);
+                    hit = (ux * ux + uy * uy + uz * uz) < rv2;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
+            if (hit) {
+                const int e = cnt + __popc(m & below);
+                if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
+            }
+            cnt += __popc(m);
+        }
+        if (live && gl == 0) {
+            cnt_out[hs] = cnt;
+            if (cnt > pair_cap) overflow = max(overflow, cnt);
+        }
+    }
+    __syncwarp();   // the next cell restages the warp's tile
+    return overflow;
+}
+
 template <int LPH>
 __global__ void __launch_bounds__(32 * kTileWarps)
 k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, int32_t *__restrict__ cnt_out,
@@ -320,58 +396,13 @@ k_tile_screen(TileArgs a, int ntot, int pair_cap, int32_t *__restrict__ alist, i
     __shared__ double4 tpos[kTileWarps][kTileCap];
     __shared__ int tidx[kTileWarps][kTileCap];
     __shared__ int tpre[kTileWarps][28], tcs[kTileWarps][28];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane / LPH, gl = lane % LPH;
-    const unsigned gmask = (LPH == 32 ? 0xffffffffu : ((1u << LPH) - 1u)) << (g * LPH);
-    const unsigned below = (1u << lane) - 1u;
+    const int w = threadIdx.x >> 5;
     const int nwork = *ntodo;
     int overflow = 0;
     // one warp per cell of the rebuilt systems (warp-uniform loop)
-    for (int t = blockIdx.x * kTileWarps + w; t < nwork; t += gridDim.x * kTileWarps) {
-        const int c = todo[t];
-        const BSys &S = a.sys[a.cell_sys[c]];
-        const int h0 = a.cell_start[c], h1 = a.cell_start[c + 1];
-        if (h1 == h0) continue;
-        double b[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) b[k] = S.b0[k];
-        const double rv2 = S.rv2;
-        const int total = stage_tile<false>(a, S, c, tpos[w], nullptr, tidx[w], tpre[w], tcs[w]);
-        for (int hb = h0; hb < h1; hb += 32 / LPH) {
-            const int hs = hb + g;
-            const bool live = hs < h1;
-            const double4 ph = live ? a.spos[hs] : make_double4(0.0, 0.0, 0.0, 0.0);
-            int cnt = 0;
-            // every lane of the warp runs the same number of rounds (ballots are warp-wide)
-            for (int k0 = 0; k0 < total; k0 += LPH) {
-                const int k = k0 + gl;
-                bool hit = false;
-                int slot = -1;
-                if (live && k < total) {
-                    double4 p; double fpk;
-                    candidate<false>(a, k, tpos[w], nullptr, tidx[w], tpre[w], tcs[w], p, fpk, slot);
-                    if (slot != hs) {
-                        double dx = ph.x - p.x, dy = ph.y - p.y, dz = ph.z - p.z;
-                        dx = dx - round(dx); dy = dy - round(dy); dz = dz - round(dz);
-                        double ux, uy, uz;
-                        pair_u(b, dx, dy, dz, ux, uy, uz);
-                        hit = (ux * ux + uy * uy + uz * uz) < rv2;
-                    }
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, hit) & gmask;
-                if (hit) {
-                    const int e = cnt + __popc(m & below);
-                    if (e < pair_cap) alist[(size_t)e * ntot + hs] = slot;
-                }
-                cnt += __popc(m);
-            }
-            if (live && gl == 0) {
-                cnt_out[hs] = cnt;
-                if (cnt > pair_cap) overflow = max(overflow, cnt);
-            }
-        }
-        __syncwarp();   // the next cell restages the warp's tile
-    }
+    for (int t = blockIdx.x * kTileWarps + w; t < nwork; t += gridDim.x * kTileWarps)
+        overflow = max(overflow, screen_cell<LPH>(a, todo[t], ntot, pair_cap, alist, cnt_out, tpos[w], tidx[w],
+                                                  tpre[w], tcs[w]));
     if (overflow) { atomicExch(&flags[0], 1); atomicMax(&flags[1], overflow); }
 }
 
@@ -542,6 +573,246 @@ k_cl_forces(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restr
         if (VIR) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) vir[6 * (size_t)at + k] = v[k];
+        }
+    }
+}
+
+// ------------------------------------------------ persistent evaluation --
+// One launch evaluates every active system in mixed precision: the force
+// routine's energy, the forces and the virial (energy_calc's exact energies
+// are left to the per-pass kernels).  A resident grid of blocks takes systems
+// from a queue in descending size.  For each system the block
+//   1. checks the list and, past half the skin, rebuilds it: binning as
+//      k_prepare, then the compact rows with the block's warps over the
+//      system's cells as k_tile_screen (the warps' tiles in the shared memory
+//      that the records use afterwards);
+//   2. stages the system's atoms in cell order as fixed-point records (x, y,
+//      z, F'(rho) as float) in shared memory, so every neighbour read of the
+//      two passes is a shared-memory load;
+//   3. runs the density pass (rho, F, F') and the force pass with LPA lanes
+//      per atom: lane g takes the row entries g, g + LPA, ...; the lanes'
+//      FP64 sums are combined by shuffles in a fixed order;
+//   4. reduces the system's energy, largest force and virial in a fixed
+//      order (the results of k_sys_reduce).
+// Separations come from the 32-bit fixed-point difference (the integer
+// difference is the minimum image); distances, table interpolation and pair
+// terms run in FP32, and every sum accumulates in FP64.  Pairs enter the
+// virial without the mass filter: the path runs only when every atom is
+// heavier than 0.05, so every pair passes m_i + m_j > 0.1.
+constexpr int kEvalThreads = 512;
+constexpr int kEvalWarps = kEvalThreads / 32;
+constexpr int kEvalGather = 4;       // row entries a lane loads before it uses any
+
+struct EvalArgs {
+    BSys *sys;
+    const int32_t *order;            // systems by descending size
+    int nsys, ntot, pair_cap;
+    int32_t *queue;                  // [0] next system, [1] blocks done (both zero between launches)
+    const double *X, *mass;
+    double *Xb;
+    int32_t *cell_of, *cell_count, *cell_start, *cursor, *sorted;
+    double4 *spos;
+    unsigned long long *stats;
+    const int32_t *cell_sys;
+    int32_t *alist, *pcnt, *flags;
+    int ncell, cap;
+    double rc2;
+    double *f, *rho, *afrho, *fp, *en_force, *sysout;
+};
+
+// sum over the LPA lanes of an atom's group, the same in every lane
+template <int LPA>
+__device__ __forceinline__ double lanes_sum(double v) {
+#pragma unroll
+    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// fractional difference of two records in fixed-point units (FP32) and r^2
+__device__ __forceinline__ float rec_sep(const float *bq, const int4 &qi, const int4 &qj, float &dx, float &dy,
+                                         float &dz) {
+    dx = fix_to_float((int32_t)((uint32_t)qi.x - (uint32_t)qj.x));
+    dy = fix_to_float((int32_t)((uint32_t)qi.y - (uint32_t)qj.y));
+    dz = fix_to_float((int32_t)((uint32_t)qi.z - (uint32_t)qj.z));
+    const float ux = fmaf(bq[6], dz, fmaf(bq[3], dy, bq[0] * dx));
+    const float uy = fmaf(bq[7], dz, fmaf(bq[4], dy, bq[1] * dx));
+    const float uz = fmaf(bq[8], dz, fmaf(bq[5], dy, bq[2] * dx));
+    return fmaf(uz, uz, fmaf(uy, uy, ux * ux));
+}
+
+template <int LPH, int LPA>
+__global__ void __launch_bounds__(kEvalThreads, 1)
+k_batch_eval(EvalArgs a, Tables t) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ int tpre[kEvalWarps][28], tcs[kEvalWarps][28];
+    __shared__ double shr[33];
+    __shared__ int s_next;
+    int4 *rec = reinterpret_cast<int4 *>(dsm);
+    const int tid = threadIdx.x, w = tid >> 5;
+    const float rc2f = (float)a.rc2;
+    constexpr int kAtomsPerRound = kEvalThreads / LPA;
+    const int g = tid % LPA;
+    int overflow = 0;
+    for (;;) {
+        if (tid == 0) s_next = atomicAdd(&a.queue[0], 1);
+        __syncthreads();
+        const int k = s_next;
+        __syncthreads();                       // s_next is rewritten only after every thread read it
+        if (k >= a.nsys) break;
+        const int sid = a.order[k];
+        BSys &S = a.sys[sid];
+        if (!S.active) continue;
+        // 1. list check, rebuild when due
+        const int rebuilt = prepare_system(S, a.X, a.mass, a.Xb, a.cell_of, a.cell_count, a.cell_start, a.cursor,
+                                           a.sorted, a.spos, a.stats, nullptr, nullptr, false);
+        if (rebuilt) {
+            TileArgs ta;
+            ta.sys = a.sys; ta.cell_sys = a.cell_sys; ta.cell_start = a.cell_start; ta.sorted = a.sorted;
+            ta.spos = a.spos; ta.sfp = nullptr; ta.ncell = a.ncell; ta.cap = a.cap; ta.rc2 = a.rc2;
+            double4 *tp = reinterpret_cast<double4 *>(dsm) + (size_t)w * a.cap;
+            int *ti = reinterpret_cast<int *>(reinterpret_cast<double4 *>(dsm) + (size_t)kEvalWarps * a.cap) +
+                      (size_t)w * a.cap;
+            for (int c = S.cell0 + w; c < S.cell0 + S.ncell; c += kEvalWarps)
+                overflow = max(overflow, screen_cell<LPH>(ta, c, a.ntot, a.pair_cap, a.alist, a.pcnt, tp, ti,
+                                                          tpre[w], tcs[w]));
+            __syncthreads();                   // rows written; the tiles' memory is reused below
+        }
+        const int a0 = S.atom0, nm = S.nm;
+        double b[9];
+        float bq[9];                           // B0 per fixed-point unit
+#pragma unroll
+        for (int q = 0; q < 9; ++q) { b[q] = S.b0[q]; bq[q] = (float)(b[q] * kFixUnit); }
+        // 2. the system's records in cell order
+#pragma unroll 4
+        for (int i = tid; i < nm; i += kEvalThreads) {
+            const size_t at = 3 * (size_t)a.sorted[a0 + i];
+            rec[i] = make_int4(fix32(a.X[at]), fix32(a.X[at + 1]), fix32(a.X[at + 2]), 0);
+        }
+        __syncthreads();
+        // 3a. density, F and F'
+        for (int i0 = 0; i0 < nm; i0 += kAtomsPerRound) {
+            const int i = i0 + tid / LPA;
+            const bool live = i < nm;
+            const int hs = a0 + (live ? i : 0);
+            const int4 qi = rec[live ? i : 0];
+            int n = live ? a.pcnt[hs] : 0;
+            n = n < a.pair_cap ? n : a.pair_cap;
+            double rho = 0.0;
+            for (int e0 = g; e0 < n; e0 += kEvalGather * LPA) {
+                int jj[kEvalGather];
+#pragma unroll
+                for (int u = 0; u < kEvalGather; ++u) {
+                    const int e = e0 + u * LPA;
+                    jj[u] = e < n ? a.alist[(size_t)e * a.ntot + hs] - a0 : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < kEvalGather; ++u) {
+                    if (jj[u] < 0) continue;
+                    const int4 qj = rec[jj[u]];
+                    float dx, dy, dz;
+                    const float r2 = rec_sep(bq, qi, qj, dx, dy, dz);
+                    if (r2 < rc2f) rho += (double)lookup_phif(t, sqrtf(r2));
+                }
+            }
+            rho = lanes_sum<LPA>(rho);
+            if (live && g == 0) {
+                double fe = 0.0, fd = 0.0;
+                if (rho > 1e-40) {
+                    const double2 e2 = lookup_e2(t, rho);
+                    fe = e2.x; fd = e2.y;
+                }
+                rec[i].w = __float_as_int((float)fd);
+                const int at = a.sorted[hs];
+                a.rho[at] = rho;
+                a.afrho[at] = fe;
+                a.fp[at] = fd;
+            }
+        }
+        __syncthreads();
+        // 3b. forces, force-routine energy, virial moments
+        double sef = 0.0, sfm = 0.0, sv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int i0 = 0; i0 < nm; i0 += kAtomsPerRound) {
+            const int i = i0 + tid / LPA;
+            const bool live = i < nm;
+            const int hs = a0 + (live ? i : 0);
+            const int4 qi = rec[live ? i : 0];
+            const float fpi = __int_as_float(qi.w);
+            int n = live ? a.pcnt[hs] : 0;
+            n = n < a.pair_cap ? n : a.pair_cap;
+            double fx = 0.0, fy = 0.0, fz = 0.0, ef = 0.0, v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int e0 = g; e0 < n; e0 += kEvalGather * LPA) {
+                int jj[kEvalGather];
+#pragma unroll
+                for (int u = 0; u < kEvalGather; ++u) {
+                    const int e = e0 + u * LPA;
+                    jj[u] = e < n ? a.alist[(size_t)e * a.ntot + hs] - a0 : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < kEvalGather; ++u) {
+                    if (jj[u] < 0) continue;
+                    const int4 qj = rec[jj[u]];
+                    float dx, dy, dz;
+                    const float r2 = rec_sep(bq, qi, qj, dx, dy, dz);
+                    if (!(r2 < rc2f)) continue;
+                    const float r = sqrtf(r2), rr = 1.0f / r;
+                    const float4 q = lookup_r4f(t, r);
+                    const float fpair = -(q.y + q.w * (fpi + __int_as_float(qj.w))) * rr;
+                    fx += (double)(dx * fpair);
+                    fy += (double)(dy * fpair);
+                    fz += (double)(dz * fpair);
+                    ef += (double)q.x;
+                    const float hf = 0.5f * fpair;
+                    const float hx = dx * hf, hy = dy * hf;
+                    v[0] += (double)(dx * hx); v[1] += (double)(dy * hy); v[2] += (double)(dz * (dz * hf));
+                    v[3] += (double)(dy * hx); v[4] += (double)(dz * hx); v[5] += (double)(dz * hy);
+                }
+            }
+            fx = lanes_sum<LPA>(fx); fy = lanes_sum<LPA>(fy); fz = lanes_sum<LPA>(fz);
+            ef = lanes_sum<LPA>(ef);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v[q] = lanes_sum<LPA>(v[q]);
+            if (live && g == 0) {
+                // fixed-point units to box lengths (exact scalings)
+                fx *= kFixUnit; fy *= kFixUnit; fz *= kFixUnit;
+                const int at = a.sorted[hs];
+                a.f[3 * (size_t)at] = fx;
+                a.f[3 * (size_t)at + 1] = fy;
+                a.f[3 * (size_t)at + 2] = fz;
+                const double eat = a.afrho[at] + 0.5 * ef;
+                a.en_force[at] = eat;
+                sef += eat;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) sv[q] += v[q] * (kFixUnit * kFixUnit);
+                double rx, ry, rz;
+                pair_u(b, fx, fy, fz, rx, ry, rz);
+                sfm = fmax(sfm, sqrt(rx * rx + ry * ry + rz * rz));
+            }
+        }
+        // 4. the system's sums (block reductions in a fixed order)
+        double o[13];
+        o[0] = 0.0;
+        o[1] = block_sum(sef, shr);
+        o[2] = block_max(sfm, shr);
+        o[3] = S.vol;
+        double sm[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sm[q] = block_sum(sv[q], shr);
+        const double S9[9] = {sm[0], sm[3], sm[4], sm[3], sm[1], sm[5], sm[4], sm[5], sm[2]};   // S(c, b) at c + 3b
+        for (int p = 0; p < 3; ++p)
+            for (int bb = 0; bb < 3; ++bb)
+                o[4 + p + 3 * bb] = b[p] * S9[3 * bb] + b[p + 3] * S9[1 + 3 * bb] + b[p + 6] * S9[2 + 3 * bb];
+        if (tid == 0)
+            for (int q = 0; q < 13; ++q) a.sysout[13 * (size_t)sid + q] = o[q];
+        __syncthreads();                       // the records are restaged for the next system
+    }
+    if (overflow) { atomicExch(&a.flags[0], 1); atomicMax(&a.flags[1], overflow); }
+    // the last block to finish resets the queue for the next launch
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&a.queue[1], 1) == (int)gridDim.x - 1) {
+            a.queue[0] = 0;
+            a.queue[1] = 0;
+            __threadfence();
         }
     }
 }
@@ -1123,6 +1394,25 @@ class BatchEngine {
     bool ecalc = true;                  // moldy_gpu_batch_force computes energy_calc's energies
     int ready();
     int take_overflow();
+    // persistent evaluation (k_batch_eval): one launch per force call in
+    // mixed precision without energy_calc, when every atom is heavier than
+    // 0.05 and the largest system's records fit in shared memory
+    bool persistent = true;             // use it where it applies
+    int lpa = 2;                        // lanes per atom in its passes (1, 2, 4)
+    bool all_heavy = true;
+    int max_atoms = 0;
+    size_t smem_optin = 0;
+    int32_t *queue = nullptr;           // [0] next system, [1] blocks done
+    bool en_calc_zero = false;          // en_calc holds zeros (no energy_calc since the last clear)
+    size_t eval_smem() const {
+        return std::max((size_t)max_atoms * sizeof(int4), (size_t)kEvalWarps * (size_t)cap * (sizeof(double4) + sizeof(int)));
+    }
+    bool persistent_applies() const {
+        return persistent && mixed && !ecalc && all_heavy && eval_smem() + 8192 <= smem_optin;
+    }
+    int queue_persistent();
+    int eval_times(double *ms2);
+    int evaluate_once(bool with_reduce);
 };
 
 #define BCHECK(call)                                                      \
@@ -1158,7 +1448,7 @@ BatchEngine::~BatchEngine() {
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
                     mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
                     tab_r4f, tab_e2f, tab_aux, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order,
-                    fm_fref, fm_sref, fm_gF, fm_gS, fm_loss, fm_mu, fm_nu, fm_grads};
+                    fm_fref, fm_sref, fm_gF, fm_gS, fm_loss, fm_mu, fm_nu, fm_grads, queue};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_active) cudaFreeHost(host_active);
@@ -1179,6 +1469,7 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     if (prop.major != 10) return set_last_error(MOLDY_ERR_NO_DEVICE, "kernels are built for sm_100a only");
     device = dev;
     nsm = prop.multiProcessorCount;
+    smem_optin = prop.sharedMemPerBlockOptin;
     nsys = n;
     press = p;
     natoms.assign(na, na + n);
@@ -1191,6 +1482,7 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     }
     if (tot > (1LL << 28)) return set_last_error(MOLDY_ERR_CAPACITY, "more than 2^28 atoms in one batch");
     ntot = (int)tot;
+    max_atoms = *std::max_element(na, na + n);
     BCUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
     size_t nt = (size_t)ntot;
     BCHECK(balloc(&sys, n, "systems"));
@@ -1220,6 +1512,8 @@ int BatchEngine::init(int n, const int32_t *na, double p, int dev) {
     BCUDA(cudaMemset(flags, 0, 2 * sizeof(int32_t)), "flags");
     BCHECK(balloc(&stats, 2, "list statistics"));
     BCHECK(balloc(&ntodo, 1, "screen work count"));
+    BCHECK(balloc(&queue, 2, "system queue"));
+    BCUDA(cudaMemset(queue, 0, 2 * sizeof(int32_t)), "system queue");
     BCUDA(cudaMemset(ntodo, 0, sizeof(int32_t)), "screen work count");
     BCUDA(cudaMemset(stats, 0, 2 * sizeof(unsigned long long)), "list statistics");
     BCUDA(cudaMallocHost((void **)&host_active, sizeof(int)), "pinned");
@@ -1265,7 +1559,10 @@ int BatchEngine::set_state(const double *x0, const double *y0, const double *z0,
         BCUDA(cudaMemcpyAsync(stage + 2 * nt, z0, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "z0");
         k_pack<<<(ntot + 255) / 256, 256, 0, stream>>>(ntot, stage, stage + nt, stage + 2 * nt, X);
     }
-    if (m) BCUDA(cudaMemcpyAsync(mass, m, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "mass");
+    if (m) {
+        BCUDA(cudaMemcpyAsync(mass, m, nt * sizeof(double), cudaMemcpyHostToDevice, stream), "mass");
+        all_heavy = *std::min_element(m, m + nt) > 0.05;
+    }
     if (b0) {
         for (int s = 0; s < nsys; ++s) {
             BSys &S = hsys[s];
@@ -1416,6 +1713,7 @@ static void launch_passes_b(const BatchEngine &E, const TileArgs &a, bool with_v
 // list check (and rebuild) and the tile passes for the systems marked active
 void BatchEngine::queue_evaluation(bool with_vir, bool use_mixed, bool ecalc, cudaEvent_t *ev) {
     cudaStream_t s = stream;
+    if (ecalc) en_calc_zero = false;
     if (ev) cudaEventRecord(ev[0], s);
     k_prepare<<<nsys, kPrepThreads, 0, s>>>(sys, X, mass, Xb, cell_of, cell_count, cell_start, cursor, sorted, spos,
                                            stats, todo, ntodo);
@@ -1457,14 +1755,95 @@ int BatchEngine::take_overflow() {
     return h[1];
 }
 
+// The launches of one force evaluation of every system: the persistent
+// launch where it applies, else the list check, tile screen, per-atom passes
+// and (with_reduce) the per-system sums
+int BatchEngine::evaluate_once(bool with_reduce) {
+    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+    ++launches;
+    if (!ecalc && !en_calc_zero) {
+        BCUDA(cudaMemsetAsync(en_calc, 0, (size_t)ntot * sizeof(double), stream), "en_calc");
+        en_calc_zero = true;
+    }
+    if (ecalc) en_calc_zero = false;
+    if (persistent_applies()) return queue_persistent();
+    queue_evaluation(true, mixed, ecalc);
+    if (with_reduce) {
+        k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
+        ++launches;
+    }
+    return MOLDY_OK;
+}
+
+template <int LPH, int LPA>
+static int launch_eval(BatchEngine &E, const EvalArgs &a, size_t smem, cudaStream_t s) {
+    auto kern = k_batch_eval<LPH, LPA>;
+    BCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "eval smem");
+    int per_sm = 0;
+    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEvalThreads, smem), "eval occupancy");
+    const int nb = std::max(1, std::min(E.nsys, std::max(1, per_sm) * E.nsm));
+    kern<<<nb, kEvalThreads, smem, s>>>(a, E.tab);
+    return MOLDY_OK;
+}
+
+template <int LPH>
+static int launch_eval_l(BatchEngine &E, const EvalArgs &a, size_t smem, cudaStream_t s) {
+    switch (E.lpa) {
+        case 1: return launch_eval<LPH, 1>(E, a, smem, s);
+        case 4: return launch_eval<LPH, 4>(E, a, smem, s);
+        default: return launch_eval<LPH, 2>(E, a, smem, s);
+    }
+}
+
+int BatchEngine::queue_persistent() {
+    EvalArgs a;
+    a.sys = sys; a.order = cg_order; a.nsys = nsys; a.ntot = ntot; a.pair_cap = pair_cap; a.queue = queue;
+    a.X = X; a.mass = mass; a.Xb = Xb; a.cell_of = cell_of; a.cell_count = cell_count; a.cell_start = cell_start;
+    a.cursor = cursor; a.sorted = sorted; a.spos = spos; a.stats = stats; a.cell_sys = cell_sys;
+    a.alist = alist; a.pcnt = pcnt; a.flags = flags; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
+    a.f = f; a.rho = rho; a.afrho = afrho; a.fp = fp; a.en_force = en_force; a.sysout = sysout;
+    const size_t smem = eval_smem();
+    ++launches;
+    switch (lph) {
+        case 4: return launch_eval_l<4>(*this, a, smem, stream);
+        case 16: return launch_eval_l<16>(*this, a, smem, stream);
+        case 32: return launch_eval_l<32>(*this, a, smem, stream);
+        default: return launch_eval_l<8>(*this, a, smem, stream);
+    }
+}
+
+// Device times of the persistent evaluation: ms2[0] with every list current,
+// ms2[1] with every list rebuilt (binning and compact rows in the same launch)
+int BatchEngine::eval_times(double *ms2) {
+    BCHECK(ready());
+    if (!persistent_applies())
+        return set_last_error(MOLDY_ERR_UNSUPPORTED, "the persistent evaluation does not apply (FP64, energy_calc, "
+                                                     "an atom of mass <= 0.05, or a system too large)");
+    cudaEvent_t e0, e1;
+    BCUDA(cudaEventCreate(&e0), "event");
+    BCUDA(cudaEventCreate(&e1), "event");
+    for (int r = 0; r < 2; ++r) {
+        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, r);
+        ++launches;
+        cudaEventRecord(e0, stream);
+        BCHECK(queue_persistent());
+        cudaEventRecord(e1, stream);
+        BCUDA(cudaEventSynchronize(e1), "eval times");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms2) ms2[r] = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BCUDA(cudaGetLastError(), "eval times");
+    if (take_overflow() != 0) return set_last_error(MOLDY_ERR_CAPACITY, "compact rows grew; time again");
+    return MOLDY_OK;
+}
+
 int BatchEngine::force(double *out13) {
     BCHECK(ready());
     for (int attempt = 0;; ++attempt) {
-        k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
-        if (!ecalc) BCUDA(cudaMemsetAsync(en_calc, 0, (size_t)ntot * sizeof(double), stream), "en_calc");
-        queue_evaluation(true, mixed, ecalc);
-        k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
-        launches += 2;
+        BCHECK(evaluate_once(true));
         BCUDA(cudaStreamSynchronize(stream), "batch force");
         BCUDA(cudaGetLastError(), "batch force");
         int ov = take_overflow();
@@ -1480,10 +1859,12 @@ int BatchEngine::force(double *out13) {
 // Chooses the tile shape and the gather width on the live configuration:
 // the lanes per home atom of the tile screen (4, 8, 16, 32) by evaluations
 // that rebuild every list, then the row entries gathered at a time by the
-// per-atom passes (1, 2, 4) by evaluations with current lists, each the mean
-// of nreps evaluations in the current precision.  times_ms (7 values) gets
-// those means in that order, chosen (2 values) the choice.  Positions and
-// boxes are left as they were; the lists are current afterwards.
+// per-atom passes (1, 2, 4) by evaluations with current lists, then, where
+// the persistent evaluation applies, its lanes per atom (1, 2, 4), each the
+// mean of nreps evaluations in the current precision.  times_ms (10 values)
+// gets those means in that order, chosen (3 values) the choice (lanes per
+// atom 0 when not tuned).  Positions and boxes are left as they were; the
+// lists are current afterwards.
 int BatchEngine::autotune(int nreps, double *times_ms, int32_t *chosen) {
     BCHECK(ready());
     if (nreps < 1) nreps = 1;
@@ -1530,14 +1911,46 @@ int BatchEngine::autotune(int nreps, double *times_ms, int32_t *chosen) {
         if (t[4 + k] < t[4 + bg]) bg = k;
     }
     gather = gathers[bg];
+    // lanes per atom of the persistent evaluation (lists current)
+    double tp[3] = {0.0, 0.0, 0.0};
+    const bool pers = persistent_applies();
+    if (pers) {
+        const int lanes_a[3] = {1, 2, 4};
+        int bp = 0;
+        for (int k = 0; k < 3; ++k) {
+            lpa = lanes_a[k];
+            // one untimed launch first: the variant's first launch also loads it
+            k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+            ++launches;
+            BCHECK(queue_persistent());
+            double total = 0.0;
+            for (int r = 0; r < nreps; ++r) {
+                k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+                ++launches;
+                cudaEventRecord(e0, stream);
+                BCHECK(queue_persistent());
+                cudaEventRecord(e1, stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                total += ms;
+            }
+            tp[k] = total / nreps;
+            if (tp[k] < tp[bp]) bp = k;
+        }
+        lpa = lanes_a[bp];
+    }
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     BCUDA(cudaStreamSynchronize(stream), "autotune");
     BCUDA(cudaGetLastError(), "autotune");
     if (take_overflow() != 0) return set_last_error(MOLDY_ERR_CAPACITY, "compact rows grew during tuning; run again");
-    if (times_ms) for (int k = 0; k < 7; ++k) times_ms[k] = t[k];
-    if (chosen) { chosen[0] = lph; chosen[1] = gather; }
+    if (times_ms) {
+        for (int k = 0; k < 7; ++k) times_ms[k] = t[k];
+        for (int k = 0; k < 3; ++k) times_ms[7 + k] = tp[k];
+    }
+    if (chosen) { chosen[0] = lph; chosen[1] = gather; chosen[2] = pers ? lpa : 0; }
     return MOLDY_OK;
 }
 
@@ -1899,6 +2312,32 @@ int moldy_gpu_batch_set_precision(moldy_batch *h, int32_t mixed) {
     if (mixed != 0 && mixed != 1) return moldy::set_last_error(MOLDY_ERR_INVALID, "mixed must be 0 or 1");
     h->e->mixed = mixed == 1;
     return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_persistent(moldy_batch *h, int32_t enable) {
+    BGUARD(h);
+    h->e->persistent = enable != 0;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_set_atom_lanes(moldy_batch *h, int32_t lanes) {
+    BGUARD(h);
+    if (lanes != 1 && lanes != 2 && lanes != 4)
+        return moldy::set_last_error(MOLDY_ERR_INVALID, "lanes per atom must be 1, 2 or 4");
+    h->e->lpa = lanes;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_persistent_applies(moldy_batch *h, int32_t *applies) {
+    BGUARD(h);
+    if (!applies) return moldy::set_last_error(MOLDY_ERR_INVALID, "null pointer");
+    *applies = h->e->persistent_applies() ? 1 : 0;
+    return MOLDY_OK;
+}
+
+int moldy_gpu_batch_eval_times(moldy_batch *h, double *ms2) {
+    BGUARD(h);
+    BTRY(h->e->eval_times(ms2));
 }
 
 int moldy_gpu_batch_set_gather(moldy_batch *h, int32_t entries) {

@@ -290,6 +290,7 @@ def test_batch_autotune_and_energy_calc_switch(gpu_lib, precision):
     ws = mixed_systems([4, 5, 6, 7, 9, 4, 5], seed=21)
     b = MoldyBatch.from_workloads(ws)
     b.set_precision(precision)
+    b.set_persistent(False)     # the per-pass launches throughout (the persistent one has its own tests)
     out0 = b.force()
     f0 = b.forces()
     tune = b.autotune(nreps=2)
@@ -311,4 +312,77 @@ def test_batch_autotune_and_energy_calc_switch(gpu_lib, precision):
     assert set(kt) == {"prepare", "tile_screen", "density", "forces"} and all(v > 0 for v in kt.values())
     assert np.array_equal(b.forces(), f0)
     assert 10 * b.ntot < b.row_entries() < 40 * b.ntot
+    b.close()
+
+
+def test_batch_persistent_evaluation(gpu_lib, oracle_mod):
+    """The persistent launch (mixed, energy_calc off): every system against the
+    oracle at the mixed path's accuracy gate, and against the per-pass mixed
+    launches, for 1, 2 and 4 lanes per atom; two evaluations bit for bit the
+    same; lists rebuilt inside the launch (after a new skin) give the same
+    results as the per-pass path's rebuild; a massless atom, FP64 or
+    energy_calc switch it off."""
+    ws = mixed_systems([4, 5, 6, 7, 9, 4, 5, 8], seed=23)
+    b = MoldyBatch.from_workloads(ws)
+    b.set_precision("mixed")
+    b.set_energy_calc(False)
+    assert b.persistent_applies()
+    ref = []
+    for w in ws:
+        o, _ = oracle_eval(oracle_mod, w)
+        ref.append((o.forces(), o.density()["rho"], o.force_out()))
+    b.set_persistent(False)
+    outp = b.force()
+    fp_ = b.forces()
+    b.set_persistent(True)
+    for lanes in (1, 2, 4):
+        b.set_atom_lanes(lanes)
+        l0 = b.launches()
+        out = b.force()
+        assert b.launches() - l0 == 2          # the activity flags and the evaluation
+        f = b.forces()
+        rho = b.split(b.density()["rho"])
+        for s, w in enumerate(ws):
+            fo, rho_o, fout = ref[s]
+            assert rel_norm_err(rho[s], rho_o) <= 1e-6, (lanes, s)
+            assert abs(out["pe"][s] - fout["pe"]) <= 1e-6 * w.nm, (lanes, s)
+            assert rel_norm_err(out["tp"][s], fout["tp"]) <= 1e-5, (lanes, s)
+            assert out["vol"][s] == outp["vol"][s]
+        assert real_force_rms(ws, b.split(f), [r[0] for r in ref]) <= 1e-5, lanes
+        assert rel_norm_err(f, fp_) <= 1e-6, lanes
+        assert np.all(out["pe_calc"] == 0.0)
+        out_again = b.force()
+        assert np.array_equal(b.forces(), f)
+        for k in ("pe", "tp", "fmax"):
+            assert np.array_equal(out_again[k], out[k]), k
+    # rebuilds inside the launch: a new skin marks every list stale
+    b.set_atom_lanes(2)
+    st0 = b.list_stats()
+    b.set_skin(0.25)
+    b.force()
+    assert b.list_stats()["builds"] - st0["builds"] == len(ws)
+    f_rb = b.forces()
+    e_rb = b.energies()[1]
+    rows_rb = b.row_entries()
+    b.set_persistent(False)
+    b.set_skin(0.25)
+    b.force()
+    assert b.row_entries() == rows_rb
+    assert rel_norm_err(f_rb, b.forces()) <= 1e-6
+    assert rel_norm_err(e_rb, b.energies()[1]) <= 1e-6
+    b.set_persistent(True)
+    t = b.eval_times()
+    assert t["current"] > 0 and t["rebuilt"] > 0
+    tune = b.autotune(nreps=1)
+    assert tune["chosen"]["atom_lanes"] in (1, 2, 4) and set(tune["atom_lanes_ms"]) == {1, 2, 4}
+    b.set_energy_calc(True)
+    assert not b.persistent_applies()
+    b.set_energy_calc(False)
+    b.set_precision("fp64")
+    assert not b.persistent_applies()
+    b.set_precision("mixed")
+    m = np.full(b.ntot, 55.845)
+    m[3] = 0.0
+    b.set_state(mass=m)
+    assert not b.persistent_applies()
     b.close()
