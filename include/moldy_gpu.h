@@ -382,8 +382,10 @@ int moldy_gpu_batch_kernel_times(moldy_batch *h, int32_t rebuild, double *ms4);
  * takes the systems in descending size from a device queue; per system the
  * block checks (and rebuilds) the list, stages the atoms in shared memory as
  * fixed-point records and runs the density and force passes with `lanes`
- * lanes per atom, then the per-system sums.  enable = 0 keeps the per-pass
- * launches (default 1). */
+ * lanes per atom, then the per-system sums.  The launch (with the kernel that
+ * marks every system active) is captured once in a CUDA graph and replayed;
+ * it is captured again when the tile or lane choices or a buffer change.
+ * enable = 0 keeps the per-pass launches (default 1). */
 int moldy_gpu_batch_set_persistent(moldy_batch *h, int32_t enable);
 /* Lanes per atom in the persistent evaluation's passes: 1, 2 or 4 (default 2;
  * moldy_gpu_batch_autotune chooses). */

@@ -1404,13 +1404,22 @@ class BatchEngine {
     size_t smem_optin = 0;
     int32_t *queue = nullptr;           // [0] next system, [1] blocks done
     bool en_calc_zero = false;          // en_calc holds zeros (no energy_calc since the last clear)
+    int eval_grid = 0;                  // resident blocks of the persistent launch
+    // the force evaluation's launches (activity flags, persistent evaluation)
+    // captured once and replayed; recaptured when a choice or a buffer changes
+    cudaGraphExec_t fgraph = nullptr;
+    int fg_lph = -1, fg_lpa = -1, fg_cap = -1;
+    void drop_force_graph() {
+        if (fgraph) { cudaGraphExecDestroy(fgraph); fgraph = nullptr; }
+    }
+    int eval_prepare();
     size_t eval_smem() const {
         return std::max((size_t)max_atoms * sizeof(int4), (size_t)kEvalWarps * (size_t)cap * (sizeof(double4) + sizeof(int)));
     }
     bool persistent_applies() const {
         return persistent && mixed && !ecalc && all_heavy && eval_smem() + 8192 <= smem_optin;
     }
-    int queue_persistent();
+    int queue_persistent(bool prepare = true);
     int eval_times(double *ms2);
     int evaluate_once(bool with_reduce);
 };
@@ -1445,6 +1454,7 @@ static int balloc(T **p, size_t n, const char *what) {
 BatchEngine::~BatchEngine() {
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
+    drop_force_graph();
     void *bufs[] = {sys, atom_sys, cell_sys, cell_of, cell_count, cell_start, cursor, sorted, n_active, X, Xb,
                     mass, f, rho, afrho, fp, en_calc, en_force, vir, sfp, sysout, cgv, spos, cg, tab_r4, tab_e2,
                     tab_r4f, tab_e2f, tab_aux, stage, alist, pcnt, flags, stats, todo, ntodo, cg_order,
@@ -1539,6 +1549,7 @@ int BatchEngine::set_fetm(int nv, const double *av, const double *rv, int np, co
     if (rc != MOLDY_OK) return set_last_error(rc, "FETRANSMETAL set-up failed");
     double rcull = 0.0;
     BCHECK(upload_device_tables(ht, &tab_r4, &tab_r4f, &tab_e2, &tab_e2f, &tab_aux, tab, &rcull));
+    drop_force_graph();   // the graph holds the table descriptor and the cut
     // every pair beyond the table cut and the pair function's knots contributes zero
     double r = rcull < 1e150 ? rcull : 0.0;
     for (int i = 0; i < nv; ++i) r = std::max(r, rv[i] * (1.0 + 1e-12));
@@ -1642,6 +1653,7 @@ int BatchEngine::layout() {
         BCHECK(balloc(&cell_start, ncell + 1, "cell_start"));
         BCHECK(balloc(&cursor, ncell, "cursor"));
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        drop_force_graph();
     }
     BCUDA(cudaMemsetAsync(cell_count, 0, ncell * sizeof(int32_t), stream), "cell_count");
     // every build writes atom0 as the first slot of a system's first cell, and
@@ -1750,23 +1762,53 @@ int BatchEngine::take_overflow() {
     if (balloc(&alist, (size_t)ntot * (size_t)need, "compact list") != MOLDY_OK) return -1;
     pair_cap = need;
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    drop_force_graph();
     k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 1);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
     return h[1];
 }
 
 // The launches of one force evaluation of every system: the persistent
-// launch where it applies, else the list check, tile screen, per-atom passes
-// and (with_reduce) the per-system sums
+// launch where it applies (captured with the activity flags in a graph and
+// replayed), else the list check, tile screen, per-atom passes and
+// (with_reduce) the per-system sums
 int BatchEngine::evaluate_once(bool with_reduce) {
-    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
-    ++launches;
     if (!ecalc && !en_calc_zero) {
         BCUDA(cudaMemsetAsync(en_calc, 0, (size_t)ntot * sizeof(double), stream), "en_calc");
         en_calc_zero = true;
     }
     if (ecalc) en_calc_zero = false;
-    if (persistent_applies()) return queue_persistent();
+    if (persistent_applies()) {
+        if (!fgraph || fg_lph != lph || fg_lpa != lpa || fg_cap != cap) {
+            drop_force_graph();
+            BCHECK(eval_prepare());
+            cudaGraph_t g = nullptr;
+            BCUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+            k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+            const int rc = queue_persistent(false);
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (rc != MOLDY_OK || e != cudaSuccess) {
+                cudaGetLastError();
+                if (g) cudaGraphDestroy(g);
+                return rc != MOLDY_OK ? rc
+                                      : set_last_error(MOLDY_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            }
+            e = cudaGraphInstantiate(&fgraph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                fgraph = nullptr;
+                return set_last_error(MOLDY_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+            }
+            fg_lph = lph; fg_lpa = lpa; fg_cap = cap;
+            launches -= 1;   // captured, not run; counted per replay below
+        }
+        BCUDA(cudaGraphLaunch(fgraph, stream), "graph launch");
+        launches += 2;
+        return MOLDY_OK;
+    }
+    k_set_active<<<(nsys + 255) / 256, 256, 0, stream>>>(nsys, sys, 1, 0);
+    ++launches;
     queue_evaluation(true, mixed, ecalc);
     if (with_reduce) {
         k_sys_reduce<<<nsys, kCgThreads, 0, stream>>>(sys, en_calc, en_force, vir, f, 1, sysout);
@@ -1775,41 +1817,45 @@ int BatchEngine::evaluate_once(bool with_reduce) {
     return MOLDY_OK;
 }
 
-template <int LPH, int LPA>
-static int launch_eval(BatchEngine &E, const EvalArgs &a, size_t smem, cudaStream_t s) {
-    auto kern = k_batch_eval<LPH, LPA>;
-    BCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "eval smem");
-    int per_sm = 0;
-    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEvalThreads, smem), "eval occupancy");
-    const int nb = std::max(1, std::min(E.nsys, std::max(1, per_sm) * E.nsm));
-    kern<<<nb, kEvalThreads, smem, s>>>(a, E.tab);
-    return MOLDY_OK;
-}
+using EvalKernel = void (*)(EvalArgs, Tables);
 
 template <int LPH>
-static int launch_eval_l(BatchEngine &E, const EvalArgs &a, size_t smem, cudaStream_t s) {
-    switch (E.lpa) {
-        case 1: return launch_eval<LPH, 1>(E, a, smem, s);
-        case 4: return launch_eval<LPH, 4>(E, a, smem, s);
-        default: return launch_eval<LPH, 2>(E, a, smem, s);
+static EvalKernel eval_kernel_l(int lpa) {
+    return lpa == 1 ? k_batch_eval<LPH, 1> : (lpa == 4 ? k_batch_eval<LPH, 4> : k_batch_eval<LPH, 2>);
+}
+
+// the instantiation for the tile screen's lanes per home atom (4 runs as 8)
+// and the lanes per atom
+static EvalKernel eval_kernel(int lph, int lpa) {
+    switch (lph) {
+        case 16: return eval_kernel_l<16>(lpa);
+        case 32: return eval_kernel_l<32>(lpa);
+        default: return eval_kernel_l<8>(lpa);
     }
 }
 
-int BatchEngine::queue_persistent() {
+// shared memory opt-in and resident grid of the current instantiation
+int BatchEngine::eval_prepare() {
+    EvalKernel kern = eval_kernel(lph, lpa);
+    const size_t smem = eval_smem();
+    BCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "eval smem");
+    int per_sm = 0;
+    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEvalThreads, smem), "eval occupancy");
+    eval_grid = std::max(1, std::min(nsys, std::max(1, per_sm) * nsm));
+    return MOLDY_OK;
+}
+
+int BatchEngine::queue_persistent(bool prepare) {
+    if (prepare) BCHECK(eval_prepare());
     EvalArgs a;
     a.sys = sys; a.order = cg_order; a.nsys = nsys; a.ntot = ntot; a.pair_cap = pair_cap; a.queue = queue;
     a.X = X; a.mass = mass; a.Xb = Xb; a.cell_of = cell_of; a.cell_count = cell_count; a.cell_start = cell_start;
     a.cursor = cursor; a.sorted = sorted; a.spos = spos; a.stats = stats; a.cell_sys = cell_sys;
     a.alist = alist; a.pcnt = pcnt; a.flags = flags; a.ncell = ncell; a.cap = cap; a.rc2 = rcut * rcut;
     a.f = f; a.rho = rho; a.afrho = afrho; a.fp = fp; a.en_force = en_force; a.sysout = sysout;
-    const size_t smem = eval_smem();
+    eval_kernel(lph, lpa)<<<eval_grid, kEvalThreads, eval_smem(), stream>>>(a, tab);
     ++launches;
-    switch (lph) {
-        case 4: return launch_eval_l<4>(*this, a, smem, stream);
-        case 16: return launch_eval_l<16>(*this, a, smem, stream);
-        case 32: return launch_eval_l<32>(*this, a, smem, stream);
-        default: return launch_eval_l<8>(*this, a, smem, stream);
-    }
+    return MOLDY_OK;
 }
 
 // Device times of the persistent evaluation: ms2[0] with every list current,
