@@ -61,10 +61,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0)
-    ap.add_argument("--workload", choices=["md", "batch", "adjoint", "liquid", "rdf"], default="md",
+    ap.add_argument("--workload", choices=["md", "batch", "adjoint", "liquid", "rdf", "small"], default="md",
                     help="md: the 2M-atom NPT step (headline); batch: 1024 supercells, force "
                          "evaluations and the CG quench; adjoint: force-matching gradients; liquid: "
-                         "the 1.024M-atom heating ramp 300 -> 2500 K with scalev")
+                         "the 1.024M-atom heating ramp 300 -> 2500 K with scalev; rdf: the structure "
+                         "analysis of the 2M-atom cell; small: the 2000-atom NVE case against the oracle")
     ap.add_argument("--nsys", type=int, default=1024, help="batch: number of supercells")
     ap.add_argument("--nconf", type=int, default=256, help="adjoint: number of configurations")
     ap.add_argument("--adj-engines", type=int, default=4, help="adjoint: engines (host threads) per rank")
@@ -987,6 +988,91 @@ def run_adjoint(args):
     return 0
 
 
+# ------------------------------------------------------------------- small --
+SMALL_METRIC = "atom-steps/s, 2000-atom bcc Fe NVE at 300 K, 100 steps (the reference's CPU-runnable case)"
+
+
+def run_small(args):
+    """The reference's own CPU-sized case (10^3 bcc cells, NVE, 100 steps): the
+    oracle on all host threads, then each GPU path from the same start, timed
+    (after a warm-up on a second copy) and compared with the oracle's final
+    positions and total energy.  One GPU; other ranks exit."""
+    import oracle
+    import torch
+    from moldy_b200 import MoldySystem
+    from moldy_b200 import workloads as wl
+    rank, local_rank, world = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    w = wl.config_small_nve()
+    nsteps = 100
+    oracle.build()
+    nth = oracle.max_threads()
+    o = oracle.from_workload(w, uselookup=True, threads=nth)
+    o.md_init()
+    t0 = time.perf_counter()
+    th_o = [o.md_step() for _ in range(nsteps)]
+    el_o = time.perf_counter() - t0
+    xo = o.get_state()["x0"]
+    o.close()
+    dt_ps = w.meta["dt_fs"] / 1000.0
+    t = np.arange(nsteps) * dt_ps
+
+    def drift(te):
+        return float(np.polyfit(t, np.asarray(te) / w.nm, 1)[0])
+
+    paths = {}
+    clk_summary = None
+    for prec in ("fp64", "mixed"):
+        s = MoldySystem.from_workload(w, precision=prec, device=local_rank)
+        s.linkup()
+        s.md_init()
+        th = s.md_steps(nsteps, thermo=True)
+        xg = s.get_state()["x0"]
+        s.close()
+        d = (xg - xo) - np.round(xg - xo)
+        pos_err = float(np.max(np.linalg.norm(d @ w.b0.T, axis=1)))
+        te_err = float(max(abs(a["te"] - b["te"]) for a, b in zip(th, th_o)) / w.nm)
+        s = MoldySystem.from_workload(w, precision=prec, device=local_rank)
+        s.linkup()
+        s.md_init()
+        s.md_steps(max(args.warmup, 3), thermo=False)
+        stream = torch.cuda.ExternalStream(s.stream_handle(), device=local_rank)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clk:
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.md_steps(nsteps, thermo=False)
+            e1.record(stream)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = int(sum(n for _, n in s.kernel_stats().values()))
+        s.close()
+        paths[prec] = {"value": w.nm * nsteps / (ms / 1000.0), "ms_per_step": ms / nsteps,
+                       "max_position_err_A_after_100_steps": pos_err, "max_te_err_eV_per_atom": te_err,
+                       "nve_drift_eV_per_atom_per_ps": drift([a["te"] for a in th]), "clocks": clk.summary()}
+        clk_summary = clk.summary()
+    m = paths["mixed"]
+    line = {
+        "metric": SMALL_METRIC, "value": m["value"], "unit": UNIT, "n_gpus": 1, "steps": nsteps,
+        "warmup": max(args.warmup, 3), "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded bcc Fe lattice, Gaussian displacements 0.05 A, Maxwell-Boltzmann velocities)",
+        "config": {"workload": w.name, "atoms": w.nm, "ensemble": "NVE", "dt_fs": w.meta["dt_fs"],
+                   "nbrupdate": w.ntcm, "precision": "mixed", "paths": paths,
+                   "note": "2000 atoms fill a few SMs: the step time is launch latency, not bandwidth"},
+        "e2e": None,
+        "cpu_baseline": {"value": w.nm * nsteps / el_o, "unit": UNIT, "cores": nth, "kind": "port",
+                         "sample": f"the same {nsteps} steps by the oracle, {nth} OpenMP threads, {el_o:.2f} s",
+                         "nve_drift_eV_per_atom_per_ps": drift([a["te"] for a in th_o])},
+        "clocks": clk_summary, "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ liquid --
 LIQ_METRIC = "atom-steps/s, 1.024M-atom bcc Fe heated 300 -> 2500 K (NPT, scalev every fs, nbrupdate 20)"
 
@@ -1212,6 +1298,8 @@ def main():
         return run_liquid(args)
     if args.workload == "rdf":
         return run_rdf(args)
+    if args.workload == "small":
+        return run_small(args)
     return run_ours(args)
 
 
