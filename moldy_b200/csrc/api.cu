@@ -646,7 +646,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     E.clear_mid_dirty();
     LAUNCH(E, K_MID, 1, s,
            launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, mode == 1 ? 1 : 0, E.therm_blocks,
-                             E.therm_rec, s));
+                             E.therm_rec, s, E.rec_indexed));
     E.therm_blocks = 0;
     E.therm_rec = nullptr;
     if (rb) {
@@ -655,7 +655,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
         list_ready = true;
     }
     if (ntc == ntcm) ntc = 0;
-    LAUNCH(E, K_MID, 3, s, launch_mid_build(d, p, E.rmid, E.rout, s));   // outer build, finish, filter
+    LAUNCH(E, K_MID, 2, s, launch_mid_build(d, p, E.rmid, E.rout, s));   // outer build, intermediate filter
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     double *pk = d.partials + 2 * (size_t)kMaxBlocks * kPartials;
@@ -826,8 +826,95 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
     // deferred into the drift kernel of step k + 1, which reads both anyway,
     // and finished by the k_mid_decide that follows it.
     bool therm_pending = false;
+    // An ordinary step (the thermo sums of the step before deferred into its
+    // drift, no half-list build or relink, no scalev, not the last step) makes
+    // the same launches with the same arguments throughout a call: it is
+    // captured once into a CUDA graph and replayed.  Its k_mid_decide takes the
+    // thermo record index from the box, which a one-thread kernel sets before
+    // the first replay after any other step.  Not while profiling (the
+    // per-launch events).
+    cudaGraphExec_t step_graph = nullptr;
+    bool graph_failed = prof.on || nsteps < 8, rec_synced = false;
+    long long per_replay[K_COUNT] = {};
     for (int k = 0; k < nsteps; ++k) {
         bool rb = false;
+        {
+            // this step's scalev decision, as made below
+            double tt = thermotimer_ + prm.deltat;
+            bool sv = false;
+            if (tt >= kFemtosecond) {
+                tt = tt - kFemtosecond;
+                sv = nose_ > 0.0;
+            }
+            const bool ordinary = therm_pending && k < nsteps - 1 && !sv && list_ready_ && cells_ready_ &&
+                                  ntc_ != 0 && ntc_ + 1 != ntcm_ && !mid_dirty_;
+            if (ordinary && !graph_failed && !step_graph) {
+                // capture one ordinary step; the host-side state it changes is
+                // put back, and advanced below for every replay
+                CHECK(ensure_active_capacity(0));
+                const int ntc0 = ntc_, kin0 = kin_blocks, tb0 = therm_blocks;
+                double *tr0 = therm_rec;
+                const bool skip0 = skip_rho, dirty0 = mid_dirty_;
+                long long l0[K_COUNT];
+                for (int q = 0; q < K_COUNT; ++q) l0[q] = prof.launches[q];
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
+                int rc = MOLDY_OK;
+                if (e == cudaSuccess) {
+                    LAUNCH(*this, K_DRIFT, 1, stream_,
+                           kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, true,
+                                                     stream_));
+                    therm_blocks = kin_blocks;
+                    therm_rec = thermo ? d.thermo_rec : nullptr;
+                    rec_indexed = 1;
+                    skip_rho = true;
+                    bool rbc = false;
+                    int ntc_c = ntc_;
+                    bool cr = cells_ready_, lr = list_ready_;
+                    rc = queue_force(*this, 1, ntc_c, ntcm_, cr, lr, &rbc, stream_);
+                    e = cudaStreamEndCapture(stream_, &g);
+                }
+                rec_indexed = 0;
+                for (int q = 0; q < K_COUNT; ++q) {
+                    per_replay[q] = prof.launches[q] - l0[q];
+                    prof.launches[q] = l0[q];
+                }
+                ntc_ = ntc0; kin_blocks = kin0; therm_blocks = tb0; therm_rec = tr0; skip_rho = skip0;
+                mid_dirty_ = dirty0;
+                if (rc == MOLDY_OK && e == cudaSuccess && g) e = cudaGraphInstantiate(&step_graph, g, 0);
+                if (g) cudaGraphDestroy(g);
+                if (rc != MOLDY_OK || e != cudaSuccess || !step_graph) {
+                    cudaGetLastError();
+                    if (step_graph) cudaGraphExecDestroy(step_graph);
+                    step_graph = nullptr;
+                    graph_failed = true;
+                }
+            }
+            if (ordinary && step_graph) {
+                if (!rec_synced) {
+                    launch_set_rec_step(d, k - 1, stream_);
+                    rec_synced = true;
+                }
+                cudaError_t e = cudaGraphLaunch(step_graph, stream_);
+                if (e != cudaSuccess) {
+                    cudaGraphExecDestroy(step_graph);
+                    return cuda_fail(e, "md_steps graph launch");
+                }
+                for (int q = 0; q < K_COUNT; ++q) prof.launches[q] += per_replay[q];
+                // the host-side state of the replayed step
+                thermotimer_ = tt;
+                ntc_ = ntc_ + 1;
+                mid_dirty_ = false;
+                therm_blocks = 0;
+                therm_rec = nullptr;
+                skip_rho = false;
+                ntcs[k] = ntc_;
+                rbs[k] = 0;
+                therm_pending = true;
+                continue;
+            }
+            rec_synced = false;
+        }
         LAUNCH(*this, K_DRIFT, 1, stream_,
                kin_blocks = launch_drift(d, prm, d.partials + 2 * (size_t)kMaxBlocks * kPartials, therm_pending,
                                          stream_));
@@ -854,6 +941,7 @@ int Engine::md_steps(int nsteps, moldy_thermo *thermo) {
         if (ntc_ == 0) LAUNCH(*this, K_RELINK, 6, stream_, launch_relink(d, prm, stream_));
         if (scalev) LAUNCH(*this, K_SCALEV, 4, stream_, launch_scalev(d, prm, nose_, rqke_, stream_));
     }
+    if (step_graph) cudaGraphExecDestroy(step_graph);
     CUDA_CHECK(cudaGetLastError(), "md_steps launch");
     if (thermo && nsteps > 0)
         CUDA_CHECK(cudaMemcpyAsync(host_rec_, d.thermo_rec, sizeof(double) * kThermoRec * nsteps,
@@ -899,7 +987,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, nullptr, stream_));
-    LAUNCH(*this, K_MID, 3, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
+    LAUNCH(*this, K_MID, 2, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
         LAUNCH(*this, K_SCREEN, 1, stream_,

@@ -34,7 +34,7 @@ struct BoxState {
     int32_t status;                // nonzero: singular box in a device-side inversion
     int32_t out_rebuild;           // 1: the outer list is rebuilt this step
     int32_t out_builds;            // number of outer-list builds so far
-    int32_t pad2;
+    int32_t rec_step;              // thermo record the next indexed k_mid_decide writes
 };
 
 // Per-launch constant parameters.

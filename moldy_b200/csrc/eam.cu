@@ -272,11 +272,21 @@ k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ 
 // moves.
 __global__ void __launch_bounds__(256)
 k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
-             int apply_box, const double *__restrict__ therm_partials, int therm_nblk, double *__restrict__ rec) {
+             int apply_box, const double *__restrict__ therm_partials, int therm_nblk, double *__restrict__ rec,
+             int rec_indexed) {
     if (therm_nblk > 0) {
         __shared__ double s3[3];
         reduce_partials<3>(therm_partials, therm_nblk, s3);
-        if (threadIdx.x == 0) therm_store(p, *box, s3, rec);
+        if (threadIdx.x == 0) {
+            // rec_indexed: rec is the first record, and the box says which one
+            // this step writes (a replayed step's launches are all alike)
+            double *r = rec;
+            if (rec_indexed) {
+                if (r) r += (size_t)kThermoRec * (size_t)box->rec_step;
+                box->rec_step += 1;
+            }
+            therm_store(p, *box, s3, r);
+        }
     }
     if (threadIdx.x != 0) return;
     BoxState &B = *box;
@@ -344,9 +354,15 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
 }
 
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, double *rec, cudaStream_t s) {
-    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk, rec);
+                       int apply_box, int therm_nblk, double *rec, cudaStream_t s, int rec_indexed) {
+    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk, rec,
+                                   rec_indexed);
 }
+
+__global__ void k_set_rec_step(BoxState *__restrict__ box, int step) { box->rec_step = step; }
+
+// the record index the next indexed k_mid_decide writes
+void launch_set_rec_step(DeviceState &d, int step, cudaStream_t s) { k_set_rec_step<<<1, 1, 0, s>>>(d.box, step); }
 
 // ------------------------------------------------------------- integrator --
 // velocityverlet first half (src/quench_m.F90:574-589): x1_dt2 = x1 + x2;

@@ -236,6 +236,7 @@ class Engine {
     bool skip_rho = false;          // the next evaluation need not store rho (an inner md_steps step)
     int therm_blocks = 0;           // > 0: the last drift took update_therm_avs, for k_mid_decide to finish
     double *therm_rec = nullptr;    // device slot for that step's thermo record (or none)
+    int rec_indexed = 0;            // therm_rec is the first record; the box holds the index
   private:
     bool mid_dirty_ = true;         // the intermediate list must be rebuilt before use
   public:
@@ -292,8 +293,11 @@ void launch_finalize_force(DeviceState &d, const Params &p, const double *part_e
 int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s);
 int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream_t s);
 // therm_nblk > 0: finish the drift kernel's deferred update_therm_avs first
+// rec_indexed: rec is the first thermo record and the box's rec_step says
+// which one this launch writes (then advances it), for replayed steps
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, double *rec, cudaStream_t s);
+                       int apply_box, int therm_nblk, double *rec, cudaStream_t s, int rec_indexed = 0);
+void launch_set_rec_step(DeviceState &d, int step, cudaStream_t s);
 // the outer list from the half list when k_mid_decide asked for it, then the
 // intermediate list from the outer list when it asked for that
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s);

@@ -577,3 +577,32 @@ def test_md_bit_reproducible(gpu_lib, prec):
     for k in ("x0", "x1", "x2", "b0", "b1"):
         assert np.array_equal(a[k], b[k]), k
     assert np.array_equal(fa, fb)
+
+
+@pytest.mark.parametrize("prec,ivol", [("mixed", 0), ("fp64", 1)])
+def test_md_steps_graph_replay_matches_launches(gpu_lib, prec, ivol):
+    """md_steps replays a captured graph for its ordinary steps (the thermo
+    record index kept on the device); with the library's profiling on it
+    launches every kernel itself.  Both give the same state, forces and
+    per-step thermo records bit for bit, over calls that cross half-list
+    rebuilds and relinks (nbrupdate 25) and end on a last step of their own."""
+    from moldy_b200 import MoldySystem
+    w = wl.make_workload(8, sigma=0.1, temperature=1200.0, ivol=ivol, seed=31, nbrupdate=25)
+    runs = []
+    for prof in (True, False):
+        s = MoldySystem.from_workload(w, precision=prec)
+        s.set_profiling(prof)
+        s.linkup()
+        s.md_init()
+        recs = s.md_steps(60, thermo=True) + s.md_steps(13, thermo=True)
+        s.md_steps(9, thermo=False)
+        recs += s.md_steps(30, thermo=True)
+        runs.append((s.get_state(), s.forces(), recs))
+        s.close()
+    (a, fa, ra), (b, fb, rb) = runs
+    for k in ("x0", "x1", "x2", "b0", "b1"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(fa, fb)
+    assert len(ra) == len(rb) == 103
+    for x, y in zip(ra, rb):
+        assert x == y
