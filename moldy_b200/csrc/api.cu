@@ -655,7 +655,7 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
         list_ready = true;
     }
     if (ntc == ntcm) ntc = 0;
-    LAUNCH(E, K_MID, 2, s, launch_mid_build(d, p, E.rmid, E.rout, s));   // outer build, intermediate filter
+    LAUNCH(E, K_MID, 1, s, launch_mid_build(d, p, E.rmid, E.rout, s));   // outer and intermediate builds
     const bool mixed = E.precision() == MOLDY_PREC_MIXED;
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     double *pk = d.partials + 2 * (size_t)kMaxBlocks * kPartials;
@@ -987,7 +987,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, nullptr, stream_));
-    LAUNCH(*this, K_MID, 2, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {
         LAUNCH(*this, K_SCREEN, 1, stream_,

@@ -562,87 +562,76 @@ __device__ __forceinline__ int filter_row(const Params &p, const int32_t *__rest
     return cnt;
 }
 
+// Both builds in one pass, each when k_mid_decide asked for it (the launch
+// returns at once when it asked for neither).  Each atom first refilters its
+// outer row from its own half-list row and its reverse half row (within
+// r_out: own entries, flagged in bit 31, then the reverse ones), then its
+// intermediate row from that outer row (within r_mid), and measures its
+// displacement since the outer build (outdisp2, for the next decision).
+// An atom reads and writes only its own rows, so there are no atomics and
+// every row is the same from run to run; a row longer than its capacity
+// keeps its true count, which the flags (outer) or the screening pass
+// (intermediate) report.
 template <bool FIX>
-__global__ void __launch_bounds__(256)
-k_out_build(Params p, double rout, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
-            const BoxState *__restrict__ box, const int32_t *__restrict__ nlist,
-            const int32_t *__restrict__ numn, const int32_t *__restrict__ rlist,
-            const int32_t *__restrict__ numr, int32_t *__restrict__ olist,
-            int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, int32_t *__restrict__ flags) {
+__global__ void __launch_bounds__(256, 3)
+k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
+             BoxState *__restrict__ box, const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
+             const int32_t *__restrict__ rlist, const int32_t *__restrict__ numr, int32_t *__restrict__ olist,
+             int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, int32_t *__restrict__ mlist,
+             int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
     __shared__ double sb[9];
-    __shared__ float skeep2;
-    __shared__ int sneed;
+    __shared__ float skeep[2];
+    __shared__ int sneed[2];
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    if (threadIdx.x == 0) sneed = box->out_rebuild;
+    if (threadIdx.x == 0) { sneed[0] = box->out_rebuild; sneed[1] = box->mid_rebuild; }
     __syncthreads();
-    if (!sneed) return;
-    if (threadIdx.x == 0) skeep2 = keep_radius2(sb, rout);
+    const bool need_out = sneed[0] != 0, need_mid = sneed[1] != 0;
+    if (!need_out && !need_mid) return;
+    if (threadIdx.x == 0) { skeep[0] = keep_radius2(sb, rout); skeep[1] = keep_radius2(sb, rmid); }
     __syncthreads();
     float bf[9];   // B0, per fixed-point unit when FIX
-#pragma unroll
-    for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
-    const float keep2 = skeep2;
-    const int nm = p.nm, cap = p.out_cap;
-    int over = 0;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const double4 pa = pos[a];
-        const int4 qa = posq[a];
-        int cnt = filter_row<FIX, 8>(p, nlist, numn[a], a, pa, qa, pos, posq, bf, keep2, kOwnBit, olist, cap, 0);
-        cnt = filter_row<FIX, 8>(p, rlist, numr[a], a, pa, qa, pos, posq, bf, keep2, 0, olist, cap, cnt);
-        out_cnt[a] = cnt;
-        if (cnt > cap) over = max(over, cnt);
-        xout[a] = qa;
-    }
-    if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
-}
-
-// The intermediate rows from the outer rows; also the largest displacement
-// since the outer build (outdisp2) for the next decision.  An intermediate
-// row longer than mid_cap keeps its true count in mid_cnt; the screening pass
-// reports it.
-template <bool FIX>
-__global__ void __launch_bounds__(256)
-k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
-            BoxState *__restrict__ box, const int32_t *__restrict__ olist, const int32_t *__restrict__ out_cnt,
-            const int4 *__restrict__ xout, int32_t *__restrict__ mlist,
-            int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild) {
-    __shared__ double sb[9];
-    __shared__ float skeep2;
-    __shared__ int sneed;
-    if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
-    if (threadIdx.x == 0) sneed = box->mid_rebuild;
-    __syncthreads();
-    if (!sneed) return;
-    if (threadIdx.x == 0) skeep2 = keep_radius2(sb, rmid);
-    __syncthreads();
-    float bf[9];   // B0, per fixed-point unit when FIX
-#pragma unroll
-    for (int k = 0; k < 9; ++k) bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
-    const float keep2 = skeep2;
-    const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
     float bq[9];   // B0 per fixed-point unit, for the displacement
 #pragma unroll
-    for (int k = 0; k < 9; ++k) bq[k] = (float)(sb[k] * kFixUnit);
+    for (int k = 0; k < 9; ++k) {
+        bf[k] = (float)(FIX ? sb[k] * kFixUnit : sb[k]);
+        bq[k] = (float)(sb[k] * kFixUnit);
+    }
+    const float keep_out = skeep[0], keep_mid = skeep[1];
+    const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
+    int over = 0;
     float d2 = 0.f;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
-        const int nt = out_cnt[a];
-        const int n = nt < ocap ? nt : ocap;
         const double4 pa = pos[a];
         const int4 qa = posq[a];
-        mid_cnt[a] = filter_row<FIX, 8>(p, olist, n, a, pa, qa, pos, posq, bf, keep2, 0, mlist, mcap, 0);
-        xbuild[a] = qa;
-        d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
+        if (need_out) {
+            int cnt = filter_row<FIX, 8>(p, nlist, numn[a], a, pa, qa, pos, posq, bf, keep_out, kOwnBit, olist,
+                                         ocap, 0);
+            cnt = filter_row<FIX, 8>(p, rlist, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist, ocap, cnt);
+            out_cnt[a] = cnt;
+            if (cnt > ocap) over = max(over, cnt);
+            xout[a] = qa;
+        }
+        if (need_mid) {
+            const int nt = out_cnt[a];
+            const int n = nt < ocap ? nt : ocap;
+            mid_cnt[a] = filter_row<FIX, 8>(p, olist, n, a, pa, qa, pos, posq, bf, keep_mid, 0, mlist, mcap, 0);
+            xbuild[a] = qa;
+            d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
+        }
     }
-    // block maximum, then one atomic per block (non-negative doubles order as their bits)
+    if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
+    if (need_mid) {
+        // block maximum, then one atomic per block (non-negative doubles order as their bits)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-    __shared__ float wmax[8];
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float m = 0.f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
-        atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong((double)m));
+        for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+        __shared__ float wmax[8];
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float m = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+            atomicMax(&box->outdisp2, (unsigned long long)__double_as_longlong((double)m));
+        }
     }
 }
 
@@ -651,20 +640,13 @@ k_mid_build(Params p, double rmid, const double4 *__restrict__ pos, const int4 *
 // resident wave
 void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout, cudaStream_t s) {
     const bool fix = p.ivol == 0 || p.ivol == 1 || p.ivol == 4;
-    int no = grid_blocks(p.nm, 256);
-    if (fix)
-        LAUNCH_WAVE(k_out_build<true>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist, d.numr,
-                    d.olist, d.out_cnt, d.xout, d.flags);
-    else
-        LAUNCH_WAVE(k_out_build<false>, no, s, p, rout, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist, d.numr,
-                    d.olist, d.out_cnt, d.xout, d.flags);
     int nb = grid_blocks(p.nm, 256);
     if (fix)
-        LAUNCH_WAVE(k_mid_build<true>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_cnt, d.xout,
-                    d.mlist, d.mid_cnt, d.xbuild);
+        LAUNCH_WAVE(k_list_build<true>, nb, s, p, rout, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist,
+                    d.numr, d.olist, d.out_cnt, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.flags);
     else
-        LAUNCH_WAVE(k_mid_build<false>, nb, s, p, rmid, d.pos, d.posq, d.box, d.olist, d.out_cnt, d.xout,
-                    d.mlist, d.mid_cnt, d.xbuild);
+        LAUNCH_WAVE(k_list_build<false>, nb, s, p, rout, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist,
+                    d.numr, d.olist, d.out_cnt, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.flags);
 }
 
 // ------------------------------------------------------------ launchers --
