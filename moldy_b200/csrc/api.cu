@@ -170,7 +170,7 @@ Engine::~Engine() {
                     d.znum, d.en_atom, d.ic, d.cell_start, d.cell_atoms, d.cell_pos, d.cell_count,
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
-                    d.pair_cnt, d.olist, d.out_cnt, d.rlist, d.numr, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
+                    d.pair_cnt, d.olist, d.out_cnt, d.rlist, d.numr, d.xout, d.xhalf, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
                     d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -241,6 +241,7 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.rlist, nm * (size_t)p.nnbrs, "reverse half rows"));
     CHECK(dev_alloc(&d.numr, nm, "numr"));
     CHECK(dev_alloc(&d.xout, nm, "xout"));
+    CHECK(dev_alloc(&d.xhalf, nm, "xhalf"));
     CHECK(dev_alloc(&d.mlist, nm * (size_t)p.mid_cap, "intermediate list"));
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
     CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
@@ -265,6 +266,7 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.mid_cnt, 0, nm * sizeof(int32_t)), "memset mid_cnt");
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(int4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.xout, 0, nm * sizeof(int4)), "memset xout");
+    CUDA_CHECK(cudaMemset(d.xhalf, 0, nm * sizeof(int4)), "memset xhalf");
     CUDA_CHECK(cudaMemset(d.flags, 0, 12 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
@@ -641,12 +643,15 @@ static int queue_force(Engine &E, int mode, int &ntc, int ntcm, bool &cells_read
     ntc = ntc + 1;
     const bool rb = (ntc == 1 || !list_ready);
     // mode 1 (velocity Verlet) advances the box here, after the drift kernel;
-    // force calls outside velocity Verlet always rebuild the intermediate list
-    const int force_mid = (mode == 1 && !rb && !E.mid_dirty()) ? 0 : 1;
+    // force calls outside velocity Verlet, and a first or invalidated half
+    // list, always rebuild the outer and intermediate lists; a scheduled
+    // half-list rebuild in velocity Verlet lets k_mid_decide keep them when
+    // they need nothing from it
+    const int force_mid = (mode == 1 && list_ready && !E.mid_dirty()) ? 0 : 1;
     E.clear_mid_dirty();
     LAUNCH(E, K_MID, 1, s,
-           launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, mode == 1 ? 1 : 0, E.therm_blocks,
-                             E.therm_rec, s, E.rec_indexed));
+           launch_mid_decide(d, p, E.rmid, E.rcut, E.rout, force_mid, rb ? 1 : 0, mode == 1 ? 1 : 0,
+                             E.therm_blocks, E.therm_rec, s, E.rec_indexed));
     E.therm_blocks = 0;
     E.therm_rec = nullptr;
     if (rb) {
@@ -986,7 +991,7 @@ int Engine::autotune(int nreps, double *times_ms) {
     }
     const bool mixed = precision_ == MOLDY_PREC_MIXED;
     const int fams[2] = {K_SCREEN, K_PAIR};   // density is fused into the screening pass
-    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, nullptr, stream_));
+    LAUNCH(*this, K_MID, 1, stream_, launch_mid_decide(d, prm, rmid, rcut, rout, 1, 0, 0, 0, nullptr, stream_));
     LAUNCH(*this, K_MID, 1, stream_, launch_mid_build(d, prm, rmid, rout, stream_));
     double *pe = d.partials, *pf = d.partials + (size_t)kMaxBlocks * kPartials;
     auto passes = [&]() {

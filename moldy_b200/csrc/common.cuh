@@ -27,6 +27,9 @@ struct BoxState {
     double th_tgid[9], th_cof[9];  // tg^-1 tgdot and cof(B0)/vol of the box k_therm sees
     double bout[9];                // B0 when the outer list was built
     double dmax_mid, dmax_out;     // rnear |B_build^-1|_F of those builds (0: none)
+    double bhalf[9], dmax_half;    // B0 and rnear |B0^-1|_F at the last half-list build
+    double bhalf_out[9], dmax_half_out;   // the same of the half list the outer list was filtered from
+    unsigned long long halfdisp2;  // max |B0 (x - x_half)|^2 at the last outer build (double bits)
     unsigned long long maxdisp2;   // max |B0 (x - x_build)|^2 of the last drift (double bits)
     unsigned long long outdisp2;   // max |B0 (x - x_out)|^2 at the last intermediate build (double bits)
     int32_t mid_rebuild;           // 1: the intermediate list is rebuilt this step

@@ -272,8 +272,8 @@ k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ 
 // moves.
 __global__ void __launch_bounds__(256)
 k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
-             int apply_box, const double *__restrict__ therm_partials, int therm_nblk, double *__restrict__ rec,
-             int rec_indexed) {
+             int half_build, int apply_box, const double *__restrict__ therm_partials, int therm_nblk,
+             double *__restrict__ rec, int rec_indexed) {
     if (therm_nblk > 0) {
         __shared__ double s3[3];
         reduce_partials<3>(therm_partials, therm_nblk, s3);
@@ -320,7 +320,32 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
     for (int k = 0; k < 9; ++k) db[k] = b0[k] - bb[k];
     const double dmax = B.dmax_mid;
     double shrink = 2.0 * md + frob(db) * dmax;
-    int need = force || !(dmax > 0.0) || !(shrink < rmid - eps - (rcut + eps));
+    // A half-list rebuild this step (half_build) keeps the outer and
+    // intermediate lists when the outer list needs no pair that its own
+    // source half list lacked.  A pair missing from that source was farther
+    // than rnear at the source's build; at the outer build it was farther
+    // than rnear - eps - shrink_h (shrink_h: twice the largest displacement
+    // between the two builds, measured by the outer build, plus the box
+    // change times the source's dmax).  When that is beyond r_out + eps the
+    // pair was left out of the outer list like any pair beyond r_out, and the
+    // outer list's own rule below bounds its approach from then on.
+    bool keep_lists = false;
+    if (half_build) {
+        double dbh[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dbh[k] = B.bout[k] - B.bhalf_out[k];
+        const double dh = sqrt(__longlong_as_double((long long)B.halfdisp2)) * (1.0 + 1.0e-5) + 1.0e-6;
+        const double shrink_h = 2.0 * dh + frob(dbh) * B.dmax_half_out;
+        keep_lists = B.dmax_half_out > 0.0 && B.dmax_out > 0.0 && B.dmax_mid > 0.0 &&
+                     shrink_h < p.rnear - eps - (rout + eps);
+        double hinv[9];
+        const double dh_new = mat_invert(b0, hinv) ? p.rnear * frob(hinv) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) B.bhalf[k] = b0[k];
+        B.dmax_half = dh_new;
+    }
+    const int forced = force || (half_build && !keep_lists);
+    int need = forced || !(dmax > 0.0) || !(shrink < rmid - eps - (rcut + eps));
     int need_out = 0;
     if (need) {
         // The intermediate list is filtered from the outer list, which must
@@ -334,7 +359,7 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
         const double dmaxo = B.dmax_out;
         const double dout = sqrt(__longlong_as_double((long long)B.outdisp2)) * (1.0 + 1.0e-5) + 1.0e-6 + md;
         const double shrink_out = 2.0 * dout + frob(dbo) * dmaxo;
-        need_out = force || !(dmaxo > 0.0) || !(shrink_out < rout - eps - (rmid + 2.0 * eps));
+        need_out = forced || !(dmaxo > 0.0) || !(shrink_out < rout - eps - (rmid + 2.0 * eps));
         double inv[9];
         const double dnew = mat_invert(b0, inv) ? p.rnear * frob(inv) : 0.0;
 #pragma unroll
@@ -343,6 +368,12 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
         B.mid_builds += 1;
         B.outdisp2 = 0ull;   // measured again by the intermediate build
         if (need_out) {
+            // the half list this outer list is filtered from, and the
+            // displacement since that half list's build (measured by the build)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) B.bhalf_out[k] = B.bhalf[k];
+            B.dmax_half_out = B.dmax_half;
+            B.halfdisp2 = 0ull;
 #pragma unroll
             for (int k = 0; k < 9; ++k) B.bout[k] = b0[k];
             B.dmax_out = dnew;
@@ -354,9 +385,10 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
 }
 
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, double *rec, cudaStream_t s, int rec_indexed) {
-    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, apply_box, d.partials, therm_nblk, rec,
-                                   rec_indexed);
+                       int half_build, int apply_box, int therm_nblk, double *rec, cudaStream_t s,
+                       int rec_indexed) {
+    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, half_build, apply_box, d.partials,
+                                   therm_nblk, rec, rec_indexed);
 }
 
 __global__ void k_set_rec_step(BoxState *__restrict__ box, int step) { box->rec_step = step; }

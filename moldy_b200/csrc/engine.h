@@ -58,6 +58,7 @@ struct DeviceState {
     // positions at build time
     int32_t *olist = nullptr, *out_cnt = nullptr;
     int4 *xout = nullptr;                  // fixed-point (posq) snapshot
+    int4 *xhalf = nullptr;                 // fixed-point snapshot at the last half-list build
     // intermediate FULL list: the outer-list pairs within r_mid = r_cut + skin
     // when built, entry-major, mid_cnt[i] entries from slot 0 (bit 31 kept);
     // xbuild holds the positions at build time
@@ -295,8 +296,11 @@ int launch_kinetic(DeviceState &d, const Params &p, double *partials, cudaStream
 // therm_nblk > 0: finish the drift kernel's deferred update_therm_avs first
 // rec_indexed: rec is the first thermo record and the box's rec_step says
 // which one this launch writes (then advances it), for replayed steps
+// half_build: the half list is rebuilt this step (the outer and intermediate
+// lists are kept when the outer list provably needs nothing new from it)
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
-                       int apply_box, int therm_nblk, double *rec, cudaStream_t s, int rec_indexed = 0);
+                       int half_build, int apply_box, int therm_nblk, double *rec, cudaStream_t s,
+                       int rec_indexed = 0);
 void launch_set_rec_step(DeviceState &d, int step, cudaStream_t s);
 // the outer list from the half list when k_mid_decide asked for it, then the
 // intermediate list from the outer list when it asked for that

@@ -245,13 +245,18 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     for (int k = 0; k < 9; ++k) bs[k] = (float)(sb[k] * kFixUnit);
     const int fwd_end = sbase[14], total = sbase[27];
     const int staged = total < kNlStage ? total : kNlStage;
-    // staging: the ids cell by cell (each cell's atoms are contiguous in
-    // cell_atoms), then the records slot by slot, so that each thread has
-    // several independent loads in flight
-#pragma unroll 9
+    // staging: the ids (each cell's atoms are contiguous in cell_atoms):
+    // thread t copies atom t of every cell, 27 independent predicated loads
+    // in flight at once, then the atoms past 64 of crowded cells; then the
+    // records slot by slot, again several independent loads per thread
+#pragma unroll
     for (int sc = 0; sc < 27; ++sc) {
-        const int kb = sbase[sc], n = min(sbase[sc + 1], staged) - kb, st = sstart[sc];
-        for (int i = t; i < n; i += 64) sid[kb + i] = cell_atoms[st + i];
+        const int kb = sbase[sc], n = min(sbase[sc + 1], staged) - kb;
+        if (t < n) sid[kb + t] = cell_atoms[sstart[sc] + t];
+    }
+    for (int sc = 0; sc < 27; ++sc) {
+        const int kb = sbase[sc], n = min(sbase[sc + 1], staged) - kb;
+        for (int i = t + 64; i < n; i += 64) sid[kb + i] = cell_atoms[sstart[sc] + i];
     }
     __syncthreads();
     if (PERIODIC) {
@@ -413,7 +418,23 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     if (over) { atomicExch(&flags[10], 1); atomicMax(&flags[11], over); }
 }
 
+// The box of a half-list build (B0 and rnear |B0^-1|_F) beside the
+// positions' snapshot, for the rule that keeps the outer list across the
+// next half-list rebuild
+__global__ void k_half_box(Params p, BoxState *__restrict__ box) {
+    if (threadIdx.x != 0) return;
+    double b0[9], inv[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b0[k] = box->b0[k];
+    const double dh = mat_invert(b0, inv) ? p.rnear * frob(inv) : 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) box->bhalf[k] = b0[k];
+    box->dmax_half = dh;
+}
+
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s) {
+    cudaMemcpyAsync(d.xhalf, d.posq, (size_t)p.nm * sizeof(int4), cudaMemcpyDeviceToDevice, s);
+    k_half_box<<<1, 32, 0, s>>>(p, d.box);
     if (p.ivol == 0 || p.ivol == 1 || p.ivol == 4)
         k_build_nlist<true><<<p.ncell, 64, 0, s>>>(p, d.pos, d.posq, d.box, d.cell_start, d.cell_count,
                                                    d.cell_atoms, d.nlist, d.numn, d.rlist, d.numr, d.flags);

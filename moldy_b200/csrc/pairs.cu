@@ -577,8 +577,9 @@ __global__ void __launch_bounds__(256, 3)
 k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
              BoxState *__restrict__ box, const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
              const int32_t *__restrict__ rlist, const int32_t *__restrict__ numr, int32_t *__restrict__ olist,
-             int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, int32_t *__restrict__ mlist,
-             int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild, int32_t *__restrict__ flags) {
+             int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, const int4 *__restrict__ xhalf,
+             int32_t *__restrict__ mlist, int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild,
+             int32_t *__restrict__ flags) {
     __shared__ double sb[9];
     __shared__ float skeep[2];
     __shared__ int sneed[2];
@@ -599,11 +600,12 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
     const float keep_out = skeep[0], keep_mid = skeep[1];
     const int nm = p.nm, ocap = p.out_cap, mcap = p.mid_cap;
     int over = 0;
-    float d2 = 0.f;
+    float d2 = 0.f, dh2 = 0.f;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nm; a += gridDim.x * blockDim.x) {
         const double4 pa = pos[a];
         const int4 qa = posq[a];
         if (need_out) {
+            dh2 = fmaxf(dh2, fix_disp2(bq, qa, xhalf[a]));
             int cnt = filter_row<FIX, 8>(p, nlist, numn[a], a, pa, qa, pos, posq, bf, keep_out, kOwnBit, olist,
                                          ocap, 0);
             cnt = filter_row<FIX, 8>(p, rlist, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist, ocap, cnt);
@@ -620,11 +622,24 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
         }
     }
     if (over) { atomicExch(&flags[8], 1); atomicMax(&flags[9], over); }
+    __shared__ float wmax[8], hmax[8];
+    if (need_out) {
+        // the displacement since the source half list's build, block maximum
+        // then one atomic per block
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dh2 = fmaxf(dh2, __shfl_xor_sync(0xffffffffu, dh2, o));
+        if ((threadIdx.x & 31) == 0) hmax[threadIdx.x >> 5] = dh2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float m = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, hmax[w]);
+            atomicMax(&box->halfdisp2, (unsigned long long)__double_as_longlong((double)m));
+        }
+    }
     if (need_mid) {
         // block maximum, then one atomic per block (non-negative doubles order as their bits)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-        __shared__ float wmax[8];
         if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -643,10 +658,10 @@ void launch_mid_build(DeviceState &d, const Params &p, double rmid, double rout,
     int nb = grid_blocks(p.nm, 256);
     if (fix)
         LAUNCH_WAVE(k_list_build<true>, nb, s, p, rout, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist,
-                    d.numr, d.olist, d.out_cnt, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.flags);
+                    d.numr, d.olist, d.out_cnt, d.xout, d.xhalf, d.mlist, d.mid_cnt, d.xbuild, d.flags);
     else
         LAUNCH_WAVE(k_list_build<false>, nb, s, p, rout, rmid, d.pos, d.posq, d.box, d.nlist, d.numn, d.rlist,
-                    d.numr, d.olist, d.out_cnt, d.xout, d.mlist, d.mid_cnt, d.xbuild, d.flags);
+                    d.numr, d.olist, d.out_cnt, d.xout, d.xhalf, d.mlist, d.mid_cnt, d.xbuild, d.flags);
 }
 
 // ------------------------------------------------------------ launchers --
