@@ -171,7 +171,7 @@ Engine::~Engine() {
                     d.ic_new, d.arr_count, d.arr_start, d.arr_list, d.work, d.new_count,
                     d.new_start, d.cell_atoms2, d.nlist, d.numn, d.posq, d.posq2, d.pos2, d.alist,
                     d.pair_cnt, d.olist, d.out_cnt, d.rlist, d.numr, d.xout, d.xhalf, d.mlist, d.mid_cnt, d.xbuild, d.tab_r4, d.tab_e2,
-                    d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.box, d.scan_tmp, d.adj, d.rdf};
+                    d.tab_r4f, d.tab_e2f, d.tab_aux, d.partials, d.flags, d.revmask, d.box, d.scan_tmp, d.adj, d.rdf};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (host_box_) cudaFreeHost(host_box_);
@@ -246,7 +246,8 @@ static int init_engine(Engine &E, int device) {
     CHECK(dev_alloc(&d.mid_cnt, nm, "mid_cnt"));
     CHECK(dev_alloc(&d.xbuild, nm, "xbuild"));
     CHECK(dev_alloc(&d.partials, 3 * (size_t)kMaxBlocks * kPartials, "partials"));
-    CHECK(dev_alloc(&d.flags, 12, "flags"));
+    CHECK(dev_alloc(&d.flags, 16, "flags"));
+    CHECK(dev_alloc(&d.revmask, (size_t)kRevPlanes * nm, "reverse-row masks"));
     CHECK(dev_alloc(&d.box, 1, "box"));
     CUDA_CHECK(cudaMemset(d.pos, 0, nm * sizeof(double4)), "memset pos");
     CUDA_CHECK(cudaMemset(d.x1, 0, 3 * nm * sizeof(double)), "memset x1");
@@ -267,7 +268,7 @@ static int init_engine(Engine &E, int device) {
     CUDA_CHECK(cudaMemset(d.xbuild, 0, nm * sizeof(int4)), "memset xbuild");
     CUDA_CHECK(cudaMemset(d.xout, 0, nm * sizeof(int4)), "memset xout");
     CUDA_CHECK(cudaMemset(d.xhalf, 0, nm * sizeof(int4)), "memset xhalf");
-    CUDA_CHECK(cudaMemset(d.flags, 0, 12 * sizeof(int32_t)), "memset flags");
+    CUDA_CHECK(cudaMemset(d.flags, 0, 16 * sizeof(int32_t)), "memset flags");
     CUDA_CHECK(cudaMemset(d.box, 0, sizeof(BoxState)), "memset box");
     if (p.nlcx > 0 && p.nlcy > 0 && p.nlcz > 0) CHECK(alloc_cells(E));
     return MOLDY_OK;

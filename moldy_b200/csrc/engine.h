@@ -79,7 +79,12 @@ struct DeviceState {
                                   // [2] overflow atom, [3] active-list overflow, [4] its count,
                                   // [5] intermediate-row overflow, [6] its count,
                                   // [8] outer-row overflow, [9] its count,
-                                  // [10] reverse half-row overflow, [11] its count
+                                  // [10] reverse half-row overflow, [11] its count,
+                                  // [12] a link cell too full for the reverse-row masks
+    // per (cell rank r of the half stencil, round of 32 home atoms, atom j):
+    // the home atoms of j's source cell whose half-list rows hold j (one bit
+    // per home atom of the round), written by the half-list build
+    uint32_t *revmask = nullptr;
     BoxState *box = nullptr;
     int32_t *scan_tmp = nullptr;
     // adjoint (allocated on first use): full tables and their gradients
@@ -311,6 +316,8 @@ void launch_md_init_x2(DeviceState &d, const Params &p, cudaStream_t s);
 // rec: where the step's thermo record goes (kThermoRec doubles, device; may be null)
 int launch_therm(DeviceState &d, const Params &p, bool prep, double *rec, cudaStream_t s);
 constexpr int kThermoRec = 11;
+constexpr int kRevRounds = 3;                  // rounds of 32 home atoms the reverse-row masks cover
+constexpr int kRevPlanes = 14 * kRevRounds;
 void launch_energy_calc(DeviceState &d, const Params &p, const Tables &t, cudaStream_t s);
 void launch_scalev(DeviceState &d, const Params &p, double nose, double rqke, cudaStream_t s);
 void launch_count_screened(const DeviceState &d, const Params &p, unsigned long long *out, cudaStream_t s);

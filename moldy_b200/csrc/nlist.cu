@@ -1,19 +1,20 @@
 // nlist.cu -- the hybrid Verlet half list (update_neighbourlist,
 // src/neighbourlist_m.F90:103-276) built on the GPU.
 //
-// One block (two warps) owns one link cell.  It stages the atoms of the 27
-// cells around it in shared memory: the home cell, the 13 further cells of
-// the reference's half stencil in the reference's order (dz in {0,+1}; at
-// dz=0 dy in {0,+1}; at dz=0,dy=0 dx in {0,+1}; otherwise dx,dy in
-// {-1,0,+1}), then the 13 mirror cells, each cell's atoms in chain order.
-// Each lane takes one home atom i; the candidates after i up to the end of
-// the half stencil form NLIST(:, i), entry for entry as the reference's walk
-// appends them, and the others (i's own cell before i, the mirror cells) form
-// i's reverse row, the atoms j with i in NLIST(:, j).  Candidates past the
-// staging capacity are read from global memory.  The lists are stored
-// entry-major (entry k of atom i at k*nm + i) so that the per-step passes, one
-// thread per atom, read them in contiguous 128-byte rows; the export
-// transposes NLIST to the reference's (nnbrs, nm).  The exact distance test
+// One block (two warps) owns one link cell.  It stages the atoms of the
+// reference's half stencil in shared memory: the home cell, then the 13
+// further cells in the reference's order (dz in {0,+1}; at dz=0 dy in {0,+1};
+// at dz=0,dy=0 dx in {0,+1}; otherwise dx,dy in {-1,0,+1}), each cell's
+// atoms in chain order.  Each lane takes one home atom i; the candidates
+// after i form NLIST(:, i), entry for entry as the reference's walk appends
+// them.  Candidates past the staging capacity are read from global memory.
+// Each atom's reverse row (the atoms j with i in NLIST(:, j), i's own cell
+// before i, then the 13 mirror cells, each in chain order) is formed
+// afterwards from the finished rows: a scatter, then a sort of each row by
+// cell and chain position.  The lists are stored entry-major (entry k of
+// atom i at k*nm + i) so that the per-step passes, one thread per atom, read
+// them in contiguous 128-byte rows; the export transposes NLIST to the
+// reference's (nnbrs, nm).  The exact distance test
 // uses separately rounded products and sums (no FMA), as the Fortran
 // evaluates pr_get_realsep_from_dx, so r < rnear gives the same pair set.
 // In a fully periodic box an FP32 distance decides first (from positions
@@ -145,40 +146,61 @@ __device__ __forceinline__ bool nl_take(const NlStage &S, int kk, const double4 
     return nl_exact(S.pos, S.b, S.ivol, S.rnear, pa, j);
 }
 
+// a / b for a >= 0, b > 0: below 2^24 an FP32 quotient corrected by one in
+// either direction (the FP32 estimate is then within one of the true quotient)
+__device__ __forceinline__ int div_small(int a, int b) {
+    if (a >= (1 << 24)) return a / b;
+    int q = __float2int_rz(__fdividef((float)a, (float)b));
+    q -= (q * b > a) ? 1 : 0;
+    q += ((q + 1) * b <= a) ? 1 : 0;
+    return q;
+}
+
 // bits [0, x) of a word, x in [0, 32]
 __device__ __forceinline__ unsigned low_bits(int x) { return x >= 32 ? ~0u : (1u << x) - 1u; }
 
-// Two warps per link cell stage the atoms of the 27 surrounding cells: the
-// home cell, the 13 cells of the reference's half stencil, then the 13 mirror
-// cells, each cell's atoms in chain order.  Each lane then takes one home atom
-// a (the cell's atoms 32 at a time) and, over the staged candidates in order,
-// every lane reading the same candidate (a shared-memory broadcast), builds
-//   row(a)      NLIST(:, a): the half-stencil candidates after a in staging
-//               order, in the reference's order (entry for entry), written by
-//               warp 0;
-//   reverse(a)  the atoms j with a in row(j): a's own cell before a, then the
-//               mirror cells, in staging order, written by warp 1.
-// In the cell-relative form the two warps first test alternate chunks of 32
-// candidates into keep masks (one word per home atom and chunk, in shared
-// memory); then each warp appends the kept candidates of its kind in order.
+// The transpose of a 32x32 bit matrix held one row per lane (bit c of lane
+// l's word is element (l, c)): lane l receives column l.  Five butterfly
+// stages swap blocks of 16, 8, 4, 2 and 1 bits between lanes l and l ^ j.
+__device__ __forceinline__ unsigned transpose_lanes(unsigned x, int lane) {
+    unsigned m = 0x0000ffffu;
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1, m ^= m << j) {
+        const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
+        x = (lane & j) ? (((y >> j) & m) | (x & ~m)) : ((x & m) | ((y & m) << j));
+    }
+    return x;
+}
+
+// Two warps per link cell stage the atoms of the reference's half stencil:
+// the home cell, then the 13 further cells, each cell's atoms in chain order.
+// Each lane then takes one home atom a (the cell's atoms 32 at a time) and,
+// over the staged candidates in order, every lane reading the same candidate
+// (a shared-memory broadcast), builds NLIST(:, a): the candidates after a,
+// in the reference's order (entry for entry).  In the cell-relative form the
+// two warps first test alternate chunks of 32 candidates into keep masks (one
+// word per home atom and chunk, in shared memory); then warp 0 appends the
+// kept candidates of the first half of the chunks and warp 1 those of the
+// second half, from the count of the first half on.  The reverse rows come
+// afterwards from the finished rows (k_rev_scatter, k_rev_sort).
 template <bool PERIODIC>
 __global__ void __launch_bounds__(64, 12)
 k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
               const BoxState *__restrict__ box,
               const int32_t *__restrict__ cell_start, const int32_t *__restrict__ cell_count,
               const int32_t *__restrict__ cell_atoms, int32_t *__restrict__ nlist,
-              int32_t *__restrict__ numn, int32_t *__restrict__ rlist, int32_t *__restrict__ numr,
-              int32_t *__restrict__ flags) {
+              int32_t *__restrict__ numn, uint32_t *__restrict__ revmask, int32_t *__restrict__ flags) {
     // per staged candidate: its fixed-point position (fixed-point form) or
     // (-2c, |c|^2) of its cell-relative Cartesian position c as float bits
     // (cell-relative form), and its atom id
     __shared__ int4 srec[kNlStage];
     __shared__ int sid[kNlStage];
-    // keep masks of each chunk of 32 candidates, per home atom (lane), and
-    // per warp and kind (forward, reverse) the chunks with candidates of
-    // that kind
+    // keep masks of each chunk of 32 candidates (forward candidates only),
+    // per home atom (lane); per warp the chunks with some; warp 1's counts
     __shared__ unsigned smask[kNlChunks][32];
-    __shared__ unsigned snz[2][2][32];
+    __shared__ unsigned snz[2][32];
+    __shared__ int scount[32];
+    __shared__ uint8_t scell[kNlStage];   // half-stencil cell (0..13) of each staged candidate
     __shared__ int sbase[28], sstart[27];
     __shared__ double sb[9];
     __shared__ int4 scen;     // the home cell's centre in fixed point; w: cell-relative form
@@ -190,7 +212,7 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     if (warp == 0) {
         if (lane < 9) sb[lane] = box->b0[lane];
         int cnt = 0, st = 0;
-        if (lane < 27) {
+        if (lane < 14) {   // the home cell and the 13 further cells of the half stencil
             const int jx = wrap(cx + c_stencil[lane][0], p.nlcx);
             const int jy = wrap(cy + c_stencil[lane][1], p.nlcy);
             const int jz = wrap(cz + c_stencil[lane][2], p.nlcz);
@@ -205,7 +227,7 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
             const int v = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= o) inc += v;
         }
-        if (lane < 27) { sbase[lane + 1] = inc; sstart[lane] = st; }
+        if (lane < 14) { sbase[lane + 1] = inc; sstart[lane] = st; }
         if (lane == 0) sbase[0] = 0;
         __syncwarp();
         if (PERIODIC) {
@@ -243,21 +265,24 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     float bs[9];   // B0 per fixed-point unit
 #pragma unroll
     for (int k = 0; k < 9; ++k) bs[k] = (float)(sb[k] * kFixUnit);
-    const int fwd_end = sbase[14], total = sbase[27];
+    const int fwd_end = sbase[14], total = fwd_end;
     const int staged = total < kNlStage ? total : kNlStage;
     // staging: the ids (each cell's atoms are contiguous in cell_atoms):
     // thread t copies atom t of every cell, 27 independent predicated loads
     // in flight at once, then the atoms past 64 of crowded cells; then the
     // records slot by slot, again several independent loads per thread
 #pragma unroll
-    for (int sc = 0; sc < 27; ++sc) {
+    for (int sc = 0; sc < 14; ++sc) {
         const int kb = sbase[sc], n = min(sbase[sc + 1], staged) - kb;
-        if (t < n) sid[kb + t] = cell_atoms[sstart[sc] + t];
+        if (t < n) { sid[kb + t] = cell_atoms[sstart[sc] + t]; scell[kb + t] = (uint8_t)sc; }
     }
-    for (int sc = 0; sc < 27; ++sc) {
+    for (int sc = 0; sc < 14; ++sc) {
         const int kb = sbase[sc], n = min(sbase[sc + 1], staged) - kb;
-        for (int i = t + 64; i < n; i += 64) sid[kb + i] = cell_atoms[sstart[sc] + i];
+        for (int i = t + 64; i < n; i += 64) { sid[kb + i] = cell_atoms[sstart[sc] + i]; scell[kb + i] = (uint8_t)sc; }
     }
+    // more home atoms than the reverse-row masks hold: the reverse rows are
+    // formed by the scatter-and-sort path instead
+    if (t == 0 && L0 > 32 * kRevRounds) atomicExch(&flags[12], 1);
     __syncthreads();
     if (PERIODIC) {
 #pragma unroll 5
@@ -291,7 +316,6 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
     const size_t nm = (size_t)p.nm;
     const int cap = p.nnbrs;
     const bool fwd_warp = warp == 0;
-    int over = 0;
     for (int q0 = 0; q0 < L0; q0 += 32) {
         if (q0 > 0) __syncthreads();             // the previous round's masks are read
         const int q = q0 + lane;                 // this lane's home atom: staged slot q
@@ -316,43 +340,63 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
                 qa = home_staged ? srec[q] : posq[a];
             }
         }
-        // this warp's row of a: entry n at base[n * nm] (entry-major)
-        int32_t *const base = (fwd_warp ? nlist : rlist) + a;
+        // the row of a: entry n at base[n * nm] (entry-major)
+        int32_t *const base = nlist + a;
         int n = 0;
         int kk = 0;
         if (rel && min(L0, q0 + 32) <= staged) {   // every live lane's home atom staged
             const int nch = (staged + 31) >> 5;
-            // keep masks against r < rnear + band: warp w tests chunks w, w + 2, ...,
-            // and splits each mask into the forward candidates (q, fwd_end) and the rest
-            const float thi = S.rhi2 - a2, tlo = S.rlo2 - a2;
-            unsigned nzf = 0u, nzr = 0u;
+            // keep masks of the candidates after q: warp w tests chunks w,
+            // w + 2, ... into those below rnear + band (m) and below rnear -
+            // band (mlo); the exact test settles those in between here, so the
+            // masks hold the final pairs
+            const float thi = S.rhi2 - a2, dlt = S.rhi2 - S.rlo2;
+            unsigned nzf = 0u;
             for (int ch = warp; ch < nch; ch += 2) {
                 const int k0 = ch << 5;
-                unsigned m = 0u;
+                unsigned m = 0u, mlo = 0u;
 #pragma unroll
                 for (int b = 0; b < 32; ++b) {
                     const int4 rec = srec[k0 + b];
+                    // s = r^2 - (rnear + band)^2
                     const float s = fmaf(ar.z, __int_as_float(rec.z),
                                          fmaf(ar.y, __int_as_float(rec.y),
                                               fmaf(ar.x, __int_as_float(rec.x), __int_as_float(rec.w) - thi)));
-                    m = __funnelshift_l(__float_as_uint(s), m, 1);   // (m << 1) | sign(s)
+                    m = __funnelshift_l(__float_as_uint(s), m, 1);            // (m << 1) | sign(s)
+                    mlo = __funnelshift_l(__float_as_uint(s + dlt), mlo, 1);
                 }
-                m = __brev(m);                                       // bit b: candidate k0 + b
-                const unsigned self = (q >= k0 && q < k0 + 32) ? (1u << (q - k0)) : 0u;
-                m = live ? m & ~self : 0u;
-                const unsigned fw = low_bits(min(max(fwd_end - k0, 0), 32)) & ~low_bits(min(max(q + 1 - k0, 0), 32));
+                const unsigned after = ~low_bits(min(max(q + 1 - k0, 0), 32));
+                m = live ? __brev(m) & after : 0u;                           // bit b: candidate k0 + b
+                unsigned band = m & ~__brev(mlo);
+                while (band) {                                               // rare
+                    const int b = __ffs(band) - 1;
+                    band &= band - 1u;
+                    if (!nl_exact(pos, sb, p.ivol, p.rnear, pa, sid[k0 + b])) m &= ~(1u << b);
+                }
                 smask[ch][lane] = m;
-                nzf |= (m & fw) ? 1u << ch : 0u;
-                nzr |= (m & ~fw) ? 1u << ch : 0u;
+                nzf |= m ? 1u << ch : 0u;
             }
-            snz[warp][0][lane] = nzf;
-            snz[warp][1][lane] = nzr;
+            snz[warp][lane] = nzf;
             __syncthreads();
-            // appends: warp 0 the forward candidates, warp 1 the rest.  Each
-            // lane walks its kept candidates over all chunks in one loop, so
-            // the warp runs as many iterations as its longest row takes
-            const int kind = fwd_warp ? 0 : 1;
-            unsigned chunks = snz[0][kind][lane] | snz[1][kind][lane];
+            // for each staged candidate j, the home atoms of this round whose
+            // rows hold it: the chunk's keep bits transposed across the lanes
+            const int round = q0 >> 5;
+            if (round < kRevRounds) {
+                for (int ch = warp; ch < nch; ch += 2) {
+                    const int k = (ch << 5) + lane;
+                    const unsigned colm = transpose_lanes(smask[ch][lane], lane);
+                    if (k < staged)
+                        revmask[(size_t)(scell[k] * kRevRounds + round) * nm + sid[k]] = colm;
+                }
+            }
+            // appends: warp 0 the chunks [0, mid), warp 1 the chunks [mid,
+            // nch) from the count of warp 0's entries on.  Each lane walks its
+            // kept candidates over its chunks in one loop, so the warp runs
+            // as many iterations as its longest share of a row takes
+            const int mid = (nch + 1) >> 1;
+            unsigned chunks = (snz[0][lane] | snz[1][lane]) & (fwd_warp ? low_bits(mid) : ~low_bits(mid));
+            if (!fwd_warp)
+                for (int ch = 0; ch < mid; ++ch) n += __popc(smask[ch][lane]);
             unsigned m = 0u;
             int k0 = 0;
             while (m | chunks) {
@@ -360,62 +404,170 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
                     const int ch = __ffs(chunks) - 1;
                     chunks &= chunks - 1u;
                     k0 = ch << 5;
-                    const unsigned fw = low_bits(min(max(fwd_end - k0, 0), 32)) & ~low_bits(min(max(q + 1 - k0, 0), 32));
-                    m = smask[ch][lane] & (kind == 0 ? fw : ~fw);
+                    m = smask[ch][lane];
                 }
                 const int k = k0 + __ffs(m) - 1;
                 m &= m - 1u;
-                const int4 rec = srec[k];
-                const float s = fmaf(ar.z, __int_as_float(rec.z),
-                                     fmaf(ar.y, __int_as_float(rec.y),
-                                          fmaf(ar.x, __int_as_float(rec.x), __int_as_float(rec.w) - tlo)));
-                const int j = sid[k];
-                // r >= rnear - band: in the band, the exact test decides
-                if (!(s < 0.f) && !nl_exact(pos, sb, p.ivol, p.rnear, pa, j)) continue;
-                if (n < cap) base[(size_t)n * nm] = j;
+                if (n < cap) base[(size_t)n * nm] = sid[k];
                 ++n;
             }
+            // warp 1's count is the row's
+            if (!fwd_warp) scount[lane] = n;
+            __syncthreads();
+            n = scount[lane];
             kk = staged;
         }
         // the rest: candidates beyond the staging, every candidate of the
-        // fixed-point form and of boxes not periodic in all three directions;
-        // each warp tests the candidates of its own row
+        // fixed-point form and of boxes not periodic in all three directions
         if (fwd_warp) {
-            for (int k = max(kk, q0 + 1); k < fwd_end; ++k) {
+            const int round = q0 >> 5;
+            for (int k = kk; k < fwd_end; ++k) {
                 int j = 0;
                 const bool take = live && k > q && nl_take<PERIODIC>(S, k, pa, qa, ar, rel, cen, j);
                 if (take && n < cap) base[(size_t)n * nm] = j;
                 n += take ? 1 : 0;
+                // this candidate's column of the reverse-row masks
+                const unsigned colm = __ballot_sync(0xffffffffu, take);
+                if (lane == 0 && round < kRevRounds) {
+                    int sc = 0;
+                    while (sbase[sc + 1] <= k) ++sc;
+                    const int jk = k < staged ? sid[k] : cell_atoms[sstart[sc] + (k - sbase[sc])];
+                    revmask[(size_t)(sc * kRevRounds + round) * nm + jk] = colm;
+                }
             }
-        } else {
-            // a's own cell before a, then the mirror cells
-            for (int k = kk; k < min(q0 + 31, fwd_end); ++k) {
-                int j = 0;
-                const bool take = live && k < q && nl_take<PERIODIC>(S, k, pa, qa, ar, rel, cen, j);
-                if (take && n < cap) base[(size_t)n * nm] = j;
-                n += take ? 1 : 0;
-            }
-            for (int k = max(kk, fwd_end); k < total; ++k) {
-                int j = 0;
-                const bool take = live && nl_take<PERIODIC>(S, k, pa, qa, ar, rel, cen, j);
-                if (take && n < cap) base[(size_t)n * nm] = j;
-                n += take ? 1 : 0;
-            }
-        }
-        if (live) {
-            if (fwd_warp) {
+            if (live) {
                 numn[a] = n < cap ? n : cap;
                 if (n > cap) {
                     atomicExch(&flags[0], 1);
                     atomicMax(&flags[2], a + 1);
                 }
-            } else {
-                numr[a] = n < cap ? n : cap;
-                if (n > cap) over = max(over, n);
             }
         }
     }
-    if (over) { atomicExch(&flags[10], 1); atomicMax(&flags[11], over); }
+}
+
+// Reverse rows: row j holds the atoms i with j in NLIST(:, i) -- j's own cell
+// first, then the 13 mirror cells of the half stencil in order, each cell in
+// chain order, the order in which a full-stencil walk from j's cell meets them.
+// The half-list build leaves, per atom j and half-stencil rank r, the home
+// atoms of the source cell (j's cell minus forward offset r) whose rows hold
+// j, as bits over the source cell's chain positions (32 per round); one thread
+// per atom expands them in rank, round and bit order.  A link cell fuller
+// than the masks hold (flag 12) leaves the rows to the scatter-and-sort path.
+__global__ void __launch_bounds__(256)
+k_rev_gather(Params p, const int32_t *__restrict__ ic, const int32_t *__restrict__ cell_start,
+             const int32_t *__restrict__ cell_count, const int32_t *__restrict__ cell_atoms,
+             const uint32_t *__restrict__ revmask, int32_t *__restrict__ rlist, int32_t *__restrict__ numr,
+             int32_t *__restrict__ flags) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.nm) return;
+    if (flags[12]) {   // the fallback counts from zero
+        numr[j] = 0;
+        return;
+    }
+    const size_t nm = (size_t)p.nm;
+    const int cap = p.nnbrs;
+    const int cj = ic[j];
+    const int nxy = p.nlcx * p.nlcy;
+    const int jz = div_small(cj, nxy), rxy = cj - jz * nxy;
+    const int jy = div_small(rxy, p.nlcx), jx = rxy - jy * p.nlcx;
+    int n = 0;
+    for (int r = 0; r < 14; ++r) {
+        const int sx = wrap(jx - c_stencil[r][0], p.nlcx), sy = wrap(jy - c_stencil[r][1], p.nlcy),
+                  sz = wrap(jz - c_stencil[r][2], p.nlcz);
+        const int cs = sx + p.nlcx * (sy + p.nlcy * sz);
+        const int cnt = cell_count[cs], st = cell_start[cs];
+        for (int round = 0; round < kRevRounds && 32 * round < cnt; ++round) {
+            unsigned m = revmask[(size_t)(r * kRevRounds + round) * nm + j];
+            while (m) {
+                const int L = __ffs(m) - 1;
+                m &= m - 1u;
+                if (n < cap) rlist[(size_t)n * nm + j] = cell_atoms[st + 32 * round + L];
+                ++n;
+            }
+        }
+    }
+    numr[j] = n < cap ? n : cap;
+    if (n > cap) { atomicExch(&flags[10], 1); atomicMax(&flags[11], n); }
+}
+
+// The fallback for link cells fuller than the masks hold: each forward entry
+// (i -> j) enters i into j's reverse row at a position taken from a counter;
+// then each row is sorted by cell (as seen from j) and chain position.
+__global__ void __launch_bounds__(256)
+k_rev_scatter(int nm, int cap, const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
+              int32_t *__restrict__ rlist, int32_t *__restrict__ numr, const int32_t *__restrict__ flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nm || !flags[12]) return;
+    int n = numn[i];
+    n = n < cap ? n : cap;
+    for (int e = 0; e < n; ++e) {
+        const int j = nlist[(size_t)e * nm + i];
+        const int r = atomicAdd(&numr[j], 1);
+        if (r < cap) rlist[(size_t)r * nm + j] = i;
+    }
+}
+
+constexpr int kRevLocal = 96;   // reverse-row entries sorted in registers / local memory
+
+__global__ void __launch_bounds__(256)
+k_rev_sort(Params p, const int32_t *__restrict__ ic, const int32_t *__restrict__ cell_pos,
+           int32_t *__restrict__ rlist, int32_t *__restrict__ numr, int32_t *__restrict__ flags) {
+    // rank of each cell offset (dx, dy, dz), at (dx+1) + 3 (dy+1) + 9 (dz+1),
+    // in a reverse row: 0 for the own cell, 1 + r for mirror offset r of the
+    // half stencil (rows 14..26 of the stencil table)
+    __shared__ int8_t srank[27];
+    if (threadIdx.x < 27) srank[threadIdx.x] = -1;
+    __syncthreads();
+    if (threadIdx.x < 14) {
+        const int r = threadIdx.x == 0 ? 0 : 13 + threadIdx.x;   // own cell, then rows 14..26
+        const int idx = (c_stencil[r][0] + 1) + 3 * (c_stencil[r][1] + 1) + 9 * (c_stencil[r][2] + 1);
+        srank[idx] = (int8_t)threadIdx.x;
+    }
+    __syncthreads();
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.nm || !flags[12]) return;
+    const size_t nm = (size_t)p.nm;
+    const int cap = p.nnbrs;
+    int n = numr[j];
+    if (n > cap) {
+        atomicExch(&flags[10], 1);
+        atomicMax(&flags[11], n);
+        n = cap;
+        numr[j] = cap;
+    }
+    const int cj = ic[j];
+    const int jx = cj % p.nlcx, jy = (cj / p.nlcx) % p.nlcy, jz = cj / (p.nlcx * p.nlcy);
+    auto key = [&](int i) {
+        const int ci = ic[i];
+        int dx = ci % p.nlcx - jx, dy = (ci / p.nlcx) % p.nlcy - jy, dz = ci / (p.nlcx * p.nlcy) - jz;
+        dx = dx > 1 ? dx - p.nlcx : (dx < -1 ? dx + p.nlcx : dx);
+        dy = dy > 1 ? dy - p.nlcy : (dy < -1 ? dy + p.nlcy : dy);
+        dz = dz > 1 ? dz - p.nlcz : (dz < -1 ? dz + p.nlcz : dz);
+        return ((int)srank[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] << 20) | cell_pos[i];
+    };
+    int32_t *row = rlist + j;
+    if (n <= kRevLocal) {
+        int kv[kRevLocal], iv[kRevLocal];
+        for (int e = 0; e < n; ++e) {
+            const int i = row[(size_t)e * nm];
+            const int kk = key(i);
+            int m = e - 1;
+            while (m >= 0 && kv[m] > kk) { kv[m + 1] = kv[m]; iv[m + 1] = iv[m]; --m; }
+            kv[m + 1] = kk;
+            iv[m + 1] = i;
+        }
+        for (int e = 0; e < n; ++e) row[(size_t)e * nm] = iv[e];
+    } else {
+        // long rows (crowded cells): insertion sort in place
+        for (int e = 1; e < n; ++e) {
+            const int i = row[(size_t)e * nm];
+            const int kk = key(i);
+            int m = e - 1;
+            while (m >= 0 && key(row[(size_t)m * nm]) > kk) { row[(size_t)(m + 1) * nm] = row[(size_t)m * nm]; --m; }
+            row[(size_t)(m + 1) * nm] = i;
+        }
+    }
 }
 
 // The box of a half-list build (B0 and rnear |B0^-1|_F) beside the
@@ -435,12 +587,19 @@ __global__ void k_half_box(Params p, BoxState *__restrict__ box) {
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s) {
     cudaMemcpyAsync(d.xhalf, d.posq, (size_t)p.nm * sizeof(int4), cudaMemcpyDeviceToDevice, s);
     k_half_box<<<1, 32, 0, s>>>(p, d.box);
+    cudaMemsetAsync(d.flags + 12, 0, sizeof(int32_t), s);
     if (p.ivol == 0 || p.ivol == 1 || p.ivol == 4)
         k_build_nlist<true><<<p.ncell, 64, 0, s>>>(p, d.pos, d.posq, d.box, d.cell_start, d.cell_count,
-                                                   d.cell_atoms, d.nlist, d.numn, d.rlist, d.numr, d.flags);
+                                                   d.cell_atoms, d.nlist, d.numn, d.revmask, d.flags);
     else
         k_build_nlist<false><<<p.ncell, 64, 0, s>>>(p, d.pos, d.posq, d.box, d.cell_start, d.cell_count,
-                                                    d.cell_atoms, d.nlist, d.numn, d.rlist, d.numr, d.flags);
+                                                    d.cell_atoms, d.nlist, d.numn, d.revmask, d.flags);
+    const int nb = (p.nm + 255) / 256;
+    k_rev_gather<<<nb, 256, 0, s>>>(p, d.ic, d.cell_start, d.cell_count, d.cell_atoms, d.revmask, d.rlist,
+                                    d.numr, d.flags);
+    // the fallback (a link cell fuller than the masks hold): both return at once otherwise
+    k_rev_scatter<<<nb, 256, 0, s>>>(p.nm, p.nnbrs, d.nlist, d.numn, d.rlist, d.numr, d.flags);
+    k_rev_sort<<<nb, 256, 0, s>>>(p, d.ic, d.cell_pos, d.rlist, d.numr, d.flags);
 }
 
 // NLIST(nnbrs, nm) with 1-based entries; unused slots are zero

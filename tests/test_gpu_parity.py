@@ -68,7 +68,7 @@ def test_strained_box_neighbour_list_exact(oracle_mod, gpu_lib):
     assert np.array_equal(nlo[mask], nlg[mask])
 
 
-@pytest.mark.parametrize("n,nlc", [(10, 3), (10, 4), (12, 4)])
+@pytest.mark.parametrize("n,nlc", [(10, 3), (10, 4), (12, 4), (12, 3)])
 def test_neighbour_list_exact_beyond_staging(oracle_mod, gpu_lib, n, nlc):
     """Few, crowded link cells: 31 to 74 atoms per cell, so the 27 cells
     around a home cell hold more than the 640 candidates the builder stages in
@@ -133,13 +133,16 @@ def _expected_reverse_rows(g, w, nlc):
     return out
 
 
-@pytest.mark.parametrize("n,nlc,strain", [(10, None, False), (9, None, True), (10, 3, False), (12, 4, False)])
+@pytest.mark.parametrize("n,nlc,strain", [(10, None, False), (9, None, True), (10, 3, False), (12, 4, False),
+                                          (12, 3, False)])
 def test_reverse_rows_are_the_ordered_transpose(gpu_lib, n, nlc, strain):
-    """The reverse rows the build writes beside NLIST hold, for every atom i,
-    exactly the atoms j with i in NLIST(:, j), in staging order; covers the
-    cell-relative pre-test (default cells, a strained box), the fixed-point
-    one (3 cells per direction) and candidates beyond the staging (12^3 bcc in
-    4^3 cells)."""
+    """The reverse rows formed with the half list hold, for every atom i,
+    exactly the atoms j with i in NLIST(:, j), in staging order (own cell,
+    then the mirror cells, each in chain order); covers the cell-relative
+    pre-test (default cells, a strained box), the fixed-point one (3 cells per
+    direction), candidates beyond the staging (12^3 bcc in 4^3 cells: 2 and 3
+    rounds of home atoms) and cells fuller than the reverse-row masks hold
+    (12^3 bcc in 3^3 cells, 128 atoms per cell: the scatter-and-sort path)."""
     rng = np.random.default_rng(21)
     w = wl.make_workload(n, sigma=0.1, temperature=0.0, seed=22,
                          strain=wl.random_symmetric_strain(rng, 0.02) if strain else None)
