@@ -191,6 +191,9 @@ static int alloc_cells(Engine &E) {
     CHECK(dev_alloc(&d.arr_start, nc + 1, "arr_start"));
     CHECK(dev_alloc(&d.new_count, nc, "new_count"));
     CHECK(dev_alloc(&d.new_start, nc + 1, "new_start"));
+    if (d.scan_tmp) cudaFree(d.scan_tmp);
+    d.scan_tmp = nullptr;
+    CHECK(dev_alloc(&d.scan_tmp, nc / 2048 + 2, "scan blocks"));
     return MOLDY_OK;
 }
 

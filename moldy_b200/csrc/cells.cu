@@ -52,45 +52,135 @@ __global__ void k_sort_cells(int ncell, const int32_t *__restrict__ start,
     for (int i = 0; i < n; ++i) cell_pos[seg[i]] = i;
 }
 
-// single-block exclusive scan: out[0..n-1] exclusive sums, out[n] total
-__global__ void k_exclusive_scan(const int32_t *__restrict__ in, int32_t *__restrict__ out, int n) {
+// single-block exclusive scan: out[0..n-1] exclusive sums, out[n] total.
+// Thread t sums the contiguous segment [t per, (t + 1) per) with its loads
+// independent of one another, the block scans the segment sums, then each
+// thread writes its segment's prefixes (the second read hits the cache).
+__global__ void __launch_bounds__(1024)
+k_exclusive_scan(const int32_t *__restrict__ in, int32_t *__restrict__ out, int n) {
     __shared__ int32_t wsum[32];
-    __shared__ int32_t carry;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
+    int v = 0;
+#pragma unroll 8
+    for (int i = b0; i < b1; ++i) v += in[i];
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    for (int base = 0; base < n; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = i < n ? in[i] : 0;
-        int x = v;
+    if (warp == 0) {
+        int w = lane < nw ? wsum[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        if (lane == 31) wsum[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int w = lane < nw ? wsum[lane] : 0;
+        if (lane < nw) wsum[lane] = w;
+    }
+    __syncthreads();
+    int run = (warp > 0 ? wsum[warp - 1] : 0) + x - v;   // exclusive prefix of this segment
+    for (int i = b0; i < b1; ++i) {
+        out[i] = run;
+        run += in[i];
+    }
+    if (threadIdx.x == blockDim.x - 1) out[n] = run;
+}
+
+// Multi-block exclusive scan for n up to 2^31: block sums of tiles of
+// kScanTile elements, a scan of the block sums, then each block's tile scanned
+// from its offset; every load and store is coalesced.  scratch holds
+// ceil(n / kScanTile) ints.
+constexpr int kScanTile = 2048;   // 256 threads x 8 contiguous elements
+
+__device__ __forceinline__ int block_excl_scan256(int v, int *wsum, int &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            if (lane < nw) wsum[lane] = w;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < 8 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        __syncthreads();
-        int excl = carry + (warp > 0 ? wsum[warp - 1] : 0) + x - v;
-        if (i < n) out[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
+        if (lane < 8) wsum[lane] = w;
+    }
+    __syncthreads();
+    total = wsum[7];
+    const int r = (warp > 0 ? wsum[warp - 1] : 0) + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_scan_reduce(const int32_t *__restrict__ in, int n, int32_t *__restrict__ bsum) {
+    __shared__ int wsum[8];
+    const int base = blockIdx.x * kScanTile;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanTile / 256; ++k) {
+        const int i = base + k * 256 + threadIdx.x;
+        if (i < n) v += in[i];
+    }
+    int total = 0;
+    block_excl_scan256(v, wsum, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(256) k_scan_blocks(int32_t *__restrict__ bsum, int nb, int32_t *__restrict__ out,
+                                                      int n) {
+    __shared__ int wsum[8];
+    int carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += 256) {
+        const int i = b0 + threadIdx.x;
+        const int v = i < nb ? bsum[i] : 0;
+        int total = 0;
+        const int e = block_excl_scan256(v, wsum, total);
+        if (i < nb) bsum[i] = carry + e;
+        carry += total;
     }
     if (threadIdx.x == 0) out[n] = carry;
 }
 
-void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s) {
-    k_exclusive_scan<<<1, 1024, 0, s>>>(in, out, n);
+__global__ void __launch_bounds__(256) k_scan_apply(const int32_t *__restrict__ in, int32_t *__restrict__ out, int n,
+                                                     const int32_t *__restrict__ bsum) {
+    __shared__ int wsum[8];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * 8;
+    int v[8];
+    int sum = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        v[u] = base + u < n ? in[base + u] : 0;
+        sum += v[u];
+    }
+    int total = 0;
+    int run = bsum[blockIdx.x] + block_excl_scan256(sum, wsum, total);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        if (base + u < n) out[base + u] = run;
+        run += v[u];
+    }
+}
+
+void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s, int32_t *scratch) {
+    if (!scratch) {
+        k_exclusive_scan<<<1, 1024, 0, s>>>(in, out, n);
+        return;
+    }
+    const int nb = (n + kScanTile - 1) / kScanTile;
+    k_scan_reduce<<<nb, 256, 0, s>>>(in, n, scratch);
+    k_scan_blocks<<<1, 256, 0, s>>>(scratch, nb, out, n);
+    k_scan_apply<<<nb, 256, 0, s>>>(in, out, n, scratch);
 }
 
 void launch_linkup(DeviceState &d, const Params &p, cudaStream_t s) {
@@ -98,7 +188,7 @@ void launch_linkup(DeviceState &d, const Params &p, cudaStream_t s) {
     int nbc = (p.ncell + kAtomThreads - 1) / kAtomThreads;
     cudaMemsetAsync(d.cell_count, 0, sizeof(int32_t) * p.ncell, s);
     k_assign_cells<<<nb, kAtomThreads, 0, s>>>(d.pos, p.nm, p.nlcx, p.nlcy, p.nlcz, d.ic, d.cell_count);
-    launch_exclusive_scan(d.cell_count, d.cell_start, p.ncell, s);
+    launch_exclusive_scan(d.cell_count, d.cell_start, p.ncell, s, d.scan_tmp);
     cudaMemsetAsync(d.new_count, 0, sizeof(int32_t) * p.ncell, s);
     k_fill_cells<<<nb, kAtomThreads, 0, s>>>(d.ic, p.nm, d.cell_start, d.new_count, d.cell_atoms);
     k_sort_cells<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms,
@@ -130,24 +220,17 @@ __global__ void k_relink_arrivals(int nm, const int32_t *__restrict__ ic,
     arr_list[arr_start[c] + k] = a;
 }
 
-// Replays relink's chain surgery for one cell.  The working sequence W holds
-// the circular chain order; st is the position of the chain start.  W has
-// room for the old atoms plus all arrivals.
-__global__ void k_relink_cells(int ncell, const int32_t *__restrict__ cell_start,
-                               const int32_t *__restrict__ cell_count,
-                               const int32_t *__restrict__ cell_atoms,
-                               const int32_t *__restrict__ ic, const int32_t *__restrict__ ic_new,
-                               const int32_t *__restrict__ arr_start,
-                               int32_t *__restrict__ arr_count_rot, int32_t *__restrict__ arr_list,
-                               int32_t *__restrict__ work, int32_t *__restrict__ new_count) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    int L = cell_count[c];
-    const int32_t *old = cell_atoms + cell_start[c];
-    int32_t *W = work + cell_start[c] + arr_start[c];
-    for (int k = 0; k < L; ++k) W[k] = old[k];
-    int na = arr_count_rot[c];
-    int32_t *A = arr_list + arr_start[c];
+// Replays relink's chain surgery for one cell (src/linkcell_m.F90:215-274).
+// The reference visits the atoms in index order; an atom that changed cell
+// is unlinked from its old chain (the chain start moves to its successor)
+// and linked into its new cell's chain after the start, becoming the start.
+// Per cell that is a merge, in atom-index order, of its departures and its
+// arrivals.  The working sequence W holds the circular chain order; st is the
+// position of the chain start.  On return W holds the new chain from its
+// start (st = 0).  Serial form, one thread: W has room for the old atoms plus
+// all arrivals.
+__device__ void relink_cell_serial(int c, int L, int32_t *W, const int32_t *__restrict__ ic,
+                                   const int32_t *__restrict__ ic_new, int32_t *A, int na, int &Lout) {
     for (int i = 1; i < na; ++i) {   // arrivals in atom-index order
         int v = A[i], k = i - 1;
         while (k >= 0 && A[k] > v) { A[k + 1] = A[k]; --k; }
@@ -180,8 +263,83 @@ __global__ void k_relink_cells(int ncell, const int32_t *__restrict__ cell_start
             ++ia;
         }
     }
-    new_count[c] = L;
-    arr_count_rot[c] = st;
+    // rotate so that the chain starts at W[0] (through the free tail of W)
+    for (int r = 0; r < st; ++r) {
+        const int x = W[0];
+        for (int k = 0; k < L - 1; ++k) W[k] = W[k + 1];
+        W[L - 1] = x;
+    }
+    Lout = L;
+}
+
+// One warp per cell.  When the old atoms and the arrivals fit in 32 lanes,
+// lane k holds W[k] and each event is a warp minimum and one shuffle shift;
+// otherwise lane 0 runs the serial form.  Writes the new chain (from its
+// start) to the cell's work segment and its length to new_count.
+__global__ void __launch_bounds__(256)
+k_relink_cells(int ncell, const int32_t *__restrict__ cell_start, const int32_t *__restrict__ cell_count,
+               const int32_t *__restrict__ cell_atoms, const int32_t *__restrict__ ic,
+               const int32_t *__restrict__ ic_new, const int32_t *__restrict__ arr_start,
+               int32_t *__restrict__ arr_count_rot, int32_t *__restrict__ arr_list, int32_t *__restrict__ work,
+               int32_t *__restrict__ new_count) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= ncell) return;   // warp-uniform
+    int L = cell_count[c];
+    const int32_t *old = cell_atoms + cell_start[c];
+    int32_t *W = work + cell_start[c] + arr_start[c];
+    const int na = arr_count_rot[c];
+    int32_t *A = arr_list + arr_start[c];
+    const unsigned full = 0xffffffffu;
+    if (L + na > 32) {
+        if (lane == 0) {
+            for (int k = 0; k < L; ++k) W[k] = old[k];
+            int Ln = 0;
+            relink_cell_serial(c, L, W, ic, ic_new, A, na, Ln);
+            new_count[c] = Ln;
+            arr_count_rot[c] = 0;
+        }
+        return;
+    }
+    const int kInf = 0x7fffffff;
+    // lane k: W[k] and whether it departs
+    int w = lane < L ? old[lane] : kInf;
+    bool dep = lane < L && ic_new[w] != c;
+    // this lane's arrival (lane < na), the arrivals taken in atom-index order
+    int arr = lane < na ? A[lane] : kInf;
+    int st = 0;
+    for (;;) {
+        const int lmin = __reduce_min_sync(full, dep ? w : kInf);
+        const int nxt = __reduce_min_sync(full, arr);
+        if (lmin == kInf && nxt == kInf) break;
+        if (lmin < nxt) {            // remove lmin; start moves to its successor
+            const int lpos = __ffs(__ballot_sync(full, dep && w == lmin)) - 1;
+            const int wn = __shfl_down_sync(full, w, 1);
+            const bool dn = __shfl_down_sync(full, dep, 1);
+            if (lane >= lpos) { w = lane + 1 < L ? wn : kInf; dep = lane + 1 < L ? dn : false; }
+            --L;
+            st = (L == 0) ? 0 : (lpos < L ? lpos : 0);
+        } else {                     // insert after the start; it becomes the start
+            if (arr == nxt) arr = kInf;   // taken
+            if (L == 0) {
+                if (lane == 0) { w = nxt; dep = false; }
+                L = 1;
+                st = 0;
+            } else {
+                const int wp = __shfl_up_sync(full, w, 1);
+                const bool dp = __shfl_up_sync(full, dep, 1);
+                if (lane > st + 1 && lane <= L) { w = wp; dep = dp; }
+                if (lane == st + 1) { w = nxt; dep = false; }
+                ++L;
+                st = st + 1;
+            }
+        }
+    }
+    // the new chain from its start
+    const int src = L > 0 ? (st + lane) % L : 0;
+    const int x = __shfl_sync(full, w, src);
+    if (lane < L) W[lane] = x;
+    if (lane == 0) { new_count[c] = L; arr_count_rot[c] = 0; }
 }
 
 __global__ void k_relink_write(int ncell, int nm, const int32_t *__restrict__ cell_start,
@@ -214,14 +372,15 @@ void launch_relink(DeviceState &d, const Params &p, cudaStream_t s) {
     cudaMemsetAsync(d.arr_count, 0, sizeof(int32_t) * p.ncell, s);
     k_relink_assign<<<nb, kAtomThreads, 0, s>>>(d.pos, p.nm, p.nlcx, p.nlcy, p.nlcz, d.ic, d.ic_new,
                                                 d.arr_count);
-    launch_exclusive_scan(d.arr_count, d.arr_start, p.ncell, s);
+    launch_exclusive_scan(d.arr_count, d.arr_start, p.ncell, s, d.scan_tmp);
     cudaMemsetAsync(d.new_count, 0, sizeof(int32_t) * p.ncell, s);
     k_relink_arrivals<<<nb, kAtomThreads, 0, s>>>(p.nm, d.ic, d.ic_new, d.arr_start, d.new_count,
                                                   d.arr_list);
-    k_relink_cells<<<nbc, kAtomThreads, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms, d.ic,
+    const int nbw = (p.ncell + 7) / 8;   // one warp per cell, 8 per block
+    k_relink_cells<<<nbw, 256, 0, s>>>(p.ncell, d.cell_start, d.cell_count, d.cell_atoms, d.ic,
                                        d.ic_new, d.arr_start, d.arr_count, d.arr_list, d.work,
                                        d.new_count);
-    launch_exclusive_scan(d.new_count, d.new_start, p.ncell, s);
+    launch_exclusive_scan(d.new_count, d.new_start, p.ncell, s, d.scan_tmp);
     k_relink_write<<<nbc, kAtomThreads, 0, s>>>(p.ncell, p.nm, d.cell_start, d.arr_start,
                                                 d.arr_count, d.work, d.new_count, d.new_start,
                                                 d.cell_atoms2, d.cell_pos, d.flags);

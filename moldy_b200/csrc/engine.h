@@ -278,7 +278,8 @@ inline int grid_blocks(long long work, int threads) {
 // kernel launchers (defined in the .cu files)
 void launch_linkup(DeviceState &d, const Params &p, cudaStream_t s);
 void launch_relink(DeviceState &d, const Params &p, cudaStream_t s);
-void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s);
+// scratch: ceil(n / 2048) ints for the multi-block scan (null: one block)
+void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t s, int32_t *scratch = nullptr);
 void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0, int32_t *link,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
