@@ -106,7 +106,7 @@ k_adj_density(AdjointArgs a, const double4 *__restrict__ pos, const int32_t *__r
         const int n = numn[i];
         double s = 0.0;
         for (int k = 0; k < n; ++k) {
-            const int j = nlist[(size_t)k * nm + i];
+            const int j = nlist[(size_t)i * a.nnbrs + k];
             double ux, uy, uz, r;
             pair_geom(a.ivol, bx, pi, pos[j], ux, uy, uz, r);
             int q; double w0, w1;
@@ -156,7 +156,7 @@ k_adj_pairs_a(AdjointArgs a, const double4 *__restrict__ pos, const int32_t *__r
         const int n = numn[i];
         double mui = 0.0;
         for (int k = 0; k < n; ++k) {
-            const int j = nlist[(size_t)k * nm + i];
+            const int j = nlist[(size_t)i * a.nnbrs + k];
             double ux, uy, uz, r;
             pair_geom(a.ivol, bx, pi, pos[j], ux, uy, uz, r);
             int q; double w0, w1;
@@ -225,7 +225,7 @@ k_adj_pairs_c(AdjointArgs a, const double4 *__restrict__ pos, const int32_t *__r
         const double nui = nu[i];
         const int n = numn[i];
         for (int k = 0; k < n; ++k) {
-            const int j = nlist[(size_t)k * nm + i];
+            const int j = nlist[(size_t)i * a.nnbrs + k];
             double ux, uy, uz, r;
             pair_geom(a.ivol, bx, pi, pos[j], ux, uy, uz, r);
             int q; double w0, w1;

@@ -300,8 +300,10 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
     }
     int nr = (cut <= n - 1) ? cut + 2 : n + 1;
     std::vector<double4> r4(nr);
-    // FP32 nodes in pairs (node k, node k+1) so that one 32-byte load brings
-    // both ends of an interval; the density tables keep phi_k, phi_k+1 side by side
+    // FP32 nodes in pairs (node k, node k+1 - node k) so that one 32-byte load
+    // brings an interval and its interpolation is one fused multiply-add per
+    // value (the difference is the FP32 subtraction the device would do); the
+    // density table keeps (phi_k, phi_k+1 - phi_k) side by side
     std::vector<float4> r4f(2 * (size_t)nr, make_float4(0.f, 0.f, 0.f, 0.f));
     std::vector<double2> phi2(nr, make_double2(0.0, 0.0));
     std::vector<float2> phi2f(nr, make_float2(0.f, 0.f));
@@ -309,10 +311,14 @@ int upload_device_tables(const HostTables &h, double4 **r4d, float4 **r4fd, doub
         r4[i] = make_double4(h.vee[i], h.dvee[i], h.phi[i], h.dphi[i]);
         const float4 q = make_float4((float)h.vee[i], (float)h.dvee[i], (float)h.phi[i], (float)h.dphi[i]);
         r4f[2 * (size_t)i] = q;
-        if (i > 0) r4f[2 * (size_t)i - 1] = q;
         phi2[i].x = h.phi[i];
         phi2f[i].x = (float)h.phi[i];
-        if (i > 0) { phi2[i - 1].y = h.phi[i]; phi2f[i - 1].y = (float)h.phi[i]; }
+        if (i > 0) phi2[i - 1].y = h.phi[i];
+    }
+    for (int i = 0; i + 1 < nr; ++i) {
+        const float4 a = r4f[2 * (size_t)i], b = r4f[2 * (size_t)i + 2];
+        r4f[2 * (size_t)i + 1] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, b.w - a.w);
+        phi2f[i].y = phi2f[i + 1].x - phi2f[i].x;
     }
     std::vector<double2> e2(n + 1);
     std::vector<float2> e2f(n + 1);
@@ -625,7 +631,7 @@ int Engine::get_neighbourlist(int32_t *nlist, int32_t *numn, bool reverse) {
     if (nlist) {
         int32_t *tmp = nullptr;
         CHECK(dev_alloc(&tmp, ne, "nlist export"));
-        launch_export_nlist(rows, cnt, prm, tmp, stream_);
+        launch_export_nlist(rows, cnt, !reverse, prm, tmp, stream_);
         cudaError_t e = cudaMemcpyAsync(nlist, tmp, ne * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
         cudaFree(tmp);
@@ -1060,7 +1066,7 @@ int Engine::table_gradients(double gE, const double *gF, const double *gS, doubl
     if (gF) CUDA_CHECK(cudaMemcpyAsync(dgF, gF, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, stream_), "dL/dF");
     else CUDA_CHECK(cudaMemsetAsync(dgF, 0, 3 * nm * sizeof(double), stream_), "dL/dF");
     AdjointArgs a;
-    a.nm = prm.nm; a.ivol = prm.ivol; a.n = n;
+    a.nm = prm.nm; a.ivol = prm.ivol; a.n = n; a.nnbrs = prm.nnbrs;
     a.vee = tabs; a.dvee = tabs + nb; a.phi = tabs + 2 * nb; a.dphi = tabs + 3 * nb;
     a.emb = tabs + 4 * nb; a.demb = tabs + 5 * nb;
     a.rmin = tab.vp_rmin; a.rmax = tab.vp_rmax;

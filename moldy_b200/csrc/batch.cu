@@ -463,7 +463,7 @@ k_cl_density(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__rest
                     pair_uf(bf, (float)dx, (float)dy, (float)dz, ux, uy, uz);
                     const float r2 = ux * ux + uy * uy + uz * uz;
                     if (!(r2 < rc2f)) continue;
-                    rho += (double)lookup_phif(t, sqrtf(r2));
+                    rho += (double)lookup_phif(t, r2 * rsqrt_ftz(r2));
                     if (ECALC) {
                         double vx, vy, vz;
                         pair_u(b, dx, dy, dz, vx, vy, vz);
@@ -541,7 +541,7 @@ k_cl_forces(TileArgs a, Tables t, int ntot, int pair_cap, const int32_t *__restr
                     pair_uf(bf, (float)dx, (float)dy, (float)dz, uxf, uyf, uzf);
                     const float r2 = uxf * uxf + uyf * uyf + uzf * uzf;
                     if (!(r2 < rc2f)) continue;
-                    const float r = sqrtf(r2), rr = 1.0f / r;
+                    const float rr = rsqrt_ftz(r2), r = r2 * rr;
                     const float4 q = lookup_r4f(t, r);
                     fpair = (double)(-(q.y + q.w * ((float)fph + (float)fq[u])) * rr);
                     vee = (double)q.x;
@@ -711,7 +711,7 @@ k_batch_eval(EvalArgs a, Tables t) {
                     const int4 qj = rec[jj[u]];
                     float dx, dy, dz;
                     const float r2 = rec_sep(bq, qi, qj, dx, dy, dz);
-                    if (r2 < rc2f) rho += (double)lookup_phif(t, sqrtf(r2));
+                    if (r2 < rc2f) rho += (double)lookup_phif(t, r2 * rsqrt_ftz(r2));
                 }
             }
             rho = lanes_sum<LPA>(rho);
@@ -754,7 +754,7 @@ k_batch_eval(EvalArgs a, Tables t) {
                     float dx, dy, dz;
                     const float r2 = rec_sep(bq, qi, qj, dx, dy, dz);
                     if (!(r2 < rc2f)) continue;
-                    const float r = sqrtf(r2), rr = 1.0f / r;
+                    const float rr = rsqrt_ftz(r2), r = r2 * rr;
                     const float4 q = lookup_r4f(t, r);
                     const float fpair = -(q.y + q.w * (fpi + __int_as_float(qj.w))) * rr;
                     fx += (double)(dx * fpair);

@@ -140,6 +140,14 @@ __device__ __forceinline__ int32_t fix32(double x) {
     return __double2loint(fma(x, kFixScale, 6755399441055744.0));
 }
 
+// 1/sqrt(x) of a positive normal x (pair distances: never denormal), with
+// no denormal handling
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // A 32-bit integer as a float, rounded once to nearest (ties to even): the
 // conversion instruction, whose throughput the pair passes measured to be
 // no limit (about 7 % faster than forming it on the FMA pipe)
@@ -219,7 +227,8 @@ __device__ __forceinline__ double2 lookup_e2(const Tables &t, double rho) {
 // its interval from a floor on the FMA pipe; at and beyond the last stored
 // node (r >= rmax: node nlookup; a culled table: its first all-zero node) the
 // value is that node's.  Below rmin the first interval is extrapolated, as
-// the FP64 lookups do (the reference reads out of bounds there).
+// the FP64 lookups do (the reference reads out of bounds there).  A stored
+// interval is its lower node and the FP32 difference to the upper one.
 __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
     const float x = fmaf(r, t.recipstep_f, t.xoff_f);
     float fl;
@@ -228,8 +237,7 @@ __device__ __forceinline__ float4 lookup_r4f(const Tables &t, float r) {
     const float dr = x - fl;
     float4 a, b;
     ldg8f(&t.r4f[2 * idx], a, b);
-    return make_float4(fmaf(b.x - a.x, dr, a.x), fmaf(b.y - a.y, dr, a.y),
-                       fmaf(b.z - a.z, dr, a.z), fmaf(b.w - a.w, dr, a.w));
+    return make_float4(fmaf(b.x, dr, a.x), fmaf(b.y, dr, a.y), fmaf(b.z, dr, a.z), fmaf(b.w, dr, a.w));
 }
 
 __device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
@@ -239,7 +247,7 @@ __device__ __forceinline__ float lookup_phif(const Tables &t, float r) {
     if (idx >= t.nr - 1) return t.tail_f.z;
     const float dr = x - fl;
     const float2 v = __ldg(&t.phi2f[idx]);
-    return fmaf(v.y - v.x, dr, v.x);
+    return fmaf(v.y, dr, v.x);
 }
 
 // ------------------------------------------------ exact FETRANSMETAL Fe-Fe --

@@ -634,7 +634,7 @@ k_energy_pairs(Params p, Tables t, const double4 *__restrict__ pos, const BoxSta
     const int n = numn[a];
     double own = 0.0;
     for (int k = 0; k < n; ++k) {
-        int j = nlist[(size_t)k * p.nm + a];
+        int j = nlist[(size_t)a * p.nnbrs + k];
         double4 pj = pos[j];
         double dx = pa.x - pj.x, dy = pa.y - pj.y, dz = pa.z - pj.z;
         min_image(p.ivol, dx, dy, dz);

@@ -33,9 +33,11 @@ struct DeviceState {
     // relink scratch
     int32_t *ic_new = nullptr, *arr_count = nullptr, *arr_start = nullptr, *arr_list = nullptr;
     int32_t *work = nullptr, *new_count = nullptr, *new_start = nullptr, *cell_atoms2 = nullptr;
-    // neighbour list (neighbourlist_m), entry-major: entry k of atom i at
-    // nlist[k*nm + i], 0-based atom ids; rlist/numr hold each atom's reverse
-    // half row (the atoms j with i in row(j)), written by the same build
+    // neighbour list (neighbourlist_m) as the reference holds NLIST(nnbrs, nm):
+    // entry k of atom i at nlist[i*nnbrs + k], 0-based atom ids; rlist/numr
+    // hold each atom's reverse half row (the atoms j with i in row(j)),
+    // written by the same build, entry-major: entry k of atom j at
+    // rlist[k*nm + j]
     int32_t *nlist = nullptr, *numn = nullptr;
     int32_t *rlist = nullptr, *numr = nullptr;
     // scratch of the structure analysis (rdf.cu), grown on demand
@@ -95,7 +97,7 @@ struct DeviceState {
 
 // Arguments of the table adjoint: the full tables (device) and dL/dE, dL/dsigma.
 struct AdjointArgs {
-    int nm, ivol, n;
+    int nm, ivol, n, nnbrs;   // nnbrs: the half list's row stride
     const double *vee, *dvee, *phi, *dphi, *emb, *demb;
     double rmin, rmax, r_reciprange, r_recipstep;
     double emin, emax, e_reciprange, e_recipstep;
@@ -283,8 +285,10 @@ void launch_exclusive_scan(const int32_t *in, int32_t *out, int n, cudaStream_t 
 void launch_export_linkcells(const DeviceState &d, const Params &p, int32_t *l0, int32_t *link,
                              cudaStream_t s);
 void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s);
-// rows (entry-major, counts cnt) as NLIST(nnbrs, nm), 1-based, unused slots zero
-void launch_export_nlist(const int32_t *rows, const int32_t *cnt, const Params &p, int32_t *out, cudaStream_t s);
+// rows (atom-major as NLIST itself, or entry-major; counts cnt) as
+// NLIST(nnbrs, nm), 1-based, unused slots zero
+void launch_export_nlist(const int32_t *rows, const int32_t *cnt, bool atom_major, const Params &p, int32_t *out,
+                         cudaStream_t s);
 constexpr int kVariants = 8;           // compiled variants per tunable pass
 // store_rho false: rho is not written (no caller reads it before the next
 // evaluation overwrites it: the inner steps of an md_steps call)

@@ -9,12 +9,15 @@
 // after i form NLIST(:, i), entry for entry as the reference's walk appends
 // them.  Candidates past the staging capacity are read from global memory.
 // Each atom's reverse row (the atoms j with i in NLIST(:, j), i's own cell
-// before i, then the 13 mirror cells, each in chain order) is formed
-// afterwards from the finished rows: a scatter, then a sort of each row by
-// cell and chain position.  The lists are stored entry-major (entry k of
-// atom i at k*nm + i) so that the per-step passes, one thread per atom, read
-// them in contiguous 128-byte rows; the export transposes NLIST to the
-// reference's (nnbrs, nm).  The exact distance test
+// before i, then the 13 mirror cells, each in chain order) is gathered
+// afterwards from keep bits the build leaves per staged candidate.  NLIST is
+// stored as the reference holds NLIST(nnbrs, nm): atom i's row at i*nnbrs,
+// its entries contiguous, so that a lane appending to its own row fills
+// whole 32-byte sectors (a cell's atoms have scattered ids, so rows stored
+// entry-major took partial-sector writes, 3x the row bytes in DRAM traffic).
+// The reverse rows, written one thread per atom in atom order, are stored
+// entry-major (entry k of atom j at k*nm + j): a warp's stores of one entry
+// index are then contiguous.  The exact distance test
 // uses separately rounded products and sums (no FMA), as the Fortran
 // evaluates pr_get_realsep_from_dx, so r < rnear gives the same pair set.
 // In a fully periodic box an FP32 distance decides first (from positions
@@ -340,8 +343,8 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
                 qa = home_staged ? srec[q] : posq[a];
             }
         }
-        // the row of a: entry n at base[n * nm] (entry-major)
-        int32_t *const base = nlist + a;
+        // the row of a: entry n at base[n] (atom-major)
+        int32_t *const base = nlist + (size_t)a * cap;
         int n = 0;
         int kk = 0;
         if (rel && min(L0, q0 + 32) <= staged) {   // every live lane's home atom staged
@@ -408,7 +411,7 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
                 }
                 const int k = k0 + __ffs(m) - 1;
                 m &= m - 1u;
-                if (n < cap) base[(size_t)n * nm] = sid[k];
+                if (n < cap) base[n] = sid[k];
                 ++n;
             }
             // warp 1's count is the row's
@@ -424,7 +427,7 @@ k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict_
             for (int k = kk; k < fwd_end; ++k) {
                 int j = 0;
                 const bool take = live && k > q && nl_take<PERIODIC>(S, k, pa, qa, ar, rel, cen, j);
-                if (take && n < cap) base[(size_t)n * nm] = j;
+                if (take && n < cap) base[n] = j;
                 n += take ? 1 : 0;
                 // this candidate's column of the reverse-row masks
                 const unsigned colm = __ballot_sync(0xffffffffu, take);
@@ -502,7 +505,7 @@ k_rev_scatter(int nm, int cap, const int32_t *__restrict__ nlist, const int32_t 
     int n = numn[i];
     n = n < cap ? n : cap;
     for (int e = 0; e < n; ++e) {
-        const int j = nlist[(size_t)e * nm + i];
+        const int j = nlist[(size_t)i * cap + e];
         const int r = atomicAdd(&numr[j], 1);
         if (r < cap) rlist[(size_t)r * nm + j] = i;
     }
@@ -602,19 +605,24 @@ void launch_build_nlist(DeviceState &d, const Params &p, cudaStream_t s) {
     k_rev_sort<<<nb, 256, 0, s>>>(p, d.ic, d.cell_pos, d.rlist, d.numr, d.flags);
 }
 
-// NLIST(nnbrs, nm) with 1-based entries; unused slots are zero
-__global__ void k_export_nlist(int nm, int nnbrs, const int32_t *__restrict__ nlist,
-                               const int32_t *__restrict__ numn, int32_t *__restrict__ out) {
+// NLIST(nnbrs, nm) with 1-based entries; unused slots are zero.  ATOM_MAJOR:
+// rows stored as NLIST itself (the half list), else entry-major (the reverse
+// rows).
+template <bool ATOM_MAJOR>
+__global__ void k_export_nlist(int nm, int nnbrs, const int32_t *__restrict__ rows,
+                               const int32_t *__restrict__ cnt, int32_t *__restrict__ out) {
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)nm * nnbrs) return;
     int a = (int)(e / nnbrs), k = (int)(e % nnbrs);
-    out[e] = k < numn[a] ? nlist[(size_t)k * nm + a] + 1 : 0;
+    out[e] = k < cnt[a] ? (ATOM_MAJOR ? rows[e] : rows[(size_t)k * nm + a]) + 1 : 0;
 }
 
-void launch_export_nlist(const int32_t *rows, const int32_t *cnt, const Params &p, int32_t *out, cudaStream_t s) {
+void launch_export_nlist(const int32_t *rows, const int32_t *cnt, bool atom_major, const Params &p, int32_t *out,
+                         cudaStream_t s) {
     long long n = (long long)p.nm * p.nnbrs;
     int nb = (int)((n + 255) / 256);
-    k_export_nlist<<<nb, 256, 0, s>>>(p.nm, p.nnbrs, rows, cnt, out);
+    if (atom_major) k_export_nlist<true><<<nb, 256, 0, s>>>(p.nm, p.nnbrs, rows, cnt, out);
+    else k_export_nlist<false><<<nb, 256, 0, s>>>(p.nm, p.nnbrs, rows, cnt, out);
 }
 
 }  // namespace moldy

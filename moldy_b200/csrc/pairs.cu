@@ -219,7 +219,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
                     if (r2 > rscreen2) continue;
                     // inside the error band: the FP64 distance decides
                     if (!(r2 < rin2) && !inside_cut_fp64(pos, a, ee[u] & kIdMask, sb, p.ivol, t.rcull2)) continue;
-                    rho_a += (double)lookup_phif(t, r2 * rsqrtf(r2));
+                    rho_a += (double)lookup_phif(t, r2 * rsqrt_ftz(r2));
                     if (cnt < p.pair_cap) alist[(size_t)cnt * stride + a] = ee[u];
                     ++cnt;
                 }
@@ -389,7 +389,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
                     const float ry = fmaf(bs[7], dz, fmaf(bs[4], dy, bs[1] * dx));
                     const float rz = fmaf(bs[8], dz, fmaf(bs[5], dy, bs[2] * dx));
                     const float r2 = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
-                    const float rr = rsqrtf(r2);
+                    const float rr = rsqrt_ftz(r2);
                     const float4 tv = lookup_r4f(t, r2 * rr);    // vee, dvee, phi, dphi
                     const float fp = -(tv.y + tv.w * (fa + __int_as_float(qj.w))) * rr;
                     const float dfx = dx * fp, dfy = dy * fp, dfz = dz * fp;
@@ -527,19 +527,20 @@ __device__ float keep_radius2(const double *sb, double r) {
     return screen_radius2(sb, r * r) > 1e37f ? 3.0e38f : keep * keep;
 }
 
-// Appends to atom a's row (entries kept in [cnt, cap)) the entries of one
-// source row (n entries, entry-major with stride nm) whose FP32 distance is
-// within keep2; own = bit 31 to set on the kept entries.
+// Appends to atom a's row (entries kept in [cnt, cap), entry-major with
+// stride nm) the entries of one source row (n entries, entry k at
+// row[k * step]) whose FP32 distance is within keep2; own = bit 31 to set on
+// the kept entries.
 template <bool FIX, int B>
-__device__ __forceinline__ int filter_row(const Params &p, const int32_t *__restrict__ src, int n, int a,
-                                          const double4 &pa, const int4 &qa, const double4 *__restrict__ pos,
+__device__ __forceinline__ int filter_row(const Params &p, const int32_t *__restrict__ row, size_t step, int n,
+                                          int a, const double4 &pa, const int4 &qa, const double4 *__restrict__ pos,
                                           const int4 *__restrict__ posq, const float *bf, float keep2,
                                           int32_t own, int32_t *__restrict__ dst, int cap, int cnt) {
     const size_t stride = (size_t)p.nm;
     for (int k0 = 0; k0 < n; k0 += B) {
         int ee[B];
 #pragma unroll
-        for (int u = 0; u < B; ++u) ee[u] = (k0 + u < n) ? __ldg(&src[(size_t)(k0 + u) * stride + a]) : -1;
+        for (int u = 0; u < B; ++u) ee[u] = (k0 + u < n) ? __ldg(&row[(size_t)(k0 + u) * step]) : -1;
         double4 qq[FIX ? 1 : B];
         int4 qi[FIX ? B : 1];
 #pragma unroll
@@ -606,9 +607,11 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
         const int4 qa = posq[a];
         if (need_out) {
             dh2 = fmaxf(dh2, fix_disp2(bq, qa, xhalf[a]));
-            int cnt = filter_row<FIX, 8>(p, nlist, numn[a], a, pa, qa, pos, posq, bf, keep_out, kOwnBit, olist,
-                                         ocap, 0);
-            cnt = filter_row<FIX, 8>(p, rlist, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist, ocap, cnt);
+            // the own row is stored atom-major (NLIST(:, a)), the reverse row entry-major
+            int cnt = filter_row<FIX, 8>(p, nlist + (size_t)a * p.nnbrs, 1, numn[a], a, pa, qa, pos, posq, bf,
+                                         keep_out, kOwnBit, olist, ocap, 0);
+            cnt = filter_row<FIX, 8>(p, rlist + a, (size_t)nm, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist,
+                                     ocap, cnt);
             out_cnt[a] = cnt;
             if (cnt > ocap) over = max(over, cnt);
             xout[a] = qa;
@@ -616,7 +619,8 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
         if (need_mid) {
             const int nt = out_cnt[a];
             const int n = nt < ocap ? nt : ocap;
-            mid_cnt[a] = filter_row<FIX, 8>(p, olist, n, a, pa, qa, pos, posq, bf, keep_mid, 0, mlist, mcap, 0);
+            mid_cnt[a] = filter_row<FIX, 8>(p, olist + a, (size_t)nm, n, a, pa, qa, pos, posq, bf, keep_mid, 0, mlist,
+                                            mcap, 0);
             xbuild[a] = qa;
             d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
         }

@@ -56,6 +56,7 @@ struct HistArgs {
     const BoxState *box;
     const int32_t *znum, *spec;
     int nm, ivol, nspec, maxbin, bpa;
+    int nnbrs;                         // mode 0: the half list's row stride
     double rsqmax;                     // mode 0 bound on rsq
     unsigned long long *hist, *natoms, *nclose;
 };
@@ -135,7 +136,7 @@ k_rdf_list(HistArgs a, const int32_t *__restrict__ nlist, const int32_t *__restr
             double4 pp[4];
             int zz[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) jj[u] = k0 + u < n ? nlist[(size_t)(k0 + u) * a.nm + i] : -1;
+            for (int u = 0; u < 4; ++u) jj[u] = k0 + u < n ? nlist[(size_t)i * a.nnbrs + k0 + u] : -1;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int j = jj[u] >= 0 ? jj[u] : 0;
@@ -247,6 +248,7 @@ struct AjArgs {
     const BoxState *box;
     const int32_t *spec;
     int nm, ivol, nspec;
+    int nnbrs;                               // mode 0: the half list's row stride
     double thr[kMaxSpecies * kMaxSpecies];   // 1.45 rn(si,sj)^2 with the single-precision 1.45
     int32_t *ncount, *near;                  // near[i * kNearCap + k]
     int32_t *flags;                          // [0]: an atom had more than kNearCap neighbours
@@ -269,7 +271,7 @@ k_aj_near_list(AjArgs a, const int32_t *__restrict__ nlist, const int32_t *__res
         const int si = species_of(a.spec, i);
         const int n = numn[i];
         for (int k = 0; k < n; ++k) {
-            const int j = nlist[(size_t)k * a.nm + i];
+            const int j = nlist[(size_t)i * a.nnbrs + k];
             const int sj = species_of(a.spec, j);
             // the same rsq from either end: the image rule and the rounding are symmetric
             const double rsq = pair_sep2(b, a.ivol, pi, a.pos[j]);
@@ -511,7 +513,7 @@ int Engine::rdf(int mode, int maxbin, int bpa, const int32_t *species, int nspec
     if (species) RCUDA(cudaMemcpyAsync(dsp, species, nm * sizeof(int32_t), cudaMemcpyHostToDevice, s), "species");
     HistArgs a;
     a.pos = d.pos; a.box = d.box; a.znum = d.znum; a.spec = dsp;
-    a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec; a.maxbin = maxbin; a.bpa = bpa;
+    a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec; a.maxbin = maxbin; a.bpa = bpa; a.nnbrs = prm.nnbrs;
     const int q = maxbin / bpa;
     a.rsqmax = (double)(q * q);
     a.hist = dh; a.natoms = dh + nh; a.nclose = a.natoms + nspec;
@@ -584,7 +586,7 @@ int Engine::ackland_jones(int mode, const int32_t *species, int nspec, const dou
     RCUDA(cudaMemsetAsync(a.ncount, 0, nm * sizeof(int32_t), s), "analysis counts");
     RCUDA(cudaMemsetAsync(a.flags, 0, sizeof(int32_t), s), "analysis flag");
     a.pos = d.pos; a.box = d.box; a.spec = species ? dsp : nullptr;
-    a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec;
+    a.nm = nm; a.ivol = prm.ivol; a.nspec = nspec; a.nnbrs = prm.nnbrs;
     const int blocks = std::max(1, std::min((nm + kRdfThreads - 1) / kRdfThreads, 8 * 148));
     if (mode == 0) {
         k_aj_near_list<<<blocks, kRdfThreads, 0, s>>>(a, d.nlist, d.numn);
