@@ -7,9 +7,10 @@
 // segment is ascending.  relink (src/linkcell_m.F90:215-274) is a sequential
 // loop over atoms; its effect on one cell depends only on the removals from
 // and insertions into that cell, taken in atom-index order, so each cell is
-// replayed independently by one thread:
+// replayed independently (one warp per cell, k_relink_cells):
 //   remove x: the chain start moves to x's successor;
 //   insert i: i goes right after the current start and becomes the start.
+// The cells' segments are placed by an exclusive scan of their sizes.
 #include "engine.h"
 
 namespace moldy {
