@@ -694,6 +694,11 @@ def run_batch(args):
                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": bpa_p * b.ntot,
                     "avg_launch_ms": eval_ms["current"]}
+        # the DRAM bytes of one launch on this workload, from an ncu capture
+        # (profiles/batch_kernels_1024_supercells.md)
+        tb = ((load_traffic() or {}).get("batch") or {}).get("kernels", {}).get("batch_eval")
+        if tb and tb.get("atoms") == b.ntot:
+            roofline["traffic"] = float(tb["dram_bytes_per_launch"])
     else:
         bpa = {"density": 4 * n_row + 4 + 32 + 32, "forces": 4 * n_row + 4 + 32 + 8 + 8 + 24 + 8 + 48}
         dom = max(("density", "forces"), key=lambda k: ktimes[k])
