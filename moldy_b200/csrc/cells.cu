@@ -273,10 +273,12 @@ __device__ void relink_cell_serial(int c, int L, int32_t *W, const int32_t *__re
     Lout = L;
 }
 
-// One warp per cell.  When the old atoms and the arrivals fit in 32 lanes,
-// lane k holds W[k] and each event is a warp minimum and one shuffle shift;
-// otherwise lane 0 runs the serial form.  Writes the new chain (from its
-// start) to the cell's work segment and its length to new_count.
+// One warp per cell.  When the old atoms and the arrivals fit in 64 slots,
+// lane k holds slots k and 32 + k of W, and each event is a warp minimum and
+// one shuffle shift of both halves; otherwise lane 0 runs the serial form.
+// (Link cells span two or three lattice planes per direction, so in bcc
+// crystals they hold 16 to 54 atoms.)  Writes the new chain (from its start)
+// to the cell's work segment and its length to new_count.
 __global__ void __launch_bounds__(256)
 k_relink_cells(int ncell, const int32_t *__restrict__ cell_start, const int32_t *__restrict__ cell_count,
                const int32_t *__restrict__ cell_atoms, const int32_t *__restrict__ ic,
@@ -292,7 +294,7 @@ k_relink_cells(int ncell, const int32_t *__restrict__ cell_start, const int32_t 
     const int na = arr_count_rot[c];
     int32_t *A = arr_list + arr_start[c];
     const unsigned full = 0xffffffffu;
-    if (L + na > 32) {
+    if (L + na > 64) {
         if (lane == 0) {
             for (int k = 0; k < L; ++k) W[k] = old[k];
             int Ln = 0;
@@ -303,64 +305,87 @@ k_relink_cells(int ncell, const int32_t *__restrict__ cell_start, const int32_t 
         return;
     }
     const int kInf = 0x7fffffff;
-    // lane k: W[k] and whether it departs
-    int w = lane < L ? old[lane] : kInf;
-    bool dep = lane < L && ic_new[w] != c;
-    // this lane's arrival (lane < na), the arrivals taken in atom-index order
-    int arr = lane < na ? A[lane] : kInf;
+    const int hi = 32 + lane;   // this lane's second slot
+    // slot k: W[k] and whether it departs
+    int w0 = lane < L ? old[lane] : kInf, w1 = hi < L ? old[hi] : kInf;
+    bool d0 = lane < L && ic_new[w0] != c, d1 = hi < L && ic_new[w1] != c;
+    // this lane's arrivals (at most two), taken in atom-index order
+    int a0 = lane < na ? A[lane] : kInf, a1 = hi < na ? A[hi] : kInf;
     int st = 0;
     for (;;) {
-        const int lmin = __reduce_min_sync(full, dep ? w : kInf);
-        const int nxt = __reduce_min_sync(full, arr);
+        const int lmin = __reduce_min_sync(full, min(d0 ? w0 : kInf, d1 ? w1 : kInf));
+        const int nxt = __reduce_min_sync(full, min(a0, a1));
         if (lmin == kInf && nxt == kInf) break;
         if (lmin < nxt) {            // remove lmin; start moves to its successor
-            const int lpos = __ffs(__ballot_sync(full, dep && w == lmin)) - 1;
-            const int wn = __shfl_down_sync(full, w, 1);
-            const bool dn = __shfl_down_sync(full, dep, 1);
-            if (lane >= lpos) { w = lane + 1 < L ? wn : kInf; dep = lane + 1 < L ? dn : false; }
+            const unsigned b0 = __ballot_sync(full, d0 && w0 == lmin);
+            const unsigned b1 = __ballot_sync(full, d1 && w1 == lmin);
+            const int lpos = b0 ? __ffs(b0) - 1 : 32 + __ffs(b1) - 1;
+            // every slot from lpos on takes the next slot's content
+            const int w0n = __shfl_down_sync(full, w0, 1), w1n = __shfl_down_sync(full, w1, 1);
+            const bool d0n = __shfl_down_sync(full, d0, 1), d1n = __shfl_down_sync(full, d1, 1);
+            const int w32 = __shfl_sync(full, w1, 0);
+            const bool d32 = __shfl_sync(full, d1, 0);
+            if (lane >= lpos) { w0 = lane < 31 ? w0n : w32; d0 = lane < 31 ? d0n : d32; }
+            if (hi >= lpos) { w1 = lane < 31 ? w1n : kInf; d1 = lane < 31 ? d1n : false; }
             --L;
             st = (L == 0) ? 0 : (lpos < L ? lpos : 0);
         } else {                     // insert after the start; it becomes the start
-            if (arr == nxt) arr = kInf;   // taken
+            if (a0 == nxt) a0 = kInf;   // taken
+            else if (a1 == nxt) a1 = kInf;
             if (L == 0) {
-                if (lane == 0) { w = nxt; dep = false; }
+                if (lane == 0) { w0 = nxt; d0 = false; }
                 L = 1;
                 st = 0;
             } else {
-                const int wp = __shfl_up_sync(full, w, 1);
-                const bool dp = __shfl_up_sync(full, dep, 1);
-                if (lane > st + 1 && lane <= L) { w = wp; dep = dp; }
-                if (lane == st + 1) { w = nxt; dep = false; }
+                const int pos = st + 1;
+                // every slot after pos, up to L, takes the previous slot's content
+                const int w0p = __shfl_up_sync(full, w0, 1), w1p = __shfl_up_sync(full, w1, 1);
+                const bool d0p = __shfl_up_sync(full, d0, 1), d1p = __shfl_up_sync(full, d1, 1);
+                const int w31 = __shfl_sync(full, w0, 31);
+                const bool d31 = __shfl_sync(full, d0, 31);
+                if (lane > pos && lane <= L) { w0 = w0p; d0 = d0p; }
+                if (lane == pos) { w0 = nxt; d0 = false; }
+                if (hi > pos && hi <= L) { w1 = lane == 0 ? w31 : w1p; d1 = lane == 0 ? d31 : d1p; }
+                if (hi == pos) { w1 = nxt; d1 = false; }
                 ++L;
-                st = st + 1;
+                st = pos;
             }
         }
     }
     // the new chain from its start
-    const int src = L > 0 ? (st + lane) % L : 0;
-    const int x = __shfl_sync(full, w, src);
-    if (lane < L) W[lane] = x;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        const int src = L > 0 ? (st + i) % L : 0;
+        const int x0 = __shfl_sync(full, w0, src & 31), x1 = __shfl_sync(full, w1, src & 31);
+        if (i < L) W[i] = src < 32 ? x0 : x1;
+    }
     if (lane == 0) { new_count[c] = L; arr_count_rot[c] = 0; }
 }
 
-__global__ void k_relink_write(int ncell, int nm, const int32_t *__restrict__ cell_start,
-                               const int32_t *__restrict__ arr_start,
-                               const int32_t *__restrict__ rot, const int32_t *__restrict__ work,
-                               const int32_t *__restrict__ new_count,
-                               const int32_t *__restrict__ new_start, int32_t *__restrict__ atoms2,
-                               int32_t *__restrict__ cell_pos, int32_t *__restrict__ flags) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    int L = new_count[c], st = rot[c];
-    int base = new_start[c];
-    if (L < 0 || base < 0 || base + L > nm) {       // inconsistent counts: record, skip
-        atomicExch(&flags[1], 1);
+// One warp per cell: the new chain (rotated by rot[c] < L) into the cell's
+// segment of the new cell lists, and each atom's chain position.
+__global__ void __launch_bounds__(256)
+k_relink_write(int ncell, int nm, const int32_t *__restrict__ cell_start,
+               const int32_t *__restrict__ arr_start,
+               const int32_t *__restrict__ rot, const int32_t *__restrict__ work,
+               const int32_t *__restrict__ new_count,
+               const int32_t *__restrict__ new_start, int32_t *__restrict__ atoms2,
+               int32_t *__restrict__ cell_pos, int32_t *__restrict__ flags) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= ncell) return;   // warp-uniform
+    const int L = new_count[c], st = rot[c];
+    const int base = new_start[c];
+    if (L < 0 || base < 0 || base + L > nm || st < 0 || (L > 0 && st >= L)) {   // inconsistent: record, skip
+        if (lane == 0) atomicExch(&flags[1], 1);
         return;
     }
     const int32_t *W = work + cell_start[c] + arr_start[c];
     int32_t *out = atoms2 + base;
-    for (int k = 0; k < L; ++k) {
-        int x = W[(st + k) % L];
+    for (int k = lane; k < L; k += 32) {
+        const int j = st + k < L ? st + k : st + k - L;
+        const int x = W[j];
         if (x < 0 || x >= nm) { atomicExch(&flags[1], 1); continue; }
         out[k] = x;
         cell_pos[x] = k;
@@ -369,7 +394,6 @@ __global__ void k_relink_write(int ncell, int nm, const int32_t *__restrict__ ce
 
 void launch_relink(DeviceState &d, const Params &p, cudaStream_t s) {
     int nb = (p.nm + kAtomThreads - 1) / kAtomThreads;
-    int nbc = (p.ncell + kAtomThreads - 1) / kAtomThreads;
     cudaMemsetAsync(d.arr_count, 0, sizeof(int32_t) * p.ncell, s);
     k_relink_assign<<<nb, kAtomThreads, 0, s>>>(d.pos, p.nm, p.nlcx, p.nlcy, p.nlcz, d.ic, d.ic_new,
                                                 d.arr_count);
@@ -382,7 +406,7 @@ void launch_relink(DeviceState &d, const Params &p, cudaStream_t s) {
                                        d.ic_new, d.arr_start, d.arr_count, d.arr_list, d.work,
                                        d.new_count);
     launch_exclusive_scan(d.new_count, d.new_start, p.ncell, s, d.scan_tmp);
-    k_relink_write<<<nbc, kAtomThreads, 0, s>>>(p.ncell, p.nm, d.cell_start, d.arr_start,
+    k_relink_write<<<(p.ncell + 7) / 8, 256, 0, s>>>(p.ncell, p.nm, d.cell_start, d.arr_start,
                                                 d.arr_count, d.work, d.new_count, d.new_start,
                                                 d.cell_atoms2, d.cell_pos, d.flags);
     // commit (copies keep buffer addresses fixed for graph capture)

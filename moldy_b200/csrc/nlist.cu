@@ -474,18 +474,29 @@ k_rev_gather(Params p, const int32_t *__restrict__ ic, const int32_t *__restrict
     const int nxy = p.nlcx * p.nlcy;
     const int jz = div_small(cj, nxy), rxy = cj - jz * nxy;
     const int jy = div_small(rxy, p.nlcx), jx = rxy - jy * p.nlcx;
-    int n = 0;
+    // the 14 source cells' sizes and starts, then their first-round words, all
+    // loads issued before any is used
+    int cnt[14], st[14];
+#pragma unroll
     for (int r = 0; r < 14; ++r) {
         const int sx = wrap(jx - c_stencil[r][0], p.nlcx), sy = wrap(jy - c_stencil[r][1], p.nlcy),
                   sz = wrap(jz - c_stencil[r][2], p.nlcz);
         const int cs = sx + p.nlcx * (sy + p.nlcy * sz);
-        const int cnt = cell_count[cs], st = cell_start[cs];
-        for (int round = 0; round < kRevRounds && 32 * round < cnt; ++round) {
-            unsigned m = revmask[(size_t)(r * kRevRounds + round) * nm + j];
+        cnt[r] = cell_count[cs];
+        st[r] = cell_start[cs];
+    }
+    unsigned w0[14];
+#pragma unroll
+    for (int r = 0; r < 14; ++r) w0[r] = cnt[r] > 0 ? revmask[(size_t)(r * kRevRounds) * nm + j] : 0u;
+    int n = 0;
+#pragma unroll
+    for (int r = 0; r < 14; ++r) {
+        for (int round = 0; round < kRevRounds && 32 * round < cnt[r]; ++round) {
+            unsigned m = round == 0 ? w0[r] : revmask[(size_t)(r * kRevRounds + round) * nm + j];
             while (m) {
                 const int L = __ffs(m) - 1;
                 m &= m - 1u;
-                if (n < cap) rlist[(size_t)n * nm + j] = cell_atoms[st + 32 * round + L];
+                if (n < cap) rlist[(size_t)n * nm + j] = cell_atoms[st[r] + 32 * round + L];
                 ++n;
             }
         }
