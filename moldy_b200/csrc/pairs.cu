@@ -574,7 +574,7 @@ __device__ __forceinline__ int filter_row(const Params &p, const int32_t *__rest
 // keeps its true count, which the flags (outer) or the screening pass
 // (intermediate) report.
 template <bool FIX>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
              BoxState *__restrict__ box, const int32_t *__restrict__ nlist, const int32_t *__restrict__ numn,
              const int32_t *__restrict__ rlist, const int32_t *__restrict__ numr, int32_t *__restrict__ olist,
@@ -608,9 +608,9 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
         if (need_out) {
             dh2 = fmaxf(dh2, fix_disp2(bq, qa, xhalf[a]));
             // the own row is stored atom-major (NLIST(:, a)), the reverse row entry-major
-            int cnt = filter_row<FIX, 8>(p, nlist + (size_t)a * p.nnbrs, 1, numn[a], a, pa, qa, pos, posq, bf,
+            int cnt = filter_row<FIX, 4>(p, nlist + (size_t)a * p.nnbrs, 1, numn[a], a, pa, qa, pos, posq, bf,
                                          keep_out, kOwnBit, olist, ocap, 0);
-            cnt = filter_row<FIX, 8>(p, rlist + a, (size_t)nm, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist,
+            cnt = filter_row<FIX, 4>(p, rlist + a, (size_t)nm, numr[a], a, pa, qa, pos, posq, bf, keep_out, 0, olist,
                                      ocap, cnt);
             out_cnt[a] = cnt;
             if (cnt > ocap) over = max(over, cnt);
@@ -619,7 +619,7 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
         if (need_mid) {
             const int nt = out_cnt[a];
             const int n = nt < ocap ? nt : ocap;
-            mid_cnt[a] = filter_row<FIX, 8>(p, olist + a, (size_t)nm, n, a, pa, qa, pos, posq, bf, keep_mid, 0, mlist,
+            mid_cnt[a] = filter_row<FIX, 4>(p, olist + a, (size_t)nm, n, a, pa, qa, pos, posq, bf, keep_mid, 0, mlist,
                                             mcap, 0);
             xbuild[a] = qa;
             d2 = fmaxf(d2, fix_disp2(bq, qa, xout[a]));
