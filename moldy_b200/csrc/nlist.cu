@@ -45,7 +45,8 @@ __constant__ int8_t c_stencil[27][3] = {
 
 __device__ __forceinline__ int wrap(int j, int n) { return j < 0 ? j + n : (j >= n ? j - n : j); }
 
-constexpr int kNlStage = 640;   // staged candidates per home cell (27 cells)
+constexpr int kNlStage = 384;   // staged candidates per home cell (its 14 half-stencil cells hold ~310
+                                // on average); the rest are read from global memory
 constexpr int kNlChunks = kNlStage / 32;
 constexpr double kNlBand = 1.0e-3;   // A; the FP32 test decides outside rnear -+ this
 
@@ -187,7 +188,7 @@ __device__ __forceinline__ unsigned transpose_lanes(unsigned x, int lane) {
 // second half, from the count of the first half on.  The reverse rows come
 // afterwards from the finished rows (k_rev_scatter, k_rev_sort).
 template <bool PERIODIC>
-__global__ void __launch_bounds__(64, 12)
+__global__ void __launch_bounds__(64, 20)
 k_build_nlist(Params p, const double4 *__restrict__ pos, const int4 *__restrict__ posq,
               const BoxState *__restrict__ box,
               const int32_t *__restrict__ cell_start, const int32_t *__restrict__ cell_count,
