@@ -433,6 +433,24 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Block-wide sum of NV values per thread into partials[blockIdx.x*kPartials + off + k].
 // Deterministic: fixed shuffle tree, then warps in order.
+// The box state of a one-block kernel in shared memory: every thread loads
+// a share of it at once (one round of global loads instead of thread 0's
+// chain of dependent ones), thread 0 works on the copy, every thread stores
+// a share back.  Only one-block kernels that own the box for their whole
+// run use these.
+__device__ __forceinline__ void box_load(BoxState &s, const BoxState *__restrict__ g) {
+    static_assert(sizeof(BoxState) % 8 == 0, "BoxState is copied in 8-byte words");
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(g);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s);
+    for (int i = threadIdx.x; i < (int)(sizeof(BoxState) / 8); i += blockDim.x) dst[i] = src[i];
+}
+
+__device__ __forceinline__ void box_store(BoxState *__restrict__ g, const BoxState &s) {
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&s);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(g);
+    for (int i = threadIdx.x; i < (int)(sizeof(BoxState) / 8); i += blockDim.x) dst[i] = src[i];
+}
+
 template <int NV>
 __device__ __forceinline__ void block_partials(double (&v)[NV], double *partials, int off) {
     __shared__ double sm[32][NV];

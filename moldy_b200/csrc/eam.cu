@@ -18,47 +18,14 @@ int stream_blocks(int nm) {
     return nb < 4 * sms ? nb : 4 * sms;
 }
 
-// mode 0: force only; 1: velocity Verlet second half (box); 2: md_init
-__global__ void __launch_bounds__(256)
-k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
-                 int nblk_embed, const double *__restrict__ part_force, int nblk_force,
-                 const double *__restrict__ part_kin, int nblk_kin, int mode) {
-    // the three sets of block partials in one pass: each thread issues the
-    // loads of all three before adding (per set, the same order as
-    // reduce_partials)
-    __shared__ double sm[8][15], sr[15];
-    double acc[15];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
-    const int nmax = max(nblk_embed, max(nblk_force, nblk_kin));
-    for (int b = threadIdx.x; b < nmax; b += blockDim.x) {
-        double e[15];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) e[k] = b < nblk_embed ? part_embed[(size_t)b * kPartials + k] : 0.0;
-#pragma unroll
-        for (int k = 0; k < 7; ++k) e[2 + k] = b < nblk_force ? part_force[(size_t)b * kPartials + k] : 0.0;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) e[9 + k] = b < nblk_kin ? part_kin[(size_t)b * kPartials + k] : 0.0;
-#pragma unroll
-        for (int k = 0; k < 15; ++k) acc[k] += e[k];
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 15; ++k) {
-        const double w = warp_sum(acc[k]);
-        if (lane == 0) sm[warp][k] = w;
-    }
-    __syncthreads();
-    if (warp == 0 && lane < 15) {
-        double w = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) w += sm[q][lane];
-        sr[lane] = w;
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
+__device__ void therm_prep(const Params &p, const double *b, const double *b1, BoxState &B);
+
+// The box algebra of k_finalize_force, by one thread on the block's shared
+// copy of the box: sr holds the 15 reduced sums (embedding energy, pair
+// count; pair energy, virial moments; kinetic moments).
+__device__ void finalize_box(const Params &p, BoxState &B, const double *sr, int mode) {
     const double *se = sr, *sf = sr + 2, *sk = sr + 9;
     // the box algebra runs on register copies and is stored once at the end
-    BoxState &B = *box;
     double b0[9], b1[9], b2[9], tp[9], tk[9], tc[9], tg[9], tgdot[9], fb[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) { b0[k] = B.b0[k]; b1[k] = B.b1[k]; b2[k] = B.b2[k]; }
@@ -117,6 +84,52 @@ k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict_
 #pragma unroll
     for (int k = 0; k < 9; ++k) { B.b1[k] = b1[k]; B.b2[k] = b2[k]; }
     therm_prep(p, b0, b1, B);       // for the update_therm_avs that follows
+}
+
+// mode 0: force only; 1: velocity Verlet second half (box); 2: md_init
+__global__ void __launch_bounds__(256)
+k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
+                 int nblk_embed, const double *__restrict__ part_force, int nblk_force,
+                 const double *__restrict__ part_kin, int nblk_kin, int mode) {
+    // the box in shared memory, loaded while the partials are summed
+    __shared__ BoxState sbox;
+    box_load(sbox, box);
+    // the three sets of block partials in one pass: each thread issues the
+    // loads of all three before adding (per set, the same order as
+    // reduce_partials)
+    __shared__ double sm[8][15], sr[15];
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    const int nmax = max(nblk_embed, max(nblk_force, nblk_kin));
+    for (int b = threadIdx.x; b < nmax; b += blockDim.x) {
+        double e[15];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) e[k] = b < nblk_embed ? part_embed[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) e[2 + k] = b < nblk_force ? part_force[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) e[9 + k] = b < nblk_kin ? part_kin[(size_t)b * kPartials + k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 15; ++k) acc[k] += e[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        const double w = warp_sum(acc[k]);
+        if (lane == 0) sm[warp][k] = w;
+    }
+    __syncthreads();
+    if (warp == 0 && lane < 15) {
+        double w = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) w += sm[q][lane];
+        sr[lane] = w;
+    }
+    __syncthreads();
+    __syncthreads();
+    if (threadIdx.x == 0) finalize_box(p, sbox, sr, mode);
+    __syncthreads();
+    box_store(box, sbox);
 }
 
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
@@ -270,26 +283,10 @@ k_therm_finish(Params p, BoxState *__restrict__ box, const double *__restrict__ 
 // therm_nblk > 0: first finish the update_therm_avs that the drift kernel
 // took for the step that has just ended (its block partials), before the box
 // moves.
-__global__ void __launch_bounds__(256)
-k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
-             int half_build, int apply_box, const double *__restrict__ therm_partials, int therm_nblk,
-             double *__restrict__ rec, int rec_indexed) {
-    if (therm_nblk > 0) {
-        __shared__ double s3[3];
-        reduce_partials<3>(therm_partials, therm_nblk, s3);
-        if (threadIdx.x == 0) {
-            // rec_indexed: rec is the first record, and the box says which one
-            // this step writes (a replayed step's launches are all alike)
-            double *r = rec;
-            if (rec_indexed) {
-                if (r) r += (size_t)kThermoRec * (size_t)box->rec_step;
-                box->rec_step += 1;
-            }
-            therm_store(p, *box, s3, r);
-        }
-    }
-    if (threadIdx.x != 0) return;
-    BoxState &B = *box;
+// The list-rebuild decisions and the box advance of k_mid_decide, by one
+// thread on the block's shared copy of the box.
+__device__ void mid_decide_box(const Params &p, BoxState &B, double rmid, double rcut, double rout, int force,
+                               int half_build, int apply_box) {
     // register copies; the box is stored back once
     double b0[9], b1[9], b2[9], bb[9];
 #pragma unroll
@@ -382,6 +379,32 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
     }
     B.mid_rebuild = need;
     B.out_rebuild = need_out;
+}
+
+__global__ void __launch_bounds__(256)
+k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
+             int half_build, int apply_box, const double *__restrict__ therm_partials, int therm_nblk,
+             double *__restrict__ rec, int rec_indexed) {
+    __shared__ BoxState sbox;
+    box_load(sbox, box);
+    __syncthreads();
+    if (therm_nblk > 0) {
+        __shared__ double s3[3];
+        reduce_partials<3>(therm_partials, therm_nblk, s3);
+        if (threadIdx.x == 0) {
+            // rec_indexed: rec is the first record, and the box says which one
+            // this step writes (a replayed step's launches are all alike)
+            double *r = rec;
+            if (rec_indexed) {
+                if (r) r += (size_t)kThermoRec * (size_t)sbox.rec_step;
+                sbox.rec_step += 1;
+            }
+            therm_store(p, sbox, s3, r);
+        }
+    }
+    if (threadIdx.x == 0) mid_decide_box(p, sbox, rmid, rcut, rout, force, half_build, apply_box);
+    __syncthreads();
+    box_store(box, sbox);
 }
 
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
