@@ -433,6 +433,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Block-wide sum of NV values per thread into partials[blockIdx.x*kPartials + off + k].
 // Deterministic: fixed shuffle tree, then warps in order.
+// Programmatic dependent launch: a step kernel launched with programmatic
+// stream serialization (launch_pdl) may be scheduled while the kernel before
+// it drains; it waits here, before it reads or writes anything, until that
+// kernel has completed and its memory is visible.  A no-op for a kernel
+// launched without the attribute.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // The box state of a one-block kernel in shared memory: every thread loads
 // a share of it at once (one round of global loads instead of thread 0's
 // chain of dependent ones), thread 0 works on the copy, every thread stores

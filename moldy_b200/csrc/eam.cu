@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(256)
 k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict__ part_embed,
                  int nblk_embed, const double *__restrict__ part_force, int nblk_force,
                  const double *__restrict__ part_kin, int nblk_kin, int mode) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     // the box in shared memory, loaded while the partials are summed
     __shared__ BoxState sbox;
     box_load(sbox, box);
@@ -135,7 +136,7 @@ k_finalize_force(Params p, BoxState *__restrict__ box, const double *__restrict_
 void launch_finalize_force(DeviceState &d, const Params &p, const double *part_embed, int nblk_embed,
                            const double *part_force, int nblk_force, const double *part_kin, int nblk_kin,
                            int mode, cudaStream_t s) {
-    k_finalize_force<<<1, 256, 0, s>>>(p, d.box, part_embed, nblk_embed, part_force, nblk_force, part_kin, nblk_kin,
+    launch_pdl(k_finalize_force, 1, 256, s, p, d.box, part_embed, nblk_embed, part_force, nblk_force, part_kin, nblk_kin,
                                         mode);
 }
 
@@ -385,6 +386,7 @@ __global__ void __launch_bounds__(256)
 k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, double rout, int force,
              int half_build, int apply_box, const double *__restrict__ therm_partials, int therm_nblk,
              double *__restrict__ rec, int rec_indexed) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     __shared__ BoxState sbox;
     box_load(sbox, box);
     __syncthreads();
@@ -410,7 +412,7 @@ k_mid_decide(Params p, BoxState *__restrict__ box, double rmid, double rcut, dou
 void launch_mid_decide(DeviceState &d, const Params &p, double rmid, double rcut, double rout, int force,
                        int half_build, int apply_box, int therm_nblk, double *rec, cudaStream_t s,
                        int rec_indexed) {
-    k_mid_decide<<<1, 256, 0, s>>>(p, d.box, rmid, rcut, rout, force, half_build, apply_box, d.partials,
+    launch_pdl(k_mid_decide, 1, 256, s, p, d.box, rmid, rcut, rout, force, half_build, apply_box, d.partials,
                                    therm_nblk, rec, rec_indexed);
 }
 
@@ -435,6 +437,7 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
         const double *__restrict__ x1, const double *__restrict__ x2, BoxState *__restrict__ box,
         const int4 *__restrict__ xbuild, const double *__restrict__ mass, const int32_t *__restrict__ znum,
         double *__restrict__ kin_partials, double *__restrict__ therm_partials) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     // every thread forms the post-drift box exactly as thread 0 stores it
     __shared__ float nbs[9];   // that box per fixed-point unit
     __shared__ double sh[THERM ? 27 : 1];   // tgid, b0, cof(b0)/vol of the previous step
@@ -502,10 +505,10 @@ k_drift(Params p, double4 *__restrict__ pos, int4 *__restrict__ posq,
 int launch_drift(DeviceState &d, const Params &p, double *kin_partials, bool therm, cudaStream_t s) {
     int nb = stream_blocks(p.nm);
     if (therm)
-        k_drift<true><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+        launch_pdl(k_drift<true>, nb, kAtomThreads, s, p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
                                                   kin_partials, d.partials);
     else
-        k_drift<false><<<nb, kAtomThreads, 0, s>>>(p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
+        launch_pdl(k_drift<false>, nb, kAtomThreads, s, p, d.pos, d.posq, d.x1, d.x2, d.box, d.xbuild, d.mass, d.znum,
                                                    kin_partials, nullptr);
     return nb;
 }

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -275,6 +276,25 @@ inline int grid_blocks(long long work, int threads) {
     long long nb = (work + threads - 1) / threads;
     if (nb < 1) nb = 1;
     return (int)(nb < kMaxBlocks ? nb : kMaxBlocks);
+}
+
+// Launches a step kernel with programmatic stream serialization: the GPU may
+// start scheduling its blocks while the previous kernel on the stream drains
+// (the kernel calls grid_dep_wait before touching any data), which hides the
+// launch gap between the kernels of a step.
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // kernel launchers (defined in the .cu files)

@@ -61,7 +61,7 @@ static int one_wave(K kernel) {
     do {                                                     \
         static const int wave_ = one_wave(KERNEL);           \
         NB = NB < wave_ ? NB : wave_;                        \
-        KERNEL<<<NB, 256, 0, S>>>(__VA_ARGS__);              \
+        launch_pdl(KERNEL, NB, 256, S, __VA_ARGS__);         \
     } while (0)
 
 
@@ -164,6 +164,7 @@ k_screen_density(Params p, Tables t, const double4 *__restrict__ pos, const int4
                  int32_t *__restrict__ alist, int32_t *__restrict__ pair_cnt,
                  double *__restrict__ rho, double *__restrict__ afrho, double *__restrict__ dafrho,
                  double *__restrict__ partials, int32_t *__restrict__ flags, int store_rho) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     __shared__ double sb[9];
     __shared__ float srs2, srin2;
     if (threadIdx.x < 9) sb[threadIdx.x] = box->b0[threadIdx.x];
@@ -305,6 +306,7 @@ k_forces(Params p, Tables t, const double4 *__restrict__ pos2, const int4 *__res
          const int32_t *__restrict__ znum, const double *__restrict__ del2,
          double *__restrict__ f, double *__restrict__ x1, double *__restrict__ x2,
          double *__restrict__ stress, double *__restrict__ partials, int mode) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     __shared__ double sb[9], stg[9];
     __shared__ int slim[3];
     if (threadIdx.x < 9) {
@@ -581,6 +583,7 @@ k_list_build(Params p, double rout, double rmid, const double4 *__restrict__ pos
              int32_t *__restrict__ out_cnt, int4 *__restrict__ xout, const int4 *__restrict__ xhalf,
              int32_t *__restrict__ mlist, int32_t *__restrict__ mid_cnt, int4 *__restrict__ xbuild,
              int32_t *__restrict__ flags) {
+    grid_dep_wait();   // launched dependent on the step's previous kernel
     __shared__ double sb[9];
     __shared__ float skeep[2];
     __shared__ int sneed[2];
